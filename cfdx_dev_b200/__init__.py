@@ -1,0 +1,28 @@
+"""cfdx_dev_b200 -- B200-native CFDX pressure-correction hot path.
+
+Unstructured finite-volume pressure-correction assembly and Rhie-Chow face
+fluxes, plus the native-AMG-preconditioned GMRES/FGMRES solve, as sm_100a
+CUDA kernels behind a C ABI (include/cfdxg.h).  See ``api`` for the
+reference-shaped Python entry points.
+"""
+from .api import (  # noqa: F401
+    CfdxgError,
+    Context,
+    HostMesh,
+    Mesh,
+    NativeBoomerAMGPreconditioner,
+    SparseMatrix,
+    assemble_cell_diffusion_matrix,
+    assemble_pressure_correction,
+    boundary_layer_case,
+    fourier_field,
+    gauss_gradient_with_boundary,
+    hex_case,
+    make_request,
+    make_rhie_chow_mass_flux,
+    random_field,
+    solve_fgmres,
+    solve_gmres,
+    solve_linear_system,
+    tet_case,
+)

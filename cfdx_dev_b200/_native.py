@@ -1,0 +1,167 @@
+"""ctypes binding of libcfdxg.so (the C ABI declared in include/cfdxg.h).
+
+The library is built in-tree by ``python -m cfdx_dev_b200.build``.  Loading
+fails loudly if it is missing: there is no CPU fallback for the hot path.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from pathlib import Path
+
+LIB_PATH = Path(__file__).resolve().parent / "_lib" / "libcfdxg.so"
+
+CFDXG_MEM_HOST = 0
+CFDXG_MEM_DEVICE = 1
+KRYLOV = {"gmres": 3, "fgmres": 4}
+PRECONDITIONER = {"none": 1, "jacobi": 2, "native_amg": 6}
+PRECISION = {"fp64": 0, "fp32_vcycle": 1}
+STATUS = {0: "converged", 1: "max_iter_reached", 2: "diverged", 3: "not_applicable"}
+ERRORS = {
+    -1: "invalid_argument", -2: "cuda", -3: "setup", -4: "not_ready",
+    -5: "nonfinite", -6: "geometry", -7: "out_of_memory", -8: "io",
+}
+
+c_double_p = C.POINTER(C.c_double)
+c_float_p = C.POINTER(C.c_float)
+c_int64_p = C.POINTER(C.c_int64)
+c_int32_p = C.POINTER(C.c_int32)
+
+
+class MeshDesc(C.Structure):
+    _fields_ = [
+        ("n_points", C.c_int64), ("n_faces", C.c_int64), ("n_cells", C.c_int64),
+        ("px", c_double_p), ("py", c_double_p), ("pz", c_double_p),
+        ("face_offsets", c_int64_p), ("face_vertices", c_int64_p),
+        ("owner", c_int64_p), ("neighbour", c_int64_p),
+        ("cell_offsets", c_int64_p), ("cell_faces", c_int64_p),
+        ("n_patches", C.c_int32), ("patch_of_face", c_int32_p), ("patch_types", c_int32_p),
+    ]
+
+
+class AmgOptions(C.Structure):
+    _fields_ = [
+        ("omega", C.c_double), ("pre_sweeps", C.c_int32), ("post_sweeps", C.c_int32),
+        ("strength_threshold", C.c_double), ("max_levels", C.c_int32),
+        ("require_smoother_certificate", C.c_int32), ("precision", C.c_int32),
+        ("coarse_dense_limit", C.c_int32),
+    ]
+
+
+class Request(C.Structure):
+    _fields_ = [
+        ("krylov", C.c_int32), ("preconditioner", C.c_int32), ("gmres_restart", C.c_int32),
+        ("precision", C.c_int32), ("restart_min", C.c_int32), ("restart_max", C.c_int32),
+        ("adaptive_restart", C.c_int32), ("residual_replacement", C.c_int32),
+        ("residual_replacement_period", C.c_int64), ("residual_replacement_gap_ratio", C.c_double),
+        ("target_reduction_per_cycle", C.c_double), ("learned", C.c_void_p),
+    ]
+
+
+class Report(C.Structure):
+    _fields_ = [
+        ("status", C.c_int32), ("iterations", C.c_int64), ("residual", C.c_double),
+        ("residual_relative", C.c_double), ("physical_residual_relative", C.c_double),
+        ("residual_replacements", C.c_int64), ("max_true_recursive_gap", C.c_double),
+        ("setup_seconds", C.c_double), ("solve_seconds", C.c_double),
+        ("preconditioner_applications", C.c_int64), ("learned_fallbacks", C.c_int64),
+    ]
+
+    def as_dict(self) -> dict:
+        d = {name: getattr(self, name) for name, _ in self._fields_}
+        d["status_name"] = STATUS.get(self.status, ERRORS.get(self.status, str(self.status)))
+        return d
+
+
+_V = C.c_void_p
+_P = C.POINTER
+# name -> (restype, argtypes)
+PROTOTYPES = {
+    "cfdxg_context_create": (C.c_int, [C.c_int32, _P(_V)]),
+    "cfdxg_context_destroy": (C.c_int, [_V]),
+    "cfdxg_last_error": (C.c_char_p, [_V]),
+    "cfdxg_kernel_launches": (C.c_int64, [_V]),
+    "cfdxg_synchronize": (C.c_int, [_V]),
+    "cfdxg_mesh_upload": (C.c_int, [_V, _P(MeshDesc), _P(_V)]),
+    "cfdxg_mesh_destroy": (C.c_int, [_V]),
+    "cfdxg_geometry_build": (C.c_int, [_V, _V]),
+    "cfdxg_geometry_download": (C.c_int, [_V, _V, _V, _V, _V, _V]),
+    "cfdxg_matrix_create": (C.c_int, [_V, C.c_int64, _V, _V, _V, C.c_int32, _P(_V)]),
+    "cfdxg_matrix_destroy": (C.c_int, [_V]),
+    "cfdxg_matrix_size": (C.c_int, [_V, c_int64_p, c_int64_p]),
+    "cfdxg_matrix_download": (C.c_int, [_V, _V, _V, _V, _V]),
+    "cfdxg_matrix_spmv": (C.c_int, [_V, _V, _V, _V, C.c_int32]),
+    "cfdxg_assemble_cell_diffusion": (C.c_int, [_V, _V, _V, _V, C.c_double, _V, C.c_int32, _P(_V), _V]),
+    "cfdxg_assemble_pressure_correction": (
+        C.c_int, [_V, _V, _V, _V, _V, C.c_double, _V, _V, C.c_int32, _P(_V), _V, _V, _V]),
+    "cfdxg_rhie_chow_flux": (C.c_int, [_V, _V, _V, _V, _V, C.c_double, _V, _V, C.c_int32, _V]),
+    "cfdxg_gauss_gradient": (C.c_int, [_V, _V, _V, _V, _V, C.c_int32, _V]),
+    "cfdxg_amg_options_default": (C.c_int, [_P(AmgOptions)]),
+    "cfdxg_amg_create": (C.c_int, [_V, _P(AmgOptions), _P(_V)]),
+    "cfdxg_amg_destroy": (C.c_int, [_V]),
+    "cfdxg_amg_setup": (C.c_int, [_V, _V, _V]),
+    "cfdxg_amg_setup_host": (C.c_int, [_V, C.c_int64, _V, _V, _V]),
+    "cfdxg_amg_update_values": (C.c_int, [_V, _V, _V]),
+    "cfdxg_amg_apply": (C.c_int, [_V, _V, _V, _V, C.c_int32]),
+    "cfdxg_amg_name": (C.c_char_p, [_V]),
+    "cfdxg_amg_last_error": (C.c_char_p, [_V]),
+    "cfdxg_amg_num_levels": (C.c_int32, [_V]),
+    "cfdxg_amg_omega": (C.c_double, [_V]),
+    "cfdxg_amg_level_info": (C.c_int, [_V, C.c_int32, c_int64_p, c_int64_p, c_int64_p]),
+    "cfdxg_amg_export_level": (C.c_int, [_V, C.c_int32, _V, _V, _V, _V, _V, _V, _V, _V]),
+    "cfdxg_amg_setup_seconds": (C.c_double, [_V]),
+    "cfdxg_request_default": (C.c_int, [_P(Request)]),
+    "cfdxg_solve_linear_system": (
+        C.c_int, [_V, _V, _V, _V, C.c_int32, _P(Request), C.c_int64, C.c_double, _P(Report)]),
+    "cfdxg_solve_gmres": (
+        C.c_int, [_V, _V, _V, _V, _V, C.c_int32, _P(Request), C.c_int64, C.c_double, _P(Report)]),
+    "cfdxg_case_hex": (C.c_int, [C.c_int64, C.c_int64, C.c_int64, _P(_V)]),
+    "cfdxg_case_tet": (C.c_int, [C.c_int64, C.c_double, C.c_uint64, _P(_V)]),
+    "cfdxg_case_boundary_layer": (
+        C.c_int, [C.c_int64, C.c_int64, C.c_int64, C.c_double, C.c_double, C.c_double, C.c_double,
+                  C.c_double, C.c_uint64, _P(_V)]),
+    "cfdxg_case_destroy": (C.c_int, [_V]),
+    "cfdxg_case_sizes": (C.c_int, [_V, c_int64_p]),
+    "cfdxg_case_export": (C.c_int, [_V] + [_V] * 11),
+    "cfdxg_field_fourier": (C.c_int, [C.c_int64, _V, C.c_int32, C.c_double, C.c_uint64, _V]),
+    "cfdxg_field_random": (C.c_int, [C.c_int64, C.c_int32, C.c_double, C.c_double, C.c_uint64, _V]),
+    "cfdxg_mpnn_create": (C.c_int, [_V, C.c_uint64, _P(_V)]),
+    "cfdxg_mpnn_destroy": (C.c_int, [_V]),
+    "cfdxg_mpnn_num_parameters": (C.c_int, [_V, c_int64_p]),
+    "cfdxg_mpnn_get_parameters": (C.c_int, [_V, _V, _V]),
+    "cfdxg_mpnn_set_parameters": (C.c_int, [_V, _V, _V]),
+    "cfdxg_mpnn_save": (C.c_int, [_V, _V, C.c_char_p]),
+    "cfdxg_mpnn_load": (C.c_int, [_V, _V, C.c_char_p]),
+    "cfdxg_mpnn_bind": (C.c_int, [_V, _V, _V, _V, _V, C.c_int32]),
+    "cfdxg_mpnn_apply": (C.c_int, [_V, _V, _V, _V, C.c_int32]),
+    "cfdxg_mpnn_train_step": (C.c_int, [_V, _V, _V, _V, C.c_int32, C.c_float, C.c_int32, c_double_p]),
+    "cfdxg_mpnn_loss_grad": (C.c_int, [_V, _V, _V, _V, C.c_int32, C.c_int32, c_double_p, _V]),
+}
+
+_lib = None
+
+
+def load() -> C.CDLL:
+    """Load libcfdxg.so (built in-tree).  Raises if it has not been built."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not LIB_PATH.exists():
+        raise RuntimeError(
+            f"{LIB_PATH} is missing: build it with `python -m cfdx_dev_b200.build` "
+            "(the CUDA path has no CPU fallback)")
+    lib = C.CDLL(str(LIB_PATH))
+    for name, (res, args) in PROTOTYPES.items():
+        fn = getattr(lib, name, None)
+        if fn is None:
+            continue
+        fn.restype = res
+        fn.argtypes = args
+    _lib = lib
+    return lib
+
+
+def ptr(a):
+    """Raw data pointer of a numpy array (or None)."""
+    if a is None:
+        return None
+    return a.ctypes.data_as(C.c_void_p)

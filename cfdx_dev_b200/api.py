@@ -1,0 +1,481 @@
+"""Python mirror of the reference's pressure-path API over the C ABI.
+
+Names and argument meanings follow the reference (stevendaix/cfdx_dev):
+
+* ``assemble_cell_diffusion_matrix``  -- core/solvers/scalar_diffusion.h:39
+* ``assemble_pressure_correction``    -- physics/steady_incompressible_solver.h:8048-8181
+* ``make_rhie_chow_mass_flux``        -- physics/steady_incompressible_solver.h:2064
+* ``gauss_gradient_with_boundary``    -- physics/steady_incompressible_solver.h:1634
+* ``NativeBoomerAMGPreconditioner``   -- core/linalg/hypre_amg.h:106 (setup / update_values /
+                                         apply / name / last_error)
+* ``solve_linear_system``             -- core/linalg/linear_solver_dispatch.h:227
+* ``solve_gmres`` / ``solve_fgmres``  -- core/linalg/gmres_solver.h:28, 612
+
+Errors surface as :class:`CfdxgError` (bad requests raise, like the
+reference's ``std::invalid_argument``); solver outcomes are reported through
+``report["status_name"]`` as the reference's ``SolverStatus``.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass
+
+import numpy as np
+
+from . import _native as N
+
+
+class CfdxgError(RuntimeError):
+    def __init__(self, code: int, message: str):
+        super().__init__(f"{N.ERRORS.get(code, code)}: {message}")
+        self.code = code
+
+
+def _f64(a, n=None):
+    a = np.ascontiguousarray(a, dtype=np.float64)
+    if n is not None and a.size != n:
+        raise ValueError(f"expected {n} values, got {a.size}")
+    return a
+
+
+def _i64(a):
+    return np.ascontiguousarray(a, dtype=np.int64)
+
+
+def _i32(a):
+    return np.ascontiguousarray(a, dtype=np.int32)
+
+
+class Context:
+    """A CUDA device + stream owned by the library (cfdxg_context)."""
+
+    def __init__(self, device: int = 0):
+        self.lib = N.load()
+        h = C.c_void_p()
+        rc = self.lib.cfdxg_context_create(device, C.byref(h))
+        if rc != 0:
+            raise CfdxgError(rc, f"cannot create a context on device {device}")
+        self.handle = h
+
+    def check(self, rc: int, what: str = "") -> int:
+        if rc < 0:
+            msg = self.lib.cfdxg_last_error(self.handle).decode()
+            raise CfdxgError(rc, f"{what}: {msg}" if what else msg)
+        return rc
+
+    @property
+    def kernel_launches(self) -> int:
+        return int(self.lib.cfdxg_kernel_launches(self.handle))
+
+    def synchronize(self):
+        self.check(self.lib.cfdxg_synchronize(self.handle))
+
+    def close(self):
+        if getattr(self, "handle", None):
+            self.lib.cfdxg_context_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):  # pragma: no cover - best effort
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+# ---------------------------------------------------------------- meshes
+@dataclass
+class HostMesh:
+    """A mesh as flat host arrays (the reference's Mesh contents, core/mesh/mesh.h:51)."""
+    px: np.ndarray
+    py: np.ndarray
+    pz: np.ndarray
+    face_offsets: np.ndarray
+    face_vertices: np.ndarray
+    owner: np.ndarray
+    neighbour: np.ndarray
+    cell_offsets: np.ndarray
+    cell_faces: np.ndarray
+    patch_of_face: np.ndarray
+    patch_types: np.ndarray
+
+    @property
+    def n_points(self):
+        return self.px.size
+
+    @property
+    def n_faces(self):
+        return self.owner.size
+
+    @property
+    def n_cells(self):
+        return self.cell_offsets.size - 1
+
+    @property
+    def n_patches(self):
+        return self.patch_types.size
+
+    def desc(self) -> N.MeshDesc:
+        d = N.MeshDesc()
+        d.n_points, d.n_faces, d.n_cells = self.n_points, self.n_faces, self.n_cells
+        for name in ("px", "py", "pz"):
+            setattr(d, name, getattr(self, name).ctypes.data_as(N.c_double_p))
+        for name in ("face_offsets", "face_vertices", "owner", "neighbour", "cell_offsets", "cell_faces"):
+            setattr(d, name, getattr(self, name).ctypes.data_as(N.c_int64_p))
+        d.n_patches = self.n_patches
+        d.patch_of_face = self.patch_of_face.ctypes.data_as(N.c_int32_p)
+        d.patch_types = self.patch_types.ctypes.data_as(N.c_int32_p)
+        return d
+
+
+def _case_to_mesh(lib, h) -> HostMesh:
+    sizes = np.zeros(6, dtype=np.int64)
+    lib.cfdxg_case_sizes(h, sizes.ctypes.data_as(N.c_int64_p))
+    npnt, nf, nfv, nc, ncf, npat = (int(v) for v in sizes)
+    m = HostMesh(
+        px=np.empty(npnt), py=np.empty(npnt), pz=np.empty(npnt),
+        face_offsets=np.empty(nf + 1, np.int64), face_vertices=np.empty(nfv, np.int64),
+        owner=np.empty(nf, np.int64), neighbour=np.empty(nf, np.int64),
+        cell_offsets=np.empty(nc + 1, np.int64), cell_faces=np.empty(ncf, np.int64),
+        patch_of_face=np.empty(nf, np.int32), patch_types=np.empty(npat, np.int32))
+    lib.cfdxg_case_export(h, *(N.ptr(getattr(m, f)) for f in (
+        "px", "py", "pz", "face_offsets", "face_vertices", "owner", "neighbour", "cell_offsets",
+        "cell_faces", "patch_of_face", "patch_types")))
+    lib.cfdxg_case_destroy(h)
+    return m
+
+
+def hex_case(nx: int, ny: int | None = None, nz: int | None = None) -> HostMesh:
+    """Hex lattice on the unit cube (reference hex-fixture numbering)."""
+    lib = N.load()
+    h = C.c_void_p()
+    rc = lib.cfdxg_case_hex(nx, ny or nx, nz or nx, C.byref(h))
+    if rc != 0:
+        raise CfdxgError(rc, "hex case")
+    return _case_to_mesh(lib, h)
+
+
+def tet_case(n: int, jitter: float = 0.0, seed: int = 0) -> HostMesh:
+    """Kuhn 6-tet split of an n^3 lattice (reference tet-fixture numbering), jittered."""
+    lib = N.load()
+    h = C.c_void_p()
+    rc = lib.cfdxg_case_tet(n, jitter, seed, C.byref(h))
+    if rc != 0:
+        raise CfdxgError(rc, "tet case")
+    return _case_to_mesh(lib, h)
+
+
+def boundary_layer_case(nx, ny, nz, lx=10.0, lz=1.0, dy0=1e-4, growth=1.08, jitter=0.05, seed=0) -> HostMesh:
+    lib = N.load()
+    h = C.c_void_p()
+    rc = lib.cfdxg_case_boundary_layer(nx, ny, nz, lx, lz, dy0, growth, jitter, seed, C.byref(h))
+    if rc != 0:
+        raise CfdxgError(rc, "boundary-layer case")
+    return _case_to_mesh(lib, h)
+
+
+def fourier_field(centres: np.ndarray, n_modes: int = 8, perturbation: float = 0.01, seed: int = 0):
+    lib = N.load()
+    centres = _f64(centres)
+    n = centres.size // 3
+    u = np.empty(3 * n)
+    rc = lib.cfdxg_field_fourier(n, N.ptr(centres), n_modes, perturbation, seed, N.ptr(u))
+    if rc != 0:
+        raise CfdxgError(rc, "fourier field")
+    return u
+
+
+def random_field(n: int, kind: str, lo: float, hi: float, seed: int):
+    lib = N.load()
+    v = np.empty(n)
+    rc = lib.cfdxg_field_random(n, 0 if kind == "loguniform" else 1, lo, hi, seed, N.ptr(v))
+    if rc != 0:
+        raise CfdxgError(rc, "random field")
+    return v
+
+
+class Mesh:
+    """A mesh resident on the device (cfdxg_mesh) with its GPU-built geometry."""
+
+    def __init__(self, ctx: Context, host: HostMesh, build_geometry: bool = True):
+        self.ctx, self.host = ctx, host
+        h = C.c_void_p()
+        d = host.desc()
+        ctx.check(ctx.lib.cfdxg_mesh_upload(ctx.handle, C.byref(d), C.byref(h)), "mesh upload")
+        self.handle = h
+        if build_geometry:
+            self.build_geometry()
+
+    def build_geometry(self):
+        self.ctx.check(self.ctx.lib.cfdxg_geometry_build(self.ctx.handle, self.handle), "geometry")
+
+    def geometry(self) -> dict:
+        nf, nc = self.host.n_faces, self.host.n_cells
+        out = dict(face_centres=np.empty(3 * nf), face_Sf=np.empty(3 * nf),
+                   cell_centres=np.empty(3 * nc), cell_volumes=np.empty(nc))
+        self.ctx.check(self.ctx.lib.cfdxg_geometry_download(
+            self.ctx.handle, self.handle, *(N.ptr(out[k]) for k in
+                                            ("face_centres", "face_Sf", "cell_centres", "cell_volumes"))))
+        return out
+
+    def __del__(self):  # pragma: no cover
+        try:
+            if self.handle:
+                self.ctx.lib.cfdxg_mesh_destroy(self.handle)
+                self.handle = None
+        except Exception:
+            pass
+
+
+class SparseMatrix:
+    """Device CSR (cfdxg_matrix), the reference's SparseMatrix (core/linalg/sparse_matrix.h:27)."""
+
+    def __init__(self, ctx: Context, handle):
+        self.ctx, self.handle = ctx, handle
+        n, nnz = C.c_int64(), C.c_int64()
+        ctx.lib.cfdxg_matrix_size(handle, C.byref(n), C.byref(nnz))
+        self.n, self.nnz = n.value, nnz.value
+
+    @classmethod
+    def from_csr(cls, ctx: Context, row_offsets, columns, values):
+        ro, co, va = _i64(row_offsets), _i64(columns), _f64(values)
+        h = C.c_void_p()
+        ctx.check(ctx.lib.cfdxg_matrix_create(ctx.handle, ro.size - 1, N.ptr(ro), N.ptr(co), N.ptr(va),
+                                              N.CFDXG_MEM_HOST, C.byref(h)), "matrix")
+        return cls(ctx, h)
+
+    def to_csr(self):
+        ro = np.empty(self.n + 1, np.int64)
+        co = np.empty(self.nnz, np.int64)
+        va = np.empty(self.nnz)
+        self.ctx.check(self.ctx.lib.cfdxg_matrix_download(self.ctx.handle, self.handle, N.ptr(ro), N.ptr(co),
+                                                          N.ptr(va)))
+        return ro, co, va
+
+    def matvec(self, x):
+        x = _f64(x, self.n)
+        y = np.empty(self.n)
+        self.ctx.check(self.ctx.lib.cfdxg_matrix_spmv(self.ctx.handle, self.handle, N.ptr(x), N.ptr(y),
+                                                      N.CFDXG_MEM_HOST))
+        return y
+
+    def __del__(self):  # pragma: no cover
+        try:
+            if self.handle:
+                self.ctx.lib.cfdxg_matrix_destroy(self.handle)
+                self.handle = None
+        except Exception:
+            pass
+
+
+def _bc_arrays(mesh_host: HostMesh, fixed, value):
+    npat = mesh_host.n_patches
+    f = np.zeros(npat, np.int32) if fixed is None else _i32(fixed)
+    v = np.zeros(npat) if value is None else _f64(value)
+    return f, v
+
+
+def assemble_cell_diffusion_matrix(mesh: Mesh, bc_face_values, diffusivity, source, bc_face_types=None):
+    """core/solvers/scalar_diffusion.h:39-163 -> (SparseMatrix, rhs)."""
+    ctx = mesh.ctx
+    bcv = _f64(bc_face_values, mesh.host.n_faces)
+    bct = None if bc_face_types is None else _i32(bc_face_types)
+    src = _f64(source, mesh.host.n_cells)
+    rhs = np.empty(mesh.host.n_cells)
+    h = C.c_void_p()
+    ctx.check(ctx.lib.cfdxg_assemble_cell_diffusion(ctx.handle, mesh.handle, N.ptr(bcv), N.ptr(bct),
+                                                    float(diffusivity), N.ptr(src), N.CFDXG_MEM_HOST,
+                                                    C.byref(h), N.ptr(rhs)), "assemble_cell_diffusion_matrix")
+    return SparseMatrix(ctx, h), rhs
+
+
+def assemble_pressure_correction(mesh: Mesh, HbyA, rAU, p, rho=1.0, p_bc_fixed=None, p_bc_value=None,
+                                 matrix: SparseMatrix | None = None):
+    """Pressure-corrector assembly (steady_incompressible_solver.h:8048-8181).
+
+    Returns (A, b, phiHbyA, grad_p)."""
+    ctx, hm = mesh.ctx, mesh.host
+    U, r, pp = _f64(HbyA, 3 * hm.n_cells), _f64(rAU, 3 * hm.n_cells), _f64(p, hm.n_cells)
+    f, v = _bc_arrays(hm, p_bc_fixed, p_bc_value)
+    b = np.empty(hm.n_cells)
+    phi = np.empty(hm.n_faces)
+    grad = np.empty(3 * hm.n_cells)
+    h = C.c_void_p(matrix.handle.value if matrix is not None else None)
+    ctx.check(ctx.lib.cfdxg_assemble_pressure_correction(
+        ctx.handle, mesh.handle, N.ptr(U), N.ptr(r), N.ptr(pp), float(rho), N.ptr(f), N.ptr(v),
+        N.CFDXG_MEM_HOST, C.byref(h), N.ptr(b), N.ptr(phi), N.ptr(grad)), "pressure-correction assembly")
+    A = matrix if matrix is not None else SparseMatrix(ctx, h)
+    return A, b, phi, grad
+
+
+def make_rhie_chow_mass_flux(mesh: Mesh, HbyA, rAU, p, rho=1.0, p_bc_fixed=None, p_bc_value=None):
+    """physics/steady_incompressible_solver.h:2064-2217 (HBYA_PREDICTOR contract)."""
+    ctx, hm = mesh.ctx, mesh.host
+    U, r, pp = _f64(HbyA, 3 * hm.n_cells), _f64(rAU, 3 * hm.n_cells), _f64(p, hm.n_cells)
+    f, v = _bc_arrays(hm, p_bc_fixed, p_bc_value)
+    flux = np.empty(hm.n_faces)
+    ctx.check(ctx.lib.cfdxg_rhie_chow_flux(ctx.handle, mesh.handle, N.ptr(U), N.ptr(r), N.ptr(pp), float(rho),
+                                           N.ptr(f), N.ptr(v), N.CFDXG_MEM_HOST, N.ptr(flux)),
+              "make_rhie_chow_mass_flux")
+    return flux
+
+
+def gauss_gradient_with_boundary(mesh: Mesh, p, p_bc_fixed=None, p_bc_value=None):
+    ctx, hm = mesh.ctx, mesh.host
+    pp = _f64(p, hm.n_cells)
+    f, v = _bc_arrays(hm, p_bc_fixed, p_bc_value)
+    g = np.empty(3 * hm.n_cells)
+    ctx.check(ctx.lib.cfdxg_gauss_gradient(ctx.handle, mesh.handle, N.ptr(pp), N.ptr(f), N.ptr(v),
+                                           N.CFDXG_MEM_HOST, N.ptr(g)), "gauss_gradient_with_boundary")
+    return g
+
+
+# ---------------------------------------------------------------- AMG
+class NativeBoomerAMGPreconditioner:
+    """Native classical RS AMG (core/linalg/hypre_amg.h:106), GPU V-cycle.
+
+    ``precision="fp32_vcycle"`` runs the V-cycle in FP32 with an FP64 dense
+    coarse solve (the hierarchy itself is identical)."""
+
+    def __init__(self, ctx: Context | None = None, precision: str = "fp64", require_smoother_certificate=False,
+                 **options):
+        self.ctx = ctx
+        self.lib = N.load()
+        o = N.AmgOptions()
+        self.lib.cfdxg_amg_options_default(C.byref(o))
+        o.precision = N.PRECISION[precision]
+        o.require_smoother_certificate = int(bool(require_smoother_certificate))
+        for k, v in options.items():
+            setattr(o, k, v)
+        h = C.c_void_p()
+        rc = self.lib.cfdxg_amg_create(ctx.handle if ctx else None, C.byref(o), C.byref(h))
+        if rc != 0:
+            raise CfdxgError(rc, "AMG options")
+        self.handle = h
+
+    def setup(self, A: SparseMatrix) -> bool:
+        rc = self.lib.cfdxg_amg_setup(self.ctx.handle, self.handle, A.handle)
+        if rc == -3:
+            return False
+        self.ctx.check(rc, "AMG setup")
+        return True
+
+    def setup_host(self, row_offsets, columns, values) -> bool:
+        ro, co, va = _i64(row_offsets), _i64(columns), _f64(values)
+        rc = self.lib.cfdxg_amg_setup_host(self.handle, ro.size - 1, N.ptr(ro), N.ptr(co), N.ptr(va))
+        if rc == -3:
+            return False
+        if rc != 0:
+            raise CfdxgError(rc, self.last_error())
+        return True
+
+    def update_values(self, A: SparseMatrix) -> bool:
+        rc = self.lib.cfdxg_amg_update_values(self.ctx.handle, self.handle, A.handle)
+        if rc == -3:
+            return False
+        self.ctx.check(rc, "AMG update_values")
+        return True
+
+    def apply(self, r) -> np.ndarray:
+        r = _f64(r)
+        z = np.empty_like(r)
+        self.ctx.check(self.lib.cfdxg_amg_apply(self.ctx.handle, self.handle, N.ptr(r), N.ptr(z), N.CFDXG_MEM_HOST),
+                       "AMG apply")
+        return z
+
+    def name(self) -> str:
+        return self.lib.cfdxg_amg_name(self.handle).decode()
+
+    def last_error(self) -> str:
+        return self.lib.cfdxg_amg_last_error(self.handle).decode()
+
+    @property
+    def omega(self) -> float:
+        return float(self.lib.cfdxg_amg_omega(self.handle))
+
+    @property
+    def setup_seconds(self) -> float:
+        return float(self.lib.cfdxg_amg_setup_seconds(self.handle))
+
+    def hierarchy_level_sizes(self):
+        return [self._info(l)[0] for l in range(self.lib.cfdxg_amg_num_levels(self.handle))]
+
+    def hierarchy_level_nnz(self):
+        return [self._info(l)[1] for l in range(self.lib.cfdxg_amg_num_levels(self.handle))]
+
+    def operator_complexity(self) -> float:
+        nnz = self.hierarchy_level_nnz()
+        return sum(nnz) / nnz[0] if nnz else 0.0
+
+    def _info(self, level):
+        n, nnz, pn = C.c_int64(), C.c_int64(), C.c_int64()
+        self.lib.cfdxg_amg_level_info(self.handle, level, C.byref(n), C.byref(nnz), C.byref(pn))
+        return n.value, nnz.value, pn.value
+
+    def export_level(self, level: int) -> dict:
+        n, nnz, pn = self._info(level)
+        out = dict(row_offsets=np.empty(n + 1, np.int64), columns=np.empty(nnz, np.int64), values=np.empty(nnz),
+                   inv_diag=np.empty(n), p_offsets=np.empty(n + 1, np.int64), p_columns=np.empty(pn, np.int64),
+                   p_values=np.empty(pn), aggregate=np.empty(n, np.int64))
+        rc = self.lib.cfdxg_amg_export_level(self.handle, level, *(N.ptr(out[k]) for k in (
+            "row_offsets", "columns", "values", "inv_diag", "p_offsets", "p_columns", "p_values", "aggregate")))
+        if rc != 0:
+            raise CfdxgError(rc, "export level")
+        if pn == 0:
+            out["p_offsets"] = None
+            out["aggregate"] = None
+        return out
+
+    def __del__(self):  # pragma: no cover
+        try:
+            if self.handle:
+                self.lib.cfdxg_amg_destroy(self.handle)
+                self.handle = None
+        except Exception:
+            pass
+
+
+def make_request(krylov="gmres", preconditioner="native_amg", restart=40, precision="fp64", learned=None, **kw):
+    lib = N.load()
+    r = N.Request()
+    lib.cfdxg_request_default(C.byref(r))
+    r.krylov = N.KRYLOV[krylov]
+    r.preconditioner = N.PRECONDITIONER[preconditioner]
+    r.gmres_restart = restart
+    r.precision = N.PRECISION[precision]
+    r.learned = learned.handle if learned is not None else None
+    for k, v in kw.items():
+        setattr(r, k, v)
+    return r
+
+
+def solve_linear_system(A: SparseMatrix, rhs, x0=None, krylov="gmres", preconditioner="native_amg",
+                        restart=40, precision="fp64", max_iterations=1000, tolerance=1e-12, learned=None, **kw):
+    """core/linalg/linear_solver_dispatch.h:227 for PressurePoisson systems -> (x, report)."""
+    ctx = A.ctx
+    b = _f64(rhs, A.n)
+    x = np.zeros(A.n) if x0 is None else _f64(x0, A.n).copy()
+    req = make_request(krylov, preconditioner, restart, precision, learned, **kw)
+    rep = N.Report()
+    rc = ctx.lib.cfdxg_solve_linear_system(ctx.handle, A.handle, N.ptr(b), N.ptr(x), N.CFDXG_MEM_HOST,
+                                           C.byref(req), int(max_iterations), float(tolerance), C.byref(rep))
+    ctx.check(rc, "solve_linear_system")
+    return x, rep.as_dict()
+
+
+def solve_gmres(A: SparseMatrix, rhs, x0=None, amg: NativeBoomerAMGPreconditioner | None = None, restart=30,
+                max_iterations=1000, tolerance=1e-12, krylov="gmres", learned=None, **kw):
+    """core/linalg/gmres_solver.h:28 with a prepared preconditioner -> (x, report)."""
+    ctx = A.ctx
+    b = _f64(rhs, A.n)
+    x = np.zeros(A.n) if x0 is None else _f64(x0, A.n).copy()
+    req = make_request(krylov, "native_amg" if amg else "none", restart, "fp64", learned, **kw)
+    rep = N.Report()
+    rc = ctx.lib.cfdxg_solve_gmres(ctx.handle, A.handle, amg.handle if amg else None, N.ptr(b), N.ptr(x),
+                                   N.CFDXG_MEM_HOST, C.byref(req), int(max_iterations), float(tolerance),
+                                   C.byref(rep))
+    ctx.check(rc, "solve_gmres")
+    return x, rep.as_dict()
+
+
+def solve_fgmres(A, rhs, x0=None, amg=None, restart=30, max_iterations=1000, tolerance=1e-12, **kw):
+    return solve_gmres(A, rhs, x0, amg, restart, max_iterations, tolerance, krylov="fgmres", **kw)

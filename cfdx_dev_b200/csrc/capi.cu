@@ -1,0 +1,587 @@
+// capi.cu -- C ABI: contexts, matrices, the native AMG preconditioner and the
+// solve_linear_system / solve_gmres entry points.
+#include <chrono>
+#include <cmath>
+#include <cstring>
+
+#include "io.h"
+#include "krylov.h"
+
+using namespace cfdxg;
+
+namespace {
+
+double now_seconds() {
+    using clock = std::chrono::steady_clock;
+    return std::chrono::duration<double>(clock::now().time_since_epoch()).count();
+}
+
+// JacobiPreconditioner (core/linalg/preconditioner.h:60-90): inverse of the first
+// diagonal entry of each row.
+__global__ void k_first_diag_inverse(int n, const int* ro, const int* co, const double* va, double* inv, int* status) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    for (int k = ro[i]; k < ro[i + 1]; ++k)
+        if (co[k] == i) {
+            const double v = 1.0 / va[k];
+            if (!isfinite(v)) atomicOr(status, kStatusNonFinite);
+            inv[i] = v;
+            return;
+        }
+    atomicOr(status, kStatusNonFinite);
+}
+
+__global__ void k_scale(int n, const double* a, const double* b, double* out) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) out[i] = a[i] * b[i];
+}
+
+__global__ void k_check_finite(int n, const double* a, int* status) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n && !isfinite(a[i])) atomicOr(status, kStatusNonFinite);
+}
+
+KrylovControls controls_from(const cfdxg_request& r) {
+    KrylovControls c;
+    c.restart_min = r.restart_min;
+    c.restart_max = r.restart_max;
+    c.adaptive_restart = r.adaptive_restart != 0;
+    c.residual_replacement = r.residual_replacement != 0;
+    c.residual_replacement_period = r.residual_replacement_period;
+    c.residual_replacement_gap_ratio = r.residual_replacement_gap_ratio;
+    c.target_reduction_per_cycle = r.target_reduction_per_cycle;
+    return c;
+}
+
+void fill_report(cfdxg_report* rep, const KrylovResult& r) {
+    if (!rep) return;
+    rep->status = r.status;
+    rep->iterations = r.iterations;
+    rep->residual = r.residual;
+    rep->residual_relative = r.residual_relative;
+    rep->residual_replacements = r.residual_replacements;
+    rep->max_true_recursive_gap = r.max_true_recursive_gap;
+    rep->preconditioner_applications = r.preconditioner_applications;
+}
+
+void amg_setup_impl(cfdxg_context* ctx, cfdxg_amg* amg, cfdxg_matrix* A) {
+    const double t0 = now_seconds();
+    matrix_sync_host_values(ctx, A);
+    AmgOptions o;
+    o.omega = amg->opts.omega;
+    o.pre = amg->opts.pre_sweeps;
+    o.post = amg->opts.post_sweeps;
+    o.strength_threshold = amg->opts.strength_threshold;
+    o.max_levels = amg->opts.max_levels;
+    o.require_smoother_certificate = amg->opts.require_smoother_certificate != 0;
+    AmgHierarchy staged;
+    std::string err;
+    if (!amg_setup(A->host, o, staged, err)) {
+        amg->error = "native AMG hierarchy construction failed: " + err;
+        throw Error(CFDXG_ERR_SETUP, amg->error);
+    }
+    std::unique_ptr<DevHierarchy<double>> d64;
+    std::unique_ptr<DevHierarchy<float>> d32;
+    if (amg->opts.precision == CFDXG_PRECISION_FP32_VCYCLE)
+        d32 = upload_hierarchy<float>(ctx, staged, amg->opts.coarse_dense_limit);
+    else
+        d64 = upload_hierarchy<double>(ctx, staged, 0);
+    // commit only after every stage succeeded (hypre_amg.cpp:163-236 is transactional)
+    amg->host = std::move(staged);
+    amg->d64 = std::move(d64);
+    amg->d32 = std::move(d32);
+    amg->ready = true;
+    amg->error.clear();
+    amg->setup_seconds = now_seconds() - t0;
+}
+
+void amg_apply_device(cfdxg_context* ctx, cfdxg_amg* amg, const double* r, double* z) {
+    if (amg->d32) vcycle_apply<float>(ctx, *amg->d32, r, z);
+    else vcycle_apply<double>(ctx, *amg->d64, r, z);
+    ++amg->applications;
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------- context
+extern "C" int cfdxg_context_create(int32_t device, cfdxg_context** out) {
+    if (!out) return CFDXG_ERR_INVALID_ARGUMENT;
+    auto* ctx = new (std::nothrow) cfdxg_context();
+    if (!ctx) return CFDXG_ERR_OUT_OF_MEMORY;
+    try {
+        CFDXG_CUDA(cudaSetDevice(device));
+        ctx->device = device;
+        CFDXG_CUDA(cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking));
+        CFDXG_CUDA(cudaDeviceGetAttribute(&ctx->sm_count, cudaDevAttrMultiProcessorCount, device));
+        CFDXG_CUDA(cudaMalloc(&ctx->scratch.partial, sizeof(double) * kMaxReduceBlocks * 4));
+        CFDXG_CUDA(cudaMalloc(&ctx->scratch.ticket, sizeof(unsigned) * 8));
+        CFDXG_CUDA(cudaMemset(ctx->scratch.ticket, 0, sizeof(unsigned) * 8));
+        CFDXG_CUDA(cudaMalloc(&ctx->scratch.scalars, sizeof(double) * 4096));
+        CFDXG_CUDA(cudaMemset(ctx->scratch.scalars, 0, sizeof(double) * 4096));
+        CFDXG_CUDA(cudaMalloc(&ctx->scratch.status, sizeof(int)));
+        CFDXG_CUDA(cudaMemset(ctx->scratch.status, 0, sizeof(int)));
+        CFDXG_CUDA(cudaMallocHost(&ctx->scratch.host_scalars, sizeof(double) * 4096));
+        CFDXG_CUDA(cudaMallocHost(&ctx->scratch.host_status, sizeof(int)));
+    } catch (const Error& e) {
+        const int code = e.code;
+        cfdxg_context_destroy(ctx);
+        return code;
+    }
+    *out = ctx;
+    return CFDXG_OK;
+}
+
+extern "C" int cfdxg_context_destroy(cfdxg_context* ctx) {
+    if (!ctx) return CFDXG_OK;
+    if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+    ctx->krylov_workspace.reset();
+    if (ctx->scratch.partial) cudaFree(ctx->scratch.partial);
+    if (ctx->scratch.ticket) cudaFree(ctx->scratch.ticket);
+    if (ctx->scratch.scalars) cudaFree(ctx->scratch.scalars);
+    if (ctx->scratch.status) cudaFree(ctx->scratch.status);
+    if (ctx->scratch.host_scalars) cudaFreeHost(ctx->scratch.host_scalars);
+    if (ctx->scratch.host_status) cudaFreeHost(ctx->scratch.host_status);
+    if (ctx->stream) cudaStreamDestroy(ctx->stream);
+    delete ctx;
+    return CFDXG_OK;
+}
+
+extern "C" const char* cfdxg_last_error(const cfdxg_context* ctx) { return ctx ? ctx->error.c_str() : "null context"; }
+extern "C" int64_t cfdxg_kernel_launches(const cfdxg_context* ctx) { return ctx ? ctx->launches : 0; }
+extern "C" int cfdxg_synchronize(cfdxg_context* ctx) {
+    if (!ctx) return CFDXG_ERR_INVALID_ARGUMENT;
+    CFDXG_GUARD_BEGIN
+    CFDXG_CUDA(cudaStreamSynchronize(ctx->stream));
+    return CFDXG_OK;
+    CFDXG_GUARD_END(ctx)
+}
+
+// ---------------------------------------------------------------- matrices
+extern "C" int cfdxg_matrix_create(cfdxg_context* ctx, int64_t n, const int64_t* ro, const int64_t* co,
+                                   const double* va, int32_t mem, cfdxg_matrix** out) {
+    if (!ctx) return CFDXG_ERR_INVALID_ARGUMENT;
+    CFDXG_GUARD_BEGIN
+    check_mem_flag(mem);
+    if (!out || n <= 0 || !ro || !co || !va) throw Error(CFDXG_ERR_INVALID_ARGUMENT, "invalid matrix arguments");
+    if (n > INT32_MAX / 2) throw Error(CFDXG_ERR_INVALID_ARGUMENT, "matrix too large for 32-bit indices");
+    auto A = std::make_unique<cfdxg_matrix>();
+    A->n = n;
+    std::vector<int64_t> hro(n + 1);
+    if (mem == CFDXG_MEM_DEVICE) CFDXG_CUDA(cudaMemcpy(hro.data(), ro, sizeof(int64_t) * (n + 1), cudaMemcpyDeviceToHost));
+    else std::memcpy(hro.data(), ro, sizeof(int64_t) * (n + 1));
+    const int64_t nnz = hro[n];
+    if (hro[0] != 0 || nnz <= 0 || nnz > INT32_MAX) throw Error(CFDXG_ERR_INVALID_ARGUMENT, "invalid row offsets");
+    std::vector<int64_t> hco(nnz);
+    std::vector<double> hva(nnz);
+    if (mem == CFDXG_MEM_DEVICE) {
+        CFDXG_CUDA(cudaMemcpy(hco.data(), co, sizeof(int64_t) * nnz, cudaMemcpyDeviceToHost));
+        CFDXG_CUDA(cudaMemcpy(hva.data(), va, sizeof(double) * nnz, cudaMemcpyDeviceToHost));
+    } else {
+        std::memcpy(hco.data(), co, sizeof(int64_t) * nnz);
+        std::memcpy(hva.data(), va, sizeof(double) * nnz);
+    }
+    // SparseMatrix::from_sorted_csr validation (sparse_matrix.h:136-163)
+    A->host.n = n;
+    A->host.ro.resize(n + 1);
+    A->host.co.resize(nnz);
+    for (int64_t i = 0; i < n; ++i) {
+        if (hro[i] > hro[i + 1] || hro[i + 1] > nnz) throw Error(CFDXG_ERR_INVALID_ARGUMENT, "invalid offsets");
+        for (int64_t k = hro[i]; k < hro[i + 1]; ++k) {
+            if (hco[k] < 0 || hco[k] >= n || !std::isfinite(hva[k]) || (k > hro[i] && hco[k - 1] >= hco[k]))
+                throw Error(CFDXG_ERR_INVALID_ARGUMENT, "invalid CSR row");
+        }
+    }
+    std::vector<int> iro(n + 1), ico(nnz);
+    for (int64_t i = 0; i <= n; ++i) { iro[i] = static_cast<int>(hro[i]); A->host.ro[i] = static_cast<uint32_t>(hro[i]); }
+    for (int64_t k = 0; k < nnz; ++k) { ico[k] = static_cast<int>(hco[k]); A->host.co[k] = static_cast<uint32_t>(hco[k]); }
+    A->host.va = std::move(hva);
+    A->host_values_valid = true;
+    A->nnz = nnz;
+    A->ro.upload(iro, ctx->stream);
+    A->co.upload(ico, ctx->stream);
+    A->va.upload(A->host.va, ctx->stream);
+    CFDXG_CUDA(cudaStreamSynchronize(ctx->stream));
+    *out = A.release();
+    ctx->error.clear();
+    return CFDXG_OK;
+    CFDXG_GUARD_END(ctx)
+}
+
+extern "C" int cfdxg_matrix_destroy(cfdxg_matrix* A) {
+    delete A;
+    return CFDXG_OK;
+}
+
+extern "C" int cfdxg_matrix_size(const cfdxg_matrix* A, int64_t* n, int64_t* nnz) {
+    if (!A) return CFDXG_ERR_INVALID_ARGUMENT;
+    if (n) *n = A->n;
+    if (nnz) *nnz = A->nnz;
+    return CFDXG_OK;
+}
+
+extern "C" int cfdxg_matrix_download(cfdxg_context* ctx, const cfdxg_matrix* A, int64_t* ro, int64_t* co, double* va) {
+    if (!ctx || !A) return CFDXG_ERR_INVALID_ARGUMENT;
+    CFDXG_GUARD_BEGIN
+    if (ro) for (int64_t i = 0; i <= A->n; ++i) ro[i] = A->host.ro[i];
+    if (co) for (int64_t k = 0; k < A->nnz; ++k) co[k] = A->host.co[k];
+    if (va) {
+        A->va.download(va, ctx->stream);
+        CFDXG_CUDA(cudaStreamSynchronize(ctx->stream));
+    }
+    return CFDXG_OK;
+    CFDXG_GUARD_END(ctx)
+}
+
+extern "C" int cfdxg_matrix_spmv(cfdxg_context* ctx, const cfdxg_matrix* A, const double* x, double* y, int32_t mem) {
+    if (!ctx || !A) return CFDXG_ERR_INVALID_ARGUMENT;
+    CFDXG_GUARD_BEGIN
+    check_mem_flag(mem);
+    In<double> xi(ctx, x, A->n, mem);
+    Out<double> yo(ctx, y, A->n, mem);
+    spmv_fp64(ctx, A, xi.get(), yo.get());
+    yo.finish();
+    CFDXG_CUDA(cudaStreamSynchronize(ctx->stream));
+    return CFDXG_OK;
+    CFDXG_GUARD_END(ctx)
+}
+
+// ---------------------------------------------------------------- AMG
+extern "C" int cfdxg_amg_options_default(cfdxg_amg_options* o) {
+    if (!o) return CFDXG_ERR_INVALID_ARGUMENT;
+    o->omega = 0.7;
+    o->pre_sweeps = 6;
+    o->post_sweeps = 6;
+    o->strength_threshold = 0.25;
+    o->max_levels = 25;
+    o->require_smoother_certificate = 0;
+    o->precision = CFDXG_PRECISION_FP64;
+    o->coarse_dense_limit = 2000;
+    return CFDXG_OK;
+}
+
+extern "C" int cfdxg_amg_create(cfdxg_context* ctx, const cfdxg_amg_options* opts, cfdxg_amg** out) {
+    if (!out) return CFDXG_ERR_INVALID_ARGUMENT;
+    CFDXG_GUARD_BEGIN
+    auto amg = std::make_unique<cfdxg_amg>();
+    if (opts) amg->opts = *opts;
+    else cfdxg_amg_options_default(&amg->opts);
+    const auto& o = amg->opts;
+    // MatrixFreeVcyclePreconditioner constructor checks (amg_preconditioner.h:64-75)
+    if (!(o.omega > 0.0 && o.omega < 2.0) || !std::isfinite(o.strength_threshold) || o.strength_threshold < 0.0 ||
+        o.strength_threshold > 1.0 || o.max_levels <= 0 || o.pre_sweeps < 0 || o.post_sweeps < 0 ||
+        (o.precision != CFDXG_PRECISION_FP64 && o.precision != CFDXG_PRECISION_FP32_VCYCLE))
+        throw Error(CFDXG_ERR_INVALID_ARGUMENT, "invalid AMG operator");
+    *out = amg.release();
+    return CFDXG_OK;
+    CFDXG_GUARD_END(ctx)
+}
+
+extern "C" int cfdxg_amg_destroy(cfdxg_amg* amg) {
+    delete amg;
+    return CFDXG_OK;
+}
+
+extern "C" int cfdxg_amg_setup(cfdxg_context* ctx, cfdxg_amg* amg, const cfdxg_matrix* A) {
+    if (!ctx || !amg) return CFDXG_ERR_INVALID_ARGUMENT;
+    CFDXG_GUARD_BEGIN
+    if (!A || A->n <= 0) {
+        amg->error = "AMG setup requires a non-empty, square, finalized CSR matrix";
+        throw Error(CFDXG_ERR_INVALID_ARGUMENT, amg->error);
+    }
+    amg_setup_impl(ctx, amg, const_cast<cfdxg_matrix*>(A));
+    ctx->error.clear();
+    return CFDXG_OK;
+    CFDXG_GUARD_END(ctx)
+}
+
+extern "C" int cfdxg_amg_update_values(cfdxg_context* ctx, cfdxg_amg* amg, const cfdxg_matrix* A) {
+    if (!ctx || !amg) return CFDXG_ERR_INVALID_ARGUMENT;
+    CFDXG_GUARD_BEGIN
+    if (!amg->ready || !A) {
+        amg->error = "native AMG numeric update requires an existing compatible hierarchy";
+        throw Error(CFDXG_ERR_NOT_READY, amg->error);
+    }
+    const double t0 = now_seconds();
+    auto* M = const_cast<cfdxg_matrix*>(A);
+    matrix_sync_host_values(ctx, M);
+    std::string err;
+    if (!amg_update_values(amg->host, M->host, err)) {
+        amg->error = err;
+        throw Error(CFDXG_ERR_SETUP, err);
+    }
+    if (amg->d32) refresh_hierarchy_values<float>(ctx, *amg->d32, amg->host);
+    if (amg->d64) refresh_hierarchy_values<double>(ctx, *amg->d64, amg->host);
+    amg->setup_seconds = now_seconds() - t0;
+    amg->error.clear();
+    ctx->error.clear();
+    return CFDXG_OK;
+    CFDXG_GUARD_END(ctx)
+}
+
+extern "C" int cfdxg_amg_apply(cfdxg_context* ctx, cfdxg_amg* amg, const double* r, double* z, int32_t mem) {
+    if (!ctx || !amg) return CFDXG_ERR_INVALID_ARGUMENT;
+    CFDXG_GUARD_BEGIN
+    check_mem_flag(mem);
+    if (!amg->ready || (!amg->d64 && !amg->d32)) {
+        amg->error = "native AMG preconditioner has not been set up on the device";
+        throw Error(CFDXG_ERR_NOT_READY, amg->error);
+    }
+    const int64_t n = amg->host.levels.front().A.n;
+    In<double> rin(ctx, r, n, mem);
+    Out<double> zout(ctx, z, n, mem);
+    clear_status(ctx);
+    k_check_finite<<<blocks_for(n, 256), 256, 0, ctx->stream>>>(static_cast<int>(n), rin.get(), ctx->scratch.status);
+    check_launch(ctx);
+    amg_apply_device(ctx, amg, rin.get(), zout.get());
+    zout.finish();
+    if (read_status(ctx) & kStatusNonFinite) {
+        amg->error = "native AMG V-cycle failed";
+        throw Error(CFDXG_ERR_NONFINITE, amg->error);
+    }
+    amg->error.clear();
+    return CFDXG_OK;
+    CFDXG_GUARD_END(ctx)
+}
+
+extern "C" int cfdxg_amg_setup_host(cfdxg_amg* amg, int64_t n, const int64_t* ro, const int64_t* co,
+                                    const double* va) {
+    if (!amg || n <= 0 || !ro || !co || !va) return CFDXG_ERR_INVALID_ARGUMENT;
+    cfdxg_context* ctx = nullptr;
+    CFDXG_GUARD_BEGIN
+    const double t0 = now_seconds();
+    HostCsr A;
+    A.n = n;
+    const int64_t nnz = ro[n];
+    if (ro[0] != 0 || nnz <= 0 || nnz > INT32_MAX) throw Error(CFDXG_ERR_INVALID_ARGUMENT, "invalid row offsets");
+    A.ro.resize(n + 1);
+    A.co.resize(nnz);
+    A.va.assign(va, va + nnz);
+    for (int64_t i = 0; i <= n; ++i) A.ro[i] = static_cast<uint32_t>(ro[i]);
+    for (int64_t k = 0; k < nnz; ++k) {
+        if (co[k] < 0 || co[k] >= n) throw Error(CFDXG_ERR_INVALID_ARGUMENT, "column out of range");
+        A.co[k] = static_cast<uint32_t>(co[k]);
+    }
+    AmgOptions o;
+    o.omega = amg->opts.omega;
+    o.pre = amg->opts.pre_sweeps;
+    o.post = amg->opts.post_sweeps;
+    o.strength_threshold = amg->opts.strength_threshold;
+    o.max_levels = amg->opts.max_levels;
+    o.require_smoother_certificate = amg->opts.require_smoother_certificate != 0;
+    AmgHierarchy staged;
+    std::string err;
+    if (!amg_setup(A, o, staged, err)) {
+        amg->error = "native AMG hierarchy construction failed: " + err;
+        return CFDXG_ERR_SETUP;
+    }
+    amg->host = std::move(staged);
+    amg->d64.reset();
+    amg->d32.reset();
+    amg->ready = true;
+    amg->error.clear();
+    amg->setup_seconds = now_seconds() - t0;
+    return CFDXG_OK;
+    CFDXG_GUARD_END(ctx)
+}
+
+extern "C" const char* cfdxg_amg_name(const cfdxg_amg* amg) {
+    if (amg && amg->opts.precision == CFDXG_PRECISION_FP32_VCYCLE) return "NativeBoomerStyleAMG-FP32Vcycle";
+    return "NativeBoomerStyleAMG";
+}
+extern "C" const char* cfdxg_amg_last_error(const cfdxg_amg* amg) { return amg ? amg->error.c_str() : ""; }
+extern "C" int32_t cfdxg_amg_num_levels(const cfdxg_amg* amg) {
+    return amg && amg->ready ? static_cast<int32_t>(amg->host.levels.size()) : 0;
+}
+extern "C" double cfdxg_amg_omega(const cfdxg_amg* amg) { return amg && amg->ready ? amg->host.omega : 0.0; }
+extern "C" double cfdxg_amg_setup_seconds(const cfdxg_amg* amg) { return amg ? amg->setup_seconds : 0.0; }
+
+extern "C" int cfdxg_amg_level_info(const cfdxg_amg* amg, int32_t level, int64_t* n, int64_t* nnz, int64_t* p_nnz) {
+    if (!amg || !amg->ready || level < 0 || level >= static_cast<int32_t>(amg->host.levels.size()))
+        return CFDXG_ERR_INVALID_ARGUMENT;
+    const auto& L = amg->host.levels[level];
+    if (n) *n = L.A.n;
+    if (nnz) *nnz = L.A.nnz();
+    if (p_nnz) *p_nnz = static_cast<int64_t>(L.p_col.size());
+    return CFDXG_OK;
+}
+
+extern "C" int cfdxg_amg_export_level(const cfdxg_amg* amg, int32_t level, int64_t* ro, int64_t* co, double* va,
+                                      double* inv_diag, int64_t* po, int64_t* pc, double* pv, int64_t* aggregate) {
+    if (!amg || !amg->ready || level < 0 || level >= static_cast<int32_t>(amg->host.levels.size()))
+        return CFDXG_ERR_INVALID_ARGUMENT;
+    const auto& L = amg->host.levels[level];
+    if (ro) for (std::size_t i = 0; i < L.A.ro.size(); ++i) ro[i] = L.A.ro[i];
+    if (co) for (std::size_t k = 0; k < L.A.co.size(); ++k) co[k] = L.A.co[k];
+    if (va) std::memcpy(va, L.A.va.data(), sizeof(double) * L.A.va.size());
+    if (inv_diag) std::memcpy(inv_diag, L.inv_diag.data(), sizeof(double) * L.inv_diag.size());
+    if (po && !L.p_off.empty()) for (std::size_t i = 0; i < L.p_off.size(); ++i) po[i] = L.p_off[i];
+    if (pc) for (std::size_t k = 0; k < L.p_col.size(); ++k) pc[k] = L.p_col[k];
+    if (pv && !L.p_val.empty()) std::memcpy(pv, L.p_val.data(), sizeof(double) * L.p_val.size());
+    if (aggregate) for (std::size_t i = 0; i < L.aggregate.size(); ++i) aggregate[i] = L.aggregate[i];
+    return CFDXG_OK;
+}
+
+// ---------------------------------------------------------------- solves
+extern "C" int cfdxg_request_default(cfdxg_request* r) {
+    if (!r) return CFDXG_ERR_INVALID_ARGUMENT;
+    std::memset(r, 0, sizeof(*r));
+    r->krylov = CFDXG_KRYLOV_GMRES;
+    r->preconditioner = CFDXG_PC_NATIVE_AMG;
+    r->gmres_restart = 40;
+    r->precision = CFDXG_PRECISION_FP64;
+    r->restart_min = 10;
+    r->restart_max = 512;
+    r->adaptive_restart = 1;
+    r->residual_replacement = 1;
+    r->residual_replacement_period = 50;
+    r->residual_replacement_gap_ratio = 10.0;
+    r->target_reduction_per_cycle = 0.1;
+    r->learned = nullptr;
+    return CFDXG_OK;
+}
+
+namespace {
+
+// Runs the Krylov solve on device vectors with an optional prepared AMG, Jacobi
+// inverse diagonal, and learned network.
+KrylovResult run_krylov(cfdxg_context* ctx, const cfdxg_matrix* A, cfdxg_amg* amg, const double* inv_diag,
+                        const double* b, double* x, const cfdxg_request& req, int64_t max_it, double tol,
+                        int64_t* learned_fallbacks) {
+    RightPreconditioner pc;
+    const int n = static_cast<int>(A->n);
+    (void)learned_fallbacks;
+    if (amg) {
+        pc = [ctx, amg](const double* v, double* z) {
+            amg_apply_device(ctx, amg, v, z);
+            return true;
+        };
+    } else if (inv_diag) {
+        pc = [ctx, inv_diag, n](const double* v, double* z) {
+            k_scale<<<blocks_for(n, 256), 256, 0, ctx->stream>>>(n, inv_diag, v, z);
+            check_launch(ctx);
+            return true;
+        };
+    }
+    const RightPreconditioner* p = pc ? &pc : nullptr;
+    return gmres_solve(ctx, A, b, x, req.gmres_restart, max_it, tol, p, controls_from(req));
+}
+
+void validate_request(const cfdxg_request& r) {
+    if (r.gmres_restart <= 0) throw Error(CFDXG_ERR_INVALID_ARGUMENT, "GMRES restart must be positive");
+    if (r.krylov != CFDXG_KRYLOV_GMRES && r.krylov != CFDXG_KRYLOV_FGMRES)
+        throw Error(CFDXG_ERR_INVALID_ARGUMENT, "only GMRES and FGMRES are provided");
+    if (r.preconditioner != CFDXG_PC_NONE && r.preconditioner != CFDXG_PC_JACOBI &&
+        r.preconditioner != CFDXG_PC_NATIVE_AMG)
+        throw Error(CFDXG_ERR_INVALID_ARGUMENT, "requested preconditioner model is not implemented");
+    if (r.precision != CFDXG_PRECISION_FP64 && r.precision != CFDXG_PRECISION_FP32_VCYCLE)
+        throw Error(CFDXG_ERR_INVALID_ARGUMENT, "unknown precision");
+    if (r.learned) throw Error(CFDXG_ERR_INVALID_ARGUMENT, "learned preconditioner not available in this build");
+}
+
+}  // namespace
+
+extern "C" int cfdxg_solve_linear_system(cfdxg_context* ctx, const cfdxg_matrix* A, const double* rhs, double* x,
+                                         int32_t mem, const cfdxg_request* req_in, int64_t max_iterations,
+                                         double tolerance, cfdxg_report* report) {
+    if (!ctx) return CFDXG_ERR_INVALID_ARGUMENT;
+    CFDXG_GUARD_BEGIN
+    check_mem_flag(mem);
+    if (!A || !rhs || !x) throw Error(CFDXG_ERR_INVALID_ARGUMENT, "missing argument");
+    cfdxg_request req;
+    if (req_in) req = *req_in;
+    else cfdxg_request_default(&req);
+    validate_request(req);
+    if (report) std::memset(report, 0, sizeof(*report));
+    const int64_t n = A->n;
+    In<double> b(ctx, rhs, n, mem);
+    Out<double> xo(ctx, x, n, mem, /*preload=*/true);
+    const double t0 = now_seconds();
+    // physical reference norms (linear_solver_dispatch.h:269-273)
+    const double rhs_norm = device_norm2(ctx, A, b.get());
+    const double homogeneous = rhs_norm == 0.0 ? device_residual_norm(ctx, A, b.get(), xo.get()) : 0.0;
+    KrylovResult r;
+    int64_t learned_fallbacks = 0;
+    double setup_s = 0.0;
+    if (req.preconditioner == CFDXG_PC_NATIVE_AMG) {
+        cfdxg_amg amg;
+        cfdxg_amg_options_default(&amg.opts);
+        amg.opts.precision = req.precision;
+        bool ok = true;
+        try {
+            amg_setup_impl(ctx, &amg, const_cast<cfdxg_matrix*>(A));
+        } catch (const Error& e) {
+            if (e.code != CFDXG_ERR_SETUP) throw;
+            ok = false;
+            ctx->error = amg.error;   // LinearSolveReport::preconditioner_error
+        }
+        setup_s = amg.setup_seconds;
+        if (ok) {
+            r = run_krylov(ctx, A, &amg, nullptr, b.get(), xo.get(), req, max_iterations, tolerance, &learned_fallbacks);
+        } else {
+            r.status = CFDXG_NOT_APPLICABLE;
+        }
+    } else if (req.preconditioner == CFDXG_PC_JACOBI) {
+        DevBuf<double> inv(n);
+        clear_status(ctx);
+        k_first_diag_inverse<<<blocks_for(n, 256), 256, 0, ctx->stream>>>(static_cast<int>(n), A->ro.get(), A->co.get(),
+                                                                          A->va.get(), inv.get(), ctx->scratch.status);
+        check_launch(ctx);
+        if (read_status(ctx)) r.status = CFDXG_NOT_APPLICABLE;
+        else r = run_krylov(ctx, A, nullptr, inv.get(), b.get(), xo.get(), req, max_iterations, tolerance, nullptr);
+    } else {
+        r = run_krylov(ctx, A, nullptr, nullptr, b.get(), xo.get(), req, max_iterations, tolerance, nullptr);
+    }
+    // final FP64 physical certificate (linear_solver_dispatch.h:469-491)
+    const double final_residual = device_residual_norm(ctx, A, b.get(), xo.get());
+    const double reference = rhs_norm > 0.0 ? rhs_norm : homogeneous;
+    const double physical = reference > 0.0 ? final_residual / reference
+                                            : (final_residual == 0.0 ? 0.0 : std::numeric_limits<double>::infinity());
+    if (r.status == CFDXG_CONVERGED && (!std::isfinite(physical) || physical > tolerance))
+        r.status = CFDXG_MAX_ITER_REACHED;
+    xo.finish();
+    CFDXG_CUDA(cudaStreamSynchronize(ctx->stream));
+    const double t1 = now_seconds();
+    fill_report(report, r);
+    if (report) {
+        report->physical_residual_relative = physical;
+        report->setup_seconds = setup_s;
+        report->solve_seconds = t1 - t0 - setup_s;
+        report->learned_fallbacks = learned_fallbacks;
+    }
+    return r.status;
+    CFDXG_GUARD_END(ctx)
+}
+
+extern "C" int cfdxg_solve_gmres(cfdxg_context* ctx, const cfdxg_matrix* A, cfdxg_amg* amg, const double* rhs,
+                                 double* x, int32_t mem, const cfdxg_request* req_in, int64_t max_iterations,
+                                 double tolerance, cfdxg_report* report) {
+    if (!ctx) return CFDXG_ERR_INVALID_ARGUMENT;
+    CFDXG_GUARD_BEGIN
+    check_mem_flag(mem);
+    if (!A || !rhs || !x) throw Error(CFDXG_ERR_INVALID_ARGUMENT, "missing argument");
+    cfdxg_request req;
+    if (req_in) req = *req_in;
+    else cfdxg_request_default(&req);
+    validate_request(req);
+    if (amg && (!amg->ready || (!amg->d64 && !amg->d32)))
+        throw Error(CFDXG_ERR_NOT_READY, "native AMG preconditioner has not been set up on the device");
+    if (amg && amg->host.levels.front().A.n != A->n) throw Error(CFDXG_ERR_INVALID_ARGUMENT, "AMG size mismatch");
+    if (report) std::memset(report, 0, sizeof(*report));
+    const int64_t n = A->n;
+    In<double> b(ctx, rhs, n, mem);
+    Out<double> xo(ctx, x, n, mem, /*preload=*/true);
+    const double t0 = now_seconds();
+    int64_t learned_fallbacks = 0;
+    const KrylovResult r = run_krylov(ctx, A, amg, nullptr, b.get(), xo.get(), req, max_iterations, tolerance,
+                                      &learned_fallbacks);
+    xo.finish();
+    CFDXG_CUDA(cudaStreamSynchronize(ctx->stream));
+    fill_report(report, r);
+    if (report) {
+        report->physical_residual_relative = r.residual_relative;
+        report->solve_seconds = now_seconds() - t0;
+        report->learned_fallbacks = learned_fallbacks;
+    }
+    return r.status;
+    CFDXG_GUARD_END(ctx)
+}

@@ -1,0 +1,169 @@
+// device.cuh -- shared device utilities of libcfdxg: the context, RAII device
+// buffers, launch accounting and deterministic block reductions.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <cstdio>
+#include <memory>
+#include <stdexcept>
+#include <string>
+#include <utility>
+#include <vector>
+
+#include "../../include/cfdxg.h"
+
+namespace cfdxg {
+
+// Thrown inside the library, converted to a status code at the C ABI.
+struct Error : std::runtime_error {
+    int code;
+    Error(int c, const std::string& m) : std::runtime_error(m), code(c) {}
+};
+
+#define CFDXG_CUDA(call)                                                                  \
+    do {                                                                                  \
+        cudaError_t e_ = (call);                                                          \
+        if (e_ != cudaSuccess)                                                            \
+            throw ::cfdxg::Error(e_ == cudaErrorMemoryAllocation ? CFDXG_ERR_OUT_OF_MEMORY \
+                                                                 : CFDXG_ERR_CUDA,        \
+                                 std::string(#call) + ": " + cudaGetErrorString(e_));     \
+    } while (0)
+
+constexpr int kReduceThreads = 256;
+constexpr int kMaxReduceBlocks = 592;   // 4 x 148 SMs: fixed partition => deterministic sums
+
+// Device-side scratch owned by a context: reduction partials, tickets, a
+// status word for device-detected errors, and pinned host mirrors.
+struct Scratch {
+    double* partial = nullptr;      // kMaxReduceBlocks * 4
+    unsigned* ticket = nullptr;     // 8 tickets
+    double* scalars = nullptr;      // 4096 device scalars (dots, norms, H columns)
+    int* status = nullptr;          // device error word
+    double* host_scalars = nullptr; // pinned mirror of `scalars`
+    int* host_status = nullptr;     // pinned
+};
+
+}  // namespace cfdxg
+
+struct cfdxg_context {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    std::string error;
+    int64_t launches = 0;
+    cfdxg::Scratch scratch;
+    int sm_count = 148;
+    std::shared_ptr<void> krylov_workspace;   // grown on demand by the Krylov driver
+};
+
+namespace cfdxg {
+
+inline void count_launch(cfdxg_context* ctx, int64_t n = 1) { ctx->launches += n; }
+
+inline void check_launch(cfdxg_context* ctx) {
+    count_launch(ctx);
+    CFDXG_CUDA(cudaGetLastError());
+}
+
+template <class T>
+class DevBuf {
+public:
+    DevBuf() = default;
+    explicit DevBuf(std::size_t n) { resize(n); }
+    DevBuf(const DevBuf&) = delete;
+    DevBuf& operator=(const DevBuf&) = delete;
+    DevBuf(DevBuf&& o) noexcept : p_(o.p_), n_(o.n_) { o.p_ = nullptr; o.n_ = 0; }
+    DevBuf& operator=(DevBuf&& o) noexcept {
+        if (this != &o) { release(); p_ = o.p_; n_ = o.n_; o.p_ = nullptr; o.n_ = 0; }
+        return *this;
+    }
+    ~DevBuf() { release(); }
+    void resize(std::size_t n) {
+        if (n == n_) return;
+        release();
+        if (n) CFDXG_CUDA(cudaMalloc(&p_, n * sizeof(T)));
+        n_ = n;
+    }
+    void upload(const T* h, std::size_t n, cudaStream_t s) {
+        resize(n);
+        if (n) CFDXG_CUDA(cudaMemcpyAsync(p_, h, n * sizeof(T), cudaMemcpyHostToDevice, s));
+    }
+    void upload(const std::vector<T>& h, cudaStream_t s) { upload(h.data(), h.size(), s); }
+    void download(T* h, cudaStream_t s) const {
+        if (n_) CFDXG_CUDA(cudaMemcpyAsync(h, p_, n_ * sizeof(T), cudaMemcpyDeviceToHost, s));
+    }
+    void zero(cudaStream_t s) {
+        if (n_) CFDXG_CUDA(cudaMemsetAsync(p_, 0, n_ * sizeof(T), s));
+    }
+    T* get() const { return p_; }
+    std::size_t size() const { return n_; }
+    void release() {
+        if (p_) cudaFree(p_);
+        p_ = nullptr;
+        n_ = 0;
+    }
+
+private:
+    T* p_ = nullptr;
+    std::size_t n_ = 0;
+};
+
+inline int blocks_for(int64_t n, int threads) {
+    return static_cast<int>((n + threads - 1) / threads);
+}
+
+inline int reduce_blocks(int64_t n) {
+    const int64_t b = (n + kReduceThreads * 4 - 1) / (kReduceThreads * 4);
+    return static_cast<int>(b < 1 ? 1 : (b > kMaxReduceBlocks ? kMaxReduceBlocks : b));
+}
+
+// ---- device helpers ----
+
+template <class T>
+__device__ __forceinline__ T block_sum(T v, T* smem) {
+    // fixed-order tree: warp shuffles, then warp partials summed by warp 0
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    if (lane == 0) smem[warp] = v;
+    __syncthreads();
+    const int nw = (blockDim.x + 31) >> 5;
+    if (warp == 0) {
+        v = lane < nw ? smem[lane] : T(0);
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    }
+    __syncthreads();
+    return v;
+}
+
+template <class T>
+__device__ __forceinline__ T block_max(T v, T* smem) {
+    for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_down_sync(0xffffffffu, v, o));
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    if (lane == 0) smem[warp] = v;
+    __syncthreads();
+    const int nw = (blockDim.x + 31) >> 5;
+    if (warp == 0) {
+        v = lane < nw ? smem[lane] : T(0);
+        for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_down_sync(0xffffffffu, v, o));
+    }
+    __syncthreads();
+    return v;
+}
+
+// Last-block-done: returns true in exactly one block, after every block's
+// partial is visible.  The final combination then runs in block-index order,
+// so the result does not depend on which block finished last.
+__device__ __forceinline__ bool last_block(unsigned* ticket) {
+    __shared__ bool is_last;
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        const unsigned t = atomicAdd(ticket, 1u);
+        is_last = (t == gridDim.x - 1);
+    }
+    __syncthreads();
+    if (is_last) __threadfence();
+    return is_last;
+}
+
+}  // namespace cfdxg

@@ -1,0 +1,594 @@
+// krylov.cu -- device-resident right-preconditioned GMRES / FGMRES.
+//
+// Restates solve_gmres (core/linalg/gmres_solver.h:28-600) with its exact
+// control flow: two-pass modified Gram-Schmidt, scaled two-pass norms
+// (krylov_norm2, core/linalg/krylov_reductions.h:84-115), Givens rotations,
+// Arnoldi/Hessenberg breakdown floors, periodic residual-replacement checks,
+// adaptive restart (krylov_controls.h:28-51), best-iterate retention, the
+// b = 0 shifted solve, and stored Z (so variable preconditioners are valid).
+//
+// Vectors (basis V, preconditioned basis Z, x, r, w) live on the device; each
+// Arnoldi step ends with one small device->host copy of its Hessenberg column
+// and norms, and the host runs the same scalar Givens / least-squares code as
+// the reference.  Dots and norms are deterministic: a fixed partition into
+// blocks (it depends only on n), a fixed in-block tree and an in-order final
+// sum, so repeated solves are bitwise identical.
+#include <algorithm>
+#include <cmath>
+#include <functional>
+#include <limits>
+
+#include "krylov.h"
+
+namespace cfdxg {
+
+namespace {
+
+constexpr int kT = kReduceThreads;
+constexpr double kEps = std::numeric_limits<double>::epsilon();
+
+// scalar slots in ctx->scratch.scalars
+enum Slot : int {
+    kMax = 0, kInvalid = 1, kNorm = 2, kDot = 3, kBeta = 4, kHnext = 5, kAction = 6,
+    kH1 = 64, kH2 = 64 + 1024, kY = 64 + 2048, kSlots = 4096
+};
+
+__global__ void k_absmax(int n, const double* __restrict__ a, double* partial, unsigned* ticket,
+                         double* out_max, double* out_invalid) {
+    __shared__ double sm[32];
+    double m = 0.0, bad = 0.0;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const double v = a[i];
+        if (!isfinite(v)) bad = 1.0;
+        m = fmax(m, fabs(v));
+    }
+    m = block_max(m, sm);
+    bad = block_max(bad, sm);
+    if (threadIdx.x == 0) { partial[2 * blockIdx.x] = m; partial[2 * blockIdx.x + 1] = bad; }
+    if (last_block(ticket)) {
+        double mm = 0.0, bb = 0.0;
+        for (int b = threadIdx.x; b < gridDim.x; b += blockDim.x) {
+            mm = fmax(mm, partial[2 * b]);
+            bb = fmax(bb, partial[2 * b + 1]);
+        }
+        mm = block_max(mm, sm);
+        bb = block_max(bb, sm);
+        if (threadIdx.x == 0) { *out_max = mm; *out_invalid = bb; *ticket = 0; }
+    }
+}
+
+// out = scale * sqrt(sum (a_i / scale)^2), NaN on invalid input, 0 when scale == 0.
+__global__ void k_sumsq(int n, const double* __restrict__ a, const double* scale_p,
+                        const double* invalid_p, double* partial, unsigned* ticket, double* out) {
+    __shared__ double sm[32];
+    const double scale = *scale_p;
+    double s = 0.0;
+    if (scale > 0.0)
+        for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+            const double q = a[i] / scale;
+            s += q * q;
+        }
+    s = block_sum(s, sm);
+    if (threadIdx.x == 0) partial[blockIdx.x] = s;
+    if (last_block(ticket)) {
+        double t = 0.0;
+        for (int b = threadIdx.x; b < gridDim.x; b += blockDim.x) t += partial[b];
+        t = block_sum(t, sm);
+        if (threadIdx.x == 0) {
+            double r;
+            if (*invalid_p > 0.0) r = nan("");
+            else if (scale == 0.0) r = 0.0;
+            else if (!isfinite(t)) r = nan("");
+            else r = scale * sqrt(fmax(0.0, t));
+            *out = r;
+            *ticket = 0;
+        }
+    }
+}
+
+__global__ void k_dot(int n, const double* __restrict__ a, const double* __restrict__ b, double* partial,
+                      unsigned* ticket, double* out) {
+    __shared__ double sm[32];
+    double s = 0.0;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) s += a[i] * b[i];
+    s = block_sum(s, sm);
+    if (threadIdx.x == 0) partial[blockIdx.x] = s;
+    if (last_block(ticket)) {
+        double t = 0.0;
+        for (int q = threadIdx.x; q < gridDim.x; q += blockDim.x) t += partial[q];
+        t = block_sum(t, sm);
+        if (threadIdx.x == 0) { *out = t; *ticket = 0; }
+    }
+}
+
+// w = w - c * v   (gmres_solver.h:283 / :289)
+__global__ void k_axpy_neg(int n, double* __restrict__ w, const double* __restrict__ v, const double* c) {
+    const double cc = *c;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) w[i] = w[i] - cc * v[i];
+}
+
+// v = w / d  when d > 0   (gmres_solver.h:183 and :322)
+__global__ void k_div(int n, const double* __restrict__ w, const double* d, double* __restrict__ v) {
+    const double dd = *d;
+    if (!(dd > 0.0)) return;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) v[i] = w[i] / dd;
+}
+
+// r = b - A x  (true residual with the FP64 operator)
+__global__ void k_true_residual(int n, const int* __restrict__ ro, const int* __restrict__ co,
+                                const double* __restrict__ va, const double* __restrict__ b,
+                                const double* __restrict__ x, double* __restrict__ r) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    double s = 0.0;
+    const int e = ro[i + 1];
+    for (int k = ro[i]; k < e; ++k) s += va[k] * __ldg(x + co[k]);
+    r[i] = b[i] - s;
+}
+
+// out = x + sum_j y_j z_j, accumulated in j order per element (gmres_solver.h:497-501)
+__global__ void k_update(int n, const double* __restrict__ x, const double* __restrict__ Z,
+                         const double* __restrict__ y, int used, double* __restrict__ out) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    double v = x[i];
+    for (int j = 0; j < used; ++j) v += y[j] * Z[static_cast<size_t>(j) * n + i];
+    out[i] = v;
+}
+
+__global__ void k_neg(int n, const double* __restrict__ a, double* __restrict__ b) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) b[i] = -a[i];
+}
+
+__global__ void k_add(int n, double* __restrict__ x, const double* __restrict__ y) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) x[i] += y[i];
+}
+
+struct Workspace {
+    int64_t n = 0;
+    int m = 0;
+    DevBuf<double> V, Z, w, r, ax, best, trial, tmp;
+};
+
+Workspace& workspace(cfdxg_context* ctx, int64_t n, int m) {
+    auto ws = std::static_pointer_cast<Workspace>(ctx->krylov_workspace);
+    if (!ws) {
+        ws = std::make_shared<Workspace>();
+        ctx->krylov_workspace = ws;
+    }
+    if (ws->n != n || ws->m < m) {
+        const int mm = std::max(m, ws->n == n ? ws->m : 0);
+        ws->V.resize(static_cast<size_t>(mm + 1) * n);
+        ws->Z.resize(static_cast<size_t>(mm) * n);
+        ws->w.resize(n); ws->r.resize(n); ws->ax.resize(n); ws->best.resize(n);
+        ws->trial.resize(n); ws->tmp.resize(n);
+        ws->n = n;
+        ws->m = mm;
+    }
+    return *ws;
+}
+
+class Engine {
+public:
+    Engine(cfdxg_context* ctx, const cfdxg_matrix* A) : ctx_(ctx), A_(A), n_(static_cast<int>(A->n)) {
+        sc_ = ctx->scratch.scalars;
+    }
+    double* slot(int s) const { return sc_ + s; }
+    int gb() const { return blocks_for(n_, kT); }
+    int rb() const { return reduce_blocks(n_); }
+
+    void norm2(const double* a, int out) {
+        k_absmax<<<rb(), kT, 0, ctx_->stream>>>(n_, a, ctx_->scratch.partial, ctx_->scratch.ticket,
+                                                slot(kMax), slot(kInvalid));
+        check_launch(ctx_);
+        k_sumsq<<<rb(), kT, 0, ctx_->stream>>>(n_, a, slot(kMax), slot(kInvalid), ctx_->scratch.partial,
+                                               ctx_->scratch.ticket, slot(out));
+        check_launch(ctx_);
+    }
+    void dot(const double* a, const double* b, int out) {
+        k_dot<<<rb(), kT, 0, ctx_->stream>>>(n_, a, b, ctx_->scratch.partial, ctx_->scratch.ticket, slot(out));
+        check_launch(ctx_);
+    }
+    void axpy_neg(double* w, const double* v, int coef) {
+        k_axpy_neg<<<gb(), kT, 0, ctx_->stream>>>(n_, w, v, slot(coef));
+        check_launch(ctx_);
+    }
+    void div(const double* w, int d, double* v) {
+        k_div<<<gb(), kT, 0, ctx_->stream>>>(n_, w, slot(d), v);
+        check_launch(ctx_);
+    }
+    void residual(const double* b, const double* x, double* r) {
+        k_true_residual<<<gb(), kT, 0, ctx_->stream>>>(n_, A_->ro.get(), A_->co.get(), A_->va.get(), b, x, r);
+        check_launch(ctx_);
+    }
+    void spmv(const double* x, double* y) { spmv_fp64(ctx_, A_, x, y); }
+    void copy(double* dst, const double* src) {
+        CFDXG_CUDA(cudaMemcpyAsync(dst, src, sizeof(double) * n_, cudaMemcpyDeviceToDevice, ctx_->stream));
+    }
+    void update(const double* x, const double* Z, const std::vector<double>& y, int used, double* out) {
+        if (used > 0)
+            CFDXG_CUDA(cudaMemcpyAsync(slot(kY), y.data(), sizeof(double) * used, cudaMemcpyHostToDevice,
+                                       ctx_->stream));
+        k_update<<<gb(), kT, 0, ctx_->stream>>>(n_, x, Z, slot(kY), used, out);
+        check_launch(ctx_);
+    }
+    void neg(const double* a, double* b) {
+        k_neg<<<gb(), kT, 0, ctx_->stream>>>(n_, a, b);
+        check_launch(ctx_);
+    }
+    void add(double* x, const double* y) {
+        k_add<<<gb(), kT, 0, ctx_->stream>>>(n_, x, y);
+        check_launch(ctx_);
+    }
+    // Copies slots [0, count) to the host and synchronises; returns the status word.
+    int fetch(int count) {
+        CFDXG_CUDA(cudaMemcpyAsync(ctx_->scratch.host_scalars, sc_, sizeof(double) * count,
+                                   cudaMemcpyDeviceToHost, ctx_->stream));
+        return read_status(ctx_);
+    }
+    double host(int s) const { return ctx_->scratch.host_scalars[s]; }
+    double scalar(int s) {   // read one slot
+        fetch(s + 1);
+        return host(s);
+    }
+
+private:
+    cfdxg_context* ctx_;
+    const cfdxg_matrix* A_;
+    int n_;
+    double* sc_;
+};
+
+// krylov_controls.h:28-51
+int choose_restart(int current, double reduction, const KrylovControls& c) {
+    if (!c.adaptive_restart) return std::clamp(current, c.restart_min, c.restart_max);
+    if (reduction > c.target_reduction_per_cycle * 2.0)
+        return current > c.restart_max - 5 ? c.restart_max : current + 5;
+    if (reduction < c.target_reduction_per_cycle * 0.5) return std::max(c.restart_min, current - 5);
+    return std::clamp(current, c.restart_min, c.restart_max);
+}
+
+}  // namespace
+
+KrylovResult gmres_solve(cfdxg_context* ctx, const cfdxg_matrix* A, const double* b, double* x,
+                         int restart, int64_t max_iter, double tolerance, const RightPreconditioner* pc,
+                         const KrylovControls& controls) {
+    KrylovResult result;
+    const int64_t n = A->n;
+    if (n == 0 || restart <= 0 || max_iter == 0 || !std::isfinite(tolerance) || tolerance <= 0.0) {
+        result.status = CFDXG_NOT_APPLICABLE;
+        return result;
+    }
+    if (controls.restart_min <= 0 || controls.restart_max < controls.restart_min ||
+        !std::isfinite(controls.target_reduction_per_cycle) || controls.target_reduction_per_cycle <= 0.0 ||
+        controls.target_reduction_per_cycle >= 1.0 || !std::isfinite(controls.residual_replacement_gap_ratio) ||
+        controls.residual_replacement_gap_ratio < 1.0) {
+        result.status = CFDXG_NOT_APPLICABLE;
+        return result;
+    }
+    if (n > std::numeric_limits<int>::max()) throw Error(CFDXG_ERR_INVALID_ARGUMENT, "system too large");
+    Engine E(ctx, A);
+    clear_status(ctx);
+    int current_restart = std::clamp(restart, controls.restart_min, controls.restart_max);
+    if (n < current_restart) current_restart = static_cast<int>(n);
+
+    E.norm2(b, kNorm);
+    const double b_norm = E.scalar(kNorm);
+    if (!std::isfinite(b_norm)) {
+        result.status = CFDXG_DIVERGED;
+        return result;
+    }
+    if (b_norm == 0.0) {
+        // gmres_solver.h:64-134: b == 0 with x0 != 0 -> solve A y = -A x0, certify on ||A x0||.
+        Workspace& ws = workspace(ctx, n, current_restart);
+        E.spmv(x, ws.ax.get());
+        E.norm2(ws.ax.get(), kNorm);
+        const double ax0_norm = E.scalar(kNorm);
+        if (!std::isfinite(ax0_norm)) {
+            result.status = CFDXG_DIVERGED;
+            result.residual = ax0_norm;
+            result.residual_relative = ax0_norm;
+            return result;
+        }
+        if (ax0_norm > 0.0) {
+            DevBuf<double> shifted(n), y(n);
+            E.neg(ws.ax.get(), shifted.get());
+            y.zero(ctx->stream);
+            const KrylovResult sh = gmres_solve(ctx, A, shifted.get(), y.get(), restart, max_iter, tolerance, pc,
+                                                controls);
+            Workspace& ws2 = workspace(ctx, n, current_restart);
+            E.add(x, y.get());
+            E.residual(b, x, ws2.r.get());
+            E.norm2(ws2.r.get(), kNorm);
+            const double residual = E.scalar(kNorm);
+            const double relative = residual / ax0_norm;
+            const bool certified = std::isfinite(residual) && std::isfinite(relative) && relative <= tolerance;
+            result = sh;
+            result.status = certified ? CFDXG_CONVERGED
+                                      : (sh.status == CFDXG_NOT_APPLICABLE ? CFDXG_NOT_APPLICABLE : CFDXG_DIVERGED);
+            result.residual = residual;
+            result.residual_relative = relative;
+            return result;
+        }
+    }
+    const double rhs_scale = std::max(b_norm, 1e-300);
+    const double tol = b_norm == 0.0 ? 0.0 : tolerance * b_norm;
+
+    Workspace* ws = &workspace(ctx, n, current_restart);
+    auto true_residual = [&]() {
+        E.residual(b, x, ws->r.get());
+        E.norm2(ws->r.get(), kBeta);
+        return E.scalar(kBeta);
+    };
+
+    double beta = true_residual();
+    if (!std::isfinite(beta)) {
+        result.status = CFDXG_DIVERGED;
+        result.residual = beta;
+        return result;
+    }
+    if (b_norm == 0.0) {
+        E.norm2(x, kNorm);
+        const double x_norm = E.scalar(kNorm);
+        const double ref_scale = std::max({x_norm, 1.0, 1e-300});
+        const double tol_b0 = tolerance * ref_scale;
+        result.status = beta <= tol_b0 ? CFDXG_CONVERGED : CFDXG_DIVERGED;
+        result.iterations = 0;
+        result.residual = beta;
+        result.residual_relative = beta / ref_scale;
+        return result;
+    }
+    if (beta <= tol) {
+        result.status = CFDXG_CONVERGED;
+        result.iterations = 0;
+        result.residual = beta;
+        result.residual_relative = beta / rhs_scale;
+        return result;
+    }
+
+    int64_t iterations = 0;
+    double previous_cycle_residual = beta;
+    E.copy(ws->best.get(), x);
+    double best_residual = beta;
+    auto restore_best = [&]() { E.copy(x, ws->best.get()); };
+    auto fail = [&](int status) {
+        restore_best();
+        result.status = status;
+        result.iterations = iterations;
+        result.residual = best_residual;
+        result.residual_relative = best_residual / rhs_scale;
+        CFDXG_CUDA(cudaStreamSynchronize(ctx->stream));
+        return result;
+    };
+
+    std::vector<double> h, cs, sn, g, y;
+    while (iterations < max_iter) {
+        ws = &workspace(ctx, n, current_restart);
+        const int m = current_restart;
+        h.assign(static_cast<size_t>(m + 1) * m, 0.0);
+        cs.assign(m, 0.0);
+        sn.assign(m, 0.0);
+        g.assign(m + 1, 0.0);
+        y.assign(m, 0.0);
+        auto H = [&](int i, int j) -> double& { return h[static_cast<size_t>(i) * m + j]; };
+        double* V = ws->V.get();
+        double* Z = ws->Z.get();
+        auto v = [&](int j) { return V + static_cast<size_t>(j) * n; };
+        auto z = [&](int j) { return Z + static_cast<size_t>(j) * n; };
+
+        beta = true_residual();
+        if (!std::isfinite(beta)) return fail(CFDXG_DIVERGED);
+        if (beta <= tol) break;
+        E.div(ws->r.get(), kBeta, v(0));
+        g[0] = beta;
+
+        int used = 0;
+        double estimated_residual = beta;
+        bool arnoldi_breakdown = false;
+        bool reliable_restart = false;
+
+        for (int j = 0; j < m && iterations < max_iter; ++j) {
+            if (pc) {
+                if (!(*pc)(v(j), z(j))) return fail(CFDXG_NOT_APPLICABLE);
+                ++result.preconditioner_applications;
+            } else {
+                E.copy(z(j), v(j));
+            }
+            E.spmv(z(j), ws->w.get());
+            E.norm2(ws->w.get(), kAction);
+            for (int i = 0; i <= j; ++i) {
+                E.dot(v(i), ws->w.get(), kH1 + i);
+                E.axpy_neg(ws->w.get(), v(i), kH1 + i);
+            }
+            for (int i = 0; i <= j; ++i) {
+                E.dot(v(i), ws->w.get(), kH2 + i);
+                E.axpy_neg(ws->w.get(), v(i), kH2 + i);
+            }
+            E.norm2(ws->w.get(), kHnext);
+            E.div(ws->w.get(), kHnext, v(j + 1));
+            const int st = E.fetch(kSlots);
+            if (st & kStatusNonFinite) {
+                if (pc) return fail(CFDXG_NOT_APPLICABLE);   // preconditioner produced a non-finite z
+            }
+            const double arnoldi_action_norm = E.host(kAction);
+            if (!std::isfinite(arnoldi_action_norm)) return fail(CFDXG_DIVERGED);
+            for (int i = 0; i <= j; ++i) {
+                H(i, j) = E.host(kH1 + i);
+                H(i, j) += E.host(kH2 + i);
+            }
+            const double hnext = E.host(kHnext);
+            if (!std::isfinite(hnext)) return fail(CFDXG_DIVERGED);
+            H(j + 1, j) = hnext;
+            const double floor = 4096.0 * kEps * std::max(arnoldi_action_norm, 1e-300);
+            const bool breakdown_detected = hnext <= floor && arnoldi_action_norm > 0.0;
+
+            for (int i = 0; i < j; ++i) {
+                const double h0 = H(i, j), h1 = H(i + 1, j);
+                H(i, j) = cs[i] * h0 + sn[i] * h1;
+                H(i + 1, j) = -sn[i] * h0 + cs[i] * h1;
+            }
+            const double a = H(j, j), b2 = H(j + 1, j);
+            const double rho = std::hypot(a, b2);
+            if (rho > 0.0) {
+                cs[j] = a / rho;
+                sn[j] = b2 / rho;
+                H(j, j) = rho;
+                H(j + 1, j) = 0.0;
+                const double gj = g[j], gj1 = g[j + 1];
+                g[j] = cs[j] * gj + sn[j] * gj1;
+                g[j + 1] = -sn[j] * gj + cs[j] * gj1;
+            }
+            ++iterations;
+            ++used;
+            estimated_residual = std::abs(g[j + 1]);
+            if (breakdown_detected) {
+                arnoldi_breakdown = true;
+                break;
+            }
+            if (estimated_residual <= tol) break;
+            if (controls.residual_replacement && controls.residual_replacement_period > 0 &&
+                iterations % controls.residual_replacement_period == 0) {
+                std::vector<double> coef(used, 0.0);
+                bool usable = true;
+                for (int i = used; i-- > 0;) {
+                    double sum = g[i];
+                    for (int k = i + 1; k < used; ++k) sum -= H(i, k) * coef[k];
+                    const double diagonal = H(i, i);
+                    if (!std::isfinite(sum) || !std::isfinite(diagonal) ||
+                        std::abs(diagonal) <= 128.0 * kEps * std::max(arnoldi_action_norm, 1e-300)) {
+                        usable = false;
+                        break;
+                    }
+                    coef[i] = sum / diagonal;
+                }
+                if (usable) {
+                    E.update(x, Z, coef, used, ws->trial.get());
+                    E.residual(b, ws->trial.get(), ws->tmp.get());
+                    E.norm2(ws->tmp.get(), kNorm);
+                    const double verified = E.scalar(kNorm);
+                    if (std::isfinite(verified)) {
+                        result.max_true_residual = std::max(result.max_true_residual, verified);
+                        result.min_true_residual = std::min(result.min_true_residual, verified);
+                        const double ratio = verified / std::max(estimated_residual, 1e-300);
+                        result.max_true_recursive_ratio = std::max(result.max_true_recursive_ratio, ratio);
+                        result.min_true_recursive_ratio = std::min(result.min_true_recursive_ratio, ratio);
+                        result.max_true_recursive_gap =
+                            std::max(result.max_true_recursive_gap, std::abs(verified - estimated_residual));
+                        if (ratio > controls.residual_replacement_gap_ratio) {
+                            reliable_restart = true;
+                            break;
+                        }
+                    } else {
+                        reliable_restart = true;
+                        break;
+                    }
+                }
+            }
+        }
+        if (used == 0) break;
+
+        std::fill(y.begin(), y.end(), 0.0);
+        for (int i = used; i-- > 0;) {
+            double sum = g[i];
+            for (int j = i + 1; j < used; ++j) sum -= H(i, j) * y[j];
+            const double diag = H(i, i);
+            double h_scale = std::abs(diag);
+            for (int k = 0; k < used; ++k) h_scale = std::max(h_scale, std::abs(H(k, i)));
+            const double diag_floor = 128.0 * kEps * std::max(h_scale, 1e-300);
+            if (std::abs(diag) <= diag_floor) {
+                if (std::abs(sum) <= diag_floor) {
+                    y[i] = 0.0;
+                    continue;
+                }
+                double breakdown_residual = true_residual();
+                if (!std::isfinite(breakdown_residual) || best_residual < breakdown_residual) {
+                    restore_best();
+                    breakdown_residual = best_residual;
+                }
+                result.status = CFDXG_DIVERGED;
+                result.iterations = iterations;
+                result.residual = breakdown_residual;
+                result.residual_relative = breakdown_residual / rhs_scale;
+                CFDXG_CUDA(cudaStreamSynchronize(ctx->stream));
+                return result;
+            }
+            y[i] = sum / diag;
+        }
+        E.update(x, Z, y, used, x);
+
+        beta = true_residual();
+        if (reliable_restart && std::isfinite(beta)) {
+            ++result.residual_replacements;
+            if (result.first_residual_replacement == 0) result.first_residual_replacement = iterations;
+            result.last_residual_replacement = iterations;
+            const double ratio = beta / std::max(estimated_residual, 1e-300);
+            result.min_true_recursive_ratio = std::min(result.min_true_recursive_ratio, ratio);
+            result.max_true_recursive_ratio = std::max(result.max_true_recursive_ratio, ratio);
+            result.max_true_recursive_gap = std::max(result.max_true_recursive_gap, std::abs(beta - estimated_residual));
+            result.min_true_residual = std::min(result.min_true_residual, beta);
+            result.max_true_residual = std::max(result.max_true_residual, beta);
+        }
+        if (!std::isfinite(beta)) return fail(CFDXG_DIVERGED);
+        if (beta < best_residual) {
+            best_residual = beta;
+            E.copy(ws->best.get(), x);
+        }
+        if (beta <= tol) {
+            result.status = CFDXG_CONVERGED;
+            result.iterations = iterations;
+            result.residual = beta;
+            result.residual_relative = beta / rhs_scale;
+            CFDXG_CUDA(cudaStreamSynchronize(ctx->stream));
+            return result;
+        }
+        if (arnoldi_breakdown) {
+            if (best_residual < beta) {
+                restore_best();
+                beta = best_residual;
+            }
+            result.status = CFDXG_DIVERGED;
+            result.iterations = iterations;
+            result.residual = beta;
+            result.residual_relative = beta / rhs_scale;
+            CFDXG_CUDA(cudaStreamSynchronize(ctx->stream));
+            return result;
+        }
+        const double reduction = beta / std::max(previous_cycle_residual, 1e-300);
+        if (!std::isfinite(reduction)) return fail(CFDXG_DIVERGED);
+        if (controls.adaptive_restart) {
+            current_restart = choose_restart(current_restart, reduction, controls);
+            if (n < current_restart) current_restart = static_cast<int>(n);
+        }
+        previous_cycle_residual = beta;
+    }
+    if (best_residual < beta) {
+        restore_best();
+        beta = best_residual;
+    }
+    result.status = CFDXG_MAX_ITER_REACHED;
+    result.iterations = iterations;
+    result.residual = beta;
+    result.residual_relative = beta / rhs_scale;
+    CFDXG_CUDA(cudaStreamSynchronize(ctx->stream));
+    return result;
+}
+
+double device_norm2(cfdxg_context* ctx, const cfdxg_matrix* A, const double* a) {
+    Engine E(ctx, A);
+    E.norm2(a, kNorm);
+    return E.scalar(kNorm);
+}
+
+double device_residual_norm(cfdxg_context* ctx, const cfdxg_matrix* A, const double* b, const double* x) {
+    Engine E(ctx, A);
+    Workspace& ws = workspace(ctx, A->n, 1);
+    E.residual(b, x, ws.tmp.get());
+    E.norm2(ws.tmp.get(), kNorm);
+    return E.scalar(kNorm);
+}
+
+}  // namespace cfdxg

@@ -1,0 +1,51 @@
+// krylov.h -- device-resident GMRES / FGMRES (see krylov.cu).
+#pragma once
+#include <functional>
+#include <limits>
+
+#include "objects.h"
+
+namespace cfdxg {
+
+// core/linalg/krylov_controls.h:10-26
+struct KrylovControls {
+    int restart_min = 10;
+    int restart_max = 512;
+    bool adaptive_restart = true;
+    int64_t residual_replacement_period = 50;
+    bool residual_replacement = true;
+    double residual_replacement_gap_ratio = 10.0;
+    double target_reduction_per_cycle = 0.1;
+};
+
+// core/linalg/solver_status.h:45-72
+struct KrylovResult {
+    int status = CFDXG_NOT_APPLICABLE;
+    int64_t iterations = 0;
+    double residual = 0.0;
+    double residual_relative = 0.0;
+    int64_t residual_replacements = 0;
+    double max_true_recursive_gap = 0.0;
+    double min_true_recursive_ratio = std::numeric_limits<double>::infinity();
+    double max_true_recursive_ratio = 0.0;
+    double max_true_residual = 0.0;
+    double min_true_residual = std::numeric_limits<double>::infinity();
+    int64_t first_residual_replacement = 0;
+    int64_t last_residual_replacement = 0;
+    int64_t preconditioner_applications = 0;
+};
+
+// Enqueues z = M^-1 v on the context stream (device vectors); returns false
+// when it cannot run.  Non-finite results are reported through the status word.
+using RightPreconditioner = std::function<bool(const double* v, double* z)>;
+
+KrylovResult gmres_solve(cfdxg_context* ctx, const cfdxg_matrix* A, const double* b, double* x,
+                         int restart, int64_t max_iter, double tolerance, const RightPreconditioner* pc,
+                         const KrylovControls& controls);
+
+// Scaled two-pass 2-norm of a device vector (krylov_norm2).
+double device_norm2(cfdxg_context* ctx, const cfdxg_matrix* A, const double* a);
+// ||b - A x|| with the FP64 operator.
+double device_residual_norm(cfdxg_context* ctx, const cfdxg_matrix* A, const double* b, const double* x);
+
+}  // namespace cfdxg

@@ -1,0 +1,115 @@
+// objects.h -- internal definitions of the opaque C-ABI handles.
+#pragma once
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "amg_setup.h"
+#include "device.cuh"
+
+namespace cfdxg {
+
+// Pressure-correction / diffusion CSR pattern of a mesh: rows sorted, one
+// entry per (cell, neighbour) plus the diagonal; per (cell, local face) the
+// CSR slot of the neighbour column (-1 on boundary faces).
+struct MeshPattern {
+    bool built = false;
+    int64_t nnz = 0;
+    std::vector<uint32_t> ro, co;
+    DevBuf<int> d_ro, d_co, d_slot, d_diag;
+};
+
+template <class T>
+struct DevLevel {
+    int n = 0, nnz = 0, nc = 0;
+    DevBuf<int> ro, co;
+    DevBuf<T> va, inv_diag;
+    DevBuf<int> p_off, p_col, r_off, r_row;
+    DevBuf<T> p_val, r_val;
+    DevBuf<T> r, x, x2, res;
+    T* xout = nullptr;   // where the level's result lives after enqueue
+};
+
+template <class T>
+struct DevHierarchy {
+    std::vector<DevLevel<T>> L;
+    int used = 0;              // levels visited by the cycle
+    T omega = T(0.7);
+    int pre = 6, post = 6;
+    int coarse_mode = 0;       // 0: 24 Jacobi sweeps, 1: reference dense LU (n <= 16), 2: FP64 inverse
+    DevBuf<double> dense;      // mode 1: n*n matrix, mode 2: n*n inverse (row-major)
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    int64_t graph_kernels = 0;
+    int* status = nullptr;
+    ~DevHierarchy() {
+        if (exec) cudaGraphExecDestroy(exec);
+        if (graph) cudaGraphDestroy(graph);
+    }
+};
+
+
+}  // namespace cfdxg
+
+struct cfdxg_mesh {
+    int64_t n_points = 0, n_faces = 0, n_cells = 0, n_internal = 0;
+    int32_t n_patches = 0;
+    int max_cell_faces = 0;
+    cfdxg::DevBuf<double> px, py, pz;
+    cfdxg::DevBuf<int> face_off, face_vert, owner, neigh, cell_off, cell_face, cell_sorted,
+        patch_of_face, patch_type;
+    // geometry (SoA)
+    bool geometry_ready = false;
+    cfdxg::DevBuf<double> face_centre, face_sf, cell_centre, cell_volume;
+    cfdxg::MeshPattern pattern;
+    // host copies needed by the pattern build
+    std::vector<int64_t> h_owner, h_neigh, h_cell_off, h_cell_face;
+    std::vector<int32_t> h_patch_types;
+};
+
+struct cfdxg_matrix {
+    int64_t n = 0, nnz = 0;
+    cfdxg::DevBuf<int> ro, co;
+    cfdxg::DevBuf<double> va;
+    // host mirror of the CSR (pattern always valid; values refreshed on demand)
+    cfdxg::HostCsr host;
+    bool host_values_valid = false;
+    const cfdxg_mesh* mesh = nullptr;   // set when assembled from a mesh pattern
+};
+
+struct cfdxg_amg {
+    cfdxg_amg_options opts{};
+    cfdxg::AmgHierarchy host;
+    bool ready = false;
+    std::string error;
+    double setup_seconds = 0.0;
+    std::unique_ptr<cfdxg::DevHierarchy<double>> d64;
+    std::unique_ptr<cfdxg::DevHierarchy<float>> d32;
+    int64_t applications = 0;
+};
+
+namespace cfdxg {
+
+// matrix helpers (matrix.cu)
+void matrix_sync_host_values(cfdxg_context* ctx, cfdxg_matrix* A);
+void spmv_fp64(cfdxg_context* ctx, const cfdxg_matrix* A, const double* x, double* y);
+
+// hierarchy (vcycle.cu)
+template <class T>
+std::unique_ptr<DevHierarchy<T>> upload_hierarchy(cfdxg_context* ctx, const AmgHierarchy& h,
+                                                  int coarse_dense_limit);
+template <class T>
+void refresh_hierarchy_values(cfdxg_context* ctx, DevHierarchy<T>& d, const AmgHierarchy& h);
+// z = V-cycle(r); r, z are FP64 device vectors.
+template <class T>
+void vcycle_apply(cfdxg_context* ctx, DevHierarchy<T>& d, const double* r, double* z);
+template <class T>
+void destroy_hierarchy(DevHierarchy<T>* d);
+
+// status word helpers (context.cu)
+void clear_status(cfdxg_context* ctx);
+int read_status(cfdxg_context* ctx);   // synchronises
+constexpr int kStatusNonFinite = 1;
+constexpr int kStatusGeometry = 2;
+
+}  // namespace cfdxg

@@ -1,0 +1,518 @@
+// vcycle.cu -- device AMG hierarchy and the V-cycle (damped-Jacobi V(pre,post)).
+//
+// The FP64 instantiation follows MatrixFreeVcyclePreconditioner::vcycle /
+// smooth / smooth_coarsest (core/linalg/amg_preconditioner.h:2369-2443,
+// 2564-2666) operation by operation: every row sum runs in CSR order from 0.0,
+// the restriction gathers P^T rows in increasing fine-row order (the order in
+// which the reference's scatter adds them), the prolongation adds P entries to
+// x one at a time, and the first sweep from x = 0 skips the product A*0 = 0.
+// It therefore returns the reference's z = M^-1 r bit for bit.  The FP32
+// instantiation runs the same cycle in single precision with FP32
+// accumulation and replaces the bottom of the hierarchy by an FP64 dense
+// solve at the first level with <= coarse_dense_limit rows.
+//
+// Level 0 is launched directly with the caller's vectors; levels >= 1 are
+// captured once into a CUDA graph with fixed buffers and replayed.
+#include <cmath>
+#include <limits>
+
+#include "objects.h"
+
+namespace cfdxg {
+
+namespace {
+
+constexpr int kT = 256;
+constexpr int kCoarseSweeps = 24;   // amg_preconditioner.h:2585
+constexpr int kDenseDirectLimit = 16;
+
+template <class T>
+__device__ __forceinline__ bool finite_(T v) { return isfinite(v); }
+
+// First sweep from x = 0 (A*0 = 0): x = 0 + omega * (inv_diag * (r - 0)).
+template <class T, class R>
+__global__ void k_sweep_zero(int n, T omega, const T* __restrict__ inv_diag, const R* __restrict__ r,
+                             T* __restrict__ r_copy, T* __restrict__ x, int* status) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const T ri = static_cast<T>(r[i]);
+    if (r_copy) r_copy[i] = ri;
+    const T delta = inv_diag[i] * (ri - T(0));
+    const T xi = T(0) + omega * delta;
+    x[i] = xi;
+    if (!finite_(xi)) atomicOr(status, kStatusNonFinite);
+}
+
+// x_out = x + omega * (inv_diag * (r - A x)), row sum in CSR order.
+template <class T, class XO>
+__global__ void k_sweep(int n, const int* __restrict__ ro, const int* __restrict__ co,
+                        const T* __restrict__ va, const T* __restrict__ inv_diag,
+                        const T* __restrict__ r, const T* __restrict__ x, XO* __restrict__ xo,
+                        T omega, int* status) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    T s = T(0);
+    const int e = ro[i + 1];
+    for (int k = ro[i]; k < e; ++k) s += va[k] * __ldg(x + co[k]);
+    const T delta = inv_diag[i] * (r[i] - s);
+    const T xi = x[i] + omega * delta;
+    xo[i] = static_cast<XO>(xi);
+    if (!finite_(xi)) atomicOr(status, kStatusNonFinite);
+}
+
+template <class T>
+__global__ void k_residual(int n, const int* __restrict__ ro, const int* __restrict__ co,
+                           const T* __restrict__ va, const T* __restrict__ r,
+                           const T* __restrict__ x, T* __restrict__ res) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    T s = T(0);
+    const int e = ro[i + 1];
+    for (int k = ro[i]; k < e; ++k) s += va[k] * __ldg(x + co[k]);
+    res[i] = r[i] - s;
+}
+
+template <class T>
+__global__ void k_restrict(int nc, const int* __restrict__ r_off, const int* __restrict__ r_row,
+                           const T* __restrict__ r_val, const T* __restrict__ res, T* __restrict__ rc) {
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= nc) return;
+    T s = T(0);
+    const int e = r_off[c + 1];
+    for (int t = r_off[c]; t < e; ++t) s += r_val[t] * __ldg(res + r_row[t]);
+    rc[c] = s;
+}
+
+template <class T>
+__global__ void k_prolong(int n, const int* __restrict__ p_off, const int* __restrict__ p_col,
+                          const T* __restrict__ p_val, const T* __restrict__ xc, T* __restrict__ x,
+                          int* status) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    T v = x[i];
+    const int e = p_off[i + 1];
+    for (int q = p_off[i]; q < e; ++q) v += p_val[q] * __ldg(xc + p_col[q]);
+    x[i] = v;
+    if (!finite_(v)) atomicOr(status, kStatusNonFinite);
+}
+
+template <class T, class XO>
+__global__ void k_copy_cast(int n, const T* __restrict__ a, XO* __restrict__ b) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) b[i] = static_cast<XO>(a[i]);
+}
+
+// Reference dense pivoted solve of the coarsest level (amg_preconditioner.h:2592-2663),
+// constant_null_space = false, executed by one thread in the reference's order.
+template <class T>
+__global__ void k_dense_lu_reference(int n, const int* __restrict__ ro, const int* __restrict__ co,
+                                     const T* __restrict__ va, const T* __restrict__ r,
+                                     T* __restrict__ x, int* status) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    double m[kDenseDirectLimit * kDenseDirectLimit];
+    double b[kDenseDirectLimit];
+    double sol[kDenseDirectLimit];
+    for (int q = 0; q < n * n; ++q) m[q] = 0.0;
+    for (int i = 0; i < n; ++i) {
+        b[i] = static_cast<double>(r[i]);
+        for (int k = ro[i]; k < ro[i + 1]; ++k) m[i * n + co[k]] += static_cast<double>(va[k]);
+    }
+    double matrix_scale = 0.0;
+    for (int q = 0; q < n * n; ++q) {
+        const double a = fabs(m[q]);
+        matrix_scale = (matrix_scale < a) ? a : matrix_scale;
+    }
+    const double pivot_tol = 128.0 * 2.220446049250313080847e-16 * (1.0 < matrix_scale ? matrix_scale : 1.0);
+    for (int k = 0; k < n; ++k) {
+        int pivot = k;
+        double pivot_abs = fabs(m[k * n + k]);
+        for (int i = k + 1; i < n; ++i) {
+            const double c = fabs(m[i * n + k]);
+            if (c > pivot_abs) { pivot_abs = c; pivot = i; }
+        }
+        if (!isfinite(pivot_abs) || pivot_abs <= pivot_tol) { atomicOr(status, kStatusNonFinite); return; }
+        if (pivot != k) {
+            for (int j = k; j < n; ++j) { const double t = m[k * n + j]; m[k * n + j] = m[pivot * n + j]; m[pivot * n + j] = t; }
+            const double t = b[k]; b[k] = b[pivot]; b[pivot] = t;
+        }
+        const double diagonal = m[k * n + k];
+        for (int i = k + 1; i < n; ++i) {
+            const double factor = m[i * n + k] / diagonal;
+            if (!isfinite(factor)) { atomicOr(status, kStatusNonFinite); return; }
+            m[i * n + k] = 0.0;
+            for (int j = k + 1; j < n; ++j) m[i * n + j] -= factor * m[k * n + j];
+            b[i] -= factor * b[k];
+        }
+    }
+    for (int ii = n - 1; ii >= 0; --ii) {
+        double sum = b[ii];
+        for (int j = ii + 1; j < n; ++j) sum -= m[ii * n + j] * sol[j];
+        const double diagonal = m[ii * n + ii];
+        if (!isfinite(diagonal) || fabs(diagonal) <= pivot_tol) { atomicOr(status, kStatusNonFinite); return; }
+        sol[ii] = sum / diagonal;
+        if (!isfinite(sol[ii])) { atomicOr(status, kStatusNonFinite); return; }
+    }
+    for (int i = 0; i < n; ++i) x[i] = static_cast<T>(sol[i]);
+}
+
+// x = Ainv * r with the FP64 inverse, one warp per row.
+template <class T>
+__global__ void k_dense_inverse_apply(int n, const double* __restrict__ inv, const T* __restrict__ r,
+                                      T* __restrict__ x, int* status) {
+    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (warp >= n) return;
+    double s = 0.0;
+    const double* row = inv + static_cast<size_t>(warp) * n;
+    for (int j = lane; j < n; j += 32) s += row[j] * static_cast<double>(r[j]);
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+    if (lane == 0) {
+        x[warp] = static_cast<T>(s);
+        if (!isfinite(s)) atomicOr(status, kStatusNonFinite);
+    }
+}
+
+// ---- Gauss-Jordan inverse (FP64, partial pivoting) for the dense coarse solve ----
+__global__ void k_gj_pivot(int n, double* a /* n x 2n */, double* factors, int k, int* status) {
+    // one block: find pivot row, swap, normalise row k, save column-k factors
+    __shared__ double best_v[kT];
+    __shared__ int best_i[kT];
+    double bv = -1.0;
+    int bi = k;
+    for (int i = k + threadIdx.x; i < n; i += blockDim.x) {
+        const double v = fabs(a[static_cast<size_t>(i) * 2 * n + k]);
+        if (v > bv) { bv = v; bi = i; }
+    }
+    best_v[threadIdx.x] = bv;
+    best_i[threadIdx.x] = bi;
+    __syncthreads();
+    for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+        if (threadIdx.x < s) {
+            const double ov = best_v[threadIdx.x + s];
+            const int oi = best_i[threadIdx.x + s];
+            if (ov > best_v[threadIdx.x] || (ov == best_v[threadIdx.x] && oi < best_i[threadIdx.x])) {
+                best_v[threadIdx.x] = ov;
+                best_i[threadIdx.x] = oi;
+            }
+        }
+        __syncthreads();
+    }
+    const int p = best_i[0];
+    if (!(best_v[0] > 0.0) || !isfinite(best_v[0])) {
+        if (threadIdx.x == 0) atomicOr(status, kStatusNonFinite);
+        return;
+    }
+    double* rk = a + static_cast<size_t>(k) * 2 * n;
+    double* rp = a + static_cast<size_t>(p) * 2 * n;
+    if (p != k)
+        for (int j = threadIdx.x; j < 2 * n; j += blockDim.x) { const double t = rk[j]; rk[j] = rp[j]; rp[j] = t; }
+    __syncthreads();
+    const double inv_piv = 1.0 / rk[k];
+    __syncthreads();
+    for (int j = threadIdx.x; j < 2 * n; j += blockDim.x) rk[j] *= inv_piv;
+    __syncthreads();
+    for (int i = threadIdx.x; i < n; i += blockDim.x) factors[i] = (i == k) ? 0.0 : a[static_cast<size_t>(i) * 2 * n + k];
+}
+
+__global__ void k_gj_eliminate(int n, double* a, const double* factors, int k) {
+    const size_t idx = static_cast<size_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    const size_t total = static_cast<size_t>(n) * 2 * n;
+    if (idx >= total) return;
+    const int i = static_cast<int>(idx / (2 * n));
+    const int j = static_cast<int>(idx % (2 * n));
+    if (i == k) return;
+    const double f = factors[i];
+    if (f == 0.0) return;
+    a[idx] -= f * a[static_cast<size_t>(k) * 2 * n + j];
+}
+
+__global__ void k_gj_extract(int n, const double* a, double* inv) {
+    const size_t idx = static_cast<size_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (idx >= static_cast<size_t>(n) * n) return;
+    const int i = static_cast<int>(idx / n), j = static_cast<int>(idx % n);
+    inv[idx] = a[static_cast<size_t>(i) * 2 * n + n + j];
+}
+
+__global__ void k_gj_init(int n, const int* ro, const int* co, const double* va, double* a) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    double* row = a + static_cast<size_t>(i) * 2 * n;
+    for (int j = 0; j < 2 * n; ++j) row[j] = 0.0;
+    for (int k = ro[i]; k < ro[i + 1]; ++k) row[co[k]] += va[k];
+    row[n + i] = 1.0;
+}
+
+template <class T>
+void upload_level_values(cfdxg_context* ctx, DevLevel<T>& D, const AmgLevel& H) {
+    std::vector<T> tmp(H.A.va.size());
+    for (std::size_t k = 0; k < tmp.size(); ++k) tmp[k] = static_cast<T>(H.A.va[k]);
+    D.va.upload(tmp, ctx->stream);
+    std::vector<T> d(H.inv_diag.size());
+    for (std::size_t k = 0; k < d.size(); ++k) d[k] = static_cast<T>(H.inv_diag[k]);
+    D.inv_diag.upload(d, ctx->stream);
+    CFDXG_CUDA(cudaStreamSynchronize(ctx->stream));
+}
+
+template <class T>
+void upload_level(cfdxg_context* ctx, DevLevel<T>& D, const AmgLevel& H, bool with_transfer) {
+    cudaStream_t s = ctx->stream;
+    D.n = static_cast<int>(H.A.n);
+    D.nnz = static_cast<int>(H.A.co.size());
+    std::vector<int> ro(H.A.ro.begin(), H.A.ro.end()), co(H.A.co.begin(), H.A.co.end());
+    D.ro.upload(ro, s);
+    D.co.upload(co, s);
+    upload_level_values(ctx, D, H);
+    D.r.resize(D.n); D.x.resize(D.n); D.x2.resize(D.n); D.res.resize(D.n);
+    if (with_transfer) {
+        const int n = D.n;
+        int nc = 0;
+        for (const uint32_t c : H.p_col) nc = std::max<int>(nc, static_cast<int>(c) + 1);
+        nc = std::max<int>(nc, static_cast<int>(H.plan.n_coarse));
+        D.nc = nc;
+        std::vector<int> po(H.p_off.begin(), H.p_off.end()), pc(H.p_col.begin(), H.p_col.end());
+        std::vector<T> pv(H.p_val.size());
+        for (std::size_t q = 0; q < pv.size(); ++q) pv[q] = static_cast<T>(H.p_val[q]);
+        // P^T in stable fine-row order (galerkin_csr_product.h:61-80 builds the same adjacency)
+        std::vector<int> to(static_cast<std::size_t>(nc) + 1, 0), tr(H.p_col.size());
+        std::vector<T> tv(H.p_col.size());
+        for (const uint32_t c : H.p_col) ++to[c + 1];
+        for (int c = 0; c < nc; ++c) to[c + 1] += to[c];
+        std::vector<int> cur(to.begin(), to.end() - 1);
+        for (int i = 0; i < n; ++i)
+            for (uint32_t q = H.p_off[i]; q < H.p_off[i + 1]; ++q) {
+                const int pos = cur[H.p_col[q]]++;
+                tr[pos] = i;
+                tv[pos] = static_cast<T>(H.p_val[q]);
+            }
+        D.p_off.upload(po, s); D.p_col.upload(pc, s); D.p_val.upload(pv, s);
+        D.r_off.upload(to, s); D.r_row.upload(tr, s); D.r_val.upload(tv, s);
+        CFDXG_CUDA(cudaStreamSynchronize(s));
+    }
+}
+
+template <class T>
+void build_dense_inverse(cfdxg_context* ctx, DevHierarchy<T>& d, const AmgLevel& H) {
+    const int n = static_cast<int>(H.A.n);
+    DevBuf<int> ro, co;
+    DevBuf<double> va, a, f;
+    std::vector<int> hro(H.A.ro.begin(), H.A.ro.end()), hco(H.A.co.begin(), H.A.co.end());
+    ro.upload(hro, ctx->stream); co.upload(hco, ctx->stream); va.upload(H.A.va, ctx->stream);
+    a.resize(static_cast<std::size_t>(n) * 2 * n);
+    f.resize(n);
+    d.dense.resize(static_cast<std::size_t>(n) * n);
+    k_gj_init<<<blocks_for(n, kT), kT, 0, ctx->stream>>>(n, ro.get(), co.get(), va.get(), a.get());
+    check_launch(ctx);
+    const size_t total = static_cast<size_t>(n) * 2 * n;
+    const int eb = static_cast<int>((total + kT - 1) / kT);
+    for (int k = 0; k < n; ++k) {
+        k_gj_pivot<<<1, kT, 0, ctx->stream>>>(n, a.get(), f.get(), k, ctx->scratch.status);
+        check_launch(ctx);
+        k_gj_eliminate<<<eb, kT, 0, ctx->stream>>>(n, a.get(), f.get(), k);
+        check_launch(ctx);
+    }
+    k_gj_extract<<<blocks_for(static_cast<int64_t>(n) * n, kT), kT, 0, ctx->stream>>>(n, a.get(), d.dense.get());
+    check_launch(ctx);
+    CFDXG_CUDA(cudaStreamSynchronize(ctx->stream));
+}
+
+template <class T>
+void sweeps_from_zero(cfdxg_context* ctx, DevHierarchy<T>& d, DevLevel<T>& L, const T* r_in,
+                      int sweeps) {
+    cudaStream_t s = ctx->stream;
+    const int gb = blocks_for(L.n, kT);
+    T* x = L.x.get();
+    T* x2 = L.x2.get();
+    if (sweeps == 0) {
+        CFDXG_CUDA(cudaMemsetAsync(x, 0, sizeof(T) * L.n, s));
+    } else {
+        k_sweep_zero<T, T><<<gb, kT, 0, s>>>(L.n, d.omega, L.inv_diag.get(), r_in, nullptr, x, d.status);
+        check_launch(ctx);
+        for (int k = 1; k < sweeps; ++k) {
+            k_sweep<T, T><<<gb, kT, 0, s>>>(L.n, L.ro.get(), L.co.get(), L.va.get(), L.inv_diag.get(),
+                                            r_in, x, x2, d.omega, d.status);
+            check_launch(ctx);
+            std::swap(x, x2);
+        }
+    }
+    L.xout = x;
+}
+
+// Enqueue the cycle for levels [l, used) with the level-l right-hand side in L[l].r.
+template <class T>
+void enqueue_from(cfdxg_context* ctx, DevHierarchy<T>& d, int l) {
+    cudaStream_t s = ctx->stream;
+    DevLevel<T>& L = d.L[l];
+    const int gb = blocks_for(L.n, kT);
+    if (l == d.used - 1) {
+        if (d.coarse_mode == 1) {
+            k_dense_lu_reference<T><<<1, 32, 0, s>>>(L.n, L.ro.get(), L.co.get(), L.va.get(), L.r.get(),
+                                                     L.x.get(), d.status);
+            check_launch(ctx);
+            L.xout = L.x.get();
+        } else if (d.coarse_mode == 2) {
+            k_dense_inverse_apply<T><<<blocks_for(static_cast<int64_t>(L.n) * 32, kT), kT, 0, s>>>(
+                L.n, d.dense.get(), L.r.get(), L.x.get(), d.status);
+            check_launch(ctx);
+            L.xout = L.x.get();
+        } else {
+            sweeps_from_zero(ctx, d, L, L.r.get(), kCoarseSweeps);
+        }
+        return;
+    }
+    sweeps_from_zero(ctx, d, L, L.r.get(), d.pre);
+    T* x = L.xout;
+    T* x2 = (x == L.x.get()) ? L.x2.get() : L.x.get();
+    k_residual<T><<<gb, kT, 0, s>>>(L.n, L.ro.get(), L.co.get(), L.va.get(), L.r.get(), x, L.res.get());
+    check_launch(ctx);
+    DevLevel<T>& C = d.L[l + 1];
+    k_restrict<T><<<blocks_for(C.n, kT), kT, 0, s>>>(C.n, L.r_off.get(), L.r_row.get(), L.r_val.get(),
+                                                      L.res.get(), C.r.get());
+    check_launch(ctx);
+    enqueue_from(ctx, d, l + 1);
+    k_prolong<T><<<gb, kT, 0, s>>>(L.n, L.p_off.get(), L.p_col.get(), L.p_val.get(), C.xout, x, d.status);
+    check_launch(ctx);
+    for (int k = 0; k < d.post; ++k) {
+        k_sweep<T, T><<<gb, kT, 0, s>>>(L.n, L.ro.get(), L.co.get(), L.va.get(), L.inv_diag.get(),
+                                        L.r.get(), x, x2, d.omega, d.status);
+        check_launch(ctx);
+        std::swap(x, x2);
+    }
+    L.xout = x;
+}
+
+template <class T>
+void ensure_graph(cfdxg_context* ctx, DevHierarchy<T>& d) {
+    if (d.exec || d.used < 2) return;
+    const int64_t before = ctx->launches;
+    CFDXG_CUDA(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
+    try {
+        enqueue_from(ctx, d, 1);
+    } catch (...) {
+        cudaGraph_t g = nullptr;
+        cudaStreamEndCapture(ctx->stream, &g);
+        if (g) cudaGraphDestroy(g);
+        throw;
+    }
+    CFDXG_CUDA(cudaStreamEndCapture(ctx->stream, &d.graph));
+    CFDXG_CUDA(cudaGraphInstantiate(&d.exec, d.graph, 0));
+    d.graph_kernels = ctx->launches - before;
+    ctx->launches = before;   // captured, not launched
+}
+
+}  // namespace
+
+template <class T>
+std::unique_ptr<DevHierarchy<T>> upload_hierarchy(cfdxg_context* ctx, const AmgHierarchy& h,
+                                                  int coarse_dense_limit) {
+    auto d = std::make_unique<DevHierarchy<T>>();
+    d->omega = static_cast<T>(h.omega);
+    d->pre = h.options.pre;
+    d->post = h.options.post;
+    d->status = ctx->scratch.status;
+    int used = static_cast<int>(h.levels.size());
+    d->coarse_mode = 0;
+    if (std::is_same<T, float>::value && coarse_dense_limit > 0) {
+        for (int l = 0; l < used; ++l)
+            if (h.levels[l].A.n <= coarse_dense_limit) { used = l + 1; d->coarse_mode = 2; break; }
+    }
+    if (d->coarse_mode == 0 && h.levels[used - 1].A.n <= kDenseDirectLimit) d->coarse_mode = 1;
+    d->used = used;
+    d->L.resize(used);
+    for (int l = 0; l < used; ++l) upload_level(ctx, d->L[l], h.levels[l], l + 1 < used);
+    if (d->coarse_mode == 2) build_dense_inverse(ctx, *d, h.levels[used - 1]);
+    return d;
+}
+
+template <class T>
+void refresh_hierarchy_values(cfdxg_context* ctx, DevHierarchy<T>& d, const AmgHierarchy& h) {
+    d.omega = static_cast<T>(h.omega);
+    for (int l = 0; l < d.used; ++l) upload_level_values(ctx, d.L[l], h.levels[l]);
+    if (d.coarse_mode == 2) build_dense_inverse(ctx, d, h.levels[d.used - 1]);
+    // omega is a kernel argument baked into the graph: recapture
+    if (d.exec) { cudaGraphExecDestroy(d.exec); d.exec = nullptr; }
+    if (d.graph) { cudaGraphDestroy(d.graph); d.graph = nullptr; }
+}
+
+template <class T>
+void vcycle_apply(cfdxg_context* ctx, DevHierarchy<T>& d, const double* r, double* z) {
+    cudaStream_t s = ctx->stream;
+    DevLevel<T>& L = d.L[0];
+    const int gb = blocks_for(L.n, kT);
+    if (d.used == 1) {
+        // single-level hierarchy: the coarsest treatment applies to the fine level
+        k_copy_cast<double, T><<<gb, kT, 0, s>>>(L.n, r, L.r.get());
+        check_launch(ctx);
+        enqueue_from(ctx, d, 0);
+        k_copy_cast<T, double><<<gb, kT, 0, s>>>(L.n, L.xout, z);
+        check_launch(ctx);
+        return;
+    }
+    ensure_graph(ctx, d);
+    // Level-0 right-hand side: FP64 reads the caller's r directly; FP32 converts it in the first sweep.
+    const T* rl = nullptr;
+    T* x = L.x.get();
+    T* x2 = L.x2.get();
+    if (std::is_same<T, double>::value) {
+        rl = reinterpret_cast<const T*>(r);
+    } else {
+        rl = L.r.get();
+    }
+    if (d.pre == 0) {
+        if (!std::is_same<T, double>::value) {
+            k_copy_cast<double, T><<<gb, kT, 0, s>>>(L.n, r, L.r.get());
+            check_launch(ctx);
+        }
+        CFDXG_CUDA(cudaMemsetAsync(x, 0, sizeof(T) * L.n, s));
+    } else {
+        k_sweep_zero<T, double><<<gb, kT, 0, s>>>(L.n, d.omega, L.inv_diag.get(), r,
+                                                  std::is_same<T, double>::value ? nullptr : L.r.get(), x,
+                                                  d.status);
+        check_launch(ctx);
+        for (int k = 1; k < d.pre; ++k) {
+            k_sweep<T, T><<<gb, kT, 0, s>>>(L.n, L.ro.get(), L.co.get(), L.va.get(), L.inv_diag.get(), rl,
+                                            x, x2, d.omega, d.status);
+            check_launch(ctx);
+            std::swap(x, x2);
+        }
+    }
+    k_residual<T><<<gb, kT, 0, s>>>(L.n, L.ro.get(), L.co.get(), L.va.get(), rl, x, L.res.get());
+    check_launch(ctx);
+    DevLevel<T>& C = d.L[1];
+    k_restrict<T><<<blocks_for(C.n, kT), kT, 0, s>>>(C.n, L.r_off.get(), L.r_row.get(), L.r_val.get(),
+                                                      L.res.get(), C.r.get());
+    check_launch(ctx);
+    CFDXG_CUDA(cudaGraphLaunch(d.exec, s));
+    count_launch(ctx, d.graph_kernels);
+    k_prolong<T><<<gb, kT, 0, s>>>(L.n, L.p_off.get(), L.p_col.get(), L.p_val.get(), C.xout, x, d.status);
+    check_launch(ctx);
+    if (d.post == 0) {
+        k_copy_cast<T, double><<<gb, kT, 0, s>>>(L.n, x, z);
+        check_launch(ctx);
+        return;
+    }
+    for (int k = 0; k < d.post; ++k) {
+        if (k + 1 == d.post) {
+            k_sweep<T, double><<<gb, kT, 0, s>>>(L.n, L.ro.get(), L.co.get(), L.va.get(), L.inv_diag.get(),
+                                                 rl, x, z, d.omega, d.status);
+        } else {
+            k_sweep<T, T><<<gb, kT, 0, s>>>(L.n, L.ro.get(), L.co.get(), L.va.get(), L.inv_diag.get(), rl,
+                                            x, x2, d.omega, d.status);
+            std::swap(x, x2);
+        }
+        check_launch(ctx);
+    }
+}
+
+template <class T>
+void destroy_hierarchy(DevHierarchy<T>* d) { delete d; }
+
+template std::unique_ptr<DevHierarchy<double>> upload_hierarchy<double>(cfdxg_context*, const AmgHierarchy&, int);
+template std::unique_ptr<DevHierarchy<float>> upload_hierarchy<float>(cfdxg_context*, const AmgHierarchy&, int);
+template void refresh_hierarchy_values<double>(cfdxg_context*, DevHierarchy<double>&, const AmgHierarchy&);
+template void refresh_hierarchy_values<float>(cfdxg_context*, DevHierarchy<float>&, const AmgHierarchy&);
+template void vcycle_apply<double>(cfdxg_context*, DevHierarchy<double>&, const double*, double*);
+template void vcycle_apply<float>(cfdxg_context*, DevHierarchy<float>&, const double*, double*);
+template void destroy_hierarchy<double>(DevHierarchy<double>*);
+template void destroy_hierarchy<float>(DevHierarchy<float>*);
+
+}  // namespace cfdxg

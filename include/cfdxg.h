@@ -1,0 +1,327 @@
+/*
+ * cfdxg.h -- C ABI of the B200-native CFDX pressure-correction hot path.
+ *
+ * One shared library (cfdx_dev_b200/_lib/libcfdxg.so) exports these entry
+ * points.  Signatures use plain pointers, sizes and POD structs only.  Every
+ * function returns an int status and never throws across the ABI:
+ *
+ *   >= 0 : mirrors the reference's SolverStatus (core/linalg/solver_status.h:18)
+ *          CFDXG_CONVERGED, CFDXG_MAX_ITER_REACHED, CFDXG_DIVERGED,
+ *          CFDXG_NOT_APPLICABLE (solves); 0 = success for everything else.
+ *   <  0 : CFDXG_ERR_* (bad argument, CUDA failure, failed setup, ...); the
+ *          message is available from cfdxg_last_error(ctx).
+ *
+ * Array arguments are host or device pointers as stated by an explicit
+ * `mem` flag (CFDXG_MEM_HOST / CFDXG_MEM_DEVICE).  Vector fields are SoA
+ * (x block, then y, then z).  All device work is ordered on the context's
+ * CUDA stream; host-memory calls synchronise before returning.
+ *
+ * The caller owns every array it passes; handles own their device memory.
+ * A handle must not be used concurrently from two threads.
+ */
+#ifndef CFDXG_H
+#define CFDXG_H
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ---- */
+#define CFDXG_OK 0
+#define CFDXG_CONVERGED 0
+#define CFDXG_MAX_ITER_REACHED 1
+#define CFDXG_DIVERGED 2
+#define CFDXG_NOT_APPLICABLE 3
+#define CFDXG_ERR_INVALID_ARGUMENT (-1)
+#define CFDXG_ERR_CUDA (-2)
+#define CFDXG_ERR_SETUP (-3)
+#define CFDXG_ERR_NOT_READY (-4)
+#define CFDXG_ERR_NONFINITE (-5)
+#define CFDXG_ERR_GEOMETRY (-6)
+#define CFDXG_ERR_OUT_OF_MEMORY (-7)
+#define CFDXG_ERR_IO (-8)
+
+#define CFDXG_MEM_HOST 0
+#define CFDXG_MEM_DEVICE 1
+
+/* Krylov / preconditioner / precision choices, numbered as the reference's
+ * KrylovModel and PreconditionerModel enums (core/linalg/linear_solver_models.h:20-55). */
+#define CFDXG_KRYLOV_GMRES 3
+#define CFDXG_KRYLOV_FGMRES 4
+#define CFDXG_PC_NONE 1
+#define CFDXG_PC_JACOBI 2
+#define CFDXG_PC_NATIVE_AMG 6
+#define CFDXG_PRECISION_FP64 0      /* the reference's plain FP64 V-cycle */
+#define CFDXG_PRECISION_FP32_VCYCLE 1  /* FP32 V-cycle inside FP64 FGMRES */
+
+typedef struct cfdxg_context cfdxg_context;
+typedef struct cfdxg_mesh cfdxg_mesh;
+typedef struct cfdxg_matrix cfdxg_matrix;
+typedef struct cfdxg_amg cfdxg_amg;
+typedef struct cfdxg_mpnn cfdxg_mpnn;
+
+/* ------------------------------------------------------------------------ */
+/* context                                                                  */
+/* ------------------------------------------------------------------------ */
+/* New: the reference runs on the host thread; the context binds a CUDA
+ * device and stream (runtime/gpu/cuda_poisson.cu:143 creates neither). */
+int cfdxg_context_create(int32_t device, cfdxg_context** out);
+int cfdxg_context_destroy(cfdxg_context* ctx);
+/* Message of the last failing call on this context ("" after success).
+ * Mirrors NativeAMGPreconditioner::last_error (core/linalg/hypre_amg.h:89-97). */
+const char* cfdxg_last_error(const cfdxg_context* ctx);
+/* Number of kernels this library launched on the context since creation. */
+int64_t cfdxg_kernel_launches(const cfdxg_context* ctx);
+int cfdxg_synchronize(cfdxg_context* ctx);
+
+/* ------------------------------------------------------------------------ */
+/* mesh + geometry  (core/mesh/mesh.h:51, core/mesh/ownership.h:25)          */
+/* ------------------------------------------------------------------------ */
+typedef struct {
+    int64_t n_points, n_faces, n_cells;
+    const double *px, *py, *pz;      /* n_points */
+    const int64_t *face_offsets;     /* n_faces + 1, face -> vertex CSR */
+    const int64_t *face_vertices;
+    const int64_t *owner;            /* n_faces */
+    const int64_t *neighbour;        /* n_faces, -1 on boundary faces */
+    const int64_t *cell_offsets;     /* n_cells + 1, cell -> face CSR */
+    const int64_t *cell_faces;
+    int32_t n_patches;
+    const int32_t *patch_of_face;    /* n_faces, -1 on internal faces */
+    const int32_t *patch_types;      /* n_patches, reference PatchType values */
+} cfdxg_mesh_desc;
+
+/* Copies a host mesh to the device and validates its connectivity. */
+int cfdxg_mesh_upload(cfdxg_context* ctx, const cfdxg_mesh_desc* desc, cfdxg_mesh** out);
+int cfdxg_mesh_destroy(cfdxg_mesh* mesh);
+/* Replaces: build_fv_geometry (physics/finite_volume_transport.h:92-176) and
+ * compute_geometry_cache (core/geometry/geometry_cache.h:66-237), which give
+ * the same centres, volumes and owner-oriented Sf.  Runs on the GPU. */
+int cfdxg_geometry_build(cfdxg_context* ctx, cfdxg_mesh* mesh);
+/* Host copies (SoA) of face centres, owner-oriented Sf, cell centres, volumes. */
+int cfdxg_geometry_download(cfdxg_context* ctx, const cfdxg_mesh* mesh, double* face_centres,
+                            double* face_Sf, double* cell_centres, double* cell_volumes);
+
+/* ------------------------------------------------------------------------ */
+/* sparse matrices  (core/linalg/sparse_matrix.h:27)                         */
+/* ------------------------------------------------------------------------ */
+/* Builds a device CSR from sorted, unique CSR arrays (SparseMatrix::from_sorted_csr,
+ * sparse_matrix.h:136-163). */
+int cfdxg_matrix_create(cfdxg_context* ctx, int64_t n, const int64_t* row_offsets,
+                        const int64_t* columns, const double* values, int32_t mem,
+                        cfdxg_matrix** out);
+int cfdxg_matrix_destroy(cfdxg_matrix* A);
+int cfdxg_matrix_size(const cfdxg_matrix* A, int64_t* n, int64_t* nnz);
+int cfdxg_matrix_download(cfdxg_context* ctx, const cfdxg_matrix* A, int64_t* row_offsets,
+                          int64_t* columns, double* values);
+/* y = A x in FP64, summed per row in CSR order (SparseMatrix::matvec, sparse_matrix.h:180-195). */
+int cfdxg_matrix_spmv(cfdxg_context* ctx, const cfdxg_matrix* A, const double* x, double* y,
+                      int32_t mem);
+
+/* ------------------------------------------------------------------------ */
+/* assembly                                                                  */
+/* ------------------------------------------------------------------------ */
+/* Replaces assemble_cell_diffusion_matrix (core/solvers/scalar_diffusion.h:39-163):
+ * two-point flux Gamma*|Sf|/d, Dirichlet elimination into rhs, Neumann flux,
+ * rhs = S*V.  bc_face_values: n_faces, NaN = unprescribed; bc_face_types:
+ * n_faces (0 Dirichlet, 1 Neumann) or NULL (all Dirichlet).  Allocates *A_out. */
+int cfdxg_assemble_cell_diffusion(cfdxg_context* ctx, cfdxg_mesh* mesh,
+                                  const double* bc_face_values, const int32_t* bc_face_types,
+                                  double diffusivity, const double* source, int32_t mem,
+                                  cfdxg_matrix** A_out, double* rhs);
+
+/* Replaces the pressure-corrector assembly block of solve_steady_incompressible
+ * (physics/steady_incompressible_solver.h:8048-8181 with :6485-6500 and the
+ * fixed-pressure CSR build :8605-8608): phiHbyA = make_mass_flux(HbyA) (:1842),
+ * grad p (:1634), continuity with the Rhie-Chow pressure flux (:1967), face
+ * coefficients (:1914), fixed-pressure boundary rows and sources.
+ * HbyA, rAU: 3*n_cells SoA; p: n_cells; p_bc_fixed / p_bc_value: per patch.
+ * If *A_inout is NULL a matrix is allocated (symbolic pattern built once),
+ * otherwise only its values are refreshed.  b: n_cells.  phiHbyA (n_faces)
+ * and grad_p (3*n_cells) are optional outputs (NULL to skip). */
+int cfdxg_assemble_pressure_correction(cfdxg_context* ctx, cfdxg_mesh* mesh,
+                                       const double* HbyA, const double* rAU, const double* p,
+                                       double rho, const int32_t* p_bc_fixed,
+                                       const double* p_bc_value, int32_t mem,
+                                       cfdxg_matrix** A_inout, double* b, double* phiHbyA,
+                                       double* grad_p);
+
+/* Replaces make_rhie_chow_mass_flux (physics/steady_incompressible_solver.h:2064-2217),
+ * HBYA_PREDICTOR contract, zero-gradient velocity boundaries. flux: n_faces. */
+int cfdxg_rhie_chow_flux(cfdxg_context* ctx, cfdxg_mesh* mesh, const double* HbyA,
+                         const double* rAU, const double* p, double rho,
+                         const int32_t* p_bc_fixed, const double* p_bc_value, int32_t mem,
+                         double* flux);
+
+/* Replaces gauss_gradient_with_boundary (physics/steady_incompressible_solver.h:1634-1744),
+ * default single sweep, distance-weighted interpolation.  grad: 3*n_cells. */
+int cfdxg_gauss_gradient(cfdxg_context* ctx, cfdxg_mesh* mesh, const double* p,
+                         const int32_t* p_bc_fixed, const double* p_bc_value, int32_t mem,
+                         double* grad);
+
+/* ------------------------------------------------------------------------ */
+/* native AMG preconditioner                                                 */
+/* Replaces NativeBoomerAMGPreconditioner (core/linalg/hypre_amg.h:26-101,    */
+/* hypre_amg.cpp:163-330): setup / update_values / apply / name / last_error. */
+/* ------------------------------------------------------------------------ */
+typedef struct {
+    double omega;                    /* 0.7 (Balanced policy, hypre_amg.cpp:172) */
+    int32_t pre_sweeps;              /* 6 */
+    int32_t post_sweeps;             /* 6 */
+    double strength_threshold;       /* 0.25 */
+    int32_t max_levels;              /* 25 */
+    int32_t require_smoother_certificate; /* 1 for CG plans, 0 for GMRES/FGMRES */
+    int32_t precision;               /* CFDXG_PRECISION_* of the V-cycle */
+    int32_t coarse_dense_limit;      /* FP32 V-cycle: dense FP64 LU at the first
+                                        level with <= this many rows (2000) */
+} cfdxg_amg_options;
+
+int cfdxg_amg_options_default(cfdxg_amg_options* opts);
+/* ctx may be NULL (host-only use). */
+int cfdxg_amg_create(cfdxg_context* ctx, const cfdxg_amg_options* opts, cfdxg_amg** out);
+int cfdxg_amg_destroy(cfdxg_amg* amg);
+/* Preconditioner::setup (core/linalg/preconditioner.h:22) */
+int cfdxg_amg_setup(cfdxg_context* ctx, cfdxg_amg* amg, const cfdxg_matrix* A);
+/* Preconditioner::update_values (preconditioner.h:26) -- unchanged pattern only */
+int cfdxg_amg_update_values(cfdxg_context* ctx, cfdxg_amg* amg, const cfdxg_matrix* A);
+/* Preconditioner::apply (preconditioner.h:27): z = one V-cycle applied to r */
+int cfdxg_amg_apply(cfdxg_context* ctx, cfdxg_amg* amg, const double* r, double* z, int32_t mem);
+const char* cfdxg_amg_name(const cfdxg_amg* amg);          /* preconditioner.h:28 */
+const char* cfdxg_amg_last_error(const cfdxg_amg* amg);    /* hypre_amg.h:97 */
+/* Hierarchy diagnostics (hypre_amg.h:66-73 hierarchy_level_sizes/_nnz, smoother omega). */
+int32_t cfdxg_amg_num_levels(const cfdxg_amg* amg);
+double cfdxg_amg_omega(const cfdxg_amg* amg);
+int cfdxg_amg_level_info(const cfdxg_amg* amg, int32_t level, int64_t* n_rows, int64_t* nnz,
+                         int64_t* p_nnz);
+/* Host copies of one level: A (CSR), inverse diagonal, prolongation (CSR),
+ * aggregate (strongest interpolation column per fine row, amg_preconditioner.h:349). */
+int cfdxg_amg_export_level(const cfdxg_amg* amg, int32_t level, int64_t* row_offsets,
+                           int64_t* columns, double* values, double* inv_diag,
+                           int64_t* p_offsets, int64_t* p_columns, double* p_values,
+                           int64_t* aggregate);
+double cfdxg_amg_setup_seconds(const cfdxg_amg* amg);
+/* Host-only hierarchy construction from host CSR arrays, without a device
+ * upload (ctx may be NULL): the same setup as cfdxg_amg_setup, for
+ * inspection and parity checks on machines without a GPU.  The handle can
+ * be exported from but not applied. */
+int cfdxg_amg_setup_host(cfdxg_amg* amg, int64_t n, const int64_t* row_offsets,
+                         const int64_t* columns, const double* values);
+
+/* ------------------------------------------------------------------------ */
+/* Krylov solves                                                             */
+/* ------------------------------------------------------------------------ */
+/* Mirrors LinearSolverRequest (core/linalg/linear_solver_models.h:164-189),
+ * KrylovControls (core/linalg/krylov_controls.h:10-26) and the precision /
+ * learned-preconditioner choices of this library. */
+typedef struct {
+    int32_t krylov;                  /* CFDXG_KRYLOV_GMRES / _FGMRES */
+    int32_t preconditioner;          /* CFDXG_PC_* */
+    int32_t gmres_restart;           /* 40 in the reference's request default */
+    int32_t precision;               /* CFDXG_PRECISION_* */
+    int32_t restart_min;             /* 10 */
+    int32_t restart_max;             /* 512 */
+    int32_t adaptive_restart;        /* 1 */
+    int32_t residual_replacement;    /* 1 */
+    int64_t residual_replacement_period; /* 50 */
+    double residual_replacement_gap_ratio; /* 10 */
+    double target_reduction_per_cycle;     /* 0.1 */
+    cfdxg_mpnn* learned;             /* NULL, or a trained network applied before the V-cycle */
+} cfdxg_request;
+
+/* Mirrors SolverResult (core/linalg/solver_status.h:45-72) + LinearSolveReport. */
+typedef struct {
+    int32_t status;
+    int64_t iterations;
+    double residual;
+    double residual_relative;
+    double physical_residual_relative;
+    int64_t residual_replacements;
+    double max_true_recursive_gap;
+    double setup_seconds;
+    double solve_seconds;
+    int64_t preconditioner_applications;
+    int64_t learned_fallbacks;
+} cfdxg_report;
+
+int cfdxg_request_default(cfdxg_request* req);
+
+/* Replaces solve_linear_system (core/linalg/linear_solver_dispatch.h:227-492) for
+ * scalar pressure systems without scaling / null space: builds the requested
+ * preconditioner (AMG setup inside, as the reference), solves with
+ * right-preconditioned GMRES/FGMRES, then certifies the FP64 physical residual. */
+int cfdxg_solve_linear_system(cfdxg_context* ctx, const cfdxg_matrix* A, const double* rhs,
+                              double* x, int32_t mem, const cfdxg_request* req,
+                              int64_t max_iterations, double tolerance, cfdxg_report* report);
+
+/* Replaces solve_gmres / solve_fgmres with an already set-up preconditioner
+ * (core/linalg/gmres_solver.h:28-600, 690-757, setup_preconditioner = false).
+ * amg may be NULL (identity). */
+int cfdxg_solve_gmres(cfdxg_context* ctx, const cfdxg_matrix* A, cfdxg_amg* amg,
+                      const double* rhs, double* x, int32_t mem, const cfdxg_request* req,
+                      int64_t max_iterations, double tolerance, cfdxg_report* report);
+
+/* ------------------------------------------------------------------------ */
+/* learned message-passing preconditioner (no reference counterpart)          */
+/* ------------------------------------------------------------------------ */
+/* A 4-round, 32-feature message-passing network on the mesh's cell-face
+ * graph; BF16 weights, FP32 state and accumulation. Applied before the AMG
+ * V-cycle inside FGMRES; plain AMG is used whenever it fails to reduce the
+ * FP64 true residual. */
+int cfdxg_mpnn_create(cfdxg_context* ctx, uint64_t seed, cfdxg_mpnn** out);
+int cfdxg_mpnn_destroy(cfdxg_mpnn* net);
+int cfdxg_mpnn_num_parameters(const cfdxg_mpnn* net, int64_t* count);
+/* Host FP32 copies of the master weights (BF16 copies are derived from them). */
+int cfdxg_mpnn_get_parameters(cfdxg_context* ctx, const cfdxg_mpnn* net, float* params);
+int cfdxg_mpnn_set_parameters(cfdxg_context* ctx, cfdxg_mpnn* net, const float* params);
+int cfdxg_mpnn_save(cfdxg_context* ctx, const cfdxg_mpnn* net, const char* path);
+int cfdxg_mpnn_load(cfdxg_context* ctx, cfdxg_mpnn* net, const char* path);
+/* Binds the network to a mesh + matrix (graph features: volume, a_P, face area/distance). */
+int cfdxg_mpnn_bind(cfdxg_context* ctx, cfdxg_mpnn* net, cfdxg_mesh* mesh, const cfdxg_matrix* A,
+                    const double* a_P, int32_t mem);
+/* y = N(r) for one residual (FP64 in/out). */
+int cfdxg_mpnn_apply(cfdxg_context* ctx, cfdxg_mpnn* net, const double* r, double* y, int32_t mem);
+/* One Adam step on a batch of (residual, error) pairs: loss = mean over pairs of
+ * (e - N(r))^T A (e - N(r)) / (e^T A e).  r, e: batch * n_cells, row-major. */
+int cfdxg_mpnn_train_step(cfdxg_context* ctx, cfdxg_mpnn* net, const double* r, const double* e,
+                          int32_t batch, float learning_rate, int32_t mem, double* loss);
+/* Loss and parameter gradient without an update (for gradient checks). */
+int cfdxg_mpnn_loss_grad(cfdxg_context* ctx, cfdxg_mpnn* net, const double* r, const double* e,
+                         int32_t batch, int32_t mem, double* loss, float* grad);
+
+/* ------------------------------------------------------------------------ */
+/* synthetic cases (seeded generators for the benchmark configurations)      */
+/* ------------------------------------------------------------------------ */
+typedef struct cfdxg_case cfdxg_case;
+/* Hex lattice nx*ny*nz on the unit cube, face numbering of the reference's
+ * hex fixture (tests/validation/thermal_3d_mesh_v36.h:18-80), patches
+ * west,east,south,north,bottom,top = 0..5. */
+int cfdxg_case_hex(int64_t nx, int64_t ny, int64_t nz, cfdxg_case** out);
+/* Kuhn 6-tet split of an n^3 lattice on the unit cube, face numbering of the
+ * reference's tet fixture (tests/validation/radiation_tetrahedral_mesh_v52.h:14-92);
+ * interior vertices jittered by U[-jitter*h, jitter*h] per coordinate.
+ * Patches xmin,xmax,ymin,ymax,zmin,zmax = 0..5. */
+int cfdxg_case_tet(int64_t n, double jitter, uint64_t seed, cfdxg_case** out);
+/* Boundary-layer hex nx*ny*nz on [0,lx]x[0,1]x[0,lz]: y spacing dy0*growth^j
+ * capped so the column fills [0,1]; x/z interior lines jittered by +-jitter*h. */
+int cfdxg_case_boundary_layer(int64_t nx, int64_t ny, int64_t nz, double lx, double lz,
+                              double dy0, double growth, double jitter, uint64_t seed,
+                              cfdxg_case** out);
+int cfdxg_case_destroy(cfdxg_case* c);
+/* sizes: n_points, n_faces, n_face_vertices, n_cells, n_cell_faces, n_patches */
+int cfdxg_case_sizes(const cfdxg_case* c, int64_t* sizes);
+int cfdxg_case_export(const cfdxg_case* c, double* px, double* py, double* pz,
+                      int64_t* face_offsets, int64_t* face_vertices, int64_t* owner,
+                      int64_t* neighbour, int64_t* cell_offsets, int64_t* cell_faces,
+                      int32_t* patch_of_face, int32_t* patch_types);
+/* Seeded fields at the given cell centres (SoA 3*n): divergence-free sum of
+ * n_modes Fourier modes with amplitude 1/|k|^2 plus U[-perturbation, perturbation]. */
+int cfdxg_field_fourier(int64_t n, const double* centres, int32_t n_modes, double perturbation,
+                        uint64_t seed, double* u);
+/* Seeded per-cell values: log-uniform on [lo, hi] (kind 0) or uniform (kind 1). */
+int cfdxg_field_random(int64_t n, int32_t kind, double lo, double hi, uint64_t seed, double* v);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* CFDXG_H */

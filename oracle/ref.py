@@ -1,0 +1,273 @@
+"""ctypes wrapper of the reference-built oracle (oracle/_ref/libcfdx_ref.so).
+
+TEST INFRASTRUCTURE ONLY: used by tests/, __graft_entry__.smoke() and the
+CPU-baseline legs of bench.py as the checker / reference timing.  The product
+(cfdx_dev_b200) never imports it.  Build it with ``make -C oracle ref`` (needs
+the reference source tree); the built .so then works without that tree.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+LIB_PATH = HERE / "_ref" / "libcfdx_ref.so"
+
+_c_i64p = C.POINTER(C.c_int64)
+_c_i32p = C.POINTER(C.c_int32)
+_c_f64p = C.POINTER(C.c_double)
+
+
+class RefMesh(C.Structure):
+    _fields_ = [
+        ("n_points", C.c_int64), ("n_faces", C.c_int64), ("n_cells", C.c_int64),
+        ("px", _c_f64p), ("py", _c_f64p), ("pz", _c_f64p),
+        ("face_offsets", _c_i64p), ("face_vertices", _c_i64p),
+        ("owner", _c_i64p), ("neighbour", _c_i64p),
+        ("cell_offsets", _c_i64p), ("cell_faces", _c_i64p),
+        ("n_patches", C.c_int32), ("patch_of_face", _c_i32p), ("patch_types", _c_i32p),
+    ]
+
+
+class RefReport(C.Structure):
+    _fields_ = [("status", C.c_int32), ("iterations", C.c_int64), ("residual", C.c_double),
+                ("residual_relative", C.c_double), ("physical_residual_relative", C.c_double),
+                ("setup_seconds", C.c_double), ("solve_seconds", C.c_double)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+_lib = None
+
+
+def available() -> bool:
+    return LIB_PATH.exists()
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not LIB_PATH.exists():
+            raise RuntimeError(f"{LIB_PATH} missing: run `make -C oracle ref`")
+        _lib = C.CDLL(str(LIB_PATH))
+        _lib.ref_last_error.restype = C.c_char_p
+        _lib.ref_amg_create.restype = C.c_void_p
+        _lib.ref_amg_create.argtypes = [C.c_int64, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int32, C.c_void_p]
+        _lib.ref_amg_destroy.argtypes = [C.c_void_p]
+        _lib.ref_amg_num_levels.argtypes = [C.c_void_p]
+        _lib.ref_amg_omega.argtypes = [C.c_void_p]
+        _lib.ref_amg_omega.restype = C.c_double
+        _lib.ref_amg_level_sizes.argtypes = [C.c_void_p, C.c_int32, _c_i64p, _c_i64p, _c_i64p]
+        _lib.ref_amg_level_matrix.argtypes = [C.c_void_p, C.c_int32] + [C.c_void_p] * 4
+        _lib.ref_amg_level_prolongation.argtypes = [C.c_void_p, C.c_int32] + [C.c_void_p] * 4
+        _lib.ref_amg_apply.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p]
+        _lib.ref_solve_gmres_prepared.argtypes = [C.c_void_p, C.c_int64, C.c_void_p, C.c_void_p, C.c_void_p,
+                                                  C.c_void_p, C.c_void_p, C.c_int32, C.c_int64, C.c_double,
+                                                  C.c_void_p]
+        _lib.ref_solve_linear_system.argtypes = [C.c_int64, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                                 C.c_void_p, C.c_int32, C.c_int32, C.c_int32, C.c_int64,
+                                                 C.c_double, C.c_void_p]
+        _lib.ref_assemble_diffusion.restype = C.c_int64
+        _lib.ref_assemble_diffusion.argtypes = [C.c_void_p, C.c_void_p, C.c_double] + [C.c_void_p] * 6
+        _lib.ref_simple_assemble.restype = C.c_int64
+        _lib.ref_simple_assemble.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_double] + \
+            [C.c_void_p] * 9
+        _lib.ref_rhie_chow_flux.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_double] + \
+            [C.c_void_p] * 3
+        _lib.ref_gauss_gradient.argtypes = [C.c_void_p] * 5
+        _lib.ref_fixture_tet_v52_sizes.argtypes = [C.c_int64, C.c_void_p]
+        _lib.ref_fixture_tet_v52.argtypes = [C.c_int64] + [C.c_void_p] * 9
+        _lib.ref_geometry_cache.argtypes = [C.c_void_p] * 5
+        _lib.ref_fv_geometry.argtypes = [C.c_void_p] * 5
+        _lib.ref_spmv.argtypes = [C.c_int64] + [C.c_void_p] * 5
+    return _lib
+
+
+def _p(a):
+    return None if a is None else a.ctypes.data_as(C.c_void_p)
+
+
+def _check(rc, what):
+    if rc < 0:
+        raise RuntimeError(f"reference {what} failed: {lib().ref_last_error().decode()}")
+    return rc
+
+
+class _MeshHolder:
+    def __init__(self, m):
+        self.m = m  # keep arrays alive
+        self.s = RefMesh()
+        s = self.s
+        s.n_points, s.n_faces, s.n_cells = m.px.size, m.owner.size, m.cell_offsets.size - 1
+        for k in ("px", "py", "pz"):
+            setattr(s, k, getattr(m, k).ctypes.data_as(_c_f64p))
+        for k in ("face_offsets", "face_vertices", "owner", "neighbour", "cell_offsets", "cell_faces"):
+            setattr(s, k, getattr(m, k).ctypes.data_as(_c_i64p))
+        s.n_patches = m.patch_types.size
+        s.patch_of_face = m.patch_of_face.ctypes.data_as(_c_i32p)
+        s.patch_types = m.patch_types.ctypes.data_as(_c_i32p)
+
+    @property
+    def ptr(self):
+        return C.byref(self.s)
+
+
+def fixture_tet_v52(n: int) -> dict:
+    sizes = np.zeros(5, np.int64)
+    _check(lib().ref_fixture_tet_v52_sizes(n, _p(sizes)), "tet fixture")
+    npnt, nf, nfv, nc, ncf = (int(v) for v in sizes)
+    out = dict(px=np.empty(npnt), py=np.empty(npnt), pz=np.empty(npnt), face_offsets=np.empty(nf + 1, np.int64),
+               face_vertices=np.empty(nfv, np.int64), owner=np.empty(nf, np.int64),
+               neighbour=np.empty(nf, np.int64), cell_offsets=np.empty(nc + 1, np.int64),
+               cell_faces=np.empty(ncf, np.int64))
+    _check(lib().ref_fixture_tet_v52(n, *(_p(out[k]) for k in (
+        "px", "py", "pz", "face_offsets", "face_vertices", "owner", "neighbour", "cell_offsets", "cell_faces"))),
+        "tet fixture")
+    return out
+
+
+def geometry(mesh, kind: str = "fv") -> dict:
+    h = _MeshHolder(mesh)
+    nf, nc = mesh.owner.size, mesh.cell_offsets.size - 1
+    out = dict(face_centres=np.empty(3 * nf), face_Sf=np.empty(3 * nf), cell_centres=np.empty(3 * nc),
+               cell_volumes=np.empty(nc))
+    fn = lib().ref_fv_geometry if kind == "fv" else lib().ref_geometry_cache
+    _check(fn(h.ptr, *(_p(out[k]) for k in ("face_centres", "face_Sf", "cell_centres", "cell_volumes"))), "geometry")
+    return out
+
+
+def assemble_diffusion(mesh, bc_values, diffusivity, source):
+    h = _MeshHolder(mesh)
+    nc, nf = mesh.cell_offsets.size - 1, mesh.owner.size
+    ro = np.empty(nc + 1, np.int64)
+    co = np.empty(nc + 2 * nf, np.int64)
+    va = np.empty(nc + 2 * nf)
+    rhs = np.empty(nc)
+    sec = C.c_double()
+    bc = np.ascontiguousarray(bc_values, dtype=np.float64)
+    src = np.ascontiguousarray(source, dtype=np.float64)
+    nnz = _check(lib().ref_assemble_diffusion(h.ptr, _p(bc), float(diffusivity), _p(src), _p(ro), _p(co), _p(va),
+                                              _p(rhs), C.byref(sec)), "assemble_cell_diffusion_matrix")
+    return ro, co[:nnz].copy(), va[:nnz].copy(), rhs, sec.value
+
+
+def simple_assemble(mesh, HbyA, rAU, p, rho, p_bc_fixed, p_bc_value):
+    h = _MeshHolder(mesh)
+    nc, nf = mesh.cell_offsets.size - 1, mesh.owner.size
+    ro = np.empty(nc + 1, np.int64)
+    co = np.empty(nc + 2 * nf, np.int64)
+    va = np.empty(nc + 2 * nf)
+    b = np.empty(nc)
+    phi = np.empty(nf)
+    grad = np.empty(3 * nc)
+    sec = C.c_double()
+    args = [np.ascontiguousarray(a, dtype=np.float64) for a in (HbyA, rAU, p)]
+    fixed = np.ascontiguousarray(p_bc_fixed, dtype=np.int32)
+    value = np.ascontiguousarray(p_bc_value, dtype=np.float64)
+    nnz = _check(lib().ref_simple_assemble(h.ptr, *(_p(a) for a in args), float(rho), _p(fixed), _p(value), _p(phi),
+                                           _p(grad), _p(ro), _p(co), _p(va), _p(b), C.byref(sec)),
+                 "pressure-corrector assembly")
+    return dict(row_offsets=ro, columns=co[:nnz].copy(), values=va[:nnz].copy(), b=b, phiHbyA=phi, grad_p=grad,
+                seconds=sec.value)
+
+
+def rhie_chow_flux(mesh, HbyA, rAU, p, rho, p_bc_fixed, p_bc_value):
+    h = _MeshHolder(mesh)
+    flux = np.empty(mesh.owner.size)
+    args = [np.ascontiguousarray(a, dtype=np.float64) for a in (HbyA, rAU, p)]
+    fixed = np.ascontiguousarray(p_bc_fixed, dtype=np.int32)
+    value = np.ascontiguousarray(p_bc_value, dtype=np.float64)
+    _check(lib().ref_rhie_chow_flux(h.ptr, *(_p(a) for a in args), float(rho), _p(fixed), _p(value), _p(flux)),
+           "make_rhie_chow_mass_flux")
+    return flux
+
+
+def gauss_gradient(mesh, p, p_bc_fixed, p_bc_value):
+    h = _MeshHolder(mesh)
+    g = np.empty(3 * (mesh.cell_offsets.size - 1))
+    pp = np.ascontiguousarray(p, dtype=np.float64)
+    fixed = np.ascontiguousarray(p_bc_fixed, dtype=np.int32)
+    value = np.ascontiguousarray(p_bc_value, dtype=np.float64)
+    _check(lib().ref_gauss_gradient(h.ptr, _p(pp), _p(fixed), _p(value), _p(g)), "gauss_gradient")
+    return g
+
+
+def spmv(ro, co, va, x):
+    y = np.empty(ro.size - 1)
+    _check(lib().ref_spmv(ro.size - 1, _p(ro), _p(co), _p(va), _p(np.ascontiguousarray(x, dtype=np.float64)), _p(y)),
+           "spmv")
+    return y
+
+
+class Amg:
+    """The reference's native Boomer-style AMG, Balanced policy."""
+
+    def __init__(self, ro, co, va, require_smoother_certificate=False):
+        self.ro, self.co, self.va = (np.ascontiguousarray(ro, np.int64), np.ascontiguousarray(co, np.int64),
+                                     np.ascontiguousarray(va, np.float64))
+        sec = C.c_double()
+        self.h = lib().ref_amg_create(self.ro.size - 1, _p(self.ro), _p(self.co), _p(self.va),
+                                      int(require_smoother_certificate), C.byref(sec))
+        if not self.h:
+            raise RuntimeError(f"reference AMG setup failed: {lib().ref_last_error().decode()}")
+        self.setup_seconds = sec.value
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            lib().ref_amg_destroy(self.h)
+            self.h = None
+
+    @property
+    def omega(self):
+        return lib().ref_amg_omega(self.h)
+
+    def num_levels(self):
+        return lib().ref_amg_num_levels(self.h)
+
+    def level(self, l: int) -> dict:
+        n, nnz, pn = C.c_int64(), C.c_int64(), C.c_int64()
+        lib().ref_amg_level_sizes(self.h, l, C.byref(n), C.byref(nnz), C.byref(pn))
+        n, nnz, pn = n.value, nnz.value, pn.value
+        out = dict(row_offsets=np.empty(n + 1, np.int64), columns=np.empty(nnz, np.int64), values=np.empty(nnz),
+                   inv_diag=np.empty(n))
+        lib().ref_amg_level_matrix(self.h, l, _p(out["row_offsets"]), _p(out["columns"]), _p(out["values"]),
+                                   _p(out["inv_diag"]))
+        if pn:
+            out.update(p_offsets=np.empty(n + 1, np.int64), p_columns=np.empty(pn, np.int64),
+                       p_values=np.empty(pn), aggregate=np.empty(n, np.int64))
+            lib().ref_amg_level_prolongation(self.h, l, _p(out["p_offsets"]), _p(out["p_columns"]),
+                                             _p(out["p_values"]), _p(out["aggregate"]))
+        else:
+            out.update(p_offsets=None, p_columns=np.empty(0, np.int64), p_values=np.empty(0), aggregate=None)
+        return out
+
+    def apply(self, r):
+        r = np.ascontiguousarray(r, np.float64)
+        z = np.empty_like(r)
+        rc = lib().ref_amg_apply(self.h, _p(r), _p(z))
+        if rc != 0:
+            raise RuntimeError("reference V-cycle failed")
+        return z
+
+    def solve_gmres(self, rhs, x0=None, restart=30, max_iterations=1000, tolerance=1e-8):
+        b = np.ascontiguousarray(rhs, np.float64)
+        x = np.zeros_like(b) if x0 is None else np.array(x0, dtype=np.float64)
+        rep = RefReport()
+        _check(lib().ref_solve_gmres_prepared(self.h, b.size, _p(self.ro), _p(self.co), _p(self.va), _p(b), _p(x),
+                                              restart, max_iterations, tolerance, C.byref(rep)), "solve_gmres")
+        return x, rep.as_dict()
+
+
+def solve_linear_system(ro, co, va, rhs, x0=None, krylov=3, preconditioner=6, restart=30, max_iterations=1000,
+                        tolerance=1e-8):
+    ro, co, va = (np.ascontiguousarray(ro, np.int64), np.ascontiguousarray(co, np.int64),
+                  np.ascontiguousarray(va, np.float64))
+    b = np.ascontiguousarray(rhs, np.float64)
+    x = np.zeros_like(b) if x0 is None else np.array(x0, dtype=np.float64)
+    rep = RefReport()
+    _check(lib().ref_solve_linear_system(b.size, _p(ro), _p(co), _p(va), _p(b), _p(x), krylov, preconditioner,
+                                         restart, max_iterations, tolerance, C.byref(rep)), "solve_linear_system")
+    return x, rep.as_dict()

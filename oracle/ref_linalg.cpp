@@ -1,0 +1,154 @@
+// ref_linalg.cpp -- oracle adapter: reference geometry cache, Poisson
+// assembly, solve_linear_system dispatch and mesh fixtures.
+//
+// TEST INFRASTRUCTURE ONLY (see ref_abi.h).  Every function forwards to the
+// reference's own implementation compiled from its sources.
+#include "cfdx/core/geometry/geometry_cache.h"
+#include "cfdx/core/linalg/linear_solver_dispatch.h"
+#include "cfdx/core/solvers/scalar_diffusion.h"
+#include "validation/radiation_tetrahedral_mesh_v52.h"
+
+#include "ref_common.h"
+
+using namespace cfdx::core;
+
+extern "C" const char* ref_last_error(void) { return cfdx_ref::g_error.c_str(); }
+
+extern "C" int ref_fixture_tet_v52_sizes(int64_t n, int64_t* sizes) {
+    try {
+        const Mesh m = cfdx::testing::radiation_v52::tetrahedral_mesh(static_cast<std::size_t>(n));
+        sizes[0] = static_cast<int64_t>(m.n_points());
+        sizes[1] = static_cast<int64_t>(m.n_faces());
+        sizes[2] = static_cast<int64_t>(m.faces().n_vertices());
+        sizes[3] = static_cast<int64_t>(m.n_cells());
+        sizes[4] = static_cast<int64_t>(m.cells().offsets_data()[m.n_cells()]);
+        return 0;
+    } catch (const std::exception& e) {
+        cfdx_ref::set_error(e);
+        return -1;
+    }
+}
+
+extern "C" int ref_fixture_tet_v52(int64_t n, double* px, double* py, double* pz,
+                                   int64_t* fo, int64_t* fv, int64_t* owner, int64_t* neighbour,
+                                   int64_t* co, int64_t* cf) {
+    try {
+        const Mesh m = cfdx::testing::radiation_v52::tetrahedral_mesh(static_cast<std::size_t>(n));
+        for (std::size_t i = 0; i < m.n_points(); ++i) {
+            px[i] = m.points().x(i);
+            py[i] = m.points().y(i);
+            pz[i] = m.points().z(i);
+        }
+        for (std::size_t f = 0; f <= m.n_faces(); ++f) fo[f] = static_cast<int64_t>(m.faces().offsets_data()[f]);
+        for (std::size_t k = 0; k < m.faces().n_vertices(); ++k) fv[k] = static_cast<int64_t>(m.faces().vertices_data()[k]);
+        for (std::size_t f = 0; f < m.n_faces(); ++f) {
+            owner[f] = static_cast<int64_t>(m.ownership().owner(f));
+            neighbour[f] = m.ownership().neighbour(f);
+        }
+        for (std::size_t c = 0; c <= m.n_cells(); ++c) co[c] = static_cast<int64_t>(m.cells().offsets_data()[c]);
+        for (std::size_t k = 0; k < m.cells().offsets_data()[m.n_cells()]; ++k)
+            cf[k] = static_cast<int64_t>(m.cells().faces_data()[k]);
+        return 0;
+    } catch (const std::exception& e) {
+        cfdx_ref::set_error(e);
+        return -1;
+    }
+}
+
+static void export_vec3(const std::vector<Vec3>& v, double* out) {
+    const std::size_t n = v.size();
+    for (std::size_t i = 0; i < n; ++i) {
+        out[i] = v[i].x;
+        out[n + i] = v[i].y;
+        out[2 * n + i] = v[i].z;
+    }
+}
+
+extern "C" int ref_geometry_cache(const ref_mesh_t* m, double* fc, double* sf, double* cc, double* cv) {
+    try {
+        const Mesh mesh = cfdx_ref::make_mesh(*m);
+        const GeometryCache g = make_geometry_cache(mesh);
+        export_vec3(g.face_centres, fc);
+        export_vec3(g.face_Sf, sf);
+        export_vec3(g.cell_centres, cc);
+        for (std::size_t c = 0; c < g.cell_volumes.size(); ++c) cv[c] = g.cell_volumes[c];
+        return 0;
+    } catch (const std::exception& e) {
+        cfdx_ref::set_error(e);
+        return -1;
+    }
+}
+
+extern "C" int64_t ref_assemble_diffusion(const ref_mesh_t* m, const double* bc, double gamma,
+                                          const double* source, int64_t* ro, int64_t* co,
+                                          double* va, double* rhs, double* seconds) {
+    try {
+        const Mesh mesh = cfdx_ref::make_mesh(*m);
+        DirichletBoundary boundary = PoissonBoundaryCondition::dirichlet(mesh.n_faces());
+        for (std::size_t f = 0; f < mesh.n_faces(); ++f) boundary.face_values[f] = bc[f];
+        const std::vector<double> src(source, source + m->n_cells);
+        Vector b;
+        const GeometryCache geometry = make_geometry_cache(mesh);
+        const double t0 = cfdx_ref::now_seconds();
+        const SparseMatrix A = assemble_cell_diffusion_matrix(mesh, boundary, gamma, src, b, geometry);
+        if (seconds) *seconds = cfdx_ref::now_seconds() - t0;
+        for (std::size_t i = 0; i < b.size(); ++i) rhs[i] = b(i);
+        return cfdx_ref::export_csr(A, ro, co, va);
+    } catch (const std::exception& e) {
+        cfdx_ref::set_error(e);
+        return -1;
+    }
+}
+
+extern "C" int ref_solve_linear_system(int64_t n, const int64_t* ro, const int64_t* co,
+                                       const double* va, const double* rhs, double* x,
+                                       int32_t krylov, int32_t preconditioner, int32_t restart,
+                                       int64_t max_iterations, double tolerance,
+                                       ref_report_t* report) {
+    try {
+        const SparseMatrix A = cfdx_ref::make_csr(n, ro, co, va);
+        Vector b(static_cast<std::size_t>(n)), xv(static_cast<std::size_t>(n));
+        for (int64_t i = 0; i < n; ++i) {
+            b(i) = rhs[i];
+            xv(i) = x[i];
+        }
+        LinearSolverRequest request;
+        request.krylov = static_cast<KrylovModel>(krylov);
+        request.preconditioner = static_cast<PreconditionerModel>(preconditioner);
+        request.gmres_restart = restart;
+        const double t0 = cfdx_ref::now_seconds();
+        const LinearSolveReport r = solve_linear_system(
+            A, b, xv, LinearProblemKind::PressurePoisson, request,
+            static_cast<std::size_t>(max_iterations), tolerance);
+        const double t1 = cfdx_ref::now_seconds();
+        for (int64_t i = 0; i < n; ++i) x[i] = xv(i);
+        if (report) {
+            report->status = static_cast<int32_t>(r.result.status);
+            report->iterations = static_cast<int64_t>(r.result.iterations);
+            report->residual = r.result.residual;
+            report->residual_relative = r.result.residual_relative;
+            report->physical_residual_relative = r.physical_residual_relative;
+            report->setup_seconds = 0.0;
+            report->solve_seconds = t1 - t0;
+        }
+        cfdx_ref::g_error = r.preconditioner_error;
+        return 0;
+    } catch (const std::exception& e) {
+        cfdx_ref::set_error(e);
+        return -1;
+    }
+}
+
+extern "C" int ref_spmv(int64_t n, const int64_t* ro, const int64_t* co, const double* va,
+                        const double* x, double* y) {
+    try {
+        const SparseMatrix A = cfdx_ref::make_csr(n, ro, co, va);
+        const std::vector<double> xv(x, x + n);
+        const auto yv = A.matvec(xv);
+        for (int64_t i = 0; i < n; ++i) y[i] = yv[i];
+        return 0;
+    } catch (const std::exception& e) {
+        cfdx_ref::set_error(e);
+        return -1;
+    }
+}

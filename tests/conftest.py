@@ -1,0 +1,58 @@
+"""Shared pytest setup.
+
+* registers the ``gpu`` marker (tests that need a B200);
+* makes the in-tree library and the reference-built oracle available,
+  building them when their sources are present and the binaries are not.
+"""
+from __future__ import annotations
+
+import os
+import subprocess
+import sys
+from pathlib import Path
+
+import pytest
+
+ROOT = Path(__file__).resolve().parents[1]
+if str(ROOT) not in sys.path:
+    sys.path.insert(0, str(ROOT))
+
+REF_SRC = Path("/root/reference")
+
+
+def pytest_configure(config):
+    config.addinivalue_line("markers", "gpu: needs a CUDA device (B200)")
+    lib = ROOT / "cfdx_dev_b200" / "_lib" / "libcfdxg.so"
+    if not lib.exists():
+        from cfdx_dev_b200 import build as b
+        b.build()
+    ref_lib = ROOT / "oracle" / "_ref" / "libcfdx_ref.so"
+    if not ref_lib.exists() and REF_SRC.exists():
+        subprocess.run(["make", "-s", "-C", str(ROOT / "oracle"), "ref", "oracle"], check=True)
+    c_lib = ROOT / "oracle" / "_build" / "libcfdx_oracle.so"
+    if not c_lib.exists() and (ROOT / "oracle" / "cfdx_oracle.c").exists():
+        subprocess.run(["make", "-s", "-C", str(ROOT / "oracle"), "oracle"], check=True)
+
+
+def gpu_available() -> bool:
+    try:
+        import torch
+        return torch.cuda.is_available()
+    except Exception:  # pragma: no cover
+        return False
+
+
+@pytest.fixture(scope="session")
+def ctx():
+    from cfdx_dev_b200 import Context
+    c = Context(int(os.environ.get("CFDXG_TEST_DEVICE", "0")))
+    yield c
+    c.close()
+
+
+@pytest.fixture(scope="session")
+def ref():
+    from oracle import ref as r
+    if not r.available():
+        pytest.skip("reference oracle library not built")
+    return r

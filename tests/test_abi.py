@@ -1,0 +1,35 @@
+"""The C ABI library loads and exports every entry point include/cfdxg.h declares."""
+import re
+from pathlib import Path
+
+ROOT = Path(__file__).resolve().parents[1]
+
+
+def declared_symbols():
+    text = (ROOT / "include" / "cfdxg.h").read_text()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(r"\b(cfdxg_[a-z0-9_]+)\s*\(", text)))
+
+
+def test_library_loads_and_exports_every_declared_symbol():
+    from cfdx_dev_b200 import _native
+    lib = _native.load()
+    syms = declared_symbols()
+    assert len(syms) > 40
+    missing = [s for s in syms if not hasattr(lib, s)]
+    assert not missing, missing
+    # and every declared entry point has a ctypes prototype in the binding
+    assert not [s for s in syms if s not in _native.PROTOTYPES]
+
+
+def test_build_targets_sm100a_only():
+    from cfdx_dev_b200 import build
+    assert build.ARCH == ["-gencode", "arch=compute_100a,code=sm_100a"]
+
+
+def test_host_only_calls_need_no_device():
+    import cfdx_dev_b200 as cg
+    m = cg.hex_case(3)
+    assert m.n_cells == 27 and m.n_faces == 108
+    amg = cg.NativeBoomerAMGPreconditioner(None)
+    assert amg.name() == "NativeBoomerStyleAMG"

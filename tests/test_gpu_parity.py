@@ -1,0 +1,173 @@
+"""GPU parity against the reference-built oracle, through the C ABI.
+
+Bit-exact: geometry, Poisson assembly, pressure-corrector assembly (CSR
+values, b, phiHbyA, grad p), Rhie-Chow face flux, one FP64 V-cycle.
+Tolerance-bound (relative L2 <= 1e-10): pressure after the full GMRES+AMG
+solve, and the corrected face fluxes; the iteration count must match.
+"""
+import numpy as np
+import pytest
+
+import cfdx_dev_b200 as cg
+from tests import cases
+
+pytestmark = pytest.mark.gpu
+
+REL_TOL = 1e-10   # pressure / face-flux parity with the FP64 reference
+
+
+def rel_l2(a, b):
+    return np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300)
+
+
+@pytest.fixture(scope="module")
+def tet_setup(ctx, ref):
+    m = cases.simple_mesh(10)
+    mesh = cg.Mesh(ctx, m)
+    g = mesh.geometry()
+    U, rAU, aP, p, fixed, value = cases.simple_fields(m, g["cell_centres"])
+    return m, mesh, g, (U, rAU, aP, p, fixed, value)
+
+
+@pytest.mark.parametrize("kind", ["hex", "tet"])
+def test_geometry_bit_exact(ctx, ref, kind):
+    m = cases.poisson_case(6)[0] if kind == "hex" else cases.simple_mesh(6)
+    mine = cg.Mesh(ctx, m).geometry()
+    for which in ("fv", "cache"):
+        theirs = ref.geometry(m, which)
+        for k in mine:
+            assert np.array_equal(mine[k], theirs[k]), (which, k)
+
+
+def test_poisson_assembly_bit_exact(ctx, ref):
+    m, bc, src = cases.poisson_case(8)
+    mesh = cg.Mesh(ctx, m)
+    A, rhs = cg.assemble_cell_diffusion_matrix(mesh, bc, 1.0, src)
+    ro, co, va, rhs_ref, _ = ref.assemble_diffusion(m, bc, 1.0, src)
+    r2, c2, v2 = A.to_csr()
+    assert np.array_equal(r2, ro) and np.array_equal(c2, co)
+    assert np.array_equal(v2, va)
+    assert np.array_equal(rhs, rhs_ref)
+
+
+def test_pressure_assembly_bit_exact(ctx, ref, tet_setup):
+    m, mesh, g, (U, rAU, aP, p, fixed, value) = tet_setup
+    A, b, phi, grad = cg.assemble_pressure_correction(mesh, U, rAU, p, 1.0, fixed, value)
+    r = ref.simple_assemble(m, U, rAU, p, 1.0, fixed, value)
+    ro, co, va = A.to_csr()
+    assert np.array_equal(ro, r["row_offsets"]) and np.array_equal(co, r["columns"])
+    assert np.array_equal(va, r["values"])
+    assert np.array_equal(b, r["b"])
+    assert np.array_equal(phi, r["phiHbyA"])
+    assert np.array_equal(grad, r["grad_p"])
+
+
+def test_pressure_assembly_nonzero_pressure_bit_exact(ctx, ref, tet_setup):
+    # a later corrector: p != 0, so the gradient and deferred fluxes are active
+    m, mesh, g, (U, rAU, aP, p, fixed, value) = tet_setup
+    cc = g["cell_centres"].reshape(3, -1)
+    p1 = np.sin(3 * cc[0]) + cc[1] * cc[2]
+    value1 = value.copy()
+    value1[0] = 0.25
+    A, b, phi, grad = cg.assemble_pressure_correction(mesh, U, rAU, p1, 1.3, fixed, value1)
+    r = ref.simple_assemble(m, U, rAU, p1, 1.3, fixed, value1)
+    assert np.array_equal(A.to_csr()[2], r["values"])
+    assert np.array_equal(b, r["b"])
+    assert np.array_equal(grad, r["grad_p"])
+    assert np.array_equal(cg.gauss_gradient_with_boundary(mesh, p1, fixed, value1),
+                          ref.gauss_gradient(m, p1, fixed, value1))
+    assert np.array_equal(cg.make_rhie_chow_mass_flux(mesh, U, rAU, p1, 1.3, fixed, value1),
+                          ref.rhie_chow_flux(m, U, rAU, p1, 1.3, fixed, value1))
+
+
+def test_spmv_bit_exact(ctx, ref, tet_setup):
+    m, mesh, g, (U, rAU, aP, p, fixed, value) = tet_setup
+    A, b, phi, grad = cg.assemble_pressure_correction(mesh, U, rAU, p, 1.0, fixed, value)
+    ro, co, va = A.to_csr()
+    x = np.random.default_rng(3).standard_normal(A.n)
+    assert np.array_equal(A.matvec(x), ref.spmv(ro, co, va, x))
+
+
+def test_vcycle_bit_exact(ctx, ref, tet_setup):
+    m, mesh, g, (U, rAU, aP, p, fixed, value) = tet_setup
+    A, b, phi, grad = cg.assemble_pressure_correction(mesh, U, rAU, p, 1.0, fixed, value)
+    ro, co, va = A.to_csr()
+    R = ref.Amg(ro, co, va)
+    amg = cg.NativeBoomerAMGPreconditioner(ctx)
+    assert amg.setup(A)
+    for seed in (0, 1):
+        r = np.random.default_rng(seed).standard_normal(A.n)
+        assert np.array_equal(amg.apply(r), R.apply(r))
+
+
+def test_poisson_solve_matches_reference(ctx, ref):
+    m, bc, src = cases.poisson_case(12)
+    mesh = cg.Mesh(ctx, m)
+    A, rhs = cg.assemble_cell_diffusion_matrix(mesh, bc, 1.0, src)
+    ro, co, va = A.to_csr()
+    x_ref, rep_ref = ref.solve_linear_system(ro, co, va, rhs, restart=30, tolerance=1e-8)
+    x, rep = cg.solve_linear_system(A, rhs, krylov="gmres", preconditioner="native_amg", restart=30,
+                                    tolerance=1e-8)
+    assert rep["status_name"] == "converged" and rep_ref["status"] == 0
+    assert rep["iterations"] == rep_ref["iterations"]
+    assert rel_l2(x, x_ref) <= REL_TOL
+    assert rep["physical_residual_relative"] <= 1e-8
+
+
+def test_pressure_solve_and_flux_match_reference(ctx, ref, tet_setup):
+    m, mesh, g, (U, rAU, aP, p, fixed, value) = tet_setup
+    A, b, phi, grad = cg.assemble_pressure_correction(mesh, U, rAU, p, 1.0, fixed, value)
+    ro, co, va = A.to_csr()
+    x_ref, rep_ref = ref.solve_linear_system(ro, co, va, b, restart=30, tolerance=1e-8)
+    x, rep = cg.solve_linear_system(A, b, restart=30, tolerance=1e-8)
+    assert rep["iterations"] == rep_ref["iterations"]
+    assert rel_l2(x, x_ref) <= REL_TOL
+    flux = cg.make_rhie_chow_mass_flux(mesh, U, rAU, x, 1.0, fixed, value)
+    flux_ref = ref.rhie_chow_flux(m, U, rAU, x_ref, 1.0, fixed, value)
+    assert rel_l2(flux, flux_ref) <= REL_TOL
+
+
+def test_prepared_gmres_matches_reference(ctx, ref, tet_setup):
+    m, mesh, g, (U, rAU, aP, p, fixed, value) = tet_setup
+    A, b, phi, grad = cg.assemble_pressure_correction(mesh, U, rAU, p, 1.0, fixed, value)
+    ro, co, va = A.to_csr()
+    R = ref.Amg(ro, co, va)
+    x_ref, rep_ref = R.solve_gmres(b, restart=30, tolerance=1e-8)
+    amg = cg.NativeBoomerAMGPreconditioner(ctx)
+    assert amg.setup(A)
+    x, rep = cg.solve_gmres(A, b, amg=amg, restart=30, tolerance=1e-8)
+    assert rep["status_name"] == "converged"
+    assert rep["iterations"] == rep_ref["iterations"]
+    assert rel_l2(x, x_ref) <= REL_TOL
+
+
+def test_fp32_vcycle_solve_reaches_fp64_tolerance(ctx, ref, tet_setup):
+    m, mesh, g, (U, rAU, aP, p, fixed, value) = tet_setup
+    A, b, phi, grad = cg.assemble_pressure_correction(mesh, U, rAU, p, 1.0, fixed, value)
+    x64, rep64 = cg.solve_linear_system(A, b, restart=30, tolerance=1e-8)
+    x32, rep32 = cg.solve_linear_system(A, b, krylov="fgmres", restart=30, precision="fp32_vcycle",
+                                        tolerance=1e-8)
+    assert rep32["status_name"] == "converged"
+    assert rep32["physical_residual_relative"] <= 1e-8
+    # error against the FP64 solution is stated and small
+    assert rel_l2(x32, x64) < 1e-6
+
+
+def test_solve_is_deterministic(ctx, tet_setup):
+    m, mesh, g, (U, rAU, aP, p, fixed, value) = tet_setup
+    A, b, phi, grad = cg.assemble_pressure_correction(mesh, U, rAU, p, 1.0, fixed, value)
+    x1, _ = cg.solve_linear_system(A, b, restart=30, tolerance=1e-8)
+    x2, _ = cg.solve_linear_system(A, b, restart=30, tolerance=1e-8)
+    assert np.array_equal(x1, x2)
+
+
+def test_zero_rhs_and_invalid_requests(ctx, tet_setup):
+    m, mesh, g, (U, rAU, aP, p, fixed, value) = tet_setup
+    A, b, phi, grad = cg.assemble_pressure_correction(mesh, U, rAU, p, 1.0, fixed, value)
+    x, rep = cg.solve_linear_system(A, np.zeros(A.n), restart=30, tolerance=1e-8)
+    assert rep["status_name"] == "converged" and np.all(x == 0)
+    with pytest.raises(cg.CfdxgError):
+        cg.solve_linear_system(A, b, restart=0)
+    amg = cg.NativeBoomerAMGPreconditioner(ctx)
+    with pytest.raises(cg.CfdxgError):
+        amg.apply(b)   # not set up

@@ -1,0 +1,111 @@
+"""Host logic without a GPU: synthetic meshes and the bit-exact AMG setup.
+
+The reference-built oracle (oracle/_ref) is the checker: mesh connectivity
+must equal the reference's own tet fixture, and every level of the AMG
+hierarchy (CSR, inverse diagonal, prolongation, aggregates, damping) must be
+bit-identical to MatrixFreeVcyclePreconditioner::setup with the Balanced
+NativeAMG parameters (core/linalg/hypre_amg.cpp:172-219)."""
+import numpy as np
+import pytest
+
+import cfdx_dev_b200 as cg
+from tests import cases
+
+
+@pytest.mark.parametrize("n", [3, 4, 7])
+def test_tet_generator_matches_reference_fixture(ref, n):
+    mine = cg.tet_case(n)
+    fix = ref.fixture_tet_v52(n)
+    for k in ("face_offsets", "face_vertices", "owner", "neighbour", "cell_offsets", "cell_faces"):
+        assert np.array_equal(getattr(mine, k), fix[k]), k
+
+
+def test_hex_generator_counts():
+    m = cg.hex_case(4, 5, 6)
+    nc = 4 * 5 * 6
+    nf_int = 3 * 4 * 5 * 6 - (5 * 6 + 4 * 6 + 4 * 5)
+    nf_bnd = 2 * (5 * 6 + 4 * 6 + 4 * 5)
+    assert m.n_cells == nc and m.n_faces == nf_int + nf_bnd
+    assert (m.neighbour >= 0).sum() == nf_int
+    assert set(np.unique(m.patch_of_face[m.neighbour < 0])) == {0, 1, 2, 3, 4, 5}
+    assert np.all(m.patch_of_face[m.neighbour >= 0] == -1)
+    # every cell lists 6 faces and each face belongs to its owner (and neighbour)
+    assert np.all(np.diff(m.cell_offsets) == 6)
+
+
+def test_jittered_tets_keep_positive_face_orientation(ref):
+    m = cases.simple_mesh(10)
+    g = ref.geometry(m)
+    nf, nc = m.n_faces, m.n_cells
+    sf = g["face_Sf"].reshape(3, nf)
+    cc = g["cell_centres"].reshape(3, nc)
+    internal = m.neighbour >= 0
+    d = cc[:, m.neighbour[internal]] - cc[:, m.owner[internal]]
+    assert np.all((sf[:, internal] * d).sum(0) > 0)
+    assert np.all(g["cell_volumes"] > 0)
+
+
+def _compare_hierarchy(ref, ro, co, va):
+    R = ref.Amg(ro, co, va)
+    amg = cg.NativeBoomerAMGPreconditioner(None)
+    assert amg.setup_host(ro, co, va), amg.last_error()
+    assert R.num_levels() == len(amg.hierarchy_level_sizes())
+    for l in range(R.num_levels()):
+        a, b = R.level(l), amg.export_level(l)
+        for k in ("row_offsets", "columns", "values", "inv_diag", "p_columns", "p_values"):
+            assert np.array_equal(a[k], b[k]), (l, k)
+        if a["p_offsets"] is not None:
+            assert np.array_equal(a["p_offsets"], b["p_offsets"])
+            assert np.array_equal(a["aggregate"], b["aggregate"])
+    assert R.omega == amg.omega
+    return amg
+
+
+@pytest.mark.parametrize("n", [8, 16])
+def test_amg_setup_bit_exact_poisson_hex(ref, n):
+    m, bc, src = cases.poisson_case(n)
+    ro, co, va, rhs, _ = ref.assemble_diffusion(m, bc, 1.0, src)
+    amg = _compare_hierarchy(ref, ro, co, va)
+    assert amg.hierarchy_level_sizes()[0] == n ** 3
+
+
+@pytest.mark.parametrize("n", [4, 8, 12])
+def test_amg_setup_bit_exact_pressure_tets(ref, n):
+    m = cases.simple_mesh(n)
+    g = ref.geometry(m)
+    U, rAU, aP, p, fixed, value = cases.simple_fields(m, g["cell_centres"])
+    r = ref.simple_assemble(m, U, rAU, p, 1.0, fixed, value)
+    _compare_hierarchy(ref, r["row_offsets"], r["columns"], r["values"])
+
+
+def test_amg_setup_bit_exact_anisotropic_boundary_layer(ref):
+    m = cg.boundary_layer_case(12, 10, 6, dy0=1e-3, growth=1.2, jitter=0.05, seed=5)
+    bc = np.full(m.n_faces, np.nan)
+    bc[m.patch_of_face == 0] = 0.0
+    src = cg.random_field(m.n_cells, "uniform", -1.0, 1.0, 3)
+    ro, co, va, rhs, _ = ref.assemble_diffusion(m, bc, 1.0, src)
+    _compare_hierarchy(ref, ro, co, va)
+
+
+def test_amg_setup_rejects_zero_diagonal():
+    ro = np.array([0, 2, 4])
+    co = np.array([0, 1, 0, 1])
+    va = np.array([0.0, -1.0, -1.0, 2.0])
+    amg = cg.NativeBoomerAMGPreconditioner(None)
+    assert not amg.setup_host(ro, co, va)
+    assert "diagonal" in amg.last_error()
+
+
+def test_amg_setup_is_deterministic_across_thread_counts(ref, monkeypatch):
+    # host threads only change the schedule, never the arithmetic
+    m = cases.simple_mesh(8)
+    g = ref.geometry(m)
+    U, rAU, aP, p, fixed, value = cases.simple_fields(m, g["cell_centres"])
+    r = ref.simple_assemble(m, U, rAU, p, 1.0, fixed, value)
+    a = cg.NativeBoomerAMGPreconditioner(None)
+    a.setup_host(r["row_offsets"], r["columns"], r["values"])
+    b = cg.NativeBoomerAMGPreconditioner(None)
+    b.setup_host(r["row_offsets"], r["columns"], r["values"])
+    for l in range(len(a.hierarchy_level_sizes())):
+        la, lb = a.export_level(l), b.export_level(l)
+        assert np.array_equal(la["values"], lb["values"])
