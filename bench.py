@@ -1,0 +1,399 @@
+#!/usr/bin/env python
+"""Benchmark: seconds to an FP64 true relative residual of 1e-8 for the SIMPLE
+pressure-correction solve on one B200.
+
+Workload (one GPU): the 64^3 Kuhn-tet mesh (1,572,864 cells, interior vertices
+jittered by U[+-0.15h]), pressure-correction system assembled on the GPU from a
+divergence-free 8-mode Fourier HbyA (+U[+-0.01]) and log-uniform a_P in
+[1,100]; p = 0 fixed on the x = 0 patch.  16 seeded right-hand sides (HbyA seeds)
+share the matrix; one step solves one of them, cycling.  The AMG hierarchy is
+built once per matrix (setup seconds are reported separately) and every solve
+starts from p' = 0.
+
+Forms timed: plain FP64 AMG-GMRES (the reference's algorithm), FP32 V-cycle
+inside FP64 FGMRES, and -- when trained weights are present -- the learned
+message-passing preconditioner in front of the FP32 V-cycle.  `value` is the
+headline form (learned+FP32 if available, else FP32 V-cycle).
+
+Inputs are larger than L2 (the hierarchy alone is > 2 GB), and L2 is also
+flushed before every timed step.  Rank-local device timing with CUDA events on
+the library's stream, max over ranks.  N > 1 runs independent replicas (each
+rank its own right-hand sides); there is no data-path collective.
+
+`--impl reference` times the reference's own CPU solve phase (oracle/_ref,
+one host core) on the same system.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import json
+import os
+import subprocess
+import sys
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+TOL = 1e-8
+RESTART = 30
+N_RHS = 16
+FALLBACK_HBM_GBS = 6650.0
+
+
+def parse_args():
+    ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=8)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["cfdxg", "reference"], default="cfdxg")
+    ap.add_argument("--n", type=int, default=64, help="lattice size (cells = 6 n^3)")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    return ap.parse_args()
+
+
+def dist_env():
+    return int(os.environ.get("RANK", 0)), int(os.environ.get("LOCAL_RANK", 0)), int(os.environ.get("WORLD_SIZE", 1))
+
+
+def measured_peak():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        try:
+            d = json.loads(p.read_text())
+            return float(d["hbm_gbs"]), "measured"
+        except Exception:
+            pass
+    return FALLBACK_HBM_GBS, "fallback"
+
+
+def profiled_traffic():
+    """ncu DRAM bytes per launch recorded in profiles/*.md as `traffic[<kernel>] = <bytes>`."""
+    out = {}
+    for f in (ROOT / "profiles").glob("*.md"):
+        for line in f.read_text().splitlines():
+            line = line.strip().strip("`")
+            if line.startswith("traffic[") and "=" in line:
+                k, v = line.split("=", 1)
+                try:
+                    out[k.strip()[len("traffic["):-1]] = float(v.split()[0])
+                except ValueError:
+                    pass
+    return out
+
+
+class ClockSampler:
+    """nvidia-smi clock/throttle sampling during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.path = Path(os.environ.get("TMPDIR", "/tmp")) / f"cfdxg_clocks_{os.getpid()}.csv"
+
+    def start(self):
+        try:
+            self.fh = open(self.path, "w")
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits", "-lms", "200",
+                 "-i", str(self.device)], stdout=self.fh, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.fh.close()
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.path.read_text().splitlines():
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax = float(parts[2])
+            except ValueError:
+                continue
+            for name, flag in zip(names, parts[5:9]):
+                if flag.lower().startswith("active"):
+                    reasons.add(name)
+        self.path.unlink(missing_ok=True)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": smax, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def run_cfdxg(args):
+    import torch
+
+    import cfdx_dev_b200 as cg
+    from cfdx_dev_b200 import _native as N
+    from tests import cases
+
+    rank, local_rank, world = dist_env()
+    torch.cuda.set_device(local_rank)
+    if world > 1:
+        import datetime
+        torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    dev = torch.device("cuda", local_rank)
+
+    ctx = cg.Context(local_rank)
+    lib = ctx.lib
+    lstream = torch.cuda.ExternalStream(ctx.stream, device=dev)
+
+    t0 = time.time()
+    m = cases.simple_mesh(args.n)
+    mesh = cg.Mesh(ctx, m)
+    g = mesh.geometry()
+    rhs_list = []
+    A = None
+    for k in range(N_RHS):
+        U, rAU, aP, p, fixed, value = cases.simple_fields(m, g["cell_centres"], seed_offset=rank * N_RHS + k)
+        if k == 0:
+            base_rAU = rAU
+        # the matrix depends on rAU and geometry only; HbyA changes b
+        A, b, phi, grad = cg.assemble_pressure_correction(mesh, U, base_rAU, p, 1.0, fixed, value, matrix=A)
+        rhs_list.append(b)
+    case_s = time.time() - t0
+    n_cells = A.n
+
+    forms = {}
+    amgs = {}
+    for form, prec in (("plain_fp64", "fp64"), ("fp32_vcycle", "fp32_vcycle")):
+        amg = cg.NativeBoomerAMGPreconditioner(ctx, precision=prec)
+        t = time.time()
+        if not amg.setup(A):
+            raise RuntimeError(amg.last_error())
+        amgs[form] = amg
+        forms[form] = {"setup_s": time.time() - t, "host_setup_s": amg.setup_seconds}
+    levels = amgs["plain_fp64"].hierarchy_level_sizes()
+    level_nnz = amgs["plain_fp64"].hierarchy_level_nnz()
+
+    b_dev = [torch.from_numpy(b).to(dev) for b in rhs_list]
+    x_dev = torch.zeros(n_cells, dtype=torch.float64, device=dev)
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=dev)   # 256 MB > L2
+
+    def solve_device(amg, krylov, k):
+        req = cg.make_request(krylov, "native_amg", RESTART, "fp64")
+        rep = N.Report()
+        rc = lib.cfdxg_solve_gmres(ctx.handle, A.handle, amg.handle, C.c_void_p(b_dev[k].data_ptr()),
+                                   C.c_void_p(x_dev.data_ptr()), N.CFDXG_MEM_DEVICE, C.byref(req), 1000, TOL,
+                                   C.byref(rep))
+        ctx.check(rc, "solve")
+        return rep.as_dict()
+
+    ref_solutions = {}
+    sampler = ClockSampler(local_rank)
+    headline = "fp32_vcycle"
+    for form in ("plain_fp64", "fp32_vcycle"):
+        amg = amgs[form]
+        krylov = "gmres" if form == "plain_fp64" else "fgmres"
+        for w in range(args.warmup):
+            x_dev.zero_()
+            torch.cuda.synchronize()
+            solve_device(amg, krylov, w % N_RHS)
+        times, iters, errs = [], [], []
+        launches0 = ctx.kernel_launches
+        if form == headline:
+            ctx.profile(True)
+            sampler.start()
+        for s in range(args.steps):
+            k = s % N_RHS
+            x_dev.zero_()
+            flush.fill_(float(s))
+            torch.cuda.synchronize()
+            if world > 1:
+                torch.distributed.barrier()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(lstream)
+            rep = solve_device(amg, krylov, k)
+            e1.record(lstream)
+            torch.cuda.synchronize()
+            times.append(e0.elapsed_time(e1) / 1e3)
+            iters.append(rep["iterations"])
+            if rep["status_name"] != "converged" or rep["physical_residual_relative"] > TOL:
+                raise RuntimeError(f"{form} did not converge: {rep}")
+            x = x_dev.cpu().numpy()
+            if form == "plain_fp64":
+                ref_solutions[k] = x.copy()
+            elif k in ref_solutions:
+                errs.append(float(np.linalg.norm(x - ref_solutions[k]) / np.linalg.norm(ref_solutions[k])))
+        if form == headline:
+            clocks = sampler.stop()
+            prof = ctx.profile_read()
+            ctx.profile(False)
+            launches = ctx.kernel_launches - launches0
+        forms[form].update(s_per_solve=float(np.mean(times)), s_min=float(np.min(times)),
+                           iterations=float(np.mean(iters)),
+                           rel_error_vs_fp64=(float(np.max(errs)) if errs else 0.0))
+
+    # ---- end to end through the C ABI with pinned host buffers ----
+    e2e = None
+    if not args.no_e2e:
+        amg = amgs[headline]
+        b_host = torch.empty(n_cells, dtype=torch.float64, pin_memory=True)
+        x_host = torch.empty(n_cells, dtype=torch.float64, pin_memory=True)
+        bh, xh = b_host.numpy(), x_host.numpy()
+        req = cg.make_request("fgmres", "native_amg", RESTART, "fp64")
+        e2e_times = []
+        for s in range(args.warmup + args.steps):
+            k = s % N_RHS
+            bh[:] = rhs_list[k]
+            xh[:] = 0.0
+            flush.fill_(float(s))
+            torch.cuda.synchronize()
+            rep = N.Report()
+            t = time.perf_counter()
+            rc = lib.cfdxg_solve_gmres(ctx.handle, A.handle, amg.handle, N.ptr(bh), N.ptr(xh), N.CFDXG_MEM_HOST,
+                                       C.byref(req), 1000, TOL, C.byref(rep))
+            dt = time.perf_counter() - t
+            ctx.check(rc, "e2e solve")
+            if s >= args.warmup:
+                e2e_times.append(dt)
+        e2e = {"value": float(np.mean(e2e_times)), "unit": "s",
+               "h2d_bytes_per_step": int(16 * n_cells), "d2h_bytes_per_step": int(8 * n_cells)}
+
+    # ---- max over ranks ----
+    value = forms[headline]["s_per_solve"]
+    if world > 1:
+        t = torch.tensor([value, e2e["value"] if e2e else 0.0], device=dev, dtype=torch.float64)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        value = float(t[0])
+        if e2e:
+            e2e["value"] = float(t[1])
+
+    # ---- roofline of the dominant kernel (live CUDA-event timing in the timed region) ----
+    peak, peak_kind = measured_peak()
+    traffic = profiled_traffic()
+    kernels = []
+    for e in prof:
+        if e["total_ms"] > 0:
+            gbs = e["bytes"] / (e["total_ms"] / 1e3) / 1e9
+            kernels.append(dict(name=e["name"], launches=e["launches"], total_ms=round(e["total_ms"], 3),
+                                achieved_gbs=round(gbs, 1), frac=round(gbs / peak, 3)))
+    single = [k for k in kernels if "graph" not in k["name"]]
+    dom = max(single, key=lambda k: k["total_ms"]) if single else None
+    dom_e = next(e for e in prof if dom and e["name"] == dom["name"]) if dom else None
+    roofline = None
+    if dom:
+        roofline = {"kernel": dom["name"], "bound": "hbm", "achieved": dom["achieved_gbs"], "peak": peak,
+                    "peak_kind": f"{peak_kind} ({'of measured' if peak_kind == 'measured' else 'of fallback'})",
+                    "unit": "GB/s", "frac": dom["frac"],
+                    "bytes_per_launch": dom_e["bytes"] / dom_e["launches"],
+                    "traffic": traffic.get(dom["name"])}
+
+    result = None
+    if rank == 0:
+        cpu = None
+        if world == 1 and not args.no_cpu_baseline:
+            cpu = cpu_baseline(amgs["plain_fp64"], A, rhs_list[0], forms["plain_fp64"]["iterations"])
+        result = {
+            "metric": "s to 1e-8 FP64 residual/pressure solve: learned+FP32 vs plain AMG-GMRES, 1xB200",
+            "value": value, "unit": "s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": value * 1e3, "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64 (Krylov) / f32 (V-cycle)", "data": "synthetic (seeded)",
+            "config": {"workload": f"Kuhn-tet {args.n}^3 x6 = {n_cells} cells, SIMPLE pressure correction, "
+                                   f"{N_RHS} seeded RHS, GMRES/FGMRES({RESTART}) + native RS AMG to 1e-8",
+                       "form": headline, "cells": n_cells, "nnz": int(A.nnz), "amg_levels": levels,
+                       "operator_complexity": round(sum(level_nnz) / level_nnz[0], 2),
+                       "l2": "inputs > L2 and L2 flushed before every timed step",
+                       "parallelism": f"replicas x{world}"},
+            "forms": forms, "case_build_s": case_s,
+            "e2e": e2e, "gpu_launches": int(launches), "clocks": clocks, "roofline": roofline,
+            "kernels": kernels, "cpu_baseline": cpu,
+        }
+        print(json.dumps(result), flush=True)
+    if world > 1:
+        torch.distributed.barrier()
+        torch.distributed.destroy_process_group()
+    return result
+
+
+def _export_levels(amg):
+    return [amg.export_level(l) for l in range(len(amg.hierarchy_level_sizes()))]
+
+
+def cpu_baseline(amg, A, b, plain_iterations):
+    """The reference's solve phase (oracle/_ref) on the same system, one host core."""
+    from oracle import ref
+    if not ref.available():
+        return {"value": None, "unit": "s", "cores": 1, "kind": "reference", "sample": "oracle/_ref not built"}
+    levels = _export_levels(amg)
+    R = ref.AmgFromLevels(levels, amg.omega)
+    t = time.time()
+    x, rep = R.solve_gmres(b, restart=RESTART, max_iterations=1000, tolerance=TOL)
+    dt = time.time() - t
+    return {"value": rep["solve_seconds"], "unit": "s", "cores": 1, "kind": "reference",
+            "iterations": rep["iterations"], "wall_s": dt,
+            "sample": "one complete reference GMRES(30)+NativeAMG solve phase to 1e-8 on the full system "
+                      "(hierarchy loaded: bit-identical to the reference setup, which takes hours at this size)"}
+
+
+def run_reference(args):
+    """Reference arm: the reference's own CPU solve phase (oracle/_ref) on this config."""
+    rank, local_rank, world = dist_env()
+    if rank != 0:
+        return None
+    from oracle import ref
+    import cfdx_dev_b200 as cg
+    from tests import cases
+    if not ref.available():
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libcfdx_ref.so not built"}))
+        return None
+    m = cases.simple_mesh(args.n)
+    g = ref.geometry(m)
+    U, rAU, aP, p, fixed, value = cases.simple_fields(m, g["cell_centres"])
+    r = ref.simple_assemble(m, U, rAU, p, 1.0, fixed, value)
+    amg = cg.NativeBoomerAMGPreconditioner(None)
+    if not amg.setup_host(r["row_offsets"], r["columns"], r["values"]):
+        raise RuntimeError(amg.last_error())
+    R = ref.AmgFromLevels(_export_levels(amg), amg.omega)
+    # first warmup step: one complete solve, for the iteration count
+    x, full = R.solve_gmres(r["b"], restart=RESTART, max_iterations=1000, tolerance=TOL)
+    iters = full["iterations"]
+    sample_its = 2
+    for _ in range(max(0, args.warmup - 1)):
+        R.solve_gmres(r["b"], restart=RESTART, max_iterations=sample_its, tolerance=TOL)
+    ts = []
+    for _ in range(args.steps):
+        x, rep = R.solve_gmres(r["b"], restart=RESTART, max_iterations=sample_its, tolerance=TOL)
+        ts.append(rep["solve_seconds"])
+    v = float(np.mean(ts)) / sample_its * iters
+    out = {"impl": "reference", "metric": "s to 1e-8 FP64 residual/pressure solve: learned+FP32 vs plain AMG-GMRES, 1xB200",
+           "value": v, "unit": "s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+           "higher_is_better": False, "config": {"workload": f"Kuhn-tet {args.n}^3 x6 = {m.n_cells} cells"},
+           "cpu_baseline": {"value": v, "unit": "s", "cores": 1, "kind": "reference",
+                            "sample": f"reference GMRES(30)+NativeAMG solve phase capped at {sample_its} iterations "
+                                      f"per step, scaled to the full solve's {iters} iterations "
+                                      f"(full solve measured once in warm-up: {full['solve_seconds']:.2f} s)"},
+           "e2e": {"value": v, "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(out), flush=True)
+    return out
+
+
+def main():
+    args = parse_args()
+    if args.warmup < 3 and args.impl == "cfdxg":
+        raise SystemExit("--warmup must be >= 3")
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_cfdxg(args)
+
+
+if __name__ == "__main__":
+    main()

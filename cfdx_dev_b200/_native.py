@@ -43,8 +43,12 @@ class AmgOptions(C.Structure):
         ("omega", C.c_double), ("pre_sweeps", C.c_int32), ("post_sweeps", C.c_int32),
         ("strength_threshold", C.c_double), ("max_levels", C.c_int32),
         ("require_smoother_certificate", C.c_int32), ("precision", C.c_int32),
-        ("coarse_dense_limit", C.c_int32),
+        ("coarse_dense_limit", C.c_int32), ("reference_order", C.c_int32),
     ]
+
+
+class KernelProfile(C.Structure):
+    _fields_ = [("name", C.c_char * 48), ("launches", C.c_int64), ("total_ms", C.c_double), ("bytes", C.c_double)]
 
 
 class Request(C.Structure):
@@ -81,6 +85,9 @@ PROTOTYPES = {
     "cfdxg_last_error": (C.c_char_p, [_V]),
     "cfdxg_kernel_launches": (C.c_int64, [_V]),
     "cfdxg_synchronize": (C.c_int, [_V]),
+    "cfdxg_context_stream": (C.c_void_p, [_V]),
+    "cfdxg_profile_enable": (C.c_int, [_V, C.c_int32]),
+    "cfdxg_profile_read": (C.c_int, [_V, _V, C.c_int32, c_int32_p]),
     "cfdxg_mesh_upload": (C.c_int, [_V, _P(MeshDesc), _P(_V)]),
     "cfdxg_mesh_destroy": (C.c_int, [_V]),
     "cfdxg_geometry_build": (C.c_int, [_V, _V]),

@@ -70,6 +70,23 @@ class Context:
     def synchronize(self):
         self.check(self.lib.cfdxg_synchronize(self.handle))
 
+    @property
+    def stream(self) -> int:
+        """The library's CUDA stream handle (cudaStream_t as an integer)."""
+        return int(self.lib.cfdxg_context_stream(self.handle) or 0)
+
+    def profile(self, on: bool = True):
+        """Enable (and reset) / disable live kernel timing."""
+        self.check(self.lib.cfdxg_profile_enable(self.handle, int(on)))
+
+    def profile_read(self) -> list[dict]:
+        """Per kernel class: launches, device ms and algorithmic bytes since profile(True)."""
+        buf = (N.KernelProfile * 64)()
+        cnt = C.c_int32()
+        self.check(self.lib.cfdxg_profile_read(self.handle, buf, 64, C.byref(cnt)))
+        return [dict(name=buf[k].name.decode(), launches=buf[k].launches, total_ms=buf[k].total_ms,
+                     bytes=buf[k].bytes) for k in range(min(cnt.value, 64))]
+
     def close(self):
         if getattr(self, "handle", None):
             self.lib.cfdxg_context_destroy(self.handle)

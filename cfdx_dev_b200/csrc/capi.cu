@@ -83,9 +83,9 @@ void amg_setup_impl(cfdxg_context* ctx, cfdxg_amg* amg, cfdxg_matrix* A) {
     std::unique_ptr<DevHierarchy<double>> d64;
     std::unique_ptr<DevHierarchy<float>> d32;
     if (amg->opts.precision == CFDXG_PRECISION_FP32_VCYCLE)
-        d32 = upload_hierarchy<float>(ctx, staged, amg->opts.coarse_dense_limit);
+        d32 = upload_hierarchy<float>(ctx, staged, amg->opts.coarse_dense_limit, amg->opts.reference_order != 0);
     else
-        d64 = upload_hierarchy<double>(ctx, staged, 0);
+        d64 = upload_hierarchy<double>(ctx, staged, 0, amg->opts.reference_order != 0);
     // commit only after every stage succeeded (hypre_amg.cpp:163-236 is transactional)
     amg->host = std::move(staged);
     amg->d64 = std::move(d64);
@@ -135,6 +135,9 @@ extern "C" int cfdxg_context_destroy(cfdxg_context* ctx) {
     if (!ctx) return CFDXG_OK;
     if (ctx->stream) cudaStreamSynchronize(ctx->stream);
     ctx->krylov_workspace.reset();
+    for (auto& e : ctx->staging.entries) if (e.ptr) cudaFree(e.ptr);
+    for (auto e : ctx->prof.pool) cudaEventDestroy(e);
+    for (auto& pe : ctx->prof.pending) { cudaEventDestroy(pe.a); cudaEventDestroy(pe.b); }
     if (ctx->scratch.partial) cudaFree(ctx->scratch.partial);
     if (ctx->scratch.ticket) cudaFree(ctx->scratch.ticket);
     if (ctx->scratch.scalars) cudaFree(ctx->scratch.scalars);
@@ -148,6 +151,38 @@ extern "C" int cfdxg_context_destroy(cfdxg_context* ctx) {
 
 extern "C" const char* cfdxg_last_error(const cfdxg_context* ctx) { return ctx ? ctx->error.c_str() : "null context"; }
 extern "C" int64_t cfdxg_kernel_launches(const cfdxg_context* ctx) { return ctx ? ctx->launches : 0; }
+extern "C" void* cfdxg_context_stream(const cfdxg_context* ctx) {
+    return ctx ? static_cast<void*>(ctx->stream) : nullptr;
+}
+
+extern "C" int cfdxg_profile_enable(cfdxg_context* ctx, int32_t on) {
+    if (!ctx) return CFDXG_ERR_INVALID_ARGUMENT;
+    CFDXG_GUARD_BEGIN
+    prof_flush(ctx);
+    ctx->prof.stats.clear();
+    ctx->prof.on = on != 0;
+    return CFDXG_OK;
+    CFDXG_GUARD_END(ctx)
+}
+
+extern "C" int cfdxg_profile_read(cfdxg_context* ctx, cfdxg_kernel_profile* out, int32_t max_entries,
+                                  int32_t* count) {
+    if (!ctx) return CFDXG_ERR_INVALID_ARGUMENT;
+    CFDXG_GUARD_BEGIN
+    prof_flush(ctx);
+    const int32_t n = static_cast<int32_t>(ctx->prof.stats.size());
+    if (count) *count = n;
+    for (int32_t k = 0; k < n && k < max_entries && out; ++k) {
+        std::memset(out[k].name, 0, sizeof(out[k].name));
+        std::strncpy(out[k].name, ctx->prof.stats[k].name.c_str(), sizeof(out[k].name) - 1);
+        out[k].launches = ctx->prof.stats[k].launches;
+        out[k].total_ms = ctx->prof.stats[k].ms;
+        out[k].bytes = ctx->prof.stats[k].bytes;
+    }
+    return CFDXG_OK;
+    CFDXG_GUARD_END(ctx)
+}
+
 extern "C" int cfdxg_synchronize(cfdxg_context* ctx) {
     if (!ctx) return CFDXG_ERR_INVALID_ARGUMENT;
     CFDXG_GUARD_BEGIN
@@ -256,6 +291,7 @@ extern "C" int cfdxg_amg_options_default(cfdxg_amg_options* o) {
     o->require_smoother_certificate = 0;
     o->precision = CFDXG_PRECISION_FP64;
     o->coarse_dense_limit = 2000;
+    o->reference_order = 0;
     return CFDXG_OK;
 }
 

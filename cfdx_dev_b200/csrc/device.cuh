@@ -44,6 +44,36 @@ struct Scratch {
     int* host_status = nullptr;     // pinned
 };
 
+// Reusable device staging buffers for host-memory arguments (avoids a
+// cudaMalloc / cudaFree pair per call).
+struct StagingPool {
+    struct Entry {
+        void* ptr = nullptr;
+        std::size_t bytes = 0;
+        bool in_use = false;
+    };
+    std::vector<Entry> entries;
+};
+
+struct KernelStats {
+    std::string name;
+    int64_t launches = 0;
+    double ms = 0.0;
+    double bytes = 0.0;
+};
+
+struct Profiler {
+    bool on = false;
+    struct Pending {
+        int idx;
+        cudaEvent_t a, b;
+        double bytes;
+    };
+    std::vector<Pending> pending;
+    std::vector<cudaEvent_t> pool;
+    std::vector<KernelStats> stats;
+};
+
 }  // namespace cfdxg
 
 struct cfdxg_context {
@@ -54,11 +84,25 @@ struct cfdxg_context {
     cfdxg::Scratch scratch;
     int sm_count = 148;
     std::shared_ptr<void> krylov_workspace;   // grown on demand by the Krylov driver
+    cfdxg::Profiler prof;
+    cfdxg::StagingPool staging;
 };
 
 namespace cfdxg {
 
 inline void count_launch(cfdxg_context* ctx, int64_t n = 1) { ctx->launches += n; }
+
+// Event bracket around one eager launch (no-op unless profiling is enabled).
+int prof_begin(cfdxg_context* ctx, const char* name, double bytes);
+void prof_end(cfdxg_context* ctx, int token);
+void prof_flush(cfdxg_context* ctx);
+
+struct ProfScope {
+    cfdxg_context* ctx;
+    int token;
+    ProfScope(cfdxg_context* c, const char* name, double bytes) : ctx(c), token(prof_begin(c, name, bytes)) {}
+    ~ProfScope() { prof_end(ctx, token); }
+};
 
 inline void check_launch(cfdxg_context* ctx) {
     count_launch(ctx);

@@ -6,23 +6,61 @@
 
 namespace cfdxg {
 
+// Borrow a device buffer of at least `bytes` from the context's staging pool.
+inline int stage_acquire(cfdxg_context* ctx, std::size_t bytes) {
+    auto& E = ctx->staging.entries;
+    int best = -1;
+    for (int k = 0; k < static_cast<int>(E.size()); ++k)
+        if (!E[k].in_use && E[k].bytes >= bytes && (best < 0 || E[k].bytes < E[best].bytes)) best = k;
+    if (best < 0) {
+        for (int k = 0; k < static_cast<int>(E.size()); ++k)
+            if (!E[k].in_use) {   // grow an idle entry
+                CFDXG_CUDA(cudaFreeAsync(E[k].ptr, ctx->stream));
+                E[k].ptr = nullptr;
+                CFDXG_CUDA(cudaMallocAsync(&E[k].ptr, bytes, ctx->stream));
+                E[k].bytes = bytes;
+                best = k;
+                break;
+            }
+    }
+    if (best < 0) {
+        StagingPool::Entry e;
+        CFDXG_CUDA(cudaMallocAsync(&e.ptr, bytes, ctx->stream));
+        e.bytes = bytes;
+        E.push_back(e);
+        best = static_cast<int>(E.size()) - 1;
+    }
+    E[best].in_use = true;
+    return best;
+}
+
+inline void stage_release(cfdxg_context* ctx, int slot) {
+    if (slot >= 0) ctx->staging.entries[slot].in_use = false;
+}
+
 // A read-only array argument that may live on the host or the device.
 template <class T>
 class In {
 public:
-    In(cfdxg_context* ctx, const T* p, int64_t n, int32_t mem) {
+    In(cfdxg_context* ctx, const T* p, int64_t n, int32_t mem) : ctx_(ctx) {
         if (!p || n == 0) return;
         if (mem == CFDXG_MEM_DEVICE) {
             ptr_ = p;
         } else {
-            buf_.upload(p, static_cast<std::size_t>(n), ctx->stream);
-            ptr_ = buf_.get();
+            slot_ = stage_acquire(ctx, sizeof(T) * static_cast<std::size_t>(n));
+            T* d = static_cast<T*>(ctx->staging.entries[slot_].ptr);
+            CFDXG_CUDA(cudaMemcpyAsync(d, p, sizeof(T) * n, cudaMemcpyHostToDevice, ctx->stream));
+            ptr_ = d;
         }
     }
+    ~In() { stage_release(ctx_, slot_); }
+    In(const In&) = delete;
+    In& operator=(const In&) = delete;
     const T* get() const { return ptr_; }
 
 private:
-    DevBuf<T> buf_;
+    cfdxg_context* ctx_;
+    int slot_ = -1;
     const T* ptr_ = nullptr;
 };
 
@@ -36,16 +74,18 @@ public:
         if (mem == CFDXG_MEM_DEVICE) {
             ptr_ = p;
         } else {
-            if (preload) buf_.upload(p, static_cast<std::size_t>(n), ctx->stream);
-            else buf_.resize(static_cast<std::size_t>(n));
-            ptr_ = buf_.get();
+            slot_ = stage_acquire(ctx, sizeof(T) * static_cast<std::size_t>(n));
+            ptr_ = static_cast<T*>(ctx->staging.entries[slot_].ptr);
+            if (preload) CFDXG_CUDA(cudaMemcpyAsync(ptr_, p, sizeof(T) * n, cudaMemcpyHostToDevice, ctx->stream));
         }
     }
+    ~Out() { stage_release(ctx_, slot_); }
+    Out(const Out&) = delete;
+    Out& operator=(const Out&) = delete;
     T* get() const { return ptr_; }
     void finish() {
-        if (host_ && mem_ != CFDXG_MEM_DEVICE && n_) {
-            buf_.download(host_, ctx_->stream);
-        }
+        if (host_ && mem_ != CFDXG_MEM_DEVICE && n_)
+            CFDXG_CUDA(cudaMemcpyAsync(host_, ptr_, sizeof(T) * n_, cudaMemcpyDeviceToHost, ctx_->stream));
     }
 
 private:
@@ -53,7 +93,7 @@ private:
     T* host_;
     int64_t n_;
     int32_t mem_;
-    DevBuf<T> buf_;
+    int slot_ = -1;
     T* ptr_ = nullptr;
 };
 

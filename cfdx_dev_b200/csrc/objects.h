@@ -28,6 +28,8 @@ struct DevLevel {
     DevBuf<T> p_val, r_val;
     DevBuf<T> r, x, x2, res;
     T* xout = nullptr;   // where the level's result lives after enqueue
+    int tpr = 1;         // threads cooperating on one row of A (1 = reference order)
+    int tpr_r = 1;       // threads cooperating on one row of P^T
 };
 
 template <class T>
@@ -41,6 +43,7 @@ struct DevHierarchy {
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
     int64_t graph_kernels = 0;
+    double graph_bytes = 0.0;   // algorithmic bytes of one replay
     int* status = nullptr;
     ~DevHierarchy() {
         if (exec) cudaGraphExecDestroy(exec);
@@ -97,7 +100,7 @@ void spmv_fp64(cfdxg_context* ctx, const cfdxg_matrix* A, const double* x, doubl
 // hierarchy (vcycle.cu)
 template <class T>
 std::unique_ptr<DevHierarchy<T>> upload_hierarchy(cfdxg_context* ctx, const AmgHierarchy& h,
-                                                  int coarse_dense_limit);
+                                                  int coarse_dense_limit, bool reference_order);
 template <class T>
 void refresh_hierarchy_values(cfdxg_context* ctx, DevHierarchy<T>& d, const AmgHierarchy& h);
 // z = V-cycle(r); r, z are FP64 device vectors.

@@ -43,44 +43,59 @@ __global__ void k_sweep_zero(int n, T omega, const T* __restrict__ inv_diag, con
     if (!finite_(xi)) atomicOr(status, kStatusNonFinite);
 }
 
-// x_out = x + omega * (inv_diag * (r - A x)), row sum in CSR order.
-template <class T, class XO>
+// Row reductions.  TPR threads cooperate on one row; TPR == 1 sums the row
+// sequentially in CSR order (the reference's order).  TPR > 1 gives each
+// thread the entries k = lane, lane + TPR, ... and combines the partial sums
+// with a fixed xor butterfly, so results are deterministic run to run.
+template <class T, int TPR>
+__device__ __forceinline__ T row_dot(int b, int e, int lane, const int* __restrict__ co,
+                                     const T* __restrict__ va, const T* __restrict__ x) {
+    T s = T(0);
+    for (int k = b + lane; k < e; k += TPR) s += va[k] * __ldg(x + co[k]);
+    if (TPR > 1) {
+#pragma unroll
+        for (int o = TPR / 2; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o, TPR);
+    }
+    return s;
+}
+
+// x_out = x + omega * (inv_diag * (r - A x))
+template <class T, class XO, int TPR>
 __global__ void k_sweep(int n, const int* __restrict__ ro, const int* __restrict__ co,
                         const T* __restrict__ va, const T* __restrict__ inv_diag,
                         const T* __restrict__ r, const T* __restrict__ x, XO* __restrict__ xo,
                         T omega, int* status) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    T s = T(0);
-    const int e = ro[i + 1];
-    for (int k = ro[i]; k < e; ++k) s += va[k] * __ldg(x + co[k]);
+    const int g = blockIdx.x * blockDim.x + threadIdx.x;
+    const int i = g / TPR, lane = g % TPR;
+    const bool valid = i < n;
+    const T s = row_dot<T, TPR>(valid ? ro[i] : 0, valid ? ro[i + 1] : 0, lane, co, va, x);
+    if (!valid || lane != 0) return;
     const T delta = inv_diag[i] * (r[i] - s);
     const T xi = x[i] + omega * delta;
     xo[i] = static_cast<XO>(xi);
     if (!finite_(xi)) atomicOr(status, kStatusNonFinite);
 }
 
-template <class T>
+template <class T, int TPR>
 __global__ void k_residual(int n, const int* __restrict__ ro, const int* __restrict__ co,
                            const T* __restrict__ va, const T* __restrict__ r,
                            const T* __restrict__ x, T* __restrict__ res) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    T s = T(0);
-    const int e = ro[i + 1];
-    for (int k = ro[i]; k < e; ++k) s += va[k] * __ldg(x + co[k]);
-    res[i] = r[i] - s;
+    const int g = blockIdx.x * blockDim.x + threadIdx.x;
+    const int i = g / TPR, lane = g % TPR;
+    const bool valid = i < n;
+    const T s = row_dot<T, TPR>(valid ? ro[i] : 0, valid ? ro[i + 1] : 0, lane, co, va, x);
+    if (valid && lane == 0) res[i] = r[i] - s;
 }
 
-template <class T>
+// coarse_r = P^T res, rows of P^T in increasing fine-row order
+template <class T, int TPR>
 __global__ void k_restrict(int nc, const int* __restrict__ r_off, const int* __restrict__ r_row,
                            const T* __restrict__ r_val, const T* __restrict__ res, T* __restrict__ rc) {
-    const int c = blockIdx.x * blockDim.x + threadIdx.x;
-    if (c >= nc) return;
-    T s = T(0);
-    const int e = r_off[c + 1];
-    for (int t = r_off[c]; t < e; ++t) s += r_val[t] * __ldg(res + r_row[t]);
-    rc[c] = s;
+    const int g = blockIdx.x * blockDim.x + threadIdx.x;
+    const int c = g / TPR, lane = g % TPR;
+    const bool valid = c < nc;
+    const T s = row_dot<T, TPR>(valid ? r_off[c] : 0, valid ? r_off[c + 1] : 0, lane, r_row, r_val, res);
+    if (valid && lane == 0) rc[c] = s;
 }
 
 template <class T>
@@ -242,6 +257,80 @@ __global__ void k_gj_init(int n, const int* ro, const int* co, const double* va,
     row[n + i] = 1.0;
 }
 
+#define CFDXG_TPR_SWITCH(tpr, ...)                            \
+    switch (tpr) {                                               \
+        case 1: { constexpr int TPR = 1; __VA_ARGS__; } break;   \
+        case 2: { constexpr int TPR = 2; __VA_ARGS__; } break;   \
+        case 4: { constexpr int TPR = 4; __VA_ARGS__; } break;   \
+        case 8: { constexpr int TPR = 8; __VA_ARGS__; } break;   \
+        case 16: { constexpr int TPR = 16; __VA_ARGS__; } break; \
+        default: { constexpr int TPR = 32; __VA_ARGS__; } break; \
+    }
+
+// Algorithmic (compulsory) bytes of one launch; accumulated into the graph
+// total while a capture is in progress.
+thread_local double* t_capture_bytes = nullptr;
+
+inline double account(double bytes) {
+    if (t_capture_bytes) *t_capture_bytes += bytes;
+    return bytes;
+}
+
+template <class T>
+const char* tname(const char* fp64, const char* fp32) { return sizeof(T) == 8 ? fp64 : fp32; }
+
+template <class T, class XO>
+void launch_sweep(cfdxg_context* ctx, const DevLevel<T>& L, const T* r, const T* x, XO* xo, T omega, int* status) {
+    // A values + columns, row offsets, x / r / inv_diag reads, x_out write
+    const double bytes = account((sizeof(T) + 4.0) * L.nnz + 4.0 * (L.n + 1) + 3.0 * sizeof(T) * L.n + sizeof(XO) * L.n);
+    ProfScope ps(ctx, tname<T>("jacobi_sweep_fp64_L0", "jacobi_sweep_fp32_L0"), bytes);
+    const int64_t threads = static_cast<int64_t>(L.n) * L.tpr;
+    CFDXG_TPR_SWITCH(L.tpr, (k_sweep<T, XO, TPR><<<blocks_for(threads, kT), kT, 0, ctx->stream>>>(
+        L.n, L.ro.get(), L.co.get(), L.va.get(), L.inv_diag.get(), r, x, xo, omega, status)));
+    check_launch(ctx);
+}
+
+template <class T>
+void launch_residual(cfdxg_context* ctx, const DevLevel<T>& L, const T* r, const T* x, T* res) {
+    const double bytes = account((sizeof(T) + 4.0) * L.nnz + 4.0 * (L.n + 1) + 3.0 * sizeof(T) * L.n);
+    ProfScope ps(ctx, tname<T>("residual_fp64_L0", "residual_fp32_L0"), bytes);
+    const int64_t threads = static_cast<int64_t>(L.n) * L.tpr;
+    CFDXG_TPR_SWITCH(L.tpr, (k_residual<T, TPR><<<blocks_for(threads, kT), kT, 0, ctx->stream>>>(
+        L.n, L.ro.get(), L.co.get(), L.va.get(), r, x, res)));
+    check_launch(ctx);
+}
+
+template <class T>
+void launch_restrict(cfdxg_context* ctx, const DevLevel<T>& L, const T* res, T* rc) {
+    const double pnnz = static_cast<double>(L.r_row.size());
+    const double bytes = account((sizeof(T) + 4.0) * pnnz + 4.0 * (L.nc + 1) + sizeof(T) * (L.n + L.nc));
+    ProfScope ps(ctx, tname<T>("restrict_fp64_L0", "restrict_fp32_L0"), bytes);
+    const int64_t threads = static_cast<int64_t>(L.nc) * L.tpr_r;
+    CFDXG_TPR_SWITCH(L.tpr_r, (k_restrict<T, TPR><<<blocks_for(threads, kT), kT, 0, ctx->stream>>>(
+        L.nc, L.r_off.get(), L.r_row.get(), L.r_val.get(), res, rc)));
+    check_launch(ctx);
+}
+
+template <class T>
+void launch_prolong(cfdxg_context* ctx, const DevLevel<T>& L, const T* xc, T* x, int* status) {
+    const double pnnz = static_cast<double>(L.p_col.size());
+    const double bytes = account((sizeof(T) + 4.0) * pnnz + 4.0 * (L.n + 1) + sizeof(T) * (L.nc + 2.0 * L.n));
+    ProfScope ps(ctx, tname<T>("prolong_fp64_L0", "prolong_fp32_L0"), bytes);
+    k_prolong<T><<<blocks_for(L.n, kT), kT, 0, ctx->stream>>>(L.n, L.p_off.get(), L.p_col.get(), L.p_val.get(),
+                                                               xc, x, status);
+    check_launch(ctx);
+}
+
+int choose_tpr(int64_t nnz, int64_t rows, bool reference_order) {
+    if (reference_order || rows == 0) return 1;
+    const double avg = static_cast<double>(nnz) / static_cast<double>(rows);
+    if (avg < 12) return 1;
+    if (avg < 24) return 4;
+    if (avg < 48) return 8;
+    if (avg < 96) return 16;
+    return 32;
+}
+
 template <class T>
 void upload_level_values(cfdxg_context* ctx, DevLevel<T>& D, const AmgLevel& H) {
     std::vector<T> tmp(H.A.va.size());
@@ -254,10 +343,12 @@ void upload_level_values(cfdxg_context* ctx, DevLevel<T>& D, const AmgLevel& H) 
 }
 
 template <class T>
-void upload_level(cfdxg_context* ctx, DevLevel<T>& D, const AmgLevel& H, bool with_transfer) {
+void upload_level(cfdxg_context* ctx, DevLevel<T>& D, const AmgLevel& H, bool with_transfer,
+                  bool reference_order) {
     cudaStream_t s = ctx->stream;
     D.n = static_cast<int>(H.A.n);
     D.nnz = static_cast<int>(H.A.co.size());
+    D.tpr = choose_tpr(D.nnz, D.n, reference_order);
     std::vector<int> ro(H.A.ro.begin(), H.A.ro.end()), co(H.A.co.begin(), H.A.co.end());
     D.ro.upload(ro, s);
     D.co.upload(co, s);
@@ -269,6 +360,7 @@ void upload_level(cfdxg_context* ctx, DevLevel<T>& D, const AmgLevel& H, bool wi
         for (const uint32_t c : H.p_col) nc = std::max<int>(nc, static_cast<int>(c) + 1);
         nc = std::max<int>(nc, static_cast<int>(H.plan.n_coarse));
         D.nc = nc;
+        D.tpr_r = choose_tpr(static_cast<int64_t>(H.p_col.size()), nc, reference_order);
         std::vector<int> po(H.p_off.begin(), H.p_off.end()), pc(H.p_col.begin(), H.p_col.end());
         std::vector<T> pv(H.p_val.size());
         for (std::size_t q = 0; q < pv.size(); ++q) pv[q] = static_cast<T>(H.p_val[q]);
@@ -325,12 +417,11 @@ void sweeps_from_zero(cfdxg_context* ctx, DevHierarchy<T>& d, DevLevel<T>& L, co
     if (sweeps == 0) {
         CFDXG_CUDA(cudaMemsetAsync(x, 0, sizeof(T) * L.n, s));
     } else {
+        account(3.0 * sizeof(T) * L.n);
         k_sweep_zero<T, T><<<gb, kT, 0, s>>>(L.n, d.omega, L.inv_diag.get(), r_in, nullptr, x, d.status);
         check_launch(ctx);
         for (int k = 1; k < sweeps; ++k) {
-            k_sweep<T, T><<<gb, kT, 0, s>>>(L.n, L.ro.get(), L.co.get(), L.va.get(), L.inv_diag.get(),
-                                            r_in, x, x2, d.omega, d.status);
-            check_launch(ctx);
+            launch_sweep<T, T>(ctx, L, r_in, x, x2, d.omega, d.status);
             std::swap(x, x2);
         }
     }
@@ -350,6 +441,7 @@ void enqueue_from(cfdxg_context* ctx, DevHierarchy<T>& d, int l) {
             check_launch(ctx);
             L.xout = L.x.get();
         } else if (d.coarse_mode == 2) {
+            account(8.0 * L.n * L.n + 2.0 * sizeof(T) * L.n);
             k_dense_inverse_apply<T><<<blocks_for(static_cast<int64_t>(L.n) * 32, kT), kT, 0, s>>>(
                 L.n, d.dense.get(), L.r.get(), L.x.get(), d.status);
             check_launch(ctx);
@@ -362,19 +454,13 @@ void enqueue_from(cfdxg_context* ctx, DevHierarchy<T>& d, int l) {
     sweeps_from_zero(ctx, d, L, L.r.get(), d.pre);
     T* x = L.xout;
     T* x2 = (x == L.x.get()) ? L.x2.get() : L.x.get();
-    k_residual<T><<<gb, kT, 0, s>>>(L.n, L.ro.get(), L.co.get(), L.va.get(), L.r.get(), x, L.res.get());
-    check_launch(ctx);
+    launch_residual<T>(ctx, L, L.r.get(), x, L.res.get());
     DevLevel<T>& C = d.L[l + 1];
-    k_restrict<T><<<blocks_for(C.n, kT), kT, 0, s>>>(C.n, L.r_off.get(), L.r_row.get(), L.r_val.get(),
-                                                      L.res.get(), C.r.get());
-    check_launch(ctx);
+    launch_restrict<T>(ctx, L, L.res.get(), C.r.get());
     enqueue_from(ctx, d, l + 1);
-    k_prolong<T><<<gb, kT, 0, s>>>(L.n, L.p_off.get(), L.p_col.get(), L.p_val.get(), C.xout, x, d.status);
-    check_launch(ctx);
+    launch_prolong<T>(ctx, L, C.xout, x, d.status);
     for (int k = 0; k < d.post; ++k) {
-        k_sweep<T, T><<<gb, kT, 0, s>>>(L.n, L.ro.get(), L.co.get(), L.va.get(), L.inv_diag.get(),
-                                        L.r.get(), x, x2, d.omega, d.status);
-        check_launch(ctx);
+        launch_sweep<T, T>(ctx, L, L.r.get(), x, x2, d.omega, d.status);
         std::swap(x, x2);
     }
     L.xout = x;
@@ -384,10 +470,14 @@ template <class T>
 void ensure_graph(cfdxg_context* ctx, DevHierarchy<T>& d) {
     if (d.exec || d.used < 2) return;
     const int64_t before = ctx->launches;
+    d.graph_bytes = 0.0;
     CFDXG_CUDA(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
     try {
+        t_capture_bytes = &d.graph_bytes;
         enqueue_from(ctx, d, 1);
+        t_capture_bytes = nullptr;
     } catch (...) {
+        t_capture_bytes = nullptr;
         cudaGraph_t g = nullptr;
         cudaStreamEndCapture(ctx->stream, &g);
         if (g) cudaGraphDestroy(g);
@@ -403,7 +493,7 @@ void ensure_graph(cfdxg_context* ctx, DevHierarchy<T>& d) {
 
 template <class T>
 std::unique_ptr<DevHierarchy<T>> upload_hierarchy(cfdxg_context* ctx, const AmgHierarchy& h,
-                                                  int coarse_dense_limit) {
+                                                  int coarse_dense_limit, bool reference_order) {
     auto d = std::make_unique<DevHierarchy<T>>();
     d->omega = static_cast<T>(h.omega);
     d->pre = h.options.pre;
@@ -418,7 +508,7 @@ std::unique_ptr<DevHierarchy<T>> upload_hierarchy(cfdxg_context* ctx, const AmgH
     if (d->coarse_mode == 0 && h.levels[used - 1].A.n <= kDenseDirectLimit) d->coarse_mode = 1;
     d->used = used;
     d->L.resize(used);
-    for (int l = 0; l < used; ++l) upload_level(ctx, d->L[l], h.levels[l], l + 1 < used);
+    for (int l = 0; l < used; ++l) upload_level(ctx, d->L[l], h.levels[l], l + 1 < used, reference_order);
     if (d->coarse_mode == 2) build_dense_inverse(ctx, *d, h.levels[used - 1]);
     return d;
 }
@@ -469,22 +559,19 @@ void vcycle_apply(cfdxg_context* ctx, DevHierarchy<T>& d, const double* r, doubl
                                                   d.status);
         check_launch(ctx);
         for (int k = 1; k < d.pre; ++k) {
-            k_sweep<T, T><<<gb, kT, 0, s>>>(L.n, L.ro.get(), L.co.get(), L.va.get(), L.inv_diag.get(), rl,
-                                            x, x2, d.omega, d.status);
-            check_launch(ctx);
+            launch_sweep<T, T>(ctx, L, rl, x, x2, d.omega, d.status);
             std::swap(x, x2);
         }
     }
-    k_residual<T><<<gb, kT, 0, s>>>(L.n, L.ro.get(), L.co.get(), L.va.get(), rl, x, L.res.get());
-    check_launch(ctx);
+    launch_residual<T>(ctx, L, rl, x, L.res.get());
     DevLevel<T>& C = d.L[1];
-    k_restrict<T><<<blocks_for(C.n, kT), kT, 0, s>>>(C.n, L.r_off.get(), L.r_row.get(), L.r_val.get(),
-                                                      L.res.get(), C.r.get());
-    check_launch(ctx);
-    CFDXG_CUDA(cudaGraphLaunch(d.exec, s));
+    launch_restrict<T>(ctx, L, L.res.get(), C.r.get());
+    {
+        ProfScope ps(ctx, tname<T>("vcycle_levels_1plus_fp64_graph", "vcycle_levels_1plus_fp32_graph"), d.graph_bytes);
+        CFDXG_CUDA(cudaGraphLaunch(d.exec, s));
+    }
     count_launch(ctx, d.graph_kernels);
-    k_prolong<T><<<gb, kT, 0, s>>>(L.n, L.p_off.get(), L.p_col.get(), L.p_val.get(), C.xout, x, d.status);
-    check_launch(ctx);
+    launch_prolong<T>(ctx, L, C.xout, x, d.status);
     if (d.post == 0) {
         k_copy_cast<T, double><<<gb, kT, 0, s>>>(L.n, x, z);
         check_launch(ctx);
@@ -492,22 +579,19 @@ void vcycle_apply(cfdxg_context* ctx, DevHierarchy<T>& d, const double* r, doubl
     }
     for (int k = 0; k < d.post; ++k) {
         if (k + 1 == d.post) {
-            k_sweep<T, double><<<gb, kT, 0, s>>>(L.n, L.ro.get(), L.co.get(), L.va.get(), L.inv_diag.get(),
-                                                 rl, x, z, d.omega, d.status);
+            launch_sweep<T, double>(ctx, L, rl, x, z, d.omega, d.status);
         } else {
-            k_sweep<T, T><<<gb, kT, 0, s>>>(L.n, L.ro.get(), L.co.get(), L.va.get(), L.inv_diag.get(), rl,
-                                            x, x2, d.omega, d.status);
+            launch_sweep<T, T>(ctx, L, rl, x, x2, d.omega, d.status);
             std::swap(x, x2);
         }
-        check_launch(ctx);
     }
 }
 
 template <class T>
 void destroy_hierarchy(DevHierarchy<T>* d) { delete d; }
 
-template std::unique_ptr<DevHierarchy<double>> upload_hierarchy<double>(cfdxg_context*, const AmgHierarchy&, int);
-template std::unique_ptr<DevHierarchy<float>> upload_hierarchy<float>(cfdxg_context*, const AmgHierarchy&, int);
+template std::unique_ptr<DevHierarchy<double>> upload_hierarchy<double>(cfdxg_context*, const AmgHierarchy&, int, bool);
+template std::unique_ptr<DevHierarchy<float>> upload_hierarchy<float>(cfdxg_context*, const AmgHierarchy&, int, bool);
 template void refresh_hierarchy_values<double>(cfdxg_context*, DevHierarchy<double>&, const AmgHierarchy&);
 template void refresh_hierarchy_values<float>(cfdxg_context*, DevHierarchy<float>&, const AmgHierarchy&);
 template void vcycle_apply<double>(cfdxg_context*, DevHierarchy<double>&, const double*, double*);

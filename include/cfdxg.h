@@ -74,6 +74,25 @@ const char* cfdxg_last_error(const cfdxg_context* ctx);
 /* Number of kernels this library launched on the context since creation. */
 int64_t cfdxg_kernel_launches(const cfdxg_context* ctx);
 int cfdxg_synchronize(cfdxg_context* ctx);
+/* The context's CUDA stream (a cudaStream_t), for callers that order or time
+ * their own work around the library's. */
+void* cfdxg_context_stream(const cfdxg_context* ctx);
+
+/* Live kernel timing: while enabled, the library brackets its eager launches
+ * (fine-level V-cycle kernels, the replay of the coarse-level V-cycle graph,
+ * the FP64 operator SpMV, assembly) with CUDA events on its stream and
+ * accumulates, per kernel class, launches, device milliseconds and the
+ * algorithmic bytes each launch must move (compulsory traffic only).
+ * Enabling resets the counters; reading synchronises the stream. */
+typedef struct {
+    char name[48];
+    int64_t launches;
+    double total_ms;
+    double bytes;
+} cfdxg_kernel_profile;
+int cfdxg_profile_enable(cfdxg_context* ctx, int32_t on);
+int cfdxg_profile_read(cfdxg_context* ctx, cfdxg_kernel_profile* out, int32_t max_entries,
+                       int32_t* count);
 
 /* ------------------------------------------------------------------------ */
 /* mesh + geometry  (core/mesh/mesh.h:51, core/mesh/ownership.h:25)          */
@@ -175,6 +194,11 @@ typedef struct {
     int32_t precision;               /* CFDXG_PRECISION_* of the V-cycle */
     int32_t coarse_dense_limit;      /* FP32 V-cycle: dense FP64 LU at the first
                                         level with <= this many rows (2000) */
+    int32_t reference_order;         /* 1: every row sum in CSR order, so the FP64
+                                        V-cycle is bit-identical to the reference's;
+                                        0 (default): levels with long rows use a
+                                        cooperative, fixed-order (deterministic) row
+                                        reduction */
 } cfdxg_amg_options;
 
 int cfdxg_amg_options_default(cfdxg_amg_options* opts);

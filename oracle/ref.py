@@ -261,6 +261,30 @@ class Amg:
         return x, rep.as_dict()
 
 
+class AmgFromLevels(Amg):
+    """The reference's V-cycle/GMRES around a supplied hierarchy (list of level dicts with
+    row_offsets, columns, values, inv_diag, p_offsets, p_columns, p_values) and damping."""
+
+    def __init__(self, levels, omega):
+        L = len(levels)
+        self._keep = levels
+        self.ro, self.co, self.va = levels[0]["row_offsets"], levels[0]["columns"], levels[0]["values"]
+        P64 = C.POINTER(C.c_int64)
+        PD = C.POINTER(C.c_double)
+        arr = lambda t, key: (t * L)(*[(levels[l][key].ctypes.data_as(t) if levels[l].get(key) is not None
+                                        else t()) for l in range(L)])
+        n_rows = np.array([lv["inv_diag"].size for lv in levels], np.int64)
+        f = lib().ref_amg_create_from_levels
+        f.restype = C.c_void_p
+        f.argtypes = [C.c_int32, C.c_void_p] + [C.c_void_p] * 7 + [C.c_double]
+        self._ptrs = [arr(P64, "row_offsets"), arr(P64, "columns"), arr(PD, "values"), arr(PD, "inv_diag"),
+                      arr(P64, "p_offsets"), arr(P64, "p_columns"), arr(PD, "p_values")]
+        self.h = f(L, n_rows.ctypes.data_as(C.c_void_p), *[C.cast(p, C.c_void_p) for p in self._ptrs], float(omega))
+        if not self.h:
+            raise RuntimeError(f"reference AMG from levels failed: {lib().ref_last_error().decode()}")
+        self.setup_seconds = float("nan")
+
+
 def solve_linear_system(ro, co, va, rhs, x0=None, krylov=3, preconditioner=6, restart=30, max_iterations=1000,
                         tolerance=1e-8):
     ro, co, va = (np.ascontiguousarray(ro, np.int64), np.ascontiguousarray(co, np.int64),

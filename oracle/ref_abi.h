@@ -91,6 +91,13 @@ int ref_gauss_gradient(const ref_mesh_t* m, const double* p,
 void* ref_amg_create(int64_t n, const int64_t* row_offsets, const int64_t* columns,
                      const double* values, int32_t require_smoother_certificate,
                      double* seconds);
+/* Reference preconditioner around a supplied hierarchy (no setup run); for
+ * timing the reference's own V-cycle / GMRES where its setup is infeasible. */
+void* ref_amg_create_from_levels(int32_t n_levels, const int64_t* n_rows,
+                                 const int64_t* const* row_offsets, const int64_t* const* columns,
+                                 const double* const* values, const double* const* inv_diag,
+                                 const int64_t* const* p_offsets, const int64_t* const* p_columns,
+                                 const double* const* p_values, double omega);
 void ref_amg_destroy(void* h);
 int32_t ref_amg_num_levels(void* h);
 double ref_amg_omega(void* h);

@@ -84,6 +84,45 @@ extern "C" void* ref_amg_create(int64_t n, const int64_t* ro, const int64_t* co,
     }
 }
 
+// Builds the reference preconditioner around an externally supplied hierarchy
+// (level CSR matrices, inverse diagonals, prolongations, aggregates, damping)
+// without running setup().  Used only to time the reference's own V-cycle and
+// GMRES at sizes where its setup would take hours; the hierarchy must be the
+// one setup() produces (the parity tests check level-by-level equality).
+extern "C" void* ref_amg_create_from_levels(int32_t n_levels, const int64_t* n_rows,
+                                            const int64_t* const* ro, const int64_t* const* co,
+                                            const double* const* va, const double* const* inv_diag,
+                                            const int64_t* const* p_off, const int64_t* const* p_col,
+                                            const double* const* p_val, double omega) {
+    try {
+        auto h = std::make_unique<AmgHandle>();
+        h->op = std::make_unique<OwnedOperator>(cfdx_ref::make_csr(n_rows[0], ro[0], co[0], va[0]));
+        h->amg = std::make_unique<MatrixFreeVcyclePreconditioner>(
+            *h->op, 0.7, 6, 6, 0.25, 25, AMGInterpolationPolicy::DirectCF, false, false,
+            AMGSmootherPolicy::DampedJacobi, 0.0, 0, 1.0);
+        auto& levels = h->amg->levels_;
+        levels.resize(static_cast<std::size_t>(n_levels));
+        for (int32_t l = 0; l < n_levels; ++l) {
+            const int64_t n = n_rows[l];
+            levels[l].A = cfdx_ref::make_csr(n, ro[l], co[l], va[l]);
+            levels[l].inv_diag.assign(inv_diag[l], inv_diag[l] + n);
+            if (l + 1 < n_levels) {
+                levels[l].prolongation.assign(static_cast<std::size_t>(n), {});
+                levels[l].aggregate.assign(static_cast<std::size_t>(n), 0);
+                for (int64_t i = 0; i < n; ++i)
+                    for (int64_t q = p_off[l][i]; q < p_off[l][i + 1]; ++q)
+                        levels[l].prolongation[i].push_back({static_cast<std::size_t>(p_col[l][q]), p_val[l][q]});
+            }
+        }
+        h->amg->omega_ = omega;
+        cfdx_ref::g_error.clear();
+        return h.release();
+    } catch (const std::exception& e) {
+        cfdx_ref::set_error(e);
+        return nullptr;
+    }
+}
+
 extern "C" void ref_amg_destroy(void* h) { delete static_cast<AmgHandle*>(h); }
 
 extern "C" int32_t ref_amg_num_levels(void* h) {

@@ -93,11 +93,16 @@ def test_vcycle_bit_exact(ctx, ref, tet_setup):
     A, b, phi, grad = cg.assemble_pressure_correction(mesh, U, rAU, p, 1.0, fixed, value)
     ro, co, va = A.to_csr()
     R = ref.Amg(ro, co, va)
-    amg = cg.NativeBoomerAMGPreconditioner(ctx)
+    amg = cg.NativeBoomerAMGPreconditioner(ctx, reference_order=1)
     assert amg.setup(A)
+    fast = cg.NativeBoomerAMGPreconditioner(ctx)
+    assert fast.setup(A)
     for seed in (0, 1):
         r = np.random.default_rng(seed).standard_normal(A.n)
-        assert np.array_equal(amg.apply(r), R.apply(r))
+        z_ref = R.apply(r)
+        assert np.array_equal(amg.apply(r), z_ref)
+        # cooperative row reductions on the dense coarse levels: same cycle, other summation order
+        assert rel_l2(fast.apply(r), z_ref) < 1e-12
 
 
 def test_poisson_solve_matches_reference(ctx, ref):
