@@ -21,6 +21,8 @@ ERRORS = {
     -5: "nonfinite", -6: "geometry", -7: "out_of_memory", -8: "io",
 }
 
+ERRORS_BY_NAME = {v: k for k, v in ERRORS.items()}
+
 c_double_p = C.POINTER(C.c_double)
 c_float_p = C.POINTER(C.c_float)
 c_int64_p = C.POINTER(C.c_int64)
@@ -102,6 +104,7 @@ PROTOTYPES = {
         C.c_int, [_V, _V, _V, _V, _V, C.c_double, _V, _V, C.c_int32, _P(_V), _V, _V, _V]),
     "cfdxg_rhie_chow_flux": (C.c_int, [_V, _V, _V, _V, _V, C.c_double, _V, _V, C.c_int32, _V]),
     "cfdxg_gauss_gradient": (C.c_int, [_V, _V, _V, _V, _V, C.c_int32, _V]),
+    "cfdxg_rhie_chow_flux_noalloc": (C.c_int, [_V, _V, _V, _V, _V, C.c_double, _V, _V, _V]),
     "cfdxg_amg_options_default": (C.c_int, [_P(AmgOptions)]),
     "cfdxg_amg_create": (C.c_int, [_V, _P(AmgOptions), _P(_V)]),
     "cfdxg_amg_destroy": (C.c_int, [_V]),

@@ -14,7 +14,9 @@
 // contraction).  Each row of the CSR is written by the thread of its cell.
 #include <algorithm>
 #include <cmath>
+#include <mutex>
 #include <numeric>
+#include <string>
 
 #include "io.h"
 
@@ -731,6 +733,97 @@ extern "C" int cfdxg_rhie_chow_flux(cfdxg_context* ctx, cfdxg_mesh* m, const dou
     check_launch(ctx);
     fl.finish();
     check_device_status(ctx, "make_rhie_chow_mass_flux");
+    ctx->error.clear();
+    return CFDXG_OK;
+    CFDXG_GUARD_END(ctx)
+}
+
+// ---------------------------------------------------------------------------
+// cfdxg_rhie_chow_flux_noalloc: the Rhie-Chow face flux with its scratch in a
+// static device array, for callers that cannot allocate device memory.
+namespace cfdxg {
+namespace {
+
+constexpr int kNoAllocMaxCells = 1 << 18;   // 262,144 cells
+constexpr int kNoAllocMaxPatches = 32;
+// layout: [3 * kNoAllocMaxCells doubles: gradient SoA][32 doubles: patch value][32 ints: patch fixed flag]
+constexpr std::size_t kNoAllocGradBytes = sizeof(double) * 3 * kNoAllocMaxCells;
+constexpr std::size_t kNoAllocBytes = kNoAllocGradBytes + sizeof(double) * kNoAllocMaxPatches +
+                                      sizeof(int) * kNoAllocMaxPatches;
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocBytes];
+
+// Host-side device address of g_noalloc_scratch, looked up once per device.
+std::mutex g_noalloc_mutex;
+void* g_noalloc_address[64] = {};
+
+struct PatchTable {
+    int n;
+    int fixed[kNoAllocMaxPatches];
+    double value[kNoAllocMaxPatches];
+};
+
+__global__ void k_fill_patch_table(PatchTable t, int* fixed, double* value) {
+    const int k = threadIdx.x;
+    if (k < kNoAllocMaxPatches) {
+        fixed[k] = k < t.n ? t.fixed[k] : 0;
+        value[k] = k < t.n ? t.value[k] : 0.0;
+    }
+}
+
+void* noalloc_scratch_address(int device) {
+    if (device < 0 || device >= 64) throw Error(CFDXG_ERR_INVALID_ARGUMENT, "device index out of range");
+    std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+    if (!g_noalloc_address[device]) {
+        void* ptr = nullptr;
+        const cudaError_t rc = cudaGetSymbolAddress(&ptr, g_noalloc_scratch);
+        if (rc != cudaSuccess || !ptr)
+            throw Error(CFDXG_ERR_CUDA, std::string("cudaGetSymbolAddress(g_noalloc_scratch): ") +
+                                            cudaGetErrorString(rc));
+        g_noalloc_address[device] = ptr;
+    }
+    return g_noalloc_address[device];
+}
+
+}  // namespace
+}  // namespace cfdxg
+
+extern "C" int cfdxg_rhie_chow_flux_noalloc(cfdxg_context* ctx, cfdxg_mesh* m, const double* HbyA,
+                                            const double* rAU, const double* p, double rho,
+                                            const int32_t* fixed, const double* value, double* flux) {
+    if (!ctx || !m) return CFDXG_ERR_INVALID_ARGUMENT;
+    CFDXG_GUARD_BEGIN
+    require_geometry(m);
+    if (!HbyA || !rAU || !p || !flux) throw Error(CFDXG_ERR_INVALID_ARGUMENT, "missing argument");
+    if (m->n_cells > kNoAllocMaxCells)
+        throw Error(CFDXG_ERR_INVALID_ARGUMENT,
+                    "cfdxg_rhie_chow_flux_noalloc: the mesh has " + std::to_string(m->n_cells) +
+                        " cells; its static scratch holds at most " + std::to_string(kNoAllocMaxCells));
+    if (m->n_patches > kNoAllocMaxPatches)
+        throw Error(CFDXG_ERR_INVALID_ARGUMENT,
+                    "cfdxg_rhie_chow_flux_noalloc: at most 32 boundary patches are supported");
+    CFDXG_CUDA(cudaSetDevice(ctx->device));
+    auto* base = static_cast<unsigned char*>(noalloc_scratch_address(ctx->device));
+    double* grad = reinterpret_cast<double*>(base);
+    double* tvalue = reinterpret_cast<double*>(base + kNoAllocGradBytes);
+    int* tfixed = reinterpret_cast<int*>(base + kNoAllocGradBytes + sizeof(double) * kNoAllocMaxPatches);
+    PatchTable t{};
+    t.n = m->n_patches;
+    for (int k = 0; k < m->n_patches; ++k) {
+        t.fixed[k] = fixed ? fixed[k] : 0;
+        t.value[k] = value ? value[k] : 0.0;
+    }
+    const int64_t nc = m->n_cells, nf = m->n_faces;
+    clear_status(ctx);
+    k_fill_patch_table<<<1, kNoAllocMaxPatches, 0, ctx->stream>>>(t, tfixed, tvalue);
+    check_launch(ctx);
+    const BcView bc{tfixed, tvalue, static_cast<int>(m->n_patches)};
+    const MeshView mv = view(m);
+    k_gauss_gradient<<<blocks_for(nc, kT), kT, 0, ctx->stream>>>(mv, bc, p, grad, ctx->scratch.status);
+    check_launch(ctx);
+    k_rhie_chow_flux<<<blocks_for(nf, kT), kT, 0, ctx->stream>>>(mv, bc, HbyA, rAU, p, grad, rho, flux,
+                                                                 ctx->scratch.status);
+    check_launch(ctx);
+    check_device_status(ctx, "make_rhie_chow_mass_flux (no-alloc)");
     ctx->error.clear();
     return CFDXG_OK;
     CFDXG_GUARD_END(ctx)

@@ -173,6 +173,27 @@ int cfdxg_rhie_chow_flux(cfdxg_context* ctx, cfdxg_mesh* mesh, const double* Hby
                          const int32_t* p_bc_fixed, const double* p_bc_value, int32_t mem,
                          double* flux);
 
+/* No counterpart in the reference.  Same result as cfdxg_rhie_chow_flux, for
+ * callers that cannot allocate device memory while they run -- for example a
+ * host solver that reserves all GPU memory up front or works under a memory
+ * pool that forbids new allocations after start-up (cudaMalloc/cudaFree may
+ * also synchronise the device).  This entry point calls no cudaMalloc,
+ * cudaFree or allocating library routine: its scratch (the cell pressure
+ * gradient and the per-patch boundary table) is one static device array of
+ * 6 MiB + 512 B that every GPU loading the library holds until exit.
+ * Limits: at most 262,144 cells and 32 patches; larger meshes are rejected
+ * with CFDXG_ERR_INVALID_ARGUMENT.  HbyA, rAU, p and flux must be device
+ * pointers (mesh already uploaded, geometry built); p_bc_fixed / p_bc_value
+ * are host arrays of n_patches entries.  The first call on a device looks up
+ * the array's device address (so make that first call before any stream
+ * capture).  All calls share the array and it keeps the last call's
+ * contents; every call overwrites what it reads, but calls that overlap on
+ * the GPU (two streams or threads at once) race on it. */
+int cfdxg_rhie_chow_flux_noalloc(cfdxg_context* ctx, cfdxg_mesh* mesh, const double* HbyA,
+                                 const double* rAU, const double* p, double rho,
+                                 const int32_t* p_bc_fixed, const double* p_bc_value,
+                                 double* flux);
+
 /* Replaces gauss_gradient_with_boundary (physics/steady_incompressible_solver.h:1634-1744),
  * default single sweep, distance-weighted interpolation.  grad: 3*n_cells. */
 int cfdxg_gauss_gradient(cfdxg_context* ctx, cfdxg_mesh* mesh, const double* p,
