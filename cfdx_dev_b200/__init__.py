@@ -9,6 +9,7 @@ from .api import (  # noqa: F401
     CfdxgError,
     Context,
     HostMesh,
+    LearnedPreconditioner,
     Mesh,
     NativeBoomerAMGPreconditioner,
     SparseMatrix,

@@ -496,3 +496,72 @@ def solve_gmres(A: SparseMatrix, rhs, x0=None, amg: NativeBoomerAMGPreconditione
 
 def solve_fgmres(A, rhs, x0=None, amg=None, restart=30, max_iterations=1000, tolerance=1e-12, **kw):
     return solve_gmres(A, rhs, x0, amg, restart, max_iterations, tolerance, krylov="fgmres", **kw)
+
+
+# ---------------------------------------------------------------- learned preconditioner
+class LearnedPreconditioner:
+    """4-round, 32-feature message-passing network on the matrix graph (no
+    reference counterpart), applied in front of the AMG V-cycle inside FGMRES.
+    Training runs on the GPU (FP32 forward/backward + Adam); inference uses
+    BF16 tensor-core MLPs with FP32 state and accumulation."""
+
+    def __init__(self, ctx: Context, seed: int = 0):
+        self.ctx, self.lib = ctx, ctx.lib
+        h = C.c_void_p()
+        ctx.check(self.lib.cfdxg_mpnn_create(ctx.handle, seed, C.byref(h)), "mpnn create")
+        self.handle = h
+        cnt = C.c_int64()
+        self.lib.cfdxg_mpnn_num_parameters(h, C.byref(cnt))
+        self.n_params = cnt.value
+        self.n = None
+
+    def bind(self, mesh: Mesh, A: SparseMatrix, a_P):
+        a = _f64(a_P, A.n)
+        self.ctx.check(self.lib.cfdxg_mpnn_bind(self.ctx.handle, self.handle, mesh.handle, A.handle, N.ptr(a),
+                                                N.CFDXG_MEM_HOST), "mpnn bind")
+        self.n = A.n
+
+    def parameters(self) -> np.ndarray:
+        p = np.empty(self.n_params, np.float32)
+        self.ctx.check(self.lib.cfdxg_mpnn_get_parameters(self.ctx.handle, self.handle, N.ptr(p)))
+        return p
+
+    def set_parameters(self, p):
+        p = np.ascontiguousarray(p, np.float32)
+        self.ctx.check(self.lib.cfdxg_mpnn_set_parameters(self.ctx.handle, self.handle, N.ptr(p)))
+
+    def save(self, path):
+        self.ctx.check(self.lib.cfdxg_mpnn_save(self.ctx.handle, self.handle, str(path).encode()), "save")
+
+    def load(self, path):
+        self.ctx.check(self.lib.cfdxg_mpnn_load(self.ctx.handle, self.handle, str(path).encode()), "load")
+
+    def apply(self, r) -> np.ndarray:
+        r = _f64(r, self.n)
+        y = np.empty(self.n)
+        self.ctx.check(self.lib.cfdxg_mpnn_apply(self.ctx.handle, self.handle, N.ptr(r), N.ptr(y), N.CFDXG_MEM_HOST))
+        return y
+
+    def loss_grad(self, R, E):
+        R, E = np.ascontiguousarray(R, np.float64), np.ascontiguousarray(E, np.float64)
+        B = R.shape[0]
+        loss = C.c_double()
+        g = np.empty(self.n_params, np.float32)
+        self.ctx.check(self.lib.cfdxg_mpnn_loss_grad(self.ctx.handle, self.handle, N.ptr(R), N.ptr(E), B,
+                                                     N.CFDXG_MEM_HOST, C.byref(loss), N.ptr(g)), "loss_grad")
+        return loss.value, g
+
+    def train_step(self, R, E, lr=1e-3) -> float:
+        R, E = np.ascontiguousarray(R, np.float64), np.ascontiguousarray(E, np.float64)
+        loss = C.c_double()
+        self.ctx.check(self.lib.cfdxg_mpnn_train_step(self.ctx.handle, self.handle, N.ptr(R), N.ptr(E), R.shape[0],
+                                                      float(lr), N.CFDXG_MEM_HOST, C.byref(loss)), "train_step")
+        return loss.value
+
+    def __del__(self):  # pragma: no cover
+        try:
+            if self.handle:
+                self.lib.cfdxg_mpnn_destroy(self.handle)
+                self.handle = None
+        except Exception:
+            pass

@@ -6,6 +6,7 @@
 
 #include "io.h"
 #include "krylov.h"
+#include "mpnn.h"
 
 using namespace cfdxg;
 
@@ -485,8 +486,13 @@ KrylovResult run_krylov(cfdxg_context* ctx, const cfdxg_matrix* A, cfdxg_amg* am
                         int64_t* learned_fallbacks) {
     RightPreconditioner pc;
     const int n = static_cast<int>(A->n);
-    (void)learned_fallbacks;
-    if (amg) {
+    if (req.learned && amg) {
+        pc = [ctx, amg, A, &req, learned_fallbacks](const double* v, double* z) {
+            return learned_then_amg(ctx, req.learned, A, v, z,
+                                    [ctx, amg](const double* r, double* zz) { amg_apply_device(ctx, amg, r, zz); },
+                                    learned_fallbacks);
+        };
+    } else if (amg) {
         pc = [ctx, amg](const double* v, double* z) {
             amg_apply_device(ctx, amg, v, z);
             return true;
@@ -499,7 +505,9 @@ KrylovResult run_krylov(cfdxg_context* ctx, const cfdxg_matrix* A, cfdxg_amg* am
         };
     }
     const RightPreconditioner* p = pc ? &pc : nullptr;
-    return gmres_solve(ctx, A, b, x, req.gmres_restart, max_it, tol, p, controls_from(req));
+    KrylovResult r = gmres_solve(ctx, A, b, x, req.gmres_restart, max_it, tol, p, controls_from(req));
+    if (req.learned && amg && learned_fallbacks) *learned_fallbacks = learned_take_fallbacks(ctx, req.learned);
+    return r;
 }
 
 void validate_request(const cfdxg_request& r) {
@@ -511,7 +519,8 @@ void validate_request(const cfdxg_request& r) {
         throw Error(CFDXG_ERR_INVALID_ARGUMENT, "requested preconditioner model is not implemented");
     if (r.precision != CFDXG_PRECISION_FP64 && r.precision != CFDXG_PRECISION_FP32_VCYCLE)
         throw Error(CFDXG_ERR_INVALID_ARGUMENT, "unknown precision");
-    if (r.learned) throw Error(CFDXG_ERR_INVALID_ARGUMENT, "learned preconditioner not available in this build");
+    if (r.learned && r.preconditioner != CFDXG_PC_NATIVE_AMG)
+        throw Error(CFDXG_ERR_INVALID_ARGUMENT, "the learned preconditioner runs in front of native AMG");
 }
 
 }  // namespace
@@ -552,6 +561,7 @@ extern "C" int cfdxg_solve_linear_system(cfdxg_context* ctx, const cfdxg_matrix*
         }
         setup_s = amg.setup_seconds;
         if (ok) {
+            if (req.learned) bind_learned_to_matrix(ctx, req.learned, A);
             r = run_krylov(ctx, A, &amg, nullptr, b.get(), xo.get(), req, max_iterations, tolerance, &learned_fallbacks);
         } else {
             r.status = CFDXG_NOT_APPLICABLE;
@@ -608,6 +618,7 @@ extern "C" int cfdxg_solve_gmres(cfdxg_context* ctx, const cfdxg_matrix* A, cfdx
     Out<double> xo(ctx, x, n, mem, /*preload=*/true);
     const double t0 = now_seconds();
     int64_t learned_fallbacks = 0;
+    if (req.learned && amg) bind_learned_to_matrix(ctx, req.learned, A);
     const KrylovResult r = run_krylov(ctx, A, amg, nullptr, b.get(), xo.get(), req, max_iterations, tolerance,
                                       &learned_fallbacks);
     xo.finish();

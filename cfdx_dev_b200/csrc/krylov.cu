@@ -577,6 +577,12 @@ KrylovResult gmres_solve(cfdxg_context* ctx, const cfdxg_matrix* A, const double
     return result;
 }
 
+void enqueue_dot(cfdxg_context* ctx, int64_t n, const double* a, const double* b, double* out) {
+    k_dot<<<reduce_blocks(n), kT, 0, ctx->stream>>>(static_cast<int>(n), a, b, ctx->scratch.partial,
+                                                    ctx->scratch.ticket, out);
+    check_launch(ctx);
+}
+
 double device_norm2(cfdxg_context* ctx, const cfdxg_matrix* A, const double* a) {
     Engine E(ctx, A);
     E.norm2(a, kNorm);

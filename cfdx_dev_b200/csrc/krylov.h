@@ -45,6 +45,8 @@ KrylovResult gmres_solve(cfdxg_context* ctx, const cfdxg_matrix* A, const double
 
 // Scaled two-pass 2-norm of a device vector (krylov_norm2).
 double device_norm2(cfdxg_context* ctx, const cfdxg_matrix* A, const double* a);
+// Enqueues out = sum_i a_i b_i (deterministic fixed-order reduction) into a device scalar.
+void enqueue_dot(cfdxg_context* ctx, int64_t n, const double* a, const double* b, double* out);
 // ||b - A x|| with the FP64 operator.
 double device_residual_norm(cfdxg_context* ctx, const cfdxg_matrix* A, const double* b, const double* x);
 

@@ -1,0 +1,130 @@
+"""Train the learned message-passing preconditioner on the GPU.
+
+Training data are (residual, error) pairs that the plain solver itself
+generates: on seeded Kuhn-tet meshes of lattice sizes between --min-n and
+--max-n (6 tets per hex, interior vertices jittered by +-0.15h) the
+pressure-correction system is assembled, and for each residual r the error
+e = A^-1 r is obtained with plain FP64 AMG-GMRES to a relative residual of
+1e-10.  Residuals mix the assembled continuity right-hand sides (other HbyA
+seeds), white noise, and smooth fields mapped through A.  The loss is the
+A-norm of the error, (e - N(r))^T A (e - N(r)) / (e^T A e), minimised with
+Adam by the library's own forward and backward kernels.
+
+    python -m cfdx_dev_b200.train_mpnn --meshes 64 --pairs-per-mesh 16 \
+        --min-n 16 --max-n 40 --epochs 30 --out weights.bin
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import sys
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parents[1]
+if str(ROOT) not in sys.path:
+    sys.path.insert(0, str(ROOT))
+
+import cfdx_dev_b200 as cg  # noqa: E402
+
+SEED_BASE = 7_000_000
+
+
+def make_system(ctx, n, seed):
+    """Jittered Kuhn-tet mesh, pressure-correction matrix and its inputs."""
+    m = cg.tet_case(n, 0.15, SEED_BASE + seed)
+    mesh = cg.Mesh(ctx, m)
+    g = mesh.geometry()
+    aP = cg.random_field(m.n_cells, "loguniform", 1.0, 100.0, SEED_BASE + 1000 + seed)
+    rAU = np.concatenate([1.0 / aP] * 3)
+    fixed = np.zeros(m.n_patches, np.int32)
+    fixed[0] = 1
+    value = np.zeros(m.n_patches)
+    U = cg.fourier_field(g["cell_centres"], 8, 0.01, SEED_BASE + 2000 + seed)
+    A, b, phi, grad = cg.assemble_pressure_correction(mesh, U, rAU, np.zeros(m.n_cells), 1.0, fixed, value)
+    return dict(m=m, mesh=mesh, g=g, aP=aP, rAU=rAU, fixed=fixed, value=value, A=A)
+
+
+def make_pairs(ctx, sysd, k, seed):
+    """k (r, e) pairs; e solved with the plain FP64 AMG-GMRES path."""
+    A, m, g = sysd["A"], sysd["m"], sysd["g"]
+    amg = cg.NativeBoomerAMGPreconditioner(ctx)
+    if not amg.setup(A):
+        raise RuntimeError(amg.last_error())
+    rng = np.random.default_rng(SEED_BASE + 3000 + seed)
+    R, E = [], []
+    for q in range(k):
+        kind = q % 3
+        if kind == 0:   # continuity residual of another predictor field
+            U = cg.fourier_field(g["cell_centres"], 8, 0.01, SEED_BASE + 4000 + 97 * seed + q)
+            _, r, _, _ = cg.assemble_pressure_correction(sysd["mesh"], U, sysd["rAU"], np.zeros(m.n_cells), 1.0,
+                                                         sysd["fixed"], sysd["value"])
+        elif kind == 1:  # white noise
+            r = rng.standard_normal(m.n_cells)
+        else:            # smooth field through the operator
+            u = cg.fourier_field(g["cell_centres"], 4, 0.0, SEED_BASE + 5000 + 97 * seed + q)[:m.n_cells]
+            r = A.matvec(u + 0.1 * rng.standard_normal(m.n_cells))
+        r = r / np.sqrt(np.mean(r * r))
+        e, rep = cg.solve_gmres(A, r, amg=amg, restart=30, tolerance=1e-10, max_iterations=2000)
+        if rep["status_name"] != "converged":
+            raise RuntimeError(f"training pair solve failed: {rep}")
+        R.append(r)
+        E.append(e)
+    return np.array(R), np.array(E)
+
+
+def train(args):
+    ctx = cg.Context(0)
+    net = cg.LearnedPreconditioner(ctx, seed=args.seed)
+    sizes = np.linspace(args.min_n, args.max_n, args.meshes).round().astype(int)
+    data = []
+    t0 = time.time()
+    for i, n in enumerate(sizes):
+        sysd = make_system(ctx, int(n), i)
+        R, E = make_pairs(ctx, sysd, args.pairs_per_mesh, i)
+        data.append((sysd, R, E))
+        print(f"mesh {i} n={n} cells={sysd['m'].n_cells} pairs={len(R)} ({time.time() - t0:.1f}s)", flush=True)
+    gen_s = time.time() - t0
+    rng = np.random.default_rng(args.seed)
+    history = []
+    t1 = time.time()
+    lr = args.lr
+    for epoch in range(args.epochs):
+        losses = []
+        for i in rng.permutation(len(data)):
+            sysd, R, E = data[i]
+            net.bind(sysd["mesh"], sysd["A"], sysd["aP"])
+            for b in range(0, len(R), args.batch):
+                losses.append(net.train_step(R[b:b + args.batch], E[b:b + args.batch], lr=lr))
+        if epoch == int(0.7 * args.epochs):
+            lr *= 0.3
+        history.append(float(np.mean(losses)))
+        print(f"epoch {epoch} loss {history[-1]:.4f} ({time.time() - t1:.1f}s)", flush=True)
+    net.save(args.out)
+    summary = {"meshes": len(data), "pairs": int(sum(len(R) for _, R, _ in data)),
+               "sizes": [int(s) for s in sizes], "generation_s": gen_s, "training_s": time.time() - t1,
+               "loss_history": history, "params": net.n_params, "out": str(args.out)}
+    print(json.dumps(summary), flush=True)
+    return net, summary
+
+
+def main(argv=None):
+    ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
+    ap.add_argument("--meshes", type=int, default=64)
+    ap.add_argument("--pairs-per-mesh", type=int, default=16)
+    ap.add_argument("--min-n", type=int, default=16)
+    ap.add_argument("--max-n", type=int, default=40)
+    ap.add_argument("--epochs", type=int, default=30)
+    ap.add_argument("--batch", type=int, default=8)
+    ap.add_argument("--lr", type=float, default=2e-3)
+    ap.add_argument("--seed", type=int, default=0)
+    ap.add_argument("--out", type=Path, default=ROOT / "cfdx_dev_b200" / "weights" / "mpnn.bin")
+    args = ap.parse_args(argv)
+    args.out.parent.mkdir(parents=True, exist_ok=True)
+    train(args)
+
+
+if __name__ == "__main__":
+    main()

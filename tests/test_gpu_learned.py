@@ -1,0 +1,90 @@
+"""GPU kernels of the learned preconditioner against the FP64 oracle
+(oracle/mpnn_oracle.py, itself pinned by finite differences)."""
+import numpy as np
+import pytest
+
+import cfdx_dev_b200 as cg
+from oracle import mpnn_oracle as mo
+from tests import cases
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def bound(ctx, ref):
+    m = cases.simple_mesh(6)
+    mesh = cg.Mesh(ctx, m)
+    g = mesh.geometry()
+    U, rAU, aP, p, fixed, value = cases.simple_fields(m, g["cell_centres"])
+    A, b, phi, grad = cg.assemble_pressure_correction(mesh, U, rAU, p, 1.0, fixed, value)
+    ro, co, va = A.to_csr()
+    G = mo.Graph(ro, co, va, g["cell_volumes"], aP)
+    net = cg.LearnedPreconditioner(ctx, seed=3)
+    net.bind(mesh, A, aP)
+    theta = mo.init_params(5)
+    net.set_parameters(theta.astype(np.float32))
+    theta32 = net.parameters().astype(np.float64)
+    return dict(mesh=mesh, A=A, b=b, G=G, net=net, theta=theta32, aP=aP, m=m)
+
+
+def _pairs(G, k=2, seed=0):
+    rng = np.random.default_rng(seed)
+    R, E = [], []
+    for _ in range(k):
+        e = rng.standard_normal(G.n)
+        R.append(G.matvec(e) + 0.05 * rng.standard_normal(G.n))
+        E.append(e)
+    return np.array(R), np.array(E)
+
+
+def test_parameter_count_matches_oracle(bound):
+    assert bound["net"].n_params == mo.N_PARAMS
+
+
+def test_training_gradient_matches_oracle(bound):
+    G, net, theta = bound["G"], bound["net"], bound["theta"]
+    R, E = _pairs(G)
+    loss, grad = net.loss_grad(R, E)
+    loss_ref, grad_ref = mo.loss_and_grad(theta, G, list(zip(R, E)))
+    assert abs(loss - loss_ref) <= 1e-5 * abs(loss_ref)
+    # FP32 kernels vs FP64 oracle
+    assert np.linalg.norm(grad - grad_ref) <= 1e-4 * np.linalg.norm(grad_ref)
+
+
+def test_tensor_core_inference_matches_oracle(bound):
+    G, net, theta = bound["G"], bound["net"], bound["theta"]
+    r = np.random.default_rng(4).standard_normal(G.n)
+    y = net.apply(r)
+    y_ref = mo.forward(theta, G, r)
+    # BF16 operands, FP32 accumulation
+    assert np.linalg.norm(y - y_ref) <= 3e-2 * np.linalg.norm(y_ref)
+    assert np.allclose(net.apply(2.0 * r), 2.0 * y, rtol=1e-5, atol=1e-12 * np.abs(y).max())
+
+
+def test_training_reduces_loss_and_weights_roundtrip(bound, tmp_path):
+    G, net = bound["G"], bound["net"]
+    R, E = _pairs(G, 4, seed=1)
+    l0 = net.train_step(R, E, lr=3e-3)
+    for _ in range(30):
+        l1 = net.train_step(R, E, lr=3e-3)
+    assert l1 < 0.7 * l0
+    p = net.parameters()
+    path = tmp_path / "w.bin"
+    net.save(path)
+    net2 = cg.LearnedPreconditioner(net.ctx, seed=99)
+    net2.load(path)
+    assert np.array_equal(net2.parameters(), p)
+    raw = bytearray(path.read_bytes())
+    raw[40] ^= 0xFF
+    path.write_bytes(bytes(raw))
+    with pytest.raises(cg.CfdxgError):
+        net2.load(path)
+
+
+def test_learned_fgmres_converges_with_fallback_accounting(bound):
+    A, b, net = bound["A"], bound["b"], bound["net"]
+    x, rep = cg.solve_linear_system(A, b, krylov="fgmres", precision="fp32_vcycle", restart=30, tolerance=1e-8,
+                                    learned=net)
+    assert rep["status_name"] == "converged"
+    assert rep["physical_residual_relative"] <= 1e-8
+    assert 0 <= rep["learned_fallbacks"] <= rep["preconditioner_applications"]
