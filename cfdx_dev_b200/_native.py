@@ -46,6 +46,7 @@ class AmgOptions(C.Structure):
         ("strength_threshold", C.c_double), ("max_levels", C.c_int32),
         ("require_smoother_certificate", C.c_int32), ("precision", C.c_int32),
         ("coarse_dense_limit", C.c_int32), ("reference_order", C.c_int32),
+        ("coarse_sweeps", C.c_int32),
     ]
 
 
@@ -143,6 +144,7 @@ PROTOTYPES = {
     "cfdxg_mpnn_load": (C.c_int, [_V, _V, C.c_char_p]),
     "cfdxg_mpnn_bind": (C.c_int, [_V, _V, _V, _V, _V, C.c_int32]),
     "cfdxg_mpnn_apply": (C.c_int, [_V, _V, _V, _V, C.c_int32]),
+    "cfdxg_mpnn_set_vcycle": (C.c_int, [_V, _V, _V]),
     "cfdxg_mpnn_train_step": (C.c_int, [_V, _V, _V, _V, C.c_int32, C.c_float, C.c_int32, c_double_p]),
     "cfdxg_mpnn_loss_grad": (C.c_int, [_V, _V, _V, _V, C.c_int32, C.c_int32, c_double_p, _V]),
 }

@@ -521,6 +521,10 @@ class LearnedPreconditioner:
                                                 N.CFDXG_MEM_HOST), "mpnn bind")
         self.n = A.n
 
+    def set_vcycle(self, amg):
+        """Train in front of this V-cycle (composed-preconditioner loss); None: the network alone."""
+        self.ctx.check(self.lib.cfdxg_mpnn_set_vcycle(self.ctx.handle, self.handle, amg.handle if amg else None))
+
     def parameters(self) -> np.ndarray:
         p = np.empty(self.n_params, np.float32)
         self.ctx.check(self.lib.cfdxg_mpnn_get_parameters(self.ctx.handle, self.handle, N.ptr(p)))

@@ -52,6 +52,7 @@ struct AmgOptions {
     double omega = 0.7;
     int pre = 6;
     int post = 6;
+    int coarse_sweeps = -1;   // sweeps on levels >= 1 (-1: pre / post)
     double strength_threshold = 0.25;
     int max_levels = 25;
     bool require_smoother_certificate = false;

@@ -72,6 +72,7 @@ void amg_setup_impl(cfdxg_context* ctx, cfdxg_amg* amg, cfdxg_matrix* A) {
     o.omega = amg->opts.omega;
     o.pre = amg->opts.pre_sweeps;
     o.post = amg->opts.post_sweeps;
+    o.coarse_sweeps = amg->opts.coarse_sweeps;
     o.strength_threshold = amg->opts.strength_threshold;
     o.max_levels = amg->opts.max_levels;
     o.require_smoother_certificate = amg->opts.require_smoother_certificate != 0;
@@ -96,13 +97,13 @@ void amg_setup_impl(cfdxg_context* ctx, cfdxg_amg* amg, cfdxg_matrix* A) {
     amg->setup_seconds = now_seconds() - t0;
 }
 
-void amg_apply_device(cfdxg_context* ctx, cfdxg_amg* amg, const double* r, double* z) {
+}  // namespace
+
+void cfdxg::amg_apply_device(cfdxg_context* ctx, cfdxg_amg* amg, const double* r, double* z) {
     if (amg->d32) vcycle_apply<float>(ctx, *amg->d32, r, z);
     else vcycle_apply<double>(ctx, *amg->d64, r, z);
     ++amg->applications;
 }
-
-}  // namespace
 
 // ---------------------------------------------------------------- context
 extern "C" int cfdxg_context_create(int32_t device, cfdxg_context** out) {
@@ -293,6 +294,7 @@ extern "C" int cfdxg_amg_options_default(cfdxg_amg_options* o) {
     o->precision = CFDXG_PRECISION_FP64;
     o->coarse_dense_limit = 2000;
     o->reference_order = 0;
+    o->coarse_sweeps = -1;
     return CFDXG_OK;
 }
 
@@ -402,6 +404,7 @@ extern "C" int cfdxg_amg_setup_host(cfdxg_amg* amg, int64_t n, const int64_t* ro
     o.omega = amg->opts.omega;
     o.pre = amg->opts.pre_sweeps;
     o.post = amg->opts.post_sweeps;
+    o.coarse_sweeps = amg->opts.coarse_sweeps;
     o.strength_threshold = amg->opts.strength_threshold;
     o.max_levels = amg->opts.max_levels;
     o.require_smoother_certificate = amg->opts.require_smoother_certificate != 0;
@@ -486,11 +489,26 @@ KrylovResult run_krylov(cfdxg_context* ctx, const cfdxg_matrix* A, cfdxg_amg* am
                         int64_t* learned_fallbacks) {
     RightPreconditioner pc;
     const int n = static_cast<int>(A->n);
+    // Learned stage: dropped for the rest of the solve (plain AMG fallback)
+    // as soon as an iteration fails to cut the residual estimate by 10%.
+    struct LearnedState {
+        bool active = true;
+        double last = std::numeric_limits<double>::infinity();
+        int64_t fallbacks = 0;
+    } state;
+    IterationObserver observer = [&state](double est) {
+        if (state.active && !(est < 0.9 * state.last)) state.active = false;
+        state.last = est;
+    };
     if (req.learned && amg) {
-        pc = [ctx, amg, A, &req, learned_fallbacks](const double* v, double* z) {
-            return learned_then_amg(ctx, req.learned, A, v, z,
-                                    [ctx, amg](const double* r, double* zz) { amg_apply_device(ctx, amg, r, zz); },
-                                    learned_fallbacks);
+        pc = [ctx, amg, A, &req, &state](const double* v, double* z) {
+            auto vcycle = [ctx, amg](const double* r, double* zz) { amg_apply_device(ctx, amg, r, zz); };
+            if (!state.active) {
+                ++state.fallbacks;
+                vcycle(v, z);
+                return true;
+            }
+            return learned_then_amg(ctx, req.learned, A, v, z, vcycle, nullptr);
         };
     } else if (amg) {
         pc = [ctx, amg](const double* v, double* z) {
@@ -505,8 +523,9 @@ KrylovResult run_krylov(cfdxg_context* ctx, const cfdxg_matrix* A, cfdxg_amg* am
         };
     }
     const RightPreconditioner* p = pc ? &pc : nullptr;
-    KrylovResult r = gmres_solve(ctx, A, b, x, req.gmres_restart, max_it, tol, p, controls_from(req));
-    if (req.learned && amg && learned_fallbacks) *learned_fallbacks = learned_take_fallbacks(ctx, req.learned);
+    KrylovResult r = gmres_solve(ctx, A, b, x, req.gmres_restart, max_it, tol, p, controls_from(req),
+                                 req.learned && amg ? &observer : nullptr);
+    if (learned_fallbacks) *learned_fallbacks = state.fallbacks;
     return r;
 }
 

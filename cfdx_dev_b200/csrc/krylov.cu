@@ -256,7 +256,7 @@ int choose_restart(int current, double reduction, const KrylovControls& c) {
 
 KrylovResult gmres_solve(cfdxg_context* ctx, const cfdxg_matrix* A, const double* b, double* x,
                          int restart, int64_t max_iter, double tolerance, const RightPreconditioner* pc,
-                         const KrylovControls& controls) {
+                         const KrylovControls& controls, const IterationObserver* observer) {
     KrylovResult result;
     const int64_t n = A->n;
     if (n == 0 || restart <= 0 || max_iter == 0 || !std::isfinite(tolerance) || tolerance <= 0.0) {
@@ -299,7 +299,7 @@ KrylovResult gmres_solve(cfdxg_context* ctx, const cfdxg_matrix* A, const double
             E.neg(ws.ax.get(), shifted.get());
             y.zero(ctx->stream);
             const KrylovResult sh = gmres_solve(ctx, A, shifted.get(), y.get(), restart, max_iter, tolerance, pc,
-                                                controls);
+                                                controls, observer);
             Workspace& ws2 = workspace(ctx, n, current_restart);
             E.add(x, y.get());
             E.residual(b, x, ws2.r.get());
@@ -445,6 +445,7 @@ KrylovResult gmres_solve(cfdxg_context* ctx, const cfdxg_matrix* A, const double
             ++iterations;
             ++used;
             estimated_residual = std::abs(g[j + 1]);
+            if (observer) (*observer)(estimated_residual);
             if (breakdown_detected) {
                 arnoldi_breakdown = true;
                 break;

@@ -39,9 +39,12 @@ struct KrylovResult {
 // when it cannot run.  Non-finite results are reported through the status word.
 using RightPreconditioner = std::function<bool(const double* v, double* z)>;
 
+// Called after every Arnoldi step with the Givens estimate of the residual norm.
+using IterationObserver = std::function<void(double estimated_residual)>;
+
 KrylovResult gmres_solve(cfdxg_context* ctx, const cfdxg_matrix* A, const double* b, double* x,
                          int restart, int64_t max_iter, double tolerance, const RightPreconditioner* pc,
-                         const KrylovControls& controls);
+                         const KrylovControls& controls, const IterationObserver* observer = nullptr);
 
 // Scaled two-pass 2-norm of a device vector (krylov_norm2).
 double device_norm2(cfdxg_context* ctx, const cfdxg_matrix* A, const double* a);

@@ -55,8 +55,8 @@ struct cfdxg_mpnn {
     cfdxg::DevBuf<double> diag;
     // work
     cfdxg::DevBuf<float> H, AG, Z, dh, dh2, dhself, da, hA, hB, dyf;
-    cfdxg::DevBuf<double> y, t, Ad, Ae, outb;
-    cfdxg::DevBuf<unsigned long long> fallbacks;
+    cfdxg::DevBuf<double> y, t, Ad, Ae, outb, w1, w2, q;
+    cfdxg_amg* vcycle = nullptr;   // V-cycle the network is trained in front of
 };
 
 namespace cfdxg {
@@ -170,13 +170,29 @@ __global__ void __launch_bounds__(kThreads) k_round_tc(int n, const int* __restr
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int c0 = (blockIdx.x * kWarps + warp) * 16;
     if (c0 >= n) return;
+    // Row ranges of the 16 cells are loaded once by lanes 0..15; each cell's
+    // (<= 32) neighbour indices and weights by one lane each, then broadcast,
+    // so the feature rows of a cell are fetched with independent loads.
+    int rb = 0, re = 0;
+    if (lane < 16 && c0 + lane < n) {
+        rb = ro[c0 + lane];
+        re = ro[c0 + lane + 1];
+    }
+#pragma unroll 2
     for (int r = 0; r < 16; ++r) {
         const int c = c0 + r;
-        float hv = 0.0f, av = 0.0f;
-        if (c < n) {
-            hv = h_in[static_cast<size_t>(c) * F + lane];
-            for (int k = ro[c]; k < ro[c + 1]; ++k) av += ew[k] * h_in[static_cast<size_t>(co[k]) * F + lane];
+        const int b = __shfl_sync(0xffffffffu, rb, r), e = __shfl_sync(0xffffffffu, re, r);
+        const int len = min(e - b, 32);
+        const int cj = lane < len ? co[b + lane] : 0;
+        const float wj = lane < len ? ew[b + lane] : 0.0f;
+        float hv = c < n ? h_in[static_cast<size_t>(c) * F + lane] : 0.0f;
+        float av = 0.0f;
+        for (int q = 0; q < len; ++q) {
+            const int j = __shfl_sync(0xffffffffu, cj, q);
+            const float w = __shfl_sync(0xffffffffu, wj, q);
+            av += w * h_in[static_cast<size_t>(j) * F + lane];
         }
+        for (int k = b + 32; k < e; ++k) av += ew[k] * h_in[static_cast<size_t>(co[k]) * F + lane];
         sU[warp][r][lane] = __float2bfloat16_rn(hv);
         sU[warp][r][F + lane] = __float2bfloat16_rn(av);
     }
@@ -433,20 +449,6 @@ __global__ void k_residual64(int n, const int* __restrict__ ro, const int* __res
     t[i] = v[i] - s;
 }
 
-// Keep the learned stage only if it reduced the residual; otherwise t = v, y = 0.
-__global__ void k_select(int n, const double* tt, const double* vv, const double* __restrict__ v, double* __restrict__ t,
-                         double* __restrict__ y, unsigned long long* fallbacks) {
-    const bool keep = isfinite(*tt) && *tt < *vv;
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (!keep) {
-        if (i < n) {
-            t[i] = v[i];
-            y[i] = 0.0;
-        }
-        if (i == 0) atomicAdd(fallbacks, 1ull);
-    }
-}
-
 __global__ void k_add_inplace(int n, double* __restrict__ z, const double* __restrict__ y) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i < n) z[i] += y[i];
@@ -534,8 +536,26 @@ double loss_grad_one(cfdxg_context* ctx, cfdxg_mpnn* net, const double* r, const
     check_launch(ctx);
     spmv_fp64(ctx, net->A, net->t.get(), net->Ad.get());
     spmv_fp64(ctx, net->A, e, net->Ae.get());
-    enqueue_dot(ctx, n, e, net->Ae.get(), eAe);
-    enqueue_dot(ctx, n, net->t.get(), net->Ad.get(), dAd);
+    if (!net->vcycle) {
+        enqueue_dot(ctx, n, e, net->Ae.get(), eAe);
+        enqueue_dot(ctx, n, net->t.get(), net->Ad.get(), dAd);
+    } else {
+        // w1 = E d, w2 = E w1 (E = I - M A); gradient direction A w2; scale by ||E e||_A^2
+        amg_apply_device(ctx, net->vcycle, net->Ad.get(), net->q.get());
+        k_sub<<<blocks_for(n, 256), 256, 0, s>>>(n, net->t.get(), net->q.get(), net->w1.get());
+        check_launch(ctx);
+        spmv_fp64(ctx, net->A, net->w1.get(), net->Ad.get());            // A w1
+        enqueue_dot(ctx, n, net->w1.get(), net->Ad.get(), dAd);
+        amg_apply_device(ctx, net->vcycle, net->Ad.get(), net->q.get());
+        k_sub<<<blocks_for(n, 256), 256, 0, s>>>(n, net->w1.get(), net->q.get(), net->w2.get());
+        check_launch(ctx);
+        spmv_fp64(ctx, net->A, net->w2.get(), net->Ad.get());            // A w2
+        amg_apply_device(ctx, net->vcycle, net->Ae.get(), net->q.get());  // M A e
+        k_sub<<<blocks_for(n, 256), 256, 0, s>>>(n, e, net->q.get(), net->w1.get());   // E e
+        check_launch(ctx);
+        spmv_fp64(ctx, net->A, net->w1.get(), net->Ae.get());
+        enqueue_dot(ctx, n, net->w1.get(), net->Ae.get(), eAe);
+    }
     k_dy<<<blocks_for(n, 256), 256, 0, s>>>(n, net->Ad.get(), eAe, rr, net->diag.get(), net->dyf.get());
     check_launch(ctx);
     k_readout_bwd<<<kGridBlocks, kThreads, 0, s>>>(n, net->H.get() + R * st, net->dyf.get(), net->params.get(),
@@ -564,6 +584,8 @@ double loss_grad_one(cfdxg_context* ctx, cfdxg_mpnn* net, const double* r, const
 
 double loss_grad_batch(cfdxg_context* ctx, cfdxg_mpnn* net, const double* r, const double* e, int batch) {
     require_bound(net);
+    if (net->vcycle && net->vcycle->host.levels.front().A.n != net->n)
+        throw Error(CFDXG_ERR_INVALID_ARGUMENT, "training V-cycle and bound matrix differ in size");
     const int n = net->n;
     net->partial.resize(static_cast<size_t>(kGridBlocks) * NP);
     net->partial.zero(ctx->stream);
@@ -602,24 +624,10 @@ bool learned_then_amg(cfdxg_context* ctx, cfdxg_mpnn* net, const cfdxg_matrix* A
     k_residual64<<<blocks_for(n, 256), 256, 0, s>>>(n, A->ro.get(), A->co.get(), A->va.get(), v, net->y.get(),
                                                      net->t.get());
     check_launch(ctx);
-    double* tt = scalar(ctx, 4);
-    double* vv = scalar(ctx, 5);
-    enqueue_dot(ctx, n, net->t.get(), net->t.get(), tt);
-    enqueue_dot(ctx, n, v, v, vv);
-    k_select<<<blocks_for(n, 256), 256, 0, s>>>(n, tt, vv, v, net->t.get(), net->y.get(), net->fallbacks.get());
-    check_launch(ctx);
     amg(net->t.get(), z);
     k_add_inplace<<<blocks_for(n, 256), 256, 0, s>>>(n, z, net->y.get());
     check_launch(ctx);
     return true;
-}
-
-int64_t learned_take_fallbacks(cfdxg_context* ctx, cfdxg_mpnn* net) {
-    unsigned long long h = 0;
-    CFDXG_CUDA(cudaMemcpyAsync(&h, net->fallbacks.get(), sizeof(h), cudaMemcpyDeviceToHost, ctx->stream));
-    CFDXG_CUDA(cudaMemsetAsync(net->fallbacks.get(), 0, sizeof(h), ctx->stream));
-    CFDXG_CUDA(cudaStreamSynchronize(ctx->stream));
-    return static_cast<int64_t>(h);
 }
 
 }  // namespace cfdxg
@@ -647,8 +655,6 @@ extern "C" int cfdxg_mpnn_create(cfdxg_context* ctx, uint64_t seed, cfdxg_mpnn**
     net->adam_v.resize(mp::NP);
     net->adam_m.zero(ctx->stream);
     net->adam_v.zero(ctx->stream);
-    net->fallbacks.resize(1);
-    net->fallbacks.zero(ctx->stream);
     upload_params(ctx, net.get());
     *out = net.release();
     return CFDXG_OK;
@@ -785,10 +791,21 @@ extern "C" int cfdxg_mpnn_bind(cfdxg_context* ctx, cfdxg_mpnn* net, cfdxg_mesh* 
     net->dh.resize(st); net->dh2.resize(st); net->dhself.resize(st); net->da.resize(st);
     net->hA.resize(st); net->hB.resize(st); net->dyf.resize(n);
     net->y.resize(n); net->t.resize(n); net->Ad.resize(n); net->Ae.resize(n); net->outb.resize(n);
+    net->w1.resize(n); net->w2.resize(n); net->q.resize(n);
     CFDXG_CUDA(cudaStreamSynchronize(ctx->stream));
     net->A = A;
     net->n = static_cast<int>(n);
     ctx->error.clear();
+    return CFDXG_OK;
+    CFDXG_GUARD_END(ctx)
+}
+
+extern "C" int cfdxg_mpnn_set_vcycle(cfdxg_context* ctx, cfdxg_mpnn* net, cfdxg_amg* amg) {
+    if (!ctx || !net) return CFDXG_ERR_INVALID_ARGUMENT;
+    CFDXG_GUARD_BEGIN
+    if (amg && (!amg->ready || (!amg->d64 && !amg->d32)))
+        throw Error(CFDXG_ERR_NOT_READY, "the V-cycle is not set up on the device");
+    net->vcycle = amg;
     return CFDXG_OK;
     CFDXG_GUARD_END(ctx)
 }

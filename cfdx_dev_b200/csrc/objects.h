@@ -38,6 +38,7 @@ struct DevHierarchy {
     int used = 0;              // levels visited by the cycle
     T omega = T(0.7);
     int pre = 6, post = 6;
+    int coarse_pre = 6, coarse_post = 6;   // sweeps on levels >= 1
     int coarse_mode = 0;       // 0: 24 Jacobi sweeps, 1: reference dense LU (n <= 16), 2: FP64 inverse
     DevBuf<double> dense;      // mode 1: n*n matrix, mode 2: n*n inverse (row-major)
     cudaGraph_t graph = nullptr;
@@ -108,6 +109,9 @@ template <class T>
 void vcycle_apply(cfdxg_context* ctx, DevHierarchy<T>& d, const double* r, double* z);
 template <class T>
 void destroy_hierarchy(DevHierarchy<T>* d);
+
+// z = one V-cycle of a device-ready hierarchy applied to r (device vectors)
+void amg_apply_device(cfdxg_context* ctx, cfdxg_amg* amg, const double* r, double* z);
 
 // status word helpers (context.cu)
 void clear_status(cfdxg_context* ctx);

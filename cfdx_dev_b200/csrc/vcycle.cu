@@ -51,6 +51,9 @@ template <class T, int TPR>
 __device__ __forceinline__ T row_dot(int b, int e, int lane, const int* __restrict__ co,
                                      const T* __restrict__ va, const T* __restrict__ x) {
     T s = T(0);
+    // unrolled so several independent (value, column, x) loads are in flight;
+    // the additions stay in the same sequential order
+#pragma unroll 4
     for (int k = b + lane; k < e; k += TPR) s += va[k] * __ldg(x + co[k]);
     if (TPR > 1) {
 #pragma unroll
@@ -451,7 +454,7 @@ void enqueue_from(cfdxg_context* ctx, DevHierarchy<T>& d, int l) {
         }
         return;
     }
-    sweeps_from_zero(ctx, d, L, L.r.get(), d.pre);
+    sweeps_from_zero(ctx, d, L, L.r.get(), d.coarse_pre);
     T* x = L.xout;
     T* x2 = (x == L.x.get()) ? L.x2.get() : L.x.get();
     launch_residual<T>(ctx, L, L.r.get(), x, L.res.get());
@@ -459,7 +462,7 @@ void enqueue_from(cfdxg_context* ctx, DevHierarchy<T>& d, int l) {
     launch_restrict<T>(ctx, L, L.res.get(), C.r.get());
     enqueue_from(ctx, d, l + 1);
     launch_prolong<T>(ctx, L, C.xout, x, d.status);
-    for (int k = 0; k < d.post; ++k) {
+    for (int k = 0; k < d.coarse_post; ++k) {
         launch_sweep<T, T>(ctx, L, L.r.get(), x, x2, d.omega, d.status);
         std::swap(x, x2);
     }
@@ -498,6 +501,8 @@ std::unique_ptr<DevHierarchy<T>> upload_hierarchy(cfdxg_context* ctx, const AmgH
     d->omega = static_cast<T>(h.omega);
     d->pre = h.options.pre;
     d->post = h.options.post;
+    d->coarse_pre = h.options.coarse_sweeps >= 0 ? h.options.coarse_sweeps : h.options.pre;
+    d->coarse_post = h.options.coarse_sweeps >= 0 ? h.options.coarse_sweeps : h.options.post;
     d->status = ctx->scratch.status;
     int used = static_cast<int>(h.levels.size());
     d->coarse_mode = 0;

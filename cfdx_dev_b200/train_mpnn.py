@@ -7,7 +7,9 @@ pressure-correction system is assembled, and for each residual r the error
 e = A^-1 r is obtained with plain FP64 AMG-GMRES to a relative residual of
 1e-10.  Residuals mix the assembled continuity right-hand sides (other HbyA
 seeds), white noise, and smooth fields mapped through A.  The loss is the
-A-norm of the error, (e - N(r))^T A (e - N(r)) / (e^T A e), minimised with
+A-norm of the error of the composed preconditioner z = N(r) + M(r - A N(r))
+with M the FP32 AMG V-cycle, ||(I - M A)(e - N(r))||_A^2 / ||(I - M A) e||_A^2
+(below 1 when the learned stage improves on the V-cycle alone), minimised with
 Adam by the library's own forward and backward kernels.
 
     python -m cfdx_dev_b200.train_mpnn --meshes 64 --pairs-per-mesh 16 \
@@ -53,6 +55,10 @@ def make_pairs(ctx, sysd, k, seed):
     amg = cg.NativeBoomerAMGPreconditioner(ctx)
     if not amg.setup(A):
         raise RuntimeError(amg.last_error())
+    # the FP32 V-cycle the learned stage runs in front of
+    sysd["vcycle"] = cg.NativeBoomerAMGPreconditioner(ctx, precision="fp32_vcycle")
+    if not sysd["vcycle"].setup(A):
+        raise RuntimeError(sysd["vcycle"].last_error())
     rng = np.random.default_rng(SEED_BASE + 3000 + seed)
     R, E = [], []
     for q in range(k):
@@ -96,6 +102,7 @@ def train(args):
         for i in rng.permutation(len(data)):
             sysd, R, E = data[i]
             net.bind(sysd["mesh"], sysd["A"], sysd["aP"])
+            net.set_vcycle(sysd["vcycle"] if args.composed else None)
             for b in range(0, len(R), args.batch):
                 losses.append(net.train_step(R[b:b + args.batch], E[b:b + args.batch], lr=lr))
         if epoch == int(0.7 * args.epochs):
@@ -120,6 +127,8 @@ def main(argv=None):
     ap.add_argument("--batch", type=int, default=8)
     ap.add_argument("--lr", type=float, default=2e-3)
     ap.add_argument("--seed", type=int, default=0)
+    ap.add_argument("--composed", type=int, default=1,
+                    help="1: loss of the learned stage in front of the FP32 V-cycle; 0: the network alone")
     ap.add_argument("--out", type=Path, default=ROOT / "cfdx_dev_b200" / "weights" / "mpnn.bin")
     args = ap.parse_args(argv)
     args.out.parent.mkdir(parents=True, exist_ok=True)

@@ -220,6 +220,9 @@ typedef struct {
                                         0 (default): levels with long rows use a
                                         cooperative, fixed-order (deterministic) row
                                         reduction */
+    int32_t coarse_sweeps;           /* pre/post sweeps on levels >= 1; -1 (default):
+                                        the same as pre_sweeps / post_sweeps, as in
+                                        the reference */
 } cfdxg_amg_options;
 
 int cfdxg_amg_options_default(cfdxg_amg_options* opts);
@@ -330,6 +333,12 @@ int cfdxg_mpnn_apply(cfdxg_context* ctx, cfdxg_mpnn* net, const double* r, doubl
  * (e - N(r))^T A (e - N(r)) / (e^T A e).  r, e: batch * n_cells, row-major. */
 int cfdxg_mpnn_train_step(cfdxg_context* ctx, cfdxg_mpnn* net, const double* r, const double* e,
                           int32_t batch, float learning_rate, int32_t mem, double* loss);
+/* Sets the V-cycle M the network is trained in front of (NULL: the network
+ * alone).  With M the loss of a pair is that of the composed preconditioner
+ * z = N(r) + M(r - A N(r)):  ||(I - M A)(e - N(r))||_A^2 / ||(I - M A) e||_A^2,
+ * i.e. below 1 exactly when the learned stage improves on the V-cycle alone.
+ * M must be symmetric (damped-Jacobi V(k,k) with Galerkin coarse levels is). */
+int cfdxg_mpnn_set_vcycle(cfdxg_context* ctx, cfdxg_mpnn* net, cfdxg_amg* amg);
 /* Loss and parameter gradient without an update (for gradient checks). */
 int cfdxg_mpnn_loss_grad(cfdxg_context* ctx, cfdxg_mpnn* net, const double* r, const double* e,
                          int32_t batch, int32_t mem, double* loss, float* grad);

@@ -111,20 +111,35 @@ def forward(theta, g: Graph, r, keep=False):
     return (out, cache) if keep else out
 
 
-def loss_and_grad(theta, g: Graph, pairs):
-    """Mean loss over pairs [(r, e), ...] and its gradient with respect to theta."""
+def loss_and_grad(theta, g: Graph, pairs, M=None):
+    """Mean loss over pairs [(r, e), ...] and its gradient with respect to theta.
+
+    With M (a symmetric V-cycle, callable r -> M r) the loss is that of the
+    composed preconditioner z = N(r) + M(r - A N(r)), whose error is
+    E (e - N(r)) with E = I - M A:
+        L = ||E (e - N(r))||_A^2 / ||E e||_A^2,   dL/dN = -2 A E^2 (e - N) / ||E e||_A^2."""
     p = unpack(theta)
     grads = {name: np.zeros(shape) for name, shape in PARAM_LAYOUT}
     total = 0.0
     for r, e in pairs:
         out, c = forward(theta, g, r, keep=True)
         d = e - out
-        Ad = g.matvec(d)
-        eAe = float(e @ g.matvec(e))
-        total += float(d @ Ad) / eAe
+        if M is None:
+            Ad = g.matvec(d)
+            eAe = float(e @ g.matvec(e))
+            total += float(d @ Ad) / eAe
+            gvec = Ad
+        else:
+            w1 = d - M(g.matvec(d))
+            Aw1 = g.matvec(w1)
+            w2 = w1 - M(Aw1)
+            Ee = e - M(g.matvec(e))
+            eAe = float(Ee @ g.matvec(Ee))
+            total += float(w1 @ Aw1) / eAe
+            gvec = g.matvec(w2)
         if c is None:
             continue
-        dout = -2.0 * Ad / eAe
+        dout = -2.0 * gvec / eAe
         dy = c["s"] * dout / g.diag
         h = c["h"][-1]
         grads["w_out"] += h.T @ dy

@@ -51,6 +51,24 @@ def test_training_gradient_matches_oracle(bound):
     assert np.linalg.norm(grad - grad_ref) <= 1e-4 * np.linalg.norm(grad_ref)
 
 
+def test_composed_training_gradient_matches_oracle(bound, ref):
+    """Gradient of the learned stage in front of the V-cycle (bit-identical to the reference's)."""
+    G, net, theta, A = bound["G"], bound["net"], bound["theta"], bound["A"]
+    ro, co, va = A.to_csr()
+    R_amg = ref.Amg(ro, co, va)
+    amg = cg.NativeBoomerAMGPreconditioner(net.ctx, reference_order=1)
+    assert amg.setup(A)
+    net.set_vcycle(amg)
+    try:
+        R, E = _pairs(G, seed=7)
+        loss, grad = net.loss_grad(R, E)
+        loss_ref, grad_ref = mo.loss_and_grad(theta, G, list(zip(R, E)), M=R_amg.apply)
+    finally:
+        net.set_vcycle(None)
+    assert abs(loss - loss_ref) <= 1e-5 * abs(loss_ref)
+    assert np.linalg.norm(grad - grad_ref) <= 1e-4 * np.linalg.norm(grad_ref)
+
+
 def test_tensor_core_inference_matches_oracle(bound):
     G, net, theta = bound["G"], bound["net"], bound["theta"]
     r = np.random.default_rng(4).standard_normal(G.n)

@@ -48,3 +48,23 @@ def test_oracle_is_homogeneous_in_the_residual(ref):
     y2 = mo.forward(theta, G, 3.5 * x)
     assert np.allclose(3.5 * y1, y2, rtol=1e-12, atol=0)
     assert np.all(mo.forward(theta, G, 0 * x) == 0)
+
+
+def test_oracle_composed_gradient_matches_finite_differences(ref):
+    """Loss of N in front of the (symmetric) reference V-cycle."""
+    G, r = small_graph(ref, 4)
+    R = ref.Amg(r["row_offsets"], r["columns"], r["values"])
+    rng = np.random.default_rng(2)
+    theta = mo.init_params(3)
+    pairs = []
+    for _ in range(2):
+        e = rng.standard_normal(G.n)
+        pairs.append((G.matvec(e), e))
+    L, grad = mo.loss_and_grad(theta, G, pairs, M=R.apply)
+    for i in rng.choice(theta.size, 30, replace=False):
+        h = 1e-6 * max(1.0, abs(theta[i]))
+        tp, tm = theta.copy(), theta.copy()
+        tp[i] += h
+        tm[i] -= h
+        fd = (mo.loss_and_grad(tp, G, pairs, M=R.apply)[0] - mo.loss_and_grad(tm, G, pairs, M=R.apply)[0]) / (2 * h)
+        assert abs(fd - grad[i]) <= 1e-5 * max(1.0, abs(fd)), (i, fd, grad[i])
