@@ -21,7 +21,8 @@ the library's stream, max over ranks.  N > 1 runs independent replicas (each
 rank its own right-hand sides); there is no data-path collective.
 
 `--impl reference` times the reference's own CPU solve phase (oracle/_ref,
-one host core) on the same system.
+one host core; the bit-identical C restatement where that build is absent)
+on the same system.
 """
 from __future__ import annotations
 
@@ -43,17 +44,20 @@ TOL = 1e-8
 RESTART = 30
 N_RHS = 16
 FALLBACK_HBM_GBS = 6650.0
+WEIGHTS = ROOT / "cfdx_dev_b200" / "weights" / "mpnn.bin"
+METRIC = "s to 1e-8 FP64 residual/pressure solve: learned+FP32 vs plain AMG-GMRES, 1xB200"
 
 
 def parse_args():
     ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=8)
+    ap.add_argument("--steps", type=int, default=24)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["cfdxg", "reference"], default="cfdxg")
     ap.add_argument("--n", type=int, default=64, help="lattice size (cells = 6 n^3)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-learned", action="store_true", help="skip the learned+FP32 form")
     return ap.parse_args()
 
 
@@ -166,19 +170,33 @@ def run_cfdxg(args):
             base_rAU = rAU
         # the matrix depends on rAU and geometry only; HbyA changes b
         A, b, phi, grad = cg.assemble_pressure_correction(mesh, U, base_rAU, p, 1.0, fixed, value, matrix=A)
+        if k == 0:
+            base_aP = aP
         rhs_list.append(b)
     case_s = time.time() - t0
     n_cells = A.n
 
+    # (form, V-cycle precision, Krylov method, learned stage)
+    plan = [("plain_fp64", "fp64", "gmres", False), ("fp32_vcycle", "fp32_vcycle", "fgmres", False)]
+    net = None
+    if WEIGHTS.exists() and not args.no_learned:
+        net = cg.LearnedPreconditioner(ctx)
+        net.load(str(WEIGHTS))
+        net.bind(mesh, A, base_aP)
+        plan.append(("learned_fp32", "fp32_vcycle", "fgmres", True))
+    headline = plan[-1][0]
     forms = {}
     amgs = {}
-    for form, prec in (("plain_fp64", "fp64"), ("fp32_vcycle", "fp32_vcycle")):
-        amg = cg.NativeBoomerAMGPreconditioner(ctx, precision=prec)
-        t = time.time()
-        if not amg.setup(A):
-            raise RuntimeError(amg.last_error())
-        amgs[form] = amg
-        forms[form] = {"setup_s": time.time() - t, "host_setup_s": amg.setup_seconds}
+    by_precision = {}   # one hierarchy per V-cycle precision, shared by the forms that use it
+    for form, prec, krylov, learned in plan:
+        if prec not in by_precision:
+            amg = cg.NativeBoomerAMGPreconditioner(ctx, precision=prec)
+            t = time.time()
+            if not amg.setup(A):
+                raise RuntimeError(amg.last_error())
+            by_precision[prec] = (amg, {"setup_s": time.time() - t, "host_setup_s": amg.setup_seconds})
+        amgs[form] = by_precision[prec][0]
+        forms[form] = dict(by_precision[prec][1])
     levels = amgs["plain_fp64"].hierarchy_level_sizes()
     level_nnz = amgs["plain_fp64"].hierarchy_level_nnz()
 
@@ -186,8 +204,10 @@ def run_cfdxg(args):
     x_dev = torch.zeros(n_cells, dtype=torch.float64, device=dev)
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=dev)   # 256 MB > L2
 
-    def solve_device(amg, krylov, k):
-        req = cg.make_request(krylov, "native_amg", RESTART, "fp64")
+    def request(krylov, learned):
+        return cg.make_request(krylov, "native_amg", RESTART, "fp64", net if learned else None)
+
+    def solve_device(amg, req, k):
         rep = N.Report()
         rc = lib.cfdxg_solve_gmres(ctx.handle, A.handle, amg.handle, C.c_void_p(b_dev[k].data_ptr()),
                                    C.c_void_p(x_dev.data_ptr()), N.CFDXG_MEM_DEVICE, C.byref(req), 1000, TOL,
@@ -197,15 +217,14 @@ def run_cfdxg(args):
 
     ref_solutions = {}
     sampler = ClockSampler(local_rank)
-    headline = "fp32_vcycle"
-    for form in ("plain_fp64", "fp32_vcycle"):
+    for form, prec, krylov, learned in plan:
         amg = amgs[form]
-        krylov = "gmres" if form == "plain_fp64" else "fgmres"
+        req = request(krylov, learned)
         for w in range(args.warmup):
             x_dev.zero_()
             torch.cuda.synchronize()
-            solve_device(amg, krylov, w % N_RHS)
-        times, iters, errs = [], [], []
+            solve_device(amg, req, w % N_RHS)
+        times, iters, errs, fallbacks = [], [], [], []
         launches0 = ctx.kernel_launches
         if form == headline:
             ctx.profile(True)
@@ -220,11 +239,12 @@ def run_cfdxg(args):
             e0 = torch.cuda.Event(enable_timing=True)
             e1 = torch.cuda.Event(enable_timing=True)
             e0.record(lstream)
-            rep = solve_device(amg, krylov, k)
+            rep = solve_device(amg, req, k)
             e1.record(lstream)
             torch.cuda.synchronize()
             times.append(e0.elapsed_time(e1) / 1e3)
             iters.append(rep["iterations"])
+            fallbacks.append(rep["learned_fallbacks"])
             if rep["status_name"] != "converged" or rep["physical_residual_relative"] > TOL:
                 raise RuntimeError(f"{form} did not converge: {rep}")
             x = x_dev.cpu().numpy()
@@ -240,6 +260,10 @@ def run_cfdxg(args):
         forms[form].update(s_per_solve=float(np.mean(times)), s_min=float(np.min(times)),
                            iterations=float(np.mean(iters)),
                            rel_error_vs_fp64=(float(np.max(errs)) if errs else 0.0))
+        if learned:
+            forms[form]["learned_fallback_applications"] = float(np.mean(fallbacks))
+    for form in forms:
+        forms[form]["speedup_vs_plain_fp64"] = forms["plain_fp64"]["s_per_solve"] / forms[form]["s_per_solve"]
 
     # ---- end to end through the C ABI with pinned host buffers ----
     e2e = None
@@ -248,7 +272,7 @@ def run_cfdxg(args):
         b_host = torch.empty(n_cells, dtype=torch.float64, pin_memory=True)
         x_host = torch.empty(n_cells, dtype=torch.float64, pin_memory=True)
         bh, xh = b_host.numpy(), x_host.numpy()
-        req = cg.make_request("fgmres", "native_amg", RESTART, "fp64")
+        req = request(plan[-1][2], plan[-1][3])
         e2e_times = []
         for s in range(args.warmup + args.steps):
             k = s % N_RHS
@@ -300,9 +324,9 @@ def run_cfdxg(args):
     if rank == 0:
         cpu = None
         if world == 1 and not args.no_cpu_baseline:
-            cpu = cpu_baseline(amgs["plain_fp64"], A, rhs_list[0], forms["plain_fp64"]["iterations"])
+            cpu = cpu_baseline(amgs["plain_fp64"], rhs_list[0])
         result = {
-            "metric": "s to 1e-8 FP64 residual/pressure solve: learned+FP32 vs plain AMG-GMRES, 1xB200",
+            "metric": METRIC,
             "value": value, "unit": "s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": value * 1e3, "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
             "dtype": "f64 (Krylov) / f32 (V-cycle)", "data": "synthetic (seeded)",
@@ -327,59 +351,77 @@ def _export_levels(amg):
     return [amg.export_level(l) for l in range(len(amg.hierarchy_level_sizes()))]
 
 
-def cpu_baseline(amg, A, b, plain_iterations):
-    """The reference's solve phase (oracle/_ref) on the same system, one host core."""
-    from oracle import ref
-    if not ref.available():
-        return {"value": None, "unit": "s", "cores": 1, "kind": "reference", "sample": "oracle/_ref not built"}
-    levels = _export_levels(amg)
-    R = ref.AmgFromLevels(levels, amg.omega)
+class _CpuSolver:
+    """The reference's CPU solve phase around a given hierarchy: the reference
+    itself (oracle/_ref, kind "reference") where it was built, else the plain-C
+    restatement (oracle/cfdx_oracle.c, bit-identical to it, kind "port")."""
+
+    def __init__(self, levels, omega):
+        from oracle import ref
+        if ref.available():
+            self.kind = "reference"
+            self.R = ref.AmgFromLevels(levels, omega)
+        else:
+            from oracle import cfdx_oracle as co
+            self.kind = "port"
+            self.co = co
+            self.H = co.Hierarchy(levels, omega)
+            self.csr = (levels[0]["row_offsets"], levels[0]["columns"], levels[0]["values"])
+
+    def solve(self, b, max_iterations):
+        """-> (iterations, solve seconds)"""
+        if self.kind == "reference":
+            x, rep = self.R.solve_gmres(b, restart=RESTART, max_iterations=max_iterations, tolerance=TOL)
+            return rep["iterations"], rep["solve_seconds"]
+        t = time.perf_counter()
+        x, rep = self.co.solve_gmres(*self.csr, b, self.H, restart=RESTART, max_iterations=max_iterations,
+                                     tolerance=TOL)
+        return rep["iterations"], time.perf_counter() - t
+
+
+def cpu_baseline(amg, b):
+    """The reference's solve phase on the same system, one host core."""
+    S = _CpuSolver(_export_levels(amg), amg.omega)
     t = time.time()
-    x, rep = R.solve_gmres(b, restart=RESTART, max_iterations=1000, tolerance=TOL)
-    dt = time.time() - t
-    return {"value": rep["solve_seconds"], "unit": "s", "cores": 1, "kind": "reference",
-            "iterations": rep["iterations"], "wall_s": dt,
-            "sample": "one complete reference GMRES(30)+NativeAMG solve phase to 1e-8 on the full system "
-                      "(hierarchy loaded: bit-identical to the reference setup, which takes hours at this size)"}
+    iters, sec = S.solve(b, 1000)
+    return {"value": sec, "unit": "s", "cores": 1, "kind": S.kind, "iterations": iters, "wall_s": time.time() - t,
+            "sample": "one complete GMRES(30)+NativeAMG solve phase to 1e-8 on the full system, first right-hand "
+                      "side (hierarchy loaded: bit-identical to the reference setup, which takes hours at this "
+                      "size)"}
 
 
 def run_reference(args):
-    """Reference arm: the reference's own CPU solve phase (oracle/_ref) on this config."""
+    """Reference arm: the reference's own CPU solve phase on this config."""
     rank, local_rank, world = dist_env()
     if rank != 0:
         return None
-    from oracle import ref
     import cfdx_dev_b200 as cg
+    from oracle import cfdx_oracle as co
     from tests import cases
-    if not ref.available():
-        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libcfdx_ref.so not built"}))
-        return None
     m = cases.simple_mesh(args.n)
-    g = ref.geometry(m)
+    g = co.geometry(m)
     U, rAU, aP, p, fixed, value = cases.simple_fields(m, g["cell_centres"])
-    r = ref.simple_assemble(m, U, rAU, p, 1.0, fixed, value)
+    r = co.simple_assemble(m, U, rAU, p, 1.0, fixed, value)
     amg = cg.NativeBoomerAMGPreconditioner(None)
     if not amg.setup_host(r["row_offsets"], r["columns"], r["values"]):
         raise RuntimeError(amg.last_error())
-    R = ref.AmgFromLevels(_export_levels(amg), amg.omega)
-    # first warmup step: one complete solve, for the iteration count
-    x, full = R.solve_gmres(r["b"], restart=RESTART, max_iterations=1000, tolerance=TOL)
-    iters = full["iterations"]
+    S = _CpuSolver(_export_levels(amg), amg.omega)
+    # first warm-up step: one complete solve, for the iteration count
+    iters, full_s = S.solve(r["b"], 1000)
     sample_its = 2
     for _ in range(max(0, args.warmup - 1)):
-        R.solve_gmres(r["b"], restart=RESTART, max_iterations=sample_its, tolerance=TOL)
-    ts = []
-    for _ in range(args.steps):
-        x, rep = R.solve_gmres(r["b"], restart=RESTART, max_iterations=sample_its, tolerance=TOL)
-        ts.append(rep["solve_seconds"])
+        S.solve(r["b"], sample_its)
+    ts = [S.solve(r["b"], sample_its)[1] for _ in range(args.steps)]
     v = float(np.mean(ts)) / sample_its * iters
-    out = {"impl": "reference", "metric": "s to 1e-8 FP64 residual/pressure solve: learned+FP32 vs plain AMG-GMRES, 1xB200",
-           "value": v, "unit": "s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
-           "higher_is_better": False, "config": {"workload": f"Kuhn-tet {args.n}^3 x6 = {m.n_cells} cells"},
-           "cpu_baseline": {"value": v, "unit": "s", "cores": 1, "kind": "reference",
-                            "sample": f"reference GMRES(30)+NativeAMG solve phase capped at {sample_its} iterations "
+    out = {"impl": "reference", "metric": METRIC, "value": v, "unit": "s", "n_gpus": world, "steps": args.steps,
+           "warmup": args.warmup, "ms_per_step": v * 1e3, "higher_is_better": False, "scaling": "weak",
+           "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)",
+           "config": {"workload": f"Kuhn-tet {args.n}^3 x6 = {m.n_cells} cells, SIMPLE pressure correction, "
+                                  f"GMRES({RESTART}) + native RS AMG to 1e-8"},
+           "cpu_baseline": {"value": v, "unit": "s", "cores": 1, "kind": S.kind,
+                            "sample": f"GMRES(30)+NativeAMG solve phase capped at {sample_its} iterations "
                                       f"per step, scaled to the full solve's {iters} iterations "
-                                      f"(full solve measured once in warm-up: {full['solve_seconds']:.2f} s)"},
+                                      f"(full solve measured once in warm-up: {full_s:.2f} s)"},
            "e2e": {"value": v, "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(out), flush=True)
     return out

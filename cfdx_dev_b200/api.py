@@ -361,6 +361,8 @@ class NativeBoomerAMGPreconditioner:
         self.lib.cfdxg_amg_options_default(C.byref(o))
         o.precision = N.PRECISION[precision]
         o.require_smoother_certificate = int(bool(require_smoother_certificate))
+        if "coarse_sweeps" in options:   # shorthand: the same count before and after
+            o.coarse_pre_sweeps = o.coarse_post_sweeps = options.pop("coarse_sweeps")
         for k, v in options.items():
             setattr(o, k, v)
         h = C.c_void_p()

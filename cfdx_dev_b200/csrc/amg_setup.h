@@ -52,7 +52,8 @@ struct AmgOptions {
     double omega = 0.7;
     int pre = 6;
     int post = 6;
-    int coarse_sweeps = -1;   // sweeps on levels >= 1 (-1: pre / post)
+    int coarse_pre = -1;    // sweeps on levels >= 1 (-1: the V-cycle precision's default)
+    int coarse_post = -1;
     double strength_threshold = 0.25;
     int max_levels = 25;
     bool require_smoother_certificate = false;

@@ -72,7 +72,8 @@ void amg_setup_impl(cfdxg_context* ctx, cfdxg_amg* amg, cfdxg_matrix* A) {
     o.omega = amg->opts.omega;
     o.pre = amg->opts.pre_sweeps;
     o.post = amg->opts.post_sweeps;
-    o.coarse_sweeps = amg->opts.coarse_sweeps;
+    o.coarse_pre = amg->opts.coarse_pre_sweeps;
+    o.coarse_post = amg->opts.coarse_post_sweeps;
     o.strength_threshold = amg->opts.strength_threshold;
     o.max_levels = amg->opts.max_levels;
     o.require_smoother_certificate = amg->opts.require_smoother_certificate != 0;
@@ -294,7 +295,8 @@ extern "C" int cfdxg_amg_options_default(cfdxg_amg_options* o) {
     o->precision = CFDXG_PRECISION_FP64;
     o->coarse_dense_limit = 2000;
     o->reference_order = 0;
-    o->coarse_sweeps = -1;
+    o->coarse_pre_sweeps = -1;
+    o->coarse_post_sweeps = -1;
     return CFDXG_OK;
 }
 
@@ -404,7 +406,8 @@ extern "C" int cfdxg_amg_setup_host(cfdxg_amg* amg, int64_t n, const int64_t* ro
     o.omega = amg->opts.omega;
     o.pre = amg->opts.pre_sweeps;
     o.post = amg->opts.post_sweeps;
-    o.coarse_sweeps = amg->opts.coarse_sweeps;
+    o.coarse_pre = amg->opts.coarse_pre_sweeps;
+    o.coarse_post = amg->opts.coarse_post_sweeps;
     o.strength_threshold = amg->opts.strength_threshold;
     o.max_levels = amg->opts.max_levels;
     o.require_smoother_certificate = amg->opts.require_smoother_certificate != 0;

@@ -15,6 +15,7 @@
 // captured once into a CUDA graph with fixed buffers and replayed.
 #include <cmath>
 #include <limits>
+#include <type_traits>
 
 #include "objects.h"
 
@@ -24,6 +25,8 @@ namespace {
 
 constexpr int kT = 256;
 constexpr int kCoarseSweeps = 24;   // amg_preconditioner.h:2585
+constexpr int kFp32CoarsePre = 0;   // FP32 cycle on levels >= 1: V(0,1)
+constexpr int kFp32CoarsePost = 1;
 constexpr int kDenseDirectLimit = 16;
 
 template <class T>
@@ -47,6 +50,8 @@ __global__ void k_sweep_zero(int n, T omega, const T* __restrict__ inv_diag, con
 // sequentially in CSR order (the reference's order).  TPR > 1 gives each
 // thread the entries k = lane, lane + TPR, ... and combines the partial sums
 // with a fixed xor butterfly, so results are deterministic run to run.
+// (A variant reading 16-byte chunks of four entries per lane measured ~5%
+// slower on the tet hierarchies: the loop is latency-bound, not issue-bound.)
 template <class T, int TPR>
 __device__ __forceinline__ T row_dot(int b, int e, int lane, const int* __restrict__ co,
                                      const T* __restrict__ va, const T* __restrict__ x) {
@@ -457,9 +462,13 @@ void enqueue_from(cfdxg_context* ctx, DevHierarchy<T>& d, int l) {
     sweeps_from_zero(ctx, d, L, L.r.get(), d.coarse_pre);
     T* x = L.xout;
     T* x2 = (x == L.x.get()) ? L.x2.get() : L.x.get();
-    launch_residual<T>(ctx, L, L.r.get(), x, L.res.get());
     DevLevel<T>& C = d.L[l + 1];
-    launch_restrict<T>(ctx, L, L.res.get(), C.r.get());
+    if (d.coarse_pre > 0) {
+        launch_residual<T>(ctx, L, L.r.get(), x, L.res.get());
+        launch_restrict<T>(ctx, L, L.res.get(), C.r.get());
+    } else {
+        launch_restrict<T>(ctx, L, L.r.get(), C.r.get());   // x = 0: the residual is r
+    }
     enqueue_from(ctx, d, l + 1);
     launch_prolong<T>(ctx, L, C.xout, x, d.status);
     for (int k = 0; k < d.coarse_post; ++k) {
@@ -501,8 +510,15 @@ std::unique_ptr<DevHierarchy<T>> upload_hierarchy(cfdxg_context* ctx, const AmgH
     d->omega = static_cast<T>(h.omega);
     d->pre = h.options.pre;
     d->post = h.options.post;
-    d->coarse_pre = h.options.coarse_sweeps >= 0 ? h.options.coarse_sweeps : h.options.pre;
-    d->coarse_post = h.options.coarse_sweeps >= 0 ? h.options.coarse_sweeps : h.options.post;
+    // Levels >= 1: the reference's pre/post counts for the FP64 cycle.  The FP32
+    // cycle defaults to one post-sweep and no pre-sweep there (its fine level
+    // keeps pre/post): the coarse operators hold ~25x the fine level's nonzeros,
+    // and V(0,1) reads each of them once per cycle instead of twice for V(1,1).
+    const bool fp32 = std::is_same<T, float>::value;
+    const int coarse_default_pre = fp32 ? kFp32CoarsePre : h.options.pre;
+    const int coarse_default_post = fp32 ? kFp32CoarsePost : h.options.post;
+    d->coarse_pre = h.options.coarse_pre >= 0 ? h.options.coarse_pre : coarse_default_pre;
+    d->coarse_post = h.options.coarse_post >= 0 ? h.options.coarse_post : coarse_default_post;
     d->status = ctx->scratch.status;
     int used = static_cast<int>(h.levels.size());
     d->coarse_mode = 0;

@@ -220,9 +220,11 @@ typedef struct {
                                         0 (default): levels with long rows use a
                                         cooperative, fixed-order (deterministic) row
                                         reduction */
-    int32_t coarse_sweeps;           /* pre/post sweeps on levels >= 1; -1 (default):
-                                        the same as pre_sweeps / post_sweeps, as in
-                                        the reference */
+    int32_t coarse_pre_sweeps;       /* pre / post sweeps on levels >= 1; -1 (default):   */
+    int32_t coarse_post_sweeps;      /* FP64 cycle -- pre_sweeps / post_sweeps, as in the
+                                        reference; FP32 cycle -- 0 / 1 (the fine level keeps
+                                        pre_sweeps / post_sweeps).  With 0 pre-sweeps a level
+                                        restricts its right-hand side directly (x = 0). */
 } cfdxg_amg_options;
 
 int cfdxg_amg_options_default(cfdxg_amg_options* opts);

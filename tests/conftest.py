@@ -1,8 +1,9 @@
 """Shared pytest setup.
 
 * registers the ``gpu`` marker (tests that need a B200);
-* makes the in-tree library and the reference-built oracle available,
-  building them when their sources are present and the binaries are not.
+* makes the in-tree library, the plain-C oracle and the reference build
+  available, building them when their sources are present and the binaries
+  are not (the reference build only where the reference tree exists).
 """
 from __future__ import annotations
 
@@ -48,6 +49,14 @@ def ctx():
     c = Context(int(os.environ.get("CFDXG_TEST_DEVICE", "0")))
     yield c
     c.close()
+
+
+@pytest.fixture(scope="session")
+def oracle():
+    """The plain-C restatement (oracle/cfdx_oracle.c), built with gcc on first use."""
+    from oracle import cfdx_oracle as co
+    co.lib()
+    return co
 
 
 @pytest.fixture(scope="session")

@@ -1,9 +1,14 @@
-"""GPU parity against the reference-built oracle, through the C ABI.
+"""GPU parity against the oracle, through the C ABI.
+
+The checker is the plain-C restatement (oracle/cfdx_oracle.c), itself pinned
+bit-for-bit to the reference by tests/test_oracle_pin.py.
 
 Bit-exact: geometry, Poisson assembly, pressure-corrector assembly (CSR
-values, b, phiHbyA, grad p), Rhie-Chow face flux, one FP64 V-cycle.
-Tolerance-bound (relative L2 <= 1e-10): pressure after the full GMRES+AMG
-solve, and the corrected face fluxes; the iteration count must match.
+values, b, phiHbyA, grad p), Gauss gradient, Rhie-Chow face flux, SpMV, one
+FP64 V-cycle in reference summation order.  Tolerance-bound (relative L2
+<= 1e-10): pressure after the full GMRES+AMG solve, and the corrected face
+fluxes; the iteration count must match.  Where the reference build is present
+the same solve is also compared with the reference itself.
 """
 import numpy as np
 import pytest
@@ -13,15 +18,22 @@ from tests import cases
 
 pytestmark = pytest.mark.gpu
 
-REL_TOL = 1e-10   # pressure / face-flux parity with the FP64 reference
+REL_TOL = 1e-10   # pressure / face-flux parity with the FP64 oracle
 
 
 def rel_l2(a, b):
     return np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300)
 
 
+def oracle_hierarchy(oracle, amg):
+    """The oracle's V-cycle on the hierarchy the library built (its host setup is
+    pinned bit-exact to the reference's by the CPU tests)."""
+    n = len(amg.hierarchy_level_sizes())
+    return oracle.Hierarchy([amg.export_level(l) for l in range(n)], amg.omega)
+
+
 @pytest.fixture(scope="module")
-def tet_setup(ctx, ref):
+def tet_setup(ctx):
     m = cases.simple_mesh(10)
     mesh = cg.Mesh(ctx, m)
     g = mesh.geometry()
@@ -29,31 +41,31 @@ def tet_setup(ctx, ref):
     return m, mesh, g, (U, rAU, aP, p, fixed, value)
 
 
-@pytest.mark.parametrize("kind", ["hex", "tet"])
-def test_geometry_bit_exact(ctx, ref, kind):
-    m = cases.poisson_case(6)[0] if kind == "hex" else cases.simple_mesh(6)
+@pytest.mark.parametrize("kind", ["hex", "tet", "bl"])
+def test_geometry_bit_exact(ctx, oracle, kind):
+    m = {"hex": lambda: cases.poisson_case(6)[0], "tet": lambda: cases.simple_mesh(6),
+         "bl": lambda: cg.boundary_layer_case(8, 6, 5)}[kind]()
     mine = cg.Mesh(ctx, m).geometry()
-    for which in ("fv", "cache"):
-        theirs = ref.geometry(m, which)
-        for k in mine:
-            assert np.array_equal(mine[k], theirs[k]), (which, k)
+    theirs = oracle.geometry(m)
+    for k in mine:
+        assert np.array_equal(mine[k], theirs[k]), k
 
 
-def test_poisson_assembly_bit_exact(ctx, ref):
+def test_poisson_assembly_bit_exact(ctx, oracle):
     m, bc, src = cases.poisson_case(8)
     mesh = cg.Mesh(ctx, m)
     A, rhs = cg.assemble_cell_diffusion_matrix(mesh, bc, 1.0, src)
-    ro, co, va, rhs_ref, _ = ref.assemble_diffusion(m, bc, 1.0, src)
+    ro, co, va, rhs_ref = oracle.assemble_diffusion(m, bc, 1.0, src)
     r2, c2, v2 = A.to_csr()
     assert np.array_equal(r2, ro) and np.array_equal(c2, co)
     assert np.array_equal(v2, va)
     assert np.array_equal(rhs, rhs_ref)
 
 
-def test_pressure_assembly_bit_exact(ctx, ref, tet_setup):
+def test_pressure_assembly_bit_exact(ctx, oracle, tet_setup):
     m, mesh, g, (U, rAU, aP, p, fixed, value) = tet_setup
     A, b, phi, grad = cg.assemble_pressure_correction(mesh, U, rAU, p, 1.0, fixed, value)
-    r = ref.simple_assemble(m, U, rAU, p, 1.0, fixed, value)
+    r = oracle.simple_assemble(m, U, rAU, p, 1.0, fixed, value)
     ro, co, va = A.to_csr()
     assert np.array_equal(ro, r["row_offsets"]) and np.array_equal(co, r["columns"])
     assert np.array_equal(va, r["values"])
@@ -62,7 +74,7 @@ def test_pressure_assembly_bit_exact(ctx, ref, tet_setup):
     assert np.array_equal(grad, r["grad_p"])
 
 
-def test_pressure_assembly_nonzero_pressure_bit_exact(ctx, ref, tet_setup):
+def test_pressure_assembly_nonzero_pressure_bit_exact(ctx, oracle, tet_setup):
     # a later corrector: p != 0, so the gradient and deferred fluxes are active
     m, mesh, g, (U, rAU, aP, p, fixed, value) = tet_setup
     cc = g["cell_centres"].reshape(3, -1)
@@ -70,47 +82,48 @@ def test_pressure_assembly_nonzero_pressure_bit_exact(ctx, ref, tet_setup):
     value1 = value.copy()
     value1[0] = 0.25
     A, b, phi, grad = cg.assemble_pressure_correction(mesh, U, rAU, p1, 1.3, fixed, value1)
-    r = ref.simple_assemble(m, U, rAU, p1, 1.3, fixed, value1)
+    r = oracle.simple_assemble(m, U, rAU, p1, 1.3, fixed, value1)
     assert np.array_equal(A.to_csr()[2], r["values"])
     assert np.array_equal(b, r["b"])
     assert np.array_equal(grad, r["grad_p"])
     assert np.array_equal(cg.gauss_gradient_with_boundary(mesh, p1, fixed, value1),
-                          ref.gauss_gradient(m, p1, fixed, value1))
+                          oracle.gauss_gradient(m, p1, fixed, value1))
     assert np.array_equal(cg.make_rhie_chow_mass_flux(mesh, U, rAU, p1, 1.3, fixed, value1),
-                          ref.rhie_chow_flux(m, U, rAU, p1, 1.3, fixed, value1))
+                          oracle.rhie_chow_flux(m, U, rAU, p1, 1.3, fixed, value1))
 
 
-def test_spmv_bit_exact(ctx, ref, tet_setup):
+def test_spmv_bit_exact(ctx, oracle, tet_setup):
     m, mesh, g, (U, rAU, aP, p, fixed, value) = tet_setup
     A, b, phi, grad = cg.assemble_pressure_correction(mesh, U, rAU, p, 1.0, fixed, value)
     ro, co, va = A.to_csr()
     x = np.random.default_rng(3).standard_normal(A.n)
-    assert np.array_equal(A.matvec(x), ref.spmv(ro, co, va, x))
+    assert np.array_equal(A.matvec(x), oracle.spmv(ro, co, va, x))
 
 
-def test_vcycle_bit_exact(ctx, ref, tet_setup):
+def test_vcycle_bit_exact(ctx, oracle, tet_setup):
     m, mesh, g, (U, rAU, aP, p, fixed, value) = tet_setup
     A, b, phi, grad = cg.assemble_pressure_correction(mesh, U, rAU, p, 1.0, fixed, value)
-    ro, co, va = A.to_csr()
-    R = ref.Amg(ro, co, va)
     amg = cg.NativeBoomerAMGPreconditioner(ctx, reference_order=1)
     assert amg.setup(A)
+    H = oracle_hierarchy(oracle, amg)
     fast = cg.NativeBoomerAMGPreconditioner(ctx)
     assert fast.setup(A)
     for seed in (0, 1):
         r = np.random.default_rng(seed).standard_normal(A.n)
-        z_ref = R.apply(r)
+        z_ref = H.apply(r)
         assert np.array_equal(amg.apply(r), z_ref)
         # cooperative row reductions on the dense coarse levels: same cycle, other summation order
         assert rel_l2(fast.apply(r), z_ref) < 1e-12
 
 
-def test_poisson_solve_matches_reference(ctx, ref):
+def test_poisson_solve_matches_oracle(ctx, oracle):
     m, bc, src = cases.poisson_case(12)
     mesh = cg.Mesh(ctx, m)
     A, rhs = cg.assemble_cell_diffusion_matrix(mesh, bc, 1.0, src)
     ro, co, va = A.to_csr()
-    x_ref, rep_ref = ref.solve_linear_system(ro, co, va, rhs, restart=30, tolerance=1e-8)
+    amg = cg.NativeBoomerAMGPreconditioner(ctx)
+    assert amg.setup(A)
+    x_ref, rep_ref = oracle.solve_gmres(ro, co, va, rhs, oracle_hierarchy(oracle, amg), restart=30, tolerance=1e-8)
     x, rep = cg.solve_linear_system(A, rhs, krylov="gmres", preconditioner="native_amg", restart=30,
                                     tolerance=1e-8)
     assert rep["status_name"] == "converged" and rep_ref["status"] == 0
@@ -119,7 +132,51 @@ def test_poisson_solve_matches_reference(ctx, ref):
     assert rep["physical_residual_relative"] <= 1e-8
 
 
-def test_pressure_solve_and_flux_match_reference(ctx, ref, tet_setup):
+def test_pressure_solve_and_flux_match_oracle(ctx, oracle, tet_setup):
+    m, mesh, g, (U, rAU, aP, p, fixed, value) = tet_setup
+    A, b, phi, grad = cg.assemble_pressure_correction(mesh, U, rAU, p, 1.0, fixed, value)
+    ro, co, va = A.to_csr()
+    amg = cg.NativeBoomerAMGPreconditioner(ctx)
+    assert amg.setup(A)
+    x_ref, rep_ref = oracle.solve_gmres(ro, co, va, b, oracle_hierarchy(oracle, amg), restart=30, tolerance=1e-8)
+    x, rep = cg.solve_linear_system(A, b, restart=30, tolerance=1e-8)
+    assert rep["iterations"] == rep_ref["iterations"]
+    assert rel_l2(x, x_ref) <= REL_TOL
+    flux = cg.make_rhie_chow_mass_flux(mesh, U, rAU, x, 1.0, fixed, value)
+    flux_ref = oracle.rhie_chow_flux(m, U, rAU, x_ref, 1.0, fixed, value)
+    assert rel_l2(flux, flux_ref) <= REL_TOL
+
+
+def test_prepared_gmres_matches_oracle(ctx, oracle, tet_setup):
+    m, mesh, g, (U, rAU, aP, p, fixed, value) = tet_setup
+    A, b, phi, grad = cg.assemble_pressure_correction(mesh, U, rAU, p, 1.0, fixed, value)
+    ro, co, va = A.to_csr()
+    amg = cg.NativeBoomerAMGPreconditioner(ctx)
+    assert amg.setup(A)
+    x_ref, rep_ref = oracle.solve_gmres(ro, co, va, b, oracle_hierarchy(oracle, amg), restart=30, tolerance=1e-8)
+    x, rep = cg.solve_gmres(A, b, amg=amg, restart=30, tolerance=1e-8)
+    assert rep["status_name"] == "converged"
+    assert rep["iterations"] == rep_ref["iterations"]
+    assert rel_l2(x, x_ref) <= REL_TOL
+
+
+def test_golden_fixture_solve(ctx):
+    # the reference's own outputs for the 4^3 x 6 tet system (tests/golden/)
+    from pathlib import Path
+    z = dict(np.load(Path(__file__).resolve().parent / "golden" / "pressure_tet4.npz"))
+    m = cases.simple_mesh(int(z["n"]))
+    mesh = cg.Mesh(ctx, m)
+    U, rAU, aP, p, fixed, value = cases.simple_fields(m, mesh.geometry()["cell_centres"])
+    A, b, phi, grad = cg.assemble_pressure_correction(mesh, U, rAU, p, 1.0, fixed, value)
+    assert np.array_equal(A.to_csr()[2], z["values"]) and np.array_equal(b, z["b"])
+    x, rep = cg.solve_linear_system(A, b, restart=30, tolerance=1e-8)
+    assert rep["iterations"] == int(z["iterations"])
+    assert rel_l2(x, z["x"]) <= REL_TOL
+    assert rel_l2(cg.make_rhie_chow_mass_flux(mesh, U, rAU, x, 1.0, fixed, value), z["flux_solved"]) <= REL_TOL
+
+
+def test_pressure_solve_matches_reference_build(ctx, ref, tet_setup):
+    # the reference's own solve_linear_system (setup + GMRES), where its build is present
     m, mesh, g, (U, rAU, aP, p, fixed, value) = tet_setup
     A, b, phi, grad = cg.assemble_pressure_correction(mesh, U, rAU, p, 1.0, fixed, value)
     ro, co, va = A.to_csr()
@@ -127,35 +184,24 @@ def test_pressure_solve_and_flux_match_reference(ctx, ref, tet_setup):
     x, rep = cg.solve_linear_system(A, b, restart=30, tolerance=1e-8)
     assert rep["iterations"] == rep_ref["iterations"]
     assert rel_l2(x, x_ref) <= REL_TOL
-    flux = cg.make_rhie_chow_mass_flux(mesh, U, rAU, x, 1.0, fixed, value)
-    flux_ref = ref.rhie_chow_flux(m, U, rAU, x_ref, 1.0, fixed, value)
-    assert rel_l2(flux, flux_ref) <= REL_TOL
 
 
-def test_prepared_gmres_matches_reference(ctx, ref, tet_setup):
-    m, mesh, g, (U, rAU, aP, p, fixed, value) = tet_setup
-    A, b, phi, grad = cg.assemble_pressure_correction(mesh, U, rAU, p, 1.0, fixed, value)
-    ro, co, va = A.to_csr()
-    R = ref.Amg(ro, co, va)
-    x_ref, rep_ref = R.solve_gmres(b, restart=30, tolerance=1e-8)
-    amg = cg.NativeBoomerAMGPreconditioner(ctx)
-    assert amg.setup(A)
-    x, rep = cg.solve_gmres(A, b, amg=amg, restart=30, tolerance=1e-8)
-    assert rep["status_name"] == "converged"
-    assert rep["iterations"] == rep_ref["iterations"]
-    assert rel_l2(x, x_ref) <= REL_TOL
-
-
-def test_fp32_vcycle_solve_reaches_fp64_tolerance(ctx, ref, tet_setup):
+def test_fp32_vcycle_solve_reaches_fp64_tolerance(ctx, tet_setup):
     m, mesh, g, (U, rAU, aP, p, fixed, value) = tet_setup
     A, b, phi, grad = cg.assemble_pressure_correction(mesh, U, rAU, p, 1.0, fixed, value)
     x64, rep64 = cg.solve_linear_system(A, b, restart=30, tolerance=1e-8)
-    x32, rep32 = cg.solve_linear_system(A, b, krylov="fgmres", restart=30, precision="fp32_vcycle",
-                                        tolerance=1e-8)
+    x32, rep32 = cg.solve_linear_system(A, b, krylov="fgmres", restart=30, precision="fp32_vcycle", tolerance=1e-8)
     assert rep32["status_name"] == "converged"
     assert rep32["physical_residual_relative"] <= 1e-8
-    # error against the FP64 solution is stated and small
     assert rel_l2(x32, x64) < 1e-6
+    for cs in (6, 1, 0):   # the reference's V(6,6) everywhere, the default, fine-level-only smoothing
+        amg = cg.NativeBoomerAMGPreconditioner(ctx, precision="fp32_vcycle", coarse_sweeps=cs)
+        assert amg.setup(A)
+        x32, rep32 = cg.solve_fgmres(A, b, amg=amg, restart=30, tolerance=1e-8)
+        assert rep32["status_name"] == "converged"
+        assert rep32["physical_residual_relative"] <= 1e-8
+        # error against the FP64 solution is stated and small
+        assert rel_l2(x32, x64) < 1e-6
 
 
 def test_solve_is_deterministic(ctx, tet_setup):

@@ -109,3 +109,21 @@ def test_amg_setup_is_deterministic_across_thread_counts(ref, monkeypatch):
     for l in range(len(a.hierarchy_level_sizes())):
         la, lb = a.export_level(l), b.export_level(l)
         assert np.array_equal(la["values"], lb["values"])
+
+
+def test_host_setup_reproduces_golden_hierarchy():
+    # the reference's own hierarchy of the 4^3 x 6 tet pressure system, stored
+    # by tests/golden/make_golden.py: no reference build needed
+    from pathlib import Path
+    z = dict(np.load(Path(__file__).resolve().parent / "golden" / "pressure_tet4.npz"))
+    amg = cg.NativeBoomerAMGPreconditioner(None)
+    assert amg.setup_host(z["row_offsets"], z["columns"], z["values"]), amg.last_error()
+    assert len(amg.hierarchy_level_sizes()) == int(z["n_levels"])
+    for l in range(int(z["n_levels"])):
+        mine = amg.export_level(l)
+        for k in ("row_offsets", "columns", "values", "inv_diag"):
+            assert np.array_equal(mine[k], z[f"L{l}_{k}"]), (l, k)
+        if f"L{l}_p_offsets" in z:
+            for k in ("p_offsets", "p_columns", "p_values"):
+                assert np.array_equal(mine[k], z[f"L{l}_{k}"]), (l, k)
+    assert amg.omega == float(z["omega"])

@@ -1,0 +1,174 @@
+"""Pins the plain-C oracle (oracle/cfdx_oracle.c) to the reference itself.
+
+No GPU: the restatement must reproduce, bit for bit, what the reference's
+own code (compiled from its sources into oracle/_ref) computes -- geometry,
+Gauss gradient, pressure-corrector assembly, Rhie-Chow face flux, Poisson
+assembly, SpMV, one V-cycle on the reference's own hierarchy and a whole
+AMG-GMRES solve -- and, without the reference tree, the committed golden
+fixtures of tests/golden/ (made by tests/golden/make_golden.py from the
+reference build).
+"""
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+from oracle import cfdx_oracle as co
+from tests import cases
+
+GOLDEN = Path(__file__).resolve().parent / "golden"
+
+
+def _pressure_inputs(n, seed_offset=0):
+    m = cases.simple_mesh(n, seed_offset=seed_offset)
+    g = co.geometry(m)
+    U, rAU, aP, p, fixed, value = cases.simple_fields(m, g["cell_centres"], seed_offset=seed_offset)
+    return m, g, U, rAU, p, fixed, value
+
+
+@pytest.mark.parametrize("kind", ["hex", "tet", "bl"])
+def test_geometry_matches_reference(ref, kind):
+    import cfdx_dev_b200 as cg
+    m = {"hex": lambda: cases.poisson_case(5)[0], "tet": lambda: cases.simple_mesh(5),
+         "bl": lambda: cg.boundary_layer_case(6, 5, 4)}[kind]()
+    mine = co.geometry(m)
+    for which in ("fv", "cache"):   # build_fv_geometry and compute_geometry_cache agree
+        theirs = ref.geometry(m, which)
+        for k in mine:
+            assert np.array_equal(mine[k], theirs[k]), (which, k)
+
+
+@pytest.mark.parametrize("nonzero_p", [False, True])
+def test_pressure_assembly_and_flux_match_reference(ref, nonzero_p):
+    m, g, U, rAU, p, fixed, value = _pressure_inputs(6)
+    rho = 1.0
+    if nonzero_p:
+        cc = g["cell_centres"].reshape(3, -1)
+        p = np.sin(3 * cc[0]) + cc[1] * cc[2]
+        value = value.copy()
+        value[0] = 0.25
+        rho = 1.3
+    a = co.simple_assemble(m, U, rAU, p, rho, fixed, value)
+    b = ref.simple_assemble(m, U, rAU, p, rho, fixed, value)
+    for k in ("row_offsets", "columns", "values", "b", "phiHbyA", "grad_p"):
+        assert np.array_equal(a[k], b[k]), k
+    assert np.array_equal(co.gauss_gradient(m, p, fixed, value), ref.gauss_gradient(m, p, fixed, value))
+    assert np.array_equal(co.rhie_chow_flux(m, U, rAU, p, rho, fixed, value),
+                          ref.rhie_chow_flux(m, U, rAU, p, rho, fixed, value))
+
+
+def test_poisson_assembly_matches_reference(ref):
+    m, bc, src = cases.poisson_case(6)
+    ro, co_, va, rhs = co.assemble_diffusion(m, bc, 1.0, src)
+    r_ro, r_co, r_va, r_rhs, _ = ref.assemble_diffusion(m, bc, 1.0, src)
+    assert np.array_equal(ro, r_ro) and np.array_equal(co_, r_co)
+    assert np.array_equal(va, r_va) and np.array_equal(rhs, r_rhs)
+
+
+def test_spmv_vcycle_and_solve_match_reference(ref):
+    m, g, U, rAU, p, fixed, value = _pressure_inputs(7)
+    A = co.simple_assemble(m, U, rAU, p, 1.0, fixed, value)
+    ro, cols, va, b = A["row_offsets"], A["columns"], A["values"], A["b"]
+    x = np.random.default_rng(5).standard_normal(ro.size - 1)
+    assert np.array_equal(co.spmv(ro, cols, va, x), ref.spmv(ro, cols, va, x))
+    R = ref.Amg(ro, cols, va)
+    H = co.Hierarchy([R.level(l) for l in range(R.num_levels())], R.omega)
+    for seed in (0, 1):
+        r = np.random.default_rng(seed).standard_normal(ro.size - 1)
+        assert np.array_equal(H.apply(r), R.apply(r))
+    x_ref, rep_ref = R.solve_gmres(b, restart=30, tolerance=1e-8)
+    x_co, rep_co = co.solve_gmres(ro, cols, va, b, H, restart=30, tolerance=1e-8)
+    assert rep_co["status"] == rep_ref["status"] == 0
+    assert rep_co["iterations"] == rep_ref["iterations"]
+    assert np.array_equal(x_co, x_ref)
+
+
+def test_small_dense_coarsest_and_unpreconditioned_gmres(ref):
+    # 1-D Poisson (known-answer shape of the reference's GMRES tests): the
+    # hierarchy ends in a <= 16-row level, so the dense pivoted LU runs.
+    n = 40
+    rows, cols, vals = [], [], []
+    for i in range(n):
+        for j, v in ((i - 1, -1.0), (i, 2.0), (i + 1, -1.0)):
+            if 0 <= j < n:
+                rows.append(i); cols.append(j); vals.append(v)
+    cols = np.array(cols, np.int64)
+    vals = np.array(vals)
+    ro = np.concatenate([[0], np.cumsum(np.bincount(rows, minlength=n))]).astype(np.int64)
+    b = np.ones(n)
+    R = ref.Amg(ro, cols, vals)
+    levels = [R.level(l) for l in range(R.num_levels())]
+    assert levels[-1]["inv_diag"].size <= 16
+    H = co.Hierarchy(levels, R.omega)
+    r = np.random.default_rng(2).standard_normal(n)
+    assert np.array_equal(H.apply(r), R.apply(r))
+    x_co, rep = co.solve_gmres(ro, cols, vals, b, None, restart=30, tolerance=1e-10, max_iterations=200)
+    assert rep["status"] == 0
+    exact = np.array([(i + 1) * (n - i) / 2.0 for i in range(n)])
+    assert np.linalg.norm(x_co - exact) / np.linalg.norm(exact) < 1e-8
+
+
+def test_exact_3x3_gmres():
+    # the reference's exact 3x3 GMRES test shape: GMRES(3) is exact in 3 steps
+    ro = np.array([0, 2, 5, 7], np.int64)
+    cols = np.array([0, 1, 0, 1, 2, 1, 2], np.int64)
+    vals = np.array([4.0, 1.0, 1.0, 3.0, 1.0, 1.0, 2.0])
+    b = np.array([1.0, 2.0, 3.0])
+    x, rep = co.solve_gmres(ro, cols, vals, b, None, restart=3, tolerance=1e-12, max_iterations=10)
+    A = np.array([[4.0, 1.0, 0.0], [1.0, 3.0, 1.0], [0.0, 1.0, 2.0]])
+    assert rep["status"] == 0 and rep["iterations"] <= 3
+    assert np.allclose(A @ x, b, rtol=0, atol=1e-12)
+
+
+def test_zero_rhs_shifted_solve():
+    ro = np.array([0, 2, 5, 7], np.int64)
+    cols = np.array([0, 1, 0, 1, 2, 1, 2], np.int64)
+    vals = np.array([4.0, 1.0, 1.0, 3.0, 1.0, 1.0, 2.0])
+    x, rep = co.solve_gmres(ro, cols, vals, np.zeros(3), None, x0=np.array([1.0, -2.0, 0.5]), restart=3,
+                            tolerance=1e-12, max_iterations=10)
+    assert rep["status"] == 0
+    assert np.abs(x).max() < 1e-10
+
+
+def test_invalid_inputs_fail_loudly():
+    m = cases.simple_mesh(2)
+    bad = cases.simple_mesh(2)
+    bad.face_offsets = bad.face_offsets.copy()
+    bad.face_offsets[1] = bad.face_offsets[0] + 2   # a two-vertex face
+    with pytest.raises(RuntimeError):
+        co.geometry(bad)
+    x, rep = co.solve_gmres(np.array([0, 1], np.int64), np.array([0], np.int64), np.array([1.0]), np.ones(1),
+                            restart=0)
+    assert rep["status"] == 3
+    assert co.geometry(m)["cell_volumes"].min() > 0
+
+
+@pytest.mark.parametrize("name", sorted(p.stem for p in GOLDEN.glob("*.npz")))
+def test_oracle_reproduces_golden_fixtures(name):
+    z = dict(np.load(GOLDEN / f"{name}.npz"))
+    n = int(z["n"])
+    if name.startswith("pressure"):
+        m, g, U, rAU, p, fixed, value = _pressure_inputs(n)
+        a = co.simple_assemble(m, U, rAU, p, 1.0, fixed, value)
+        for k in ("row_offsets", "columns", "values", "b"):
+            assert np.array_equal(a[k], z[k]), k
+        assert np.array_equal(co.rhie_chow_flux(m, U, rAU, p, 1.0, fixed, value), z["flux"])
+        levels = []
+        for l in range(int(z["n_levels"])):
+            lv = {k: z[f"L{l}_{k}"] for k in ("row_offsets", "columns", "values", "inv_diag")}
+            if f"L{l}_p_offsets" in z:
+                lv.update({k: z[f"L{l}_{k}"] for k in ("p_offsets", "p_columns", "p_values")})
+            levels.append(lv)
+        H = co.Hierarchy(levels, float(z["omega"]))
+        assert np.array_equal(H.apply(z["vcycle_r"]), z["vcycle_z"])
+        x, rep = co.solve_gmres(a["row_offsets"], a["columns"], a["values"], a["b"], H, restart=30, tolerance=1e-8)
+        assert rep["iterations"] == int(z["iterations"])
+        assert np.array_equal(x, z["x"])
+        assert np.array_equal(co.rhie_chow_flux(m, U, rAU, x, 1.0, fixed, value), z["flux_solved"])
+    elif name.startswith("poisson"):
+        m, bc, src = cases.poisson_case(n)
+        ro, cols, va, rhs = co.assemble_diffusion(m, bc, 1.0, src)
+        for k, v in (("row_offsets", ro), ("columns", cols), ("values", va), ("rhs", rhs)):
+            assert np.array_equal(v, z[k]), k
+    else:
+        pytest.fail(f"unknown fixture {name}")
