@@ -480,6 +480,7 @@ extern "C" int cfdxg_request_default(cfdxg_request* r) {
     r->residual_replacement_gap_ratio = 10.0;
     r->target_reduction_per_cycle = 0.1;
     r->learned = nullptr;
+    r->learned_applications = 1;
     return CFDXG_OK;
 }
 
@@ -504,8 +505,13 @@ KrylovResult run_krylov(cfdxg_context* ctx, const cfdxg_matrix* A, cfdxg_amg* am
         state.last = est;
     };
     if (req.learned && amg) {
-        pc = [ctx, amg, A, &req, &state](const double* v, double* z) {
+        const int limit = req.learned_applications;
+        pc = [ctx, amg, A, &req, &state, limit](const double* v, double* z, int j) {
             auto vcycle = [ctx, amg](const double* r, double* zz) { amg_apply_device(ctx, amg, r, zz); };
+            if (limit > 0 && j >= limit) {   // the cycle's later Arnoldi vectors: the V-cycle alone
+                vcycle(v, z);
+                return true;
+            }
             if (!state.active) {
                 ++state.fallbacks;
                 vcycle(v, z);
@@ -514,12 +520,12 @@ KrylovResult run_krylov(cfdxg_context* ctx, const cfdxg_matrix* A, cfdxg_amg* am
             return learned_then_amg(ctx, req.learned, A, v, z, vcycle, nullptr);
         };
     } else if (amg) {
-        pc = [ctx, amg](const double* v, double* z) {
+        pc = [ctx, amg](const double* v, double* z, int) {
             amg_apply_device(ctx, amg, v, z);
             return true;
         };
     } else if (inv_diag) {
-        pc = [ctx, inv_diag, n](const double* v, double* z) {
+        pc = [ctx, inv_diag, n](const double* v, double* z, int) {
             k_scale<<<blocks_for(n, 256), 256, 0, ctx->stream>>>(n, inv_diag, v, z);
             check_launch(ctx);
             return true;
@@ -543,6 +549,7 @@ void validate_request(const cfdxg_request& r) {
         throw Error(CFDXG_ERR_INVALID_ARGUMENT, "unknown precision");
     if (r.learned && r.preconditioner != CFDXG_PC_NATIVE_AMG)
         throw Error(CFDXG_ERR_INVALID_ARGUMENT, "the learned preconditioner runs in front of native AMG");
+    if (r.learned_applications < 0) throw Error(CFDXG_ERR_INVALID_ARGUMENT, "learned_applications must be >= 0");
 }
 
 }  // namespace

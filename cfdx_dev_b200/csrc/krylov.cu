@@ -393,7 +393,7 @@ KrylovResult gmres_solve(cfdxg_context* ctx, const cfdxg_matrix* A, const double
 
         for (int j = 0; j < m && iterations < max_iter; ++j) {
             if (pc) {
-                if (!(*pc)(v(j), z(j))) return fail(CFDXG_NOT_APPLICABLE);
+                if (!(*pc)(v(j), z(j), j)) return fail(CFDXG_NOT_APPLICABLE);
                 ++result.preconditioner_applications;
             } else {
                 E.copy(z(j), v(j));

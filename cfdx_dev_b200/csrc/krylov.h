@@ -37,7 +37,9 @@ struct KrylovResult {
 
 // Enqueues z = M^-1 v on the context stream (device vectors); returns false
 // when it cannot run.  Non-finite results are reported through the status word.
-using RightPreconditioner = std::function<bool(const double* v, double* z)>;
+// z = M v for the j-th Arnoldi vector of the current restart cycle (j = 0: the
+// normalised true residual the cycle starts from).
+using RightPreconditioner = std::function<bool(const double* v, double* z, int j)>;
 
 // Called after every Arnoldi step with the Givens estimate of the residual norm.
 using IterationObserver = std::function<void(double estimated_residual)>;

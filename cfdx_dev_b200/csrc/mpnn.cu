@@ -52,6 +52,8 @@ struct cfdxg_mpnn {
     const cfdxg_matrix* A = nullptr;
     int n = 0;
     cfdxg::DevBuf<float> ew, feats;
+    cfdxg::DevBuf<int> gro, gco;   // off-diagonal couplings only (inference gather)
+    cfdxg::DevBuf<float> gew;
     cfdxg::DevBuf<double> diag;
     // work
     cfdxg::DevBuf<float> H, AG, Z, dh, dh2, dhself, da, hA, hB, dyf;
@@ -70,18 +72,31 @@ __device__ __forceinline__ float warp_sum(float v) {
     return v;
 }
 
-// x = [r/s, feats]; h0 = relu(W_in x + b_in).  One thread per (cell, feature).
+// x = [r/s, feats]; h0 = relu(W_in x + b_in).  Eight lanes per cell, each
+// lane four features (one 16-byte store); the group's first lane forms r/s.
 __global__ void k_encode(int n, const double* __restrict__ r, const double* __restrict__ rr,
                          const float* __restrict__ feats, const float* __restrict__ P, float* __restrict__ h) {
-    const int idx = blockIdx.x * blockDim.x + threadIdx.x;
-    if (idx >= n * F) return;
-    const int i = idx / F, f = idx % F;
-    const double s = sqrt(*rr / n);
-    const float x0 = s > 0.0 ? static_cast<float>(r[i] / s) : 0.0f;
+    const int64_t t = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    const int i = static_cast<int>(t >> 3), quarter = static_cast<int>(t & 7);
+    const unsigned grp_mask = 0xffu << (threadIdx.x & 24);
+    float x0 = 0.0f;
+    if (i < n && quarter == 0) {
+        const double s = sqrt(*rr / n);
+        x0 = s > 0.0 ? static_cast<float>(r[i] / s) : 0.0f;
+    }
+    x0 = __shfl_sync(grp_mask, x0, 0, 8);
+    if (i >= n) return;
+    const float fv = feats[i], fp = feats[n + i], fd = feats[2 * n + i];
     const float* W = P + OFF_WIN;
-    float pre = P[OFF_BIN + f] + W[f * 4 + 0] * x0 + W[f * 4 + 1] * feats[i] + W[f * 4 + 2] * feats[n + i] +
-                W[f * 4 + 3] * feats[2 * n + i];
-    h[idx] = fmaxf(pre, 0.0f);
+    float o[4];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+        const int f = 4 * quarter + q;
+        const float pre = P[OFF_BIN + f] + W[f * 4 + 0] * x0 + W[f * 4 + 1] * fv + W[f * 4 + 2] * fp +
+                          W[f * 4 + 3] * fd;
+        o[q] = fmaxf(pre, 0.0f);
+    }
+    reinterpret_cast<float4*>(h)[static_cast<size_t>(i) * (F / 4) + quarter] = make_float4(o[0], o[1], o[2], o[3]);
 }
 
 // a_i = sum_k ew[k] h[co[k]]  (ew = 0 on the diagonal).  Warp per cell, lane = feature.
@@ -117,15 +132,24 @@ __global__ void k_mlp_fwd(int n, const float* __restrict__ h, const float* __res
     }
 }
 
-// out_i = s (w_out . h_i + b_out) / a_ii
+// out_i = s (w_out . h_i + b_out) / a_ii.  Eight lanes per cell (16-byte loads),
+// combined with a fixed butterfly.
 __global__ void k_readout(int n, const float* __restrict__ h, const float* __restrict__ P, const double* rr,
                           const double* __restrict__ diag, double* __restrict__ out) {
-    const int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
-    if (w >= n) return;
-    const float y = warp_sum(P[OFF_WOUT + lane] * h[static_cast<size_t>(w) * F + lane]) + P[OFF_BOUT];
-    if (lane == 0) {
+    const int64_t t = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    const int i = static_cast<int>(t >> 3), quarter = static_cast<int>(t & 7);
+    const unsigned grp_mask = 0xffu << (threadIdx.x & 24);
+    float y = 0.0f;
+    if (i < n) {
+        const float4 v = reinterpret_cast<const float4*>(h)[static_cast<size_t>(i) * (F / 4) + quarter];
+        const float* w = P + OFF_WOUT + 4 * quarter;
+        y = w[0] * v.x + w[1] * v.y + w[2] * v.z + w[3] * v.w;
+    }
+#pragma unroll
+    for (int o = 4; o > 0; o >>= 1) y += __shfl_xor_sync(grp_mask, y, o, 8);
+    if (i < n && quarter == 0) {
         const double s = sqrt(*rr / n);
-        out[w] = s * static_cast<double>(y) / diag[w];
+        out[i] = s * static_cast<double>(y + P[OFF_BOUT]) / diag[i];
     }
 }
 
@@ -149,16 +173,78 @@ __device__ __forceinline__ uint32_t ld32(const __nv_bfloat16* p) { return *reint
 constexpr int kUPad = 2 * F + 8;   // 72 bf16 per row: 144 B, keeps 4-byte loads conflict-light
 constexpr int kW2Pad = F + 8;
 
-// h_out = h_in + W2 relu(W1 [h_in, gather(h_in)] + b1) + b2 for 16 cells per warp.
-__global__ void __launch_bounds__(kThreads) k_round_tc(int n, const int* __restrict__ ro, const int* __restrict__ co,
-                                                       const float* __restrict__ ew, const float* __restrict__ h_in,
-                                                       float* __restrict__ h_out,
-                                                       const __nv_bfloat16* __restrict__ W1g,
-                                                       const __nv_bfloat16* __restrict__ W2g,
-                                                       const float* __restrict__ Pr) {
+// Inference round, gather-optimised.  A warp owns 16 consecutive cells.  Their
+// off-diagonal couplings are one contiguous CSR segment, staged in shared
+// memory with coalesced loads; the gather then runs 8 lanes per cell (each
+// lane a 16-byte quarter-row of 4 features) over 4 cells at a time, with four
+// neighbour rows in flight per lane.  [h, a] goes to shared memory as BF16 for
+// the two tensor-core layers; the FP32 h stays in shared memory for the
+// residual update.
+constexpr int kTileCells = 16;
+constexpr int kSegCap = 128;           // staged couplings per 16-cell tile
+constexpr int kRoundWarps = 6;
+constexpr int kRoundThreads = 32 * kRoundWarps;
+
+// Gather of one 16-cell tile: sH = h (FP32), sU = [h, a] (BF16), a_i = sum_j w_ij h_j.
+// Lanes 8q..8q+7 take cell 4 * pass + q, each lane one 16-byte quarter-row.
+// STAGED: the tile's couplings are in sIdx / sW (index k - seg_b); otherwise
+// they are read from global memory.
+template <bool STAGED>
+__device__ __forceinline__ void gather_tile(int c0, int cells, int rb, int re, int seg_b, const int* sIdx,
+                                            const float* sW, const int* __restrict__ gco,
+                                            const float* __restrict__ gew, const float* __restrict__ h_in,
+                                            float (*sH)[F], __nv_bfloat16 (*sU)[kUPad]) {
+    const int lane = threadIdx.x & 31;
+    const float4* h4 = reinterpret_cast<const float4*>(h_in);
+    const int grp = lane >> 3, quarter = lane & 7;
+#pragma unroll 1
+    for (int pass = 0; pass < kTileCells / 4; ++pass) {
+        const int r = pass * 4 + grp;
+        const int b = __shfl_sync(0xffffffffu, rb, r), e = __shfl_sync(0xffffffffu, re, r);
+        float4 hv = make_float4(0.f, 0.f, 0.f, 0.f), av = make_float4(0.f, 0.f, 0.f, 0.f);
+        if (r < cells) hv = h4[static_cast<size_t>(c0 + r) * (F / 4) + quarter];
+        int k = b;
+        for (; k + 4 <= e; k += 4) {
+            int j[4];
+            float w[4];
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                j[u] = STAGED ? sIdx[k + u - seg_b] : gco[k + u];
+                w[u] = STAGED ? sW[k + u - seg_b] : gew[k + u];
+            }
+            float4 v[4];
+#pragma unroll
+            for (int u = 0; u < 4; ++u) v[u] = h4[static_cast<size_t>(j[u]) * (F / 4) + quarter];
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                av.x += w[u] * v[u].x; av.y += w[u] * v[u].y; av.z += w[u] * v[u].z; av.w += w[u] * v[u].w;
+            }
+        }
+        for (; k < e; ++k) {
+            const int j = STAGED ? sIdx[k - seg_b] : gco[k];
+            const float w = STAGED ? sW[k - seg_b] : gew[k];
+            const float4 v = h4[static_cast<size_t>(j) * (F / 4) + quarter];
+            av.x += w * v.x; av.y += w * v.y; av.z += w * v.z; av.w += w * v.w;
+        }
+        *reinterpret_cast<float4*>(&sH[r][4 * quarter]) = hv;
+        uint2 hp, ap;
+        hp.x = pack_bf16(hv.x, hv.y); hp.y = pack_bf16(hv.z, hv.w);
+        ap.x = pack_bf16(av.x, av.y); ap.y = pack_bf16(av.z, av.w);
+        *reinterpret_cast<uint2*>(&sU[r][4 * quarter]) = hp;
+        *reinterpret_cast<uint2*>(&sU[r][F + 4 * quarter]) = ap;
+    }
+}
+
+__global__ void __launch_bounds__(kRoundThreads) k_round_gather_tc(
+    int n, const int* __restrict__ gro, const int* __restrict__ gco, const float* __restrict__ gew,
+    const float* __restrict__ h_in, float* __restrict__ h_out, const __nv_bfloat16* __restrict__ W1g,
+    const __nv_bfloat16* __restrict__ W2g, const float* __restrict__ Pr) {
     __shared__ __align__(16) __nv_bfloat16 sW1[F][kUPad];
     __shared__ __align__(16) __nv_bfloat16 sW2[F][kW2Pad];
-    __shared__ __align__(16) __nv_bfloat16 sU[kWarps][16][kUPad];
+    __shared__ __align__(16) __nv_bfloat16 sU[kRoundWarps][kTileCells][kUPad];
+    __shared__ __align__(16) float sH[kRoundWarps][kTileCells][F];
+    __shared__ int sIdx[kRoundWarps][kSegCap];
+    __shared__ float sW[kRoundWarps][kSegCap];
     __shared__ float sb1[F], sb2[F];
     for (int q = threadIdx.x; q < F * 2 * F; q += blockDim.x) sW1[q / (2 * F)][q % (2 * F)] = W1g[q];
     for (int q = threadIdx.x; q < F * F; q += blockDim.x) sW2[q / F][q % F] = W2g[q];
@@ -168,34 +254,25 @@ __global__ void __launch_bounds__(kThreads) k_round_tc(int n, const int* __restr
     }
     __syncthreads();
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int c0 = (blockIdx.x * kWarps + warp) * 16;
+    const int c0 = (blockIdx.x * kRoundWarps + warp) * kTileCells;
     if (c0 >= n) return;
-    // Row ranges of the 16 cells are loaded once by lanes 0..15; each cell's
-    // (<= 32) neighbour indices and weights by one lane each, then broadcast,
-    // so the feature rows of a cell are fetched with independent loads.
-    int rb = 0, re = 0;
-    if (lane < 16 && c0 + lane < n) {
-        rb = ro[c0 + lane];
-        re = ro[c0 + lane + 1];
-    }
-#pragma unroll 2
-    for (int r = 0; r < 16; ++r) {
-        const int c = c0 + r;
-        const int b = __shfl_sync(0xffffffffu, rb, r), e = __shfl_sync(0xffffffffu, re, r);
-        const int len = min(e - b, 32);
-        const int cj = lane < len ? co[b + lane] : 0;
-        const float wj = lane < len ? ew[b + lane] : 0.0f;
-        float hv = c < n ? h_in[static_cast<size_t>(c) * F + lane] : 0.0f;
-        float av = 0.0f;
-        for (int q = 0; q < len; ++q) {
-            const int j = __shfl_sync(0xffffffffu, cj, q);
-            const float w = __shfl_sync(0xffffffffu, wj, q);
-            av += w * h_in[static_cast<size_t>(j) * F + lane];
+    const int cells = min(kTileCells, n - c0);
+    // tile segment of the coupling list
+    const int seg_b = gro[c0], seg_e = gro[c0 + cells];
+    const bool staged = seg_e - seg_b <= kSegCap;
+    if (staged)
+        for (int q = lane; q < seg_e - seg_b; q += 32) {
+            sIdx[warp][q] = gco[seg_b + q];
+            sW[warp][q] = gew[seg_b + q];
         }
-        for (int k = b + 32; k < e; ++k) av += ew[k] * h_in[static_cast<size_t>(co[k]) * F + lane];
-        sU[warp][r][lane] = __float2bfloat16_rn(hv);
-        sU[warp][r][F + lane] = __float2bfloat16_rn(av);
+    int rb = 0, re = 0;   // lanes 0..15: row range of cell c0 + lane
+    if (lane < cells) {
+        rb = gro[c0 + lane];
+        re = gro[c0 + lane + 1];
     }
+    __syncwarp();
+    if (staged) gather_tile<true>(c0, cells, rb, re, seg_b, sIdx[warp], sW[warp], gco, gew, h_in, sH[warp], sU[warp]);
+    else gather_tile<false>(c0, cells, rb, re, seg_b, sIdx[warp], sW[warp], gco, gew, h_in, sH[warp], sU[warp]);
     __syncwarp();
     const int g = lane >> 2, t = lane & 3;
     float acc[4][4];
@@ -219,7 +296,6 @@ __global__ void __launch_bounds__(kThreads) k_round_tc(int n, const int* __restr
             mma_bf16(acc[j], a0, a1, a2, a3, b0, b1);
         }
     }
-    // ReLU, and the accumulators become the A operand of the second layer
     uint32_t A2[2][4];
 #pragma unroll
     for (int kk = 0; kk < 2; ++kk) {
@@ -228,15 +304,14 @@ __global__ void __launch_bounds__(kThreads) k_round_tc(int n, const int* __restr
         A2[kk][2] = pack_bf16(fmaxf(acc[2 * kk + 1][0], 0.f), fmaxf(acc[2 * kk + 1][1], 0.f));
         A2[kk][3] = pack_bf16(fmaxf(acc[2 * kk + 1][2], 0.f), fmaxf(acc[2 * kk + 1][3], 0.f));
     }
-    const int rowa = c0 + g, rowb = c0 + g + 8;
     float out[4][4];
 #pragma unroll
     for (int j = 0; j < 4; ++j) {
         const int col = 8 * j + 2 * t;
-        out[j][0] = sb2[col] + (rowa < n ? h_in[static_cast<size_t>(rowa) * F + col] : 0.f);
-        out[j][1] = sb2[col + 1] + (rowa < n ? h_in[static_cast<size_t>(rowa) * F + col + 1] : 0.f);
-        out[j][2] = sb2[col] + (rowb < n ? h_in[static_cast<size_t>(rowb) * F + col] : 0.f);
-        out[j][3] = sb2[col + 1] + (rowb < n ? h_in[static_cast<size_t>(rowb) * F + col + 1] : 0.f);
+        out[j][0] = sb2[col] + sH[warp][g][col];
+        out[j][1] = sb2[col + 1] + sH[warp][g][col + 1];
+        out[j][2] = sb2[col] + sH[warp][g + 8][col];
+        out[j][3] = sb2[col + 1] + sH[warp][g + 8][col + 1];
     }
 #pragma unroll
     for (int kk = 0; kk < 2; ++kk) {
@@ -247,17 +322,14 @@ __global__ void __launch_bounds__(kThreads) k_round_tc(int n, const int* __restr
             mma_bf16(out[j], A2[kk][0], A2[kk][1], A2[kk][2], A2[kk][3], b0, b1);
         }
     }
+    const int rowa = g, rowb = g + 8;
 #pragma unroll
     for (int j = 0; j < 4; ++j) {
         const int col = 8 * j + 2 * t;
-        if (rowa < n) {
-            h_out[static_cast<size_t>(rowa) * F + col] = out[j][0];
-            h_out[static_cast<size_t>(rowa) * F + col + 1] = out[j][1];
-        }
-        if (rowb < n) {
-            h_out[static_cast<size_t>(rowb) * F + col] = out[j][2];
-            h_out[static_cast<size_t>(rowb) * F + col + 1] = out[j][3];
-        }
+        if (rowa < cells)
+            *reinterpret_cast<float2*>(&h_out[static_cast<size_t>(c0 + rowa) * F + col]) = make_float2(out[j][0], out[j][1]);
+        if (rowb < cells)
+            *reinterpret_cast<float2*>(&h_out[static_cast<size_t>(c0 + rowb) * F + col]) = make_float2(out[j][2], out[j][3]);
     }
 }
 
@@ -467,12 +539,6 @@ void upload_params(cfdxg_context* ctx, cfdxg_mpnn* net) {
     CFDXG_CUDA(cudaStreamSynchronize(ctx->stream));
 }
 
-void sync_host_params(cfdxg_context* ctx, cfdxg_mpnn* net) {
-    net->host.resize(NP);
-    net->params.download(net->host.data(), ctx->stream);
-    CFDXG_CUDA(cudaStreamSynchronize(ctx->stream));
-}
-
 double* scalar(cfdxg_context* ctx, int k) { return ctx->scratch.scalars + 3000 + k; }
 
 // Inference: out = N(r) (tensor-core rounds).
@@ -481,21 +547,28 @@ void infer(cfdxg_context* ctx, cfdxg_mpnn* net, const double* r, double* out) {
     cudaStream_t s = ctx->stream;
     double* rr = scalar(ctx, 0);
     enqueue_dot(ctx, n, r, r, rr);
-    k_encode<<<blocks_for(static_cast<int64_t>(n) * F, 256), 256, 0, s>>>(n, r, rr, net->feats.get(),
-                                                                          net->params.get(), net->hA.get());
-    check_launch(ctx);
+    {
+        ProfScope ps(ctx, "mpnn_encode", (8.0 + 12.0 + 4.0 * F) * n);
+        k_encode<<<blocks_for(static_cast<int64_t>(n) * 8, 256), 256, 0, s>>>(n, r, rr, net->feats.get(),
+                                                                              net->params.get(), net->hA.get());
+        check_launch(ctx);
+    }
     float* hin = net->hA.get();
     float* hout = net->hB.get();
-    const int tiles = (n + 15) / 16;
+    const int tiles = (n + kTileCells - 1) / kTileCells;
     for (int k = 0; k < R; ++k) {
         const __nv_bfloat16* w = net->wbf.get() + static_cast<size_t>(k) * 3 * F * F;
-        k_round_tc<<<(tiles + kWarps - 1) / kWarps, kThreads, 0, s>>>(
-            n, net->A->ro.get(), net->A->co.get(), net->ew.get(), hin, hout, w, w + 2 * F * F,
+        // compulsory bytes: h read and written once, the coupling list once
+        ProfScope ps(ctx, "mpnn_round_gather_tc",
+                     2.0 * sizeof(float) * F * n + 4.0 * (n + 1) + 8.0 * static_cast<double>(net->gco.size()));
+        k_round_gather_tc<<<(tiles + kRoundWarps - 1) / kRoundWarps, kRoundThreads, 0, s>>>(
+            n, net->gro.get(), net->gco.get(), net->gew.get(), hin, hout, w, w + 2 * F * F,
             net->params.get() + ROUND0 + k * ROUND_SIZE);
         check_launch(ctx);
         std::swap(hin, hout);
     }
-    k_readout<<<blocks_for(static_cast<int64_t>(n) * 32, 256), 256, 0, s>>>(n, hin, net->params.get(), rr,
+    ProfScope ps(ctx, "mpnn_readout", (4.0 * F + 16.0) * n);
+    k_readout<<<blocks_for(static_cast<int64_t>(n) * 8, 256), 256, 0, s>>>(n, hin, net->params.get(), rr,
                                                                             net->diag.get(), out);
     check_launch(ctx);
 }
@@ -506,7 +579,7 @@ void forward_train(cfdxg_context* ctx, cfdxg_mpnn* net, const double* r, double*
     cudaStream_t s = ctx->stream;
     const size_t st = static_cast<size_t>(n) * F;
     enqueue_dot(ctx, n, r, r, rr);
-    k_encode<<<blocks_for(static_cast<int64_t>(n) * F, 256), 256, 0, s>>>(n, r, rr, net->feats.get(),
+    k_encode<<<blocks_for(static_cast<int64_t>(n) * 8, 256), 256, 0, s>>>(n, r, rr, net->feats.get(),
                                                                           net->params.get(), net->H.get());
     check_launch(ctx);
     for (int k = 0; k < R; ++k) {
@@ -518,7 +591,7 @@ void forward_train(cfdxg_context* ctx, cfdxg_mpnn* net, const double* r, double*
                                                    net->H.get() + (k + 1) * st);
         check_launch(ctx);
     }
-    k_readout<<<blocks_for(static_cast<int64_t>(n) * 32, 256), 256, 0, s>>>(n, net->H.get() + R * st,
+    k_readout<<<blocks_for(static_cast<int64_t>(n) * 8, 256), 256, 0, s>>>(n, net->H.get() + R * st,
                                                                             net->params.get(), rr, net->diag.get(), out);
     check_launch(ctx);
 }
@@ -782,6 +855,21 @@ extern "C" int cfdxg_mpnn_bind(cfdxg_context* ctx, cfdxg_mpnn* net, cfdxg_mesh* 
     standardise(ap, 1);
     standardise(diag, 2);
     net->ew.upload(ew, ctx->stream);
+    std::vector<int> gro(n + 1, 0), gco;
+    std::vector<float> gew;
+    gco.reserve(H.co.size());
+    gew.reserve(H.co.size());
+    for (int64_t i = 0; i < n; ++i) {
+        for (uint32_t k = H.ro[i]; k < H.ro[i + 1]; ++k)
+            if (H.co[k] != i) {
+                gco.push_back(static_cast<int>(H.co[k]));
+                gew.push_back(ew[k]);
+            }
+        gro[i + 1] = static_cast<int>(gco.size());
+    }
+    net->gro.upload(gro, ctx->stream);
+    net->gco.upload(gco, ctx->stream);
+    net->gew.upload(gew, ctx->stream);
     net->feats.upload(feats, ctx->stream);
     net->diag.upload(diag, ctx->stream);
     const size_t st = static_cast<size_t>(n) * mp::F;

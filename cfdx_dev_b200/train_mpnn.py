@@ -6,7 +6,10 @@ generates: on seeded Kuhn-tet meshes of lattice sizes between --min-n and
 pressure-correction system is assembled, and for each residual r the error
 e = A^-1 r is obtained with plain FP64 AMG-GMRES to a relative residual of
 1e-10.  Residuals mix the assembled continuity right-hand sides (other HbyA
-seeds), white noise, and smooth fields mapped through A.  The loss is the
+seeds), white noise, and smooth fields mapped through A; half of them are then
+advanced 1..--richardson-steps steps of the V-cycle-preconditioned Richardson
+iteration (the error is updated exactly alongside), which leaves the slowly
+converging components the learned stage is meant to remove.  The loss is the
 A-norm of the error of the composed preconditioner z = N(r) + M(r - A N(r))
 with M the FP32 AMG V-cycle, ||(I - M A)(e - N(r))||_A^2 / ||(I - M A) e||_A^2
 (below 1 when the learned stage improves on the V-cycle alone), minimised with
@@ -49,8 +52,13 @@ def make_system(ctx, n, seed):
     return dict(m=m, mesh=mesh, g=g, aP=aP, rAU=rAU, fixed=fixed, value=value, A=A)
 
 
-def make_pairs(ctx, sysd, k, seed):
-    """k (r, e) pairs; e solved with the plain FP64 AMG-GMRES path."""
+def make_pairs(ctx, sysd, k, seed, richardson_steps=0):
+    """k (r, e) pairs; e solved with the plain FP64 AMG-GMRES path.
+
+    With richardson_steps > 0, the second half of the pairs are carried
+    1..richardson_steps steps of the preconditioned Richardson iteration with
+    the FP32 V-cycle M (e <- e - M r, r <- A e): the residuals the Krylov
+    solver meets after the V-cycle has removed what it handles well."""
     A, m, g = sysd["A"], sysd["m"], sysd["g"]
     amg = cg.NativeBoomerAMGPreconditioner(ctx)
     if not amg.setup(A):
@@ -76,6 +84,12 @@ def make_pairs(ctx, sysd, k, seed):
         e, rep = cg.solve_gmres(A, r, amg=amg, restart=30, tolerance=1e-10, max_iterations=2000)
         if rep["status_name"] != "converged":
             raise RuntimeError(f"training pair solve failed: {rep}")
+        if richardson_steps and q >= k // 2:
+            for _ in range(1 + q % richardson_steps):
+                e = e - sysd["vcycle"].apply(r)
+                r = A.matvec(e)
+            scale = 1.0 / np.sqrt(np.mean(r * r))
+            r, e = r * scale, e * scale
         R.append(r)
         E.append(e)
     return np.array(R), np.array(E)
@@ -89,7 +103,7 @@ def train(args):
     t0 = time.time()
     for i, n in enumerate(sizes):
         sysd = make_system(ctx, int(n), i)
-        R, E = make_pairs(ctx, sysd, args.pairs_per_mesh, i)
+        R, E = make_pairs(ctx, sysd, args.pairs_per_mesh, i, args.richardson_steps)
         data.append((sysd, R, E))
         print(f"mesh {i} n={n} cells={sysd['m'].n_cells} pairs={len(R)} ({time.time() - t0:.1f}s)", flush=True)
     gen_s = time.time() - t0
@@ -127,6 +141,8 @@ def main(argv=None):
     ap.add_argument("--batch", type=int, default=8)
     ap.add_argument("--lr", type=float, default=2e-3)
     ap.add_argument("--seed", type=int, default=0)
+    ap.add_argument("--richardson-steps", type=int, default=4,
+                    help="carry half of the pairs up to this many V-cycle Richardson steps (0: off)")
     ap.add_argument("--composed", type=int, default=1,
                     help="1: loss of the learned stage in front of the FP32 V-cycle; 0: the network alone")
     ap.add_argument("--out", type=Path, default=ROOT / "cfdx_dev_b200" / "weights" / "mpnn.bin")

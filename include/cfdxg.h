@@ -277,6 +277,9 @@ typedef struct {
     double residual_replacement_gap_ratio; /* 10 */
     double target_reduction_per_cycle;     /* 0.1 */
     cfdxg_mpnn* learned;             /* NULL, or a trained network applied before the V-cycle */
+    int32_t learned_applications;    /* the learned stage serves the first this-many Arnoldi
+                                        vectors of each restart cycle (the V-cycle alone the
+                                        rest); 0: every application.  Default 1. */
 } cfdxg_request;
 
 /* Mirrors SolverResult (core/linalg/solver_status.h:45-72) + LinearSolveReport. */

@@ -7,9 +7,13 @@ and the reference oracle see identical arrays.
 """
 from __future__ import annotations
 
+from pathlib import Path
+
 import numpy as np
 
 import cfdx_dev_b200 as cg
+
+ROOT = Path(__file__).resolve().parents[1]
 
 SEED_MESH = 20240601
 SEED_HBYA = 20240602
