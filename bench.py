@@ -58,6 +58,7 @@ def parse_args():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-learned", action="store_true", help="skip the learned+FP32 form")
+    ap.add_argument("--no-assembly", action="store_true", help="skip the face-loop timing")
     return ap.parse_args()
 
 
@@ -172,6 +173,7 @@ def run_cfdxg(args):
         A, b, phi, grad = cg.assemble_pressure_correction(mesh, U, base_rAU, p, 1.0, fixed, value, matrix=A)
         if k == 0:
             base_aP = aP
+            base_fields = (U, rAU, p, fixed, value)
         rhs_list.append(b)
     case_s = time.time() - t0
     n_cells = A.n
@@ -265,6 +267,11 @@ def run_cfdxg(args):
     for form in forms:
         forms[form]["speedup_vs_plain_fp64"] = forms["plain_fp64"]["s_per_solve"] / forms[form]["s_per_solve"]
 
+    # ---- the face loop: pressure-corrector assembly and Rhie-Chow face flux ----
+    assembly = None
+    if not args.no_assembly:
+        assembly = time_face_loop(ctx, lib, N, mesh, A, base_fields, dev, lstream, flush, args)
+
     # ---- end to end through the C ABI with pinned host buffers ----
     e2e = None
     if not args.no_e2e:
@@ -338,6 +345,7 @@ def run_cfdxg(args):
                        "parallelism": f"replicas x{world}"},
             "forms": forms, "case_build_s": case_s,
             "e2e": e2e, "gpu_launches": int(launches), "clocks": clocks, "roofline": roofline,
+            "assembly": assembly,
             "kernels": kernels, "cpu_baseline": cpu,
         }
         print(json.dumps(result), flush=True)
@@ -345,6 +353,67 @@ def run_cfdxg(args):
         torch.distributed.barrier()
         torch.distributed.destroy_process_group()
     return result
+
+
+def time_face_loop(ctx, lib, N, mesh, A, fields, dev, lstream, flush, args):
+    """Device time of the pressure-corrector assembly (Gauss gradient + face loop
+    writing the CSR values, b and phiHbyA) and of the Rhie-Chow face flux, inputs
+    resident on the device, L2 flushed before each call; per-kernel achieved
+    bandwidth from the library's profiler (CUDA events on its stream)."""
+    import torch
+    U, rAU, p, fixed, value = fields
+    nc, nf = A.n, mesh.host.n_faces
+    Ud, rd, pd = (torch.from_numpy(np.ascontiguousarray(a)).to(dev) for a in (U, rAU, p))
+    bd = torch.empty(nc, dtype=torch.float64, device=dev)
+    phid = torch.empty(nf, dtype=torch.float64, device=dev)
+    gd = torch.empty(3 * nc, dtype=torch.float64, device=dev)
+    fl = torch.empty(nf, dtype=torch.float64, device=dev)
+    fx = np.ascontiguousarray(fixed, np.int32)
+    vv = np.ascontiguousarray(value, np.float64)
+    h = C.c_void_p(A.handle.value)
+    ptr = lambda t: C.c_void_p(t.data_ptr())
+
+    def assemble():
+        ctx.check(lib.cfdxg_assemble_pressure_correction(ctx.handle, mesh.handle, ptr(Ud), ptr(rd), ptr(pd), 1.0,
+                                                         N.ptr(fx), N.ptr(vv), N.CFDXG_MEM_DEVICE, C.byref(h),
+                                                         ptr(bd), ptr(phid), ptr(gd)), "assembly")
+
+    def flux():
+        ctx.check(lib.cfdxg_rhie_chow_flux(ctx.handle, mesh.handle, ptr(Ud), ptr(rd), ptr(pd), 1.0, N.ptr(fx),
+                                           N.ptr(vv), N.CFDXG_MEM_DEVICE, ptr(fl)), "rhie-chow flux")
+
+    out = {}
+    for name, fn in (("assembly", assemble), ("rhie_chow_flux", flux)):
+        for _ in range(args.warmup):
+            fn()
+        ctx.profile(True)
+        ts = []
+        for s in range(args.steps):
+            flush.fill_(float(s))
+            torch.cuda.synchronize()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(lstream)
+            fn()
+            e1.record(lstream)
+            torch.cuda.synchronize()
+            ts.append(e0.elapsed_time(e1))
+        prof = ctx.profile_read()
+        ctx.profile(False)
+        out[f"{name}_ms"] = float(np.mean(ts))
+        for e in prof:
+            if e["total_ms"] > 0:
+                gbs = e["bytes"] / (e["total_ms"] / 1e3) / 1e9
+                out.setdefault("kernels", {})[e["name"]] = {
+                    "launches": e["launches"], "ms_per_launch": e["total_ms"] / e["launches"],
+                    "bytes_per_launch": e["bytes"] / e["launches"], "achieved_gbs": round(gbs, 1)}
+    peak, kind = measured_peak()
+    for v in out.get("kernels", {}).values():
+        v["frac"] = round(v["achieved_gbs"] / peak, 3)
+    out["peak_gbs"] = peak
+    out["peak_kind"] = kind
+    out["workload"] = f"{nc} cells, {nf} faces, {A.nnz} nonzeros"
+    return out
 
 
 def _export_levels(amg):

@@ -66,6 +66,10 @@ struct cfdxg_mesh {
     bool geometry_ready = false;
     cfdxg::DevBuf<double> face_centre, face_sf, cell_centre, cell_volume;
     cfdxg::MeshPattern pattern;
+    // per-call boundary table and gradient scratch, kept so the face-loop entry
+    // points neither allocate nor free device memory after their first call
+    cfdxg::DevBuf<int> bc_fixed;
+    cfdxg::DevBuf<double> bc_value, grad_scratch;
     // host copies needed by the pattern build
     std::vector<int64_t> h_owner, h_neigh, h_cell_off, h_cell_face;
     std::vector<int32_t> h_patch_types;

@@ -61,8 +61,23 @@ __device__ __forceinline__ T row_dot(int b, int e, int lane, const int* __restri
 #pragma unroll 4
     for (int k = b + lane; k < e; k += TPR) s += va[k] * __ldg(x + co[k]);
     if (TPR > 1) {
+        constexpr int W = TPR < 32 ? TPR : 32;
 #pragma unroll
-        for (int o = TPR / 2; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o, TPR);
+        for (int o = W / 2; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o, W);
+    }
+    if constexpr (TPR > 32) {
+        // rows spread over TPR / 32 warps of the block (levels with few, long
+        // rows): warp partials summed in warp order by the row's first thread
+        __shared__ T part[kT / 32];
+        const int warp = threadIdx.x >> 5;
+        if ((threadIdx.x & 31) == 0) part[warp] = s;
+        __syncthreads();
+        if (lane == 0) {
+            T t = part[warp];
+#pragma unroll
+            for (int q = 1; q < TPR / 32; ++q) t += part[warp + q];
+            s = t;
+        }
     }
     return s;
 }
@@ -272,7 +287,10 @@ __global__ void k_gj_init(int n, const int* ro, const int* co, const double* va,
         case 4: { constexpr int TPR = 4; __VA_ARGS__; } break;   \
         case 8: { constexpr int TPR = 8; __VA_ARGS__; } break;   \
         case 16: { constexpr int TPR = 16; __VA_ARGS__; } break; \
-        default: { constexpr int TPR = 32; __VA_ARGS__; } break; \
+        case 32: { constexpr int TPR = 32; __VA_ARGS__; } break; \
+        case 64: { constexpr int TPR = 64; __VA_ARGS__; } break; \
+        case 128: { constexpr int TPR = 128; __VA_ARGS__; } break; \
+        default: { constexpr int TPR = 256; __VA_ARGS__; } break; \
     }
 
 // Algorithmic (compulsory) bytes of one launch; accumulated into the graph
@@ -336,7 +354,12 @@ int choose_tpr(int64_t nnz, int64_t rows, bool reference_order) {
     if (avg < 24) return 4;
     if (avg < 48) return 8;
     if (avg < 96) return 16;
-    return 32;
+    // long rows: a warp per row, or several warps per row when the level has
+    // too few rows to fill the GPU (148 SMs x 2048 threads), keeping at least
+    // eight entries per thread
+    int tpr = 32;
+    while (tpr < 256 && static_cast<double>(rows) * tpr < 148.0 * 2048.0 && avg >= 8.0 * 2 * tpr) tpr *= 2;
+    return tpr;
 }
 
 template <class T>
