@@ -30,6 +30,7 @@ struct DevLevel {
     T* xout = nullptr;   // where the level's result lives after enqueue
     int tpr = 1;         // threads cooperating on one row of A (1 = reference order)
     int tpr_r = 1;       // threads cooperating on one row of P^T
+    int tpr_p = 1;       // threads cooperating on one row of P (prolongation)
 };
 
 template <class T>

@@ -50,8 +50,10 @@ __global__ void k_sweep_zero(int n, T omega, const T* __restrict__ inv_diag, con
 // sequentially in CSR order (the reference's order).  TPR > 1 gives each
 // thread the entries k = lane, lane + TPR, ... and combines the partial sums
 // with a fixed xor butterfly, so results are deterministic run to run.
-// (A variant reading 16-byte chunks of four entries per lane measured ~5%
-// slower on the tet hierarchies: the loop is latency-bound, not issue-bound.)
+// Measured alternatives that were slower on the 64^3 tet hierarchy: 16-byte
+// chunks of four entries per lane (~5%), eight lanes per short row with the
+// sum formed in order through shuffles (~4x), and a sliced-ELL copy of the
+// fine level (32-row slices, column-major; ~10%).
 template <class T, int TPR>
 __device__ __forceinline__ T row_dot(int b, int e, int lane, const int* __restrict__ co,
                                      const T* __restrict__ va, const T* __restrict__ x) {
@@ -121,17 +123,30 @@ __global__ void k_restrict(int nc, const int* __restrict__ r_off, const int* __r
     if (valid && lane == 0) rc[c] = s;
 }
 
-template <class T>
+// x += P xc.  TPR == 1 adds the entries to x one by one in P's row order (the
+// reference's order); TPR > 1 forms the row sum cooperatively (deterministic
+// butterfly, as row_dot) and adds it once.
+template <class T, int TPR>
 __global__ void k_prolong(int n, const int* __restrict__ p_off, const int* __restrict__ p_col,
                           const T* __restrict__ p_val, const T* __restrict__ xc, T* __restrict__ x,
                           int* status) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    T v = x[i];
-    const int e = p_off[i + 1];
-    for (int q = p_off[i]; q < e; ++q) v += p_val[q] * __ldg(xc + p_col[q]);
-    x[i] = v;
-    if (!finite_(v)) atomicOr(status, kStatusNonFinite);
+    const int g = blockIdx.x * blockDim.x + threadIdx.x;
+    const int i = g / TPR, lane = g % TPR;
+    if constexpr (TPR == 1) {
+        if (i >= n) return;
+        T v = x[i];
+        const int e = p_off[i + 1];
+        for (int q = p_off[i]; q < e; ++q) v += p_val[q] * __ldg(xc + p_col[q]);
+        x[i] = v;
+        if (!finite_(v)) atomicOr(status, kStatusNonFinite);
+    } else {
+        const bool valid = i < n;
+        const T s = row_dot<T, TPR>(valid ? p_off[i] : 0, valid ? p_off[i + 1] : 0, lane, p_col, p_val, xc);
+        if (!valid || lane != 0) return;
+        const T v = x[i] + s;
+        x[i] = v;
+        if (!finite_(v)) atomicOr(status, kStatusNonFinite);
+    }
 }
 
 template <class T, class XO>
@@ -342,8 +357,9 @@ void launch_prolong(cfdxg_context* ctx, const DevLevel<T>& L, const T* xc, T* x,
     const double pnnz = static_cast<double>(L.p_col.size());
     const double bytes = account((sizeof(T) + 4.0) * pnnz + 4.0 * (L.n + 1) + sizeof(T) * (L.nc + 2.0 * L.n));
     ProfScope ps(ctx, tname<T>("prolong_fp64_L0", "prolong_fp32_L0"), bytes);
-    k_prolong<T><<<blocks_for(L.n, kT), kT, 0, ctx->stream>>>(L.n, L.p_off.get(), L.p_col.get(), L.p_val.get(),
-                                                               xc, x, status);
+    const int64_t threads = static_cast<int64_t>(L.n) * L.tpr_p;
+    CFDXG_TPR_SWITCH(L.tpr_p, (k_prolong<T, TPR><<<blocks_for(threads, kT), kT, 0, ctx->stream>>>(
+        L.n, L.p_off.get(), L.p_col.get(), L.p_val.get(), xc, x, status)));
     check_launch(ctx);
 }
 
@@ -362,11 +378,23 @@ int choose_tpr(int64_t nnz, int64_t rows, bool reference_order) {
     return tpr;
 }
 
+// Transfer operators (rows of P or P^T): as choose_tpr, then more threads per
+// row while the level has too few rows to fill the GPU (ragged rows on the deep
+// levels otherwise leave a few threads walking long rows alone).
+int choose_transfer_tpr(int64_t nnz, int64_t rows, bool reference_order) {
+    int tpr = choose_tpr(nnz, rows, reference_order);
+    if (reference_order) return tpr;
+    tpr = std::min(tpr, 32);
+    while (tpr < 32 && static_cast<double>(rows) * tpr < 148.0 * 1024.0) tpr *= 2;
+    return tpr;
+}
+
 template <class T>
 void upload_level_values(cfdxg_context* ctx, DevLevel<T>& D, const AmgLevel& H) {
     std::vector<T> tmp(H.A.va.size());
     for (std::size_t k = 0; k < tmp.size(); ++k) tmp[k] = static_cast<T>(H.A.va[k]);
     D.va.upload(tmp, ctx->stream);
+
     std::vector<T> d(H.inv_diag.size());
     for (std::size_t k = 0; k < d.size(); ++k) d[k] = static_cast<T>(H.inv_diag[k]);
     D.inv_diag.upload(d, ctx->stream);
@@ -391,7 +419,8 @@ void upload_level(cfdxg_context* ctx, DevLevel<T>& D, const AmgLevel& H, bool wi
         for (const uint32_t c : H.p_col) nc = std::max<int>(nc, static_cast<int>(c) + 1);
         nc = std::max<int>(nc, static_cast<int>(H.plan.n_coarse));
         D.nc = nc;
-        D.tpr_r = choose_tpr(static_cast<int64_t>(H.p_col.size()), nc, reference_order);
+        D.tpr_r = choose_transfer_tpr(static_cast<int64_t>(H.p_col.size()), nc, reference_order);
+        D.tpr_p = choose_transfer_tpr(static_cast<int64_t>(H.p_col.size()), n, reference_order);
         std::vector<int> po(H.p_off.begin(), H.p_off.end()), pc(H.p_col.begin(), H.p_col.end());
         std::vector<T> pv(H.p_val.size());
         for (std::size_t q = 0; q < pv.size(); ++q) pv[q] = static_cast<T>(H.p_val[q]);
