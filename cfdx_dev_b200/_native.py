@@ -111,6 +111,7 @@ PROTOTYPES = {
     "cfdxg_amg_create": (C.c_int, [_V, _P(AmgOptions), _P(_V)]),
     "cfdxg_amg_destroy": (C.c_int, [_V]),
     "cfdxg_amg_setup": (C.c_int, [_V, _V, _V]),
+    "cfdxg_amg_update_values_host": (C.c_int, [C.c_void_p, C.c_int64, C.c_void_p, C.c_void_p, C.c_void_p]),
     "cfdxg_amg_setup_host": (C.c_int, [_V, C.c_int64, _V, _V, _V]),
     "cfdxg_amg_update_values": (C.c_int, [_V, _V, _V]),
     "cfdxg_amg_apply": (C.c_int, [_V, _V, _V, _V, C.c_int32]),

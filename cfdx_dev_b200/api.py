@@ -388,10 +388,21 @@ class NativeBoomerAMGPreconditioner:
         return True
 
     def update_values(self, A: SparseMatrix) -> bool:
+        """Numeric refresh on an unchanged pattern, computed on the device."""
         rc = self.lib.cfdxg_amg_update_values(self.ctx.handle, self.handle, A.handle)
         if rc == -3:
             return False
         self.ctx.check(rc, "AMG update_values")
+        return True
+
+    def update_values_host(self, row_offsets, columns, values) -> bool:
+        """Numeric refresh of a setup_host hierarchy on the host."""
+        ro, co, va = _i64(row_offsets), _i64(columns), _f64(values)
+        rc = self.lib.cfdxg_amg_update_values_host(self.handle, ro.size - 1, N.ptr(ro), N.ptr(co), N.ptr(va))
+        if rc == -3:
+            return False
+        if rc != 0:
+            raise CfdxgError(rc, self.last_error())
         return True
 
     def apply(self, r) -> np.ndarray:

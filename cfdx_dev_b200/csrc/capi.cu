@@ -93,6 +93,9 @@ void amg_setup_impl(cfdxg_context* ctx, cfdxg_amg* amg, cfdxg_matrix* A) {
     amg->host = std::move(staged);
     amg->d64 = std::move(d64);
     amg->d32 = std::move(d32);
+    amg->refresh.reset();
+    amg->host_values_stale = false;
+    amg->ctx = ctx;
     amg->ready = true;
     amg->error.clear();
     amg->setup_seconds = now_seconds() - t0;
@@ -343,18 +346,59 @@ extern "C" int cfdxg_amg_update_values(cfdxg_context* ctx, cfdxg_amg* amg, const
         throw Error(CFDXG_ERR_NOT_READY, amg->error);
     }
     const double t0 = now_seconds();
-    auto* M = const_cast<cfdxg_matrix*>(A);
-    matrix_sync_host_values(ctx, M);
     std::string err;
-    if (!amg_update_values(amg->host, M->host, err)) {
-        amg->error = err;
-        throw Error(CFDXG_ERR_SETUP, err);
+    if (amg->d64 || amg->d32) {
+        // Galerkin refresh on the device, bit-identical to the host restatement
+        if (!amg_refresh_device(ctx, amg, A, err)) {
+            amg->error = err;
+            throw Error(CFDXG_ERR_SETUP, err);
+        }
+    } else {
+        auto* M = const_cast<cfdxg_matrix*>(A);
+        matrix_sync_host_values(ctx, M);
+        if (!amg_update_values(amg->host, M->host, err)) {
+            amg->error = err;
+            throw Error(CFDXG_ERR_SETUP, err);
+        }
     }
-    if (amg->d32) refresh_hierarchy_values<float>(ctx, *amg->d32, amg->host);
-    if (amg->d64) refresh_hierarchy_values<double>(ctx, *amg->d64, amg->host);
     amg->setup_seconds = now_seconds() - t0;
     amg->error.clear();
     ctx->error.clear();
+    return CFDXG_OK;
+    CFDXG_GUARD_END(ctx)
+}
+
+extern "C" int cfdxg_amg_update_values_host(cfdxg_amg* amg, int64_t n, const int64_t* ro, const int64_t* co,
+                                            const double* va) {
+    if (!amg || n <= 0 || !ro || !co || !va) return CFDXG_ERR_INVALID_ARGUMENT;
+    cfdxg_context* ctx = nullptr;
+    CFDXG_GUARD_BEGIN
+    if (!amg->ready) {
+        amg->error = "native AMG numeric update requires an existing compatible hierarchy";
+        throw Error(CFDXG_ERR_NOT_READY, amg->error);
+    }
+    if (amg->d64 || amg->d32)
+        throw Error(CFDXG_ERR_INVALID_ARGUMENT, "the hierarchy lives on a device: use cfdxg_amg_update_values");
+    const double t0 = now_seconds();
+    HostCsr A;
+    A.n = n;
+    const int64_t nnz = ro[n];
+    if (ro[0] != 0 || nnz <= 0 || nnz > INT32_MAX) throw Error(CFDXG_ERR_INVALID_ARGUMENT, "invalid row offsets");
+    A.ro.resize(n + 1);
+    A.co.resize(nnz);
+    A.va.assign(va, va + nnz);
+    for (int64_t i = 0; i <= n; ++i) A.ro[i] = static_cast<uint32_t>(ro[i]);
+    for (int64_t k = 0; k < nnz; ++k) {
+        if (co[k] < 0 || co[k] >= n) throw Error(CFDXG_ERR_INVALID_ARGUMENT, "column out of range");
+        A.co[k] = static_cast<uint32_t>(co[k]);
+    }
+    std::string err;
+    if (!amg_update_values(amg->host, A, err)) {
+        amg->error = err;
+        throw Error(CFDXG_ERR_SETUP, err);
+    }
+    amg->setup_seconds = now_seconds() - t0;
+    amg->error.clear();
     return CFDXG_OK;
     CFDXG_GUARD_END(ctx)
 }
@@ -420,6 +464,9 @@ extern "C" int cfdxg_amg_setup_host(cfdxg_amg* amg, int64_t n, const int64_t* ro
     amg->host = std::move(staged);
     amg->d64.reset();
     amg->d32.reset();
+    amg->refresh.reset();
+    amg->host_values_stale = false;
+    amg->ctx = nullptr;
     amg->ready = true;
     amg->error.clear();
     amg->setup_seconds = now_seconds() - t0;
@@ -452,6 +499,13 @@ extern "C" int cfdxg_amg_export_level(const cfdxg_amg* amg, int32_t level, int64
                                       double* inv_diag, int64_t* po, int64_t* pc, double* pv, int64_t* aggregate) {
     if (!amg || !amg->ready || level < 0 || level >= static_cast<int32_t>(amg->host.levels.size()))
         return CFDXG_ERR_INVALID_ARGUMENT;
+    if (amg->host_values_stale) {   // values refreshed on the device since setup
+        try {
+            amg_sync_host_values(amg->ctx, const_cast<cfdxg_amg*>(amg));
+        } catch (const std::exception&) {
+            return CFDXG_ERR_CUDA;
+        }
+    }
     const auto& L = amg->host.levels[level];
     if (ro) for (std::size_t i = 0; i < L.A.ro.size(); ++i) ro[i] = L.A.ro[i];
     if (co) for (std::size_t k = 0; k < L.A.co.size(); ++k) co[k] = L.A.co[k];

@@ -86,6 +86,25 @@ struct cfdxg_matrix {
     const cfdxg_mesh* mesh = nullptr;   // set when assembled from a mesh pattern
 };
 
+namespace cfdxg {
+// FP64 device copy of the hierarchy's numeric state and of the symbolic
+// Galerkin plans, for the numeric refresh on the GPU (galerkin.cu).
+struct DevRefreshLevel {
+    int n = 0, n_coarse = 0;
+    int64_t nnz = 0;
+    DevBuf<int> ro, co;                       // this level's CSR pattern
+    DevBuf<double> va, inv_diag;              // this level's values (FP64)
+    DevBuf<int> p_off, p_col;                 // P to the next level
+    DevBuf<double> p_val;
+    DevBuf<int> ap_off, ap_col, c_off, c_col, t_off, t_row, t_pos, keep_pos;
+    DevBuf<double> ap, cv;
+};
+struct DevRefresh {
+    std::vector<DevRefreshLevel> L;
+    DevBuf<double> bounds;                    // per-level normalised Gershgorin bound
+};
+}  // namespace cfdxg
+
 struct cfdxg_amg {
     cfdxg_amg_options opts{};
     cfdxg::AmgHierarchy host;
@@ -95,9 +114,25 @@ struct cfdxg_amg {
     std::unique_ptr<cfdxg::DevHierarchy<double>> d64;
     std::unique_ptr<cfdxg::DevHierarchy<float>> d32;
     int64_t applications = 0;
+    // numeric refresh on the device; the host mirror of the level values is
+    // then stale until amg_sync_host_values
+    std::unique_ptr<cfdxg::DevRefresh> refresh;
+    bool host_values_stale = false;
+    cfdxg_context* ctx = nullptr;   // context the device hierarchy lives on
 };
 
 namespace cfdxg {
+
+// numeric refresh of the hierarchy on the device (galerkin.cu): the
+// reference's update_values (amg_preconditioner.h:245-314) with the Galerkin
+// products, pruning check, inverse diagonals and damping computed in its
+// order on the GPU; false (hierarchy unchanged) when the pruned pattern or a
+// diagonal no longer qualifies
+bool amg_refresh_device(cfdxg_context* ctx, cfdxg_amg* amg, const cfdxg_matrix* A, std::string& error);
+// copies refreshed level values and inverse diagonals back to the host mirror
+void amg_sync_host_values(cfdxg_context* ctx, cfdxg_amg* amg);
+template <class T>
+void set_hierarchy_values_device(cfdxg_context* ctx, DevHierarchy<T>& d, const DevRefresh& R, double omega);
 
 // matrix helpers (matrix.cu)
 void matrix_sync_host_values(cfdxg_context* ctx, cfdxg_matrix* A);

@@ -442,17 +442,15 @@ void upload_level(cfdxg_context* ctx, DevLevel<T>& D, const AmgLevel& H, bool wi
     }
 }
 
+// FP64 Gauss-Jordan inverse of the dense coarse level from its device CSR.
 template <class T>
-void build_dense_inverse(cfdxg_context* ctx, DevHierarchy<T>& d, const AmgLevel& H) {
-    const int n = static_cast<int>(H.A.n);
-    DevBuf<int> ro, co;
-    DevBuf<double> va, a, f;
-    std::vector<int> hro(H.A.ro.begin(), H.A.ro.end()), hco(H.A.co.begin(), H.A.co.end());
-    ro.upload(hro, ctx->stream); co.upload(hco, ctx->stream); va.upload(H.A.va, ctx->stream);
+void build_dense_inverse_dev(cfdxg_context* ctx, DevHierarchy<T>& d, int n, const int* ro, const int* co,
+                             const double* va) {
+    DevBuf<double> a, f;
     a.resize(static_cast<std::size_t>(n) * 2 * n);
     f.resize(n);
     d.dense.resize(static_cast<std::size_t>(n) * n);
-    k_gj_init<<<blocks_for(n, kT), kT, 0, ctx->stream>>>(n, ro.get(), co.get(), va.get(), a.get());
+    k_gj_init<<<blocks_for(n, kT), kT, 0, ctx->stream>>>(n, ro, co, va, a.get());
     check_launch(ctx);
     const size_t total = static_cast<size_t>(n) * 2 * n;
     const int eb = static_cast<int>((total + kT - 1) / kT);
@@ -465,6 +463,16 @@ void build_dense_inverse(cfdxg_context* ctx, DevHierarchy<T>& d, const AmgLevel&
     k_gj_extract<<<blocks_for(static_cast<int64_t>(n) * n, kT), kT, 0, ctx->stream>>>(n, a.get(), d.dense.get());
     check_launch(ctx);
     CFDXG_CUDA(cudaStreamSynchronize(ctx->stream));
+}
+
+template <class T>
+void build_dense_inverse(cfdxg_context* ctx, DevHierarchy<T>& d, const AmgLevel& H) {
+    const int n = static_cast<int>(H.A.n);
+    DevBuf<int> ro, co;
+    DevBuf<double> va;
+    std::vector<int> hro(H.A.ro.begin(), H.A.ro.end()), hco(H.A.co.begin(), H.A.co.end());
+    ro.upload(hro, ctx->stream); co.upload(hco, ctx->stream); va.upload(H.A.va, ctx->stream);
+    build_dense_inverse_dev(ctx, d, n, ro.get(), co.get(), va.get());
 }
 
 template <class T>
@@ -597,6 +605,42 @@ void refresh_hierarchy_values(cfdxg_context* ctx, DevHierarchy<T>& d, const AmgH
 }
 
 template <class T>
+__global__ void k_cast_values(int64_t n, const double* __restrict__ a, T* __restrict__ b) {
+    const int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i < n) b[i] = static_cast<T>(a[i]);
+}
+
+template <class T>
+void copy_or_cast(cfdxg_context* ctx, const double* src, T* dst, int64_t n) {
+    if (n <= 0) return;
+    if (std::is_same<T, double>::value) {
+        CFDXG_CUDA(cudaMemcpyAsync(dst, src, sizeof(double) * n, cudaMemcpyDeviceToDevice, ctx->stream));
+    } else {
+        k_cast_values<T><<<blocks_for(n, kT), kT, 0, ctx->stream>>>(n, src, dst);
+        check_launch(ctx);
+    }
+}
+
+// New level values, inverse diagonals and damping from the device refresh
+// (the transfer operators and every pattern are unchanged).
+template <class T>
+void set_hierarchy_values_device(cfdxg_context* ctx, DevHierarchy<T>& d, const DevRefresh& R, double omega) {
+    d.omega = static_cast<T>(omega);
+    for (int l = 0; l < d.used; ++l) {
+        copy_or_cast<T>(ctx, R.L[l].va.get(), d.L[l].va.get(), R.L[l].nnz);
+        copy_or_cast<T>(ctx, R.L[l].inv_diag.get(), d.L[l].inv_diag.get(), R.L[l].n);
+    }
+    if (d.coarse_mode == 2) {
+        const DevRefreshLevel& C = R.L[d.used - 1];
+        build_dense_inverse_dev(ctx, d, C.n, C.ro.get(), C.co.get(), C.va.get());
+    }
+    // omega is a kernel argument baked into the graph: recapture
+    if (d.exec) { cudaGraphExecDestroy(d.exec); d.exec = nullptr; }
+    if (d.graph) { cudaGraphDestroy(d.graph); d.graph = nullptr; }
+    CFDXG_CUDA(cudaStreamSynchronize(ctx->stream));
+}
+
+template <class T>
 void vcycle_apply(cfdxg_context* ctx, DevHierarchy<T>& d, const double* r, double* z) {
     cudaStream_t s = ctx->stream;
     DevLevel<T>& L = d.L[0];
@@ -667,6 +711,8 @@ template std::unique_ptr<DevHierarchy<double>> upload_hierarchy<double>(cfdxg_co
 template std::unique_ptr<DevHierarchy<float>> upload_hierarchy<float>(cfdxg_context*, const AmgHierarchy&, int, bool);
 template void refresh_hierarchy_values<double>(cfdxg_context*, DevHierarchy<double>&, const AmgHierarchy&);
 template void refresh_hierarchy_values<float>(cfdxg_context*, DevHierarchy<float>&, const AmgHierarchy&);
+template void set_hierarchy_values_device<double>(cfdxg_context*, DevHierarchy<double>&, const DevRefresh&, double);
+template void set_hierarchy_values_device<float>(cfdxg_context*, DevHierarchy<float>&, const DevRefresh&, double);
 template void vcycle_apply<double>(cfdxg_context*, DevHierarchy<double>&, const double*, double*);
 template void vcycle_apply<float>(cfdxg_context*, DevHierarchy<float>&, const double*, double*);
 template void destroy_hierarchy<double>(DevHierarchy<double>*);

@@ -1,0 +1,83 @@
+"""A small, self-contained workload for kernel profilers (ncu).
+
+Builds the seeded Kuhn-tet pressure-correction system of an n^3 lattice
+(6 tets per hex cell, interior vertices jittered by +-0.15h; divergence-free
+Fourier HbyA, log-uniform a_P on [1, 100], p = 0 fixed on the x = 0 patch),
+sets up the AMG hierarchy and runs each hot-path kernel a few times:
+
+  * ``vcycle``: three V-cycle applications (``--precision fp32_vcycle|fp64``);
+  * ``solve``: one FGMRES(30) solve to 1e-8 with the FP32 V-cycle, two
+    applications of the learned stage (when trained weights are present) and
+    the Rhie-Chow face flux of the solution.
+
+Example (one kernel, one launch, at 663,552 cells):
+
+    ncu --set full --clock-control none --kernel-name-base demangled \\
+        -k 'regex:k_sweep<float, float, \\(int\\)1>' -s 1 -c 1 -o sweep \\
+        python -m cfdx_dev_b200.profile_case --n 48 --mode solve
+"""
+from __future__ import annotations
+
+import argparse
+import sys
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parents[1]
+if str(ROOT) not in sys.path:
+    sys.path.insert(0, str(ROOT))
+
+import cfdx_dev_b200 as cg  # noqa: E402
+
+SEED_MESH, SEED_HBYA, SEED_AP = 20240601, 20240602, 20240603
+WEIGHTS = Path(__file__).resolve().parent / "weights" / "mpnn.bin"
+
+
+def build_system(ctx, n):
+    m = cg.tet_case(n, 0.15, SEED_MESH)
+    mesh = cg.Mesh(ctx, m)
+    g = mesh.geometry()
+    U = cg.fourier_field(g["cell_centres"], 8, 0.01, SEED_HBYA)
+    aP = cg.random_field(m.n_cells, "loguniform", 1.0, 100.0, SEED_AP)
+    rAU = np.concatenate([1.0 / aP] * 3)
+    p = np.zeros(m.n_cells)
+    fixed = np.zeros(m.n_patches, np.int32)
+    fixed[0] = 1
+    value = np.zeros(m.n_patches)
+    A, b, phi, grad = cg.assemble_pressure_correction(mesh, U, rAU, p, 1.0, fixed, value)
+    return m, mesh, (U, rAU, aP, p, fixed, value), A, b
+
+
+def main(argv=None):
+    ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
+    ap.add_argument("--n", type=int, default=48, help="lattice size (cells = 6 n^3)")
+    ap.add_argument("--mode", choices=["vcycle", "solve"], default="solve")
+    ap.add_argument("--precision", choices=["fp32_vcycle", "fp64"], default="fp32_vcycle")
+    args = ap.parse_args(argv)
+    ctx = cg.Context(0)
+    m, mesh, (U, rAU, aP, p, fixed, value), A, b = build_system(ctx, args.n)
+    amg = cg.NativeBoomerAMGPreconditioner(ctx, precision=args.precision)
+    if not amg.setup(A):
+        raise SystemExit(amg.last_error())
+    if args.mode == "vcycle":
+        for _ in range(3):
+            z = amg.apply(b)
+        print(f"vcycle n={args.n} cells={A.n} levels={amg.hierarchy_level_sizes()} |z|={np.linalg.norm(z):.6e}")
+        return
+    x, rep = cg.solve_fgmres(A, b, amg=amg, restart=30, tolerance=1e-8)
+    if rep["status_name"] != "converged":
+        raise SystemExit(f"solve did not converge: {rep}")
+    if WEIGHTS.exists():
+        net = cg.LearnedPreconditioner(ctx)
+        net.load(WEIGHTS)
+        net.bind(mesh, A, aP)
+        for _ in range(2):
+            y = net.apply(b)
+    flux = cg.make_rhie_chow_mass_flux(mesh, U, rAU, x, 1.0, fixed, value)
+    print(f"solve n={args.n} cells={A.n} iterations={rep['iterations']} |flux|={np.linalg.norm(flux):.6e}")
+    ctx.close()
+
+
+if __name__ == "__main__":
+    main()

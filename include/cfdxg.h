@@ -233,7 +233,12 @@ int cfdxg_amg_create(cfdxg_context* ctx, const cfdxg_amg_options* opts, cfdxg_am
 int cfdxg_amg_destroy(cfdxg_amg* amg);
 /* Preconditioner::setup (core/linalg/preconditioner.h:22) */
 int cfdxg_amg_setup(cfdxg_context* ctx, cfdxg_amg* amg, const cfdxg_matrix* A);
-/* Preconditioner::update_values (preconditioner.h:26) -- unchanged pattern only */
+/* Preconditioner::update_values (preconditioner.h:26; hypre_amg.cpp:238-281,
+ * amg_preconditioner.h:245-314) -- unchanged pattern only.  The Galerkin
+ * products, inverse diagonals and damping are recomputed on the device in the
+ * reference's order (bit-identical to the host restatement); on failure
+ * (pruned coarse pattern changed, zero diagonal) the hierarchy is unchanged
+ * and the status is CFDXG_ERR_SETUP, as the reference's returns false. */
 int cfdxg_amg_update_values(cfdxg_context* ctx, cfdxg_amg* amg, const cfdxg_matrix* A);
 /* Preconditioner::apply (preconditioner.h:27): z = one V-cycle applied to r */
 int cfdxg_amg_apply(cfdxg_context* ctx, cfdxg_amg* amg, const double* r, double* z, int32_t mem);
@@ -257,6 +262,10 @@ double cfdxg_amg_setup_seconds(const cfdxg_amg* amg);
  * be exported from but not applied. */
 int cfdxg_amg_setup_host(cfdxg_amg* amg, int64_t n, const int64_t* row_offsets,
                          const int64_t* columns, const double* values);
+/* Host-only numeric refresh of a cfdxg_amg_setup_host hierarchy
+ * (amg_preconditioner.h:245-314 update_values): same pattern, new values. */
+int cfdxg_amg_update_values_host(cfdxg_amg* amg, int64_t n, const int64_t* row_offsets,
+                                 const int64_t* columns, const double* values);
 
 /* ------------------------------------------------------------------------ */
 /* Krylov solves                                                             */

@@ -244,6 +244,16 @@ class Amg:
             out.update(p_offsets=None, p_columns=np.empty(0, np.int64), p_values=np.empty(0), aggregate=None)
         return out
 
+    def update_values(self, ro, co, va) -> bool:
+        ro, co, va = (np.ascontiguousarray(ro, np.int64), np.ascontiguousarray(co, np.int64),
+                      np.ascontiguousarray(va, np.float64))
+        f = lib().ref_amg_update_values
+        f.argtypes = [C.c_void_p, C.c_int64, C.c_void_p, C.c_void_p, C.c_void_p]
+        rc = _check(f(self.h, ro.size - 1, _p(ro), _p(co), _p(va)), "update_values")
+        if rc == 0:
+            self.ro, self.co, self.va = ro, co, va
+        return rc == 0
+
     def apply(self, r):
         r = np.ascontiguousarray(r, np.float64)
         z = np.empty_like(r)

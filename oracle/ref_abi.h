@@ -99,6 +99,9 @@ void* ref_amg_create_from_levels(int32_t n_levels, const int64_t* n_rows,
                                  const int64_t* const* p_offsets, const int64_t* const* p_columns,
                                  const double* const* p_values, double omega);
 void ref_amg_destroy(void* h);
+/* core/linalg/amg_preconditioner.h:245  update_values (same pattern, new values); 1 = refused */
+int ref_amg_update_values(void* h, int64_t n, const int64_t* row_offsets, const int64_t* columns,
+                          const double* values);
 int32_t ref_amg_num_levels(void* h);
 double ref_amg_omega(void* h);
 int ref_amg_level_sizes(void* h, int32_t level, int64_t* n_rows, int64_t* nnz, int64_t* p_nnz);

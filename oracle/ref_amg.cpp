@@ -123,6 +123,25 @@ extern "C" void* ref_amg_create_from_levels(int32_t n_levels, const int64_t* n_r
     }
 }
 
+// MatrixFreeVcyclePreconditioner::update_values (amg_preconditioner.h:245-314)
+// on the owned operator's matrix replaced by the new values (same pattern).
+extern "C" int ref_amg_update_values(void* hv, int64_t n, const int64_t* ro, const int64_t* co,
+                                     const double* va) {
+    try {
+        auto* h = static_cast<AmgHandle*>(hv);
+        h->op->matrix_ = cfdx_ref::make_csr(n, ro, co, va);
+        if (!h->amg->update_values(h->op->matrix_)) {
+            cfdx_ref::g_error = "AMG update_values failed";
+            return 1;
+        }
+        cfdx_ref::g_error.clear();
+        return 0;
+    } catch (const std::exception& e) {
+        cfdx_ref::set_error(e);
+        return -1;
+    }
+}
+
 extern "C" void ref_amg_destroy(void* h) { delete static_cast<AmgHandle*>(h); }
 
 extern "C" int32_t ref_amg_num_levels(void* h) {

@@ -222,3 +222,55 @@ def test_zero_rhs_and_invalid_requests(ctx, tet_setup):
     amg = cg.NativeBoomerAMGPreconditioner(ctx)
     with pytest.raises(cg.CfdxgError):
         amg.apply(b)   # not set up
+
+
+def test_device_numeric_refresh_bit_exact(ctx, oracle):
+    """update_values on the device (Galerkin products, inverse diagonals,
+    damping) against the host restatement, itself pinned to the reference's
+    update_values by the CPU tests."""
+    m = cases.simple_mesh(10)
+    mesh = cg.Mesh(ctx, m)
+    g = mesh.geometry()
+    systems = []
+    A = None
+    for off in (0, 11):
+        U, rAU, aP, p, fixed, value = cases.simple_fields(m, g["cell_centres"], seed_offset=off)
+        A, b, phi, grad = cg.assemble_pressure_correction(mesh, U, rAU, p, 1.0, fixed, value, matrix=A)
+        systems.append((A.to_csr(), b))
+        if off == 0:
+            dev = cg.NativeBoomerAMGPreconditioner(ctx, reference_order=1)
+            assert dev.setup(A)
+            dev32 = cg.NativeBoomerAMGPreconditioner(ctx, precision="fp32_vcycle")
+            assert dev32.setup(A)
+    (ro, co, va1), b1 = systems[0]
+    (_, _, va2), b2 = systems[1]
+    host = cg.NativeBoomerAMGPreconditioner(None)
+    assert host.setup_host(ro, co, va1)
+    assert host.update_values_host(ro, co, va2)
+    assert dev.update_values(A) and dev32.update_values(A)
+    for amg in (dev, dev32):
+        assert amg.omega == host.omega
+        for l in range(len(host.hierarchy_level_sizes())):
+            a, b = host.export_level(l), amg.export_level(l)
+            for k in ("values", "inv_diag"):
+                assert np.array_equal(a[k], b[k]), (l, k)
+    H = oracle.Hierarchy([host.export_level(l) for l in range(len(host.hierarchy_level_sizes()))], host.omega)
+    r = np.random.default_rng(9).standard_normal(A.n)
+    assert np.array_equal(dev.apply(r), H.apply(r))
+    x, rep = cg.solve_fgmres(A, b2, amg=dev32, restart=30, tolerance=1e-8)
+    assert rep["status_name"] == "converged" and rep["physical_residual_relative"] <= 1e-8
+
+
+def test_simple_outer_iterations_small(ctx):
+    """Five SIMPLE outer iterations on a small anisotropic boundary-layer mesh:
+    every pressure solve converges after the device numeric refresh and the
+    continuity defect falls."""
+    from cfdx_dev_b200 import simple_loop as sl
+    m = cg.boundary_layer_case(24, 24, 8, 10.0, 1.0, 1e-4, 1.08, 0.05, sl.SEED)
+    mesh = cg.Mesh(ctx, m)
+    g = mesh.geometry()
+    nu_t = sl.smoothed_eddy_ratio(m, sl.SEED + 2)
+    for form in ("plain_fp64", "fp32_vcycle"):
+        out = sl.run_form(ctx, form, m, mesh, g, nu_t, 5, 0.3, None, ctx.synchronize)
+        assert all(r["status"] == "converged" for r in out["records"])
+        assert out["final_continuity_l2"] < out["first_continuity_l2"]

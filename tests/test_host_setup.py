@@ -127,3 +127,37 @@ def test_host_setup_reproduces_golden_hierarchy():
             for k in ("p_offsets", "p_columns", "p_values"):
                 assert np.array_equal(mine[k], z[f"L{l}_{k}"]), (l, k)
     assert amg.omega == float(z["omega"])
+
+
+def _pressure_pair(n):
+    """Two pressure-correction systems on one mesh (same pattern, other a_P)."""
+    from oracle import cfdx_oracle as co
+    m = cases.simple_mesh(n)
+    g = co.geometry(m)
+    out = []
+    for off in (0, 11):
+        U, rAU, aP, p, fixed, value = cases.simple_fields(m, g["cell_centres"], seed_offset=off)
+        a = co.simple_assemble(m, U, rAU, p, 1.0, fixed, value)
+        out.append((a["row_offsets"], a["columns"], a["values"]))
+    assert np.array_equal(out[0][0], out[1][0]) and np.array_equal(out[0][1], out[1][1])
+    return out
+
+
+def test_host_numeric_refresh_matches_reference(ref):
+    (ro, co_, va1), (_, _, va2) = _pressure_pair(8)
+    R = ref.Amg(ro, co_, va1)
+    assert R.update_values(ro, co_, va2)
+    amg = cg.NativeBoomerAMGPreconditioner(None)
+    assert amg.setup_host(ro, co_, va1)
+    assert amg.update_values_host(ro, co_, va2)
+    assert R.num_levels() == len(amg.hierarchy_level_sizes())
+    for l in range(R.num_levels()):
+        a, b = R.level(l), amg.export_level(l)
+        for k in ("row_offsets", "columns", "values", "inv_diag", "p_values"):
+            assert np.array_equal(a[k], b[k]), (l, k)
+    assert R.omega == amg.omega
+    # a changed pattern is refused and leaves the hierarchy as it was
+    before = amg.export_level(1)["values"].copy()
+    assert not amg.update_values_host(ro, np.roll(co_, 1), va2)
+    assert "pattern" in amg.last_error()
+    assert np.array_equal(amg.export_level(1)["values"], before)
