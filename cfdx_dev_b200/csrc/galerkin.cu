@@ -322,18 +322,23 @@ bool amg_refresh_device(cfdxg_context* ctx, cfdxg_amg* amg, const cfdxg_matrix* 
         DevRefreshLevel& L = R.L[l];
         if (l > 0) {
             DevRefreshLevel& F = R.L[l - 1];
-            ProfScope ps(ctx, "refresh_galerkin_level", 0.0);
-            const int rows_grid = std::min<int64_t>((F.n + kWarpRows - 1) / kWarpRows, 148 * 32);
-            k_ap_rows<<<rows_grid, 32 * kWarpRows, 0, s>>>(F.n, F.ro.get(), F.co.get(), F.va.get(), F.p_off.get(),
-                                                           F.p_col.get(), F.p_val.get(), F.ap_off.get(),
-                                                           F.ap_col.get(), F.ap.get(), st);
-            check_launch(ctx);
-            const int crows_grid = std::min<int64_t>((F.n_coarse + kWarpRows - 1) / kWarpRows, 148 * 32);
-            k_c_rows<<<crows_grid, 32 * kWarpRows, 0, s>>>(F.n_coarse, F.t_off.get(), F.t_row.get(), F.t_pos.get(),
-                                                           F.p_off.get(), F.p_val.get(), F.ap_off.get(),
-                                                           F.ap_col.get(), F.ap.get(), F.c_off.get(), F.c_col.get(),
-                                                           F.cv.get(), st);
-            check_launch(ctx);
+            {
+                ProfScope ps(ctx, "refresh_galerkin_ap", 0.0);
+                const int grid = std::min<int64_t>((F.n + kWarpRows - 1) / kWarpRows, 148 * 32);
+                k_ap_rows<<<grid, 32 * kWarpRows, 0, s>>>(F.n, F.ro.get(), F.co.get(), F.va.get(), F.p_off.get(),
+                                                          F.p_col.get(), F.p_val.get(), F.ap_off.get(),
+                                                          F.ap_col.get(), F.ap.get(), st);
+                check_launch(ctx);
+            }
+            {
+                ProfScope ps(ctx, "refresh_galerkin_c", 0.0);
+                const int grid = std::min<int64_t>((F.n_coarse + kWarpRows - 1) / kWarpRows, 148 * 32);
+                k_c_rows<<<grid, 32 * kWarpRows, 0, s>>>(F.n_coarse, F.t_off.get(), F.t_row.get(), F.t_pos.get(),
+                                                         F.p_off.get(), F.p_val.get(), F.ap_off.get(),
+                                                         F.ap_col.get(), F.ap.get(), F.c_off.get(), F.c_col.get(),
+                                                         F.cv.get(), st);
+                check_launch(ctx);
+            }
             const int64_t entries = static_cast<int64_t>(F.cv.size());
             k_prune_into<<<blocks_for(entries, kT), kT, 0, s>>>(entries, F.cv.get(), F.keep_pos.get(), L.va.get(), st);
             check_launch(ctx);
