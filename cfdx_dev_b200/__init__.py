@@ -21,9 +21,12 @@ from .api import (  # noqa: F401
     hex_case,
     make_request,
     make_rhie_chow_mass_flux,
+    parse_linear_capture_iterations,
     random_field,
+    read_linear_system_capture,
     solve_fgmres,
     solve_gmres,
     solve_linear_system,
     tet_case,
+    write_linear_system_capture,
 )

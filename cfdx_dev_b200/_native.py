@@ -80,6 +80,13 @@ class Report(C.Structure):
         return d
 
 
+class CaptureInfo(C.Structure):
+    _fields_ = [
+        ("problem", C.c_int32), ("null_space", C.c_int32), ("scaling", C.c_int32), ("n", C.c_int64),
+        ("nnz", C.c_int64), ("max_iterations", C.c_int64), ("tolerance", C.c_double), ("checksum", C.c_uint64),
+    ]
+
+
 _V = C.c_void_p
 _P = C.POINTER
 # name -> (restype, argtypes)
@@ -149,6 +156,11 @@ PROTOTYPES = {
     "cfdxg_mpnn_set_vcycle": (C.c_int, [_V, _V, _V]),
     "cfdxg_mpnn_train_step": (C.c_int, [_V, _V, _V, _V, C.c_int32, C.c_float, C.c_int32, c_double_p]),
     "cfdxg_mpnn_loss_grad": (C.c_int, [_V, _V, _V, _V, C.c_int32, C.c_int32, c_double_p, _V]),
+    "cfdxg_capture_read": (C.c_int, [C.c_char_p, _P(_V), _P(CaptureInfo)]),
+    "cfdxg_capture_export": (C.c_int, [_V] * 6),
+    "cfdxg_capture_write": (C.c_int, [C.c_char_p, C.c_int64] + [_V] * 5 + [_P(CaptureInfo)]),
+    "cfdxg_capture_destroy": (C.c_int, [_V]),
+    "cfdxg_capture_last_error": (C.c_char_p, []),
 }
 
 _lib = None

@@ -479,11 +479,20 @@ def make_request(krylov="gmres", preconditioner="native_amg", restart=40, precis
 
 
 def solve_linear_system(A: SparseMatrix, rhs, x0=None, krylov="gmres", preconditioner="native_amg",
-                        restart=40, precision="fp64", max_iterations=1000, tolerance=1e-12, learned=None, **kw):
-    """core/linalg/linear_solver_dispatch.h:227 for PressurePoisson systems -> (x, report)."""
+                        restart=40, precision="fp64", max_iterations=1000, tolerance=1e-12, learned=None,
+                        linear_capture_path=None, **kw):
+    """core/linalg/linear_solver_dispatch.h:227 for PressurePoisson systems -> (x, report).
+
+    ``linear_capture_path`` (opt-in, as LinearSolverRequest::linear_capture_path)
+    writes the system with its initial guess to a .cfdxlin file before the
+    solve (linear_solver_dispatch.h:236-239)."""
     ctx = A.ctx
     b = _f64(rhs, A.n)
     x = np.zeros(A.n) if x0 is None else _f64(x0, A.n).copy()
+    if linear_capture_path:
+        ro, co, va = A.to_csr()
+        write_linear_system_capture(linear_capture_path, ro, co, va, b, x, problem=CAPTURE_PRESSURE_POISSON,
+                                    max_iterations=max_iterations, tolerance=tolerance)
     req = make_request(krylov, preconditioner, restart, precision, learned, **kw)
     rep = N.Report()
     rc = ctx.lib.cfdxg_solve_linear_system(ctx.handle, A.handle, N.ptr(b), N.ptr(x), N.CFDXG_MEM_HOST,
@@ -582,3 +591,74 @@ class LearnedPreconditioner:
                 self.handle = None
         except Exception:
             pass
+
+
+# ---------------------------------------------------------------------------
+# linear-system replay files (.cfdxlin)
+# ---------------------------------------------------------------------------
+# LinearProblemKind (core/linalg/linear_solver_models.h:11-18): General 0,
+# PressurePoisson 1, Diffusion 2, Momentum 3, ScalarTransport 4,
+# CoupledPressureVelocity 5; NullSpaceModel None 0 / Constant 1.
+CAPTURE_GENERAL, CAPTURE_PRESSURE_POISSON, CAPTURE_DIFFUSION = 0, 1, 2
+
+
+def parse_linear_capture_iterations(csv: str, max_count: int = 32) -> list[int]:
+    """parse_linear_capture_iterations (core/linalg/linear_system_capture.h:39-65):
+    a comma-separated list of distinct positive outer iterations; ValueError on
+    an empty, malformed, zero, duplicated or over-long list."""
+    if not csv or max_count == 0:
+        raise ValueError("capture iterations: missing selection")
+    values = []
+    for token in csv.split(","):
+        if not token or len(values) >= max_count or not all("0" <= ch <= "9" for ch in token):
+            raise ValueError("capture iterations: malformed list")
+        number = int(token)
+        if number == 0 or number > 2**64 - 1:
+            raise ValueError("capture iterations: invalid value")
+        values.append(number)
+    if not values or csv.endswith(","):
+        raise ValueError("capture iterations: empty selection")
+    if len(set(values)) != len(values):
+        raise ValueError("capture iterations: duplicated selection")
+    return values
+
+
+def read_linear_system_capture(path) -> dict:
+    """read_linear_system_capture (core/linalg/linear_system_capture.h:233-284):
+    CSR, right-hand side, initial guess and solver metadata of a .cfdxlin file.
+    Raises CfdxgError on a malformed, truncated or corrupted file."""
+    lib = N.load()
+    h = C.c_void_p()
+    info = N.CaptureInfo()
+    rc = lib.cfdxg_capture_read(str(path).encode(), C.byref(h), C.byref(info))
+    if rc != 0:
+        raise CfdxgError(rc, lib.cfdxg_capture_last_error().decode())
+    try:
+        out = dict(row_offsets=np.empty(info.n + 1, np.int64), columns=np.empty(info.nnz, np.int64),
+                   values=np.empty(info.nnz), rhs=np.empty(info.n), initial_solution=np.empty(info.n))
+        lib.cfdxg_capture_export(h, *(N.ptr(out[k]) for k in ("row_offsets", "columns", "values", "rhs",
+                                                               "initial_solution")))
+    finally:
+        lib.cfdxg_capture_destroy(h)
+    out.update(problem=info.problem, null_space=info.null_space, scaling=info.scaling,
+               max_iterations=info.max_iterations, tolerance=info.tolerance, checksum=info.checksum)
+    return out
+
+
+def write_linear_system_capture(path, row_offsets, columns, values, rhs, initial_solution,
+                                problem=CAPTURE_PRESSURE_POISSON, null_space=0, scaling=0, max_iterations=1000,
+                                tolerance=1e-8) -> int:
+    """write_linear_system_capture (core/linalg/linear_system_capture.h:170-231);
+    returns the file's checksum.  Invalid input raises before a file exists."""
+    lib = N.load()
+    ro, co, va = _i64(row_offsets), _i64(columns), _f64(values)
+    n = ro.size - 1
+    if n < 1 or co.size != ro[-1] or va.size != ro[-1]:
+        raise ValueError("linear capture: CSR arrays of inconsistent sizes")
+    b, x = _f64(rhs, n), _f64(initial_solution, n)
+    info = N.CaptureInfo(problem, null_space, scaling, n, va.size, max_iterations, tolerance, 0)
+    rc = lib.cfdxg_capture_write(str(path).encode(), n, N.ptr(ro), N.ptr(co), N.ptr(va), N.ptr(b), N.ptr(x),
+                                 C.byref(info))
+    if rc != 0:
+        raise CfdxgError(rc, lib.cfdxg_capture_last_error().decode())
+    return int(info.checksum)

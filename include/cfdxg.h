@@ -358,6 +358,45 @@ int cfdxg_mpnn_loss_grad(cfdxg_context* ctx, cfdxg_mpnn* net, const double* r, c
                          int32_t batch, int32_t mem, double* loss, float* grad);
 
 /* ------------------------------------------------------------------------ */
+/* Linear-system replay files (".cfdxlin")                                   */
+/* Replaces write_linear_system_capture / read_linear_system_capture         */
+/* (core/linalg/linear_system_capture.h:170-231, :233-284): the same text     */
+/* format (FP64 bit patterns in hex, FNV-1a checksum), so a pressure system   */
+/* captured by CFDX replays here bit for bit and files written here are      */
+/* byte-identical to the reference writer's.  Host-only; no device needed.   */
+/* ------------------------------------------------------------------------ */
+typedef struct cfdxg_capture cfdxg_capture;
+typedef struct {
+    int32_t problem;                 /* LinearProblemKind 0..5 (General, PressurePoisson, ...) */
+    int32_t null_space;              /* NullSpaceModel: 0 none, 1 constant */
+    int32_t scaling;                 /* LinearScalingModel 0..4 */
+    int64_t n;                       /* rows (= columns) */
+    int64_t nnz;
+    int64_t max_iterations;          /* 1 .. 1e8 */
+    double tolerance;                /* > 0, finite */
+    uint64_t checksum;               /* the file's FNV-1a checksum */
+} cfdxg_capture_info;
+
+/* Reads and verifies a capture (format, limits rows <= 2e6 and nnz <= 1e8,
+ * CSR invariants, finite values, checksum).  CFDXG_ERR_IO with the reason in
+ * cfdxg_capture_last_error() on any failure; *out is then NULL. */
+int cfdxg_capture_read(const char* path, cfdxg_capture** out, cfdxg_capture_info* info);
+/* Copies the arrays out (sizes n + 1, nnz, nnz, n, n); NULL skips an array. */
+int cfdxg_capture_export(const cfdxg_capture* c, int64_t* row_offsets, int64_t* columns, double* values,
+                         double* rhs, double* initial_solution);
+/* Writes a capture of a host CSR system.  info supplies problem, null_space,
+ * scaling, max_iterations and tolerance; n, nnz and checksum are written back.
+ * Invalid input (non-finite values, unsorted or out-of-range columns, unknown
+ * metadata, limits) is refused with CFDXG_ERR_INVALID_ARGUMENT before any
+ * file is created; the file appears by rename of "<path>.tmp" once complete. */
+int cfdxg_capture_write(const char* path, int64_t n, const int64_t* row_offsets, const int64_t* columns,
+                        const double* values, const double* rhs, const double* initial_solution,
+                        cfdxg_capture_info* info);
+int cfdxg_capture_destroy(cfdxg_capture* c);
+/* Reason of the calling thread's last failed capture call. */
+const char* cfdxg_capture_last_error(void);
+
+/* ------------------------------------------------------------------------ */
 /* synthetic cases (seeded generators for the benchmark configurations)      */
 /* ------------------------------------------------------------------------ */
 typedef struct cfdxg_case cfdxg_case;

@@ -305,3 +305,32 @@ def solve_linear_system(ro, co, va, rhs, x0=None, krylov=3, preconditioner=6, re
     _check(lib().ref_solve_linear_system(b.size, _p(ro), _p(co), _p(va), _p(b), _p(x), krylov, preconditioner,
                                          restart, max_iterations, tolerance, C.byref(rep)), "solve_linear_system")
     return x, rep.as_dict()
+
+
+def write_capture(path, ro, co, va, rhs, guess, problem=1, null_space=0, scaling=0, max_iterations=1000,
+                  tolerance=1e-8):
+    """The reference's write_linear_system_capture (linear_system_capture.h:170)."""
+    f = lib().ref_write_capture
+    f.argtypes = [C.c_char_p, C.c_int64] + [C.c_void_p] * 5 + [C.c_int32] * 3 + [C.c_int64, C.c_double]
+    ro, co = np.ascontiguousarray(ro, np.int64), np.ascontiguousarray(co, np.int64)
+    va, b, x = (np.ascontiguousarray(a, np.float64) for a in (va, rhs, guess))
+    _check(f(str(path).encode(), b.size, _p(ro), _p(co), _p(va), _p(b), _p(x), problem, null_space, scaling,
+             max_iterations, tolerance), "write_linear_system_capture")
+
+
+def read_capture(path) -> dict:
+    """The reference's read_linear_system_capture (linear_system_capture.h:233)."""
+    f = lib().ref_read_capture
+    f.argtypes = [C.c_char_p] + [C.c_void_p] * 7
+    meta = np.zeros(6, np.int64)
+    tol = C.c_double()
+    _check(f(str(path).encode(), _p(meta), C.byref(tol), None, None, None, None, None),
+           "read_linear_system_capture")
+    n, nnz = int(meta[0]), int(meta[1])
+    out = dict(row_offsets=np.empty(n + 1, np.int64), columns=np.empty(nnz, np.int64), values=np.empty(nnz),
+               rhs=np.empty(n), initial_solution=np.empty(n))
+    _check(f(str(path).encode(), _p(meta), C.byref(tol), *(_p(out[k]) for k in (
+        "row_offsets", "columns", "values", "rhs", "initial_solution"))), "read_linear_system_capture")
+    out.update(problem=int(meta[2]), null_space=int(meta[3]), scaling=int(meta[4]), max_iterations=int(meta[5]),
+               tolerance=tol.value)
+    return out

@@ -124,6 +124,13 @@ int ref_solve_gmres_prepared(void* amg, int64_t n, const int64_t* row_offsets,
                              const double* rhs, double* x, int32_t restart,
                              int64_t max_iterations, double tolerance,
                              ref_report_t* report);
+/* core/linalg/linear_system_capture.h:170 / :233 -- the .cfdxlin replay format */
+int ref_write_capture(const char* path, int64_t n, const int64_t* row_offsets, const int64_t* columns,
+                      const double* values, const double* rhs, const double* guess, int32_t problem,
+                      int32_t null_space, int32_t scaling, int64_t max_iterations, double tolerance);
+int ref_read_capture(const char* path, int64_t* meta /* n, nnz, problem, null_space, scaling, max_it */,
+                     double* tolerance, int64_t* row_offsets, int64_t* columns, double* values,
+                     double* rhs, double* guess);
 /* one SpMV with SparseMatrix::matvec (sparse_matrix.h:180) */
 int ref_spmv(int64_t n, const int64_t* row_offsets, const int64_t* columns,
              const double* values, const double* x, double* y);

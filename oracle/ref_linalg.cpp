@@ -5,6 +5,7 @@
 // reference's own implementation compiled from its sources.
 #include "cfdx/core/geometry/geometry_cache.h"
 #include "cfdx/core/linalg/linear_solver_dispatch.h"
+#include "cfdx/core/linalg/linear_system_capture.h"
 #include "cfdx/core/solvers/scalar_diffusion.h"
 #include "validation/radiation_tetrahedral_mesh_v52.h"
 
@@ -146,6 +147,63 @@ extern "C" int ref_spmv(int64_t n, const int64_t* ro, const int64_t* co, const d
         const std::vector<double> xv(x, x + n);
         const auto yv = A.matvec(xv);
         for (int64_t i = 0; i < n; ++i) y[i] = yv[i];
+        return 0;
+    } catch (const std::exception& e) {
+        cfdx_ref::set_error(e);
+        return -1;
+    }
+}
+
+// core/linalg/linear_system_capture.h:170  write_linear_system_capture
+extern "C" int ref_write_capture(const char* path, int64_t n, const int64_t* ro, const int64_t* co,
+                                 const double* va, const double* rhs, const double* guess, int32_t problem,
+                                 int32_t null_space, int32_t scaling, int64_t max_iterations, double tolerance) {
+    try {
+        const SparseMatrix A = cfdx_ref::make_csr(n, ro, co, va);
+        Vector b(static_cast<std::size_t>(n)), x(static_cast<std::size_t>(n));
+        for (int64_t i = 0; i < n; ++i) {
+            b(i) = rhs[i];
+            x(i) = guess[i];
+        }
+        write_linear_system_capture(path, A, b, x, static_cast<LinearProblemKind>(problem),
+                                    static_cast<NullSpaceModel>(null_space),
+                                    static_cast<LinearScalingModel>(scaling),
+                                    static_cast<std::size_t>(max_iterations), tolerance);
+        cfdx_ref::g_error.clear();
+        return 0;
+    } catch (const std::exception& e) {
+        cfdx_ref::set_error(e);
+        return -1;
+    }
+}
+
+// core/linalg/linear_system_capture.h:233  read_linear_system_capture: sizes
+// and metadata (n, nnz, problem, null_space, scaling, max_iterations) into
+// meta[6] and the tolerance into *tolerance, then the arrays when given.
+extern "C" int ref_read_capture(const char* path, int64_t* meta, double* tolerance, int64_t* ro, int64_t* co,
+                                double* va, double* rhs, double* guess) {
+    try {
+        const LinearSystemCapture c = read_linear_system_capture(path);
+        const std::size_t n = c.matrix.n_rows(), nnz = c.matrix.nnz();
+        meta[0] = static_cast<int64_t>(n);
+        meta[1] = static_cast<int64_t>(nnz);
+        meta[2] = static_cast<int64_t>(c.problem);
+        meta[3] = static_cast<int64_t>(c.null_space);
+        meta[4] = static_cast<int64_t>(c.scaling);
+        meta[5] = static_cast<int64_t>(c.max_iterations);
+        *tolerance = c.tolerance;
+        if (ro) {
+            for (std::size_t i = 0; i <= n; ++i) ro[i] = c.matrix.row_offsets_data()[i];
+            for (std::size_t k = 0; k < nnz; ++k) {
+                co[k] = c.matrix.columns_data()[k];
+                va[k] = c.matrix.values_data()[k];
+            }
+            for (std::size_t i = 0; i < n; ++i) {
+                rhs[i] = c.rhs(i);
+                guess[i] = c.initial_solution(i);
+            }
+        }
+        cfdx_ref::g_error.clear();
         return 0;
     } catch (const std::exception& e) {
         cfdx_ref::set_error(e);

@@ -9,7 +9,10 @@ inputs of tests/cases.py and stores its outputs:
   the AMG hierarchy (every level's CSR, inverse diagonal and prolongation,
   damping omega), one V-cycle (r, z) and the AMG-GMRES(30) solution to 1e-8
   with its iteration count;
-* poisson_hex6.npz -- hex 6^3 Poisson system (CSR and right-hand side).
+* poisson_hex6.npz -- hex 6^3 Poisson system (CSR and right-hand side);
+* pressure_tet4.cfdxlin -- the pressure system of pressure_tet4.npz with a
+  zero initial guess, written by the reference's write_linear_system_capture
+  (PressurePoisson, no null space, tolerance 1e-8, 1000 iterations).
 
     python tests/golden/make_golden.py
 """
@@ -54,6 +57,13 @@ def pressure(n: int):
     np.savez_compressed(HERE / f"pressure_tet{n}.npz", **out)
 
 
+def capture(n: int):
+    z = np.load(HERE / f"pressure_tet{n}.npz")
+    b = z["b"]
+    ref.write_capture(HERE / f"pressure_tet{n}.cfdxlin", z["row_offsets"], z["columns"], z["values"], b,
+                      np.zeros_like(b), problem=1, null_space=0, scaling=0, max_iterations=1000, tolerance=1e-8)
+
+
 def poisson(n: int):
     m, bc, src = cases.poisson_case(n)
     ro, co, va, rhs, _ = ref.assemble_diffusion(m, bc, 1.0, src)
@@ -62,6 +72,7 @@ def poisson(n: int):
 
 if __name__ == "__main__":
     pressure(4)
+    capture(4)
     poisson(6)
-    for p in sorted(HERE.glob("*.npz")):
+    for p in sorted(HERE.glob("*.npz")) + sorted(HERE.glob("*.cfdxlin")):
         print(p.name, p.stat().st_size)
