@@ -955,3 +955,188 @@ int co_solve_gmres(int64_t n, const int64_t* ro, const int64_t* co, const double
     co_report_t* R = report ? report : &local;
     return gmres(&S, b, x, restart, max_iterations, tolerance, R);
 }
+
+/* ---------------------------------------------------------------- CG */
+
+/* The preconditioner of one CG solve: the solver's own diagonal (no object,
+ * the legacy solve_cg overload), or one of the objects the dispatch builds
+ * (linear_solver_dispatch.h:169-189): identity, Jacobi, native AMG. */
+typedef struct {
+    int32_t kind;
+    const co_hierarchy_t* h;
+    const double* diag;      /* kind 0: first diagonal entry; kind 2: its inverse */
+} cg_pc_t;
+
+/* cg_solver.h:203-216 apply_preconditioner: z = M^-1 r, every entry finite */
+static int cg_apply(const cg_pc_t* P, int64_t n, const double* r, double* z) {
+    switch (P->kind) {
+        case CO_CG_INTERNAL_JACOBI:
+            for (int64_t i = 0; i < n; ++i) z[i] = r[i] / P->diag[i];
+            break;
+        case CO_CG_IDENTITY:                       /* preconditioner.h:39-45 */
+            memcpy(z, r, sizeof(double) * (size_t)n);
+            break;
+        case CO_CG_JACOBI:                         /* preconditioner.h:87-91 */
+            for (int64_t i = 0; i < n; ++i) z[i] = P->diag[i] * r[i];
+            break;
+        default:
+            memset(z, 0, sizeof(double) * (size_t)n);
+            if (vcycle(P->h, 0, r, z)) return 0;
+    }
+    for (int64_t i = 0; i < n; ++i)
+        if (!isfinite(z[i])) return 0;
+    return 1;
+}
+
+int co_solve_cg(int64_t n, const int64_t* ro, const int64_t* co, const double* va, int32_t preconditioner,
+                const co_hierarchy_t* h, const double* b, double* x, int64_t max_iter, double tolerance,
+                co_report_t* report) {
+    co_report_t local;
+    co_report_t* R = report ? report : &local;
+    memset(R, 0, sizeof *R);
+    if (n <= 0) { R->status = 3; return 0; }
+    if (preconditioner == CO_CG_AMG && !h) return fail("CG with native AMG needs a hierarchy");
+    if (preconditioner != CO_CG_INTERNAL_JACOBI && preconditioner != CO_CG_IDENTITY &&
+        preconditioner != CO_CG_JACOBI && preconditioner != CO_CG_AMG)
+        return fail("unknown CG preconditioner %d", (int)preconditioner);
+    const int has_pc = preconditioner != CO_CG_INTERNAL_JACOBI;
+    for (int64_t k = 0; k < ro[n]; ++k)
+        if (!isfinite(va[k])) { R->status = 2; return 0; }
+    for (int64_t i = 0; i < n; ++i)
+        if (!isfinite(b[i]) || !isfinite(x[i])) { R->status = 2; return 0; }
+    const size_t N = (size_t)n;
+    double *r = malloc(sizeof(double) * N), *rv = malloc(sizeof(double) * N), *z = malloc(sizeof(double) * N);
+    double *p = malloc(sizeof(double) * N), *Ap = malloc(sizeof(double) * N), *M = calloc(N, sizeof(double));
+    int rc = -1;
+    if (!r || !rv || !z || !p || !Ap || !M) { fail("out of memory"); goto out; }
+    cg_pc_t P = {preconditioner, h, M};
+    double homogeneous = 0.0;
+    /* cg_solver.h:108-120 update_true_residual (reports of failed solves) */
+#define TRUE_RES()                                                                   \
+    do {                                                                             \
+        co_spmv(n, ro, co, va, x, Ap);                                               \
+        for (int64_t i_ = 0; i_ < n; ++i_) rv[i_] = b[i_] - Ap[i_];                  \
+    } while (0)
+#define FAILED_REPORT(st, it)                                                        \
+    do {                                                                             \
+        R->status = (st);                                                            \
+        R->iterations = (it);                                                        \
+        TRUE_RES();                                                                  \
+        R->residual = norm2(n, rv);                                                  \
+        const double bn_ = norm2(n, b);                                              \
+        R->residual_relative = bn_ > 0.0 ? R->residual / bn_                         \
+            : (homogeneous > 0.0 ? R->residual / homogeneous                         \
+               : (R->residual == 0.0 ? 0.0 : INFINITY));                             \
+        rc = 0;                                                                      \
+        goto out;                                                                    \
+    } while (0)
+#define FINISH(st, it, res)                                                          \
+    do {                                                                             \
+        R->status = (st);                                                            \
+        R->iterations = (it);                                                        \
+        R->residual = (res);                                                         \
+        R->residual_relative = reference > 0.0 ? (res) / reference : 0.0;            \
+        rc = 0;                                                                      \
+        goto out;                                                                    \
+    } while (0)
+#define APPLY() (++R->preconditioner_applications, cg_apply(&P, n, r, z))
+    /* :149-169 initial true residual, converged before any preconditioner work */
+    TRUE_RES();
+    memcpy(r, rv, sizeof(double) * N);
+    const double b_norm = norm2(n, b);
+    const double initial = norm2(n, rv);
+    homogeneous = b_norm == 0.0 ? initial : 0.0;
+    const double reference = b_norm > 0.0 ? b_norm : initial;
+    const double tol_abs = tolerance * reference;
+    if (initial <= tol_abs) FINISH(0, 0, initial);
+    /* :171-189 the solver's own diagonal / the Jacobi object's inverse diagonal */
+    if (preconditioner == CO_CG_INTERNAL_JACOBI || preconditioner == CO_CG_JACOBI) {
+        for (int64_t i = 0; i < n; ++i) {
+            int found = 0;
+            for (int64_t k = ro[i]; k < ro[i + 1]; ++k)
+                if (co[k] == i) {
+                    M[i] = preconditioner == CO_CG_JACOBI ? 1.0 / va[k] : va[k];
+                    found = 1;
+                    break;
+                }
+            if (preconditioner == CO_CG_INTERNAL_JACOBI ? (!(M[i] > 0.0) || !isfinite(M[i]))
+                                                        : (!found || !isfinite(M[i])))
+                FAILED_REPORT(3, 0);
+        }
+    }
+    if (!APPLY()) FAILED_REPORT(3, 0);
+    memcpy(p, z, sizeof(double) * N);
+    double rsold = dot(n, r, z);
+    if (!isfinite(rsold)) FAILED_REPORT(2, 0);
+    if (!(rsold > 0.0)) FAILED_REPORT(3, 0);
+    double at_last_replacement = INFINITY;
+    for (int64_t iter = 1; iter <= max_iter; ++iter) {
+        co_spmv(n, ro, co, va, p, Ap);
+        const double pAp = dot(n, p, Ap);
+        if (!(pAp > 0.0) || !isfinite(pAp)) FAILED_REPORT(3, iter);
+        const double alpha = rsold / pAp;
+        if (!isfinite(alpha)) FAILED_REPORT(2, iter);
+        for (int64_t i = 0; i < n; ++i) {
+            x[i] += alpha * p[i];
+            r[i] -= alpha * Ap[i];
+        }
+        for (int64_t i = 0; i < n; ++i)
+            if (!isfinite(x[i]) || !isfinite(r[i])) FAILED_REPORT(2, iter);
+        if (!APPLY()) FAILED_REPORT(3, iter);
+        const double rsnew = dot(n, r, z);
+        if (!isfinite(rsnew)) FAILED_REPORT(2, iter);
+        TRUE_RES();
+        const double res = norm2(n, rv);
+        if (res <= tol_abs) FINISH(0, iter, res);
+        if (!has_pc) {
+            /* :321-352 the internal-Jacobi residual replacement */
+            double rr = 0.0;
+            for (int64_t i = 0; i < n; ++i) rr = hypot(rr, r[i]);
+            if (isfinite(rr) && rr <= tol_abs && res > tol_abs) {
+                ++R->residual_replacements;
+                memcpy(r, rv, sizeof(double) * N);
+                if (!APPLY()) { R->status = 3; R->iterations = iter; rc = 0; goto out; }
+                const double replaced = dot(n, r, z);
+                if (!isfinite(replaced) || !(replaced > 0.0)) FINISH(1, iter, res);
+                memcpy(p, z, sizeof(double) * N);
+                rsold = replaced;
+                continue;
+            }
+        } else {
+            /* :399-525 adaptive residual replacement and collapse repair */
+            double rr2 = 0.0;
+            for (int64_t i = 0; i < n; ++i) rr2 += r[i] * r[i];
+            const double rr = sqrt(rr2);
+            const double gap = fabs(res - rr);
+            const double scale = fmax(res, rr);
+            const int progress = res < 0.5 * at_last_replacement;
+            const int collapsed = !(rsnew > 0.0);
+            const int adaptive = isfinite(rr) && scale > 0.0 && gap > 0.25 * scale && progress;
+            const int repair = collapsed && progress;
+            if (collapsed && !repair) FINISH(1, iter, res);
+            if (adaptive || repair) {
+                ++R->residual_replacements;
+                at_last_replacement = res;
+                memcpy(r, rv, sizeof(double) * N);
+                if (!APPLY()) FAILED_REPORT(3, iter);
+                const double replaced = dot(n, r, z);
+                if (!isfinite(replaced) || !(replaced > 0.0)) FAILED_REPORT(3, iter);
+                memcpy(p, z, sizeof(double) * N);
+                rsold = replaced;
+                continue;
+            }
+        }
+        const double beta = rsnew / rsold;
+        for (int64_t i = 0; i < n; ++i) p[i] = z[i] + beta * p[i];
+        rsold = rsnew;
+    }
+    TRUE_RES();
+    FINISH(1, max_iter, norm2(n, rv));
+#undef TRUE_RES
+#undef FAILED_REPORT
+#undef FINISH
+#undef APPLY
+out:
+    free(r); free(rv); free(z); free(p); free(Ap); free(M);
+    return rc;
+}

@@ -125,6 +125,23 @@ int co_solve_gmres(int64_t n, const int64_t* row_offsets, const int64_t* columns
                    double* x, int32_t restart, int64_t max_iterations, double tolerance,
                    co_report_t* report);
 
+/* core/linalg/cg_solver.h:45-560 solve_cg_impl, FP64 without a null space:
+ * the true residual certifies every iteration, residual replacement as the
+ * reference (adaptive with a preconditioner object, the recursive-norm rule
+ * without).  preconditioner: CO_CG_INTERNAL_JACOBI -- no object, the solver's
+ * own diagonal (the legacy solve_cg overload); CO_CG_IDENTITY, CO_CG_JACOBI,
+ * CO_CG_AMG -- the objects solve_linear_system builds for None / Jacobi /
+ * NativeAMG (linear_solver_dispatch.h:169-189), AMG applying co_vcycle on h.
+ * x holds the initial guess and receives the solution. */
+#define CO_CG_INTERNAL_JACOBI 0
+#define CO_CG_IDENTITY 1
+#define CO_CG_JACOBI 2
+#define CO_CG_AMG 6
+int co_solve_cg(int64_t n, const int64_t* row_offsets, const int64_t* columns,
+                const double* values, int32_t preconditioner, const co_hierarchy_t* h,
+                const double* b, double* x, int64_t max_iterations, double tolerance,
+                co_report_t* report);
+
 #ifdef __cplusplus
 }
 #endif

@@ -82,6 +82,8 @@ def lib():
             L.co_vcycle.argtypes = [C.c_void_p] * 3
             L.co_solve_gmres.argtypes = [C.c_int64] + [C.c_void_p] * 6 + [C.c_int32, C.c_int64, C.c_double,
                                                                           C.c_void_p]
+            L.co_solve_cg.argtypes = [C.c_int64] + [C.c_void_p] * 3 + [C.c_int32] + [C.c_void_p] * 3 + [
+                C.c_int64, C.c_double, C.c_void_p]
             _lib = L
     return _lib
 
@@ -229,4 +231,21 @@ def solve_gmres(ro, co, va, b, hierarchy=None, x0=None, restart=30, max_iteratio
     rep = CoReport()
     _check(lib().co_solve_gmres(b.size, _p(ro), _p(co), _p(va), hierarchy.ptr if hierarchy else None, _p(b), _p(x),
                                 int(restart), int(max_iterations), float(tolerance), C.byref(rep)), "GMRES")
+    return x, rep.as_dict()
+
+
+CG_PRECONDITIONERS = {"internal_jacobi": 0, "none": 1, "jacobi": 2, "native_amg": 6}
+
+
+def solve_cg(ro, co, va, b, preconditioner="native_amg", hierarchy=None, x0=None, max_iterations=1000,
+             tolerance=1e-8):
+    """co_solve_cg: the reference's CG (cg_solver.h:45-560) with the solver's
+    own diagonal ("internal_jacobi") or the dispatch's identity / Jacobi /
+    native-AMG preconditioner object (the AMG one applies ``hierarchy``)."""
+    ro, co, va, b = (np.ascontiguousarray(ro, np.int64), np.ascontiguousarray(co, np.int64), _f64(va), _f64(b))
+    x = np.zeros_like(b) if x0 is None else np.array(x0, dtype=np.float64)
+    rep = CoReport()
+    _check(lib().co_solve_cg(b.size, _p(ro), _p(co), _p(va), CG_PRECONDITIONERS[preconditioner],
+                             hierarchy.ptr if hierarchy else None, _p(b), _p(x), int(max_iterations),
+                             float(tolerance), C.byref(rep)), "CG")
     return x, rep.as_dict()

@@ -334,3 +334,15 @@ def read_capture(path) -> dict:
     out.update(problem=int(meta[2]), null_space=int(meta[3]), scaling=int(meta[4]), max_iterations=int(meta[5]),
                tolerance=tol.value)
     return out
+
+
+def solve_cg_internal(ro, co, va, rhs, x0=None, max_iterations=1000, tolerance=1e-8):
+    """The reference's solve_cg without a preconditioner object (cg_solver.h:591)."""
+    f = lib().ref_solve_cg_internal
+    f.argtypes = [C.c_int64] + [C.c_void_p] * 5 + [C.c_int64, C.c_double, C.c_void_p]
+    ro, co = np.ascontiguousarray(ro, np.int64), np.ascontiguousarray(co, np.int64)
+    va, b = np.ascontiguousarray(va, np.float64), np.ascontiguousarray(rhs, np.float64)
+    x = np.zeros_like(b) if x0 is None else np.array(x0, dtype=np.float64)
+    rep = RefReport()
+    _check(f(b.size, _p(ro), _p(co), _p(va), _p(b), _p(x), max_iterations, tolerance, C.byref(rep)), "solve_cg")
+    return x, rep.as_dict()

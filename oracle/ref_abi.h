@@ -131,6 +131,10 @@ int ref_write_capture(const char* path, int64_t n, const int64_t* row_offsets, c
 int ref_read_capture(const char* path, int64_t* meta /* n, nnz, problem, null_space, scaling, max_it */,
                      double* tolerance, int64_t* row_offsets, int64_t* columns, double* values,
                      double* rhs, double* guess);
+/* core/linalg/cg_solver.h:591 solve_cg(A, b, x, max_iter, tolerance): CG with its own diagonal */
+int ref_solve_cg_internal(int64_t n, const int64_t* row_offsets, const int64_t* columns, const double* values,
+                          const double* rhs, double* x, int64_t max_iterations, double tolerance,
+                          ref_report_t* report);
 /* one SpMV with SparseMatrix::matvec (sparse_matrix.h:180) */
 int ref_spmv(int64_t n, const int64_t* row_offsets, const int64_t* columns,
              const double* values, const double* x, double* y);

@@ -11,6 +11,8 @@
 
 #include "ref_common.h"
 
+#include <cstring>
+
 using namespace cfdx::core;
 
 extern "C" const char* ref_last_error(void) { return cfdx_ref::g_error.c_str(); }
@@ -202,6 +204,35 @@ extern "C" int ref_read_capture(const char* path, int64_t* meta, double* toleran
                 rhs[i] = c.rhs(i);
                 guess[i] = c.initial_solution(i);
             }
+        }
+        cfdx_ref::g_error.clear();
+        return 0;
+    } catch (const std::exception& e) {
+        cfdx_ref::set_error(e);
+        return -1;
+    }
+}
+
+// core/linalg/cg_solver.h:591-603 solve_cg without a preconditioner object:
+// the solver's own diagonal scaling (the legacy overload).
+extern "C" int ref_solve_cg_internal(int64_t n, const int64_t* ro, const int64_t* co, const double* va,
+                                     const double* rhs, double* x, int64_t max_iterations, double tolerance,
+                                     ref_report_t* report) {
+    try {
+        const SparseMatrix A = cfdx_ref::make_csr(n, ro, co, va);
+        Vector b(static_cast<std::size_t>(n)), xv(static_cast<std::size_t>(n));
+        for (int64_t i = 0; i < n; ++i) {
+            b(i) = rhs[i];
+            xv(i) = x[i];
+        }
+        const SolverResult r = solve_cg(A, b, xv, static_cast<std::size_t>(max_iterations), tolerance);
+        for (int64_t i = 0; i < n; ++i) x[i] = xv(i);
+        if (report) {
+            std::memset(report, 0, sizeof(*report));
+            report->status = static_cast<int32_t>(r.status);
+            report->iterations = static_cast<int64_t>(r.iterations);
+            report->residual = r.residual;
+            report->residual_relative = r.residual_relative;
         }
         cfdx_ref::g_error.clear();
         return 0;

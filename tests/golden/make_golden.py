@@ -7,8 +7,9 @@ inputs of tests/cases.py and stores its outputs:
 * pressure_tet4.npz -- Kuhn-tet 4^3 x 6 pressure-correction system: CSR,
   right-hand side, Rhie-Chow face flux at p = 0 and at the solved pressure,
   the AMG hierarchy (every level's CSR, inverse diagonal and prolongation,
-  damping omega), one V-cycle (r, z) and the AMG-GMRES(30) solution to 1e-8
-  with its iteration count;
+  damping omega), one V-cycle (r, z), the AMG-GMRES(30) solution to 1e-8
+  with its iteration count, and the CG + native-AMG solution of the
+  reference's solve_linear_system to 1e-10 (cg_x, cg_iterations);
 * poisson_hex6.npz -- hex 6^3 Poisson system (CSR and right-hand side);
 * pressure_tet4.cfdxlin -- the pressure system of pressure_tet4.npz with a
   zero initial guess, written by the reference's write_linear_system_capture
@@ -54,6 +55,10 @@ def pressure(n: int):
     assert rep["status"] == 0
     out.update(x=x, iterations=rep["iterations"],
                flux_solved=ref.rhie_chow_flux(m, U, rAU, x, 1.0, fixed, value))
+    xc, repc = ref.solve_linear_system(ro, co, va, b, krylov=1, preconditioner=6, max_iterations=1000,
+                                       tolerance=1e-10)
+    assert repc["status"] == 0
+    out.update(cg_x=xc, cg_iterations=repc["iterations"])
     np.savez_compressed(HERE / f"pressure_tet{n}.npz", **out)
 
 

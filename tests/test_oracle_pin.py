@@ -83,6 +83,55 @@ def test_spmv_vcycle_and_solve_match_reference(ref):
     assert np.array_equal(x_co, x_ref)
 
 
+@pytest.mark.parametrize("pc", ["native_amg", "jacobi", "none", "internal_jacobi"])
+def test_cg_matches_reference(ref, pc):
+    """CG (cg_solver.h:45-560) with each preconditioner object the dispatch
+    builds (solve_linear_system, KrylovModel::CG) and with the solver's own
+    diagonal (the legacy solve_cg overload): iterate and count bit-identical."""
+    m, g, U, rAU, p, fixed, value = _pressure_inputs(7)
+    A = co.simple_assemble(m, U, rAU, p, 1.0, fixed, value)
+    ro, cols, va, b = A["row_offsets"], A["columns"], A["values"], A["b"]
+    x0 = np.random.default_rng(9).standard_normal(b.size) * 1e-2
+    if pc == "internal_jacobi":
+        x_ref, rep_ref = ref.solve_cg_internal(ro, cols, va, b, x0=x0, max_iterations=2000, tolerance=1e-10)
+        H = None
+    else:
+        x_ref, rep_ref = ref.solve_linear_system(ro, cols, va, b, x0=x0, krylov=1,
+                                                 preconditioner={"native_amg": 6, "jacobi": 2, "none": 1}[pc],
+                                                 max_iterations=2000, tolerance=1e-10)
+        R = ref.Amg(ro, cols, va) if pc == "native_amg" else None
+        H = co.Hierarchy([R.level(l) for l in range(R.num_levels())], R.omega) if R else None
+    x_co, rep_co = co.solve_cg(ro, cols, va, b, pc, H, x0=x0, max_iterations=2000, tolerance=1e-10)
+    assert rep_co["status"] == rep_ref["status"] == 0
+    assert rep_co["iterations"] == rep_ref["iterations"]
+    assert np.array_equal(x_co, x_ref)
+
+
+def test_cg_edge_cases():
+    ro = np.array([0, 2, 5, 7], np.int64)
+    cols = np.array([0, 1, 0, 1, 2, 1, 2], np.int64)
+    vals = np.array([4.0, 1.0, 1.0, 3.0, 1.0, 1.0, 2.0])
+    # SPD 3x3: CG is exact in at most 3 steps
+    x, rep = co.solve_cg(ro, cols, vals, np.array([1.0, 2.0, 3.0]), "jacobi", max_iterations=10, tolerance=1e-13)
+    A = np.array([[4.0, 1.0, 0.0], [1.0, 3.0, 1.0], [0.0, 1.0, 2.0]])
+    assert rep["status"] == 0 and rep["iterations"] <= 3
+    assert np.allclose(A @ x, [1.0, 2.0, 3.0], rtol=0, atol=1e-12)
+    # b = 0, x0 = 0: converged before any preconditioner work
+    x, rep = co.solve_cg(ro, cols, vals, np.zeros(3), "none")
+    assert rep["status"] == 0 and rep["iterations"] == 0 and rep["preconditioner_applications"] == 0
+    # a non-positive diagonal: the solver's own Jacobi scaling is not applicable
+    x, rep = co.solve_cg(ro, cols, -vals, np.ones(3), "internal_jacobi")
+    assert rep["status"] == 3
+    # an indefinite operator: non-positive curvature -> not applicable
+    x, rep = co.solve_cg(ro, cols, np.array([1.0, 2.0, 2.0, 1.0, 0.0, 0.0, 1.0]), np.array([1.0, -1.0, 0.0]),
+                         "none", max_iterations=10)
+    assert rep["status"] == 3
+    # non-finite input: diverged
+    bad = vals.copy()
+    bad[3] = np.nan
+    assert co.solve_cg(ro, cols, bad, np.ones(3), "none")[1]["status"] == 2
+
+
 def test_small_dense_coarsest_and_unpreconditioned_gmres(ref):
     # 1-D Poisson (known-answer shape of the reference's GMRES tests): the
     # hierarchy ends in a <= 16-row level, so the dense pivoted LU runs.
@@ -165,6 +214,10 @@ def test_oracle_reproduces_golden_fixtures(name):
         assert rep["iterations"] == int(z["iterations"])
         assert np.array_equal(x, z["x"])
         assert np.array_equal(co.rhie_chow_flux(m, U, rAU, x, 1.0, fixed, value), z["flux_solved"])
+        xc, repc = co.solve_cg(a["row_offsets"], a["columns"], a["values"], a["b"], "native_amg", H,
+                               max_iterations=1000, tolerance=1e-10)
+        assert repc["status"] == 0 and repc["iterations"] == int(z["cg_iterations"])
+        assert np.array_equal(xc, z["cg_x"])
     elif name.startswith("poisson"):
         m, bc, src = cases.poisson_case(n)
         ro, cols, va, rhs = co.assemble_diffusion(m, bc, 1.0, src)
