@@ -24,6 +24,7 @@ from .api import (  # noqa: F401
     parse_linear_capture_iterations,
     random_field,
     read_linear_system_capture,
+    solve_cg,
     solve_fgmres,
     solve_gmres,
     solve_linear_system,

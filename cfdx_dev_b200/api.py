@@ -10,6 +10,9 @@ Names and argument meanings follow the reference (stevendaix/cfdx_dev):
                                          apply / name / last_error)
 * ``solve_linear_system``             -- core/linalg/linear_solver_dispatch.h:227
 * ``solve_gmres`` / ``solve_fgmres``  -- core/linalg/gmres_solver.h:28, 612
+* ``solve_cg``                        -- core/linalg/cg_solver.h:605
+* ``read_linear_system_capture`` /
+  ``write_linear_system_capture``     -- core/linalg/linear_system_capture.h:170, 233
 
 Errors surface as :class:`CfdxgError` (bad requests raise, like the
 reference's ``std::invalid_argument``); solver outcomes are reported through
@@ -518,6 +521,13 @@ def solve_gmres(A: SparseMatrix, rhs, x0=None, amg: NativeBoomerAMGPreconditione
 
 def solve_fgmres(A, rhs, x0=None, amg=None, restart=30, max_iterations=1000, tolerance=1e-12, **kw):
     return solve_gmres(A, rhs, x0, amg, restart, max_iterations, tolerance, krylov="fgmres", **kw)
+
+
+def solve_cg(A: SparseMatrix, rhs, x0=None, amg: NativeBoomerAMGPreconditioner | None = None, max_iterations=1000,
+             tolerance=1e-12):
+    """core/linalg/cg_solver.h:605 solve_cg(A, b, x, preconditioner) with a
+    prepared native AMG (or the identity) -> (x, report)."""
+    return solve_gmres(A, rhs, x0, amg, 30, max_iterations, tolerance, krylov="cg")
 
 
 # ---------------------------------------------------------------- learned preconditioner

@@ -37,6 +37,47 @@ __global__ void k_scale(int n, const double* a, const double* b, double* out) {
     if (i < n) out[i] = a[i] * b[i];
 }
 
+// max |a_k| over the stored values (diagnose_matrix max_abs_value); a
+// non-finite value makes the slot NaN.
+__global__ void k_absmax_values(int64_t nnz, const double* va, unsigned long long* bits) {
+    double m = 0.0;
+    for (int64_t k = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; k < nnz; k += int64_t(gridDim.x) * blockDim.x)
+        m = fmax(m, fabs(va[k]));
+    // non-negative doubles order like their bit patterns
+    atomicMax(bits, static_cast<unsigned long long>(__double_as_longlong(m)));
+}
+
+// measure_matrix_characteristics (core/linalg/matrix_diagnostics.h:317-355):
+// bit 1 -- some |a_ij - a_ji| > 1e-12 max(1, max|a|) (a_ji = 0 when absent);
+// bit 2 -- a row whose diagonal (sum of its diagonal entries) is missing,
+// non-positive or not finite.
+__global__ void k_cg_gate(int n, const int* ro, const int* co, const double* va,
+                          const unsigned long long* max_bits, int* flags) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const double scale = fmax(1.0, __longlong_as_double(static_cast<long long>(*max_bits)));
+    const double tol = 1e-12 * scale;
+    double diag = 0.0;
+    bool has_diag = false;
+    for (int k = ro[i]; k < ro[i + 1]; ++k) {
+        const int j = co[k];
+        if (j == i) {
+            diag += va[k];
+            has_diag = true;
+        }
+        double aji = 0.0;
+        for (int q = ro[j]; q < ro[j + 1]; ++q)
+            if (co[q] == i) aji += va[q];
+        if (fabs(va[k] - aji) > tol) atomicOr(flags, 1);
+    }
+    if (!has_diag || !(diag > 0.0) || !isfinite(diag)) atomicOr(flags, 2);
+}
+
+__global__ void k_copy(int n, const double* a, double* b) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) b[i] = a[i];
+}
+
 __global__ void k_check_finite(int n, const double* a, int* status) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i < n && !isfinite(a[i])) atomicOr(status, kStatusNonFinite);
@@ -544,9 +585,32 @@ namespace {
 // inverse diagonal, and learned network.
 KrylovResult run_krylov(cfdxg_context* ctx, const cfdxg_matrix* A, cfdxg_amg* amg, const double* inv_diag,
                         const double* b, double* x, const cfdxg_request& req, int64_t max_it, double tol,
-                        int64_t* learned_fallbacks) {
+                        int64_t* learned_fallbacks, const std::function<bool()>* cg_setup = nullptr) {
     RightPreconditioner pc;
     const int n = static_cast<int>(A->n);
+    if (req.krylov == CFDXG_KRYLOV_CG) {
+        // The preconditioner objects solve_linear_system builds for CG
+        // (linear_solver_dispatch.h:169-189): identity for None, Jacobi's
+        // inverse diagonal, or the native AMG V-cycle.
+        if (req.preconditioner == CFDXG_PC_NATIVE_AMG)
+            pc = [ctx, amg](const double* v, double* z, int) {
+                amg_apply_device(ctx, amg, v, z);
+                return true;
+            };
+        else if (req.preconditioner == CFDXG_PC_JACOBI)
+            pc = [ctx, inv_diag, n](const double* v, double* z, int) {
+                k_scale<<<blocks_for(n, 256), 256, 0, ctx->stream>>>(n, inv_diag, v, z);
+                check_launch(ctx);
+                return true;
+            };
+        else
+            pc = [ctx, n](const double* v, double* z, int) {
+                k_copy<<<blocks_for(n, 256), 256, 0, ctx->stream>>>(n, v, z);
+                check_launch(ctx);
+                return true;
+            };
+        return cg_solve(ctx, A, b, x, max_it, tol, pc, cg_setup);
+    }
     // Learned stage: dropped for the rest of the solve (plain AMG fallback)
     // as soon as an iteration fails to cut the residual estimate by 10%.
     struct LearnedState {
@@ -594,8 +658,10 @@ KrylovResult run_krylov(cfdxg_context* ctx, const cfdxg_matrix* A, cfdxg_amg* am
 
 void validate_request(const cfdxg_request& r) {
     if (r.gmres_restart <= 0) throw Error(CFDXG_ERR_INVALID_ARGUMENT, "GMRES restart must be positive");
-    if (r.krylov != CFDXG_KRYLOV_GMRES && r.krylov != CFDXG_KRYLOV_FGMRES)
-        throw Error(CFDXG_ERR_INVALID_ARGUMENT, "only GMRES and FGMRES are provided");
+    if (r.krylov != CFDXG_KRYLOV_GMRES && r.krylov != CFDXG_KRYLOV_FGMRES && r.krylov != CFDXG_KRYLOV_CG)
+        throw Error(CFDXG_ERR_INVALID_ARGUMENT, "only CG, GMRES and FGMRES are provided");
+    if (r.krylov == CFDXG_KRYLOV_CG && r.learned)
+        throw Error(CFDXG_ERR_INVALID_ARGUMENT, "the learned stage is a variable preconditioner: it needs FGMRES");
     if (r.preconditioner != CFDXG_PC_NONE && r.preconditioner != CFDXG_PC_JACOBI &&
         r.preconditioner != CFDXG_PC_NATIVE_AMG)
         throw Error(CFDXG_ERR_INVALID_ARGUMENT, "requested preconditioner model is not implemented");
@@ -604,6 +670,23 @@ void validate_request(const cfdxg_request& r) {
     if (r.learned && r.preconditioner != CFDXG_PC_NATIVE_AMG)
         throw Error(CFDXG_ERR_INVALID_ARGUMENT, "the learned preconditioner runs in front of native AMG");
     if (r.learned_applications < 0) throw Error(CFDXG_ERR_INVALID_ARGUMENT, "learned_applications must be >= 0");
+}
+
+// measure_matrix_characteristics' symmetry and positive-diagonal test, on the device.
+bool symmetric_positive_diagonal(cfdxg_context* ctx, const cfdxg_matrix* A) {
+    DevBuf<unsigned long long> max_bits(1);
+    DevBuf<int> flags(1);
+    CFDXG_CUDA(cudaMemsetAsync(max_bits.get(), 0, sizeof(unsigned long long), ctx->stream));
+    CFDXG_CUDA(cudaMemsetAsync(flags.get(), 0, sizeof(int), ctx->stream));
+    const int nb = static_cast<int>(std::min<int64_t>(std::max<int64_t>(blocks_for(A->nnz, 256), 1), 148 * 8));
+    k_absmax_values<<<nb, 256, 0, ctx->stream>>>(A->nnz, A->va.get(), max_bits.get());
+    k_cg_gate<<<blocks_for(A->n, 256), 256, 0, ctx->stream>>>(static_cast<int>(A->n), A->ro.get(), A->co.get(),
+                                                              A->va.get(), max_bits.get(), flags.get());
+    check_launch(ctx);
+    int h = 0;
+    CFDXG_CUDA(cudaMemcpyAsync(&h, flags.get(), sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+    CFDXG_CUDA(cudaStreamSynchronize(ctx->stream));
+    return h == 0;
 }
 
 }  // namespace
@@ -630,7 +713,44 @@ extern "C" int cfdxg_solve_linear_system(cfdxg_context* ctx, const cfdxg_matrix*
     KrylovResult r;
     int64_t learned_fallbacks = 0;
     double setup_s = 0.0;
-    if (req.preconditioner == CFDXG_PC_NATIVE_AMG) {
+    const bool cg = req.krylov == CFDXG_KRYLOV_CG;
+    if (cg && !symmetric_positive_diagonal(ctx, A)) {
+        // linear_solver_dispatch.h:259-267: a forced CG on a matrix that is not
+        // symmetric with a positive diagonal fails closed, x untouched
+        r.status = CFDXG_NOT_APPLICABLE;
+        ctx->error = "CG rejected: measured matrix is not symmetric with a positive diagonal";
+    } else if (cg) {
+        // the preconditioner is set up inside CG, after the initial-residual
+        // check (cg_solver.h:171-176); AMG keeps the smoother certificate
+        cfdxg_amg amg;
+        cfdxg_amg_options_default(&amg.opts);
+        amg.opts.precision = req.precision;
+        amg.opts.require_smoother_certificate = 1;
+        DevBuf<double> inv(req.preconditioner == CFDXG_PC_JACOBI ? n : 0);
+        std::function<bool()> setup = [&]() {
+            if (req.preconditioner == CFDXG_PC_NATIVE_AMG) {
+                try {
+                    amg_setup_impl(ctx, &amg, const_cast<cfdxg_matrix*>(A));
+                } catch (const Error& e) {
+                    if (e.code != CFDXG_ERR_SETUP) throw;
+                    ctx->error = amg.error;
+                    setup_s = amg.setup_seconds;
+                    return false;
+                }
+                setup_s = amg.setup_seconds;
+                return true;
+            }
+            if (req.preconditioner == CFDXG_PC_JACOBI) {
+                clear_status(ctx);
+                k_first_diag_inverse<<<blocks_for(n, 256), 256, 0, ctx->stream>>>(
+                    static_cast<int>(n), A->ro.get(), A->co.get(), A->va.get(), inv.get(), ctx->scratch.status);
+                check_launch(ctx);
+                return read_status(ctx) == 0;
+            }
+            return true;
+        };
+        r = run_krylov(ctx, A, &amg, inv.get(), b.get(), xo.get(), req, max_iterations, tolerance, nullptr, &setup);
+    } else if (req.preconditioner == CFDXG_PC_NATIVE_AMG) {
         cfdxg_amg amg;
         cfdxg_amg_options_default(&amg.opts);
         amg.opts.precision = req.precision;
@@ -695,6 +815,8 @@ extern "C" int cfdxg_solve_gmres(cfdxg_context* ctx, const cfdxg_matrix* A, cfdx
     if (amg && (!amg->ready || (!amg->d64 && !amg->d32)))
         throw Error(CFDXG_ERR_NOT_READY, "native AMG preconditioner has not been set up on the device");
     if (amg && amg->host.levels.front().A.n != A->n) throw Error(CFDXG_ERR_INVALID_ARGUMENT, "AMG size mismatch");
+    // CG here takes the given hierarchy, or the identity without one
+    if (req.krylov == CFDXG_KRYLOV_CG) req.preconditioner = amg ? CFDXG_PC_NATIVE_AMG : CFDXG_PC_NONE;
     if (report) std::memset(report, 0, sizeof(*report));
     const int64_t n = A->n;
     In<double> b(ctx, rhs, n, mem);

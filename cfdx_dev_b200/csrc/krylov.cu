@@ -243,6 +243,69 @@ private:
     double* sc_;
 };
 
+// ---------------------------------------------------------------- CG kernels
+// CG scalar slots (below GMRES's Hessenberg area)
+enum CgSlot : int {
+    kCgPAp = 8, kCgRsOld = 9, kCgRsNew = 10, kCgZBad = 11, kCgRes = 12, kCgRR2 = 13, kCgXBad = 14,
+    kCgMax = 15, kCgInvalid = 16, kCgCount = 17
+};
+
+// out_dot = sum_i r_i z_i (the k_dot partition and order); out_bad = 1 when a
+// z_i is not finite (cg_solver.h:213-215, the preconditioner's result check).
+__global__ void k_dot_check(int n, const double* __restrict__ r, const double* __restrict__ z, double* partial,
+                            unsigned* ticket, double* out_dot, double* out_bad) {
+    __shared__ double sm[32];
+    double s = 0.0, bad = 0.0;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const double zi = z[i];
+        if (!isfinite(zi)) bad = 1.0;
+        s += r[i] * zi;
+    }
+    s = block_sum(s, sm);
+    bad = block_max(bad, sm);
+    if (threadIdx.x == 0) { partial[2 * blockIdx.x] = s; partial[2 * blockIdx.x + 1] = bad; }
+    if (last_block(ticket)) {
+        double t = 0.0, bb = 0.0;
+        for (int q = threadIdx.x; q < gridDim.x; q += blockDim.x) {
+            t += partial[2 * q];
+            bb = fmax(bb, partial[2 * q + 1]);
+        }
+        t = block_sum(t, sm);
+        bb = block_max(bb, sm);
+        if (threadIdx.x == 0) { *out_dot = t; *out_bad = bb; *ticket = 0; }
+    }
+}
+
+// x += alpha p, r -= alpha Ap with alpha = rsold / pAp, only when p^T A p > 0
+// and alpha are finite (cg_solver.h:287-313); bad = 1 on a non-finite x_i or r_i.
+__global__ void k_cg_update(int n, double* __restrict__ x, double* __restrict__ r, const double* __restrict__ p,
+                            const double* __restrict__ Ap, double* slots) {
+    const double pAp = slots[kCgPAp];
+    if (!(pAp > 0.0) || !isfinite(pAp)) return;
+    const double alpha = slots[kCgRsOld] / pAp;
+    if (!isfinite(alpha)) return;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const double xi = x[i] + alpha * p[i];
+    const double ri = r[i] - alpha * Ap[i];
+    x[i] = xi;
+    r[i] = ri;
+    if (!isfinite(xi) || !isfinite(ri)) slots[kCgXBad] = 1.0;
+}
+
+// p = z + beta p with beta = rsnew / rsold (cg_solver.h:532-539)
+__global__ void k_cg_direction(int n, double* __restrict__ p, const double* __restrict__ z, const double* slots) {
+    const double beta = slots[kCgRsNew] / slots[kCgRsOld];
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) p[i] = z[i] + beta * p[i];
+}
+
+// flag = 1 when any of a[0..n) is not finite
+__global__ void k_any_nonfinite(int64_t n, const double* __restrict__ a, double* flag) {
+    for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < n; i += int64_t(gridDim.x) * blockDim.x)
+        if (!isfinite(a[i])) *flag = 1.0;
+}
+
 // krylov_controls.h:28-51
 int choose_restart(int current, double reduction, const KrylovControls& c) {
     if (!c.adaptive_restart) return std::clamp(current, c.restart_min, c.restart_max);
@@ -576,6 +639,160 @@ KrylovResult gmres_solve(cfdxg_context* ctx, const cfdxg_matrix* A, const double
     result.residual_relative = beta / rhs_scale;
     CFDXG_CUDA(cudaStreamSynchronize(ctx->stream));
     return result;
+}
+
+// ---------------------------------------------------------------- CG
+// cg_solver.h:45-560 solve_cg_impl (FP64 operator and reductions, no null
+// space, adaptive residual replacement) with a preconditioner object.  Each
+// iteration is one stream of kernels -- A p, p^T A p, the fused x/r update,
+// z = M^-1 r, r^T z with the z check, the FP64 true residual b - A x and its
+// scaled norm, ||r||^2 -- and one read-back of eight scalars, after which the
+// host takes the reference's decisions in the reference's order.
+KrylovResult cg_solve(cfdxg_context* ctx, const cfdxg_matrix* A, const double* b, double* x, int64_t max_iter,
+                      double tolerance, const RightPreconditioner& pc, const std::function<bool()>* setup) {
+    KrylovResult result;
+    const int64_t n = A->n;
+    if (n == 0) return result;   // NOT_APPLICABLE
+    if (n > std::numeric_limits<int>::max()) throw Error(CFDXG_ERR_INVALID_ARGUMENT, "system too large");
+    Engine E(ctx, A);
+    clear_status(ctx);
+    const int ni = static_cast<int>(n);
+    const int gb = blocks_for(n, kT);
+    Workspace& ws = workspace(ctx, n, 1);
+    DevBuf<double> p(n), z(n), Ap(n);
+    double* r = ws.r.get();
+    double* rv = ws.tmp.get();
+    auto zero_flags = [&]() {
+        CFDXG_CUDA(cudaMemsetAsync(E.slot(kCgZBad), 0, sizeof(double), ctx->stream));
+        CFDXG_CUDA(cudaMemsetAsync(E.slot(kCgXBad), 0, sizeof(double), ctx->stream));
+    };
+    auto dot_check = [&](const double* a, const double* zz, int out) {
+        k_dot_check<<<E.rb(), kT, 0, ctx->stream>>>(ni, a, zz, ctx->scratch.partial, ctx->scratch.ticket,
+                                                     E.slot(out), E.slot(kCgZBad));
+        check_launch(ctx);
+    };
+    auto apply = [&]() {
+        ++result.preconditioner_applications;
+        return pc(r, z.get(), 0);
+    };
+
+    // :75-85 non-finite operator, right-hand side or initial guess
+    zero_flags();
+    const int nnz_blocks = static_cast<int>(std::min<int64_t>(blocks_for(A->nnz, kT), 148 * 8));
+    k_any_nonfinite<<<std::max(nnz_blocks, 1), kT, 0, ctx->stream>>>(A->nnz, A->va.get(), E.slot(kCgXBad));
+    k_any_nonfinite<<<gb, kT, 0, ctx->stream>>>(n, b, E.slot(kCgXBad));
+    k_any_nonfinite<<<gb, kT, 0, ctx->stream>>>(n, x, E.slot(kCgXBad));
+    check_launch(ctx);
+    // :149-169 r = b - A x before any preconditioner work
+    E.residual(b, x, rv);
+    E.norm2(b, kCgMax);                 // ||b|| (slots kMax/kInvalid are the norm's own scratch)
+    E.norm2(rv, kCgRes);
+    E.fetch(kCgCount);
+    if (E.host(kCgXBad) > 0.0) {
+        result.status = CFDXG_DIVERGED;
+        return result;
+    }
+    const double b_norm = E.host(kCgMax);
+    const double initial = E.host(kCgRes);
+    const double homogeneous = b_norm == 0.0 ? initial : 0.0;
+    const double reference = b_norm > 0.0 ? b_norm : initial;
+    const double tol_abs = tolerance * reference;
+    auto finish = [&](int status, int64_t it, double res) {
+        result.status = status;
+        result.iterations = it;
+        result.residual = res;
+        result.residual_relative = reference > 0.0 ? res / reference : 0.0;
+        CFDXG_CUDA(cudaStreamSynchronize(ctx->stream));
+        return result;
+    };
+    // :108-131 failure reports carry the recomputed FP64 residual of x
+    auto failed = [&](int status, int64_t it, double res) {
+        result.status = status;
+        result.iterations = it;
+        result.residual = res;
+        result.residual_relative = b_norm > 0.0 ? res / b_norm
+                                   : (homogeneous > 0.0 ? res / homogeneous
+                                                        : (res == 0.0 ? 0.0 : std::numeric_limits<double>::infinity()));
+        CFDXG_CUDA(cudaStreamSynchronize(ctx->stream));
+        return result;
+    };
+    if (initial <= tol_abs) return finish(CFDXG_CONVERGED, 0, initial);
+    if (setup && !(*setup)()) return failed(CFDXG_NOT_APPLICABLE, 0, initial);
+    E.copy(r, rv);
+    zero_flags();
+    if (!apply()) return failed(CFDXG_NOT_APPLICABLE, 0, initial);
+    dot_check(r, z.get(), kCgRsOld);
+    E.copy(p.get(), z.get());
+    E.fetch(kCgCount);
+    if (E.host(kCgZBad) > 0.0) return failed(CFDXG_NOT_APPLICABLE, 0, initial);
+    double rsold = E.host(kCgRsOld);
+    if (!std::isfinite(rsold)) return failed(CFDXG_DIVERGED, 0, initial);
+    if (!(rsold > 0.0)) return failed(CFDXG_NOT_APPLICABLE, 0, initial);
+
+    double at_last_replacement = std::numeric_limits<double>::infinity();
+    for (int64_t iter = 1; iter <= max_iter; ++iter) {
+        zero_flags();
+        E.spmv(p.get(), Ap.get());
+        E.dot(p.get(), Ap.get(), kCgPAp);
+        k_cg_update<<<gb, kT, 0, ctx->stream>>>(ni, x, r, p.get(), Ap.get(), E.slot(0));
+        check_launch(ctx);
+        if (!apply()) return failed(CFDXG_NOT_APPLICABLE, iter, std::numeric_limits<double>::quiet_NaN());
+        dot_check(r, z.get(), kCgRsNew);
+        E.residual(b, x, rv);
+        E.norm2(rv, kCgRes);
+        E.dot(r, r, kCgRR2);
+        E.fetch(kCgCount);
+        const double pAp = E.host(kCgPAp);
+        const double res = E.host(kCgRes);
+        if (!(pAp > 0.0) || !std::isfinite(pAp)) return failed(CFDXG_NOT_APPLICABLE, iter, res);
+        if (!std::isfinite(rsold / pAp)) return failed(CFDXG_DIVERGED, iter, res);
+        if (E.host(kCgXBad) > 0.0) return failed(CFDXG_DIVERGED, iter, res);
+        if (E.host(kCgZBad) > 0.0) return failed(CFDXG_NOT_APPLICABLE, iter, res);
+        const double rsnew = E.host(kCgRsNew);
+        if (!std::isfinite(rsnew)) return failed(CFDXG_DIVERGED, iter, res);
+        if (res <= tol_abs) return finish(CFDXG_CONVERGED, iter, res);
+        // :399-525 adaptive residual replacement and collapse repair
+        const double rr = std::sqrt(E.host(kCgRR2));
+        const double gap = std::abs(res - rr);
+        const double scale = std::max(res, rr);
+        result.max_true_recursive_gap = std::max(result.max_true_recursive_gap, gap);
+        if (rr > 0.0 && std::isfinite(rr) && std::isfinite(res / rr)) {
+            result.min_true_recursive_ratio = std::min(result.min_true_recursive_ratio, res / rr);
+            result.max_true_recursive_ratio = std::max(result.max_true_recursive_ratio, res / rr);
+        }
+        result.max_true_residual = std::max(result.max_true_residual, res);
+        result.min_true_residual = std::min(result.min_true_residual, res);
+        const bool progress = res < 0.5 * at_last_replacement;
+        const bool collapsed = !(rsnew > 0.0);
+        const bool adaptive = std::isfinite(rr) && scale > 0.0 && gap > 0.25 * scale && progress;
+        const bool repair = collapsed && progress;
+        if (collapsed && !repair) return finish(CFDXG_MAX_ITER_REACHED, iter, res);
+        if (adaptive || repair) {
+            ++result.residual_replacements;
+            at_last_replacement = res;
+            if (result.first_residual_replacement == 0) result.first_residual_replacement = iter;
+            result.last_residual_replacement = iter;
+            E.copy(r, rv);
+            zero_flags();
+            if (!apply()) return failed(CFDXG_NOT_APPLICABLE, iter, res);
+            dot_check(r, z.get(), kCgRsOld);
+            E.copy(p.get(), z.get());
+            E.fetch(kCgCount);
+            const double replaced = E.host(kCgRsOld);
+            if (E.host(kCgZBad) > 0.0 || !std::isfinite(replaced) || !(replaced > 0.0))
+                return failed(CFDXG_NOT_APPLICABLE, iter, res);
+            rsold = replaced;
+            continue;
+        }
+        k_cg_direction<<<gb, kT, 0, ctx->stream>>>(ni, p.get(), z.get(), E.slot(0));
+        check_launch(ctx);
+        CFDXG_CUDA(cudaMemcpyAsync(E.slot(kCgRsOld), E.slot(kCgRsNew), sizeof(double), cudaMemcpyDeviceToDevice,
+                                   ctx->stream));
+        rsold = rsnew;
+    }
+    E.residual(b, x, rv);
+    E.norm2(rv, kCgRes);
+    return finish(CFDXG_MAX_ITER_REACHED, max_iter, E.scalar(kCgRes));
 }
 
 void enqueue_dot(cfdxg_context* ctx, int64_t n, const double* a, const double* b, double* out) {

@@ -48,6 +48,13 @@ KrylovResult gmres_solve(cfdxg_context* ctx, const cfdxg_matrix* A, const double
                          int restart, int64_t max_iter, double tolerance, const RightPreconditioner* pc,
                          const KrylovControls& controls, const IterationObserver* observer = nullptr);
 
+// core/linalg/cg_solver.h:45-560 with a preconditioner object (pc, its j
+// argument unused); `setup`, when given, runs after the initial-residual
+// check as the reference's setup_preconditioner and a false return makes the
+// solve NOT_APPLICABLE.
+KrylovResult cg_solve(cfdxg_context* ctx, const cfdxg_matrix* A, const double* b, double* x, int64_t max_iter,
+                      double tolerance, const RightPreconditioner& pc, const std::function<bool()>* setup);
+
 // Scaled two-pass 2-norm of a device vector (krylov_norm2).
 double device_norm2(cfdxg_context* ctx, const cfdxg_matrix* A, const double* a);
 // Enqueues out = sum_i a_i b_i (deterministic fixed-order reduction) into a device scalar.

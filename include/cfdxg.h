@@ -47,6 +47,7 @@ extern "C" {
 
 /* Krylov / preconditioner / precision choices, numbered as the reference's
  * KrylovModel and PreconditionerModel enums (core/linalg/linear_solver_models.h:20-55). */
+#define CFDXG_KRYLOV_CG 1           /* KrylovModel::CG: SPD systems, cg_solver.h */
 #define CFDXG_KRYLOV_GMRES 3
 #define CFDXG_KRYLOV_FGMRES 4
 #define CFDXG_PC_NONE 1
@@ -274,7 +275,7 @@ int cfdxg_amg_update_values_host(cfdxg_amg* amg, int64_t n, const int64_t* row_o
  * KrylovControls (core/linalg/krylov_controls.h:10-26) and the precision /
  * learned-preconditioner choices of this library. */
 typedef struct {
-    int32_t krylov;                  /* CFDXG_KRYLOV_GMRES / _FGMRES */
+    int32_t krylov;                  /* CFDXG_KRYLOV_CG / _GMRES / _FGMRES */
     int32_t preconditioner;          /* CFDXG_PC_* */
     int32_t gmres_restart;           /* 40 in the reference's request default */
     int32_t precision;               /* CFDXG_PRECISION_* */
@@ -311,14 +312,22 @@ int cfdxg_request_default(cfdxg_request* req);
 /* Replaces solve_linear_system (core/linalg/linear_solver_dispatch.h:227-492) for
  * scalar pressure systems without scaling / null space: builds the requested
  * preconditioner (AMG setup inside, as the reference), solves with
- * right-preconditioned GMRES/FGMRES, then certifies the FP64 physical residual. */
+ * right-preconditioned GMRES/FGMRES or with CG (cg_solver.h:45-560), then
+ * certifies the FP64 physical residual.  CG first measures the matrix
+ * (matrix_diagnostics.h:317-355): not symmetric within 1e-12 max(1, max|a|),
+ * or a diagonal that is not positive, returns CFDXG_NOT_APPLICABLE with x
+ * untouched (linear_solver_dispatch.h:259-267); its AMG keeps the smoother
+ * certificate and is set up only when the initial residual has not already
+ * converged.  CG takes no learned stage. */
 int cfdxg_solve_linear_system(cfdxg_context* ctx, const cfdxg_matrix* A, const double* rhs,
                               double* x, int32_t mem, const cfdxg_request* req,
                               int64_t max_iterations, double tolerance, cfdxg_report* report);
 
 /* Replaces solve_gmres / solve_fgmres with an already set-up preconditioner
  * (core/linalg/gmres_solver.h:28-600, 690-757, setup_preconditioner = false).
- * amg may be NULL (identity). */
+ * amg may be NULL (identity).  With req->krylov == CFDXG_KRYLOV_CG it runs
+ * solve_cg(A, b, x, preconditioner) (cg_solver.h:605-618) on that hierarchy,
+ * or the identity without one. */
 int cfdxg_solve_gmres(cfdxg_context* ctx, const cfdxg_matrix* A, cfdxg_amg* amg,
                       const double* rhs, double* x, int32_t mem, const cfdxg_request* req,
                       int64_t max_iterations, double tolerance, cfdxg_report* report);

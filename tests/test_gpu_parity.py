@@ -274,3 +274,106 @@ def test_simple_outer_iterations_small(ctx):
         out = sl.run_form(ctx, form, m, mesh, g, nu_t, 5, 0.3, None, ctx.synchronize)
         assert all(r["status"] == "converged" for r in out["records"])
         assert out["final_continuity_l2"] < out["first_continuity_l2"]
+
+
+# ---------------------------------------------------------------- CG
+# CG's dots and norms are fixed-order parallel reductions here and sequential
+# sums in the reference, so the iterates agree to rounding, not bit for bit.
+# With AMG (8-10 iterations) the iteration count must match and the pressure
+# agree to REL_TOL; the identity / Jacobi objects take hundreds of iterations,
+# over which rounding differences grow, so there the count may differ by 2 and
+# the pressure by CG_LONG_TOL, each solution certified to the solve tolerance.
+CG_LONG_TOL = 1e-7
+
+
+@pytest.mark.parametrize("pc", ["native_amg", "jacobi", "none"])
+def test_cg_matches_oracle(ctx, oracle, tet_setup, pc):
+    m, mesh, g, (U, rAU, aP, p, fixed, value) = tet_setup
+    A, b, phi, grad = cg.assemble_pressure_correction(mesh, U, rAU, p, 1.0, fixed, value)
+    ro, co, va = A.to_csr()
+    H = None
+    if pc == "native_amg":
+        amg = cg.NativeBoomerAMGPreconditioner(ctx, require_smoother_certificate=True)
+        assert amg.setup(A)
+        H = oracle_hierarchy(oracle, amg)
+    x_ref, rep_ref = oracle.solve_cg(ro, co, va, b, pc, H, max_iterations=3000, tolerance=1e-10)
+    x, rep = cg.solve_linear_system(A, b, krylov="cg", preconditioner=pc, max_iterations=3000, tolerance=1e-10)
+    assert rep["status_name"] == "converged" and rep_ref["status"] == 0
+    assert rep["physical_residual_relative"] <= 1e-10
+    if pc == "native_amg":
+        assert rep["iterations"] == rep_ref["iterations"]
+        assert rel_l2(x, x_ref) <= REL_TOL
+    else:
+        assert abs(rep["iterations"] - rep_ref["iterations"]) <= 2
+        assert rel_l2(x, x_ref) <= CG_LONG_TOL
+
+
+def test_prepared_cg_matches_oracle(ctx, oracle, tet_setup):
+    m, mesh, g, (U, rAU, aP, p, fixed, value) = tet_setup
+    A, b, phi, grad = cg.assemble_pressure_correction(mesh, U, rAU, p, 1.0, fixed, value)
+    ro, co, va = A.to_csr()
+    amg = cg.NativeBoomerAMGPreconditioner(ctx, require_smoother_certificate=True)
+    assert amg.setup(A)
+    x0 = np.random.default_rng(4).standard_normal(A.n) * 1e-2
+    x_ref, rep_ref = oracle.solve_cg(ro, co, va, b, "native_amg", oracle_hierarchy(oracle, amg), x0=x0,
+                                     tolerance=1e-10)
+    x, rep = cg.solve_cg(A, b, x0=x0, amg=amg, tolerance=1e-10)
+    assert rep["status_name"] == "converged"
+    assert rep["iterations"] == rep_ref["iterations"]
+    assert rel_l2(x, x_ref) <= REL_TOL
+
+
+def test_cg_golden_fixture(ctx):
+    # the reference's own CG + native AMG solve of the 4^3 x 6 tet system
+    from pathlib import Path
+    z = dict(np.load(Path(__file__).resolve().parent / "golden" / "pressure_tet4.npz"))
+    A = cg.SparseMatrix.from_csr(ctx, z["row_offsets"], z["columns"], z["values"])
+    x, rep = cg.solve_linear_system(A, z["b"], krylov="cg", max_iterations=1000, tolerance=1e-10)
+    assert rep["status_name"] == "converged"
+    assert rep["iterations"] == int(z["cg_iterations"])
+    assert rel_l2(x, z["cg_x"]) <= REL_TOL
+
+
+def test_cg_rejects_nonsymmetric_or_nonpositive_diagonal(ctx, tet_setup):
+    m, mesh, g, (U, rAU, aP, p, fixed, value) = tet_setup
+    A, b, phi, grad = cg.assemble_pressure_correction(mesh, U, rAU, p, 1.0, fixed, value)
+    ro, co, va = A.to_csr()
+    x0 = np.full(A.n, 0.25)
+    off = next(k for k in range(ro[1]) if co[k] != 0)      # an off-diagonal entry of row 0
+    skew = va.copy()
+    skew[off] *= 1.5
+    diag0 = next(k for k in range(ro[1]) if co[k] == 0)
+    negdiag = va.copy()
+    negdiag[diag0] = -negdiag[diag0]
+    for bad in (skew, negdiag):
+        B = cg.SparseMatrix.from_csr(ctx, ro, co, bad)
+        x, rep = cg.solve_linear_system(B, b, x0=x0, krylov="cg", tolerance=1e-10)
+        assert rep["status_name"] == "not_applicable"
+        assert np.array_equal(x, x0)
+    # the same system with symmetric coefficients is accepted
+    x, rep = cg.solve_linear_system(A, b, krylov="cg", tolerance=1e-10)
+    assert rep["status_name"] == "converged"
+    with pytest.raises(cg.CfdxgError):
+        cg.solve_linear_system(A, b, krylov="cg", learned=cg.LearnedPreconditioner(ctx))
+
+
+# ---------------------------------------------------------------- .cfdxlin replay
+def test_capture_replay_matches_reference_solution(ctx, tmp_path):
+    """A pressure system written by the reference's write_linear_system_capture
+    replays through the library: same CSR and right-hand side, and the solve
+    with the file's tolerance and iteration limit reproduces the reference's
+    solution and iteration count.  The library's own opt-in capture of the
+    same solve is byte-identical to the reference's file."""
+    from pathlib import Path
+    golden = Path(__file__).resolve().parent / "golden"
+    c = cg.read_linear_system_capture(golden / "pressure_tet4.cfdxlin")
+    z = dict(np.load(golden / "pressure_tet4.npz"))
+    A = cg.SparseMatrix.from_csr(ctx, c["row_offsets"], c["columns"], c["values"])
+    path = tmp_path / "replay.cfdxlin"
+    x, rep = cg.solve_linear_system(A, c["rhs"], c["initial_solution"], restart=30,
+                                    max_iterations=c["max_iterations"], tolerance=c["tolerance"],
+                                    linear_capture_path=str(path))
+    assert rep["status_name"] == "converged"
+    assert rep["iterations"] == int(z["iterations"])
+    assert rel_l2(x, z["x"]) <= REL_TOL
+    assert path.read_bytes() == (golden / "pressure_tet4.cfdxlin").read_bytes()
