@@ -229,7 +229,6 @@ def run_cfdxg(args):
         times, iters, errs, fallbacks = [], [], [], []
         launches0 = ctx.kernel_launches
         if form == headline:
-            ctx.profile(True)
             sampler.start()
         for s in range(args.steps):
             k = s % N_RHS
@@ -256,9 +255,19 @@ def run_cfdxg(args):
                 errs.append(float(np.linalg.norm(x - ref_solutions[k]) / np.linalg.norm(ref_solutions[k])))
         if form == headline:
             clocks = sampler.stop()
+            launches = ctx.kernel_launches - launches0
+            # Per-kernel live timing (CUDA events on the library stream around
+            # every kernel class) is a second pass over the same solves: the
+            # events would otherwise sit inside the timed region above.
+            ctx.profile(True)
+            for s in range(args.steps):
+                x_dev.zero_()
+                flush.fill_(float(s))
+                torch.cuda.synchronize()
+                solve_device(amg, req, s % N_RHS)
+            torch.cuda.synchronize()
             prof = ctx.profile_read()
             ctx.profile(False)
-            launches = ctx.kernel_launches - launches0
         forms[form].update(s_per_solve=float(np.mean(times)), s_min=float(np.min(times)),
                            iterations=float(np.mean(iters)),
                            rel_error_vs_fp64=(float(np.max(errs)) if errs else 0.0))

@@ -46,7 +46,7 @@ class AmgOptions(C.Structure):
         ("strength_threshold", C.c_double), ("max_levels", C.c_int32),
         ("require_smoother_certificate", C.c_int32), ("precision", C.c_int32),
         ("coarse_dense_limit", C.c_int32), ("reference_order", C.c_int32),
-        ("coarse_pre_sweeps", C.c_int32), ("coarse_post_sweeps", C.c_int32),
+        ("coarse_pre_sweeps", C.c_int32), ("coarse_post_sweeps", C.c_int32), ("narrow_columns", C.c_int32),
     ]
 
 

@@ -127,9 +127,11 @@ void amg_setup_impl(cfdxg_context* ctx, cfdxg_amg* amg, cfdxg_matrix* A) {
     std::unique_ptr<DevHierarchy<double>> d64;
     std::unique_ptr<DevHierarchy<float>> d32;
     if (amg->opts.precision == CFDXG_PRECISION_FP32_VCYCLE)
-        d32 = upload_hierarchy<float>(ctx, staged, amg->opts.coarse_dense_limit, amg->opts.reference_order != 0);
+        d32 = upload_hierarchy<float>(ctx, staged, amg->opts.coarse_dense_limit, amg->opts.reference_order != 0,
+                                      amg->opts.narrow_columns != 0);
     else
-        d64 = upload_hierarchy<double>(ctx, staged, 0, amg->opts.reference_order != 0);
+        d64 = upload_hierarchy<double>(ctx, staged, 0, amg->opts.reference_order != 0,
+                                       amg->opts.narrow_columns != 0);
     // commit only after every stage succeeded (hypre_amg.cpp:163-236 is transactional)
     amg->host = std::move(staged);
     amg->d64 = std::move(d64);
@@ -341,6 +343,7 @@ extern "C" int cfdxg_amg_options_default(cfdxg_amg_options* o) {
     o->reference_order = 0;
     o->coarse_pre_sweeps = -1;
     o->coarse_post_sweeps = -1;
+    o->narrow_columns = 1;
     return CFDXG_OK;
 }
 

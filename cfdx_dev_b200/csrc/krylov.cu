@@ -101,6 +101,58 @@ __global__ void k_dot(int n, const double* __restrict__ a, const double* __restr
     }
 }
 
+// Modified Gram-Schmidt step fused with the next step's dot: w = w - c v
+// (k_axpy_neg's arithmetic), then out = sum_i u_i w_i over the updated w with
+// k_dot's partition and order -- bit-identical to the two kernels in turn,
+// one pass over w instead of two.
+__global__ void k_axpy_dot(int n, double* __restrict__ w, const double* __restrict__ v, const double* c,
+                           const double* __restrict__ u, double* partial, unsigned* ticket, double* out) {
+    __shared__ double sm[32];
+    const double cc = *c;
+    double s = 0.0;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const double wi = w[i] - cc * v[i];
+        w[i] = wi;
+        s += u[i] * wi;
+    }
+    s = block_sum(s, sm);
+    if (threadIdx.x == 0) partial[blockIdx.x] = s;
+    if (last_block(ticket)) {
+        double t = 0.0;
+        for (int q = threadIdx.x; q < gridDim.x; q += blockDim.x) t += partial[q];
+        t = block_sum(t, sm);
+        if (threadIdx.x == 0) { *out = t; *ticket = 0; }
+    }
+}
+
+// The last Gram-Schmidt step fused with the first pass of the norm: w = w - c v,
+// then k_absmax over the updated w.
+__global__ void k_axpy_absmax(int n, double* __restrict__ w, const double* __restrict__ v, const double* c,
+                              double* partial, unsigned* ticket, double* out_max, double* out_invalid) {
+    __shared__ double sm[32];
+    const double cc = *c;
+    double m = 0.0, bad = 0.0;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const double wi = w[i] - cc * v[i];
+        w[i] = wi;
+        if (!isfinite(wi)) bad = 1.0;
+        m = fmax(m, fabs(wi));
+    }
+    m = block_max(m, sm);
+    bad = block_max(bad, sm);
+    if (threadIdx.x == 0) { partial[2 * blockIdx.x] = m; partial[2 * blockIdx.x + 1] = bad; }
+    if (last_block(ticket)) {
+        double mm = 0.0, bb = 0.0;
+        for (int b = threadIdx.x; b < gridDim.x; b += blockDim.x) {
+            mm = fmax(mm, partial[2 * b]);
+            bb = fmax(bb, partial[2 * b + 1]);
+        }
+        mm = block_max(mm, sm);
+        bb = block_max(bb, sm);
+        if (threadIdx.x == 0) { *out_max = mm; *out_invalid = bb; *ticket = 0; }
+    }
+}
+
 // w = w - c * v   (gmres_solver.h:283 / :289)
 __global__ void k_axpy_neg(int n, double* __restrict__ w, const double* __restrict__ v, const double* c) {
     const double cc = *c;
@@ -191,6 +243,21 @@ public:
     }
     void dot(const double* a, const double* b, int out) {
         k_dot<<<rb(), kT, 0, ctx_->stream>>>(n_, a, b, ctx_->scratch.partial, ctx_->scratch.ticket, slot(out));
+        check_launch(ctx_);
+    }
+    // w -= H[coef] v, then H[out] = u . w
+    void axpy_dot(double* w, const double* v, int coef, const double* u, int out) {
+        k_axpy_dot<<<rb(), kT, 0, ctx_->stream>>>(n_, w, v, slot(coef), u, ctx_->scratch.partial,
+                                                  ctx_->scratch.ticket, slot(out));
+        check_launch(ctx_);
+    }
+    // w -= H[coef] v, then the norm of w into slot out (two passes, as norm2)
+    void axpy_norm2(double* w, const double* v, int coef, int out) {
+        k_axpy_absmax<<<rb(), kT, 0, ctx_->stream>>>(n_, w, v, slot(coef), ctx_->scratch.partial,
+                                                     ctx_->scratch.ticket, slot(kMax), slot(kInvalid));
+        check_launch(ctx_);
+        k_sumsq<<<rb(), kT, 0, ctx_->stream>>>(n_, w, slot(kMax), slot(kInvalid), ctx_->scratch.partial,
+                                               ctx_->scratch.ticket, slot(out));
         check_launch(ctx_);
     }
     void axpy_neg(double* w, const double* v, int coef) {
@@ -463,16 +530,15 @@ KrylovResult gmres_solve(cfdxg_context* ctx, const cfdxg_matrix* A, const double
             }
             E.spmv(z(j), ws->w.get());
             E.norm2(ws->w.get(), kAction);
-            for (int i = 0; i <= j; ++i) {
-                E.dot(v(i), ws->w.get(), kH1 + i);
-                E.axpy_neg(ws->w.get(), v(i), kH1 + i);
-            }
-            for (int i = 0; i <= j; ++i) {
-                E.dot(v(i), ws->w.get(), kH2 + i);
-                E.axpy_neg(ws->w.get(), v(i), kH2 + i);
-            }
-            E.norm2(ws->w.get(), kHnext);
-            E.div(ws->w.get(), kHnext, v(j + 1));
+            // two passes of modified Gram-Schmidt (h = v_i . w; w -= h v_i for
+            // i = 0..j, twice), each update fused with the next dot
+            double* w = ws->w.get();
+            E.dot(v(0), w, kH1);
+            for (int i = 0; i < j; ++i) E.axpy_dot(w, v(i), kH1 + i, v(i + 1), kH1 + i + 1);
+            E.axpy_dot(w, v(j), kH1 + j, v(0), kH2);
+            for (int i = 0; i < j; ++i) E.axpy_dot(w, v(i), kH2 + i, v(i + 1), kH2 + i + 1);
+            E.axpy_norm2(w, v(j), kH2 + j, kHnext);
+            E.div(w, kHnext, v(j + 1));
             const int st = E.fetch(kSlots);
             if (st & kStatusNonFinite) {
                 if (pc) return fail(CFDXG_NOT_APPLICABLE);   // preconditioner produced a non-finite z

@@ -23,6 +23,11 @@ template <class T>
 struct DevLevel {
     int n = 0, nnz = 0, nc = 0;
     DevBuf<int> ro, co;
+    // Narrow columns: when every |column - row| of the level fits in 16 bits,
+    // the columns are stored as int16 offsets from the row (co16) and co is
+    // left empty -- 2 bytes instead of 4 per nonzero on the HBM-bound sweeps.
+    DevBuf<int16_t> co16;
+    bool narrow = false;
     DevBuf<T> va, inv_diag;
     DevBuf<int> p_off, p_col, r_off, r_row;
     DevBuf<T> p_val, r_val;
@@ -141,7 +146,8 @@ void spmv_fp64(cfdxg_context* ctx, const cfdxg_matrix* A, const double* x, doubl
 // hierarchy (vcycle.cu)
 template <class T>
 std::unique_ptr<DevHierarchy<T>> upload_hierarchy(cfdxg_context* ctx, const AmgHierarchy& h,
-                                                  int coarse_dense_limit, bool reference_order);
+                                                  int coarse_dense_limit, bool reference_order,
+                                                  bool narrow_columns);
 template <class T>
 void refresh_hierarchy_values(cfdxg_context* ctx, DevHierarchy<T>& d, const AmgHierarchy& h);
 // z = V-cycle(r); r, z are FP64 device vectors.

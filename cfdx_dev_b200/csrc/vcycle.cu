@@ -54,14 +54,17 @@ __global__ void k_sweep_zero(int n, T omega, const T* __restrict__ inv_diag, con
 // chunks of four entries per lane (~5%), eight lanes per short row with the
 // sum formed in order through shuffles (~4x), and a sliced-ELL copy of the
 // fine level (32-row slices, column-major; ~10%).
-template <class T, int TPR>
-__device__ __forceinline__ T row_dot(int b, int e, int lane, const int* __restrict__ co,
-                                     const T* __restrict__ va, const T* __restrict__ x) {
+//
+// CI is the column index type: int (absolute columns, base 0) or int16_t
+// (offsets from the row, base = the row index).
+template <class T, int TPR, class CI = int>
+__device__ __forceinline__ T row_dot(int b, int e, int lane, const CI* __restrict__ co,
+                                     const T* __restrict__ va, const T* __restrict__ x, int base = 0) {
     T s = T(0);
     // unrolled so several independent (value, column, x) loads are in flight;
     // the additions stay in the same sequential order
 #pragma unroll 4
-    for (int k = b + lane; k < e; k += TPR) s += va[k] * __ldg(x + co[k]);
+    for (int k = b + lane; k < e; k += TPR) s += va[k] * __ldg(x + (base + static_cast<int>(co[k])));
     if (TPR > 1) {
         constexpr int W = TPR < 32 ? TPR : 32;
 #pragma unroll
@@ -84,16 +87,19 @@ __device__ __forceinline__ T row_dot(int b, int e, int lane, const int* __restri
     return s;
 }
 
+template <class CI>
+__device__ __forceinline__ int column_base(int row) { return sizeof(CI) == 2 ? row : 0; }
+
 // x_out = x + omega * (inv_diag * (r - A x))
-template <class T, class XO, int TPR>
-__global__ void k_sweep(int n, const int* __restrict__ ro, const int* __restrict__ co,
+template <class T, class XO, int TPR, class CI>
+__global__ void k_sweep(int n, const int* __restrict__ ro, const CI* __restrict__ co,
                         const T* __restrict__ va, const T* __restrict__ inv_diag,
                         const T* __restrict__ r, const T* __restrict__ x, XO* __restrict__ xo,
                         T omega, int* status) {
     const int g = blockIdx.x * blockDim.x + threadIdx.x;
     const int i = g / TPR, lane = g % TPR;
     const bool valid = i < n;
-    const T s = row_dot<T, TPR>(valid ? ro[i] : 0, valid ? ro[i + 1] : 0, lane, co, va, x);
+    const T s = row_dot<T, TPR, CI>(valid ? ro[i] : 0, valid ? ro[i + 1] : 0, lane, co, va, x, column_base<CI>(i));
     if (!valid || lane != 0) return;
     const T delta = inv_diag[i] * (r[i] - s);
     const T xi = x[i] + omega * delta;
@@ -101,14 +107,14 @@ __global__ void k_sweep(int n, const int* __restrict__ ro, const int* __restrict
     if (!finite_(xi)) atomicOr(status, kStatusNonFinite);
 }
 
-template <class T, int TPR>
-__global__ void k_residual(int n, const int* __restrict__ ro, const int* __restrict__ co,
+template <class T, int TPR, class CI>
+__global__ void k_residual(int n, const int* __restrict__ ro, const CI* __restrict__ co,
                            const T* __restrict__ va, const T* __restrict__ r,
                            const T* __restrict__ x, T* __restrict__ res) {
     const int g = blockIdx.x * blockDim.x + threadIdx.x;
     const int i = g / TPR, lane = g % TPR;
     const bool valid = i < n;
-    const T s = row_dot<T, TPR>(valid ? ro[i] : 0, valid ? ro[i + 1] : 0, lane, co, va, x);
+    const T s = row_dot<T, TPR, CI>(valid ? ro[i] : 0, valid ? ro[i + 1] : 0, lane, co, va, x, column_base<CI>(i));
     if (valid && lane == 0) res[i] = r[i] - s;
 }
 
@@ -320,24 +326,38 @@ inline double account(double bytes) {
 template <class T>
 const char* tname(const char* fp64, const char* fp32) { return sizeof(T) == 8 ? fp64 : fp32; }
 
+template <class T>
+double column_bytes(const DevLevel<T>& L) { return L.narrow ? 2.0 : 4.0; }
+
 template <class T, class XO>
 void launch_sweep(cfdxg_context* ctx, const DevLevel<T>& L, const T* r, const T* x, XO* xo, T omega, int* status) {
     // A values + columns, row offsets, x / r / inv_diag reads, x_out write
-    const double bytes = account((sizeof(T) + 4.0) * L.nnz + 4.0 * (L.n + 1) + 3.0 * sizeof(T) * L.n + sizeof(XO) * L.n);
+    const double bytes = account((sizeof(T) + column_bytes(L)) * L.nnz + 4.0 * (L.n + 1) + 3.0 * sizeof(T) * L.n +
+                                 sizeof(XO) * L.n);
     ProfScope ps(ctx, tname<T>("jacobi_sweep_fp64_L0", "jacobi_sweep_fp32_L0"), bytes);
     const int64_t threads = static_cast<int64_t>(L.n) * L.tpr;
-    CFDXG_TPR_SWITCH(L.tpr, (k_sweep<T, XO, TPR><<<blocks_for(threads, kT), kT, 0, ctx->stream>>>(
-        L.n, L.ro.get(), L.co.get(), L.va.get(), L.inv_diag.get(), r, x, xo, omega, status)));
+    if (L.narrow) {
+        CFDXG_TPR_SWITCH(L.tpr, (k_sweep<T, XO, TPR, int16_t><<<blocks_for(threads, kT), kT, 0, ctx->stream>>>(
+            L.n, L.ro.get(), L.co16.get(), L.va.get(), L.inv_diag.get(), r, x, xo, omega, status)));
+    } else {
+        CFDXG_TPR_SWITCH(L.tpr, (k_sweep<T, XO, TPR, int><<<blocks_for(threads, kT), kT, 0, ctx->stream>>>(
+            L.n, L.ro.get(), L.co.get(), L.va.get(), L.inv_diag.get(), r, x, xo, omega, status)));
+    }
     check_launch(ctx);
 }
 
 template <class T>
 void launch_residual(cfdxg_context* ctx, const DevLevel<T>& L, const T* r, const T* x, T* res) {
-    const double bytes = account((sizeof(T) + 4.0) * L.nnz + 4.0 * (L.n + 1) + 3.0 * sizeof(T) * L.n);
+    const double bytes = account((sizeof(T) + column_bytes(L)) * L.nnz + 4.0 * (L.n + 1) + 3.0 * sizeof(T) * L.n);
     ProfScope ps(ctx, tname<T>("residual_fp64_L0", "residual_fp32_L0"), bytes);
     const int64_t threads = static_cast<int64_t>(L.n) * L.tpr;
-    CFDXG_TPR_SWITCH(L.tpr, (k_residual<T, TPR><<<blocks_for(threads, kT), kT, 0, ctx->stream>>>(
-        L.n, L.ro.get(), L.co.get(), L.va.get(), r, x, res)));
+    if (L.narrow) {
+        CFDXG_TPR_SWITCH(L.tpr, (k_residual<T, TPR, int16_t><<<blocks_for(threads, kT), kT, 0, ctx->stream>>>(
+            L.n, L.ro.get(), L.co16.get(), L.va.get(), r, x, res)));
+    } else {
+        CFDXG_TPR_SWITCH(L.tpr, (k_residual<T, TPR, int><<<blocks_for(threads, kT), kT, 0, ctx->stream>>>(
+            L.n, L.ro.get(), L.co.get(), L.va.get(), r, x, res)));
+    }
     check_launch(ctx);
 }
 
@@ -401,16 +421,48 @@ void upload_level_values(cfdxg_context* ctx, DevLevel<T>& D, const AmgLevel& H) 
     CFDXG_CUDA(cudaStreamSynchronize(ctx->stream));
 }
 
+// Narrow columns (int16 offsets from the row) for a level whose every
+// |column - row| fits; the coarsest level keeps absolute columns for its
+// direct solvers.
+template <class T>
+void upload_columns(cfdxg_context* ctx, DevLevel<T>& D, const AmgLevel& H, bool allow_narrow) {
+    const int n = static_cast<int>(H.A.n);
+    bool narrow = allow_narrow;
+    for (int i = 0; i < n && narrow; ++i)
+        for (uint32_t k = H.A.ro[i]; k < H.A.ro[i + 1]; ++k) {
+            const int64_t d = static_cast<int64_t>(H.A.co[k]) - i;
+            if (d < INT16_MIN || d > INT16_MAX) { narrow = false; break; }
+        }
+    D.narrow = narrow;
+    if (narrow) {
+        std::vector<int16_t> c16(H.A.co.size());
+        for (int i = 0; i < n; ++i)
+            for (uint32_t k = H.A.ro[i]; k < H.A.ro[i + 1]; ++k)
+                c16[k] = static_cast<int16_t>(static_cast<int64_t>(H.A.co[k]) - i);
+        D.co16.upload(c16, ctx->stream);
+        D.co.release();
+    } else {
+        std::vector<int> co(H.A.co.begin(), H.A.co.end());
+        D.co.upload(co, ctx->stream);
+        D.co16.release();
+    }
+    CFDXG_CUDA(cudaStreamSynchronize(ctx->stream));
+}
+
 template <class T>
 void upload_level(cfdxg_context* ctx, DevLevel<T>& D, const AmgLevel& H, bool with_transfer,
-                  bool reference_order) {
+                  bool reference_order, bool narrow_columns) {
     cudaStream_t s = ctx->stream;
     D.n = static_cast<int>(H.A.n);
     D.nnz = static_cast<int>(H.A.co.size());
     D.tpr = choose_tpr(D.nnz, D.n, reference_order);
-    std::vector<int> ro(H.A.ro.begin(), H.A.ro.end()), co(H.A.co.begin(), H.A.co.end());
+    std::vector<int> ro(H.A.ro.begin(), H.A.ro.end());
     D.ro.upload(ro, s);
-    D.co.upload(co, s);
+    // Narrow columns pay on short rows (one thread per row: 21.1 vs 22.5 us per
+    // fine-level FP32 sweep at 64^3); on the long rows that a warp shares they
+    // measured 10-20% slower (58.9 -> 70.6 us on the 77,039-row level), so
+    // those keep int32 columns.
+    upload_columns(ctx, D, H, with_transfer && narrow_columns && D.tpr == 1);
     upload_level_values(ctx, D, H);
     D.r.resize(D.n); D.x.resize(D.n); D.x2.resize(D.n); D.res.resize(D.n);
     if (with_transfer) {
@@ -565,7 +617,8 @@ void ensure_graph(cfdxg_context* ctx, DevHierarchy<T>& d) {
 
 template <class T>
 std::unique_ptr<DevHierarchy<T>> upload_hierarchy(cfdxg_context* ctx, const AmgHierarchy& h,
-                                                  int coarse_dense_limit, bool reference_order) {
+                                                  int coarse_dense_limit, bool reference_order,
+                                                  bool narrow_columns) {
     auto d = std::make_unique<DevHierarchy<T>>();
     d->omega = static_cast<T>(h.omega);
     d->pre = h.options.pre;
@@ -589,7 +642,7 @@ std::unique_ptr<DevHierarchy<T>> upload_hierarchy(cfdxg_context* ctx, const AmgH
     if (d->coarse_mode == 0 && h.levels[used - 1].A.n <= kDenseDirectLimit) d->coarse_mode = 1;
     d->used = used;
     d->L.resize(used);
-    for (int l = 0; l < used; ++l) upload_level(ctx, d->L[l], h.levels[l], l + 1 < used, reference_order);
+    for (int l = 0; l < used; ++l) upload_level(ctx, d->L[l], h.levels[l], l + 1 < used, reference_order, narrow_columns);
     if (d->coarse_mode == 2) build_dense_inverse(ctx, *d, h.levels[used - 1]);
     return d;
 }
@@ -707,8 +760,8 @@ void vcycle_apply(cfdxg_context* ctx, DevHierarchy<T>& d, const double* r, doubl
 template <class T>
 void destroy_hierarchy(DevHierarchy<T>* d) { delete d; }
 
-template std::unique_ptr<DevHierarchy<double>> upload_hierarchy<double>(cfdxg_context*, const AmgHierarchy&, int, bool);
-template std::unique_ptr<DevHierarchy<float>> upload_hierarchy<float>(cfdxg_context*, const AmgHierarchy&, int, bool);
+template std::unique_ptr<DevHierarchy<double>> upload_hierarchy<double>(cfdxg_context*, const AmgHierarchy&, int, bool, bool);
+template std::unique_ptr<DevHierarchy<float>> upload_hierarchy<float>(cfdxg_context*, const AmgHierarchy&, int, bool, bool);
 template void refresh_hierarchy_values<double>(cfdxg_context*, DevHierarchy<double>&, const AmgHierarchy&);
 template void refresh_hierarchy_values<float>(cfdxg_context*, DevHierarchy<float>&, const AmgHierarchy&);
 template void set_hierarchy_values_device<double>(cfdxg_context*, DevHierarchy<double>&, const DevRefresh&, double);

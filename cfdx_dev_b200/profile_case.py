@@ -54,14 +54,17 @@ def main(argv=None):
     ap.add_argument("--n", type=int, default=48, help="lattice size (cells = 6 n^3)")
     ap.add_argument("--mode", choices=["vcycle", "solve"], default="solve")
     ap.add_argument("--precision", choices=["fp32_vcycle", "fp64"], default="fp32_vcycle")
+    ap.add_argument("--wide-columns", action="store_true", help="int32 columns on every level (narrow_columns = 0)")
+    ap.add_argument("--cycles", type=int, default=3, help="V-cycle applications in --mode vcycle")
     args = ap.parse_args(argv)
     ctx = cg.Context(0)
     m, mesh, (U, rAU, aP, p, fixed, value), A, b = build_system(ctx, args.n)
-    amg = cg.NativeBoomerAMGPreconditioner(ctx, precision=args.precision)
+    amg = cg.NativeBoomerAMGPreconditioner(ctx, precision=args.precision,
+                                           narrow_columns=0 if args.wide_columns else 1)
     if not amg.setup(A):
         raise SystemExit(amg.last_error())
     if args.mode == "vcycle":
-        for _ in range(3):
+        for _ in range(args.cycles):
             z = amg.apply(b)
         print(f"vcycle n={args.n} cells={A.n} levels={amg.hierarchy_level_sizes()} |z|={np.linalg.norm(z):.6e}")
         return

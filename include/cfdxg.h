@@ -226,6 +226,11 @@ typedef struct {
                                         reference; FP32 cycle -- 0 / 1 (the fine level keeps
                                         pre_sweeps / post_sweeps).  With 0 pre-sweeps a level
                                         restricts its right-hand side directly (x = 0). */
+    int32_t narrow_columns;          /* 1 (default): short-row levels (one thread per row)
+                                        whose every |column - row| fits in 16 bits store int16
+                                        column offsets (2 bytes less per nonzero read); 0:
+                                        int32 columns everywhere.  The arithmetic is the same
+                                        either way. */
 } cfdxg_amg_options;
 
 int cfdxg_amg_options_default(cfdxg_amg_options* opts);
