@@ -10,10 +10,12 @@ share the matrix; one step solves one of them, cycling.  The AMG hierarchy is
 built once per matrix (setup seconds are reported separately) and every solve
 starts from p' = 0.
 
-Forms timed: plain FP64 AMG-GMRES (the reference's algorithm), FP32 V-cycle
-inside FP64 FGMRES, and -- when trained weights are present -- the learned
-message-passing preconditioner in front of the FP32 V-cycle.  `value` is the
-headline form (learned+FP32 if available, else FP32 V-cycle).
+Forms timed: plain FP64 AMG-GMRES (the reference's algorithm, two-pass
+modified Gram-Schmidt), FP32 V-cycle inside FP64 FGMRES, and -- when trained
+weights are present -- the learned message-passing preconditioner in front of
+the FP32 V-cycle; the two FGMRES forms orthogonalise with two-pass classical
+Gram-Schmidt.  `value` is the headline form (learned+FP32 if available, else
+FP32 V-cycle).
 
 Inputs are larger than L2 (the hierarchy alone is > 2 GB), and L2 is also
 flushed before every timed step.  Rank-local device timing with CUDA events on
@@ -207,7 +209,11 @@ def run_cfdxg(args):
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=dev)   # 256 MB > L2
 
     def request(krylov, learned):
-        return cg.make_request(krylov, "native_amg", RESTART, "fp64", net if learned else None)
+        # The plain form is the reference's algorithm (two-pass modified
+        # Gram-Schmidt); the FGMRES forms use two-pass classical Gram-Schmidt.
+        ortho = 0 if krylov == "gmres" else 1
+        return cg.make_request(krylov, "native_amg", RESTART, "fp64", net if learned else None,
+                               orthogonalization=ortho)
 
     def solve_device(amg, req, k):
         rep = N.Report()

@@ -61,7 +61,7 @@ class Request(C.Structure):
         ("adaptive_restart", C.c_int32), ("residual_replacement", C.c_int32),
         ("residual_replacement_period", C.c_int64), ("residual_replacement_gap_ratio", C.c_double),
         ("target_reduction_per_cycle", C.c_double), ("learned", C.c_void_p),
-        ("learned_applications", C.c_int32),
+        ("learned_applications", C.c_int32), ("orthogonalization", C.c_int32),
     ]
 
 

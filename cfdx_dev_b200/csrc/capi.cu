@@ -92,6 +92,7 @@ KrylovControls controls_from(const cfdxg_request& r) {
     c.residual_replacement_period = r.residual_replacement_period;
     c.residual_replacement_gap_ratio = r.residual_replacement_gap_ratio;
     c.target_reduction_per_cycle = r.target_reduction_per_cycle;
+    c.classical_gram_schmidt = r.orthogonalization == CFDXG_ORTHO_CGS2;
     return c;
 }
 
@@ -673,6 +674,8 @@ void validate_request(const cfdxg_request& r) {
     if (r.learned && r.preconditioner != CFDXG_PC_NATIVE_AMG)
         throw Error(CFDXG_ERR_INVALID_ARGUMENT, "the learned preconditioner runs in front of native AMG");
     if (r.learned_applications < 0) throw Error(CFDXG_ERR_INVALID_ARGUMENT, "learned_applications must be >= 0");
+    if (r.orthogonalization != CFDXG_ORTHO_MGS2 && r.orthogonalization != CFDXG_ORTHO_CGS2)
+        throw Error(CFDXG_ERR_INVALID_ARGUMENT, "unknown orthogonalization");
 }
 
 // measure_matrix_characteristics' symmetry and positive-diagonal test, on the device.

@@ -30,6 +30,33 @@ struct Error : std::runtime_error {
                                  std::string(#call) + ": " + cudaGetErrorString(e_));     \
     } while (0)
 
+// Programmatic dependent launch (sm_90+): a kernel launched with launch_pdl
+// may be scheduled while its predecessor on the stream drains.  It lets its
+// own dependents schedule early (pdl_trigger) and waits for the predecessor's
+// completion and memory flush (pdl_wait) before it reads anything the
+// predecessor wrote.  Both are no-ops for an ordinary launch.
+__device__ __forceinline__ void pdl_trigger() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void pdl_entry() {
+    pdl_trigger();
+    pdl_wait();
+}
+
+template <typename... KArgs, typename... Args>
+inline void launch_pdl(cudaStream_t stream, void (*kern)(KArgs...), dim3 grid, dim3 block, Args... args) {
+    cudaLaunchConfig_t cfg{};
+    cfg.gridDim = grid;
+    cfg.blockDim = block;
+    cfg.dynamicSmemBytes = 0;
+    cfg.stream = stream;
+    cudaLaunchAttribute attr{};
+    attr.id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr.val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = &attr;
+    cfg.numAttrs = 1;
+    CFDXG_CUDA(cudaLaunchKernelEx(&cfg, kern, static_cast<KArgs>(args)...));
+}
+
 constexpr int kReduceThreads = 256;
 constexpr int kMaxReduceBlocks = 592;   // 4 x 148 SMs: fixed partition => deterministic sums
 

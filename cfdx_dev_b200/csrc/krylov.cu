@@ -35,6 +35,7 @@ enum Slot : int {
 
 __global__ void k_absmax(int n, const double* __restrict__ a, double* partial, unsigned* ticket,
                          double* out_max, double* out_invalid) {
+    pdl_entry();
     __shared__ double sm[32];
     double m = 0.0, bad = 0.0;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
@@ -60,6 +61,7 @@ __global__ void k_absmax(int n, const double* __restrict__ a, double* partial, u
 // out = scale * sqrt(sum (a_i / scale)^2), NaN on invalid input, 0 when scale == 0.
 __global__ void k_sumsq(int n, const double* __restrict__ a, const double* scale_p,
                         const double* invalid_p, double* partial, unsigned* ticket, double* out) {
+    pdl_entry();
     __shared__ double sm[32];
     const double scale = *scale_p;
     double s = 0.0;
@@ -88,6 +90,7 @@ __global__ void k_sumsq(int n, const double* __restrict__ a, const double* scale
 
 __global__ void k_dot(int n, const double* __restrict__ a, const double* __restrict__ b, double* partial,
                       unsigned* ticket, double* out) {
+    pdl_entry();
     __shared__ double sm[32];
     double s = 0.0;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) s += a[i] * b[i];
@@ -107,6 +110,7 @@ __global__ void k_dot(int n, const double* __restrict__ a, const double* __restr
 // one pass over w instead of two.
 __global__ void k_axpy_dot(int n, double* __restrict__ w, const double* __restrict__ v, const double* c,
                            const double* __restrict__ u, double* partial, unsigned* ticket, double* out) {
+    pdl_entry();
     __shared__ double sm[32];
     const double cc = *c;
     double s = 0.0;
@@ -129,6 +133,7 @@ __global__ void k_axpy_dot(int n, double* __restrict__ w, const double* __restri
 // then k_absmax over the updated w.
 __global__ void k_axpy_absmax(int n, double* __restrict__ w, const double* __restrict__ v, const double* c,
                               double* partial, unsigned* ticket, double* out_max, double* out_invalid) {
+    pdl_entry();
     __shared__ double sm[32];
     const double cc = *c;
     double m = 0.0, bad = 0.0;
@@ -153,8 +158,84 @@ __global__ void k_axpy_absmax(int n, double* __restrict__ w, const double* __res
     }
 }
 
+// ---- classical Gram-Schmidt (the CGS2 option): up to kChunk basis vectors per launch
+constexpr int kChunk = 16;
+
+// out[q] = v_{i0+q} . w for q < c, one pass over w.  Each block's partial sums
+// land in partial[q * gridDim.x + block]; the last block adds them in block
+// order (deterministic, as k_dot).
+__global__ void k_multidot(int n, const double* __restrict__ V, int i0, int c, const double* __restrict__ w,
+                           double* partial, unsigned* ticket, double* out) {
+    pdl_entry();
+    __shared__ double sm[32];
+    double acc[kChunk];
+#pragma unroll
+    for (int q = 0; q < kChunk; ++q) acc[q] = 0.0;
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
+        const double wk = w[k];
+#pragma unroll
+        for (int q = 0; q < kChunk; ++q)
+            if (q < c) acc[q] += V[static_cast<size_t>(i0 + q) * n + k] * wk;
+    }
+#pragma unroll
+    for (int q = 0; q < kChunk; ++q) {
+        if (q >= c) break;
+        const double s = block_sum(acc[q], sm);
+        if (threadIdx.x == 0) partial[q * gridDim.x + blockIdx.x] = s;
+    }
+    if (last_block(ticket)) {
+        for (int q = 0; q < c; ++q) {
+            double t = 0.0;
+            for (int b = threadIdx.x; b < gridDim.x; b += blockDim.x) t += partial[q * gridDim.x + b];
+            t = block_sum(t, sm);
+            if (threadIdx.x == 0) out[q] = t;
+        }
+        if (threadIdx.x == 0) *ticket = 0;
+    }
+}
+
+// w -= sum_{q<c} h[q] v_{i0+q}, subtracting in q order per element; with
+// absmax, also the first pass of the norm of the updated w (as k_absmax).
+template <bool ABSMAX>
+__global__ void k_multi_axpy(int n, const double* __restrict__ V, int i0, int c, const double* h,
+                             double* __restrict__ w, double* partial, unsigned* ticket, double* out_max,
+                             double* out_invalid) {
+    pdl_entry();
+    __shared__ double sm[32];
+    __shared__ double hs[kChunk];
+    if (threadIdx.x < c) hs[threadIdx.x] = h[threadIdx.x];
+    __syncthreads();
+    double m = 0.0, bad = 0.0;
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
+        double wk = w[k];
+#pragma unroll
+        for (int q = 0; q < kChunk; ++q)
+            if (q < c) wk = wk - hs[q] * V[static_cast<size_t>(i0 + q) * n + k];
+        w[k] = wk;
+        if (ABSMAX) {
+            if (!isfinite(wk)) bad = 1.0;
+            m = fmax(m, fabs(wk));
+        }
+    }
+    if (!ABSMAX) return;
+    m = block_max(m, sm);
+    bad = block_max(bad, sm);
+    if (threadIdx.x == 0) { partial[2 * blockIdx.x] = m; partial[2 * blockIdx.x + 1] = bad; }
+    if (last_block(ticket)) {
+        double mm = 0.0, bb = 0.0;
+        for (int b = threadIdx.x; b < gridDim.x; b += blockDim.x) {
+            mm = fmax(mm, partial[2 * b]);
+            bb = fmax(bb, partial[2 * b + 1]);
+        }
+        mm = block_max(mm, sm);
+        bb = block_max(bb, sm);
+        if (threadIdx.x == 0) { *out_max = mm; *out_invalid = bb; *ticket = 0; }
+    }
+}
+
 // w = w - c * v   (gmres_solver.h:283 / :289)
 __global__ void k_axpy_neg(int n, double* __restrict__ w, const double* __restrict__ v, const double* c) {
+    pdl_entry();
     const double cc = *c;
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i < n) w[i] = w[i] - cc * v[i];
@@ -162,6 +243,7 @@ __global__ void k_axpy_neg(int n, double* __restrict__ w, const double* __restri
 
 // v = w / d  when d > 0   (gmres_solver.h:183 and :322)
 __global__ void k_div(int n, const double* __restrict__ w, const double* d, double* __restrict__ v) {
+    pdl_entry();
     const double dd = *d;
     if (!(dd > 0.0)) return;
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -172,6 +254,7 @@ __global__ void k_div(int n, const double* __restrict__ w, const double* d, doub
 __global__ void k_true_residual(int n, const int* __restrict__ ro, const int* __restrict__ co,
                                 const double* __restrict__ va, const double* __restrict__ b,
                                 const double* __restrict__ x, double* __restrict__ r) {
+    pdl_entry();
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     double s = 0.0;
@@ -183,6 +266,7 @@ __global__ void k_true_residual(int n, const int* __restrict__ ro, const int* __
 // out = x + sum_j y_j z_j, accumulated in j order per element (gmres_solver.h:497-501)
 __global__ void k_update(int n, const double* __restrict__ x, const double* __restrict__ Z,
                          const double* __restrict__ y, int used, double* __restrict__ out) {
+    pdl_entry();
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     double v = x[i];
@@ -204,6 +288,7 @@ struct Workspace {
     int64_t n = 0;
     int m = 0;
     DevBuf<double> V, Z, w, r, ax, best, trial, tmp;
+    DevBuf<double> mpartial;   // kChunk x kMaxReduceBlocks partial sums of the multi-dot
 };
 
 Workspace& workspace(cfdxg_context* ctx, int64_t n, int m) {
@@ -218,6 +303,7 @@ Workspace& workspace(cfdxg_context* ctx, int64_t n, int m) {
         ws->Z.resize(static_cast<size_t>(mm) * n);
         ws->w.resize(n); ws->r.resize(n); ws->ax.resize(n); ws->best.resize(n);
         ws->trial.resize(n); ws->tmp.resize(n);
+        ws->mpartial.resize(static_cast<size_t>(kChunk) * kMaxReduceBlocks);
         ws->n = n;
         ws->m = mm;
     }
@@ -234,42 +320,71 @@ public:
     int rb() const { return reduce_blocks(n_); }
 
     void norm2(const double* a, int out) {
-        k_absmax<<<rb(), kT, 0, ctx_->stream>>>(n_, a, ctx_->scratch.partial, ctx_->scratch.ticket,
+        launch_pdl(ctx_->stream, k_absmax, rb(), kT, n_, a, ctx_->scratch.partial, ctx_->scratch.ticket,
                                                 slot(kMax), slot(kInvalid));
         check_launch(ctx_);
-        k_sumsq<<<rb(), kT, 0, ctx_->stream>>>(n_, a, slot(kMax), slot(kInvalid), ctx_->scratch.partial,
+        launch_pdl(ctx_->stream, k_sumsq, rb(), kT, n_, a, slot(kMax), slot(kInvalid), ctx_->scratch.partial,
                                                ctx_->scratch.ticket, slot(out));
         check_launch(ctx_);
     }
     void dot(const double* a, const double* b, int out) {
-        k_dot<<<rb(), kT, 0, ctx_->stream>>>(n_, a, b, ctx_->scratch.partial, ctx_->scratch.ticket, slot(out));
+        launch_pdl(ctx_->stream, k_dot, rb(), kT, n_, a, b, ctx_->scratch.partial, ctx_->scratch.ticket, slot(out));
         check_launch(ctx_);
     }
     // w -= H[coef] v, then H[out] = u . w
     void axpy_dot(double* w, const double* v, int coef, const double* u, int out) {
-        k_axpy_dot<<<rb(), kT, 0, ctx_->stream>>>(n_, w, v, slot(coef), u, ctx_->scratch.partial,
+        launch_pdl(ctx_->stream, k_axpy_dot, rb(), kT, n_, w, v, slot(coef), u, ctx_->scratch.partial,
                                                   ctx_->scratch.ticket, slot(out));
         check_launch(ctx_);
     }
     // w -= H[coef] v, then the norm of w into slot out (two passes, as norm2)
     void axpy_norm2(double* w, const double* v, int coef, int out) {
-        k_axpy_absmax<<<rb(), kT, 0, ctx_->stream>>>(n_, w, v, slot(coef), ctx_->scratch.partial,
+        launch_pdl(ctx_->stream, k_axpy_absmax, rb(), kT, n_, w, v, slot(coef), ctx_->scratch.partial,
                                                      ctx_->scratch.ticket, slot(kMax), slot(kInvalid));
         check_launch(ctx_);
-        k_sumsq<<<rb(), kT, 0, ctx_->stream>>>(n_, w, slot(kMax), slot(kInvalid), ctx_->scratch.partial,
+        launch_pdl(ctx_->stream, k_sumsq, rb(), kT, n_, w, slot(kMax), slot(kInvalid), ctx_->scratch.partial,
                                                ctx_->scratch.ticket, slot(out));
         check_launch(ctx_);
     }
+    // h[out + i] = v_i . w for i <= j (classical Gram-Schmidt), in chunks
+    void multidot(const double* V, int count, const double* w, int out, double* mpartial) {
+        for (int i0 = 0; i0 < count; i0 += kChunk) {
+            const int c = std::min(kChunk, count - i0);
+            launch_pdl(ctx_->stream, k_multidot, rb(), kT, n_, V, i0, c, w, mpartial, ctx_->scratch.ticket,
+                                                      slot(out + i0));
+            check_launch(ctx_);
+        }
+    }
+    // w -= sum_i h[coef + i] v_i, then (last) the norm of w into slot out
+    void multi_axpy(const double* V, int count, int coef, double* w, int norm_out) {
+        for (int i0 = 0; i0 < count; i0 += kChunk) {
+            const int c = std::min(kChunk, count - i0);
+            const bool last = i0 + c == count && norm_out >= 0;
+            if (last)
+                launch_pdl(ctx_->stream, k_multi_axpy<true>, rb(), kT, n_, V, i0, c, slot(coef + i0), w,
+                                                                 ctx_->scratch.partial, ctx_->scratch.ticket,
+                                                                 slot(kMax), slot(kInvalid));
+            else
+                launch_pdl(ctx_->stream, k_multi_axpy<false>, rb(), kT, n_, V, i0, c, slot(coef + i0), w, nullptr,
+                                                                  nullptr, nullptr, nullptr);
+            check_launch(ctx_);
+        }
+        if (norm_out >= 0) {
+            launch_pdl(ctx_->stream, k_sumsq, rb(), kT, n_, w, slot(kMax), slot(kInvalid), ctx_->scratch.partial,
+                                                   ctx_->scratch.ticket, slot(norm_out));
+            check_launch(ctx_);
+        }
+    }
     void axpy_neg(double* w, const double* v, int coef) {
-        k_axpy_neg<<<gb(), kT, 0, ctx_->stream>>>(n_, w, v, slot(coef));
+        launch_pdl(ctx_->stream, k_axpy_neg, gb(), kT, n_, w, v, slot(coef));
         check_launch(ctx_);
     }
     void div(const double* w, int d, double* v) {
-        k_div<<<gb(), kT, 0, ctx_->stream>>>(n_, w, slot(d), v);
+        launch_pdl(ctx_->stream, k_div, gb(), kT, n_, w, slot(d), v);
         check_launch(ctx_);
     }
     void residual(const double* b, const double* x, double* r) {
-        k_true_residual<<<gb(), kT, 0, ctx_->stream>>>(n_, A_->ro.get(), A_->co.get(), A_->va.get(), b, x, r);
+        launch_pdl(ctx_->stream, k_true_residual, gb(), kT, n_, A_->ro.get(), A_->co.get(), A_->va.get(), b, x, r);
         check_launch(ctx_);
     }
     void spmv(const double* x, double* y) { spmv_fp64(ctx_, A_, x, y); }
@@ -280,7 +395,7 @@ public:
         if (used > 0)
             CFDXG_CUDA(cudaMemcpyAsync(slot(kY), y.data(), sizeof(double) * used, cudaMemcpyHostToDevice,
                                        ctx_->stream));
-        k_update<<<gb(), kT, 0, ctx_->stream>>>(n_, x, Z, slot(kY), used, out);
+        launch_pdl(ctx_->stream, k_update, gb(), kT, n_, x, Z, slot(kY), used, out);
         check_launch(ctx_);
     }
     void neg(const double* a, double* b) {
@@ -533,11 +648,19 @@ KrylovResult gmres_solve(cfdxg_context* ctx, const cfdxg_matrix* A, const double
             // two passes of modified Gram-Schmidt (h = v_i . w; w -= h v_i for
             // i = 0..j, twice), each update fused with the next dot
             double* w = ws->w.get();
-            E.dot(v(0), w, kH1);
-            for (int i = 0; i < j; ++i) E.axpy_dot(w, v(i), kH1 + i, v(i + 1), kH1 + i + 1);
-            E.axpy_dot(w, v(j), kH1 + j, v(0), kH2);
-            for (int i = 0; i < j; ++i) E.axpy_dot(w, v(i), kH2 + i, v(i + 1), kH2 + i + 1);
-            E.axpy_norm2(w, v(j), kH2 + j, kHnext);
+            if (controls.classical_gram_schmidt) {
+                // two passes of classical Gram-Schmidt: h = V^T w; w -= V h, twice
+                E.multidot(V, j + 1, w, kH1, ws->mpartial.get());
+                E.multi_axpy(V, j + 1, kH1, w, -1);
+                E.multidot(V, j + 1, w, kH2, ws->mpartial.get());
+                E.multi_axpy(V, j + 1, kH2, w, kHnext);
+            } else {
+                E.dot(v(0), w, kH1);
+                for (int i = 0; i < j; ++i) E.axpy_dot(w, v(i), kH1 + i, v(i + 1), kH1 + i + 1);
+                E.axpy_dot(w, v(j), kH1 + j, v(0), kH2);
+                for (int i = 0; i < j; ++i) E.axpy_dot(w, v(i), kH2 + i, v(i + 1), kH2 + i + 1);
+                E.axpy_norm2(w, v(j), kH2 + j, kHnext);
+            }
             E.div(w, kHnext, v(j + 1));
             const int st = E.fetch(kSlots);
             if (st & kStatusNonFinite) {
@@ -862,7 +985,7 @@ KrylovResult cg_solve(cfdxg_context* ctx, const cfdxg_matrix* A, const double* b
 }
 
 void enqueue_dot(cfdxg_context* ctx, int64_t n, const double* a, const double* b, double* out) {
-    k_dot<<<reduce_blocks(n), kT, 0, ctx->stream>>>(static_cast<int>(n), a, b, ctx->scratch.partial,
+    launch_pdl(ctx->stream, k_dot, reduce_blocks(n), kT, static_cast<int>(n), a, b, ctx->scratch.partial,
                                                     ctx->scratch.ticket, out);
     check_launch(ctx);
 }

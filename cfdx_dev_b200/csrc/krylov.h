@@ -16,6 +16,10 @@ struct KrylovControls {
     bool residual_replacement = true;
     double residual_replacement_gap_ratio = 10.0;
     double target_reduction_per_cycle = 0.1;
+    // Two passes of classical instead of modified Gram-Schmidt: the same
+    // projections, formed as h = V^T w and w -= V h (two passes over the basis
+    // per pass instead of 2(j+1)); not the reference's order of operations.
+    bool classical_gram_schmidt = false;
 };
 
 // core/linalg/solver_status.h:45-72

@@ -12,6 +12,7 @@ constexpr int kT = 256;
 __global__ void k_spmv64(int n, const int* __restrict__ ro, const int* __restrict__ co,
                          const double* __restrict__ va, const double* __restrict__ x,
                          double* __restrict__ y) {
+    pdl_entry();
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     double s = 0.0;
@@ -23,7 +24,7 @@ __global__ void k_spmv64(int n, const int* __restrict__ ro, const int* __restric
 
 void spmv_fp64(cfdxg_context* ctx, const cfdxg_matrix* A, const double* x, double* y) {
     ProfScope ps(ctx, "spmv_fp64", 12.0 * A->nnz + 4.0 * (A->n + 1) + 16.0 * A->n);
-    k_spmv64<<<blocks_for(A->n, kT), kT, 0, ctx->stream>>>(static_cast<int>(A->n), A->ro.get(), A->co.get(),
+    launch_pdl(ctx->stream, k_spmv64, blocks_for(A->n, kT), kT, static_cast<int>(A->n), A->ro.get(), A->co.get(),
                                                            A->va.get(), x, y);
     check_launch(ctx);
 }

@@ -36,6 +36,7 @@ __device__ __forceinline__ bool finite_(T v) { return isfinite(v); }
 template <class T, class R>
 __global__ void k_sweep_zero(int n, T omega, const T* __restrict__ inv_diag, const R* __restrict__ r,
                              T* __restrict__ r_copy, T* __restrict__ x, int* status) {
+    pdl_entry();
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     const T ri = static_cast<T>(r[i]);
@@ -96,6 +97,7 @@ __global__ void k_sweep(int n, const int* __restrict__ ro, const CI* __restrict_
                         const T* __restrict__ va, const T* __restrict__ inv_diag,
                         const T* __restrict__ r, const T* __restrict__ x, XO* __restrict__ xo,
                         T omega, int* status) {
+    pdl_entry();
     const int g = blockIdx.x * blockDim.x + threadIdx.x;
     const int i = g / TPR, lane = g % TPR;
     const bool valid = i < n;
@@ -120,6 +122,7 @@ template <class T, int TPR, class CI>
 __global__ void k_residual(int n, const int* __restrict__ ro, const CI* __restrict__ co,
                            const T* __restrict__ va, const T* __restrict__ r,
                            const T* __restrict__ x, T* __restrict__ res) {
+    pdl_entry();
     const int g = blockIdx.x * blockDim.x + threadIdx.x;
     const int i = g / TPR, lane = g % TPR;
     const bool valid = i < n;
@@ -137,6 +140,7 @@ __global__ void k_residual(int n, const int* __restrict__ ro, const CI* __restri
 template <class T, int TPR>
 __global__ void k_restrict(int nc, const int* __restrict__ r_off, const int* __restrict__ r_row,
                            const T* __restrict__ r_val, const T* __restrict__ res, T* __restrict__ rc) {
+    pdl_entry();
     const int g = blockIdx.x * blockDim.x + threadIdx.x;
     const int c = g / TPR, lane = g % TPR;
     const bool valid = c < nc;
@@ -151,6 +155,7 @@ template <class T, int TPR>
 __global__ void k_prolong(int n, const int* __restrict__ p_off, const int* __restrict__ p_col,
                           const T* __restrict__ p_val, const T* __restrict__ xc, T* __restrict__ x,
                           int* status) {
+    pdl_entry();
     const int g = blockIdx.x * blockDim.x + threadIdx.x;
     const int i = g / TPR, lane = g % TPR;
     if constexpr (TPR == 1) {
@@ -172,6 +177,7 @@ __global__ void k_prolong(int n, const int* __restrict__ p_off, const int* __res
 
 template <class T, class XO>
 __global__ void k_copy_cast(int n, const T* __restrict__ a, XO* __restrict__ b) {
+    pdl_entry();
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i < n) b[i] = static_cast<XO>(a[i]);
 }
@@ -233,6 +239,7 @@ __global__ void k_dense_lu_reference(int n, const int* __restrict__ ro, const in
 template <class T>
 __global__ void k_dense_inverse_apply(int n, const double* __restrict__ inv, const T* __restrict__ r,
                                       T* __restrict__ x, int* status) {
+    pdl_entry();
     const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int lane = threadIdx.x & 31;
     if (warp >= n) return;
@@ -352,10 +359,10 @@ void launch_sweep(cfdxg_context* ctx, const DevLevel<T>& L, const T* r, const T*
     ProfScope ps(ctx, tname<T>("jacobi_sweep_fp64_L0", "jacobi_sweep_fp32_L0"), bytes);
     const int64_t threads = static_cast<int64_t>(L.n) * L.tpr;
     if (L.narrow) {
-        CFDXG_TPR_SWITCH(L.tpr, (k_sweep<T, XO, TPR, int16_t><<<blocks_for(threads, kT), kT, 0, ctx->stream>>>(
+        CFDXG_TPR_SWITCH(L.tpr, (launch_pdl(ctx->stream, k_sweep<T, XO, TPR, int16_t>, blocks_for(threads, kT), kT, 
             L.n, L.ro.get(), L.co16.get(), L.va.get(), L.inv_diag.get(), r, x, xo, omega, status)));
     } else {
-        CFDXG_TPR_SWITCH(L.tpr, (k_sweep<T, XO, TPR, int><<<blocks_for(threads, kT), kT, 0, ctx->stream>>>(
+        CFDXG_TPR_SWITCH(L.tpr, (launch_pdl(ctx->stream, k_sweep<T, XO, TPR, int>, blocks_for(threads, kT), kT, 
             L.n, L.ro.get(), L.co.get(), L.va.get(), L.inv_diag.get(), r, x, xo, omega, status)));
     }
     check_launch(ctx);
@@ -367,10 +374,10 @@ void launch_residual(cfdxg_context* ctx, const DevLevel<T>& L, const T* r, const
     ProfScope ps(ctx, tname<T>("residual_fp64_L0", "residual_fp32_L0"), bytes);
     const int64_t threads = static_cast<int64_t>(L.n) * L.tpr;
     if (L.narrow) {
-        CFDXG_TPR_SWITCH(L.tpr, (k_residual<T, TPR, int16_t><<<blocks_for(threads, kT), kT, 0, ctx->stream>>>(
+        CFDXG_TPR_SWITCH(L.tpr, (launch_pdl(ctx->stream, k_residual<T, TPR, int16_t>, blocks_for(threads, kT), kT, 
             L.n, L.ro.get(), L.co16.get(), L.va.get(), r, x, res)));
     } else {
-        CFDXG_TPR_SWITCH(L.tpr, (k_residual<T, TPR, int><<<blocks_for(threads, kT), kT, 0, ctx->stream>>>(
+        CFDXG_TPR_SWITCH(L.tpr, (launch_pdl(ctx->stream, k_residual<T, TPR, int>, blocks_for(threads, kT), kT, 
             L.n, L.ro.get(), L.co.get(), L.va.get(), r, x, res)));
     }
     check_launch(ctx);
@@ -382,7 +389,7 @@ void launch_restrict(cfdxg_context* ctx, const DevLevel<T>& L, const T* res, T* 
     const double bytes = account((sizeof(T) + 4.0) * pnnz + 4.0 * (L.nc + 1) + sizeof(T) * (L.n + L.nc));
     ProfScope ps(ctx, tname<T>("restrict_fp64_L0", "restrict_fp32_L0"), bytes);
     const int64_t threads = static_cast<int64_t>(L.nc) * L.tpr_r;
-    CFDXG_TPR_SWITCH(L.tpr_r, (k_restrict<T, TPR><<<blocks_for(threads, kT), kT, 0, ctx->stream>>>(
+    CFDXG_TPR_SWITCH(L.tpr_r, (launch_pdl(ctx->stream, k_restrict<T, TPR>, blocks_for(threads, kT), kT, 
         L.nc, L.r_off.get(), L.r_row.get(), L.r_val.get(), res, rc)));
     check_launch(ctx);
 }
@@ -393,7 +400,7 @@ void launch_prolong(cfdxg_context* ctx, const DevLevel<T>& L, const T* xc, T* x,
     const double bytes = account((sizeof(T) + 4.0) * pnnz + 4.0 * (L.n + 1) + sizeof(T) * (L.nc + 2.0 * L.n));
     ProfScope ps(ctx, tname<T>("prolong_fp64_L0", "prolong_fp32_L0"), bytes);
     const int64_t threads = static_cast<int64_t>(L.n) * L.tpr_p;
-    CFDXG_TPR_SWITCH(L.tpr_p, (k_prolong<T, TPR><<<blocks_for(threads, kT), kT, 0, ctx->stream>>>(
+    CFDXG_TPR_SWITCH(L.tpr_p, (launch_pdl(ctx->stream, k_prolong<T, TPR>, blocks_for(threads, kT), kT, 
         L.n, L.p_off.get(), L.p_col.get(), L.p_val.get(), xc, x, status)));
     check_launch(ctx);
 }
@@ -554,7 +561,7 @@ void sweeps_from_zero(cfdxg_context* ctx, DevHierarchy<T>& d, DevLevel<T>& L, co
         CFDXG_CUDA(cudaMemsetAsync(x, 0, sizeof(T) * L.n, s));
     } else {
         account(3.0 * sizeof(T) * L.n);
-        k_sweep_zero<T, T><<<gb, kT, 0, s>>>(L.n, d.omega, L.inv_diag.get(), r_in, nullptr, x, d.status);
+        launch_pdl(s, k_sweep_zero<T, T>, gb, kT, L.n, d.omega, L.inv_diag.get(), r_in, nullptr, x, d.status);
         check_launch(ctx);
         for (int k = 1; k < sweeps; ++k) {
             launch_sweep<T, T>(ctx, L, r_in, x, x2, d.omega, d.status);
@@ -578,7 +585,7 @@ void enqueue_from(cfdxg_context* ctx, DevHierarchy<T>& d, int l) {
             L.xout = L.x.get();
         } else if (d.coarse_mode == 2) {
             account(8.0 * L.n * L.n + 2.0 * sizeof(T) * L.n);
-            k_dense_inverse_apply<T><<<blocks_for(static_cast<int64_t>(L.n) * 32, kT), kT, 0, s>>>(
+            launch_pdl(s, k_dense_inverse_apply<T>, blocks_for(static_cast<int64_t>(L.n) * 32, kT), kT, 
                 L.n, d.dense.get(), L.r.get(), L.x.get(), d.status);
             check_launch(ctx);
             L.xout = L.x.get();
@@ -716,10 +723,10 @@ void vcycle_apply(cfdxg_context* ctx, DevHierarchy<T>& d, const double* r, doubl
     const int gb = blocks_for(L.n, kT);
     if (d.used == 1) {
         // single-level hierarchy: the coarsest treatment applies to the fine level
-        k_copy_cast<double, T><<<gb, kT, 0, s>>>(L.n, r, L.r.get());
+        launch_pdl(s, k_copy_cast<double, T>, gb, kT, L.n, r, L.r.get());
         check_launch(ctx);
         enqueue_from(ctx, d, 0);
-        k_copy_cast<T, double><<<gb, kT, 0, s>>>(L.n, L.xout, z);
+        launch_pdl(s, k_copy_cast<T, double>, gb, kT, L.n, L.xout, z);
         check_launch(ctx);
         return;
     }
@@ -735,12 +742,12 @@ void vcycle_apply(cfdxg_context* ctx, DevHierarchy<T>& d, const double* r, doubl
     }
     if (d.pre == 0) {
         if (!std::is_same<T, double>::value) {
-            k_copy_cast<double, T><<<gb, kT, 0, s>>>(L.n, r, L.r.get());
+            launch_pdl(s, k_copy_cast<double, T>, gb, kT, L.n, r, L.r.get());
             check_launch(ctx);
         }
         CFDXG_CUDA(cudaMemsetAsync(x, 0, sizeof(T) * L.n, s));
     } else {
-        k_sweep_zero<T, double><<<gb, kT, 0, s>>>(L.n, d.omega, L.inv_diag.get(), r,
+        launch_pdl(s, k_sweep_zero<T, double>, gb, kT, L.n, d.omega, L.inv_diag.get(), r,
                                                   std::is_same<T, double>::value ? nullptr : L.r.get(), x,
                                                   d.status);
         check_launch(ctx);
@@ -759,7 +766,7 @@ void vcycle_apply(cfdxg_context* ctx, DevHierarchy<T>& d, const double* r, doubl
     count_launch(ctx, d.graph_kernels);
     launch_prolong<T>(ctx, L, C.xout, x, d.status);
     if (d.post == 0) {
-        k_copy_cast<T, double><<<gb, kT, 0, s>>>(L.n, x, z);
+        launch_pdl(s, k_copy_cast<T, double>, gb, kT, L.n, x, z);
         check_launch(ctx);
         return;
     }

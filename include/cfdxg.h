@@ -55,6 +55,8 @@ extern "C" {
 #define CFDXG_PC_NATIVE_AMG 6
 #define CFDXG_PRECISION_FP64 0      /* the reference's plain FP64 V-cycle */
 #define CFDXG_PRECISION_FP32_VCYCLE 1  /* FP32 V-cycle inside FP64 FGMRES */
+#define CFDXG_ORTHO_MGS2 0          /* two-pass modified Gram-Schmidt, gmres_solver.h:270-295 */
+#define CFDXG_ORTHO_CGS2 1          /* two-pass classical Gram-Schmidt (no reference counterpart) */
 
 typedef struct cfdxg_context cfdxg_context;
 typedef struct cfdxg_mesh cfdxg_mesh;
@@ -295,6 +297,10 @@ typedef struct {
     int32_t learned_applications;    /* the learned stage serves the first this-many Arnoldi
                                         vectors of each restart cycle (the V-cycle alone the
                                         rest); 0: every application.  Default 1. */
+    int32_t orthogonalization;       /* CFDXG_ORTHO_MGS2 (default, the reference's order) or
+                                        CFDXG_ORTHO_CGS2: h = V^T w, w -= V h, twice -- the same
+                                        projections in 4 passes over the basis per Arnoldi step
+                                        instead of 4(j+1); rounding differs from MGS2's */
 } cfdxg_request;
 
 /* Mirrors SolverResult (core/linalg/solver_status.h:45-72) + LinearSolveReport. */

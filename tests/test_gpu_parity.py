@@ -377,3 +377,38 @@ def test_capture_replay_matches_reference_solution(ctx, tmp_path):
     assert rep["iterations"] == int(z["iterations"])
     assert rel_l2(x, z["x"]) <= REL_TOL
     assert path.read_bytes() == (golden / "pressure_tet4.cfdxlin").read_bytes()
+
+
+# ---------------------------------------------------------------- CGS2 option
+def test_classical_gram_schmidt_matches_oracle(ctx, oracle, tet_setup):
+    """orthogonalization = CGS2 forms the same projections as the reference's
+    two-pass MGS with different rounding: the FP64 AMG-GMRES iterate agrees
+    with the oracle's to REL_TOL at the same iteration count, and the FP32
+    V-cycle FGMRES still reaches the FP64 certificate."""
+    m, mesh, g, (U, rAU, aP, p, fixed, value) = tet_setup
+    A, b, phi, grad = cg.assemble_pressure_correction(mesh, U, rAU, p, 1.0, fixed, value)
+    ro, co, va = A.to_csr()
+    amg = cg.NativeBoomerAMGPreconditioner(ctx)
+    assert amg.setup(A)
+    x_ref, rep_ref = oracle.solve_gmres(ro, co, va, b, oracle_hierarchy(oracle, amg), restart=30, tolerance=1e-8)
+    x, rep = cg.solve_gmres(A, b, amg=amg, restart=30, tolerance=1e-8, orthogonalization=1)
+    assert rep["status_name"] == "converged"
+    assert rep["iterations"] == rep_ref["iterations"]
+    assert rel_l2(x, x_ref) <= REL_TOL
+    amg32 = cg.NativeBoomerAMGPreconditioner(ctx, precision="fp32_vcycle")
+    assert amg32.setup(A)
+    x_m, rep_m = cg.solve_fgmres(A, b, amg=amg32, restart=30, tolerance=1e-8)
+    x_c, rep_c = cg.solve_fgmres(A, b, amg=amg32, restart=30, tolerance=1e-8, orthogonalization=1)
+    assert rep_c["status_name"] == "converged" and rep_c["physical_residual_relative"] <= 1e-8
+    assert abs(rep_c["iterations"] - rep_m["iterations"]) <= 1
+    assert rel_l2(x_c, x_ref) < 1e-6
+    # Arnoldi cycles longer than one 16-vector chunk: Jacobi-preconditioned GMRES(40)
+    kw = dict(krylov="gmres", preconditioner="jacobi", restart=40, tolerance=1e-8, max_iterations=4000)
+    x0, rep0 = cg.solve_linear_system(A, b, **kw)
+    x1, rep1 = cg.solve_linear_system(A, b, orthogonalization=1, **kw)
+    assert rep1["status_name"] == rep0["status_name"] == "converged"
+    assert rep0["iterations"] > 40
+    assert abs(rep1["iterations"] - rep0["iterations"]) <= max(2, 0.05 * rep0["iterations"])
+    assert rel_l2(x1, x0) < 1e-6
+    with pytest.raises(cg.CfdxgError):
+        cg.solve_gmres(A, b, amg=amg, orthogonalization=7)
