@@ -14,6 +14,8 @@
 // Inference runs each round as one fused kernel: the neighbour gather builds
 // [h, a] in shared memory as BF16 and both MLP layers run on the tensor cores
 // (mma.sync m16n8k16, BF16 operands, FP32 accumulation); the state h stays FP32.
+// The encoder is folded into the first round (h0 formed from r where it is
+// read) and the readout into the last, so inference is four kernels.
 #include <cuda_bf16.h>
 
 #include <cmath>
@@ -185,24 +187,65 @@ constexpr int kSegCap = 128;           // staged couplings per 16-cell tile
 constexpr int kRoundWarps = 6;
 constexpr int kRoundThreads = 32 * kRoundWarps;
 
+// x_i = [r_i / s, f_V, f_P, f_D] packed as one float4 per cell (k_encode's
+// input, 16 bytes), so the first round reads it instead of a 128-byte h0 row.
+__global__ void k_pack_input(int n, const double* __restrict__ r, const double* __restrict__ rr,
+                             const float* __restrict__ feats, float4* __restrict__ xin) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const double s = sqrt(*rr / n);
+    const float x0 = s > 0.0 ? static_cast<float>(r[i] / s) : 0.0f;
+    xin[i] = make_float4(x0, feats[i], feats[n + i], feats[2 * n + i]);
+}
+
+// The first round's input state h0 = relu(W_in x + b_in), formed where the
+// round reads it (k_encode's arithmetic) instead of being written by a
+// separate kernel and read back: one lane's quarter-row (four features).
+struct Encoder {
+    const float4* xin;
+    float w[4][4], b[4];
+    __device__ __forceinline__ void load(const float4* xin_, const float* P, int quarter) {
+        xin = xin_;
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            const int f = 4 * quarter + q;
+            b[q] = P[OFF_BIN + f];
+#pragma unroll
+            for (int c = 0; c < 4; ++c) w[q][c] = P[OFF_WIN + f * 4 + c];
+        }
+    }
+    __device__ __forceinline__ float4 h0(int j) const {
+        const float4 x = xin[j];
+        float o[4];
+#pragma unroll
+        for (int q = 0; q < 4; ++q)
+            o[q] = fmaxf(b[q] + w[q][0] * x.x + w[q][1] * x.y + w[q][2] * x.z + w[q][3] * x.w, 0.0f);
+        return make_float4(o[0], o[1], o[2], o[3]);
+    }
+};
+
 // Gather of one 16-cell tile: sH = h (FP32), sU = [h, a] (BF16), a_i = sum_j w_ij h_j.
 // Lanes 8q..8q+7 take cell 4 * pass + q, each lane one 16-byte quarter-row.
 // STAGED: the tile's couplings are in sIdx / sW (index k - seg_b); otherwise
-// they are read from global memory.
-template <bool STAGED>
+// they are read from global memory.  FIRST: h is the encoder's h0.
+template <bool STAGED, bool FIRST>
 __device__ __forceinline__ void gather_tile(int c0, int cells, int rb, int re, int seg_b, const int* sIdx,
                                             const float* sW, const int* __restrict__ gco,
                                             const float* __restrict__ gew, const float* __restrict__ h_in,
-                                            float (*sH)[F], __nv_bfloat16 (*sU)[kUPad]) {
+                                            const Encoder& enc, float (*sH)[F], __nv_bfloat16 (*sU)[kUPad]) {
     const int lane = threadIdx.x & 31;
     const float4* h4 = reinterpret_cast<const float4*>(h_in);
     const int grp = lane >> 3, quarter = lane & 7;
+    auto hrow = [&](int j) -> float4 {
+        if constexpr (FIRST) return enc.h0(j);
+        else return h4[static_cast<size_t>(j) * (F / 4) + quarter];
+    };
 #pragma unroll 1
     for (int pass = 0; pass < kTileCells / 4; ++pass) {
         const int r = pass * 4 + grp;
         const int b = __shfl_sync(0xffffffffu, rb, r), e = __shfl_sync(0xffffffffu, re, r);
         float4 hv = make_float4(0.f, 0.f, 0.f, 0.f), av = make_float4(0.f, 0.f, 0.f, 0.f);
-        if (r < cells) hv = h4[static_cast<size_t>(c0 + r) * (F / 4) + quarter];
+        if (r < cells) hv = hrow(c0 + r);
         int k = b;
         for (; k + 4 <= e; k += 4) {
             int j[4];
@@ -214,7 +257,7 @@ __device__ __forceinline__ void gather_tile(int c0, int cells, int rb, int re, i
             }
             float4 v[4];
 #pragma unroll
-            for (int u = 0; u < 4; ++u) v[u] = h4[static_cast<size_t>(j[u]) * (F / 4) + quarter];
+            for (int u = 0; u < 4; ++u) v[u] = hrow(j[u]);
 #pragma unroll
             for (int u = 0; u < 4; ++u) {
                 av.x += w[u] * v[u].x; av.y += w[u] * v[u].y; av.z += w[u] * v[u].z; av.w += w[u] * v[u].w;
@@ -223,7 +266,7 @@ __device__ __forceinline__ void gather_tile(int c0, int cells, int rb, int re, i
         for (; k < e; ++k) {
             const int j = STAGED ? sIdx[k - seg_b] : gco[k];
             const float w = STAGED ? sW[k - seg_b] : gew[k];
-            const float4 v = h4[static_cast<size_t>(j) * (F / 4) + quarter];
+            const float4 v = hrow(j);
             av.x += w * v.x; av.y += w * v.y; av.z += w * v.z; av.w += w * v.w;
         }
         *reinterpret_cast<float4*>(&sH[r][4 * quarter]) = hv;
@@ -235,10 +278,16 @@ __device__ __forceinline__ void gather_tile(int c0, int cells, int rb, int re, i
     }
 }
 
+// One round.  FIRST: the input state is formed from r by the encoder (no h0
+// in memory).  LAST: the new state goes straight to the readout,
+// out_i = s (w_out . h_i + b_out) / a_ii, instead of to h_out.
+template <bool FIRST, bool LAST>
 __global__ void __launch_bounds__(kRoundThreads) k_round_gather_tc(
     int n, const int* __restrict__ gro, const int* __restrict__ gco, const float* __restrict__ gew,
     const float* __restrict__ h_in, float* __restrict__ h_out, const __nv_bfloat16* __restrict__ W1g,
-    const __nv_bfloat16* __restrict__ W2g, const float* __restrict__ Pr) {
+    const __nv_bfloat16* __restrict__ W2g, const float* __restrict__ Pr, const float* __restrict__ P,
+    const double* __restrict__ r, const double* __restrict__ rr, const float* __restrict__ feats,
+    const double* __restrict__ diag, double* __restrict__ yout) {
     __shared__ __align__(16) __nv_bfloat16 sW1[F][kUPad];
     __shared__ __align__(16) __nv_bfloat16 sW2[F][kW2Pad];
     __shared__ __align__(16) __nv_bfloat16 sU[kRoundWarps][kTileCells][kUPad];
@@ -270,9 +319,15 @@ __global__ void __launch_bounds__(kRoundThreads) k_round_gather_tc(
         rb = gro[c0 + lane];
         re = gro[c0 + lane + 1];
     }
+    Encoder enc;
+    if constexpr (FIRST) enc.load(reinterpret_cast<const float4*>(feats), P, lane & 7);
     __syncwarp();
-    if (staged) gather_tile<true>(c0, cells, rb, re, seg_b, sIdx[warp], sW[warp], gco, gew, h_in, sH[warp], sU[warp]);
-    else gather_tile<false>(c0, cells, rb, re, seg_b, sIdx[warp], sW[warp], gco, gew, h_in, sH[warp], sU[warp]);
+    if (staged)
+        gather_tile<true, FIRST>(c0, cells, rb, re, seg_b, sIdx[warp], sW[warp], gco, gew, h_in, enc, sH[warp],
+                                 sU[warp]);
+    else
+        gather_tile<false, FIRST>(c0, cells, rb, re, seg_b, sIdx[warp], sW[warp], gco, gew, h_in, enc, sH[warp],
+                                  sU[warp]);
     __syncwarp();
     const int g = lane >> 2, t = lane & 3;
     float acc[4][4];
@@ -323,13 +378,37 @@ __global__ void __launch_bounds__(kRoundThreads) k_round_gather_tc(
         }
     }
     const int rowa = g, rowb = g + 8;
+    if constexpr (LAST) {
+        // readout: row sums over this lane's columns, then across the 4 lanes of the row
+        float ya = 0.0f, yb = 0.0f;
 #pragma unroll
-    for (int j = 0; j < 4; ++j) {
-        const int col = 8 * j + 2 * t;
-        if (rowa < cells)
-            *reinterpret_cast<float2*>(&h_out[static_cast<size_t>(c0 + rowa) * F + col]) = make_float2(out[j][0], out[j][1]);
-        if (rowb < cells)
-            *reinterpret_cast<float2*>(&h_out[static_cast<size_t>(c0 + rowb) * F + col]) = make_float2(out[j][2], out[j][3]);
+        for (int j = 0; j < 4; ++j) {
+            const int col = 8 * j + 2 * t;
+            const float w0 = P[OFF_WOUT + col], w1 = P[OFF_WOUT + col + 1];
+            ya += w0 * out[j][0] + w1 * out[j][1];
+            yb += w0 * out[j][2] + w1 * out[j][3];
+        }
+        ya += __shfl_xor_sync(0xffffffffu, ya, 1);
+        ya += __shfl_xor_sync(0xffffffffu, ya, 2);
+        yb += __shfl_xor_sync(0xffffffffu, yb, 1);
+        yb += __shfl_xor_sync(0xffffffffu, yb, 2);
+        if (t == 0) {
+            const double s = sqrt(*rr / n);
+            const float bo = P[OFF_BOUT];
+            if (rowa < cells) yout[c0 + rowa] = s * static_cast<double>(ya + bo) / diag[c0 + rowa];
+            if (rowb < cells) yout[c0 + rowb] = s * static_cast<double>(yb + bo) / diag[c0 + rowb];
+        }
+    } else {
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            const int col = 8 * j + 2 * t;
+            if (rowa < cells)
+                *reinterpret_cast<float2*>(&h_out[static_cast<size_t>(c0 + rowa) * F + col]) =
+                    make_float2(out[j][0], out[j][1]);
+            if (rowb < cells)
+                *reinterpret_cast<float2*>(&h_out[static_cast<size_t>(c0 + rowb) * F + col]) =
+                    make_float2(out[j][2], out[j][3]);
+        }
     }
 }
 
@@ -547,10 +626,13 @@ void infer(cfdxg_context* ctx, cfdxg_mpnn* net, const double* r, double* out) {
     cudaStream_t s = ctx->stream;
     double* rr = scalar(ctx, 0);
     enqueue_dot(ctx, n, r, r, rr);
+    // the packed first-round input x (16 bytes per cell) in the first quarter
+    // of hA: the first round reads it and writes hB, and hA is next written by
+    // the second round
+    float4* xin = reinterpret_cast<float4*>(net->hA.get());
     {
-        ProfScope ps(ctx, "mpnn_encode", (8.0 + 12.0 + 4.0 * F) * n);
-        k_encode<<<blocks_for(static_cast<int64_t>(n) * 8, 256), 256, 0, s>>>(n, r, rr, net->feats.get(),
-                                                                              net->params.get(), net->hA.get());
+        ProfScope ps(ctx, "mpnn_pack_input", (8.0 + 12.0 + 16.0) * n);
+        k_pack_input<<<blocks_for(n, 256), 256, 0, s>>>(n, r, rr, net->feats.get(), xin);
         check_launch(ctx);
     }
     float* hin = net->hA.get();
@@ -558,19 +640,23 @@ void infer(cfdxg_context* ctx, cfdxg_mpnn* net, const double* r, double* out) {
     const int tiles = (n + kTileCells - 1) / kTileCells;
     for (int k = 0; k < R; ++k) {
         const __nv_bfloat16* w = net->wbf.get() + static_cast<size_t>(k) * 3 * F * F;
-        // compulsory bytes: h read and written once, the coupling list once
-        ProfScope ps(ctx, "mpnn_round_gather_tc",
-                     2.0 * sizeof(float) * F * n + 4.0 * (n + 1) + 8.0 * static_cast<double>(net->gco.size()));
-        k_round_gather_tc<<<(tiles + kRoundWarps - 1) / kRoundWarps, kRoundThreads, 0, s>>>(
+        const bool first = k == 0, last = k == R - 1;
+        // compulsory bytes: the state read (r and the cell features in the
+        // first round) and written (the output and diagonal in the last), the
+        // coupling list once
+        const double in_bytes = first ? 16.0 * n : sizeof(float) * F * n;
+        const double out_bytes = last ? 16.0 * n : sizeof(float) * F * n;
+        ProfScope ps(ctx, first ? "mpnn_round_first_tc" : (last ? "mpnn_round_last_tc" : "mpnn_round_gather_tc"),
+                     in_bytes + out_bytes + 4.0 * (n + 1) + 8.0 * static_cast<double>(net->gco.size()));
+        auto kern = first ? k_round_gather_tc<true, false>
+                          : (last ? k_round_gather_tc<false, true> : k_round_gather_tc<false, false>);
+        kern<<<(tiles + kRoundWarps - 1) / kRoundWarps, kRoundThreads, 0, s>>>(
             n, net->gro.get(), net->gco.get(), net->gew.get(), hin, hout, w, w + 2 * F * F,
-            net->params.get() + ROUND0 + k * ROUND_SIZE);
+            net->params.get() + ROUND0 + k * ROUND_SIZE, net->params.get(), r, rr,
+            first ? reinterpret_cast<const float*>(xin) : nullptr, net->diag.get(), out);
         check_launch(ctx);
         std::swap(hin, hout);
     }
-    ProfScope ps(ctx, "mpnn_readout", (4.0 * F + 16.0) * n);
-    k_readout<<<blocks_for(static_cast<int64_t>(n) * 8, 256), 256, 0, s>>>(n, hin, net->params.get(), rr,
-                                                                            net->diag.get(), out);
-    check_launch(ctx);
 }
 
 // Training forward for one sample; keeps activations in H, AG, Z.
