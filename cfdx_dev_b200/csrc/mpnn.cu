@@ -13,7 +13,8 @@
 // combined in a fixed order per block and blocks in a fixed order at the end.
 // Inference runs each round as one fused kernel: the neighbour gather builds
 // [h, a] in shared memory as BF16 and both MLP layers run on the tensor cores
-// (mma.sync m16n8k16, BF16 operands, FP32 accumulation); the state h stays FP32.
+// (mma.sync m16n8k16, BF16 operands, FP32 accumulation); the state h is
+// stored as BF16 between rounds and carried in FP32 within one.
 // The encoder is folded into the first round (h0 formed from r where it is
 // read) and the readout into the last, so inference is four kernels.
 #include <cuda_bf16.h>
@@ -228,17 +229,24 @@ struct Encoder {
 // Lanes 8q..8q+7 take cell 4 * pass + q, each lane one 16-byte quarter-row.
 // STAGED: the tile's couplings are in sIdx / sW (index k - seg_b); otherwise
 // they are read from global memory.  FIRST: h is the encoder's h0.
+__device__ __forceinline__ float4 unpack_bf16x4(uint2 u) {
+    const float2 a = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162*>(&u.x));
+    const float2 b = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162*>(&u.y));
+    return make_float4(a.x, a.y, b.x, b.y);
+}
+
 template <bool STAGED, bool FIRST>
 __device__ __forceinline__ void gather_tile(int c0, int cells, int rb, int re, int seg_b, const int* sIdx,
                                             const float* sW, const int* __restrict__ gco,
-                                            const float* __restrict__ gew, const float* __restrict__ h_in,
+                                            const float* __restrict__ gew, const __nv_bfloat16* __restrict__ h_in,
                                             const Encoder& enc, float (*sH)[F], __nv_bfloat16 (*sU)[kUPad]) {
     const int lane = threadIdx.x & 31;
-    const float4* h4 = reinterpret_cast<const float4*>(h_in);
+    // the state between rounds is BF16: a lane's quarter-row is 8 bytes
+    const uint2* h8 = reinterpret_cast<const uint2*>(h_in);
     const int grp = lane >> 3, quarter = lane & 7;
     auto hrow = [&](int j) -> float4 {
         if constexpr (FIRST) return enc.h0(j);
-        else return h4[static_cast<size_t>(j) * (F / 4) + quarter];
+        else return unpack_bf16x4(h8[static_cast<size_t>(j) * (F / 4) + quarter]);
     };
 #pragma unroll 1
     for (int pass = 0; pass < kTileCells / 4; ++pass) {
@@ -284,7 +292,7 @@ __device__ __forceinline__ void gather_tile(int c0, int cells, int rb, int re, i
 template <bool FIRST, bool LAST>
 __global__ void __launch_bounds__(kRoundThreads) k_round_gather_tc(
     int n, const int* __restrict__ gro, const int* __restrict__ gco, const float* __restrict__ gew,
-    const float* __restrict__ h_in, float* __restrict__ h_out, const __nv_bfloat16* __restrict__ W1g,
+    const __nv_bfloat16* __restrict__ h_in, __nv_bfloat16* __restrict__ h_out, const __nv_bfloat16* __restrict__ W1g,
     const __nv_bfloat16* __restrict__ W2g, const float* __restrict__ Pr, const float* __restrict__ P,
     const double* __restrict__ r, const double* __restrict__ rr, const float* __restrict__ feats,
     const double* __restrict__ diag, double* __restrict__ yout) {
@@ -403,11 +411,11 @@ __global__ void __launch_bounds__(kRoundThreads) k_round_gather_tc(
         for (int j = 0; j < 4; ++j) {
             const int col = 8 * j + 2 * t;
             if (rowa < cells)
-                *reinterpret_cast<float2*>(&h_out[static_cast<size_t>(c0 + rowa) * F + col]) =
-                    make_float2(out[j][0], out[j][1]);
+                *reinterpret_cast<uint32_t*>(&h_out[static_cast<size_t>(c0 + rowa) * F + col]) =
+                    pack_bf16(out[j][0], out[j][1]);
             if (rowb < cells)
-                *reinterpret_cast<float2*>(&h_out[static_cast<size_t>(c0 + rowb) * F + col]) =
-                    make_float2(out[j][2], out[j][3]);
+                *reinterpret_cast<uint32_t*>(&h_out[static_cast<size_t>(c0 + rowb) * F + col]) =
+                    pack_bf16(out[j][2], out[j][3]);
         }
     }
 }
@@ -635,8 +643,10 @@ void infer(cfdxg_context* ctx, cfdxg_mpnn* net, const double* r, double* out) {
         k_pack_input<<<blocks_for(n, 256), 256, 0, s>>>(n, r, rr, net->feats.get(), xin);
         check_launch(ctx);
     }
-    float* hin = net->hA.get();
-    float* hout = net->hB.get();
+    // the state between rounds is BF16 (64 bytes per cell: the 1.57 M-cell
+    // state fits in L2, so the neighbour gathers hit it there)
+    __nv_bfloat16* hin = reinterpret_cast<__nv_bfloat16*>(net->hA.get());
+    __nv_bfloat16* hout = reinterpret_cast<__nv_bfloat16*>(net->hB.get());
     const int tiles = (n + kTileCells - 1) / kTileCells;
     for (int k = 0; k < R; ++k) {
         const __nv_bfloat16* w = net->wbf.get() + static_cast<size_t>(k) * 3 * F * F;
@@ -644,8 +654,8 @@ void infer(cfdxg_context* ctx, cfdxg_mpnn* net, const double* r, double* out) {
         // compulsory bytes: the state read (r and the cell features in the
         // first round) and written (the output and diagonal in the last), the
         // coupling list once
-        const double in_bytes = first ? 16.0 * n : sizeof(float) * F * n;
-        const double out_bytes = last ? 16.0 * n : sizeof(float) * F * n;
+        const double in_bytes = first ? 16.0 * n : 2.0 * F * n;
+        const double out_bytes = last ? 16.0 * n : 2.0 * F * n;
         ProfScope ps(ctx, first ? "mpnn_round_first_tc" : (last ? "mpnn_round_last_tc" : "mpnn_round_gather_tc"),
                      in_bytes + out_bytes + 4.0 * (n + 1) + 8.0 * static_cast<double>(net->gco.size()));
         auto kern = first ? k_round_gather_tc<true, false>
