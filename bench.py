@@ -61,6 +61,9 @@ def parse_args():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-learned", action="store_true", help="skip the learned+FP32 form")
     ap.add_argument("--no-assembly", action="store_true", help="skip the face-loop timing")
+    ap.add_argument("--half-values", type=int, default=1,
+                    help="FP32 V-cycle coarse levels store FP16 row-scaled values (1, the library default) "
+                         "or FP32 values (0)")
     return ap.parse_args()
 
 
@@ -194,7 +197,8 @@ def run_cfdxg(args):
     by_precision = {}   # one hierarchy per V-cycle precision, shared by the forms that use it
     for form, prec, krylov, learned in plan:
         if prec not in by_precision:
-            amg = cg.NativeBoomerAMGPreconditioner(ctx, precision=prec)
+            extra = {"half_values": args.half_values} if prec == "fp32_vcycle" else {}
+            amg = cg.NativeBoomerAMGPreconditioner(ctx, precision=prec, **extra)
             t = time.time()
             if not amg.setup(A):
                 raise RuntimeError(amg.last_error())

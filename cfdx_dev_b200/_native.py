@@ -47,6 +47,7 @@ class AmgOptions(C.Structure):
         ("require_smoother_certificate", C.c_int32), ("precision", C.c_int32),
         ("coarse_dense_limit", C.c_int32), ("reference_order", C.c_int32),
         ("coarse_pre_sweeps", C.c_int32), ("coarse_post_sweeps", C.c_int32), ("narrow_columns", C.c_int32),
+        ("half_values", C.c_int32),
     ]
 
 

@@ -127,12 +127,16 @@ void amg_setup_impl(cfdxg_context* ctx, cfdxg_amg* amg, cfdxg_matrix* A) {
     }
     std::unique_ptr<DevHierarchy<double>> d64;
     std::unique_ptr<DevHierarchy<float>> d32;
-    if (amg->opts.precision == CFDXG_PRECISION_FP32_VCYCLE)
-        d32 = upload_hierarchy<float>(ctx, staged, amg->opts.coarse_dense_limit, amg->opts.reference_order != 0,
-                                      amg->opts.narrow_columns != 0);
-    else
-        d64 = upload_hierarchy<double>(ctx, staged, 0, amg->opts.reference_order != 0,
-                                       amg->opts.narrow_columns != 0);
+    UploadOptions up;
+    up.reference_order = amg->opts.reference_order != 0;
+    up.narrow_columns = amg->opts.narrow_columns != 0;
+    if (amg->opts.precision == CFDXG_PRECISION_FP32_VCYCLE) {
+        up.coarse_dense_limit = amg->opts.coarse_dense_limit;
+        up.half_values = amg->opts.half_values != 0;
+        d32 = upload_hierarchy<float>(ctx, staged, up);
+    } else {
+        d64 = upload_hierarchy<double>(ctx, staged, up);
+    }
     // commit only after every stage succeeded (hypre_amg.cpp:163-236 is transactional)
     amg->host = std::move(staged);
     amg->d64 = std::move(d64);
@@ -345,6 +349,7 @@ extern "C" int cfdxg_amg_options_default(cfdxg_amg_options* o) {
     o->coarse_pre_sweeps = -1;
     o->coarse_post_sweeps = -1;
     o->narrow_columns = 1;
+    o->half_values = 1;
     return CFDXG_OK;
 }
 

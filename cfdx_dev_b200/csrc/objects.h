@@ -1,5 +1,6 @@
 // objects.h -- internal definitions of the opaque C-ABI handles.
 #pragma once
+#include <cuda_fp16.h>
 #include <memory>
 #include <string>
 #include <vector>
@@ -28,6 +29,12 @@ struct DevLevel {
     // left empty -- 2 bytes instead of 4 per nonzero on the HBM-bound sweeps.
     DevBuf<int16_t> co16;
     bool narrow = false;
+    // Half values (FP32 cycle, option half_values): each row of A stored as
+    // FP16 fractions of its largest magnitude (vh) times that magnitude
+    // (rscale); va is then left empty.
+    DevBuf<__half> vh;
+    DevBuf<T> rscale;
+    bool half = false;
     DevBuf<T> va, inv_diag;
     DevBuf<int> p_off, p_col, r_off, r_row;
     DevBuf<T> p_val, r_val;
@@ -144,10 +151,17 @@ void matrix_sync_host_values(cfdxg_context* ctx, cfdxg_matrix* A);
 void spmv_fp64(cfdxg_context* ctx, const cfdxg_matrix* A, const double* x, double* y);
 
 // hierarchy (vcycle.cu)
+// Device layout choices for one hierarchy.
+struct UploadOptions {
+    int coarse_dense_limit = 0;   // FP32: dense FP64 inverse at the first level with <= this many rows
+    bool reference_order = false; // one thread per row everywhere (the reference's sums)
+    bool narrow_columns = true;   // int16 column offsets on one-thread-per-row levels
+    bool half_values = false;     // FP32: FP16 row-scaled matrix values
+};
+
 template <class T>
 std::unique_ptr<DevHierarchy<T>> upload_hierarchy(cfdxg_context* ctx, const AmgHierarchy& h,
-                                                  int coarse_dense_limit, bool reference_order,
-                                                  bool narrow_columns);
+                                                  const UploadOptions& opt);
 template <class T>
 void refresh_hierarchy_values(cfdxg_context* ctx, DevHierarchy<T>& d, const AmgHierarchy& h);
 // z = V-cycle(r); r, z are FP64 device vectors.

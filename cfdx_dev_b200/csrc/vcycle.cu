@@ -58,6 +58,13 @@ __global__ void k_sweep_zero(int n, T omega, const T* __restrict__ inv_diag, con
 //
 // CI is the column index type: int (absolute columns, base 0) or int16_t
 // (offsets from the row, base = the row index).
+// A stored value as T: FP32 / FP64 as is, FP16 (half_values) widened.
+template <class T, class VS>
+__device__ __forceinline__ T ldv(const VS* __restrict__ p, int k) {
+    if constexpr (std::is_same<VS, __half>::value) return static_cast<T>(__half2float(p[k]));
+    else return p[k];
+}
+
 template <class T, int TPR>
 __device__ __forceinline__ T row_reduce(T s, int lane) {
     if (TPR > 1) {
@@ -82,14 +89,14 @@ __device__ __forceinline__ T row_reduce(T s, int lane) {
     return s;
 }
 
-template <class T, int TPR, class CI = int>
+template <class T, int TPR, class CI = int, class VS = T>
 __device__ __forceinline__ T row_dot(int b, int e, int lane, const CI* __restrict__ co,
-                                     const T* __restrict__ va, const T* __restrict__ x, int base = 0) {
+                                     const VS* __restrict__ va, const T* __restrict__ x, int base = 0) {
     T s = T(0);
     // unrolled so several independent (value, column, x) loads are in flight;
     // the additions stay in the same sequential order
 #pragma unroll 4
-    for (int k = b + lane; k < e; k += TPR) s += va[k] * __ldg(x + (base + static_cast<int>(co[k])));
+    for (int k = b + lane; k < e; k += TPR) s += ldv<T>(va, k) * __ldg(x + (base + static_cast<int>(co[k])));
     return row_reduce<T, TPR>(s, lane);
 }
 
@@ -104,27 +111,28 @@ struct RowHead {
     CI c[PF];
 };
 
-template <class T, int TPR, class CI, int PF>
+template <class T, int TPR, class CI, int PF, class VS = T>
 __device__ __forceinline__ void row_head_load(RowHead<T, CI, PF>& h, int b, int e, int lane,
-                                              const CI* __restrict__ co, const T* __restrict__ va) {
+                                              const CI* __restrict__ co, const VS* __restrict__ va) {
 #pragma unroll
     for (int q = 0; q < PF; ++q) {
         const int k = b + lane + q * TPR;
-        h.v[q] = k < e ? va[k] : T(0);
+        h.v[q] = k < e ? ldv<T>(va, k) : T(0);
         h.c[q] = k < e ? co[k] : CI(0);
     }
 }
 
-template <class T, int TPR, class CI, int PF>
+template <class T, int TPR, class CI, int PF, class VS = T>
 __device__ __forceinline__ T row_dot_head(const RowHead<T, CI, PF>& h, int b, int e, int lane,
-                                          const CI* __restrict__ co, const T* __restrict__ va,
+                                          const CI* __restrict__ co, const VS* __restrict__ va,
                                           const T* __restrict__ x, int base) {
     T s = T(0);
 #pragma unroll
     for (int q = 0; q < PF; ++q)
         if (b + lane + q * TPR < e) s += h.v[q] * __ldg(x + (base + static_cast<int>(h.c[q])));
 #pragma unroll 4
-    for (int k = b + lane + PF * TPR; k < e; k += TPR) s += va[k] * __ldg(x + (base + static_cast<int>(co[k])));
+    for (int k = b + lane + PF * TPR; k < e; k += TPR)
+        s += ldv<T>(va, k) * __ldg(x + (base + static_cast<int>(co[k])));
     return row_reduce<T, TPR>(s, lane);
 }
 
@@ -137,10 +145,11 @@ __host__ __device__ constexpr int head_entries() { return TPR == 1 ? 1 : 4; }
 template <class CI>
 __device__ __forceinline__ int column_base(int row) { return sizeof(CI) == 2 ? row : 0; }
 
-// x_out = x + omega * (inv_diag * (r - A x))
-template <class T, class XO, int TPR, class CI>
+// x_out = x + omega * (inv_diag * (r - A x)).  With FP16 values (VS = __half)
+// the row sum is formed on the stored fractions and scaled once by rscale.
+template <class T, class XO, int TPR, class CI, class VS>
 __global__ void k_sweep(int n, const int* __restrict__ ro, const CI* __restrict__ co,
-                        const T* __restrict__ va, const T* __restrict__ inv_diag,
+                        const VS* __restrict__ va, const T* __restrict__ rscale, const T* __restrict__ inv_diag,
                         const T* __restrict__ r, const T* __restrict__ x, XO* __restrict__ xo,
                         T omega, int* status) {
     pdl_trigger();
@@ -156,25 +165,26 @@ __global__ void k_sweep(int n, const int* __restrict__ ro, const CI* __restrict_
     if constexpr (TPR == 1) {
         pdl_wait();
         if (valid) { ri = r[i]; xi = x[i]; di = inv_diag[i]; }
-        s = row_dot<T, TPR, CI>(valid ? ro[i] : 0, valid ? ro[i + 1] : 0, lane, co, va, x, column_base<CI>(i));
+        s = row_dot<T, TPR, CI, VS>(valid ? ro[i] : 0, valid ? ro[i + 1] : 0, lane, co, va, x, column_base<CI>(i));
     } else {
         const int b = valid ? ro[i] : 0, e = valid ? ro[i + 1] : 0;
         RowHead<T, CI, head_entries<TPR>()> head;
-        row_head_load<T, TPR, CI, head_entries<TPR>()>(head, b, e, lane, co, va);
+        row_head_load<T, TPR, CI, head_entries<TPR>(), VS>(head, b, e, lane, co, va);
         pdl_wait();
-        s = row_dot_head<T, TPR, CI, head_entries<TPR>()>(head, b, e, lane, co, va, x, column_base<CI>(i));
+        s = row_dot_head<T, TPR, CI, head_entries<TPR>(), VS>(head, b, e, lane, co, va, x, column_base<CI>(i));
     }
     if (!valid || lane != 0) return;
     if constexpr (TPR > 1) { ri = r[i]; xi = x[i]; di = inv_diag[i]; }
+    if constexpr (std::is_same<VS, __half>::value) s = s * rscale[i];
     const T delta = di * (ri - s);
     const T xn = xi + omega * delta;
     xo[i] = static_cast<XO>(xn);
     if (!finite_(xn)) atomicOr(status, kStatusNonFinite);
 }
 
-template <class T, int TPR, class CI>
+template <class T, int TPR, class CI, class VS>
 __global__ void k_residual(int n, const int* __restrict__ ro, const CI* __restrict__ co,
-                           const T* __restrict__ va, const T* __restrict__ r,
+                           const VS* __restrict__ va, const T* __restrict__ rscale, const T* __restrict__ r,
                            const T* __restrict__ x, T* __restrict__ res) {
     pdl_trigger();
     const int g = blockIdx.x * blockDim.x + threadIdx.x;
@@ -185,16 +195,17 @@ __global__ void k_residual(int n, const int* __restrict__ ro, const CI* __restri
     if constexpr (TPR == 1) {
         pdl_wait();
         if (valid) ri = r[i];
-        s = row_dot<T, TPR, CI>(valid ? ro[i] : 0, valid ? ro[i + 1] : 0, lane, co, va, x, column_base<CI>(i));
+        s = row_dot<T, TPR, CI, VS>(valid ? ro[i] : 0, valid ? ro[i + 1] : 0, lane, co, va, x, column_base<CI>(i));
     } else {
         const int b = valid ? ro[i] : 0, e = valid ? ro[i + 1] : 0;
         RowHead<T, CI, head_entries<TPR>()> head;
-        row_head_load<T, TPR, CI, head_entries<TPR>()>(head, b, e, lane, co, va);
+        row_head_load<T, TPR, CI, head_entries<TPR>(), VS>(head, b, e, lane, co, va);
         pdl_wait();
-        s = row_dot_head<T, TPR, CI, head_entries<TPR>()>(head, b, e, lane, co, va, x, column_base<CI>(i));
+        s = row_dot_head<T, TPR, CI, head_entries<TPR>(), VS>(head, b, e, lane, co, va, x, column_base<CI>(i));
     }
     if (!valid || lane != 0) return;
     if constexpr (TPR > 1) ri = r[i];
+    if constexpr (std::is_same<VS, __half>::value) s = s * rscale[i];
     res[i] = ri - s;
 }
 
@@ -424,38 +435,54 @@ inline double account(double bytes) {
 template <class T>
 const char* tname(const char* fp64, const char* fp32) { return sizeof(T) == 8 ? fp64 : fp32; }
 
+// Bytes of one stored nonzero of A (value + column) and per row (offset, and
+// the row scale of FP16 values).
 template <class T>
-double column_bytes(const DevLevel<T>& L) { return L.narrow ? 2.0 : 4.0; }
+double nonzero_bytes(const DevLevel<T>& L) { return (L.half ? 2.0 : sizeof(T)) + (L.narrow ? 2.0 : 4.0); }
+template <class T>
+double row_bytes(const DevLevel<T>& L) { return 4.0 + (L.half ? sizeof(T) : 0.0); }
+
+// Calls go(columns, values, row_scale) with the level's storage types.
+template <class T, class Go>
+void with_level_storage(const DevLevel<T>& L, Go&& go) {
+    if constexpr (std::is_same<T, float>::value) {
+        if (L.half) {
+            if (L.narrow) go(L.co16.get(), L.vh.get(), L.rscale.get());
+            else go(L.co.get(), L.vh.get(), L.rscale.get());
+            return;
+        }
+    }
+    if (L.narrow) go(L.co16.get(), L.va.get(), static_cast<const T*>(nullptr));
+    else go(L.co.get(), L.va.get(), static_cast<const T*>(nullptr));
+}
 
 template <class T, class XO>
 void launch_sweep(cfdxg_context* ctx, const DevLevel<T>& L, const T* r, const T* x, XO* xo, T omega, int* status) {
-    // A values + columns, row offsets, x / r / inv_diag reads, x_out write
-    const double bytes = account((sizeof(T) + column_bytes(L)) * L.nnz + 4.0 * (L.n + 1) + 3.0 * sizeof(T) * L.n +
+    // A values + columns, row offsets (+ scales), x / r / inv_diag reads, x_out write
+    const double bytes = account(nonzero_bytes(L) * L.nnz + row_bytes(L) * L.n + 4.0 + 3.0 * sizeof(T) * L.n +
                                  sizeof(XO) * L.n);
     ProfScope ps(ctx, tname<T>("jacobi_sweep_fp64_L0", "jacobi_sweep_fp32_L0"), bytes);
-    const int64_t threads = static_cast<int64_t>(L.n) * L.tpr;
-    if (L.narrow) {
-        CFDXG_TPR_SWITCH(L.tpr, (launch_pdl(ctx->stream, k_sweep<T, XO, TPR, int16_t>, blocks_for(threads, kT), kT, 
-            L.n, L.ro.get(), L.co16.get(), L.va.get(), L.inv_diag.get(), r, x, xo, omega, status)));
-    } else {
-        CFDXG_TPR_SWITCH(L.tpr, (launch_pdl(ctx->stream, k_sweep<T, XO, TPR, int>, blocks_for(threads, kT), kT, 
-            L.n, L.ro.get(), L.co.get(), L.va.get(), L.inv_diag.get(), r, x, xo, omega, status)));
-    }
+    const int grid = blocks_for(static_cast<int64_t>(L.n) * L.tpr, kT);
+    with_level_storage(L, [&](const auto* co, const auto* va, const T* rs) {
+        using CI = std::remove_cv_t<std::remove_pointer_t<decltype(co)>>;
+        using VS = std::remove_cv_t<std::remove_pointer_t<decltype(va)>>;
+        CFDXG_TPR_SWITCH(L.tpr, (launch_pdl(ctx->stream, k_sweep<T, XO, TPR, CI, VS>, grid, kT, L.n, L.ro.get(), co,
+                                            va, rs, L.inv_diag.get(), r, x, xo, omega, status)));
+    });
     check_launch(ctx);
 }
 
 template <class T>
 void launch_residual(cfdxg_context* ctx, const DevLevel<T>& L, const T* r, const T* x, T* res) {
-    const double bytes = account((sizeof(T) + column_bytes(L)) * L.nnz + 4.0 * (L.n + 1) + 3.0 * sizeof(T) * L.n);
+    const double bytes = account(nonzero_bytes(L) * L.nnz + row_bytes(L) * L.n + 4.0 + 3.0 * sizeof(T) * L.n);
     ProfScope ps(ctx, tname<T>("residual_fp64_L0", "residual_fp32_L0"), bytes);
-    const int64_t threads = static_cast<int64_t>(L.n) * L.tpr;
-    if (L.narrow) {
-        CFDXG_TPR_SWITCH(L.tpr, (launch_pdl(ctx->stream, k_residual<T, TPR, int16_t>, blocks_for(threads, kT), kT, 
-            L.n, L.ro.get(), L.co16.get(), L.va.get(), r, x, res)));
-    } else {
-        CFDXG_TPR_SWITCH(L.tpr, (launch_pdl(ctx->stream, k_residual<T, TPR, int>, blocks_for(threads, kT), kT, 
-            L.n, L.ro.get(), L.co.get(), L.va.get(), r, x, res)));
-    }
+    const int grid = blocks_for(static_cast<int64_t>(L.n) * L.tpr, kT);
+    with_level_storage(L, [&](const auto* co, const auto* va, const T* rs) {
+        using CI = std::remove_cv_t<std::remove_pointer_t<decltype(co)>>;
+        using VS = std::remove_cv_t<std::remove_pointer_t<decltype(va)>>;
+        CFDXG_TPR_SWITCH(L.tpr, (launch_pdl(ctx->stream, k_residual<T, TPR, CI, VS>, grid, kT, L.n, L.ro.get(), co,
+                                            va, rs, r, x, res)));
+    });
     check_launch(ctx);
 }
 
@@ -510,9 +537,27 @@ int choose_transfer_tpr(int64_t nnz, int64_t rows, bool reference_order) {
 
 template <class T>
 void upload_level_values(cfdxg_context* ctx, DevLevel<T>& D, const AmgLevel& H) {
-    std::vector<T> tmp(H.A.va.size());
-    for (std::size_t k = 0; k < tmp.size(); ++k) tmp[k] = static_cast<T>(H.A.va[k]);
-    D.va.upload(tmp, ctx->stream);
+    if (D.half) {
+        // FP16 fractions of each row's largest magnitude (the same rounding as k_quantize_rows)
+        const int n = static_cast<int>(H.A.n);
+        std::vector<__half> q(H.A.va.size());
+        std::vector<T> sc(n);
+        for (int i = 0; i < n; ++i) {
+            double m = 0.0;
+            for (uint32_t k = H.A.ro[i]; k < H.A.ro[i + 1]; ++k) m = std::max(m, std::fabs(H.A.va[k]));
+            const float s = m > 0.0 ? static_cast<float>(m) : 1.0f;
+            sc[i] = static_cast<T>(s);
+            for (uint32_t k = H.A.ro[i]; k < H.A.ro[i + 1]; ++k)
+                q[k] = __float2half_rn(static_cast<float>(H.A.va[k] / static_cast<double>(s)));
+        }
+        D.vh.upload(q, ctx->stream);
+        D.rscale.upload(sc, ctx->stream);
+        D.va.release();
+    } else {
+        std::vector<T> tmp(H.A.va.size());
+        for (std::size_t k = 0; k < tmp.size(); ++k) tmp[k] = static_cast<T>(H.A.va[k]);
+        D.va.upload(tmp, ctx->stream);
+    }
 
     std::vector<T> d(H.inv_diag.size());
     for (std::size_t k = 0; k < d.size(); ++k) d[k] = static_cast<T>(H.inv_diag[k]);
@@ -550,7 +595,8 @@ void upload_columns(cfdxg_context* ctx, DevLevel<T>& D, const AmgLevel& H, bool 
 
 template <class T>
 void upload_level(cfdxg_context* ctx, DevLevel<T>& D, const AmgLevel& H, bool with_transfer,
-                  bool reference_order, bool narrow_columns) {
+                  const UploadOptions& opt) {
+    const bool reference_order = opt.reference_order;
     cudaStream_t s = ctx->stream;
     D.n = static_cast<int>(H.A.n);
     D.nnz = static_cast<int>(H.A.co.size());
@@ -561,7 +607,12 @@ void upload_level(cfdxg_context* ctx, DevLevel<T>& D, const AmgLevel& H, bool wi
     // fine-level FP32 sweep at 64^3); on the long rows that a warp shares they
     // measured 10-20% slower (58.9 -> 70.6 us on the 77,039-row level), so
     // those keep int32 columns.
-    upload_columns(ctx, D, H, with_transfer && narrow_columns && D.tpr == 1);
+    upload_columns(ctx, D, H, with_transfer && opt.narrow_columns && D.tpr == 1);
+    // FP16 values on the shared-row levels (the dense coarse operators: 475 vs
+    // 501 us per FP32 cycle of levels >= 1 at 64^3, iterations unchanged); on
+    // one-thread rows the conversion cost more than the bytes saved
+    // (18.1 vs 17.7 us per fine-level sweep)
+    D.half = std::is_same<T, float>::value && opt.half_values && with_transfer && D.tpr > 1;
     upload_level_values(ctx, D, H);
     D.r.resize(D.n); D.x.resize(D.n); D.x2.resize(D.n); D.res.resize(D.n);
     if (with_transfer) {
@@ -716,8 +767,8 @@ void ensure_graph(cfdxg_context* ctx, DevHierarchy<T>& d) {
 
 template <class T>
 std::unique_ptr<DevHierarchy<T>> upload_hierarchy(cfdxg_context* ctx, const AmgHierarchy& h,
-                                                  int coarse_dense_limit, bool reference_order,
-                                                  bool narrow_columns) {
+                                                  const UploadOptions& opt) {
+    const int coarse_dense_limit = opt.coarse_dense_limit;
     auto d = std::make_unique<DevHierarchy<T>>();
     d->omega = static_cast<T>(h.omega);
     d->pre = h.options.pre;
@@ -741,7 +792,7 @@ std::unique_ptr<DevHierarchy<T>> upload_hierarchy(cfdxg_context* ctx, const AmgH
     if (d->coarse_mode == 0 && h.levels[used - 1].A.n <= kDenseDirectLimit) d->coarse_mode = 1;
     d->used = used;
     d->L.resize(used);
-    for (int l = 0; l < used; ++l) upload_level(ctx, d->L[l], h.levels[l], l + 1 < used, reference_order, narrow_columns);
+    for (int l = 0; l < used; ++l) upload_level(ctx, d->L[l], h.levels[l], l + 1 < used, opt);
     if (d->coarse_mode == 2) build_dense_inverse(ctx, *d, h.levels[used - 1]);
     return d;
 }
@@ -754,6 +805,19 @@ void refresh_hierarchy_values(cfdxg_context* ctx, DevHierarchy<T>& d, const AmgH
     // omega is a kernel argument baked into the graph: recapture
     if (d.exec) { cudaGraphExecDestroy(d.exec); d.exec = nullptr; }
     if (d.graph) { cudaGraphDestroy(d.graph); d.graph = nullptr; }
+}
+
+// FP16 fractions of each row's largest magnitude and that magnitude (the
+// host upload's rounding, operation for operation).
+__global__ void k_quantize_rows(int n, const int* __restrict__ ro, const double* __restrict__ va,
+                                __half* __restrict__ vh, float* __restrict__ rscale) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    double m = 0.0;
+    for (int k = ro[i]; k < ro[i + 1]; ++k) m = fmax(m, fabs(va[k]));
+    const float s = m > 0.0 ? static_cast<float>(m) : 1.0f;
+    rscale[i] = s;
+    for (int k = ro[i]; k < ro[i + 1]; ++k) vh[k] = __float2half_rn(static_cast<float>(va[k] / static_cast<double>(s)));
 }
 
 template <class T>
@@ -779,7 +843,15 @@ template <class T>
 void set_hierarchy_values_device(cfdxg_context* ctx, DevHierarchy<T>& d, const DevRefresh& R, double omega) {
     d.omega = static_cast<T>(omega);
     for (int l = 0; l < d.used; ++l) {
-        copy_or_cast<T>(ctx, R.L[l].va.get(), d.L[l].va.get(), R.L[l].nnz);
+        if (d.L[l].half) {
+            if constexpr (std::is_same<T, float>::value) {
+                k_quantize_rows<<<blocks_for(d.L[l].n, kT), kT, 0, ctx->stream>>>(
+                    d.L[l].n, d.L[l].ro.get(), R.L[l].va.get(), d.L[l].vh.get(), d.L[l].rscale.get());
+                check_launch(ctx);
+            }
+        } else {
+            copy_or_cast<T>(ctx, R.L[l].va.get(), d.L[l].va.get(), R.L[l].nnz);
+        }
         copy_or_cast<T>(ctx, R.L[l].inv_diag.get(), d.L[l].inv_diag.get(), R.L[l].n);
     }
     if (d.coarse_mode == 2) {
@@ -859,8 +931,8 @@ void vcycle_apply(cfdxg_context* ctx, DevHierarchy<T>& d, const double* r, doubl
 template <class T>
 void destroy_hierarchy(DevHierarchy<T>* d) { delete d; }
 
-template std::unique_ptr<DevHierarchy<double>> upload_hierarchy<double>(cfdxg_context*, const AmgHierarchy&, int, bool, bool);
-template std::unique_ptr<DevHierarchy<float>> upload_hierarchy<float>(cfdxg_context*, const AmgHierarchy&, int, bool, bool);
+template std::unique_ptr<DevHierarchy<double>> upload_hierarchy<double>(cfdxg_context*, const AmgHierarchy&, const UploadOptions&);
+template std::unique_ptr<DevHierarchy<float>> upload_hierarchy<float>(cfdxg_context*, const AmgHierarchy&, const UploadOptions&);
 template void refresh_hierarchy_values<double>(cfdxg_context*, DevHierarchy<double>&, const AmgHierarchy&);
 template void refresh_hierarchy_values<float>(cfdxg_context*, DevHierarchy<float>&, const AmgHierarchy&);
 template void set_hierarchy_values_device<double>(cfdxg_context*, DevHierarchy<double>&, const DevRefresh&, double);

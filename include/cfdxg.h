@@ -233,6 +233,12 @@ typedef struct {
                                         column offsets (2 bytes less per nonzero read); 0:
                                         int32 columns everywhere.  The arithmetic is the same
                                         either way. */
+    int32_t half_values;             /* FP32 V-cycle only.  1 (default): levels whose rows
+                                        are shared by several threads (the dense coarse
+                                        operators; not the coarsest) store A as FP16 fractions
+                                        of each row's largest magnitude, times that magnitude
+                                        in FP32: 2 bytes per nonzero instead of 4, sums stay
+                                        FP32.  0: FP32 values everywhere. */
 } cfdxg_amg_options;
 
 int cfdxg_amg_options_default(cfdxg_amg_options* opts);

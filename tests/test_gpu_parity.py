@@ -412,3 +412,33 @@ def test_classical_gram_schmidt_matches_oracle(ctx, oracle, tet_setup):
     assert rel_l2(x1, x0) < 1e-6
     with pytest.raises(cg.CfdxgError):
         cg.solve_gmres(A, b, amg=amg, orthogonalization=7)
+
+
+# ---------------------------------------------------------------- FP16 level values
+def test_half_values_fp32_vcycle(ctx, tet_setup):
+    """half_values = 1 stores each level's rows as FP16 fractions of the row's
+    largest magnitude: the FP32 V-cycle stays within 1e-2 of the FP32-value
+    cycle, FGMRES reaches the FP64 certificate within one extra iteration, and
+    after a numeric refresh on the device (which quantises the new values on
+    the device) the cycle again stays within 1e-2 of the refreshed FP32-value
+    cycle and FGMRES converges."""
+    m, mesh, g, (U, rAU, aP, p, fixed, value) = tet_setup
+    A, b, phi, grad = cg.assemble_pressure_correction(mesh, U, rAU, p, 1.0, fixed, value)
+    full = cg.NativeBoomerAMGPreconditioner(ctx, precision="fp32_vcycle", half_values=0)
+    half = cg.NativeBoomerAMGPreconditioner(ctx, precision="fp32_vcycle", half_values=1)
+    assert full.setup(A) and half.setup(A)
+    r = np.random.default_rng(3).standard_normal(A.n)
+    z_full, z_half = full.apply(r), half.apply(r)
+    assert rel_l2(z_half, z_full) < 1e-2
+    x_f, rep_f = cg.solve_fgmres(A, b, amg=full, restart=30, tolerance=1e-8)
+    x_h, rep_h = cg.solve_fgmres(A, b, amg=half, restart=30, tolerance=1e-8)
+    assert rep_h["status_name"] == "converged" and rep_h["physical_residual_relative"] <= 1e-8
+    assert rep_h["iterations"] <= rep_f["iterations"] + 1
+    assert rel_l2(x_h, x_f) < 1e-6
+    # numeric refresh on the device: the same values quantised on the device
+    U2, rAU2, aP2, p2, fixed2, value2 = cases.simple_fields(m, g["cell_centres"], seed_offset=11)
+    A2, b2, _, _ = cg.assemble_pressure_correction(mesh, U2, rAU2, p2, 1.0, fixed2, value2)
+    assert half.update_values(A2) and full.update_values(A2)
+    assert rel_l2(half.apply(r), full.apply(r)) < 1e-2
+    x2, rep2 = cg.solve_fgmres(A2, b2, amg=half, restart=30, tolerance=1e-8)
+    assert rep2["status_name"] == "converged" and rep2["physical_residual_relative"] <= 1e-8
