@@ -52,8 +52,8 @@ struct DevHierarchy {
     T omega = T(0.7);
     int pre = 6, post = 6;
     int coarse_pre = 6, coarse_post = 6;   // sweeps on levels >= 1
-    int coarse_mode = 0;       // 0: 24 Jacobi sweeps, 1: reference dense LU (n <= 16), 2: FP64 inverse
-    DevBuf<double> dense;      // mode 1: n*n matrix, mode 2: n*n inverse (row-major)
+    int coarse_mode = 0;       // 0: 24 Jacobi sweeps, 1: reference dense LU (n <= 16), 2: dense inverse
+    DevBuf<float> dense;       // mode 2: the n*n inverse (row-major), formed in FP64, stored FP32
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
     int64_t graph_kernels = 0;

@@ -322,17 +322,20 @@ __global__ void k_dense_lu_reference(int n, const int* __restrict__ ro, const in
     for (int i = 0; i < n; ++i) x[i] = static_cast<T>(sol[i]);
 }
 
-// x = Ainv * r with the FP64 inverse, one warp per row.
+// x = Ainv * r, one warp per row: the inverse (formed in FP64) is read as
+// FP32 -- half the bytes of the largest single read of the FP32 cycle -- and
+// the products are summed in FP64.
 template <class T>
-__global__ void k_dense_inverse_apply(int n, const double* __restrict__ inv, const T* __restrict__ r,
+__global__ void k_dense_inverse_apply(int n, const float* __restrict__ inv, const T* __restrict__ r,
                                       T* __restrict__ x, int* status) {
     pdl_entry();
     const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int lane = threadIdx.x & 31;
     if (warp >= n) return;
     double s = 0.0;
-    const double* row = inv + static_cast<size_t>(warp) * n;
-    for (int j = lane; j < n; j += 32) s += row[j] * static_cast<double>(r[j]);
+    const float* row = inv + static_cast<size_t>(warp) * n;
+#pragma unroll 4
+    for (int j = lane; j < n; j += 32) s += static_cast<double>(row[j]) * static_cast<double>(r[j]);
     for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
     if (lane == 0) {
         x[warp] = static_cast<T>(s);
@@ -394,11 +397,11 @@ __global__ void k_gj_eliminate(int n, double* a, const double* factors, int k) {
     a[idx] -= f * a[static_cast<size_t>(k) * 2 * n + j];
 }
 
-__global__ void k_gj_extract(int n, const double* a, double* inv) {
+__global__ void k_gj_extract(int n, const double* a, float* inv) {
     const size_t idx = static_cast<size_t>(blockIdx.x) * blockDim.x + threadIdx.x;
     if (idx >= static_cast<size_t>(n) * n) return;
     const int i = static_cast<int>(idx / n), j = static_cast<int>(idx % n);
-    inv[idx] = a[static_cast<size_t>(i) * 2 * n + n + j];
+    inv[idx] = static_cast<float>(a[static_cast<size_t>(i) * 2 * n + n + j]);
 }
 
 __global__ void k_gj_init(int n, const int* ro, const int* co, const double* va, double* a) {
@@ -711,7 +714,7 @@ void enqueue_from(cfdxg_context* ctx, DevHierarchy<T>& d, int l) {
             check_launch(ctx);
             L.xout = L.x.get();
         } else if (d.coarse_mode == 2) {
-            account(8.0 * L.n * L.n + 2.0 * sizeof(T) * L.n);
+            account(4.0 * L.n * L.n + 2.0 * sizeof(T) * L.n);
             launch_pdl(s, k_dense_inverse_apply<T>, blocks_for(static_cast<int64_t>(L.n) * 32, kT), kT, 
                 L.n, d.dense.get(), L.r.get(), L.x.get(), d.status);
             check_launch(ctx);
