@@ -22,6 +22,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <limits>
 #include <random>
 
 #include "io.h"
@@ -229,10 +230,12 @@ struct Encoder {
 // Lanes 8q..8q+7 take cell 4 * pass + q, each lane one 16-byte quarter-row.
 // STAGED: the tile's couplings are in sIdx / sW (index k - seg_b); otherwise
 // they are read from global memory.  FIRST: h is the encoder's h0.
+// BF16 -> FP32 is exact: the BF16 bits are the upper half of the FP32 word.
+// Done with integer shifts and masks (the ALU), which measured faster here
+// than the conversion instructions.
 __device__ __forceinline__ float4 unpack_bf16x4(uint2 u) {
-    const float2 a = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162*>(&u.x));
-    const float2 b = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162*>(&u.y));
-    return make_float4(a.x, a.y, b.x, b.y);
+    return make_float4(__uint_as_float(u.x << 16), __uint_as_float(u.x & 0xffff0000u),
+                       __uint_as_float(u.y << 16), __uint_as_float(u.y & 0xffff0000u));
 }
 
 template <bool STAGED, bool FIRST>
@@ -244,24 +247,30 @@ __device__ __forceinline__ void gather_tile(int c0, int cells, int rb, int re, i
     // the state between rounds is BF16: a lane's quarter-row is 8 bytes
     const uint2* h8 = reinterpret_cast<const uint2*>(h_in);
     const int grp = lane >> 3, quarter = lane & 7;
+    // 32-bit row offsets (the binding keeps n * F / 4 below 2^31)
     auto hrow = [&](int j) -> float4 {
         if constexpr (FIRST) return enc.h0(j);
-        else return unpack_bf16x4(h8[static_cast<size_t>(j) * (F / 4) + quarter]);
+        else return unpack_bf16x4(h8[j * (F / 4) + quarter]);
     };
-#pragma unroll 1
+    // the four passes unrolled: their neighbour rows are loaded together
+#pragma unroll
     for (int pass = 0; pass < kTileCells / 4; ++pass) {
         const int r = pass * 4 + grp;
         const int b = __shfl_sync(0xffffffffu, rb, r), e = __shfl_sync(0xffffffffu, re, r);
         float4 hv = make_float4(0.f, 0.f, 0.f, 0.f), av = make_float4(0.f, 0.f, 0.f, 0.f);
-        if (r < cells) hv = hrow(c0 + r);
-        int k = b;
-        for (; k + 4 <= e; k += 4) {
+        const int self = r < cells ? c0 + r : c0;
+        if (r < cells) hv = hrow(self);
+        // neighbours four at a time, the last group predicated (a tet cell has
+        // at most four): the padding terms read the cell's own row with weight 0
+        for (int k0 = b; k0 < e; k0 += 4) {
             int j[4];
             float w[4];
 #pragma unroll
             for (int u = 0; u < 4; ++u) {
-                j[u] = STAGED ? sIdx[k + u - seg_b] : gco[k + u];
-                w[u] = STAGED ? sW[k + u - seg_b] : gew[k + u];
+                const int k = k0 + u;
+                const bool ok = k < e;
+                j[u] = ok ? (STAGED ? sIdx[k - seg_b] : gco[k]) : self;
+                w[u] = ok ? (STAGED ? sW[k - seg_b] : gew[k]) : 0.0f;
             }
             float4 v[4];
 #pragma unroll
@@ -270,12 +279,6 @@ __device__ __forceinline__ void gather_tile(int c0, int cells, int rb, int re, i
             for (int u = 0; u < 4; ++u) {
                 av.x += w[u] * v[u].x; av.y += w[u] * v[u].y; av.z += w[u] * v[u].z; av.w += w[u] * v[u].w;
             }
-        }
-        for (; k < e; ++k) {
-            const int j = STAGED ? sIdx[k - seg_b] : gco[k];
-            const float w = STAGED ? sW[k - seg_b] : gew[k];
-            const float4 v = hrow(j);
-            av.x += w * v.x; av.y += w * v.y; av.z += w * v.z; av.w += w * v.w;
         }
         *reinterpret_cast<float4*>(&sH[r][4 * quarter]) = hv;
         uint2 hp, ap;
@@ -908,6 +911,9 @@ extern "C" int cfdxg_mpnn_bind(cfdxg_context* ctx, cfdxg_mpnn* net, cfdxg_mesh* 
     check_mem_flag(mem);
     if (!mesh->geometry_ready) throw Error(CFDXG_ERR_NOT_READY, "geometry not built");
     if (A->n != mesh->n_cells) throw Error(CFDXG_ERR_INVALID_ARGUMENT, "matrix and mesh sizes differ");
+    // inference addresses the state with 32-bit row offsets (n * F / 4 quarter-rows)
+    if (A->n > std::numeric_limits<int>::max() / mp::F)
+        throw Error(CFDXG_ERR_INVALID_ARGUMENT, "mesh too large for the learned stage");
     auto* M = const_cast<cfdxg_matrix*>(A);
     matrix_sync_host_values(ctx, M);
     const int64_t n = A->n;
