@@ -68,7 +68,8 @@ def parse_args():
 
 
 def dist_env():
-    return int(os.environ.get("RANK", 0)), int(os.environ.get("LOCAL_RANK", 0)), int(os.environ.get("WORLD_SIZE", 1))
+    from cfdx_dev_b200.replicas import dist_env as env
+    return env()
 
 
 def measured_peak():
@@ -151,6 +152,7 @@ def run_cfdxg(args):
 
     import cfdx_dev_b200 as cg
     from cfdx_dev_b200 import _native as N
+    from cfdx_dev_b200.replicas import max_over_ranks, seed_offsets
     from tests import cases
 
     rank, local_rank, world = dist_env()
@@ -170,8 +172,9 @@ def run_cfdxg(args):
     g = mesh.geometry()
     rhs_list = []
     A = None
+    seeds = seed_offsets(rank, N_RHS)   # each replica its own right-hand sides
     for k in range(N_RHS):
-        U, rAU, aP, p, fixed, value = cases.simple_fields(m, g["cell_centres"], seed_offset=rank * N_RHS + k)
+        U, rAU, aP, p, fixed, value = cases.simple_fields(m, g["cell_centres"], seed_offset=seeds[k])
         if k == 0:
             base_rAU = rAU
         # the matrix depends on rAU and geometry only; HbyA changes b
@@ -318,13 +321,9 @@ def run_cfdxg(args):
                "h2d_bytes_per_step": int(16 * n_cells), "d2h_bytes_per_step": int(8 * n_cells)}
 
     # ---- max over ranks ----
-    value = forms[headline]["s_per_solve"]
-    if world > 1:
-        t = torch.tensor([value, e2e["value"] if e2e else 0.0], device=dev, dtype=torch.float64)
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        value = float(t[0])
-        if e2e:
-            e2e["value"] = float(t[1])
+    value, e2e_max = max_over_ranks([forms[headline]["s_per_solve"], e2e["value"] if e2e else 0.0], dev)
+    if e2e:
+        e2e["value"] = e2e_max
 
     # ---- roofline of the dominant kernel (live CUDA-event timing in the timed region) ----
     peak, peak_kind = measured_peak()
