@@ -60,6 +60,8 @@ def parse_args():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-learned", action="store_true", help="skip the learned+FP32 form")
+    ap.add_argument("--no-plain", action="store_true",
+                    help="skip the plain FP64 form (profiling runs; no speed-ups or errors against it)")
     ap.add_argument("--no-assembly", action="store_true", help="skip the face-loop timing")
     ap.add_argument("--half-values", type=int, default=1,
                     help="FP32 V-cycle coarse levels store FP16 row-scaled values (1, the library default) "
@@ -188,6 +190,8 @@ def run_cfdxg(args):
 
     # (form, V-cycle precision, Krylov method, learned stage)
     plan = [("plain_fp64", "fp64", "gmres", False), ("fp32_vcycle", "fp32_vcycle", "fgmres", False)]
+    if args.no_plain:
+        plan = plan[1:]
     net = None
     if WEIGHTS.exists() and not args.no_learned:
         net = cg.LearnedPreconditioner(ctx)
@@ -208,8 +212,8 @@ def run_cfdxg(args):
             by_precision[prec] = (amg, {"setup_s": time.time() - t, "host_setup_s": amg.setup_seconds})
         amgs[form] = by_precision[prec][0]
         forms[form] = dict(by_precision[prec][1])
-    levels = amgs["plain_fp64"].hierarchy_level_sizes()
-    level_nnz = amgs["plain_fp64"].hierarchy_level_nnz()
+    levels = amgs[plan[0][0]].hierarchy_level_sizes()
+    level_nnz = amgs[plan[0][0]].hierarchy_level_nnz()
 
     b_dev = [torch.from_numpy(b).to(dev) for b in rhs_list]
     x_dev = torch.zeros(n_cells, dtype=torch.float64, device=dev)
@@ -287,7 +291,8 @@ def run_cfdxg(args):
         if learned:
             forms[form]["learned_fallback_applications"] = float(np.mean(fallbacks))
     for form in forms:
-        forms[form]["speedup_vs_plain_fp64"] = forms["plain_fp64"]["s_per_solve"] / forms[form]["s_per_solve"]
+        if "plain_fp64" in forms:
+            forms[form]["speedup_vs_plain_fp64"] = forms["plain_fp64"]["s_per_solve"] / forms[form]["s_per_solve"]
 
     # ---- the face loop: pressure-corrector assembly and Rhie-Chow face flux ----
     assembly = None
@@ -348,7 +353,7 @@ def run_cfdxg(args):
     result = None
     if rank == 0:
         cpu = None
-        if world == 1 and not args.no_cpu_baseline:
+        if world == 1 and not args.no_cpu_baseline and "plain_fp64" in amgs:
             cpu = cpu_baseline(amgs["plain_fp64"], rhs_list[0])
         result = {
             "metric": METRIC,

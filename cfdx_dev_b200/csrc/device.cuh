@@ -58,7 +58,7 @@ inline void launch_pdl(cudaStream_t stream, void (*kern)(KArgs...), dim3 grid, d
 }
 
 constexpr int kReduceThreads = 256;
-constexpr int kMaxReduceBlocks = 592;   // 4 x 148 SMs: fixed partition => deterministic sums
+constexpr int kMaxReduceBlocks = 1184;  // 8 x 148 SMs: fixed partition => deterministic sums
 
 // Device-side scratch owned by a context: reduction partials, tickets, a
 // status word for device-detected errors, and pinned host mirrors.

@@ -160,6 +160,9 @@ __global__ void k_axpy_absmax(int n, double* __restrict__ w, const double* __res
 
 // ---- classical Gram-Schmidt (the CGS2 option): up to kChunk basis vectors per launch
 constexpr int kChunk = 16;
+// The multi-vector passes take the same fixed grid of eight blocks per SM as
+// the single-vector reductions (the reduction partition, so deterministic).
+constexpr int kWideBlocks = kMaxReduceBlocks;
 
 // out[q] = v_{i0+q} . w for q < c, one pass over w.  Each block's partial sums
 // land in partial[q * gridDim.x + block]; the last block adds them in block
@@ -288,7 +291,7 @@ struct Workspace {
     int64_t n = 0;
     int m = 0;
     DevBuf<double> V, Z, w, r, ax, best, trial, tmp;
-    DevBuf<double> mpartial;   // kChunk x kMaxReduceBlocks partial sums of the multi-dot
+    DevBuf<double> mpartial;   // kChunk x kWideBlocks partial sums of the multi-dot
 };
 
 Workspace& workspace(cfdxg_context* ctx, int64_t n, int m) {
@@ -303,7 +306,7 @@ Workspace& workspace(cfdxg_context* ctx, int64_t n, int m) {
         ws->Z.resize(static_cast<size_t>(mm) * n);
         ws->w.resize(n); ws->r.resize(n); ws->ax.resize(n); ws->best.resize(n);
         ws->trial.resize(n); ws->tmp.resize(n);
-        ws->mpartial.resize(static_cast<size_t>(kChunk) * kMaxReduceBlocks);
+        ws->mpartial.resize(static_cast<size_t>(kChunk) * kWideBlocks);
         ws->n = n;
         ws->m = mm;
     }
@@ -347,10 +350,11 @@ public:
         check_launch(ctx_);
     }
     // h[out + i] = v_i . w for i <= j (classical Gram-Schmidt), in chunks
+    int wb() const { return std::min(kWideBlocks, blocks_for(n_, kT)); }
     void multidot(const double* V, int count, const double* w, int out, double* mpartial) {
         for (int i0 = 0; i0 < count; i0 += kChunk) {
             const int c = std::min(kChunk, count - i0);
-            launch_pdl(ctx_->stream, k_multidot, rb(), kT, n_, V, i0, c, w, mpartial, ctx_->scratch.ticket,
+            launch_pdl(ctx_->stream, k_multidot, wb(), kT, n_, V, i0, c, w, mpartial, ctx_->scratch.ticket,
                                                       slot(out + i0));
             check_launch(ctx_);
         }
@@ -361,11 +365,11 @@ public:
             const int c = std::min(kChunk, count - i0);
             const bool last = i0 + c == count && norm_out >= 0;
             if (last)
-                launch_pdl(ctx_->stream, k_multi_axpy<true>, rb(), kT, n_, V, i0, c, slot(coef + i0), w,
+                launch_pdl(ctx_->stream, k_multi_axpy<true>, wb(), kT, n_, V, i0, c, slot(coef + i0), w,
                                                                  ctx_->scratch.partial, ctx_->scratch.ticket,
                                                                  slot(kMax), slot(kInvalid));
             else
-                launch_pdl(ctx_->stream, k_multi_axpy<false>, rb(), kT, n_, V, i0, c, slot(coef + i0), w, nullptr,
+                launch_pdl(ctx_->stream, k_multi_axpy<false>, blocks_for(n_, kT), kT, n_, V, i0, c, slot(coef + i0), w, nullptr,
                                                                   nullptr, nullptr, nullptr);
             check_launch(ctx_);
         }
