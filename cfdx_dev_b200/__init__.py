@@ -12,6 +12,7 @@ from .api import (  # noqa: F401
     LearnedPreconditioner,
     Mesh,
     NativeBoomerAMGPreconditioner,
+    ReferenceCellGauge,
     SparseMatrix,
     assemble_cell_diffusion_matrix,
     assemble_pressure_correction,

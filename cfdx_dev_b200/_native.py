@@ -157,6 +157,11 @@ PROTOTYPES = {
     "cfdxg_mpnn_set_vcycle": (C.c_int, [_V, _V, _V]),
     "cfdxg_mpnn_train_step": (C.c_int, [_V, _V, _V, _V, C.c_int32, C.c_float, C.c_int32, c_double_p]),
     "cfdxg_mpnn_loss_grad": (C.c_int, [_V, _V, _V, _V, C.c_int32, C.c_int32, c_double_p, _V]),
+    "cfdxg_gauge_create": (C.c_int, [_V, _V, C.c_int32, C.c_int64, C.c_double, _P(_V)]),
+    "cfdxg_gauge_apply": (C.c_int, [_V, _V, _V, _V, C.c_int32, _P(_V), _V]),
+    "cfdxg_gauge_expand": (C.c_int, [_V, _V, _V, C.c_int32, _V]),
+    "cfdxg_gauge_size": (C.c_int, [_V, c_int64_p, c_int64_p]),
+    "cfdxg_gauge_destroy": (C.c_int, [_V]),
     "cfdxg_capture_read": (C.c_int, [C.c_char_p, _P(_V), _P(CaptureInfo)]),
     "cfdxg_capture_export": (C.c_int, [_V] * 6),
     "cfdxg_capture_write": (C.c_int, [C.c_char_p, C.c_int64] + [_V] * 5 + [_P(CaptureInfo)]),

@@ -530,6 +530,60 @@ def solve_cg(A: SparseMatrix, rhs, x0=None, amg: NativeBoomerAMGPreconditioner |
     return solve_gmres(A, rhs, x0, amg, 30, max_iterations, tolerance, krylov="cg")
 
 
+# ---------------------------------------------------------------- pressure gauge
+class ReferenceCellGauge:
+    """Gauge of a pure-Neumann system on the device.
+
+    ``mode="eliminate"``: the pure-Neumann branch of the pressure corrector
+    (physics/steady_incompressible_solver.h:8617-8654) -- the system without
+    cell ``ref``; ``expand`` gives the full correction with 0 at ``ref``.
+    ``mode="identity_row"``: apply_reference_cell_gauge
+    (core/solvers/scalar_diffusion.h:177-210) -- a unit row at ``ref`` and
+    rhs_i -= a_i,ref * value.  The plan is built once from A's pattern; each
+    ``apply`` gathers the current values and right-hand side on the device."""
+
+    MODES = {"eliminate": 0, "identity_row": 1}
+
+    def __init__(self, ctx: Context, A: SparseMatrix, ref: int = 0, mode: str = "eliminate", value: float = 0.0):
+        self.ctx, self.lib = ctx, ctx.lib
+        h = C.c_void_p()
+        ctx.check(self.lib.cfdxg_gauge_create(ctx.handle, A.handle, self.MODES[mode], int(ref), float(value),
+                                              C.byref(h)), "gauge")
+        self.handle = h
+        n, nnz = C.c_int64(), C.c_int64()
+        self.lib.cfdxg_gauge_size(h, C.byref(n), C.byref(nnz))
+        self.n_out, self.nnz_out = n.value, nnz.value
+        self.n = A.n
+        self._gauged = None
+
+    def apply(self, A: SparseMatrix, rhs):
+        """-> (gauged SparseMatrix, gauged right-hand side); the matrix object is
+        reused (values refreshed) on later calls."""
+        b = _f64(rhs, self.n)
+        out = np.empty(self.n_out)
+        h = C.c_void_p(self._gauged.handle.value if self._gauged is not None else None)
+        self.ctx.check(self.lib.cfdxg_gauge_apply(self.ctx.handle, self.handle, A.handle, N.ptr(b),
+                                                  N.CFDXG_MEM_HOST, C.byref(h), N.ptr(out)), "gauge apply")
+        if self._gauged is None:
+            self._gauged = SparseMatrix(self.ctx, h)
+        return self._gauged, out
+
+    def expand(self, x_reduced) -> np.ndarray:
+        xr = _f64(x_reduced, self.n_out)
+        x = np.empty(self.n)
+        self.ctx.check(self.lib.cfdxg_gauge_expand(self.ctx.handle, self.handle, N.ptr(xr), N.CFDXG_MEM_HOST,
+                                                   N.ptr(x)), "gauge expand")
+        return x
+
+    def __del__(self):  # pragma: no cover
+        try:
+            if self.handle:
+                self.lib.cfdxg_gauge_destroy(self.handle)
+                self.handle = None
+        except Exception:
+            pass
+
+
 # ---------------------------------------------------------------- learned preconditioner
 class LearnedPreconditioner:
     """4-round, 32-feature message-passing network on the matrix graph (no

@@ -27,7 +27,7 @@ LIB = OUT / "libcfdxg.so"
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_COMMON = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-I", str(INCLUDE), *ARCH]
 # units whose FP64 arithmetic is compared bit-exactly with the reference
-EXACT_CUDA = {"assembly.cu", "vcycle.cu", "krylov.cu", "matrix.cu", "capi.cu", "galerkin.cu"}
+EXACT_CUDA = {"assembly.cu", "vcycle.cu", "krylov.cu", "matrix.cu", "capi.cu", "galerkin.cu", "gauge.cu"}
 CXXFLAGS = ["-O2", "-std=c++17", "-fPIC", "-pthread", "-ffp-contract=off", f"-I{INCLUDE}"]
 
 

@@ -204,6 +204,34 @@ int cfdxg_gauss_gradient(cfdxg_context* ctx, cfdxg_mesh* mesh, const double* p,
                          double* grad);
 
 /* ------------------------------------------------------------------------ */
+/* Pressure gauge of a pure-Neumann system                                   */
+/* ------------------------------------------------------------------------ */
+/* CFDXG_GAUGE_ELIMINATE replaces the pure-Neumann branch of the pressure
+ * corrector (physics/steady_incompressible_solver.h:8617-8654): the
+ * principal submatrix without row and column ref (later indices shift down
+ * by one) and the right-hand side without entry ref; cfdxg_gauge_expand then
+ * gives the full correction, 0 at ref.  With one unknown the reference keeps
+ * the trivial equation p = 0 instead (:8610-8616); create refuses n == 1.
+ * CFDXG_GAUGE_IDENTITY_ROW replaces apply_reference_cell_gauge
+ * (core/solvers/scalar_diffusion.h:177-210): row and column ref removed, a
+ * unit diagonal at (ref, ref), rhs_i -= a_i,ref * value, rhs_ref = value.
+ * The plan holds the output pattern (built once, on the host, from the input
+ * pattern); cfdxg_gauge_apply gathers values and right-hand side on the
+ * device, creating *gauged on its first call and refreshing its values after
+ * (a matrix of another pattern is refused).  rhs_out must not alias rhs for
+ * the elimination. */
+#define CFDXG_GAUGE_ELIMINATE 0
+#define CFDXG_GAUGE_IDENTITY_ROW 1
+typedef struct cfdxg_gauge cfdxg_gauge;
+int cfdxg_gauge_create(cfdxg_context* ctx, const cfdxg_matrix* A, int32_t mode, int64_t ref, double value,
+                       cfdxg_gauge** out);
+int cfdxg_gauge_apply(cfdxg_context* ctx, const cfdxg_gauge* g, const cfdxg_matrix* A, const double* rhs,
+                      int32_t mem, cfdxg_matrix** gauged, double* rhs_out);
+int cfdxg_gauge_expand(cfdxg_context* ctx, const cfdxg_gauge* g, const double* x_reduced, int32_t mem, double* x);
+int cfdxg_gauge_size(const cfdxg_gauge* g, int64_t* n_out, int64_t* nnz_out);
+int cfdxg_gauge_destroy(cfdxg_gauge* g);
+
+/* ------------------------------------------------------------------------ */
 /* native AMG preconditioner                                                 */
 /* Replaces NativeBoomerAMGPreconditioner (core/linalg/hypre_amg.h:26-101,    */
 /* hypre_amg.cpp:163-330): setup / update_values / apply / name / last_error. */

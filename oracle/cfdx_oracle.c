@@ -1140,3 +1140,61 @@ out:
     free(r); free(rv); free(z); free(p); free(Ap); free(M);
     return rc;
 }
+
+/* ------------------------------------------------------------- gauge */
+
+/* physics/steady_incompressible_solver.h:8617-8654, the pure-Neumann branch of
+ * the pressure corrector: skip row ref, skip column ref in every other row,
+ * shift later indices down by one, keep b without entry ref. */
+int64_t co_gauge_eliminate(int64_t n, const int64_t* ro, const int64_t* co, const double* va, const double* b,
+                           int64_t ref, int64_t* ro_out, int64_t* co_out, double* va_out, double* b_out) {
+    if (n <= 1 || ref < 0 || ref >= n) return fail("gauge: invalid size or reference cell");
+    int64_t nnz = 0, r = 0;
+    ro_out[0] = 0;
+    for (int64_t i = 0; i < n; ++i) {
+        if (i == ref) continue;
+        b_out[r] = b[i];
+        for (int64_t k = ro[i]; k < ro[i + 1]; ++k) {
+            if (co[k] == ref) continue;
+            co_out[nnz] = co[k] < ref ? co[k] : co[k] - 1;
+            va_out[nnz] = va[k];
+            ++nnz;
+        }
+        ro_out[++r] = nnz;
+    }
+    return nnz;
+}
+
+/* :8645-8653: p_corr(cell) = reduced(cell < ref ? cell : cell - 1), p_corr(ref) = 0 */
+void co_gauge_expand(int64_t n, const double* x_reduced, int64_t ref, double* x) {
+    for (int64_t i = 0; i < n; ++i) x[i] = i == ref ? 0.0 : x_reduced[i < ref ? i : i - 1];
+}
+
+/* core/solvers/scalar_diffusion.h:177-210 apply_reference_cell_gauge */
+int64_t co_gauge_identity_row(int64_t n, const int64_t* ro, const int64_t* co, const double* va, const double* b,
+                              int64_t ref, double value, int64_t* ro_out, int64_t* co_out, double* va_out,
+                              double* b_out) {
+    if (n <= 0 || ref < 0 || ref >= n || !isfinite(value)) return fail("gauge: invalid arguments");
+    int64_t nnz = 0;
+    ro_out[0] = 0;
+    for (int64_t i = 0; i < n; ++i) {
+        double a_iref = 0.0;   /* matrix(i, ref): the sum of the row's entries in column ref */
+        for (int64_t k = ro[i]; k < ro[i + 1]; ++k)
+            if (co[k] == ref) a_iref += va[k];
+        b_out[i] = i == ref ? value : b[i] - a_iref * value;
+        if (i == ref) {
+            co_out[nnz] = ref;
+            va_out[nnz] = 1.0;
+            ++nnz;
+        } else {
+            for (int64_t k = ro[i]; k < ro[i + 1]; ++k) {
+                if (co[k] == ref) continue;
+                co_out[nnz] = co[k];
+                va_out[nnz] = va[k];
+                ++nnz;
+            }
+        }
+        ro_out[i + 1] = nnz;
+    }
+    return nnz;
+}

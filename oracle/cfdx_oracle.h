@@ -142,6 +142,22 @@ int co_solve_cg(int64_t n, const int64_t* row_offsets, const int64_t* columns,
                 const double* b, double* x, int64_t max_iterations, double tolerance,
                 co_report_t* report);
 
+/* Pressure gauge of a pure-Neumann system.  co_gauge_eliminate: the
+ * pure-Neumann branch of the corrector (physics/steady_incompressible_solver.h
+ * :8617-8654), the principal submatrix without row/column ref and b without
+ * entry ref (returns nnz, outputs sized n, nnz_in, nnz_in, n - 1);
+ * co_gauge_expand: the full correction with 0 at ref (:8645-8653);
+ * co_gauge_identity_row: core/solvers/scalar_diffusion.h:177-210
+ * apply_reference_cell_gauge (returns nnz; outputs sized n + 1, nnz_in + 1,
+ * nnz_in + 1, n). */
+int64_t co_gauge_eliminate(int64_t n, const int64_t* row_offsets, const int64_t* columns, const double* values,
+                           const double* b, int64_t ref, int64_t* ro_out, int64_t* co_out, double* va_out,
+                           double* b_out);
+void co_gauge_expand(int64_t n, const double* x_reduced, int64_t ref, double* x);
+int64_t co_gauge_identity_row(int64_t n, const int64_t* row_offsets, const int64_t* columns, const double* values,
+                              const double* b, int64_t ref, double value, int64_t* ro_out, int64_t* co_out,
+                              double* va_out, double* b_out);
+
 #ifdef __cplusplus
 }
 #endif

@@ -249,3 +249,38 @@ def solve_cg(ro, co, va, b, preconditioner="native_amg", hierarchy=None, x0=None
                              hierarchy.ptr if hierarchy else None, _p(b), _p(x), int(max_iterations),
                              float(tolerance), C.byref(rep)), "CG")
     return x, rep.as_dict()
+
+
+def gauge_eliminate(ro, co, va, b, ref):
+    """co_gauge_eliminate: (row_offsets, columns, values, b) of the system without cell ref."""
+    ro, co, va, b = (np.ascontiguousarray(ro, np.int64), np.ascontiguousarray(co, np.int64), _f64(va), _f64(b))
+    n = b.size
+    f = lib().co_gauge_eliminate
+    f.restype = C.c_int64
+    f.argtypes = [C.c_int64] + [C.c_void_p] * 4 + [C.c_int64] + [C.c_void_p] * 4
+    ro_o, co_o, va_o, b_o = np.empty(n, np.int64), np.empty(co.size, np.int64), np.empty(va.size), np.empty(n - 1)
+    nnz = _check(f(n, _p(ro), _p(co), _p(va), _p(b), int(ref), _p(ro_o), _p(co_o), _p(va_o), _p(b_o)), "gauge")
+    return ro_o, co_o[:nnz].copy(), va_o[:nnz].copy(), b_o
+
+
+def gauge_expand(x_reduced, ref):
+    xr = _f64(x_reduced)
+    x = np.empty(xr.size + 1)
+    f = lib().co_gauge_expand
+    f.argtypes = [C.c_int64, C.c_void_p, C.c_int64, C.c_void_p]
+    f(x.size, _p(xr), int(ref), _p(x))
+    return x
+
+
+def gauge_identity_row(ro, co, va, b, ref, value=0.0):
+    """co_gauge_identity_row: apply_reference_cell_gauge (scalar_diffusion.h:177-210)."""
+    ro, co, va, b = (np.ascontiguousarray(ro, np.int64), np.ascontiguousarray(co, np.int64), _f64(va), _f64(b))
+    n = b.size
+    f = lib().co_gauge_identity_row
+    f.restype = C.c_int64
+    f.argtypes = [C.c_int64] + [C.c_void_p] * 4 + [C.c_int64, C.c_double] + [C.c_void_p] * 4
+    ro_o, co_o, va_o, b_o = (np.empty(n + 1, np.int64), np.empty(co.size + 1, np.int64), np.empty(va.size + 1),
+                             np.empty(n))
+    nnz = _check(f(n, _p(ro), _p(co), _p(va), _p(b), int(ref), float(value), _p(ro_o), _p(co_o), _p(va_o),
+                   _p(b_o)), "gauge")
+    return ro_o, co_o[:nnz].copy(), va_o[:nnz].copy(), b_o

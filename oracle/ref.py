@@ -346,3 +346,18 @@ def solve_cg_internal(ro, co, va, rhs, x0=None, max_iterations=1000, tolerance=1
     rep = RefReport()
     _check(f(b.size, _p(ro), _p(co), _p(va), _p(b), _p(x), max_iterations, tolerance, C.byref(rep)), "solve_cg")
     return x, rep.as_dict()
+
+
+def apply_reference_cell_gauge(ro, co, va, rhs, ref, value=0.0):
+    """The reference's apply_reference_cell_gauge (scalar_diffusion.h:177-210)."""
+    f = lib().ref_apply_reference_cell_gauge
+    f.restype = C.c_int64
+    f.argtypes = [C.c_int64] + [C.c_void_p] * 4 + [C.c_int64, C.c_double] + [C.c_void_p] * 4
+    ro, co = np.ascontiguousarray(ro, np.int64), np.ascontiguousarray(co, np.int64)
+    va, b = np.ascontiguousarray(va, np.float64), np.ascontiguousarray(rhs, np.float64)
+    n = b.size
+    ro_o, co_o, va_o, b_o = (np.empty(n + 1, np.int64), np.empty(co.size + 1, np.int64), np.empty(va.size + 1),
+                             np.empty(n))
+    nnz = _check(f(n, _p(ro), _p(co), _p(va), _p(b), int(ref), float(value), _p(ro_o), _p(co_o), _p(va_o), _p(b_o)),
+                 "apply_reference_cell_gauge")
+    return ro_o, co_o[:nnz].copy(), va_o[:nnz].copy(), b_o

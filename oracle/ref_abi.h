@@ -135,6 +135,10 @@ int ref_read_capture(const char* path, int64_t* meta /* n, nnz, problem, null_sp
 int ref_solve_cg_internal(int64_t n, const int64_t* row_offsets, const int64_t* columns, const double* values,
                           const double* rhs, double* x, int64_t max_iterations, double tolerance,
                           ref_report_t* report);
+/* core/solvers/scalar_diffusion.h:177-210 apply_reference_cell_gauge (returns the output nnz) */
+int64_t ref_apply_reference_cell_gauge(int64_t n, const int64_t* row_offsets, const int64_t* columns,
+                                       const double* values, const double* rhs, int64_t ref, double value,
+                                       int64_t* ro_out, int64_t* co_out, double* va_out, double* rhs_out);
 /* one SpMV with SparseMatrix::matvec (sparse_matrix.h:180) */
 int ref_spmv(int64_t n, const int64_t* row_offsets, const int64_t* columns,
              const double* values, const double* x, double* y);

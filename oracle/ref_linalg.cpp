@@ -241,3 +241,27 @@ extern "C" int ref_solve_cg_internal(int64_t n, const int64_t* ro, const int64_t
         return -1;
     }
 }
+
+// core/solvers/scalar_diffusion.h:177-210 apply_reference_cell_gauge; the
+// output CSR has at most nnz + 1 entries and n + 1 offsets.  Returns its nnz.
+extern "C" int64_t ref_apply_reference_cell_gauge(int64_t n, const int64_t* ro, const int64_t* co, const double* va,
+                                                  const double* rhs, int64_t ref, double value, int64_t* ro_out,
+                                                  int64_t* co_out, double* va_out, double* rhs_out) {
+    try {
+        const SparseMatrix A = cfdx_ref::make_csr(n, ro, co, va);
+        Vector b(static_cast<std::size_t>(n));
+        for (int64_t i = 0; i < n; ++i) b(i) = rhs[i];
+        const SparseMatrix G = apply_reference_cell_gauge(A, b, static_cast<std::size_t>(ref), value);
+        for (std::size_t i = 0; i <= G.n_rows(); ++i) ro_out[i] = G.row_offsets_data()[i];
+        for (std::size_t k = 0; k < G.nnz(); ++k) {
+            co_out[k] = G.columns_data()[k];
+            va_out[k] = G.values_data()[k];
+        }
+        for (int64_t i = 0; i < n; ++i) rhs_out[i] = b(i);
+        cfdx_ref::g_error.clear();
+        return static_cast<int64_t>(G.nnz());
+    } catch (const std::exception& e) {
+        cfdx_ref::set_error(e);
+        return -1;
+    }
+}

@@ -442,3 +442,49 @@ def test_half_values_fp32_vcycle(ctx, tet_setup):
     assert rel_l2(half.apply(r), full.apply(r)) < 1e-2
     x2, rep2 = cg.solve_fgmres(A2, b2, amg=half, restart=30, tolerance=1e-8)
     assert rep2["status_name"] == "converged" and rep2["physical_residual_relative"] <= 1e-8
+
+
+# ---------------------------------------------------------------- pure-Neumann gauge
+def test_pure_neumann_gauge_matches_oracle(ctx, oracle):
+    """Every patch zero-gradient: the corrector's reference-cell elimination
+    (steady_incompressible_solver.h:8617-8654) and apply_reference_cell_gauge
+    (scalar_diffusion.h:177-210) on the device equal the oracle's bit for bit,
+    twice on one plan (the second time with new values); the eliminated
+    system's AMG-GMRES solve and its expansion match the oracle's."""
+    m = cases.simple_mesh(8)
+    mesh = cg.Mesh(ctx, m)
+    g = mesh.geometry()
+    ref_cell = 37
+    gauge = ident = None
+    A = None
+    for off in (0, 5):
+        U, rAU, aP, p, fixed, value = cases.simple_fields(m, g["cell_centres"], seed_offset=off)
+        fixed[:] = 0
+        A, b, phi, grad = cg.assemble_pressure_correction(mesh, U, rAU, p, 1.0, fixed, value, matrix=A)
+        ro, co, va = A.to_csr()
+        if gauge is None:
+            gauge = cg.ReferenceCellGauge(ctx, A, ref=ref_cell)
+            ident = cg.ReferenceCellGauge(ctx, A, ref=ref_cell, mode="identity_row", value=0.5)
+        B, bB = gauge.apply(A, b)
+        expect = oracle.gauge_eliminate(ro, co, va, b, ref_cell)
+        for got, want in zip(B.to_csr() + (bB,), expect):
+            assert np.array_equal(got, want)
+        C, bC = ident.apply(A, b)
+        expect = oracle.gauge_identity_row(ro, co, va, b, ref_cell, 0.5)
+        for got, want in zip(C.to_csr() + (bC,), expect):
+            assert np.array_equal(got, want)
+    amg = cg.NativeBoomerAMGPreconditioner(ctx)
+    assert amg.setup(B)
+    e_ro, e_co, e_va, e_b = expect_elim = oracle.gauge_eliminate(ro, co, va, b, ref_cell)
+    x_ref, rep_ref = oracle.solve_gmres(e_ro, e_co, e_va, e_b, oracle_hierarchy(oracle, amg), restart=30,
+                                        tolerance=1e-8)
+    xr, rep = cg.solve_gmres(B, bB, amg=amg, restart=30, tolerance=1e-8)
+    assert rep["status_name"] == "converged" and rep["iterations"] == rep_ref["iterations"]
+    assert rel_l2(xr, x_ref) <= REL_TOL
+    x = gauge.expand(xr)
+    assert x[ref_cell] == 0.0 and np.array_equal(x, oracle.gauge_expand(xr, ref_cell))
+    # the full system is satisfied on every row but the reference cell's
+    res = b - oracle.spmv(ro, co, va, x)
+    assert np.linalg.norm(np.delete(res, ref_cell)) <= 1e-8 * np.linalg.norm(np.delete(b, ref_cell)) * 1.0001
+    with pytest.raises(cg.CfdxgError):
+        cg.ReferenceCellGauge(ctx, A, ref=A.n)
