@@ -29,6 +29,7 @@ from .api import (  # noqa: F401
     solve_fgmres,
     solve_gmres,
     solve_linear_system,
+    solve_poisson_mixed,
     tet_case,
     write_linear_system_capture,
 )

@@ -13,7 +13,7 @@ LIB_PATH = Path(__file__).resolve().parent / "_lib" / "libcfdxg.so"
 CFDXG_MEM_HOST = 0
 CFDXG_MEM_DEVICE = 1
 KRYLOV = {"cg": 1, "gmres": 3, "fgmres": 4}
-PRECONDITIONER = {"none": 1, "jacobi": 2, "native_amg": 6}
+PRECONDITIONER = {"none": 1, "jacobi": 2, "native_amg": 6, "own_diagonal": 32}
 PRECISION = {"fp64": 0, "fp32_vcycle": 1}
 STATUS = {0: "converged", 1: "max_iter_reached", 2: "diverged", 3: "not_applicable"}
 ERRORS = {

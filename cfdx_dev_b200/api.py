@@ -308,6 +308,47 @@ def assemble_cell_diffusion_matrix(mesh: Mesh, bc_face_values, diffusivity, sour
     return SparseMatrix(ctx, h), rhs
 
 
+def solve_poisson_mixed(mesh: Mesh, bc_face_values, source, bc_face_types=None, diffusivity=1.0,
+                        max_iterations=2000, tolerance=1e-10, reference_cell=0, reference_value=0.0,
+                        compatibility_tolerance=1e-12) -> dict:
+    """solve_poisson_mixed (core/solvers/scalar_diffusion.h:294-340), the
+    Poisson driver of the reference's apps/poisson: cell-centred diffusion
+    assembly; without a Dirichlet face the pure-Neumann compatibility check
+    (:306-325) and the reference-cell identity-row gauge (:326-333); then CG
+    with the solver's own diagonal scaling, from zero (the reference value at
+    the reference cell).  bc_face_types: 0 Dirichlet (default), 1 Neumann
+    (prescribed flux).  Returns dict(solution, report, matrix, rhs); ValueError
+    on incompatible pure-Neumann data."""
+    A, rhs = assemble_cell_diffusion_matrix(mesh, bc_face_values, diffusivity, source, bc_face_types)
+    bcv = _f64(bc_face_values, mesh.host.n_faces)
+    types = np.zeros(bcv.size, np.int32) if bc_face_types is None else _i32(bc_face_types)
+    x0 = np.zeros(A.n)
+    finite = np.isfinite(bcv)
+    if not np.any(finite & (types == 0)):
+        # scalar_diffusion.h:223-238 pure_neumann_compatibility_residual and the scale of :309-317
+        g = mesh.geometry()
+        vol = g["cell_volumes"]
+        area = np.linalg.norm(g["face_Sf"].reshape(3, -1), axis=0)
+        src = _f64(source, A.n)
+        neumann = finite & (types == 1)
+        balance = 0.0
+        for c in range(A.n):
+            balance += src[c] * vol[c]
+        for f in np.flatnonzero(neumann):
+            balance += bcv[f] * area[f]
+        scale = 1.0 + float(np.sum(np.abs(src) * vol)) + float(np.sum(np.abs(bcv[neumann]) * area[neumann]))
+        if not np.isfinite(balance) or not (compatibility_tolerance >= 0.0) or \
+                abs(balance) > compatibility_tolerance * scale:
+            raise ValueError("solve_poisson_mixed: incompatible pure-Neumann data; "
+                             "integral(S dV) + integral(q_n dA) must be zero")
+        gauge = ReferenceCellGauge(A.ctx, A, ref=reference_cell, mode="identity_row", value=reference_value)
+        A, rhs = gauge.apply(A, rhs)
+        x0[reference_cell] = reference_value
+    x, report = solve_linear_system(A, rhs, x0, krylov="cg", preconditioner="own_diagonal",
+                                    max_iterations=max_iterations, tolerance=tolerance)
+    return dict(solution=x, report=report, matrix=A, rhs=rhs)
+
+
 def assemble_pressure_correction(mesh: Mesh, HbyA, rAU, p, rho=1.0, p_bc_fixed=None, p_bc_value=None,
                                  matrix: SparseMatrix | None = None):
     """Pressure-corrector assembly (steady_incompressible_solver.h:8048-8181).

@@ -32,6 +32,28 @@ __global__ void k_first_diag_inverse(int n, const int* ro, const int* co, const 
     atomicOr(status, kStatusNonFinite);
 }
 
+// The solver's own diagonal (cg_solver.h:171-189, no preconditioner object):
+// the first diagonal entry of each row, which must be positive and finite.
+__global__ void k_first_diag_positive(int n, const int* ro, const int* co, const double* va, double* d,
+                                      int* status) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    double v = 0.0;
+    for (int k = ro[i]; k < ro[i + 1]; ++k)
+        if (co[k] == i) {
+            v = va[k];
+            break;
+        }
+    d[i] = v;
+    if (!(v > 0.0) || !isfinite(v)) atomicOr(status, kStatusNonFinite);
+}
+
+// z = r / d (cg_solver.h:212)
+__global__ void k_div_diag(int n, const double* d, const double* r, double* z) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) z[i] = r[i] / d[i];
+}
+
 __global__ void k_scale(int n, const double* a, const double* b, double* out) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i < n) out[i] = a[i] * b[i];
@@ -620,13 +642,19 @@ KrylovResult run_krylov(cfdxg_context* ctx, const cfdxg_matrix* A, cfdxg_amg* am
                 check_launch(ctx);
                 return true;
             };
+        else if (req.preconditioner == CFDXG_PC_OWN_DIAGONAL)   // inv_diag holds the diagonal itself
+            pc = [ctx, inv_diag, n](const double* v, double* z, int) {
+                k_div_diag<<<blocks_for(n, 256), 256, 0, ctx->stream>>>(n, inv_diag, v, z);
+                check_launch(ctx);
+                return true;
+            };
         else
             pc = [ctx, n](const double* v, double* z, int) {
                 k_copy<<<blocks_for(n, 256), 256, 0, ctx->stream>>>(n, v, z);
                 check_launch(ctx);
                 return true;
             };
-        return cg_solve(ctx, A, b, x, max_it, tol, pc, cg_setup);
+        return cg_solve(ctx, A, b, x, max_it, tol, pc, cg_setup, req.preconditioner == CFDXG_PC_OWN_DIAGONAL);
     }
     // Learned stage: dropped for the rest of the solve (plain AMG fallback)
     // as soon as an iteration fails to cut the residual estimate by 10%.
@@ -680,8 +708,10 @@ void validate_request(const cfdxg_request& r) {
     if (r.krylov == CFDXG_KRYLOV_CG && r.learned)
         throw Error(CFDXG_ERR_INVALID_ARGUMENT, "the learned stage is a variable preconditioner: it needs FGMRES");
     if (r.preconditioner != CFDXG_PC_NONE && r.preconditioner != CFDXG_PC_JACOBI &&
-        r.preconditioner != CFDXG_PC_NATIVE_AMG)
+        r.preconditioner != CFDXG_PC_NATIVE_AMG && r.preconditioner != CFDXG_PC_OWN_DIAGONAL)
         throw Error(CFDXG_ERR_INVALID_ARGUMENT, "requested preconditioner model is not implemented");
+    if (r.preconditioner == CFDXG_PC_OWN_DIAGONAL && r.krylov != CFDXG_KRYLOV_CG)
+        throw Error(CFDXG_ERR_INVALID_ARGUMENT, "the solver's own diagonal scaling is CG's");
     if (r.precision != CFDXG_PRECISION_FP64 && r.precision != CFDXG_PRECISION_FP32_VCYCLE)
         throw Error(CFDXG_ERR_INVALID_ARGUMENT, "unknown precision");
     if (r.learned && r.preconditioner != CFDXG_PC_NATIVE_AMG)
@@ -745,7 +775,7 @@ extern "C" int cfdxg_solve_linear_system(cfdxg_context* ctx, const cfdxg_matrix*
         cfdxg_amg_options_default(&amg.opts);
         amg.opts.precision = req.precision;
         amg.opts.require_smoother_certificate = 1;
-        DevBuf<double> inv(req.preconditioner == CFDXG_PC_JACOBI ? n : 0);
+        DevBuf<double> inv(req.preconditioner == CFDXG_PC_JACOBI || req.preconditioner == CFDXG_PC_OWN_DIAGONAL ? n : 0);
         std::function<bool()> setup = [&]() {
             if (req.preconditioner == CFDXG_PC_NATIVE_AMG) {
                 try {
@@ -762,6 +792,13 @@ extern "C" int cfdxg_solve_linear_system(cfdxg_context* ctx, const cfdxg_matrix*
             if (req.preconditioner == CFDXG_PC_JACOBI) {
                 clear_status(ctx);
                 k_first_diag_inverse<<<blocks_for(n, 256), 256, 0, ctx->stream>>>(
+                    static_cast<int>(n), A->ro.get(), A->co.get(), A->va.get(), inv.get(), ctx->scratch.status);
+                check_launch(ctx);
+                return read_status(ctx) == 0;
+            }
+            if (req.preconditioner == CFDXG_PC_OWN_DIAGONAL) {
+                clear_status(ctx);
+                k_first_diag_positive<<<blocks_for(n, 256), 256, 0, ctx->stream>>>(
                     static_cast<int>(n), A->ro.get(), A->co.get(), A->va.get(), inv.get(), ctx->scratch.status);
                 check_launch(ctx);
                 return read_status(ctx) == 0;

@@ -842,7 +842,8 @@ KrylovResult gmres_solve(cfdxg_context* ctx, const cfdxg_matrix* A, const double
 // scaled norm, ||r||^2 -- and one read-back of eight scalars, after which the
 // host takes the reference's decisions in the reference's order.
 KrylovResult cg_solve(cfdxg_context* ctx, const cfdxg_matrix* A, const double* b, double* x, int64_t max_iter,
-                      double tolerance, const RightPreconditioner& pc, const std::function<bool()>* setup) {
+                      double tolerance, const RightPreconditioner& pc, const std::function<bool()>* setup,
+                      bool own_diagonal) {
     KrylovResult result;
     const int64_t n = A->n;
     if (n == 0) return result;   // NOT_APPLICABLE
@@ -944,6 +945,33 @@ KrylovResult cg_solve(cfdxg_context* ctx, const cfdxg_matrix* A, const double* b
         const double rsnew = E.host(kCgRsNew);
         if (!std::isfinite(rsnew)) return failed(CFDXG_DIVERGED, iter, res);
         if (res <= tol_abs) return finish(CFDXG_CONVERGED, iter, res);
+        if (own_diagonal) {
+            // :321-352 the solver's own diagonal: replace the recursive residual
+            // when it claims convergence that b - A x does not confirm
+            const double rr = std::sqrt(E.host(kCgRR2));
+            if (std::isfinite(rr) && rr <= tol_abs && res > tol_abs) {
+                ++result.residual_replacements;
+                if (result.first_residual_replacement == 0) result.first_residual_replacement = iter;
+                result.last_residual_replacement = iter;
+                E.copy(r, rv);
+                zero_flags();
+                if (!apply()) return failed(CFDXG_NOT_APPLICABLE, iter, res);
+                dot_check(r, z.get(), kCgRsOld);
+                E.copy(p.get(), z.get());
+                E.fetch(kCgCount);
+                const double replaced = E.host(kCgRsOld);
+                if (E.host(kCgZBad) > 0.0) return failed(CFDXG_NOT_APPLICABLE, iter, res);
+                if (!std::isfinite(replaced) || !(replaced > 0.0)) return finish(CFDXG_MAX_ITER_REACHED, iter, res);
+                rsold = replaced;
+                continue;
+            }
+            k_cg_direction<<<gb, kT, 0, ctx->stream>>>(ni, p.get(), z.get(), E.slot(0));
+            check_launch(ctx);
+            CFDXG_CUDA(cudaMemcpyAsync(E.slot(kCgRsOld), E.slot(kCgRsNew), sizeof(double), cudaMemcpyDeviceToDevice,
+                                       ctx->stream));
+            rsold = rsnew;
+            continue;
+        }
         // :399-525 adaptive residual replacement and collapse repair
         const double rr = std::sqrt(E.host(kCgRR2));
         const double gap = std::abs(res - rr);

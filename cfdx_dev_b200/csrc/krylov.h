@@ -55,9 +55,13 @@ KrylovResult gmres_solve(cfdxg_context* ctx, const cfdxg_matrix* A, const double
 // core/linalg/cg_solver.h:45-560 with a preconditioner object (pc, its j
 // argument unused); `setup`, when given, runs after the initial-residual
 // check as the reference's setup_preconditioner and a false return makes the
-// solve NOT_APPLICABLE.
+// solve NOT_APPLICABLE.  own_diagonal: pc divides by the matrix diagonal and
+// the solve follows the solver's own-diagonal branch (no preconditioner
+// object, the legacy solve_cg overload, cg_solver.h:591-603) -- its residual
+// replacement rule instead of the adaptive one.
 KrylovResult cg_solve(cfdxg_context* ctx, const cfdxg_matrix* A, const double* b, double* x, int64_t max_iter,
-                      double tolerance, const RightPreconditioner& pc, const std::function<bool()>* setup);
+                      double tolerance, const RightPreconditioner& pc, const std::function<bool()>* setup,
+                      bool own_diagonal = false);
 
 // Scaled two-pass 2-norm of a device vector (krylov_norm2).
 double device_norm2(cfdxg_context* ctx, const cfdxg_matrix* A, const double* a);

@@ -53,6 +53,9 @@ extern "C" {
 #define CFDXG_PC_NONE 1
 #define CFDXG_PC_JACOBI 2
 #define CFDXG_PC_NATIVE_AMG 6
+#define CFDXG_PC_OWN_DIAGONAL 32    /* CG only: the solver's own diagonal scaling, i.e. solve_cg
+                                       without a preconditioner object (cg_solver.h:591-603), as
+                                       solve_poisson_mixed calls it (scalar_diffusion.h:336-338) */
 #define CFDXG_PRECISION_FP64 0      /* the reference's plain FP64 V-cycle */
 #define CFDXG_PRECISION_FP32_VCYCLE 1  /* FP32 V-cycle inside FP64 FGMRES */
 #define CFDXG_ORTHO_MGS2 0          /* two-pass modified Gram-Schmidt, gmres_solver.h:270-295 */

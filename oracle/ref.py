@@ -361,3 +361,21 @@ def apply_reference_cell_gauge(ro, co, va, rhs, ref, value=0.0):
     nnz = _check(f(n, _p(ro), _p(co), _p(va), _p(b), int(ref), float(value), _p(ro_o), _p(co_o), _p(va_o), _p(b_o)),
                  "apply_reference_cell_gauge")
     return ro_o, co_o[:nnz].copy(), va_o[:nnz].copy(), b_o
+
+
+def solve_poisson_mixed(mesh, bc_values, source, bc_types=None, diffusivity=1.0, max_iterations=2000,
+                        tolerance=1e-10, reference_cell=0, reference_value=0.0):
+    """The reference's solve_poisson_mixed (scalar_diffusion.h:294-340) -> (x, report)."""
+    f = lib().ref_solve_poisson_mixed
+    f.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_double, C.c_void_p, C.c_int64, C.c_double, C.c_int64,
+                  C.c_double, C.c_void_p, C.c_void_p]
+    h = _MeshHolder(mesh)
+    nc = mesh.cell_offsets.size - 1
+    bc = np.ascontiguousarray(bc_values, np.float64)
+    ty = None if bc_types is None else np.ascontiguousarray(bc_types, np.int32)
+    src = np.ascontiguousarray(source, np.float64)
+    x = np.empty(nc)
+    rep = RefReport()
+    _check(f(h.ptr, _p(bc), _p(ty), float(diffusivity), _p(src), int(max_iterations), float(tolerance),
+             int(reference_cell), float(reference_value), _p(x), C.byref(rep)), "solve_poisson_mixed")
+    return x, rep.as_dict()

@@ -139,6 +139,10 @@ int ref_solve_cg_internal(int64_t n, const int64_t* row_offsets, const int64_t* 
 int64_t ref_apply_reference_cell_gauge(int64_t n, const int64_t* row_offsets, const int64_t* columns,
                                        const double* values, const double* rhs, int64_t ref, double value,
                                        int64_t* ro_out, int64_t* co_out, double* va_out, double* rhs_out);
+/* core/solvers/scalar_diffusion.h:294-340 solve_poisson_mixed; types NULL = all Dirichlet */
+int ref_solve_poisson_mixed(const ref_mesh_t* m, const double* bc, const int32_t* types, double gamma,
+                            const double* source, int64_t max_iterations, double tolerance, int64_t reference_cell,
+                            double reference_value, double* x, ref_report_t* report);
 /* one SpMV with SparseMatrix::matvec (sparse_matrix.h:180) */
 int ref_spmv(int64_t n, const int64_t* row_offsets, const int64_t* columns,
              const double* values, const double* x, double* y);

@@ -265,3 +265,41 @@ extern "C" int64_t ref_apply_reference_cell_gauge(int64_t n, const int64_t* ro, 
         return -1;
     }
 }
+
+// core/solvers/scalar_diffusion.h:294-340 solve_poisson_mixed (the apps/poisson
+// driver): types NULL = all Dirichlet, else 0 Dirichlet / 1 Neumann per face.
+extern "C" int ref_solve_poisson_mixed(const ref_mesh_t* m, const double* bc, const int32_t* types, double gamma,
+                                       const double* source, int64_t max_iterations, double tolerance,
+                                       int64_t reference_cell, double reference_value, double* x,
+                                       ref_report_t* report) {
+    try {
+        const Mesh mesh = cfdx_ref::make_mesh(*m);
+        PoissonBoundaryCondition boundary = PoissonBoundaryCondition::mixed(mesh.n_faces());
+        for (std::size_t f = 0; f < mesh.n_faces(); ++f) {
+            boundary.face_values[f] = bc[f];
+            boundary.face_types[f] = (types && types[f] == 1) ? PoissonBoundaryType::NEUMANN
+                                                               : PoissonBoundaryType::DIRICHLET;
+        }
+        const std::vector<double> src(source, source + m->n_cells);
+        ScalarDiffusionConfig config;
+        config.diffusivity = gamma;
+        config.max_iterations = static_cast<std::size_t>(max_iterations);
+        config.tolerance = tolerance;
+        config.gauge.reference_cell = static_cast<std::size_t>(reference_cell);
+        config.gauge.reference_value = reference_value;
+        const ScalarDiffusionResult r = solve_poisson_mixed(mesh, boundary, src, config);
+        for (int64_t i = 0; i < m->n_cells; ++i) x[i] = r.solution(i);
+        if (report) {
+            std::memset(report, 0, sizeof(*report));
+            report->status = static_cast<int32_t>(r.linear_result.status);
+            report->iterations = static_cast<int64_t>(r.linear_result.iterations);
+            report->residual = r.linear_result.residual;
+            report->residual_relative = r.linear_result.residual_relative;
+        }
+        cfdx_ref::g_error.clear();
+        return 0;
+    } catch (const std::exception& e) {
+        cfdx_ref::set_error(e);
+        return -1;
+    }
+}

@@ -488,3 +488,33 @@ def test_pure_neumann_gauge_matches_oracle(ctx, oracle):
     assert np.linalg.norm(np.delete(res, ref_cell)) <= 1e-8 * np.linalg.norm(np.delete(b, ref_cell)) * 1.0001
     with pytest.raises(cg.CfdxgError):
         cg.ReferenceCellGauge(ctx, A, ref=A.n)
+
+
+# ---------------------------------------------------------------- Poisson driver
+@pytest.mark.parametrize("kind", ["dirichlet", "neumann"])
+def test_poisson_driver_matches_oracle(ctx, oracle, kind):
+    """solve_poisson_mixed (scalar_diffusion.h:294-340) on the device against
+    the oracle's composition, itself bit-identical to the reference's driver:
+    the apps/poisson case and a pure-Neumann case with the reference-cell
+    gauge.  The own-diagonal CG takes tens of iterations with parallel dots, so
+    the count may differ by 2 and the solution by CG_LONG_TOL; each solve is
+    certified to its 1e-10 residual."""
+    from tests.test_poisson_driver import apps_poisson_case, neumann_case, oracle_poisson_mixed
+    if kind == "dirichlet":
+        m, bc, src = apps_poisson_case(8)
+        types, cell, value = None, 0, 0.0
+    else:
+        m, bc, src, types = neumann_case(8)
+        cell, value = 11, 1.5
+    x_ref, rep_ref = oracle_poisson_mixed(m, bc, src, types, ref_cell=cell, ref_value=value)
+    mesh = cg.Mesh(ctx, m)
+    out = cg.solve_poisson_mixed(mesh, bc, src, types, reference_cell=cell, reference_value=value)
+    rep = out["report"]
+    assert rep["status_name"] == "converged" and rep_ref["status"] == 0
+    assert rep["physical_residual_relative"] <= 1e-10
+    assert abs(rep["iterations"] - rep_ref["iterations"]) <= 2
+    assert rel_l2(out["solution"], x_ref) <= CG_LONG_TOL
+    if kind == "neumann":
+        assert out["solution"][cell] == value
+        with pytest.raises(ValueError):
+            cg.solve_poisson_mixed(mesh, bc, src + 1.0, types)
