@@ -314,8 +314,12 @@ __global__ void __launch_bounds__(kRoundThreads) k_round_gather_tc(
     }
     __syncthreads();
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int c0 = (blockIdx.x * kRoundWarps + warp) * kTileCells;
-    if (c0 >= n) return;
+    Encoder enc;
+    if constexpr (FIRST) enc.load(reinterpret_cast<const float4*>(feats), P, lane & 7);
+    // persistent: each warp walks tiles with the grid's stride, the weights
+    // staged once per block
+    for (int tile = blockIdx.x * kRoundWarps + warp; tile * kTileCells < n; tile += gridDim.x * kRoundWarps) {
+    const int c0 = tile * kTileCells;
     const int cells = min(kTileCells, n - c0);
     // tile segment of the coupling list
     const int seg_b = gro[c0], seg_e = gro[c0 + cells];
@@ -330,8 +334,6 @@ __global__ void __launch_bounds__(kRoundThreads) k_round_gather_tc(
         rb = gro[c0 + lane];
         re = gro[c0 + lane + 1];
     }
-    Encoder enc;
-    if constexpr (FIRST) enc.load(reinterpret_cast<const float4*>(feats), P, lane & 7);
     __syncwarp();
     if (staged)
         gather_tile<true, FIRST>(c0, cells, rb, re, seg_b, sIdx[warp], sW[warp], gco, gew, h_in, enc, sH[warp],
@@ -420,6 +422,8 @@ __global__ void __launch_bounds__(kRoundThreads) k_round_gather_tc(
                 *reinterpret_cast<uint32_t*>(&h_out[static_cast<size_t>(c0 + rowb) * F + col]) =
                     pack_bf16(out[j][2], out[j][3]);
         }
+    }
+    __syncwarp();   // the warp's sU / sH are rewritten by its next tile
     }
 }
 
@@ -663,7 +667,13 @@ void infer(cfdxg_context* ctx, cfdxg_mpnn* net, const double* r, double* out) {
                      in_bytes + out_bytes + 4.0 * (n + 1) + 8.0 * static_cast<double>(net->gco.size()));
         auto kern = first ? k_round_gather_tc<true, false>
                           : (last ? k_round_gather_tc<false, true> : k_round_gather_tc<false, false>);
-        kern<<<(tiles + kRoundWarps - 1) / kRoundWarps, kRoundThreads, 0, s>>>(
+        // persistent grid of five blocks per SM (the shared-memory limit) for
+        // the middle and last rounds: 166 / 171 instead of 210 / 220 us at
+        // 64^3.  The first round, which forms h0 per neighbour, measured
+        // slower that way (277 vs 243 us) and takes one tile per warp.
+        const int all = (tiles + kRoundWarps - 1) / kRoundWarps;
+        const int grid = first ? all : std::min(all, 5 * ctx->sm_count);
+        kern<<<grid, kRoundThreads, 0, s>>>(
             n, net->gro.get(), net->gco.get(), net->gew.get(), hin, hout, w, w + 2 * F * F,
             net->params.get() + ROUND0 + k * ROUND_SIZE, net->params.get(), r, rr,
             first ? reinterpret_cast<const float*>(xin) : nullptr, net->diag.get(), out);
