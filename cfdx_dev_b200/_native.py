@@ -88,6 +88,23 @@ class CaptureInfo(C.Structure):
     ]
 
 
+class DomainPartInfo(C.Structure):
+    _fields_ = [
+        ("row_begin", C.c_int64), ("row_end", C.c_int64), ("n_local", C.c_int64), ("owned_offset", C.c_int64),
+        ("nnz_local", C.c_int64), ("nnz_block", C.c_int64), ("n_neighbours", C.c_int32), ("n_recv", C.c_int64),
+        ("n_send", C.c_int64),
+    ]
+
+
+DOMAIN_ARRAYS = ("local_row_offsets", "local_columns", "local_source", "block_row_offsets", "block_columns",
+                 "block_source", "neighbours", "recv_offsets", "recv_start", "ghost_rows", "send_offsets",
+                 "send_rows")
+
+
+class DomainPartArrays(C.Structure):
+    _fields_ = [(name, C.c_void_p) for name in DOMAIN_ARRAYS]
+
+
 _V = C.c_void_p
 _P = C.POINTER
 # name -> (restype, argtypes)
@@ -167,6 +184,12 @@ PROTOTYPES = {
     "cfdxg_capture_write": (C.c_int, [C.c_char_p, C.c_int64] + [_V] * 5 + [_P(CaptureInfo)]),
     "cfdxg_capture_destroy": (C.c_int, [_V]),
     "cfdxg_capture_last_error": (C.c_char_p, []),
+    "cfdxg_domain_plan_create": (C.c_int, [C.c_int64, _V, _V, C.c_int32, _V, _P(_V)]),
+    "cfdxg_domain_plan_parts": (C.c_int, [_V, _V]),
+    "cfdxg_domain_plan_info": (C.c_int, [_V, C.c_int32, _P(DomainPartInfo)]),
+    "cfdxg_domain_plan_export": (C.c_int, [_V, C.c_int32, _P(DomainPartArrays)]),
+    "cfdxg_domain_plan_destroy": (C.c_int, [_V]),
+    "cfdxg_domain_last_error": (C.c_char_p, []),
 }
 
 _lib = None

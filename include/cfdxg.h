@@ -457,6 +457,63 @@ int cfdxg_capture_destroy(cfdxg_capture* c);
 const char* cfdxg_capture_last_error(void);
 
 /* ------------------------------------------------------------------------ */
+/* Domain decomposition plan (row blocks with halos)                         */
+/* New: the reference solves one system on one rank (its MPI layer does not  */
+/* reach this path; linear_solver_dispatch.h:227-234 takes the whole        */
+/* SparseMatrix).  A plan splits the rows of a square CSR system into       */
+/* contiguous blocks ("parts", one or more per GPU) and lists, per part:   */
+/*  - its local system: the owned rows with their columns renumbered into   */
+/*    the local vector [ghosts below | owned | ghosts above], increasing in  */
+/*    the global column order, so every local row keeps the global row's    */
+/*    entry order (a local product sums exactly as the global one does);    */
+/*  - its diagonal block (owned columns only, owned numbering) for a        */
+/*    subdomain preconditioner;                                            */
+/*  - per neighbouring part the ghosts it receives (a contiguous slice of    */
+/*    the local vector) and the owned rows it sends.                         */
+/* Each entry carries the index of the global CSR entry it copies, so a      */
+/* numeric refresh is a gather.  Host-only; no device needed.               */
+/* ------------------------------------------------------------------------ */
+typedef struct cfdxg_domain_plan cfdxg_domain_plan;
+typedef struct {
+    int64_t row_begin, row_end;      /* owned global rows [row_begin, row_end) */
+    int64_t n_local;                 /* local vector length: ghosts + owned */
+    int64_t owned_offset;            /* local position of row_begin (= ghosts below) */
+    int64_t nnz_local;               /* entries of the owned rows */
+    int64_t nnz_block;               /* entries of the diagonal block */
+    int32_t n_neighbours;
+    int64_t n_recv, n_send;          /* ghost values received / owned values sent */
+} cfdxg_domain_part_info;
+typedef struct {                     /* output arrays; NULL skips one */
+    int64_t* local_row_offsets;      /* n_local + 1 (ghost rows are empty) */
+    int64_t* local_columns;          /* nnz_local, local numbering */
+    int64_t* local_source;           /* nnz_local, global CSR entry index */
+    int64_t* block_row_offsets;      /* (row_end - row_begin) + 1 */
+    int64_t* block_columns;          /* nnz_block, owned numbering */
+    int64_t* block_source;           /* nnz_block */
+    int32_t* neighbours;             /* n_neighbours, increasing part ids */
+    int64_t* recv_offsets;           /* n_neighbours + 1 into ghost_rows */
+    int64_t* recv_start;             /* n_neighbours: local position of each slice */
+    int64_t* ghost_rows;             /* n_recv global rows, increasing */
+    int64_t* send_offsets;           /* n_neighbours + 1 into send_rows */
+    int64_t* send_rows;              /* n_send owned indices (0-based in the part) */
+} cfdxg_domain_part_arrays;
+
+/* Builds the plan of an n x n CSR pattern (row offsets, columns strictly
+ * increasing in each row) split into `parts` row blocks.  row_splits
+ * (parts + 1 increasing offsets from 0 to n) fixes the blocks; NULL splits
+ * the rows into blocks of nearly equal entry counts.  Every block must own
+ * at least one row.  CFDXG_ERR_INVALID_ARGUMENT with the reason in
+ * cfdxg_domain_last_error() on bad input. */
+int cfdxg_domain_plan_create(int64_t n, const int64_t* row_offsets, const int64_t* columns, int32_t parts,
+                             const int64_t* row_splits, cfdxg_domain_plan** out);
+/* row_splits (parts + 1) of the plan; returns the number of parts. */
+int cfdxg_domain_plan_parts(const cfdxg_domain_plan* plan, int64_t* row_splits);
+int cfdxg_domain_plan_info(const cfdxg_domain_plan* plan, int32_t part, cfdxg_domain_part_info* info);
+int cfdxg_domain_plan_export(const cfdxg_domain_plan* plan, int32_t part, const cfdxg_domain_part_arrays* out);
+int cfdxg_domain_plan_destroy(cfdxg_domain_plan* plan);
+const char* cfdxg_domain_last_error(void);
+
+/* ------------------------------------------------------------------------ */
 /* synthetic cases (seeded generators for the benchmark configurations)      */
 /* ------------------------------------------------------------------------ */
 typedef struct cfdxg_case cfdxg_case;
