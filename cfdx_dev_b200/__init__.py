@@ -21,10 +21,12 @@ from .api import (  # noqa: F401
     gauss_gradient_with_boundary,
     hex_case,
     make_request,
+    measure_matrix_characteristics,
     make_rhie_chow_mass_flux,
     parse_linear_capture_iterations,
     random_field,
     read_linear_system_capture,
+    select_linear_solver,
     solve_cg,
     solve_fgmres,
     solve_gmres,

@@ -12,8 +12,18 @@ LIB_PATH = Path(__file__).resolve().parent / "_lib" / "libcfdxg.so"
 
 CFDXG_MEM_HOST = 0
 CFDXG_MEM_DEVICE = 1
-KRYLOV = {"cg": 1, "gmres": 3, "fgmres": 4}
-PRECONDITIONER = {"none": 1, "jacobi": 2, "native_amg": 6, "own_diagonal": 32}
+KRYLOV = {"auto": 0, "cg": 1, "gmres": 3, "fgmres": 4}
+PRECONDITIONER = {"auto": 0, "none": 1, "jacobi": 2, "native_amg": 6, "own_diagonal": 32}
+# the reference's full model enums (core/linalg/linear_solver_models.h:11-61), for plan selection
+PROBLEMS = ["general", "pressure_poisson", "diffusion", "momentum", "scalar_transport", "coupled_pressure_velocity"]
+KRYLOV_MODELS = ["auto", "cg", "bicgstab", "gmres", "fgmres", "lgmres", "pipecg", "pipefgmres"]
+PRECONDITIONER_MODELS = [
+    "auto", "none", "jacobi", "gauss_seidel", "ilu0", "ilut", "native_amg", "smoothed_aggregation_amg",
+    "anisotropic_line_amg", "fsai", "ras", "native_fieldsplit", "coupled_block_schur", "pcd", "lsc", "mgr",
+    "anisotropic_line", "anisotropic_boomer_amg", "anisotropic_smoothed_aggregation_amg",
+    "directional_semi_coarsening_amg", "energy_minimizing_amg", "vanka_pressure_patch", "braess_sarazin"]
+NULL_SPACES = ["none", "constant"]
+SCALINGS = ["none", "row", "column", "row_column", "symmetric_diagonal"]
 PRECISION = {"fp64": 0, "fp32_vcycle": 1}
 STATUS = {0: "converged", 1: "max_iter_reached", 2: "diverged", 3: "not_applicable"}
 ERRORS = {
@@ -62,7 +72,7 @@ class Request(C.Structure):
         ("adaptive_restart", C.c_int32), ("residual_replacement", C.c_int32),
         ("residual_replacement_period", C.c_int64), ("residual_replacement_gap_ratio", C.c_double),
         ("target_reduction_per_cycle", C.c_double), ("learned", C.c_void_p),
-        ("learned_applications", C.c_int32), ("orthogonalization", C.c_int32),
+        ("learned_applications", C.c_int32), ("orthogonalization", C.c_int32), ("problem", C.c_int32),
     ]
 
 
@@ -73,6 +83,7 @@ class Report(C.Structure):
         ("residual_replacements", C.c_int64), ("max_true_recursive_gap", C.c_double),
         ("setup_seconds", C.c_double), ("solve_seconds", C.c_double),
         ("preconditioner_applications", C.c_int64), ("learned_fallbacks", C.c_int64),
+        ("plan_krylov", C.c_int32), ("plan_preconditioner", C.c_int32),
     ]
 
     def as_dict(self) -> dict:
@@ -86,6 +97,29 @@ class CaptureInfo(C.Structure):
         ("problem", C.c_int32), ("null_space", C.c_int32), ("scaling", C.c_int32), ("n", C.c_int64),
         ("nnz", C.c_int64), ("max_iterations", C.c_int64), ("tolerance", C.c_double), ("checksum", C.c_uint64),
     ]
+
+
+class MatrixCharacteristics(C.Structure):
+    _fields_ = [
+        ("equations", C.c_int64), ("average_nnz_per_row", C.c_double), ("coefficient_range", C.c_double),
+        ("square", C.c_int32), ("numerically_symmetric", C.c_int32), ("diagonally_dominant", C.c_int32),
+        ("strongly_scaled", C.c_int32), ("large_diagonal_dynamic_range", C.c_int32),
+        ("strongly_directional_coupling", C.c_int32), ("positive_diagonal", C.c_int32), ("saddle_point", C.c_int32),
+    ]
+
+    def as_dict(self) -> dict:
+        return {name: getattr(self, name) for name, _ in self._fields_}
+
+
+class PlanRequest(C.Structure):
+    _fields_ = [("krylov", C.c_int32), ("preconditioner", C.c_int32), ("gmres_restart", C.c_int32),
+                ("null_space", C.c_int32), ("scaling", C.c_int32), ("braess_sarazin_alpha", C.c_double)]
+
+
+class SolverPlan(C.Structure):
+    _fields_ = [("problem", C.c_int32), ("krylov", C.c_int32), ("preconditioner", C.c_int32),
+                ("null_space", C.c_int32), ("automatic_krylov", C.c_int32), ("automatic_preconditioner", C.c_int32),
+                ("reason", C.c_char * 512)]
 
 
 class DomainPartInfo(C.Structure):
@@ -184,6 +218,12 @@ PROTOTYPES = {
     "cfdxg_capture_write": (C.c_int, [C.c_char_p, C.c_int64] + [_V] * 5 + [_P(CaptureInfo)]),
     "cfdxg_capture_destroy": (C.c_int, [_V]),
     "cfdxg_capture_last_error": (C.c_char_p, []),
+    "cfdxg_measure_matrix_characteristics": (C.c_int, [C.c_int64, _V, _V, _V, C.c_int32, C.c_double,
+                                                      _P(MatrixCharacteristics)]),
+    "cfdxg_select_linear_solver": (C.c_int, [C.c_int32, _P(MatrixCharacteristics), _P(PlanRequest),
+                                            _P(SolverPlan)]),
+    "cfdxg_plan_last_error": (C.c_char_p, []),
+    "cfdxg_plan_reason": (C.c_char_p, [_V]),
     "cfdxg_domain_plan_create": (C.c_int, [C.c_int64, _V, _V, C.c_int32, _V, _P(_V)]),
     "cfdxg_domain_plan_parts": (C.c_int, [_V, _V]),
     "cfdxg_domain_plan_info": (C.c_int, [_V, C.c_int32, _P(DomainPartInfo)]),

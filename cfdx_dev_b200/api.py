@@ -508,7 +508,9 @@ class NativeBoomerAMGPreconditioner:
             pass
 
 
-def make_request(krylov="gmres", preconditioner="native_amg", restart=40, precision="fp64", learned=None, **kw):
+def make_request(krylov="gmres", preconditioner="native_amg", restart=40, precision="fp64", learned=None,
+                 problem="pressure_poisson", **kw):
+    """A cfdxg_request; krylov / preconditioner "auto" select the plan from the measured matrix."""
     lib = N.load()
     r = N.Request()
     lib.cfdxg_request_default(C.byref(r))
@@ -517,9 +519,43 @@ def make_request(krylov="gmres", preconditioner="native_amg", restart=40, precis
     r.gmres_restart = restart
     r.precision = N.PRECISION[precision]
     r.learned = learned.handle if learned is not None else None
+    r.problem = N.PROBLEMS.index(problem)
     for k, v in kw.items():
         setattr(r, k, v)
     return r
+
+
+def measure_matrix_characteristics(row_offsets, columns, values, saddle_point=False,
+                                   symmetry_tolerance=1e-12) -> dict:
+    """core/linalg/matrix_diagnostics.h:285 measure_matrix_characteristics, on the host."""
+    lib = N.load()
+    ro, co, va = _i64(row_offsets), _i64(columns), _f64(values)
+    c = N.MatrixCharacteristics()
+    rc = lib.cfdxg_measure_matrix_characteristics(ro.size - 1, N.ptr(ro), N.ptr(co), N.ptr(va),
+                                                  int(bool(saddle_point)), float(symmetry_tolerance), C.byref(c))
+    if rc != 0:
+        raise CfdxgError(rc, lib.cfdxg_plan_last_error().decode())
+    return c.as_dict()
+
+
+def select_linear_solver(problem: str, characteristics: dict, krylov="auto", preconditioner="auto",
+                         gmres_restart=40, null_space="none", scaling="none", braess_sarazin_alpha=1.0) -> dict:
+    """core/linalg/linear_solver_models.h:228 select_linear_solver -> plan (model names and flags).
+
+    Raises CfdxgError where the reference throws std::invalid_argument."""
+    lib = N.load()
+    c = N.MatrixCharacteristics(**{k: characteristics[k] for k, _ in N.MatrixCharacteristics._fields_})
+    r = N.PlanRequest(N.KRYLOV_MODELS.index(krylov), N.PRECONDITIONER_MODELS.index(preconditioner),
+                      int(gmres_restart), N.NULL_SPACES.index(null_space), N.SCALINGS.index(scaling),
+                      float(braess_sarazin_alpha))
+    plan = N.SolverPlan()
+    rc = lib.cfdxg_select_linear_solver(N.PROBLEMS.index(problem), C.byref(c), C.byref(r), C.byref(plan))
+    if rc != 0:
+        raise CfdxgError(rc, lib.cfdxg_plan_last_error().decode())
+    return dict(problem=N.PROBLEMS[plan.problem], krylov=N.KRYLOV_MODELS[plan.krylov],
+                preconditioner=N.PRECONDITIONER_MODELS[plan.preconditioner], null_space=N.NULL_SPACES[plan.null_space],
+                automatic_krylov=bool(plan.automatic_krylov),
+                automatic_preconditioner=bool(plan.automatic_preconditioner), reason=plan.reason.decode())
 
 
 def solve_linear_system(A: SparseMatrix, rhs, x0=None, krylov="gmres", preconditioner="native_amg",

@@ -7,6 +7,7 @@
 #include "io.h"
 #include "krylov.h"
 #include "mpnn.h"
+#include "plan.h"
 
 using namespace cfdxg;
 
@@ -615,8 +616,11 @@ extern "C" int cfdxg_request_default(cfdxg_request* r) {
     r->target_reduction_per_cycle = 0.1;
     r->learned = nullptr;
     r->learned_applications = 1;
+    r->problem = CFDXG_PROBLEM_PRESSURE_POISSON;
     return CFDXG_OK;
 }
+
+extern "C" const char* cfdxg_plan_reason(const cfdxg_context* ctx) { return ctx ? ctx->plan_reason.c_str() : ""; }
 
 namespace {
 
@@ -703,6 +707,14 @@ KrylovResult run_krylov(cfdxg_context* ctx, const cfdxg_matrix* A, cfdxg_amg* am
 
 void validate_request(const cfdxg_request& r) {
     if (r.gmres_restart <= 0) throw Error(CFDXG_ERR_INVALID_ARGUMENT, "GMRES restart must be positive");
+    if (r.problem < CFDXG_PROBLEM_GENERAL || r.problem > CFDXG_PROBLEM_COUPLED_PRESSURE_VELOCITY)
+        throw Error(CFDXG_ERR_INVALID_ARGUMENT, "unknown problem kind");
+    // select_linear_solver's model checks (linear_solver_models.h:389-398)
+    const bool elliptic = r.problem == CFDXG_PROBLEM_PRESSURE_POISSON || r.problem == CFDXG_PROBLEM_DIFFUSION;
+    if (r.krylov == CFDXG_KRYLOV_CG && !elliptic)
+        throw Error(CFDXG_ERR_INVALID_ARGUMENT, "CG needs a pressure or diffusion operator");
+    if (r.preconditioner == CFDXG_PC_NATIVE_AMG && !elliptic)
+        throw Error(CFDXG_ERR_INVALID_ARGUMENT, "native AMG is qualified for SPD elliptic problems only");
     if (r.krylov != CFDXG_KRYLOV_GMRES && r.krylov != CFDXG_KRYLOV_FGMRES && r.krylov != CFDXG_KRYLOV_CG)
         throw Error(CFDXG_ERR_INVALID_ARGUMENT, "only CG, GMRES and FGMRES are provided");
     if (r.krylov == CFDXG_KRYLOV_CG && r.learned)
@@ -750,6 +762,44 @@ extern "C" int cfdxg_solve_linear_system(cfdxg_context* ctx, const cfdxg_matrix*
     cfdxg_request req;
     if (req_in) req = *req_in;
     else cfdxg_request_default(&req);
+    ctx->plan_reason.clear();
+    // automatic plan (linear_solver_dispatch.h:251-268): measure, then select
+    bool not_provided = false;
+    if (req.krylov == CFDXG_KRYLOV_AUTO || req.preconditioner == CFDXG_PC_AUTO) {
+        std::vector<double> downloaded;
+        const double* hv = A->host.va.data();
+        if (!A->host_values_valid) {
+            downloaded.resize(static_cast<size_t>(A->nnz));
+            A->va.download(downloaded.data(), ctx->stream);
+            CFDXG_CUDA(cudaStreamSynchronize(ctx->stream));
+            hv = downloaded.data();
+        }
+        cfdxg_matrix_characteristics ch;
+        measure_characteristics(A->n, A->host.ro.data(), A->host.co.data(), hv,
+                                req.problem == CFDXG_PROBLEM_COUPLED_PRESSURE_VELOCITY, 1e-12, ch);
+        if (req.krylov == CFDXG_KRYLOV_CG && !(ch.numerically_symmetric && ch.positive_diagonal)) {
+            // a forced CG fails closed before any plan is drawn
+            req.preconditioner = CFDXG_PC_NONE;
+        } else {
+            const cfdxg_plan_request pr{req.krylov, req.preconditioner, req.gmres_restart, 0, 0, 1.0};
+            cfdxg_solver_plan plan;
+            std::string why;
+            if (!select_solver(req.problem, ch, pr, plan, why)) throw Error(CFDXG_ERR_INVALID_ARGUMENT, why);
+            ctx->plan_reason = plan.reason;
+            const bool krylov_ok = plan.krylov == CFDXG_KRYLOV_CG || plan.krylov == CFDXG_KRYLOV_GMRES ||
+                                   plan.krylov == CFDXG_KRYLOV_FGMRES;
+            const bool pc_ok = plan.preconditioner == CFDXG_PC_NONE || plan.preconditioner == CFDXG_PC_JACOBI ||
+                               plan.preconditioner == CFDXG_PC_NATIVE_AMG;
+            if (krylov_ok && pc_ok) {
+                req.krylov = plan.krylov;
+                req.preconditioner = plan.preconditioner;
+            } else {
+                not_provided = true;
+                req.krylov = krylov_ok ? plan.krylov : CFDXG_KRYLOV_GMRES;
+                req.preconditioner = CFDXG_PC_NONE;
+            }
+        }
+    }
     validate_request(req);
     if (report) std::memset(report, 0, sizeof(*report));
     const int64_t n = A->n;
@@ -763,7 +813,11 @@ extern "C" int cfdxg_solve_linear_system(cfdxg_context* ctx, const cfdxg_matrix*
     int64_t learned_fallbacks = 0;
     double setup_s = 0.0;
     const bool cg = req.krylov == CFDXG_KRYLOV_CG;
-    if (cg && !symmetric_positive_diagonal(ctx, A)) {
+    if (not_provided) {
+        // the plan names a model outside this path (BiCGStab, ILU0): x untouched
+        r.status = CFDXG_NOT_APPLICABLE;
+        ctx->error = "automatic plan not provided by this library: " + ctx->plan_reason;
+    } else if (cg && !symmetric_positive_diagonal(ctx, A)) {
         // linear_solver_dispatch.h:259-267: a forced CG on a matrix that is not
         // symmetric with a positive diagonal fails closed, x untouched
         r.status = CFDXG_NOT_APPLICABLE;
@@ -852,6 +906,8 @@ extern "C" int cfdxg_solve_linear_system(cfdxg_context* ctx, const cfdxg_matrix*
         report->setup_seconds = setup_s;
         report->solve_seconds = t1 - t0 - setup_s;
         report->learned_fallbacks = learned_fallbacks;
+        report->plan_krylov = req.krylov;
+        report->plan_preconditioner = req.preconditioner;
     }
     return r.status;
     CFDXG_GUARD_END(ctx)
@@ -889,6 +945,8 @@ extern "C" int cfdxg_solve_gmres(cfdxg_context* ctx, const cfdxg_matrix* A, cfdx
         report->physical_residual_relative = r.residual_relative;
         report->solve_seconds = now_seconds() - t0;
         report->learned_fallbacks = learned_fallbacks;
+        report->plan_krylov = req.krylov;
+        report->plan_preconditioner = amg ? CFDXG_PC_NATIVE_AMG : CFDXG_PC_NONE;
     }
     return r.status;
     CFDXG_GUARD_END(ctx)

@@ -107,6 +107,7 @@ struct cfdxg_context {
     int device = 0;
     cudaStream_t stream = nullptr;
     std::string error;
+    std::string plan_reason;   // plan of the last solve_linear_system
     int64_t launches = 0;
     cfdxg::Scratch scratch;
     int sm_count = 148;

@@ -47,9 +47,11 @@ extern "C" {
 
 /* Krylov / preconditioner / precision choices, numbered as the reference's
  * KrylovModel and PreconditionerModel enums (core/linalg/linear_solver_models.h:20-55). */
+#define CFDXG_KRYLOV_AUTO 0         /* KrylovModel::Auto: chosen by select_linear_solver */
 #define CFDXG_KRYLOV_CG 1           /* KrylovModel::CG: SPD systems, cg_solver.h */
 #define CFDXG_KRYLOV_GMRES 3
 #define CFDXG_KRYLOV_FGMRES 4
+#define CFDXG_PC_AUTO 0             /* PreconditionerModel::Auto */
 #define CFDXG_PC_NONE 1
 #define CFDXG_PC_JACOBI 2
 #define CFDXG_PC_NATIVE_AMG 6
@@ -60,6 +62,13 @@ extern "C" {
 #define CFDXG_PRECISION_FP32_VCYCLE 1  /* FP32 V-cycle inside FP64 FGMRES */
 #define CFDXG_ORTHO_MGS2 0          /* two-pass modified Gram-Schmidt, gmres_solver.h:270-295 */
 #define CFDXG_ORTHO_CGS2 1          /* two-pass classical Gram-Schmidt (no reference counterpart) */
+/* LinearProblemKind (core/linalg/linear_solver_models.h:11-18) */
+#define CFDXG_PROBLEM_GENERAL 0
+#define CFDXG_PROBLEM_PRESSURE_POISSON 1
+#define CFDXG_PROBLEM_DIFFUSION 2
+#define CFDXG_PROBLEM_MOMENTUM 3
+#define CFDXG_PROBLEM_SCALAR_TRANSPORT 4
+#define CFDXG_PROBLEM_COUPLED_PRESSURE_VELOCITY 5
 
 typedef struct cfdxg_context cfdxg_context;
 typedef struct cfdxg_mesh cfdxg_mesh;
@@ -341,6 +350,9 @@ typedef struct {
                                         CFDXG_ORTHO_CGS2: h = V^T w, w -= V h, twice -- the same
                                         projections in 4 passes over the basis per Arnoldi step
                                         instead of 4(j+1); rounding differs from MGS2's */
+    int32_t problem;                 /* CFDXG_PROBLEM_* (default PRESSURE_POISSON): steers the
+                                        automatic choice and the model checks of
+                                        select_linear_solver */
 } cfdxg_request;
 
 /* Mirrors SolverResult (core/linalg/solver_status.h:45-72) + LinearSolveReport. */
@@ -356,12 +368,19 @@ typedef struct {
     double solve_seconds;
     int64_t preconditioner_applications;
     int64_t learned_fallbacks;
+    int32_t plan_krylov;             /* the Krylov model that ran (KrylovModel numbering) */
+    int32_t plan_preconditioner;     /* the preconditioner model that ran */
 } cfdxg_report;
 
 int cfdxg_request_default(cfdxg_request* req);
 
 /* Replaces solve_linear_system (core/linalg/linear_solver_dispatch.h:227-492) for
- * scalar pressure systems without scaling / null space: builds the requested
+ * scalar pressure systems without scaling / null space.  With krylov or
+ * preconditioner CFDXG_*_AUTO it first measures the matrix and selects the
+ * plan (cfdxg_measure_matrix_characteristics, cfdxg_select_linear_solver, on the
+ * host); a plan whose model this library does not provide (BiCGStab, ILU0, ...)
+ * returns CFDXG_NOT_APPLICABLE with x untouched and the plan in
+ * cfdxg_plan_reason().  Then it builds the requested
  * preconditioner (AMG setup inside, as the reference), solves with
  * right-preconditioned GMRES/FGMRES or with CG (cg_solver.h:45-560), then
  * certifies the FP64 physical residual.  CG first measures the matrix
@@ -382,6 +401,61 @@ int cfdxg_solve_linear_system(cfdxg_context* ctx, const cfdxg_matrix* A, const d
 int cfdxg_solve_gmres(cfdxg_context* ctx, const cfdxg_matrix* A, cfdxg_amg* amg,
                       const double* rhs, double* x, int32_t mem, const cfdxg_request* req,
                       int64_t max_iterations, double tolerance, cfdxg_report* report);
+
+/* ------------------------------------------------------------------------ */
+/* Automatic solver selection (host-only; no device needed)                  */
+/* ------------------------------------------------------------------------ */
+/* measure_matrix_characteristics (core/linalg/matrix_diagnostics.h:285-358). */
+typedef struct {
+    int64_t equations;
+    double average_nnz_per_row;
+    double coefficient_range;        /* max|a| / min nonzero |a| (1 when undefined) */
+    int32_t square;
+    int32_t numerically_symmetric;   /* |a_ij - a_ji| <= tol * max(1, max|a|) */
+    int32_t diagonally_dominant;     /* min Gershgorin margin >= -1e-14 max(1, max|a_ii|) */
+    int32_t strongly_scaled;         /* coefficient_range >= 1e8 */
+    int32_t large_diagonal_dynamic_range;  /* max|a_ii| / min nonzero |a_ii| >= 1e4 */
+    int32_t strongly_directional_coupling; /* a row whose negative couplings differ by >= 1e3 */
+    int32_t positive_diagonal;
+    int32_t saddle_point;            /* given by the caller */
+} cfdxg_matrix_characteristics;
+/* The fields of LinearSolverRequest that select_linear_solver reads. */
+typedef struct {
+    int32_t krylov;                  /* KrylovModel 0..7 (0 = auto) */
+    int32_t preconditioner;          /* PreconditionerModel 0..22 (0 = auto) */
+    int32_t gmres_restart;
+    int32_t null_space;              /* NullSpaceModel: 0 none, 1 constant */
+    int32_t scaling;                 /* LinearScalingModel 0..4 */
+    double braess_sarazin_alpha;     /* 1 by default */
+} cfdxg_plan_request;
+/* LinearSolverPlan (linear_solver_models.h:206-214); reason is this
+ * library's own wording. */
+typedef struct {
+    int32_t problem;
+    int32_t krylov;
+    int32_t preconditioner;
+    int32_t null_space;
+    int32_t automatic_krylov;
+    int32_t automatic_preconditioner;
+    char reason[512];
+} cfdxg_solver_plan;
+
+/* Characteristics of a square CSR matrix (columns strictly increasing in each
+ * row; symmetry_tolerance finite and >= 0, 1e-12 in the dispatcher).  A
+ * non-finite value leaves the coefficient evidence at its defaults, as the
+ * reference's diagnosis of an inconsistent matrix does. */
+int cfdxg_measure_matrix_characteristics(int64_t n, const int64_t* row_offsets, const int64_t* columns,
+                                         const double* values, int32_t saddle_point,
+                                         double symmetry_tolerance, cfdxg_matrix_characteristics* out);
+/* select_linear_solver (core/linalg/linear_solver_models.h:228-425): the same
+ * plan for every problem kind, characteristics and request; where the
+ * reference throws std::invalid_argument this returns
+ * CFDXG_ERR_INVALID_ARGUMENT with the reason in cfdxg_plan_last_error(). */
+int cfdxg_select_linear_solver(int32_t problem, const cfdxg_matrix_characteristics* characteristics,
+                               const cfdxg_plan_request* request, cfdxg_solver_plan* plan);
+const char* cfdxg_plan_last_error(void);
+/* The plan and its reason of the last cfdxg_solve_linear_system on the context. */
+const char* cfdxg_plan_reason(const cfdxg_context* ctx);
 
 /* ------------------------------------------------------------------------ */
 /* learned message-passing preconditioner (no reference counterpart)          */

@@ -379,3 +379,40 @@ def solve_poisson_mixed(mesh, bc_values, source, bc_types=None, diffusivity=1.0,
     _check(f(h.ptr, _p(bc), _p(ty), float(diffusivity), _p(src), int(max_iterations), float(tolerance),
              int(reference_cell), float(reference_value), _p(x), C.byref(rep)), "solve_poisson_mixed")
     return x, rep.as_dict()
+
+
+_FLAG_NAMES = ("square", "numerically_symmetric", "diagonally_dominant", "strongly_scaled",
+               "large_diagonal_dynamic_range", "strongly_directional_coupling", "positive_diagonal", "saddle_point")
+
+
+def measure_characteristics(ro, co, va, saddle_point=False, symmetry_tolerance=1e-12) -> dict:
+    """core/linalg/matrix_diagnostics.h:285 measure_matrix_characteristics."""
+    ro, co, va = (np.ascontiguousarray(ro, np.int64), np.ascontiguousarray(co, np.int64),
+                  np.ascontiguousarray(va, np.float64))
+    d = np.empty(3)
+    f = np.empty(8, np.int32)
+    L = lib()
+    L.ref_measure_characteristics.argtypes = [C.c_int64, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int32,
+                                              C.c_double, C.c_void_p, C.c_void_p]
+    _check(L.ref_measure_characteristics(ro.size - 1, _p(ro), _p(co), _p(va), int(bool(saddle_point)),
+                                         float(symmetry_tolerance), _p(d), _p(f)), "characteristics")
+    out = dict(equations=int(d[0]), average_nnz_per_row=float(d[1]), coefficient_range=float(d[2]))
+    out.update({k: int(v) for k, v in zip(_FLAG_NAMES, f)})
+    return out
+
+
+def select_linear_solver(problem: int, characteristics: dict, krylov=0, preconditioner=0, gmres_restart=40,
+                         null_space=0, scaling=0, braess_sarazin_alpha=1.0):
+    """core/linalg/linear_solver_models.h:228 select_linear_solver -> (krylov, preconditioner,
+    null_space, automatic_krylov, automatic_preconditioner), or None where it throws."""
+    c = characteristics
+    flags = np.array([c[k] for k in _FLAG_NAMES], np.int32)
+    req = np.array([krylov, preconditioner, gmres_restart, null_space, scaling], np.int32)
+    plan = np.zeros(5, np.int32)
+    L = lib()
+    L.ref_select_linear_solver.argtypes = [C.c_int32, C.c_int64, C.c_double, C.c_double, C.c_void_p, C.c_void_p,
+                                           C.c_double, C.c_void_p]
+    rc = L.ref_select_linear_solver(int(problem), int(c["equations"]), float(c["average_nnz_per_row"]),
+                                    float(c["coefficient_range"]), _p(flags), _p(req), float(braess_sarazin_alpha),
+                                    _p(plan))
+    return None if rc != 0 else tuple(int(v) for v in plan)

@@ -143,6 +143,22 @@ int64_t ref_apply_reference_cell_gauge(int64_t n, const int64_t* row_offsets, co
 int ref_solve_poisson_mixed(const ref_mesh_t* m, const double* bc, const int32_t* types, double gamma,
                             const double* source, int64_t max_iterations, double tolerance, int64_t reference_cell,
                             double reference_value, double* x, ref_report_t* report);
+
+/* --- automatic solver selection --- */
+/* core/linalg/matrix_diagnostics.h:285  measure_matrix_characteristics
+ * out_d: equations, average_nnz_per_row, coefficient_range; out_flags: square,
+ * numerically_symmetric, diagonally_dominant, strongly_scaled,
+ * large_diagonal_dynamic_range, strongly_directional_coupling, positive_diagonal,
+ * saddle_point */
+int ref_measure_characteristics(int64_t n, const int64_t* row_offsets, const int64_t* columns,
+                                const double* values, int32_t saddle_point, double symmetry_tolerance,
+                                double* out_d, int32_t* out_flags);
+/* core/linalg/linear_solver_models.h:228  select_linear_solver; -1 where it throws.
+ * req: krylov, preconditioner, gmres_restart, null_space, scaling (reference enums);
+ * plan: krylov, preconditioner, null_space, automatic_krylov, automatic_preconditioner */
+int ref_select_linear_solver(int32_t problem, int64_t equations, double average_nnz,
+                             double coefficient_range, const int32_t* flags, const int32_t* req,
+                             double braess_sarazin_alpha, int32_t* plan);
 /* one SpMV with SparseMatrix::matvec (sparse_matrix.h:180) */
 int ref_spmv(int64_t n, const int64_t* row_offsets, const int64_t* columns,
              const double* values, const double* x, double* y);

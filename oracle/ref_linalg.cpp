@@ -303,3 +303,69 @@ extern "C" int ref_solve_poisson_mixed(const ref_mesh_t* m, const double* bc, co
         return -1;
     }
 }
+
+// core/linalg/matrix_diagnostics.h:285  measure_matrix_characteristics
+// out_d: equations, average_nnz_per_row, coefficient_range
+// out_flags: square, numerically_symmetric, diagonally_dominant, strongly_scaled,
+//            large_diagonal_dynamic_range, strongly_directional_coupling,
+//            positive_diagonal, saddle_point
+extern "C" int ref_measure_characteristics(int64_t n, const int64_t* ro, const int64_t* co, const double* va,
+                                           int32_t saddle_point, double symmetry_tolerance, double* out_d,
+                                           int32_t* out_flags) {
+    try {
+        const SparseMatrix A = cfdx_ref::make_csr(n, ro, co, va);
+        const MatrixCharacteristics c = measure_matrix_characteristics(A, saddle_point != 0, symmetry_tolerance);
+        out_d[0] = static_cast<double>(c.equations);
+        out_d[1] = c.average_nnz_per_row;
+        out_d[2] = c.coefficient_range;
+        const bool flags[8] = {c.square, c.numerically_symmetric, c.diagonally_dominant, c.strongly_scaled,
+                               c.large_diagonal_dynamic_range, c.strongly_directional_coupling,
+                               c.positive_diagonal, c.saddle_point};
+        for (int k = 0; k < 8; ++k) out_flags[k] = flags[k] ? 1 : 0;
+        cfdx_ref::g_error.clear();
+        return 0;
+    } catch (const std::exception& e) {
+        cfdx_ref::set_error(e);
+        return -1;
+    }
+}
+
+// core/linalg/linear_solver_models.h:228  select_linear_solver
+// flags as above; req: krylov, preconditioner, gmres_restart, null_space, scaling;
+// plan: krylov, preconditioner, null_space, automatic_krylov, automatic_preconditioner
+extern "C" int ref_select_linear_solver(int32_t problem, int64_t equations, double average_nnz,
+                                        double coefficient_range, const int32_t* flags, const int32_t* req,
+                                        double braess_sarazin_alpha, int32_t* plan) {
+    try {
+        MatrixCharacteristics c;
+        c.equations = static_cast<std::size_t>(equations);
+        c.average_nnz_per_row = average_nnz;
+        c.coefficient_range = coefficient_range;
+        c.square = flags[0] != 0;
+        c.numerically_symmetric = flags[1] != 0;
+        c.diagonally_dominant = flags[2] != 0;
+        c.strongly_scaled = flags[3] != 0;
+        c.large_diagonal_dynamic_range = flags[4] != 0;
+        c.strongly_directional_coupling = flags[5] != 0;
+        c.positive_diagonal = flags[6] != 0;
+        c.saddle_point = flags[7] != 0;
+        LinearSolverRequest r;
+        r.krylov = static_cast<KrylovModel>(req[0]);
+        r.preconditioner = static_cast<PreconditionerModel>(req[1]);
+        r.gmres_restart = req[2];
+        r.null_space = static_cast<NullSpaceModel>(req[3]);
+        r.scaling = static_cast<LinearScalingModel>(req[4]);
+        r.braess_sarazin_alpha = braess_sarazin_alpha;
+        const LinearSolverPlan p = select_linear_solver(static_cast<LinearProblemKind>(problem), c, r);
+        plan[0] = static_cast<int32_t>(p.krylov);
+        plan[1] = static_cast<int32_t>(p.preconditioner);
+        plan[2] = static_cast<int32_t>(p.null_space);
+        plan[3] = p.automatic_krylov ? 1 : 0;
+        plan[4] = p.automatic_preconditioner ? 1 : 0;
+        cfdx_ref::g_error.clear();
+        return 0;
+    } catch (const std::exception& e) {
+        cfdx_ref::set_error(e);
+        return -1;
+    }
+}
