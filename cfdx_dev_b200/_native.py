@@ -126,7 +126,8 @@ class DomainPartInfo(C.Structure):
     _fields_ = [
         ("row_begin", C.c_int64), ("row_end", C.c_int64), ("n_local", C.c_int64), ("owned_offset", C.c_int64),
         ("nnz_local", C.c_int64), ("nnz_block", C.c_int64), ("n_neighbours", C.c_int32), ("n_recv", C.c_int64),
-        ("n_send", C.c_int64),
+        ("n_send", C.c_int64), ("col_begin", C.c_int64), ("col_end", C.c_int64), ("n_local_rows", C.c_int64),
+        ("first_row", C.c_int64),
     ]
 
 
@@ -225,7 +226,8 @@ PROTOTYPES = {
     "cfdxg_plan_last_error": (C.c_char_p, []),
     "cfdxg_plan_reason": (C.c_char_p, [_V]),
     "cfdxg_domain_plan_create": (C.c_int, [C.c_int64, _V, _V, C.c_int32, _V, _P(_V)]),
-    "cfdxg_domain_plan_parts": (C.c_int, [_V, _V]),
+    "cfdxg_domain_plan_create_rect": (C.c_int, [C.c_int64, C.c_int64, _V, _V, C.c_int32, _V, _V, _P(_V)]),
+    "cfdxg_domain_plan_parts": (C.c_int, [_V, _V, _V]),
     "cfdxg_domain_plan_info": (C.c_int, [_V, C.c_int32, _P(DomainPartInfo)]),
     "cfdxg_domain_plan_export": (C.c_int, [_V, C.c_int32, _P(DomainPartArrays)]),
     "cfdxg_domain_plan_destroy": (C.c_int, [_V]),

@@ -1,5 +1,10 @@
 // Domain decomposition plan: contiguous row blocks with halos.
 //
+// A square plan splits a system's rows and, with the same splits, its
+// unknowns; a rectangular plan (a transfer operator between two AMG levels)
+// splits its rows and its columns separately, each part owning a block of
+// each.
+//
 // The reference solves each pressure system on one rank
 // (core/linalg/linear_solver_dispatch.h:227-234 takes the whole SparseMatrix,
 // and the Krylov and AMG code has no distributed form), so this plan has no
@@ -30,10 +35,13 @@
 namespace {
 
 struct Part {
-    int64_t r0 = 0, r1 = 0, below = 0;
-    std::vector<int64_t> lro, lco, lsrc;     // local system (n_local rows)
-    std::vector<int64_t> bro, bco, bsrc;     // diagonal block (owned rows and columns)
-    std::vector<int64_t> ghosts;             // global rows, increasing
+    int64_t r0 = 0, r1 = 0;                  // owned rows
+    int64_t c0 = 0, c1 = 0;                  // owned columns (= rows for a square plan)
+    int64_t below = 0;                       // ghosts below c0
+    int64_t first_row = 0;                   // local row of r0
+    std::vector<int64_t> lro, lco, lsrc;     // local system
+    std::vector<int64_t> bro, bco, bsrc;     // owned-column block
+    std::vector<int64_t> ghosts;             // global columns, increasing
     std::vector<int32_t> nb;                 // neighbours (receive from or send to)
     std::vector<int64_t> recv_off, recv_start, send_off, send_rows;
 };
@@ -45,29 +53,37 @@ int fail(int code, const std::string& why) {
     return code;
 }
 
-int owner_of(const std::vector<int64_t>& splits, int64_t row) {
-    return static_cast<int>(std::upper_bound(splits.begin(), splits.end(), row) - splits.begin()) - 1;
+int owner_of(const std::vector<int64_t>& splits, int64_t index) {
+    return static_cast<int>(std::upper_bound(splits.begin(), splits.end(), index) - splits.begin()) - 1;
 }
 
 }  // namespace
 
 struct cfdxg_domain_plan {
-    int64_t n = 0;
-    std::vector<int64_t> splits;
+    int64_t n_rows = 0, n_cols = 0;
+    bool square = true;
+    std::vector<int64_t> row_splits, col_splits;
     std::vector<Part> parts;
 };
 
 namespace {
 
-std::string validate_pattern(int64_t n, const int64_t* ro, const int64_t* co) {
+std::string validate_pattern(int64_t n_rows, int64_t n_cols, const int64_t* ro, const int64_t* co) {
     if (ro[0] != 0) return "domain plan: row offsets must start at 0";
-    for (int64_t i = 0; i < n; ++i) {
+    for (int64_t i = 0; i < n_rows; ++i) {
         if (ro[i + 1] < ro[i]) return "domain plan: row offsets decrease";
         for (int64_t k = ro[i]; k < ro[i + 1]; ++k) {
-            if (co[k] < 0 || co[k] >= n) return "domain plan: column out of range";
+            if (co[k] < 0 || co[k] >= n_cols) return "domain plan: column out of range";
             if (k > ro[i] && co[k - 1] >= co[k]) return "domain plan: columns not strictly increasing in a row";
         }
     }
+    return {};
+}
+
+std::string validate_splits(const std::vector<int64_t>& s, int64_t n, const char* what) {
+    if (s.front() != 0 || s.back() != n) return std::string("domain plan: ") + what + " splits must run from 0 to n";
+    for (size_t k = 0; k + 1 < s.size(); ++k)
+        if (s[k + 1] <= s[k]) return std::string("domain plan: every part must own at least one ") + what;
     return {};
 }
 
@@ -88,86 +104,101 @@ std::vector<int64_t> balanced_splits(int64_t n, const int64_t* ro, int parts) {
     return s;
 }
 
-void build_local(const int64_t* ro, const int64_t* co, Part& P) {
-    const int64_t r0 = P.r0, r1 = P.r1, owned = r1 - r0;
+// Local numbering of the column space [ghosts below | owned | ghosts above].
+// A square plan pads the local rows to the local vector (owned rows at the
+// owned columns' positions, ghost rows empty), so one square product maps a
+// local vector to a local vector; a rectangular plan keeps the owned rows only.
+void build_local(const int64_t* ro, const int64_t* co, bool square, Part& P) {
+    const int64_t r0 = P.r0, r1 = P.r1, c0 = P.c0, c1 = P.c1, owned = c1 - c0;
     for (int64_t i = r0; i < r1; ++i)
         for (int64_t k = ro[i]; k < ro[i + 1]; ++k)
-            if (co[k] < r0 || co[k] >= r1) P.ghosts.push_back(co[k]);
+            if (co[k] < c0 || co[k] >= c1) P.ghosts.push_back(co[k]);
     std::sort(P.ghosts.begin(), P.ghosts.end());
     P.ghosts.erase(std::unique(P.ghosts.begin(), P.ghosts.end()), P.ghosts.end());
-    P.below = std::lower_bound(P.ghosts.begin(), P.ghosts.end(), r0) - P.ghosts.begin();
+    P.below = std::lower_bound(P.ghosts.begin(), P.ghosts.end(), c0) - P.ghosts.begin();
     const int64_t n_local = owned + static_cast<int64_t>(P.ghosts.size());
     auto local_of = [&](int64_t c) -> int64_t {
-        if (c >= r0 && c < r1) return P.below + (c - r0);
+        if (c >= c0 && c < c1) return P.below + (c - c0);
         const int64_t g = std::lower_bound(P.ghosts.begin(), P.ghosts.end(), c) - P.ghosts.begin();
-        return c < r0 ? g : g + owned;
+        return c < c0 ? g : g + owned;
     };
-    P.lro.assign(static_cast<size_t>(P.below) + 1, 0);
+    P.first_row = square ? P.below : 0;
+    P.lro.assign(static_cast<size_t>(P.first_row) + 1, 0);
     P.bro.assign(1, 0);
     for (int64_t i = r0; i < r1; ++i) {
         for (int64_t k = ro[i]; k < ro[i + 1]; ++k) {
             P.lco.push_back(local_of(co[k]));
             P.lsrc.push_back(k);
-            if (co[k] >= r0 && co[k] < r1) {
-                P.bco.push_back(co[k] - r0);
+            if (co[k] >= c0 && co[k] < c1) {
+                P.bco.push_back(co[k] - c0);
                 P.bsrc.push_back(k);
             }
         }
         P.lro.push_back(static_cast<int64_t>(P.lco.size()));
         P.bro.push_back(static_cast<int64_t>(P.bco.size()));
     }
-    while (static_cast<int64_t>(P.lro.size()) < n_local + 1) P.lro.push_back(static_cast<int64_t>(P.lco.size()));
+    if (square)
+        while (static_cast<int64_t>(P.lro.size()) < n_local + 1) P.lro.push_back(static_cast<int64_t>(P.lco.size()));
 }
 
-}  // namespace
-
-extern "C" {
-
-int cfdxg_domain_plan_create(int64_t n, const int64_t* ro, const int64_t* co, int32_t parts,
-                             const int64_t* row_splits, cfdxg_domain_plan** out) {
+int create(int64_t n_rows, int64_t n_cols, const int64_t* ro, const int64_t* co, int32_t parts,
+           const int64_t* row_splits, const int64_t* col_splits, bool square, cfdxg_domain_plan** out) {
     if (!out) return fail(CFDXG_ERR_INVALID_ARGUMENT, "domain plan: null argument");
     *out = nullptr;
-    if (n <= 0 || !ro || (ro[n] > 0 && !co)) return fail(CFDXG_ERR_INVALID_ARGUMENT, "domain plan: empty or null system");
-    if (parts < 1 || parts > n) return fail(CFDXG_ERR_INVALID_ARGUMENT, "domain plan: need 1 <= parts <= rows");
+    if (n_rows <= 0 || n_cols <= 0 || !ro || (ro[n_rows] > 0 && !co))
+        return fail(CFDXG_ERR_INVALID_ARGUMENT, "domain plan: empty or null system");
+    if (parts < 1 || parts > n_rows || parts > n_cols)
+        return fail(CFDXG_ERR_INVALID_ARGUMENT, "domain plan: need 1 <= parts <= rows and columns");
+    if (!square && (!row_splits || !col_splits))
+        return fail(CFDXG_ERR_INVALID_ARGUMENT, "domain plan: a rectangular plan needs row and column splits");
     try {
-        const std::string why = validate_pattern(n, ro, co);
+        std::string why = validate_pattern(n_rows, n_cols, ro, co);
         if (!why.empty()) return fail(CFDXG_ERR_INVALID_ARGUMENT, why);
         auto plan = std::make_unique<cfdxg_domain_plan>();
-        plan->n = n;
+        plan->n_rows = n_rows;
+        plan->n_cols = n_cols;
+        plan->square = square;
         if (row_splits) {
-            plan->splits.assign(row_splits, row_splits + parts + 1);
-            if (plan->splits.front() != 0 || plan->splits.back() != n)
-                return fail(CFDXG_ERR_INVALID_ARGUMENT, "domain plan: row splits must run from 0 to n");
-            for (int k = 0; k < parts; ++k)
-                if (plan->splits[k + 1] <= plan->splits[k])
-                    return fail(CFDXG_ERR_INVALID_ARGUMENT, "domain plan: every part must own at least one row");
+            plan->row_splits.assign(row_splits, row_splits + parts + 1);
+            why = validate_splits(plan->row_splits, n_rows, "row");
+            if (!why.empty()) return fail(CFDXG_ERR_INVALID_ARGUMENT, why);
         } else {
-            plan->splits = balanced_splits(n, ro, parts);
+            plan->row_splits = balanced_splits(n_rows, ro, parts);
         }
+        if (square) {
+            plan->col_splits = plan->row_splits;
+        } else {
+            plan->col_splits.assign(col_splits, col_splits + parts + 1);
+            why = validate_splits(plan->col_splits, n_cols, "column");
+            if (!why.empty()) return fail(CFDXG_ERR_INVALID_ARGUMENT, why);
+        }
+        const auto& cs = plan->col_splits;
         plan->parts.resize(parts);
         for (int p = 0; p < parts; ++p) {
             Part& P = plan->parts[p];
-            P.r0 = plan->splits[p];
-            P.r1 = plan->splits[p + 1];
-            build_local(ro, co, P);
+            P.r0 = plan->row_splits[p];
+            P.r1 = plan->row_splits[p + 1];
+            P.c0 = cs[p];
+            P.c1 = cs[p + 1];
+            build_local(ro, co, square, P);
         }
-        // per part and neighbour: [ghost range received] and [owned rows sent]
+        // per part and neighbour: [ghost range received] and [owned columns sent]
         std::vector<std::map<int, std::pair<std::pair<int64_t, int64_t>, std::vector<int64_t>>>> links(parts);
         for (int p = 0; p < parts; ++p) {
             const Part& P = plan->parts[p];
             for (size_t g = 0; g < P.ghosts.size();) {
-                const int q = owner_of(plan->splits, P.ghosts[g]);
+                const int q = owner_of(cs, P.ghosts[g]);
                 size_t e = g;
-                while (e < P.ghosts.size() && P.ghosts[e] < plan->splits[q + 1]) ++e;
+                while (e < P.ghosts.size() && P.ghosts[e] < cs[q + 1]) ++e;
                 links[p][q].first = {static_cast<int64_t>(g), static_cast<int64_t>(e)};
                 auto& send = links[q][p].second;
-                for (size_t t = g; t < e; ++t) send.push_back(P.ghosts[t] - plan->splits[q]);
+                for (size_t t = g; t < e; ++t) send.push_back(P.ghosts[t] - cs[q]);
                 g = e;
             }
         }
         for (int p = 0; p < parts; ++p) {
             Part& P = plan->parts[p];
-            const int64_t owned = P.r1 - P.r0;
+            const int64_t owned = P.c1 - P.c0;
             P.recv_off.push_back(0);
             P.send_off.push_back(0);
             for (auto& [q, link] : links[p]) {
@@ -189,9 +220,25 @@ int cfdxg_domain_plan_create(int64_t n, const int64_t* ro, const int64_t* co, in
     return CFDXG_OK;
 }
 
-int cfdxg_domain_plan_parts(const cfdxg_domain_plan* plan, int64_t* row_splits) {
+}  // namespace
+
+extern "C" {
+
+int cfdxg_domain_plan_create(int64_t n, const int64_t* ro, const int64_t* co, int32_t parts,
+                             const int64_t* row_splits, cfdxg_domain_plan** out) {
+    return create(n, n, ro, co, parts, row_splits, nullptr, true, out);
+}
+
+int cfdxg_domain_plan_create_rect(int64_t n_rows, int64_t n_cols, const int64_t* ro, const int64_t* co,
+                                  int32_t parts, const int64_t* row_splits, const int64_t* col_splits,
+                                  cfdxg_domain_plan** out) {
+    return create(n_rows, n_cols, ro, co, parts, row_splits, col_splits, false, out);
+}
+
+int cfdxg_domain_plan_parts(const cfdxg_domain_plan* plan, int64_t* row_splits, int64_t* col_splits) {
     if (!plan) return fail(CFDXG_ERR_INVALID_ARGUMENT, "domain plan: null handle");
-    if (row_splits) std::memcpy(row_splits, plan->splits.data(), plan->splits.size() * sizeof(int64_t));
+    if (row_splits) std::memcpy(row_splits, plan->row_splits.data(), plan->row_splits.size() * sizeof(int64_t));
+    if (col_splits) std::memcpy(col_splits, plan->col_splits.data(), plan->col_splits.size() * sizeof(int64_t));
     return static_cast<int>(plan->parts.size());
 }
 
@@ -202,13 +249,17 @@ int cfdxg_domain_plan_info(const cfdxg_domain_plan* plan, int32_t part, cfdxg_do
     const Part& P = plan->parts[part];
     info->row_begin = P.r0;
     info->row_end = P.r1;
-    info->n_local = static_cast<int64_t>(P.lro.size()) - 1;
+    info->n_local = (P.c1 - P.c0) + static_cast<int64_t>(P.ghosts.size());
     info->owned_offset = P.below;
     info->nnz_local = static_cast<int64_t>(P.lco.size());
     info->nnz_block = static_cast<int64_t>(P.bco.size());
     info->n_neighbours = static_cast<int32_t>(P.nb.size());
     info->n_recv = static_cast<int64_t>(P.ghosts.size());
     info->n_send = static_cast<int64_t>(P.send_rows.size());
+    info->col_begin = P.c0;
+    info->col_end = P.c1;
+    info->n_local_rows = static_cast<int64_t>(P.lro.size()) - 1;
+    info->first_row = P.first_row;
     return CFDXG_OK;
 }
 

@@ -550,26 +550,30 @@ const char* cfdxg_capture_last_error(void);
 typedef struct cfdxg_domain_plan cfdxg_domain_plan;
 typedef struct {
     int64_t row_begin, row_end;      /* owned global rows [row_begin, row_end) */
-    int64_t n_local;                 /* local vector length: ghosts + owned */
-    int64_t owned_offset;            /* local position of row_begin (= ghosts below) */
+    int64_t n_local;                 /* local vector length: ghosts + owned columns */
+    int64_t owned_offset;            /* local position of col_begin (= ghosts below) */
     int64_t nnz_local;               /* entries of the owned rows */
-    int64_t nnz_block;               /* entries of the diagonal block */
+    int64_t nnz_block;               /* entries in owned columns */
     int32_t n_neighbours;
     int64_t n_recv, n_send;          /* ghost values received / owned values sent */
+    int64_t col_begin, col_end;      /* owned columns (= the rows for a square plan) */
+    int64_t n_local_rows;            /* rows of the local system: n_local for a square
+                                        plan (ghost rows empty), owned rows otherwise */
+    int64_t first_row;               /* local row of row_begin: owned_offset or 0 */
 } cfdxg_domain_part_info;
 typedef struct {                     /* output arrays; NULL skips one */
-    int64_t* local_row_offsets;      /* n_local + 1 (ghost rows are empty) */
+    int64_t* local_row_offsets;      /* n_local_rows + 1 */
     int64_t* local_columns;          /* nnz_local, local numbering */
     int64_t* local_source;           /* nnz_local, global CSR entry index */
     int64_t* block_row_offsets;      /* (row_end - row_begin) + 1 */
-    int64_t* block_columns;          /* nnz_block, owned numbering */
+    int64_t* block_columns;          /* nnz_block, column - col_begin */
     int64_t* block_source;           /* nnz_block */
     int32_t* neighbours;             /* n_neighbours, increasing part ids */
     int64_t* recv_offsets;           /* n_neighbours + 1 into ghost_rows */
     int64_t* recv_start;             /* n_neighbours: local position of each slice */
-    int64_t* ghost_rows;             /* n_recv global rows, increasing */
+    int64_t* ghost_rows;             /* n_recv global columns, increasing */
     int64_t* send_offsets;           /* n_neighbours + 1 into send_rows */
-    int64_t* send_rows;              /* n_send owned indices (0-based in the part) */
+    int64_t* send_rows;              /* n_send owned column indices (0-based in the part) */
 } cfdxg_domain_part_arrays;
 
 /* Builds the plan of an n x n CSR pattern (row offsets, columns strictly
@@ -580,8 +584,15 @@ typedef struct {                     /* output arrays; NULL skips one */
  * cfdxg_domain_last_error() on bad input. */
 int cfdxg_domain_plan_create(int64_t n, const int64_t* row_offsets, const int64_t* columns, int32_t parts,
                              const int64_t* row_splits, cfdxg_domain_plan** out);
-/* row_splits (parts + 1) of the plan; returns the number of parts. */
-int cfdxg_domain_plan_parts(const cfdxg_domain_plan* plan, int64_t* row_splits);
+/* The plan of an n_rows x n_cols operator (an AMG transfer: P or P^T) whose
+ * rows are split by row_splits and whose input vector by col_splits (both
+ * parts + 1 offsets, required): part p owns rows and input entries of its
+ * blocks; the local input vector is [ghosts below | owned | ghosts above]. */
+int cfdxg_domain_plan_create_rect(int64_t n_rows, int64_t n_cols, const int64_t* row_offsets,
+                                  const int64_t* columns, int32_t parts, const int64_t* row_splits,
+                                  const int64_t* col_splits, cfdxg_domain_plan** out);
+/* Row and column splits (parts + 1 each, NULL skips); returns the number of parts. */
+int cfdxg_domain_plan_parts(const cfdxg_domain_plan* plan, int64_t* row_splits, int64_t* col_splits);
 int cfdxg_domain_plan_info(const cfdxg_domain_plan* plan, int32_t part, cfdxg_domain_part_info* info);
 int cfdxg_domain_plan_export(const cfdxg_domain_plan* plan, int32_t part, const cfdxg_domain_part_arrays* out);
 int cfdxg_domain_plan_destroy(cfdxg_domain_plan* plan);

@@ -250,3 +250,141 @@ def test_gloo_ranks_solve_one_system(parts):
     _, (xs, rs) = _solve_parts(ro, co_, va, b, parts, domain.PartComm(parts))
     assert rs["iterations"] == reps[0]["iterations"]
     assert np.linalg.norm(np.concatenate([xs[p] for p in range(parts)]) - xg) <= 1e-9 * np.linalg.norm(xg)
+
+
+# ------------------------------------------------- the distributed V-cycle
+class HostOperator:
+    """The oracle's product with a host CSR operator (the CPU stand-in for CudaOperator)."""
+
+    def __init__(self, ro, co_, va, n_rows, n_cols):
+        self.ro, self.co, self.va = (np.ascontiguousarray(ro, np.int64), np.ascontiguousarray(co_, np.int64),
+                                     np.ascontiguousarray(va, np.float64))
+
+    def __call__(self, x):
+        return torch.from_numpy(co.spmv(self.ro, self.co, self.va, x.contiguous().numpy()))
+
+
+def _hierarchy(ro, co_, va):
+    amg = NativeBoomerAMGPreconditioner()
+    assert amg.setup_host(ro, co_, va), amg.last_error()
+    levels = [amg.export_level(l) for l in range(len(amg.hierarchy_level_sizes()))]
+    return levels, amg.omega
+
+
+def _distributed_amg(ro, co_, va, parts, comm, replicate_below, levels=None):
+    levels, omega = levels or _hierarchy(ro, co_, va)
+    plan = domain.DomainPlan(ro, co_, parts)
+    dm = domain.DistributedAMG(comm, levels, omega, plan.row_splits, HostOperator, torch.device("cpu"),
+                               replicate_below=replicate_below)
+    return plan, dm, levels, omega
+
+
+@pytest.mark.parametrize("parts,replicate_below", [(1, 4096), (2, 64), (3, 64), (5, 200), (4, 10 ** 9), (3, 16)])
+def test_distributed_vcycle_is_the_undivided_vcycle_bit_for_bit(parts, replicate_below):
+    ro, co_, va, b = _system(8)
+    levels, omega = _hierarchy(ro, co_, va)
+    plan, dm, _, _ = _distributed_amg(ro, co_, va, parts, domain.PartComm(parts), replicate_below, (levels, omega))
+    if replicate_below == 64:
+        assert sum(dm.dist) >= 3                                  # several split levels, then replicated ones
+    H = co.Hierarchy(levels, omega)
+    rng = np.random.default_rng(parts)
+    for _ in range(2):
+        r = rng.standard_normal(ro.size - 1)
+        want = H.apply(r)
+        z = {p: torch.empty(int(plan.row_splits[p + 1] - plan.row_splits[p]), dtype=torch.float64)
+             for p in range(parts)}
+        dm.apply({p: torch.from_numpy(r[plan.row_splits[p]:plan.row_splits[p + 1]].copy()) for p in range(parts)},
+                 z)
+        got = np.concatenate([z[p].numpy() for p in range(parts)])
+        assert np.array_equal(got, want)
+
+
+def test_coarse_blocks_follow_the_fine_blocks():
+    ro, co_, va, b = _system(8)
+    levels, omega = _hierarchy(ro, co_, va)
+    plan, dm, _, _ = _distributed_amg(ro, co_, va, 4, domain.PartComm(4), 64, (levels, omega))
+    for l in range(1, len(dm.splits)):
+        S = dm.splits[l]
+        assert S[0] == 0 and S[-1] == dm.n[l] and np.all(np.diff(S) > 0)
+    # the first transfer: each part interpolates almost only from its own coarse block
+    lv, F, S = levels[0], dm.splits[0], dm.splits[1]
+    inside = 0
+    for p in range(4):
+        cols = lv["p_columns"][lv["p_offsets"][F[p]]:lv["p_offsets"][F[p + 1]]]
+        inside += np.count_nonzero((cols >= S[p]) & (cols < S[p + 1]))
+    assert inside >= 0.95 * lv["p_columns"].size
+
+
+def test_fgmres_with_the_distributed_vcycle_keeps_the_iteration_count():
+    ro, co_, va, b = _system(8)
+    levels, omega = _hierarchy(ro, co_, va)
+    its = {}
+    for parts in (1, 2, 4, 7):
+        comm = domain.PartComm(parts)
+        plan, dm, _, _ = _distributed_amg(ro, co_, va, parts, comm, 64, (levels, omega))
+        local = {p: OraclePart.__new__(OraclePart) for p in comm.local_parts}
+        for p in local:
+            local[p].layout = plan.part(p)
+            local[p].lv = np.ascontiguousarray(va[local[p].layout.local_source])
+        solver = domain.DistributedFGMRES(comm, local, restart=30, preconditioner=dm)
+        x, rep = solver.solve(domain.split_rows(plan, comm, b), tolerance=1e-8)
+        xg = np.concatenate([x[p] for p in range(parts)])
+        assert rep["status_name"] == "converged"
+        assert np.linalg.norm(b - co.spmv(ro, co_, va, xg)) <= 1e-8 * np.linalg.norm(b)
+        its[parts] = rep["iterations"]
+    assert len(set(its.values())) == 1, its                        # block-Jacobi needed 35-116 here
+    _, ref = co.solve_gmres(ro, co_, va, b, co.Hierarchy(levels, omega), restart=30, tolerance=1e-8)
+    assert abs(its[1] - ref["iterations"]) <= 1
+
+
+def _rank_vcycle(rank, world, port, parts, out):
+    import datetime
+
+    import torch.distributed as dist
+
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=60))
+    try:
+        ro, co_, va, b = _system(8)
+        comm = domain.PartComm(parts, rank, world)
+        plan, dm, levels, omega = _distributed_amg(ro, co_, va, parts, comm, 64)
+        r = np.random.default_rng(9).standard_normal(ro.size - 1)
+        z = {p: torch.empty(int(plan.row_splits[p + 1] - plan.row_splits[p]), dtype=torch.float64)
+             for p in comm.local_parts}
+        dm.apply({p: torch.from_numpy(r[plan.row_splits[p]:plan.row_splits[p + 1]].copy())
+                  for p in comm.local_parts}, z)
+        local = {p: OraclePart.__new__(OraclePart) for p in comm.local_parts}
+        for p in local:
+            local[p].layout = plan.part(p)
+            local[p].lv = np.ascontiguousarray(va[local[p].layout.local_source])
+        x, rep = domain.DistributedFGMRES(comm, local, preconditioner=dm).solve(domain.split_rows(plan, comm, b),
+                                                                               tolerance=1e-8)
+        out.put((rank, {p: v.numpy() for p, v in z.items()}, x, rep["iterations"]))
+        dist.barrier()
+    finally:
+        dist.destroy_process_group()
+
+
+def test_gloo_ranks_run_the_distributed_vcycle():
+    world, parts = 2, 4
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_rank_vcycle, args=(r, world, port, parts, q)) for r in range(world)]
+    for p in procs:
+        p.start()
+    results = [q.get(timeout=240) for _ in range(world)]
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    ro, co_, va, b = _system(8)
+    levels, omega = _hierarchy(ro, co_, va)
+    want = co.Hierarchy(levels, omega).apply(np.random.default_rng(9).standard_normal(ro.size - 1))
+    z, x = {}, {}
+    for rank, zr, xr, its in results:
+        z.update(zr)
+        x.update(xr)
+    assert np.array_equal(np.concatenate([z[p] for p in range(parts)]), want)
+    assert results[0][3] == results[1][3]
+    xg = np.concatenate([x[p] for p in range(parts)])
+    assert np.linalg.norm(b - co.spmv(ro, co_, va, xg)) <= 1e-8 * np.linalg.norm(b)

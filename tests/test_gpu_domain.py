@@ -54,7 +54,8 @@ def test_cuda_parts_product_is_bit_identical(ctx, system):
 def test_cuda_parts_solve(ctx, system, precision):
     ro, co_, va, b = system
     launches = ctx.kernel_launches
-    x, rep = domain.solve_distributed(ctx, ro, co_, va, b, 3, precision=precision, tolerance=1e-8)
+    x, rep = domain.solve_distributed(ctx, ro, co_, va, b, 3, preconditioner="block_jacobi", precision=precision,
+                                      tolerance=1e-8)
     assert ctx.kernel_launches > launches
     xg = np.concatenate([x[p] for p in range(3)])
     res = np.linalg.norm(b - co.spmv(ro, co_, va, xg)) / np.linalg.norm(b)
