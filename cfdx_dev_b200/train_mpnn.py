@@ -17,6 +17,16 @@ Adam by the library's own forward and backward kernels.
 
     python -m cfdx_dev_b200.train_mpnn --meshes 64 --pairs-per-mesh 16 \
         --min-n 16 --max-n 40 --epochs 30 --out weights.bin
+
+Data-parallel over the GPUs of one node (one process per GPU, NCCL):
+
+    torchrun --nproc-per-node 8 --master-addr 127.0.0.1 -m cfdx_dev_b200.train_mpnn --meshes 64 ...
+
+Each rank generates and holds its own meshes (mesh i goes to rank i mod
+world); every step each rank takes the loss gradient of its own batch with the
+library's kernels, one all-reduce averages the gradients weighted by the pair
+counts, and every rank applies the same FP32 Adam update, so the parameters
+stay identical everywhere.
 """
 from __future__ import annotations
 
@@ -35,6 +45,53 @@ if str(ROOT) not in sys.path:
 import cfdx_dev_b200 as cg  # noqa: E402
 
 SEED_BASE = 7_000_000
+
+
+class DataParallelAdam:
+    """Adam on gradients averaged over the processes of a torch.distributed group.
+
+    ``step(grad, loss, count)`` takes this process's mean loss gradient over
+    ``count`` pairs; one all-reduce of [count * grad, count * loss, count]
+    gives the mean over every pair of every process, and the update is the
+    library's FP32 Adam (beta1 0.9, beta2 0.999, eps 1e-8, bias-corrected:
+    the k_adam kernel of train_step) applied identically on every process.
+    Without a process group it is plain Adam on one process's gradient."""
+
+    def __init__(self, params, lr: float, group=None):
+        self.p = np.array(params, np.float32)
+        self.m = np.zeros_like(self.p)
+        self.v = np.zeros_like(self.p)
+        self.t = 0
+        self.lr = np.float32(lr)
+        self.group = group
+
+    def _allreduce(self, buf: np.ndarray) -> np.ndarray:
+        import torch
+        import torch.distributed as dist
+        if not (dist.is_available() and dist.is_initialized()) or dist.get_world_size(self.group) == 1:
+            return buf
+        backend = dist.get_backend(self.group)
+        dev = torch.device("cuda", torch.cuda.current_device()) if backend == "nccl" else torch.device("cpu")
+        t = torch.as_tensor(buf, device=dev)
+        dist.all_reduce(t, group=self.group)
+        return t.cpu().numpy()
+
+    def step(self, grad, loss: float, count: int, lr: float | None = None):
+        """One update; returns (mean loss over all pairs, new parameters)."""
+        g = np.asarray(grad, np.float64)
+        buf = np.concatenate([g * count, [loss * count, float(count)]])
+        buf = self._allreduce(buf)
+        total = buf[-1]
+        g = (buf[:-2] / total).astype(np.float32)
+        self.t += 1
+        f32 = np.float32
+        bc1 = f32(1.0) - f32(0.9) ** f32(self.t)
+        bc2 = f32(1.0) - f32(0.999) ** f32(self.t)
+        self.m = f32(0.9) * self.m + f32(0.1) * g
+        self.v = f32(0.999) * self.v + f32(0.001) * g * g
+        step_lr = self.lr if lr is None else f32(lr)
+        self.p = self.p - step_lr * (self.m / bc1) / (np.sqrt(self.v / bc2) + f32(1e-8))
+        return float(buf[-2] / total), self.p
 
 
 def make_system(ctx, n, seed):
@@ -96,12 +153,26 @@ def make_pairs(ctx, sysd, k, seed, richardson_steps=0):
 
 
 def train(args):
-    ctx = cg.Context(0)
+    from cfdx_dev_b200 import replicas
+    rank, local_rank, world = replicas.dist_env()
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+        if args.meshes % world:
+            raise SystemExit("--meshes must be a multiple of the number of processes")
+        torch.cuda.set_device(local_rank)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    ctx = cg.Context(local_rank)
     net = cg.LearnedPreconditioner(ctx, seed=args.seed)
+    opt = DataParallelAdam(net.parameters(), args.lr) if world > 1 else None
     sizes = np.linspace(args.min_n, args.max_n, args.meshes).round().astype(int)
     data = []
     t0 = time.time()
     for i, n in enumerate(sizes):
+        if i % world != rank:
+            continue
         sysd = make_system(ctx, int(n), i)
         R, E = make_pairs(ctx, sysd, args.pairs_per_mesh, i, args.richardson_steps)
         data.append((sysd, R, E))
@@ -118,13 +189,24 @@ def train(args):
             net.bind(sysd["mesh"], sysd["A"], sysd["aP"])
             net.set_vcycle(sysd["vcycle"] if args.composed else None)
             for b in range(0, len(R), args.batch):
-                losses.append(net.train_step(R[b:b + args.batch], E[b:b + args.batch], lr=lr))
+                Rb, Eb = R[b:b + args.batch], E[b:b + args.batch]
+                if opt is None:
+                    losses.append(net.train_step(Rb, Eb, lr=lr))
+                else:
+                    loss, grad = net.loss_grad(Rb, Eb)
+                    loss, params = opt.step(grad, loss, len(Rb), lr=lr)
+                    net.set_parameters(params)
+                    losses.append(loss)
         if epoch == int(0.7 * args.epochs):
             lr *= 0.3
         history.append(float(np.mean(losses)))
         print(f"epoch {epoch} loss {history[-1]:.4f} ({time.time() - t1:.1f}s)", flush=True)
-    net.save(args.out)
-    summary = {"meshes": len(data), "pairs": int(sum(len(R) for _, R, _ in data)),
+    if rank == 0:
+        net.save(args.out)
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+    summary = {"meshes": len(data), "pairs": int(sum(len(R) for _, R, _ in data)), "rank": rank, "world": world,
                "sizes": [int(s) for s in sizes], "generation_s": gen_s, "training_s": time.time() - t1,
                "loss_history": history, "params": net.n_params, "out": str(args.out)}
     print(json.dumps(summary), flush=True)
