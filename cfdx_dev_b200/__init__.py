@@ -26,6 +26,7 @@ from .api import (  # noqa: F401
     parse_linear_capture_iterations,
     random_field,
     read_linear_system_capture,
+    scale_matrix,
     select_linear_solver,
     solve_cg,
     solve_fgmres,

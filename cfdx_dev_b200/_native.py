@@ -73,6 +73,7 @@ class Request(C.Structure):
         ("residual_replacement_period", C.c_int64), ("residual_replacement_gap_ratio", C.c_double),
         ("target_reduction_per_cycle", C.c_double), ("learned", C.c_void_p),
         ("learned_applications", C.c_int32), ("orthogonalization", C.c_int32), ("problem", C.c_int32),
+        ("scaling", C.c_int32),
     ]
 
 
@@ -224,6 +225,7 @@ PROTOTYPES = {
     "cfdxg_select_linear_solver": (C.c_int, [C.c_int32, _P(MatrixCharacteristics), _P(PlanRequest),
                                             _P(SolverPlan)]),
     "cfdxg_plan_last_error": (C.c_char_p, []),
+    "cfdxg_scale_matrix": (C.c_int, [C.c_int64, _V, _V, _V, C.c_int32, C.c_double, _V, _V, _V, _V]),
     "cfdxg_plan_reason": (C.c_char_p, [_V]),
     "cfdxg_domain_plan_create": (C.c_int, [C.c_int64, _V, _V, C.c_int32, _V, _P(_V)]),
     "cfdxg_domain_plan_create_rect": (C.c_int, [C.c_int64, C.c_int64, _V, _V, C.c_int32, _V, _V, _P(_V)]),

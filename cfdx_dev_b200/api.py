@@ -509,7 +509,7 @@ class NativeBoomerAMGPreconditioner:
 
 
 def make_request(krylov="gmres", preconditioner="native_amg", restart=40, precision="fp64", learned=None,
-                 problem="pressure_poisson", **kw):
+                 problem="pressure_poisson", scaling="none", **kw):
     """A cfdxg_request; krylov / preconditioner "auto" select the plan from the measured matrix."""
     lib = N.load()
     r = N.Request()
@@ -520,6 +520,7 @@ def make_request(krylov="gmres", preconditioner="native_amg", restart=40, precis
     r.precision = N.PRECISION[precision]
     r.learned = learned.handle if learned is not None else None
     r.problem = N.PROBLEMS.index(problem)
+    r.scaling = N.SCALINGS.index(scaling)
     for k, v in kw.items():
         setattr(r, k, v)
     return r
@@ -536,6 +537,22 @@ def measure_matrix_characteristics(row_offsets, columns, values, saddle_point=Fa
     if rc != 0:
         raise CfdxgError(rc, lib.cfdxg_plan_last_error().decode())
     return c.as_dict()
+
+
+def scale_matrix(row_offsets, columns, values, scaling: str, zero_tolerance=0.0):
+    """core/linalg/matrix_diagnostics.h:410 scale_matrix on the host -> dict of the
+    row and column scales, the scaled values (same pattern) and the zero counts."""
+    lib = N.load()
+    ro, co, va = _i64(row_offsets), _i64(columns), _f64(values)
+    n = ro.size - 1
+    out = dict(row_scale=np.empty(n), column_scale=np.empty(n), values=np.empty(va.size))
+    zc = np.zeros(2, np.int64)
+    rc = lib.cfdxg_scale_matrix(n, N.ptr(ro), N.ptr(co), N.ptr(va), N.SCALINGS.index(scaling), float(zero_tolerance),
+                                N.ptr(out["row_scale"]), N.ptr(out["column_scale"]), N.ptr(out["values"]), N.ptr(zc))
+    if rc != 0:
+        raise CfdxgError(rc, lib.cfdxg_plan_last_error().decode())
+    out.update(zero_rows=int(zc[0]), zero_columns=int(zc[1]))
+    return out
 
 
 def select_linear_solver(problem: str, characteristics: dict, krylov="auto", preconditioner="auto",
@@ -572,6 +589,7 @@ def solve_linear_system(A: SparseMatrix, rhs, x0=None, krylov="gmres", precondit
     if linear_capture_path:
         ro, co, va = A.to_csr()
         write_linear_system_capture(linear_capture_path, ro, co, va, b, x, problem=CAPTURE_PRESSURE_POISSON,
+                                    scaling=N.SCALINGS.index(kw.get("scaling", "none")),
                                     max_iterations=max_iterations, tolerance=tolerance)
     req = make_request(krylov, preconditioner, restart, precision, learned, **kw)
     rep = N.Report()

@@ -731,6 +731,93 @@ void validate_request(const cfdxg_request& r) {
     if (r.learned_applications < 0) throw Error(CFDXG_ERR_INVALID_ARGUMENT, "learned_applications must be >= 0");
     if (r.orthogonalization != CFDXG_ORTHO_MGS2 && r.orthogonalization != CFDXG_ORTHO_CGS2)
         throw Error(CFDXG_ERR_INVALID_ARGUMENT, "unknown orthogonalization");
+    if (r.scaling < CFDXG_SCALING_NONE || r.scaling > CFDXG_SCALING_SYMMETRIC_DIAGONAL)
+        throw Error(CFDXG_ERR_INVALID_ARGUMENT, "unknown scaling model");
+    // linear_solver_dispatch.h:283-297
+    if (r.krylov == CFDXG_KRYLOV_CG && r.scaling != CFDXG_SCALING_NONE && r.scaling != CFDXG_SCALING_SYMMETRIC_DIAGONAL)
+        throw Error(CFDXG_ERR_INVALID_ARGUMENT, "CG requires symmetry-preserving scaling (symmetric_diagonal)");
+    if (r.scaling != CFDXG_SCALING_NONE && r.problem == CFDXG_PROBLEM_COUPLED_PRESSURE_VELOCITY)
+        throw Error(CFDXG_ERR_INVALID_ARGUMENT, "scaling is provided for scalar systems only");
+}
+
+// Scaled solve (linear_solver_dispatch.h:302-328, 466-490): scale_matrix on
+// the host, the scaled system solved to a tenth of the tolerance by the
+// unscaled dispatch, the solution unscaled (x_i = c_i * y_i) and certified on
+// the original system, whose FP64 true residual also replaces the reported
+// residuals.  Rows or columns left unscaled (zero maximum) make the request
+// NOT_APPLICABLE with x untouched and an infinite physical residual.
+int solve_scaled(cfdxg_context* ctx, const cfdxg_matrix* A, const double* rhs, double* x, int32_t mem,
+                 const cfdxg_request& req, int64_t max_iterations, double tolerance, cfdxg_report* report) {
+    const int64_t n = A->n, nnz = A->nnz;
+    std::vector<double> downloaded;
+    const double* hv = A->host.va.data();
+    if (!A->host_values_valid) {
+        downloaded.resize(static_cast<size_t>(nnz));
+        A->va.download(downloaded.data(), ctx->stream);
+        CFDXG_CUDA(cudaStreamSynchronize(ctx->stream));
+        hv = downloaded.data();
+    }
+    std::vector<double> b(n), x0(n), rs(n), cs(n), sv(nnz);
+    const cudaMemcpyKind to_host = mem == CFDXG_MEM_DEVICE ? cudaMemcpyDeviceToHost : cudaMemcpyHostToHost;
+    CFDXG_CUDA(cudaMemcpy(b.data(), rhs, sizeof(double) * n, to_host));
+    CFDXG_CUDA(cudaMemcpy(x0.data(), x, sizeof(double) * n, to_host));
+    int64_t zero_rows = 0, zero_cols = 0;
+    scale_values(req.scaling, n, A->host.ro.data(), A->host.co.data(), hv, 0.0, rs.data(), cs.data(), sv.data(),
+                 zero_rows, zero_cols);
+    if (report) std::memset(report, 0, sizeof(*report));
+    if (zero_rows || zero_cols) {
+        ctx->error = "scaling left a zero row or column";
+        if (report) {
+            report->status = CFDXG_NOT_APPLICABLE;
+            report->physical_residual_relative = std::numeric_limits<double>::infinity();
+            report->plan_krylov = req.krylov;
+            report->plan_preconditioner = req.preconditioner;
+        }
+        return CFDXG_NOT_APPLICABLE;
+    }
+    std::vector<int64_t> ro(A->host.ro.begin(), A->host.ro.end()), co(A->host.co.begin(), A->host.co.end());
+    cfdxg_matrix* As = nullptr;
+    int rc = cfdxg_matrix_create(ctx, n, ro.data(), co.data(), sv.data(), CFDXG_MEM_HOST, &As);
+    if (rc != CFDXG_OK) return rc;
+    std::unique_ptr<cfdxg_matrix, int (*)(cfdxg_matrix*)> hold(As, cfdxg_matrix_destroy);
+    std::vector<double> bs(n), xs(n);
+    for (int64_t i = 0; i < n; ++i) {
+        bs[i] = rs[i] * b[i];
+        xs[i] = x0[i] / cs[i];
+    }
+    cfdxg_request inner = req;
+    inner.scaling = CFDXG_SCALING_NONE;
+    cfdxg_report rin{};
+    const double t0 = now_seconds();
+    rc = cfdxg_solve_linear_system(ctx, As, bs.data(), xs.data(), CFDXG_MEM_HOST, &inner, max_iterations,
+                                   0.1 * tolerance, &rin);
+    if (rc < 0) return rc;
+    std::vector<double> xr(n);
+    for (int64_t i = 0; i < n; ++i) xr[i] = cs[i] * xs[i];
+    // the certificate on the original system, with the homogeneous reference for b = 0
+    DevBuf<double> db(n), dx(n);
+    db.upload(b, ctx->stream);
+    dx.upload(x0, ctx->stream);
+    const double rhs_norm = device_norm2(ctx, A, db.get());
+    const double homogeneous = rhs_norm == 0.0 ? device_residual_norm(ctx, A, db.get(), dx.get()) : 0.0;
+    dx.upload(xr, ctx->stream);
+    const double final_residual = device_residual_norm(ctx, A, db.get(), dx.get());
+    const double reference = rhs_norm > 0.0 ? rhs_norm : homogeneous;
+    const double physical = reference > 0.0 ? final_residual / reference
+                                            : (final_residual == 0.0 ? 0.0 : std::numeric_limits<double>::infinity());
+    int status = rin.status;
+    if (status == CFDXG_CONVERGED && (!std::isfinite(physical) || physical > tolerance)) status = CFDXG_MAX_ITER_REACHED;
+    const cudaMemcpyKind from_host = mem == CFDXG_MEM_DEVICE ? cudaMemcpyHostToDevice : cudaMemcpyHostToHost;
+    CFDXG_CUDA(cudaMemcpy(x, xr.data(), sizeof(double) * n, from_host));
+    if (report) {
+        *report = rin;
+        report->status = status;
+        report->physical_residual_relative = physical;
+        report->residual_relative = physical;
+        report->residual = physical * rhs_norm;
+        report->solve_seconds = now_seconds() - t0 - rin.setup_seconds;
+    }
+    return status;
 }
 
 // measure_matrix_characteristics' symmetry and positive-diagonal test, on the device.
@@ -781,7 +868,7 @@ extern "C" int cfdxg_solve_linear_system(cfdxg_context* ctx, const cfdxg_matrix*
             // a forced CG fails closed before any plan is drawn
             req.preconditioner = CFDXG_PC_NONE;
         } else {
-            const cfdxg_plan_request pr{req.krylov, req.preconditioner, req.gmres_restart, 0, 0, 1.0};
+            const cfdxg_plan_request pr{req.krylov, req.preconditioner, req.gmres_restart, 0, req.scaling, 1.0};
             cfdxg_solver_plan plan;
             std::string why;
             if (!select_solver(req.problem, ch, pr, plan, why)) throw Error(CFDXG_ERR_INVALID_ARGUMENT, why);
@@ -801,6 +888,8 @@ extern "C" int cfdxg_solve_linear_system(cfdxg_context* ctx, const cfdxg_matrix*
         }
     }
     validate_request(req);
+    if (req.scaling != CFDXG_SCALING_NONE && !not_provided)
+        return solve_scaled(ctx, A, rhs, x, mem, req, max_iterations, tolerance, report);
     if (report) std::memset(report, 0, sizeof(*report));
     const int64_t n = A->n;
     In<double> b(ctx, rhs, n, mem);

@@ -211,6 +211,37 @@ int cfdxg_select_linear_solver(int32_t problem, const cfdxg_matrix_characteristi
     return CFDXG_OK;
 }
 
+int cfdxg_scale_matrix(int64_t n, const int64_t* ro, const int64_t* co, const double* va, int32_t scaling,
+                       double zero_tolerance, double* row_scale, double* column_scale, double* scaled_values,
+                       int64_t* zero_counts) {
+    if (!ro || n <= 0 || !row_scale || !column_scale || !scaled_values || (ro[n] > 0 && (!co || !va))) {
+        g_plan_error = "scaling: null argument";
+        return CFDXG_ERR_INVALID_ARGUMENT;
+    }
+    if (scaling < 0 || scaling > 4) {
+        g_plan_error = "scaling: unknown scaling model";
+        return CFDXG_ERR_INVALID_ARGUMENT;
+    }
+    if (!(zero_tolerance >= 0.0) || !std::isfinite(zero_tolerance)) {
+        g_plan_error = "scaling: the zero-row tolerance must be finite and non-negative";
+        return CFDXG_ERR_INVALID_ARGUMENT;
+    }
+    for (int64_t i = 0; i < n; ++i)
+        for (int64_t k = ro[i]; k < ro[i + 1]; ++k)
+            if (co[k] < 0 || co[k] >= n) {
+                g_plan_error = "scaling: column out of range";
+                return CFDXG_ERR_INVALID_ARGUMENT;
+            }
+    int64_t zr = 0, zc = 0;
+    cfdxg::scale_values(scaling, n, ro, co, va, zero_tolerance, row_scale, column_scale, scaled_values, zr, zc);
+    if (zero_counts) {
+        zero_counts[0] = zr;
+        zero_counts[1] = zc;
+    }
+    g_plan_error.clear();
+    return CFDXG_OK;
+}
+
 const char* cfdxg_plan_last_error(void) { return g_plan_error.c_str(); }
 
 }  // extern "C"

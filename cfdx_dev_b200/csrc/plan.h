@@ -13,6 +13,7 @@
 #include <cstdint>
 #include <limits>
 #include <string>
+#include <vector>
 
 #include "cfdxg.h"
 
@@ -104,6 +105,54 @@ void measure_characteristics(int64_t n, const I* ro, const I* co, const double* 
             }
         }
     }
+}
+
+// scale_matrix (core/linalg/matrix_diagnostics.h:410-490): row/column scales
+// 1 / max|a| (Row, Column, RowColumn) or 1 / sqrt|a_ii| on both sides
+// (SymmetricDiagonal, a_ii = the sum of the row's diagonal entries), left at 1
+// where the maximum (or |a_ii|) is <= zero_tolerance, which is counted; the
+// scaled entry is (a_ij * r_i) * c_j, re-stored as 0 + value the way the
+// reference's finalize re-accumulates each entry.
+template <class I>
+void scale_values(int32_t mode, int64_t n, const I* ro, const I* co, const double* va, double zero_tolerance,
+                  double* row_scale, double* col_scale, double* scaled, int64_t& zero_rows, int64_t& zero_cols) {
+    zero_rows = zero_cols = 0;
+    for (int64_t i = 0; i < n; ++i) row_scale[i] = col_scale[i] = 1.0;
+    const bool rows = mode == 1 || mode == 3, cols = mode == 2 || mode == 3;
+    if (rows || cols) {
+        std::vector<double> row_max(static_cast<size_t>(n), 0.0), col_max(static_cast<size_t>(n), 0.0);
+        for (int64_t i = 0; i < n; ++i)
+            for (int64_t k = static_cast<int64_t>(ro[i]); k < static_cast<int64_t>(ro[i + 1]); ++k) {
+                const double m = std::fabs(va[k]);
+                row_max[i] = ref_max(row_max[i], m);
+                col_max[co[k]] = ref_max(col_max[co[k]], m);
+            }
+        for (int64_t i = 0; i < n && rows; ++i) {
+            if (row_max[i] <= zero_tolerance) ++zero_rows;
+            else row_scale[i] = 1.0 / row_max[i];
+        }
+        for (int64_t j = 0; j < n && cols; ++j) {
+            if (col_max[j] <= zero_tolerance) ++zero_cols;
+            else col_scale[j] = 1.0 / col_max[j];
+        }
+    }
+    if (mode == 4) {
+        for (int64_t i = 0; i < n; ++i) {
+            double d = 0.0;
+            for (int64_t k = static_cast<int64_t>(ro[i]); k < static_cast<int64_t>(ro[i + 1]); ++k)
+                if (static_cast<int64_t>(co[k]) == i) d += va[k];
+            d = std::fabs(d);
+            if (d <= zero_tolerance) {
+                ++zero_rows;
+                ++zero_cols;
+            } else {
+                row_scale[i] = col_scale[i] = 1.0 / std::sqrt(d);
+            }
+        }
+    }
+    for (int64_t i = 0; i < n; ++i)
+        for (int64_t k = static_cast<int64_t>(ro[i]); k < static_cast<int64_t>(ro[i + 1]); ++k)
+            scaled[k] = 0.0 + va[k] * row_scale[i] * col_scale[co[k]];
 }
 
 // select_linear_solver; false with the reason in `why` where the reference

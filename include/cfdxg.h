@@ -69,6 +69,12 @@ extern "C" {
 #define CFDXG_PROBLEM_MOMENTUM 3
 #define CFDXG_PROBLEM_SCALAR_TRANSPORT 4
 #define CFDXG_PROBLEM_COUPLED_PRESSURE_VELOCITY 5
+/* LinearScalingModel (core/linalg/linear_solver_models.h:61) */
+#define CFDXG_SCALING_NONE 0
+#define CFDXG_SCALING_ROW 1
+#define CFDXG_SCALING_COLUMN 2
+#define CFDXG_SCALING_ROW_COLUMN 3
+#define CFDXG_SCALING_SYMMETRIC_DIAGONAL 4
 
 typedef struct cfdxg_context cfdxg_context;
 typedef struct cfdxg_mesh cfdxg_mesh;
@@ -353,6 +359,10 @@ typedef struct {
     int32_t problem;                 /* CFDXG_PROBLEM_* (default PRESSURE_POISSON): steers the
                                         automatic choice and the model checks of
                                         select_linear_solver */
+    int32_t scaling;                 /* CFDXG_SCALING_* (default NONE): cfdxg_solve_linear_system
+                                        solves the scaled system to 0.1 tolerance and certifies
+                                        the unscaled one (linear_solver_dispatch.h:302-328,
+                                        466-490); CG takes NONE or SYMMETRIC_DIAGONAL only */
 } cfdxg_request;
 
 /* Mirrors SolverResult (core/linalg/solver_status.h:45-72) + LinearSolveReport. */
@@ -454,6 +464,14 @@ int cfdxg_measure_matrix_characteristics(int64_t n, const int64_t* row_offsets, 
 int cfdxg_select_linear_solver(int32_t problem, const cfdxg_matrix_characteristics* characteristics,
                                const cfdxg_plan_request* request, cfdxg_solver_plan* plan);
 const char* cfdxg_plan_last_error(void);
+/* scale_matrix (core/linalg/matrix_diagnostics.h:410-490) of a square CSR
+ * matrix: scaling CFDXG_SCALING_* (LinearScalingModel numbering); writes the
+ * row and column scales (n each), the scaled values (nnz, the input pattern)
+ * and, in zero_counts[0..1], the rows and columns left unscaled because their
+ * maximum magnitude (or |diagonal|) is <= zero_tolerance. */
+int cfdxg_scale_matrix(int64_t n, const int64_t* row_offsets, const int64_t* columns, const double* values,
+                       int32_t scaling, double zero_tolerance, double* row_scale, double* column_scale,
+                       double* scaled_values, int64_t* zero_counts);
 /* The plan and its reason of the last cfdxg_solve_linear_system on the context. */
 const char* cfdxg_plan_reason(const cfdxg_context* ctx);
 

@@ -416,3 +416,21 @@ def select_linear_solver(problem: int, characteristics: dict, krylov=0, precondi
                                     float(c["coefficient_range"]), _p(flags), _p(req), float(braess_sarazin_alpha),
                                     _p(plan))
     return None if rc != 0 else tuple(int(v) for v in plan)
+
+
+def scale_matrix(ro, co, va, scaling, zero_tolerance=0.0):
+    """core/linalg/matrix_diagnostics.h:410 scale_matrix -> (row_scale, column_scale,
+    scaled values, zero rows, zero columns)."""
+    ro, co, va = (np.ascontiguousarray(ro, np.int64), np.ascontiguousarray(co, np.int64),
+                  np.ascontiguousarray(va, np.float64))
+    n = ro.size - 1
+    rs, cs, sv = np.empty(n), np.empty(n), np.empty(va.size)
+    zc = np.zeros(2, np.int64)
+    nnz = C.c_int64()
+    L = lib()
+    L.ref_scale_matrix.argtypes = [C.c_int64, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int32, C.c_double] + \
+        [C.c_void_p] * 5
+    _check(L.ref_scale_matrix(n, _p(ro), _p(co), _p(va), int(scaling), float(zero_tolerance), _p(rs), _p(cs),
+                              _p(sv), _p(zc), C.byref(nnz)), "scale_matrix")
+    assert nnz.value == va.size
+    return rs, cs, sv, int(zc[0]), int(zc[1])

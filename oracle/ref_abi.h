@@ -159,6 +159,10 @@ int ref_measure_characteristics(int64_t n, const int64_t* row_offsets, const int
 int ref_select_linear_solver(int32_t problem, int64_t equations, double average_nnz,
                              double coefficient_range, const int32_t* flags, const int32_t* req,
                              double braess_sarazin_alpha, int32_t* plan);
+/* core/linalg/matrix_diagnostics.h:410  scale_matrix (MatrixScaling numbering) */
+int ref_scale_matrix(int64_t n, const int64_t* row_offsets, const int64_t* columns, const double* values,
+                     int32_t scaling, double zero_tolerance, double* row_scale, double* column_scale,
+                     double* scaled_values, int64_t* zero_counts, int64_t* nnz_out);
 /* one SpMV with SparseMatrix::matvec (sparse_matrix.h:180) */
 int ref_spmv(int64_t n, const int64_t* row_offsets, const int64_t* columns,
              const double* values, const double* x, double* y);

@@ -369,3 +369,27 @@ extern "C" int ref_select_linear_solver(int32_t problem, int64_t equations, doub
         return -1;
     }
 }
+
+// core/linalg/matrix_diagnostics.h:410  scale_matrix (values keep the input pattern
+// when no entry merges; nnz_out receives the scaled matrix's entry count)
+extern "C" int ref_scale_matrix(int64_t n, const int64_t* ro, const int64_t* co, const double* va,
+                                int32_t scaling, double zero_tolerance, double* row_scale, double* column_scale,
+                                double* scaled_values, int64_t* zero_counts, int64_t* nnz_out) {
+    try {
+        const SparseMatrix A = cfdx_ref::make_csr(n, ro, co, va);
+        const MatrixScalingResult r = scale_matrix(A, static_cast<MatrixScaling>(scaling), zero_tolerance);
+        for (int64_t i = 0; i < n; ++i) {
+            row_scale[i] = r.row_scale[i];
+            column_scale[i] = r.column_scale[i];
+        }
+        *nnz_out = static_cast<int64_t>(r.matrix.nnz());
+        for (std::size_t k = 0; k < r.matrix.nnz(); ++k) scaled_values[k] = r.matrix.values_data()[k];
+        zero_counts[0] = static_cast<int64_t>(r.zero_rows);
+        zero_counts[1] = static_cast<int64_t>(r.zero_columns);
+        cfdx_ref::g_error.clear();
+        return 0;
+    } catch (const std::exception& e) {
+        cfdx_ref::set_error(e);
+        return -1;
+    }
+}

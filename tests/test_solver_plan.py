@@ -189,3 +189,27 @@ def test_pressure_systems_select_cg_with_native_amg():
     for name in ("asymmetric", "diagonal_range"):
         plan = cg.select_linear_solver("pressure_poisson", cg.measure_matrix_characteristics(*MATRICES[name]))
         assert (plan["krylov"], plan["preconditioner"]) == ("gmres", "ilu0"), name
+
+
+@pytest.mark.parametrize("name", sorted(MATRICES))
+@pytest.mark.parametrize("scaling", ["none", "row", "column", "row_column", "symmetric_diagonal"])
+@pytest.mark.parametrize("zero_tolerance", [0.0, 0.5])
+def test_scaling_matches_reference(ref, name, scaling, zero_tolerance):
+    ro, co_, va = MATRICES[name]
+    mine = cg.scale_matrix(ro, co_, va, scaling, zero_tolerance)
+    rs, cs, sv, zr, zc = ref.scale_matrix(ro, co_, va, N.SCALINGS.index(scaling), zero_tolerance)
+    for a, b in ((mine["row_scale"], rs), (mine["column_scale"], cs), (mine["values"], sv)):
+        assert a.tobytes() == b.tobytes()
+    assert (mine["zero_rows"], mine["zero_columns"]) == (zr, zc)
+
+
+def test_symmetric_diagonal_scaling_gives_a_unit_diagonal():
+    ro, co_, va = MATRICES["pressure_tet5"]
+    s = cg.scale_matrix(ro, co_, va, "symmetric_diagonal")
+    rows = np.repeat(np.arange(ro.size - 1), np.diff(ro))
+    diag = s["values"][rows == co_]
+    assert np.allclose(diag, 1.0, rtol=1e-15, atol=0)
+    c = cg.measure_matrix_characteristics(ro, co_, s["values"])
+    assert c["numerically_symmetric"] and c["positive_diagonal"]
+    with pytest.raises(CfdxgError):
+        cg.scale_matrix(ro, co_, va, "row", zero_tolerance=-1.0)
