@@ -1,0 +1,244 @@
+"""Known-answer tests of the reference's own test suite, restated against the
+oracle and the library's host code (no GPU).
+
+Each case names the reference test it mirrors and keeps that test's inputs
+and expected values:
+
+* tests/unit/test_scalar_diffusion.cpp:156-233 -- the 1-D chain of n hex
+  cells with phi = x^2 (source -2): Dirichlet/Dirichlet and
+  Dirichlet/Neumann give x_c^2 - dx^2/4 (the two-point stencil's known
+  offset), pure Neumann with the reference-cell gauge gives x_c^2 + 3, each
+  with a zero conservation balance;
+* tests/unit/test_gmres_solver.cpp:125-233 -- the diagonal 3x3, the 1-D
+  Poisson system, an already converged solve, a restarted solve and the exact
+  nonsymmetric 3x3;
+* tests/validation/test_amg_preconditioner_qualification.cpp -- the small
+  multilevel case (1-D Poisson, N = 17, :805-830), the transfer gates
+  (Galerkin and symmetric coarse operators, unit row sums of P, no empty
+  column, :262-273) and the stable smoother damping (:1018-1047).
+"""
+import numpy as np
+import pytest
+
+import cfdx_dev_b200 as cg
+from cfdx_dev_b200.api import HostMesh
+from oracle import cfdx_oracle as co
+from tests import cases
+from tests.test_poisson_driver import oracle_poisson_mixed
+
+
+# ------------------------------------------------------------ 1-D chain mesh
+def chain_mesh(n):
+    """make_1d_chain (test_scalar_diffusion.cpp:12-71): n unit-section hex cells
+    along x with their own 8 points each; faces: left end, right end, then per
+    cell y0, y1, z0, z1, then the n-1 internal faces."""
+    dx = 1.0 / n
+    pts = []
+    for i in range(n):
+        x0, x1 = dx * i, dx * (i + 1)
+        pts += [(x0, 0, 0), (x1, 0, 0), (x1, 1, 0), (x0, 1, 0), (x0, 0, 1), (x1, 0, 1), (x1, 1, 1), (x0, 1, 1)]
+    pts = np.array(pts, float)
+    faces, owner, neighbour, patch = [], [], [], []
+
+    def add(v, o, nb, pt):
+        faces.append(v)
+        owner.append(o)
+        neighbour.append(nb)
+        patch.append(pt)
+        return len(faces) - 1
+
+    left = add([0, 4, 7, 3], 0, -1, 0)
+    b = 8 * (n - 1)
+    right = add([b + 1, b + 2, b + 6, b + 5], n - 1, -1, 1)
+    side = []
+    for i in range(n):
+        b = 8 * i
+        side.append([add([b, b + 1, b + 5, b + 4], i, -1, 2), add([b + 3, b + 7, b + 6, b + 2], i, -1, 2),
+                     add([b, b + 3, b + 2, b + 1], i, -1, 2), add([b + 4, b + 5, b + 6, b + 7], i, -1, 2)])
+    internal = [add([8 * i + 1, 8 * i + 2, 8 * i + 6, 8 * i + 5], i, i + 1, -1) for i in range(n - 1)]
+    cells = [[left if i == 0 else internal[i - 1], right if i + 1 == n else internal[i]] + side[i] for i in range(n)]
+    fo = np.concatenate([[0], np.cumsum([len(f) for f in faces])]).astype(np.int64)
+    co_ = np.concatenate([[0], np.cumsum([len(c) for c in cells])]).astype(np.int64)
+    types = cg.hex_case(1).patch_types[:3].copy()
+    return HostMesh(px=pts[:, 0].copy(), py=pts[:, 1].copy(), pz=pts[:, 2].copy(), face_offsets=fo,
+                    face_vertices=np.concatenate(faces).astype(np.int64), owner=np.array(owner, np.int64),
+                    neighbour=np.array(neighbour, np.int64), cell_offsets=co_,
+                    cell_faces=np.concatenate(cells).astype(np.int64), patch_of_face=np.array(patch, np.int32),
+                    patch_types=types)
+
+
+def conservation_balance(m, bc, types, src, x, diffusivity=1.0):
+    """poisson_conservation_balance (core/solvers/scalar_diffusion.h:241-300):
+    the sources plus the prescribed boundary fluxes."""
+    g = co.geometry(m)
+    balance = float(np.sum(src * g["cell_volumes"]))
+    nf = m.owner.size
+    for f in range(nf):
+        if m.neighbour[f] >= 0 or not np.isfinite(bc[f]):
+            continue
+        o = m.owner[f]
+        area = np.linalg.norm(g["face_Sf"][[f, nf + f, 2 * nf + f]])
+        if types is not None and types[f] == 1:
+            balance += bc[f] * area
+        else:
+            fc = g["face_centres"][[f, nf + f, 2 * nf + f]]
+            nc = m.cell_offsets.size - 1
+            cc = g["cell_centres"][[o, nc + o, 2 * nc + o]]
+            d = np.linalg.norm(fc - cc)
+            balance += diffusivity * area * (bc[f] - x[o]) / d
+    return balance
+
+
+N_CHAIN = 8
+
+
+def _chain_case(kind):
+    m = chain_mesh(N_CHAIN)
+    nf = m.owner.size
+    bc = np.full(nf, np.nan)
+    types = np.zeros(nf, np.int32)
+    if kind == "dirichlet":
+        bc[0], bc[1] = 0.0, 1.0
+    elif kind == "mixed":
+        bc[0], bc[1] = 0.0, 2.0
+        types[1] = 1
+    else:                                   # pure Neumann: every face a flux
+        types[:] = 1
+        bc[0], bc[1] = 0.0, 2.0
+    return m, bc, types, np.full(N_CHAIN, -2.0)
+
+
+@pytest.mark.parametrize("kind", ["dirichlet", "mixed", "neumann"])
+def test_chain_poisson_known_answers(kind):
+    m, bc, types, src = _chain_case(kind)
+    xc = co.geometry(m)["cell_centres"][:N_CHAIN]
+    dx = 1.0 / N_CHAIN
+    if kind == "neumann":
+        ref_value = xc[0] ** 2 + 3.0
+        x, rep = oracle_poisson_mixed(m, bc, src, types, tolerance=1e-12, ref_cell=0, ref_value=ref_value)
+        want = xc ** 2 + 3.0
+    else:
+        x, rep = oracle_poisson_mixed(m, bc, src, types, tolerance=1e-12)
+        want = xc ** 2 - dx * dx / 4.0
+    assert rep["status"] == 0
+    np.testing.assert_allclose(x, want, rtol=0, atol=1e-12)
+    assert abs(conservation_balance(m, bc, types, src, x)) <= 1e-12
+
+
+def test_chain_mesh_matches_reference_solver(ref):
+    """The same chain through the reference's own solve_poisson_mixed."""
+    for kind in ("dirichlet", "mixed"):
+        m, bc, types, src = _chain_case(kind)
+        x, rep = oracle_poisson_mixed(m, bc, src, types, tolerance=1e-12)
+        xr, rr = ref.solve_poisson_mixed(m, bc, src, types, tolerance=1e-12)
+        assert rep["iterations"] == rr["iterations"] and np.array_equal(x, xr)
+
+
+# ---------------------------------------------------------------- GMRES KATs
+def _csr(dense):
+    ro, cols, va = [0], [], []
+    for row in dense:
+        nz = np.nonzero(row)[0]
+        cols += nz.tolist()
+        va += row[nz].tolist()
+        ro.append(len(cols))
+    return np.array(ro), np.array(cols), np.array(va, float)
+
+
+def _poisson_1d(n):
+    return _csr(2 * np.eye(n) - np.eye(n, k=1) - np.eye(n, k=-1))
+
+
+def test_gmres_diagonal_and_1d_poisson():
+    ro, cols, va = _csr(np.diag([2.0, 3.0, 4.0]))
+    x, rep = co.solve_gmres(ro, cols, va, np.array([2.0, 6.0, 12.0]), None, tolerance=1e-12)
+    assert rep["status"] == 0 and rep["iterations"] > 0 and rep["residual_relative"] < 1e-10
+    np.testing.assert_allclose(x, [1.0, 2.0, 3.0], atol=1e-10)
+    ro, cols, va = _poisson_1d(5)
+    b = np.array([0.0, 1.0, 1.0, 1.0, 0.0])
+    x, rep = co.solve_gmres(ro, cols, va, b, None, tolerance=1e-12)
+    assert rep["status"] == 0 and rep["residual_relative"] < 1e-10
+    np.testing.assert_allclose(co.spmv(ro, cols, va, x), b, atol=1e-10)
+
+
+def test_gmres_already_converged_and_restarted():
+    ro, cols, va = _csr(np.eye(2))
+    x, rep = co.solve_gmres(ro, cols, va, np.zeros(2), None, tolerance=1e-12)
+    assert rep["status"] == 0 and rep["iterations"] == 0
+    ro, cols, va = _poisson_1d(10)
+    b = np.ones(10)
+    x, rep = co.solve_gmres(ro, cols, va, b, None, restart=5, tolerance=1e-12)
+    assert rep["status"] == 0 and rep["residual_relative"] < 1e-10
+    np.testing.assert_allclose(co.spmv(ro, cols, va, x), b, atol=1e-10)
+
+
+def test_gmres_exact_nonsymmetric_3x3():
+    A = np.array([[4.0, 1.0, 0.0], [-2.0, 5.0, 1.0], [1.0, -1.0, 3.0]])
+    ro, cols, va = _csr(A)
+    x_exact = np.array([1.0, -2.0, 0.5])
+    b = co.spmv(ro, cols, va, x_exact)
+    x, rep = co.solve_gmres(ro, cols, va, b, None, restart=3, max_iterations=20, tolerance=1e-12)
+    assert rep["status"] == 0 and rep["residual_relative"] < 1e-11
+    np.testing.assert_allclose(x, x_exact, atol=1e-10)
+    assert np.linalg.norm(A @ x - b) / np.linalg.norm(b) < 1e-9
+
+
+# ------------------------------------------------------------- AMG KATs
+def _levels(ro, cols, va):
+    amg = cg.NativeBoomerAMGPreconditioner()
+    assert amg.setup_host(ro, cols, va), amg.last_error()
+    return amg, [amg.export_level(l) for l in range(len(amg.hierarchy_level_sizes()))]
+
+
+def _dense(ro, cols, va, n_cols):
+    D = np.zeros((ro.size - 1, n_cols))
+    for i in range(ro.size - 1):
+        for k in range(ro[i], ro[i + 1]):
+            D[i, cols[k]] += va[k]
+    return D
+
+
+def test_small_multilevel_poisson_17():
+    amg, levels = _levels(*_poisson_1d(17))
+    assert len(levels) >= 2
+    lv = levels[0]
+    assert lv["p_columns"].size > 0
+    P = _dense(lv["p_offsets"], lv["p_columns"], lv["p_values"], levels[1]["inv_diag"].size)
+    assert np.max(np.abs(P.sum(axis=1) - 1.0)) < 1e-12
+
+
+@pytest.mark.parametrize("system", ["poisson_hex6", "pressure_tet5"])
+def test_transfer_gates(system):
+    if system == "poisson_hex6":
+        m, bc, src = cases.poisson_case(6)
+        ro, cols, va, _ = co.assemble_diffusion(m, bc, 1.0, src)
+    else:
+        m = cases.simple_mesh(5)
+        g = co.geometry(m)
+        U, rAU, aP, p, fixed, value = cases.simple_fields(m, g["cell_centres"])
+        a = co.simple_assemble(m, U, rAU, p, 1.0, fixed, value)
+        ro, cols, va = a["row_offsets"], a["columns"], a["values"]
+    amg, levels = _levels(ro, cols, va)
+    for l in range(len(levels) - 1):
+        f, c = levels[l], levels[l + 1]
+        nf, nc = f["inv_diag"].size, c["inv_diag"].size
+        A = _dense(f["row_offsets"], f["columns"], f["values"], nf)
+        P = _dense(f["p_offsets"], f["p_columns"], f["p_values"], nc)
+        Ac = _dense(c["row_offsets"], c["columns"], c["values"], nc)
+        galerkin = P.T @ A @ P
+        assert np.linalg.norm(Ac - galerkin) <= 1e-12 * np.linalg.norm(galerkin)
+        assert np.linalg.norm(Ac - Ac.T) <= 1e-12 * np.linalg.norm(Ac)
+        assert np.max(np.abs(P.sum(axis=1) - 1.0)) <= 1e-12
+        assert np.all(np.count_nonzero(P, axis=0) > 0)                 # no empty coarse column
+
+
+def test_stable_smoother_damping():
+    high = _csr(np.where(np.eye(3) > 0, 1.0, 0.9))                    # normalised Gershgorin bound 2.8
+    low = _csr(np.where(np.eye(3) > 0, 1.0, 0.1))
+    amg = cg.NativeBoomerAMGPreconditioner()
+    assert amg.setup_host(*high)
+    assert amg.omega == pytest.approx(1.8 / 2.8, abs=1e-14)
+    assert amg.update_values_host(*low)
+    assert amg.omega == pytest.approx(0.7, abs=1e-14)
+    assert amg.setup_host(*high)
+    assert amg.omega == pytest.approx(1.8 / 2.8, abs=1e-14)
