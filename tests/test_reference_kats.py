@@ -12,6 +12,11 @@ and expected values:
 * tests/unit/test_gmres_solver.cpp:125-233 -- the diagonal 3x3, the 1-D
   Poisson system, an already converged solve, a restarted solve and the exact
   nonsymmetric 3x3;
+* tests/validation/test_n9_s9_rhie_chow_consistency.cpp:324-422 -- the
+  Rhie-Chow face flux on channels of hex cells: invariant under a constant
+  pressure offset, and on a non-uniform channel under an affine pressure the
+  face-averaged gradient is exact and each internal face carries the linear
+  flux minus the pressure-jump response;
 * tests/validation/test_amg_preconditioner_qualification.cpp -- the small
   multilevel case (1-D Poisson, N = 17, :805-830), the transfer gates
   (Galerkin and symmetric coarse operators, unit row sums of P, no empty
@@ -28,14 +33,16 @@ from tests.test_poisson_driver import oracle_poisson_mixed
 
 
 # ------------------------------------------------------------ 1-D chain mesh
-def chain_mesh(n):
+def chain_mesh(n, nodes=None):
     """make_1d_chain (test_scalar_diffusion.cpp:12-71): n unit-section hex cells
     along x with their own 8 points each; faces: left end, right end, then per
-    cell y0, y1, z0, z1, then the n-1 internal faces."""
-    dx = 1.0 / n
+    cell y0, y1, z0, z1, then the n-1 internal faces.  ``nodes`` (n + 1 x
+    positions) replaces the uniform spacing on [0, 1]; patches are the left
+    end (0), the right end (1) and the side walls (2)."""
+    xs = np.linspace(0.0, 1.0, n + 1) if nodes is None else np.asarray(nodes, float)
     pts = []
     for i in range(n):
-        x0, x1 = dx * i, dx * (i + 1)
+        x0, x1 = (i / n, (i + 1) / n) if nodes is None else (xs[i], xs[i + 1])
         pts += [(x0, 0, 0), (x1, 0, 0), (x1, 1, 0), (x0, 1, 0), (x0, 0, 1), (x1, 0, 1), (x1, 1, 1), (x0, 1, 1)]
     pts = np.array(pts, float)
     faces, owner, neighbour, patch = [], [], [], []
@@ -132,6 +139,46 @@ def test_chain_mesh_matches_reference_solver(ref):
         x, rep = oracle_poisson_mixed(m, bc, src, types, tolerance=1e-12)
         xr, rr = ref.solve_poisson_mixed(m, bc, src, types, tolerance=1e-12)
         assert rep["iterations"] == rr["iterations"] and np.array_equal(x, xr)
+
+
+# ------------------------------------------------------------ Rhie-Chow KATs
+def test_rhie_chow_flux_pressure_offset_invariance():
+    m = chain_mesh(2)
+    nf = m.owner.size
+    U = np.zeros(6)
+    rAU = np.ones(6)
+    fixed, value = np.zeros(3, np.int32), np.zeros(3)            # zero-gradient pressure everywhere
+    phi0 = co.rhie_chow_flux(m, U, rAU, np.array([-2.0, 4.0]), 1.0, fixed, value)
+    phi1 = co.rhie_chow_flux(m, U, rAU, np.array([1002.0, 1008.0]), 1.0, fixed, value)
+    assert phi0.size == nf
+    np.testing.assert_allclose(phi0, phi1, rtol=0, atol=1e-12)
+
+
+def test_rhie_chow_flux_affine_pressure_nonuniform_channel():
+    nodes = [0.0, 0.5, 2.0, 4.0, 7.0]
+    m = chain_mesh(4, nodes)
+    g = co.geometry(m)
+    nc, nf = 4, m.owner.size
+    xc = g["cell_centres"][:nc]
+    U = np.concatenate([np.full(nc, 2.0), np.zeros(2 * nc)])
+    rAU = np.ones(3 * nc)
+    p = 1.0 + 2.0 * xc
+    fixed = np.array([1, 1, 0], np.int32)                          # inlet, outlet fixed; walls zero-gradient
+    value = np.array([1.0, 15.0, 0.0])
+    phi = co.rhie_chow_flux(m, U, rAU, p, 1.0, fixed, value)
+    grad = co.gauss_gradient(m, p, fixed, value)
+    vol = g["cell_volumes"]
+    internal = np.nonzero(m.neighbour >= 0)[0]
+    assert internal.size == 3
+    for f in internal:
+        o, n_ = m.owner[f], m.neighbour[f]
+        dau = 0.5 * (vol[o] * rAU[o] + vol[n_] * rAU[n_])
+        dx = xc[n_] - xc[o]
+        sfx = g["face_Sf"][f]
+        grad_face = 0.5 * (grad[o] + grad[n_])
+        assert grad_face == pytest.approx(2.0, abs=1e-12)
+        linear = 2.0 * sfx
+        assert phi[f] == pytest.approx(linear - dau * (p[n_] - p[o]) / dx * sfx, abs=1e-12)
 
 
 # ---------------------------------------------------------------- GMRES KATs
