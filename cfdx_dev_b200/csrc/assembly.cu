@@ -696,6 +696,7 @@ extern "C" int cfdxg_assemble_pressure_correction(cfdxg_context* ctx, cfdxg_mesh
                                                   double* grad_p) {
     if (!ctx || !m) return CFDXG_ERR_INVALID_ARGUMENT;
     CFDXG_GUARD_BEGIN
+    NvtxRange nvtx_range("cfdxg.assemble_pressure_correction");
     check_mem_flag(mem);
     require_geometry(m);
     if (!HbyA || !rAU || !p || !A_inout || !b) throw Error(CFDXG_ERR_INVALID_ARGUMENT, "missing argument");
@@ -745,6 +746,7 @@ extern "C" int cfdxg_rhie_chow_flux(cfdxg_context* ctx, cfdxg_mesh* m, const dou
                                     int32_t mem, double* flux) {
     if (!ctx || !m) return CFDXG_ERR_INVALID_ARGUMENT;
     CFDXG_GUARD_BEGIN
+    NvtxRange nvtx_range("cfdxg.rhie_chow_flux");
     check_mem_flag(mem);
     require_geometry(m);
     if (!HbyA || !rAU || !p || !flux) throw Error(CFDXG_ERR_INVALID_ARGUMENT, "missing argument");

@@ -409,6 +409,7 @@ extern "C" int cfdxg_amg_destroy(cfdxg_amg* amg) {
 extern "C" int cfdxg_amg_setup(cfdxg_context* ctx, cfdxg_amg* amg, const cfdxg_matrix* A) {
     if (!ctx || !amg) return CFDXG_ERR_INVALID_ARGUMENT;
     CFDXG_GUARD_BEGIN
+    NvtxRange nvtx_range("cfdxg.amg_setup");
     if (!A || A->n <= 0) {
         amg->error = "AMG setup requires a non-empty, square, finalized CSR matrix";
         throw Error(CFDXG_ERR_INVALID_ARGUMENT, amg->error);
@@ -422,6 +423,7 @@ extern "C" int cfdxg_amg_setup(cfdxg_context* ctx, cfdxg_amg* amg, const cfdxg_m
 extern "C" int cfdxg_amg_update_values(cfdxg_context* ctx, cfdxg_amg* amg, const cfdxg_matrix* A) {
     if (!ctx || !amg) return CFDXG_ERR_INVALID_ARGUMENT;
     CFDXG_GUARD_BEGIN
+    NvtxRange nvtx_range("cfdxg.amg_update_values");
     if (!amg->ready || !A) {
         amg->error = "native AMG numeric update requires an existing compatible hierarchy";
         throw Error(CFDXG_ERR_NOT_READY, amg->error);
@@ -487,6 +489,7 @@ extern "C" int cfdxg_amg_update_values_host(cfdxg_amg* amg, int64_t n, const int
 extern "C" int cfdxg_amg_apply(cfdxg_context* ctx, cfdxg_amg* amg, const double* r, double* z, int32_t mem) {
     if (!ctx || !amg) return CFDXG_ERR_INVALID_ARGUMENT;
     CFDXG_GUARD_BEGIN
+    NvtxRange nvtx_range("cfdxg.amg_apply");
     check_mem_flag(mem);
     if (!amg->ready || (!amg->d64 && !amg->d32)) {
         amg->error = "native AMG preconditioner has not been set up on the device";
@@ -820,6 +823,30 @@ int solve_scaled(cfdxg_context* ctx, const cfdxg_matrix* A, const double* rhs, d
     return status;
 }
 
+// CFDX_KRYLOV_DIAGNOSTICS, the reference's switch (core/linalg/krylov_diagnostics.h:25-41):
+// unset or "0" is off; any other value prints one summary line per solve on stderr.
+bool krylov_diagnostics() {
+    static const bool on = [] {
+        const char* e = std::getenv("CFDX_KRYLOV_DIAGNOSTICS");
+        return e && e[0] && std::string(e) != "0";
+    }();
+    return on;
+}
+
+void log_solve(const char* entry, const cfdxg_request& req, const KrylovResult& r, double physical,
+               const std::string& plan) {
+    if (!krylov_diagnostics()) return;
+    std::fprintf(stderr,
+                 "KRYLOV_SUMMARY entry=%s krylov=%s preconditioner=%s precision=%d status=%d iterations=%lld "
+                 "residual_relative=%.6e physical_residual_relative=%.6e replacements=%lld%s%s%s\n",
+                 entry, krylov_model_name(req.krylov),
+                 req.preconditioner == CFDXG_PC_OWN_DIAGONAL ? "own_diagonal"
+                                                             : preconditioner_model_name(req.preconditioner),
+                 req.precision, r.status, static_cast<long long>(r.iterations), r.residual_relative, physical,
+                 static_cast<long long>(r.residual_replacements), plan.empty() ? "" : " plan=\"",
+                 plan.c_str(), plan.empty() ? "" : "\"");
+}
+
 // measure_matrix_characteristics' symmetry and positive-diagonal test, on the device.
 bool symmetric_positive_diagonal(cfdxg_context* ctx, const cfdxg_matrix* A) {
     DevBuf<unsigned long long> max_bits(1);
@@ -844,6 +871,7 @@ extern "C" int cfdxg_solve_linear_system(cfdxg_context* ctx, const cfdxg_matrix*
                                          double tolerance, cfdxg_report* report) {
     if (!ctx) return CFDXG_ERR_INVALID_ARGUMENT;
     CFDXG_GUARD_BEGIN
+    NvtxRange nvtx_range("cfdxg.solve_linear_system");
     check_mem_flag(mem);
     if (!A || !rhs || !x) throw Error(CFDXG_ERR_INVALID_ARGUMENT, "missing argument");
     cfdxg_request req;
@@ -998,6 +1026,7 @@ extern "C" int cfdxg_solve_linear_system(cfdxg_context* ctx, const cfdxg_matrix*
         report->plan_krylov = req.krylov;
         report->plan_preconditioner = req.preconditioner;
     }
+    log_solve("solve_linear_system", req, r, physical, ctx->plan_reason);
     return r.status;
     CFDXG_GUARD_END(ctx)
 }
@@ -1007,6 +1036,7 @@ extern "C" int cfdxg_solve_gmres(cfdxg_context* ctx, const cfdxg_matrix* A, cfdx
                                  double tolerance, cfdxg_report* report) {
     if (!ctx) return CFDXG_ERR_INVALID_ARGUMENT;
     CFDXG_GUARD_BEGIN
+    NvtxRange nvtx_range("cfdxg.solve_gmres");
     check_mem_flag(mem);
     if (!A || !rhs || !x) throw Error(CFDXG_ERR_INVALID_ARGUMENT, "missing argument");
     cfdxg_request req;
@@ -1037,6 +1067,7 @@ extern "C" int cfdxg_solve_gmres(cfdxg_context* ctx, const cfdxg_matrix* A, cfdx
         report->plan_krylov = req.krylov;
         report->plan_preconditioner = amg ? CFDXG_PC_NATIVE_AMG : CFDXG_PC_NONE;
     }
+    log_solve("solve_gmres", req, r, r.residual_relative, std::string());
     return r.status;
     CFDXG_GUARD_END(ctx)
 }

@@ -2,6 +2,7 @@
 // buffers, launch accounting and deterministic block reductions.
 #pragma once
 #include <cuda_runtime.h>
+#include <nvtx3/nvToolsExt.h>
 
 #include <cstdint>
 #include <cstdio>
@@ -117,6 +118,16 @@ struct cfdxg_context {
 };
 
 namespace cfdxg {
+
+// NVTX range over one library call: phases show up by name in Nsight
+// timelines and can filter ncu captures; without a tool attached the calls do
+// nothing.
+struct NvtxRange {
+    explicit NvtxRange(const char* name) { nvtxRangePushA(name); }
+    ~NvtxRange() { nvtxRangePop(); }
+    NvtxRange(const NvtxRange&) = delete;
+    NvtxRange& operator=(const NvtxRange&) = delete;
+};
 
 inline void count_launch(cfdxg_context* ctx, int64_t n = 1) { ctx->launches += n; }
 

@@ -1013,6 +1013,7 @@ extern "C" int cfdxg_mpnn_set_vcycle(cfdxg_context* ctx, cfdxg_mpnn* net, cfdxg_
 extern "C" int cfdxg_mpnn_apply(cfdxg_context* ctx, cfdxg_mpnn* net, const double* r, double* y, int32_t mem) {
     if (!ctx || !net || !r || !y) return CFDXG_ERR_INVALID_ARGUMENT;
     CFDXG_GUARD_BEGIN
+    NvtxRange nvtx_range("cfdxg.mpnn_apply");
     check_mem_flag(mem);
     require_bound(net);
     In<double> rin(ctx, r, net->n, mem);
