@@ -1,0 +1,33 @@
+"""The replay tool on a B200: the reference-written golden capture replays
+with every candidate this library provides to the capture's tolerance on the
+FP64 true residual, the automatic plan is CG, and models outside the library
+are reported as not applicable.  The automatic candidate's iteration count is
+the reference's own replay of the same file (oracle/_ref, where built)."""
+import numpy as np
+import pytest
+
+import cfdx_dev_b200 as cg
+from cfdx_dev_b200 import replay
+from tests import cases
+
+pytestmark = pytest.mark.gpu
+
+GOLDEN = cases.ROOT / "tests" / "golden" / "pressure_tet4.cfdxlin"
+
+
+def test_golden_capture_replays(ctx):
+    rows, passed = replay.replay(GOLDEN, ["auto", "jacobi", "native", "none", "ilu0"], ctx=ctx)
+    assert not passed                                   # ilu0 is not provided here
+    by_name = {r.split(",")[0]: r.split(",") for r in rows}
+    for name in ("auto", "jacobi", "native", "none"):
+        row = by_name[name]
+        assert row[1] == "cg" and row[2] == "converged", row
+        assert float(row[6]) <= 1e-8
+    assert by_name["ilu0"][2] == "not_applicable"
+    from oracle import ref
+    if ref.available():
+        c = cg.read_linear_system_capture(GOLDEN)
+        _, rr = ref.solve_linear_system(c["row_offsets"], c["columns"], c["values"], c["rhs"], krylov=0,
+                                        preconditioner=0, restart=40, max_iterations=int(c["max_iterations"]),
+                                        tolerance=float(c["tolerance"]))
+        assert int(by_name["auto"][3]) == rr["iterations"]
