@@ -213,3 +213,27 @@ def test_symmetric_diagonal_scaling_gives_a_unit_diagonal():
     assert c["numerically_symmetric"] and c["positive_diagonal"]
     with pytest.raises(CfdxgError):
         cg.scale_matrix(ro, co_, va, "row", zero_tolerance=-1.0)
+
+
+# ---------------------------------------------- tests/unit/test_matrix_characteristics.cpp
+def test_reference_case_coupled_dispatch():
+    c = cg.measure_matrix_characteristics([0, 2, 5, 7], [0, 1, 0, 1, 2, 1, 2], [4.0, -1.0, -1.0, 4.0, -1.0, -1.0, 4.0],
+                                          saddle_point=True)
+    assert c["square"] and c["saddle_point"] and c["numerically_symmetric"] and c["diagonally_dominant"]
+    assert abs(c["average_nnz_per_row"] - 7.0 / 3.0) < 1e-14
+    plan = cg.select_linear_solver("coupled_pressure_velocity", c)
+    assert (plan["krylov"], plan["preconditioner"]) == ("fgmres", "coupled_block_schur")
+
+
+def test_reference_case_nonsymmetry_and_scaling():
+    c = cg.measure_matrix_characteristics([0, 2, 4], [0, 1, 0, 1], [1.0e9, 1.0, 0.5, 1.0e-2])
+    assert c["square"] and not c["numerically_symmetric"] and c["strongly_scaled"]
+    assert c["coefficient_range"] > 1.0e10
+
+
+def test_reference_case_diagonal_dynamic_range_avoids_cg_amg():
+    c = cg.measure_matrix_characteristics([0, 2, 4], [0, 1, 0, 1], [1.0e5, -1.0e-1, -1.0e-1, 1.0])
+    assert c["numerically_symmetric"] and c["diagonally_dominant"] and c["large_diagonal_dynamic_range"]
+    assert not c["strongly_scaled"]
+    plan = cg.select_linear_solver("pressure_poisson", c)
+    assert (plan["krylov"], plan["preconditioner"]) == ("gmres", "jacobi")
