@@ -44,13 +44,15 @@ class OraclePart:
 
     device = torch.device("cpu")
 
-    def __init__(self, layout, values):
+    def __init__(self, layout, values, block_amg=True):
         self.layout = layout
         self.lv = np.ascontiguousarray(values[layout.local_source])
-        bv = np.ascontiguousarray(values[layout.block_source])
-        amg = NativeBoomerAMGPreconditioner()
-        assert amg.setup_host(layout.block_row_offsets, layout.block_columns, bv), amg.last_error()
-        self.H = co.Hierarchy([amg.export_level(l) for l in range(len(amg.hierarchy_level_sizes()))], amg.omega)
+        if block_amg:
+            bv = np.ascontiguousarray(values[layout.block_source])
+            amg = NativeBoomerAMGPreconditioner()
+            assert amg.setup_host(layout.block_row_offsets, layout.block_columns, bv), amg.last_error()
+            self.H = co.Hierarchy([amg.export_level(l) for l in range(len(amg.hierarchy_level_sizes()))],
+                                  amg.omega)
 
     def matvec(self, x_local):
         y = co.spmv(self.layout.local_row_offsets, self.layout.local_columns, self.lv, x_local.numpy())
@@ -322,10 +324,7 @@ def test_fgmres_with_the_distributed_vcycle_keeps_the_iteration_count():
     for parts in (1, 2, 4, 7):
         comm = domain.PartComm(parts)
         plan, dm, _, _ = _distributed_amg(ro, co_, va, parts, comm, 64, (levels, omega))
-        local = {p: OraclePart.__new__(OraclePart) for p in comm.local_parts}
-        for p in local:
-            local[p].layout = plan.part(p)
-            local[p].lv = np.ascontiguousarray(va[local[p].layout.local_source])
+        local = {p: OraclePart(plan.part(p), va, block_amg=False) for p in comm.local_parts}
         solver = domain.DistributedFGMRES(comm, local, restart=30, preconditioner=dm)
         x, rep = solver.solve(domain.split_rows(plan, comm, b), tolerance=1e-8)
         xg = np.concatenate([x[p] for p in range(parts)])
@@ -353,10 +352,7 @@ def _rank_vcycle(rank, world, port, parts, out):
              for p in comm.local_parts}
         dm.apply({p: torch.from_numpy(r[plan.row_splits[p]:plan.row_splits[p + 1]].copy())
                   for p in comm.local_parts}, z)
-        local = {p: OraclePart.__new__(OraclePart) for p in comm.local_parts}
-        for p in local:
-            local[p].layout = plan.part(p)
-            local[p].lv = np.ascontiguousarray(va[local[p].layout.local_source])
+        local = {p: OraclePart(plan.part(p), va, block_amg=False) for p in comm.local_parts}
         x, rep = domain.DistributedFGMRES(comm, local, preconditioner=dm).solve(domain.split_rows(plan, comm, b),
                                                                                tolerance=1e-8)
         out.put((rank, {p: v.numpy() for p, v in z.items()}, x, rep["iterations"]))
