@@ -13,6 +13,7 @@ from .api import (  # noqa: F401
     Mesh,
     NativeBoomerAMGPreconditioner,
     ReferenceCellGauge,
+    ReusablePreconditionerContext,
     SparseMatrix,
     assemble_cell_diffusion_matrix,
     assemble_pressure_correction,

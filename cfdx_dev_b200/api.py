@@ -508,6 +508,67 @@ class NativeBoomerAMGPreconditioner:
             pass
 
 
+class ReusablePreconditionerContext:
+    """ReusablePreconditionerContext (core/linalg/linear_solver_context.h:15-65):
+    owns the lifecycle of one preconditioner across a sequence of matrices --
+    a full setup when the CSR structure changed, the numeric refresh when only
+    the values changed (a full setup again if the refresh is refused), nothing
+    when the matrix is unchanged -- with the reference's statistics
+    (full_setups, numeric_updates, unchanged_reuses, solves).
+
+    ``prepare`` takes a device ``SparseMatrix`` (device setup and refresh) or
+    host CSR arrays ``(row_offsets, columns, values)`` (host setup and refresh).
+    The comparison is against a snapshot of the last prepared matrix, as the
+    reference keeps one."""
+
+    def __init__(self, preconditioner: NativeBoomerAMGPreconditioner):
+        self.pc = preconditioner
+        self.stats = dict(full_setups=0, numeric_updates=0, unchanged_reuses=0, solves=0)
+        self._snapshot = None
+
+    def invalidate(self):
+        self._snapshot = None
+
+    def prepare(self, A) -> bool:
+        if isinstance(A, SparseMatrix):
+            ro, co, va = A.to_csr()
+            setup, update = (lambda: self.pc.setup(A)), (lambda: self.pc.update_values(A))
+        else:
+            ro, co, va = (np.ascontiguousarray(A[0], np.int64), np.ascontiguousarray(A[1], np.int64),
+                          np.ascontiguousarray(A[2], np.float64))
+            setup, update = (lambda: self.pc.setup_host(ro, co, va)), (lambda: self.pc.update_values_host(ro, co, va))
+        if ro.size < 2 or ro[-1] != co.size or co.size != va.size or not np.all(np.isfinite(va)):
+            return False
+        snap = self._snapshot
+        same_structure = snap is not None and np.array_equal(snap[0], ro) and np.array_equal(snap[1], co)
+        same_values = same_structure and np.array_equal(snap[2], va)
+        if not same_structure:
+            ready = setup()
+            self.stats["full_setups"] += int(ready)
+        elif not same_values:
+            ready = update()
+            if ready:
+                self.stats["numeric_updates"] += 1
+            else:                              # a refused refresh rebuilds from the current matrix
+                ready = setup()
+                self.stats["full_setups"] += int(ready)
+        else:
+            ready = True
+            self.stats["unchanged_reuses"] += 1
+        if not ready:
+            self.invalidate()
+            return False
+        self._snapshot = (ro.copy(), co.copy(), va.copy())
+        return True
+
+    def solve(self, A: SparseMatrix, rhs, x0=None, **kw):
+        """prepare(A), then the prepared solve (solve_gmres; krylov="cg" for CG) -> (x, report)."""
+        if not self.prepare(A):
+            raise CfdxgError(N.CFDXG_ERR_SETUP, f"preconditioner preparation failed: {self.pc.last_error()}")
+        self.stats["solves"] += 1
+        return solve_gmres(A, rhs, x0=x0, amg=self.pc, **kw)
+
+
 def make_request(krylov="gmres", preconditioner="native_amg", restart=40, precision="fp64", learned=None,
                  problem="pressure_poisson", scaling="none", **kw):
     """A cfdxg_request; krylov / preconditioner "auto" select the plan from the measured matrix."""

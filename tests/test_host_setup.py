@@ -161,3 +161,30 @@ def test_host_numeric_refresh_matches_reference(ref):
     assert not amg.update_values_host(ro, np.roll(co_, 1), va2)
     assert "pattern" in amg.last_error()
     assert np.array_equal(amg.export_level(1)["values"], before)
+
+
+def test_reusable_context_lifecycle_on_the_host():
+    """linear_solver_context.h:30-65: structure change -> setup, value change ->
+    refresh, unchanged -> reuse; a refused refresh rebuilds."""
+    import cfdx_dev_b200 as cg
+    from tests import cases
+    from oracle import cfdx_oracle as co_
+    m = cases.simple_mesh(4)
+    g = co_.geometry(m)
+    U, rAU, aP, p, fixed, value = cases.simple_fields(m, g["cell_centres"])
+    a = co_.simple_assemble(m, U, rAU, p, 1.0, fixed, value)
+    ro, co, va = a["row_offsets"], a["columns"], a["values"]
+    ctx = cg.ReusablePreconditionerContext(cg.NativeBoomerAMGPreconditioner())
+    assert ctx.prepare((ro, co, va))
+    assert ctx.prepare((ro, co, va))
+    assert ctx.prepare((ro, co, va * 1.5))                 # same pattern, new values
+    assert ctx.stats == dict(full_setups=1, numeric_updates=1, unchanged_reuses=1, solves=0)
+    # a different structure (one coupling dropped symmetrically) sets up again
+    rows = np.repeat(np.arange(ro.size - 1), np.diff(ro))
+    drop = np.nonzero((rows != co) & (((rows == 0) & (co == co[ro[0]:ro[1]][-1])) |
+                                      ((co == 0) & (rows == co[ro[0]:ro[1]][-1]))))[0]
+    keep = np.setdiff1d(np.arange(co.size), drop)
+    ro2 = np.concatenate([[0], np.cumsum(np.bincount(rows[keep], minlength=ro.size - 1))])
+    assert ctx.prepare((ro2, co[keep], va[keep]))
+    assert ctx.stats["full_setups"] == 2
+    assert not ctx.prepare((ro, co, np.where(np.arange(va.size) == 3, np.nan, va)))   # rejected input
