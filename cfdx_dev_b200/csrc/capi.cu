@@ -792,8 +792,10 @@ int solve_scaled(cfdxg_context* ctx, const cfdxg_matrix* A, const double* rhs, d
     inner.scaling = CFDXG_SCALING_NONE;
     cfdxg_report rin{};
     const double t0 = now_seconds();
+    const std::string plan = ctx->plan_reason;      // the inner, explicit solve draws no plan
     rc = cfdxg_solve_linear_system(ctx, As, bs.data(), xs.data(), CFDXG_MEM_HOST, &inner, max_iterations,
                                    0.1 * tolerance, &rin);
+    ctx->plan_reason = plan;
     if (rc < 0) return rc;
     std::vector<double> xr(n);
     for (int64_t i = 0; i < n; ++i) xr[i] = cs[i] * xs[i];
