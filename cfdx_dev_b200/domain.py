@@ -530,7 +530,8 @@ class DistributedAMG:
         L = len(levels)
         n = [int(lv["inv_diag"].size) for lv in levels]
         parts = comm.parts
-        dist = [True]
+        # a one-level hierarchy of at most 16 rows is the dense coarsest solve: replicated
+        dist = [not (L == 1 and n[0] <= 16)]
         for l in range(1, L):
             dist.append(dist[-1] and n[l] >= max(replicate_below, 2 * parts) and not (l == L - 1 and n[l] <= 16))
         self.L, self.n, self.dist = L, n, dist
@@ -596,6 +597,12 @@ class DistributedAMG:
     # ---------------------------------------------------------------- cycle
     def apply(self, r: dict, z: dict) -> None:
         """z = V-cycle(r) for every local part (owned pieces of the finest level)."""
+        if not self.dist[0]:
+            S = self.splits[0]
+            x = self._cycle_full(0, self.comm.allgather(r, S, self.n[0]))
+            for p in z:
+                z[p].copy_(x[int(S[p]):int(S[p + 1])])
+            return
         x = self._cycle_split(0, r)
         for p in z:
             z[p].copy_(x[p])

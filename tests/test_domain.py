@@ -384,3 +384,23 @@ def test_gloo_ranks_run_the_distributed_vcycle():
     assert results[0][3] == results[1][3]
     xg = np.concatenate([x[p] for p in range(parts)])
     assert np.linalg.norm(b - co.spmv(ro, co_, va, xg)) <= 1e-8 * np.linalg.norm(b)
+
+
+def test_one_level_hierarchy_uses_the_dense_coarsest_solve():
+    # 12 rows: the setup stops at one level, whose V-cycle is the pivoted dense solve
+    n = 12
+    D = 2.0 * np.eye(n) - 0.9 * np.eye(n, k=1) - 0.9 * np.eye(n, k=-1)
+    D[0, 0] += 1.0
+    ro = np.concatenate([[0], np.cumsum(np.count_nonzero(D, axis=1))])
+    co_ = np.nonzero(D)[1]
+    va = D[np.nonzero(D)]
+    levels, omega = _hierarchy(ro, co_, va)
+    assert len(levels) == 1
+    plan, dm, _, _ = _distributed_amg(ro, co_, va, 3, domain.PartComm(3), 4096, (levels, omega))
+    r = np.random.default_rng(1).standard_normal(n)
+    S = plan.row_splits
+    z = {p: torch.empty(int(S[p + 1] - S[p]), dtype=torch.float64) for p in range(3)}
+    dm.apply({p: torch.from_numpy(r[S[p]:S[p + 1]].copy()) for p in range(3)}, z)
+    got = np.concatenate([z[p].numpy() for p in range(3)])
+    assert np.array_equal(got, co.Hierarchy(levels, omega).apply(r))
+    np.testing.assert_allclose(D @ got, r, rtol=0, atol=1e-12)
