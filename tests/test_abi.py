@@ -33,3 +33,20 @@ def test_host_only_calls_need_no_device():
     assert m.n_cells == 27 and m.n_faces == 108
     amg = cg.NativeBoomerAMGPreconditioner(None)
     assert amg.name() == "NativeBoomerStyleAMG"
+
+
+def test_header_is_plain_c_and_links_from_c(tmp_path):
+    """include/cfdxg.h is a C header (C99, no warnings under -Wall -Wextra
+    -pedantic) and a C program links against libcfdxg.so and calls a host-only
+    entry point."""
+    import subprocess
+    from tests.conftest import ROOT
+    src = tmp_path / "abi.c"
+    src.write_text('#include "cfdxg.h"\n'
+                   "int main(void) { cfdxg_request r; cfdxg_request_default(&r);\n"
+                   "  return r.krylov == CFDXG_KRYLOV_GMRES && r.problem == CFDXG_PROBLEM_PRESSURE_POISSON ? 0 : 1; }\n")
+    lib_dir = ROOT / "cfdx_dev_b200" / "_lib"
+    exe = tmp_path / "abi"
+    subprocess.run(["gcc", "-std=c99", "-Wall", "-Wextra", "-pedantic", "-Werror", f"-I{ROOT / 'include'}", str(src),
+                    f"-L{lib_dir}", "-lcfdxg", f"-Wl,-rpath,{lib_dir}", "-o", str(exe)], check=True)
+    assert subprocess.run([str(exe)]).returncode == 0
