@@ -3,7 +3,9 @@
 Unstructured finite-volume pressure-correction assembly and Rhie-Chow face
 fluxes, plus the native-AMG-preconditioned GMRES/FGMRES solve, as sm_100a
 CUDA kernels behind a C ABI (include/cfdxg.h).  See ``api`` for the
-reference-shaped Python entry points.
+reference-shaped Python entry points, ``domain`` for one system split over
+several GPUs, ``replay`` for replaying captured systems and ``train_mpnn`` for
+training the learned stage.
 """
 from .api import (  # noqa: F401
     CfdxgError,
