@@ -23,6 +23,7 @@ from .api import (  # noqa: F401
     fourier_field,
     gauss_gradient_with_boundary,
     hex_case,
+    diagnose_matrix,
     make_request,
     measure_matrix_characteristics,
     make_rhie_chow_mass_flux,

@@ -112,6 +112,22 @@ class MatrixCharacteristics(C.Structure):
         return {name: getattr(self, name) for name, _ in self._fields_}
 
 
+DIAG_COUNTS = ("empty_rows", "empty_columns", "missing_diagonal", "near_zero_diagonal", "isolated_dofs",
+               "duplicate_entries")
+DIAG_VALUES = ("max_abs_value", "min_nonzero_abs_value", "max_row_sum", "min_nonzero_row_sum", "max_column_sum",
+               "min_nonzero_column_sum", "max_abs_diagonal", "min_nonzero_abs_diagonal", "diagonal_dynamic_range",
+               "row_sum_dynamic_range", "column_sum_dynamic_range", "minimum_gershgorin_margin")
+
+
+class MatrixDiagnostics(C.Structure):
+    _fields_ = ([("rows", C.c_int64), ("columns", C.c_int64), ("nnz", C.c_int64), ("finite", C.c_int32),
+                 ("structurally_consistent", C.c_int32)] + [(k, C.c_int64) for k in DIAG_COUNTS] +
+                [(k, C.c_double) for k in DIAG_VALUES] + [("connected_components", C.c_int64)])
+
+    def as_dict(self) -> dict:
+        return {name: getattr(self, name) for name, _ in self._fields_}
+
+
 class PlanRequest(C.Structure):
     _fields_ = [("krylov", C.c_int32), ("preconditioner", C.c_int32), ("gmres_restart", C.c_int32),
                 ("null_space", C.c_int32), ("scaling", C.c_int32), ("braess_sarazin_alpha", C.c_double)]
@@ -225,6 +241,8 @@ PROTOTYPES = {
     "cfdxg_select_linear_solver": (C.c_int, [C.c_int32, _P(MatrixCharacteristics), _P(PlanRequest),
                                             _P(SolverPlan)]),
     "cfdxg_plan_last_error": (C.c_char_p, []),
+    "cfdxg_diagnose_matrix": (C.c_int, [C.c_int64, C.c_int64, _V, _V, _V, C.c_double, C.c_int32,
+                                        _P(MatrixDiagnostics)]),
     "cfdxg_scale_matrix": (C.c_int, [C.c_int64, _V, _V, _V, C.c_int32, C.c_double, _V, _V, _V, _V]),
     "cfdxg_plan_reason": (C.c_char_p, [_V]),
     "cfdxg_domain_plan_create": (C.c_int, [C.c_int64, _V, _V, C.c_int32, _V, _P(_V)]),

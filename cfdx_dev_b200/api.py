@@ -600,6 +600,20 @@ def measure_matrix_characteristics(row_offsets, columns, values, saddle_point=Fa
     return c.as_dict()
 
 
+def diagnose_matrix(row_offsets, columns, values, n_cols=None, diagonal_relative_tolerance=1e-14,
+                    include_topology=True) -> dict:
+    """core/linalg/matrix_diagnostics.h:126 diagnose_matrix on the host (MatrixDiagnostics fields)."""
+    lib = N.load()
+    ro, co, va = _i64(row_offsets), _i64(columns), _f64(values)
+    n = ro.size - 1
+    d = N.MatrixDiagnostics()
+    rc = lib.cfdxg_diagnose_matrix(n, n if n_cols is None else int(n_cols), N.ptr(ro), N.ptr(co), N.ptr(va),
+                                   float(diagonal_relative_tolerance), int(bool(include_topology)), C.byref(d))
+    if rc != 0:
+        raise CfdxgError(rc, lib.cfdxg_plan_last_error().decode())
+    return d.as_dict()
+
+
 def scale_matrix(row_offsets, columns, values, scaling: str, zero_tolerance=0.0):
     """core/linalg/matrix_diagnostics.h:410 scale_matrix on the host -> dict of the
     row and column scales, the scaled values (same pattern) and the zero counts."""

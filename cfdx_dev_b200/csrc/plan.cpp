@@ -11,6 +11,7 @@
 
 #include <cstdio>
 #include <cstring>
+#include <limits>
 #include <vector>
 
 namespace cfdxg {
@@ -237,6 +238,119 @@ int cfdxg_scale_matrix(int64_t n, const int64_t* ro, const int64_t* co, const do
     if (zero_counts) {
         zero_counts[0] = zr;
         zero_counts[1] = zc;
+    }
+    g_plan_error.clear();
+    return CFDXG_OK;
+}
+
+int cfdxg_diagnose_matrix(int64_t nr, int64_t nc, const int64_t* ro, const int64_t* co, const double* va,
+                          double tol, int32_t topology, cfdxg_matrix_diagnostics* d) {
+    if (!d || !ro || nr < 0 || nc < 0 || (nr > 0 && ro[nr] > 0 && (!co || !va))) {
+        g_plan_error = "diagnosis: null argument";
+        return CFDXG_ERR_INVALID_ARGUMENT;
+    }
+    if (!(tol >= 0.0) || !std::isfinite(tol)) {
+        g_plan_error = "diagnosis: the diagonal tolerance must be finite and non-negative";
+        return CFDXG_ERR_INVALID_ARGUMENT;
+    }
+    const double inf = std::numeric_limits<double>::infinity();
+    *d = cfdxg_matrix_diagnostics{};
+    d->rows = nr;
+    d->columns = nc;
+    d->nnz = ro[nr];
+    d->finite = 1;
+    d->min_nonzero_abs_value = d->min_nonzero_row_sum = d->min_nonzero_column_sum = inf;
+    d->min_nonzero_abs_diagonal = inf;
+    d->diagonal_dynamic_range = d->row_sum_dynamic_range = d->column_sum_dynamic_range = 1.0;
+    d->minimum_gershgorin_margin = inf;
+    // SparseMatrix::is_consistent (sparse_matrix.h:256-275)
+    bool consistent = ro[0] == 0;
+    for (int64_t i = 0; i < nr && consistent; ++i) {
+        if (ro[i + 1] < ro[i]) consistent = false;
+        for (int64_t k = ro[i]; k < ro[i + 1] && consistent; ++k)
+            if (co[k] < 0 || co[k] >= nc || !std::isfinite(va[k]) || (k > ro[i] && co[k] <= co[k - 1]))
+                consistent = false;
+    }
+    d->structurally_consistent = consistent;
+    if (!consistent) {
+        d->finite = 0;
+        g_plan_error.clear();
+        return CFDXG_OK;
+    }
+    std::vector<double> row_sum(static_cast<size_t>(nr), 0.0), col_sum(static_cast<size_t>(nc), 0.0);
+    std::vector<char> row_off(static_cast<size_t>(nr), 0), col_off(static_cast<size_t>(nc), 0);
+    for (int64_t i = 0; i < nr; ++i) {
+        if (ro[i] == ro[i + 1]) ++d->empty_rows;
+        bool present = false;
+        double diagonal = 0.0;
+        for (int64_t k = ro[i]; k < ro[i + 1]; ++k) {
+            const int64_t j = co[k];
+            const double m = std::fabs(va[k]);
+            d->max_abs_value = cfdxg::ref_max(d->max_abs_value, m);
+            if (m > 0.0) d->min_nonzero_abs_value = cfdxg::ref_min(d->min_nonzero_abs_value, m);
+            row_sum[i] += m;
+            col_sum[j] += m;
+            if (j == i) {
+                present = true;
+                diagonal += va[k];
+            } else if (m > 0.0) {
+                row_off[i] = 1;
+                col_off[j] = 1;
+            }
+        }
+        if (!present && i < nc) ++d->missing_diagonal;
+        const double dabs = std::fabs(diagonal);
+        if (dabs > 0.0) {
+            d->max_abs_diagonal = cfdxg::ref_max(d->max_abs_diagonal, dabs);
+            d->min_nonzero_abs_diagonal = cfdxg::ref_min(d->min_nonzero_abs_diagonal, dabs);
+        }
+        // against the running max |a| over the rows so far, as the reference's loop has it
+        if (i < nc && dabs <= tol * cfdxg::ref_max(1.0, d->max_abs_value)) ++d->near_zero_diagonal;
+        if (i < nc) {
+            double off = 0.0;
+            for (int64_t k = ro[i]; k < ro[i + 1]; ++k)
+                if (co[k] != i) off += std::fabs(va[k]);
+            d->minimum_gershgorin_margin = cfdxg::ref_min(d->minimum_gershgorin_margin, dabs - off);
+        }
+    }
+    for (int64_t j = 0; j < nc; ++j)
+        if (col_sum[j] == 0.0) ++d->empty_columns;
+    for (int64_t i = 0; i < std::min(nr, nc); ++i)
+        if (!row_off[i] && !col_off[i]) ++d->isolated_dofs;
+    for (const double v : row_sum)
+        if (v > 0.0) {
+            d->max_row_sum = cfdxg::ref_max(d->max_row_sum, v);
+            d->min_nonzero_row_sum = cfdxg::ref_min(d->min_nonzero_row_sum, v);
+        }
+    for (const double v : col_sum)
+        if (v > 0.0) {
+            d->max_column_sum = cfdxg::ref_max(d->max_column_sum, v);
+            d->min_nonzero_column_sum = cfdxg::ref_min(d->min_nonzero_column_sum, v);
+        }
+    if (d->min_nonzero_abs_diagonal < inf) d->diagonal_dynamic_range = d->max_abs_diagonal / d->min_nonzero_abs_diagonal;
+    if (d->min_nonzero_row_sum < inf) d->row_sum_dynamic_range = d->max_row_sum / d->min_nonzero_row_sum;
+    if (d->min_nonzero_column_sum < inf)
+        d->column_sum_dynamic_range = d->max_column_sum / d->min_nonzero_column_sum;
+    if (nr != nc) d->minimum_gershgorin_margin = std::numeric_limits<double>::quiet_NaN();
+    if (topology) {
+        // components of the bipartite graph (row nodes, then column nodes), nonzero entries as edges
+        std::vector<int64_t> parent(static_cast<size_t>(nr + nc));
+        for (int64_t v = 0; v < nr + nc; ++v) parent[v] = v;
+        auto find = [&](int64_t v) {
+            while (parent[v] != v) v = parent[v] = parent[parent[v]];
+            return v;
+        };
+        int64_t components = nr + nc;
+        for (int64_t i = 0; i < nr; ++i)
+            for (int64_t k = ro[i]; k < ro[i + 1]; ++k) {
+                if (std::fabs(va[k]) == 0.0) continue;
+                const int64_t a = find(i), b = find(nr + co[k]);
+                if (a != b) {
+                    parent[a] = b;
+                    --components;
+                }
+            }
+        d->connected_components = components;
     }
     g_plan_error.clear();
     return CFDXG_OK;

@@ -26,7 +26,8 @@ import time
 import numpy as np
 
 from . import _native as N
-from .api import (CfdxgError, Context, SparseMatrix, read_linear_system_capture, solve_linear_system)
+from .api import (CfdxgError, Context, SparseMatrix, diagnose_matrix, read_linear_system_capture,
+                  solve_linear_system)
 
 CANDIDATES = {"auto": "auto", "jacobi": "jacobi", "native": "native_amg", "none": "none"}
 NOT_PROVIDED = ("ilu0", "directional", "energy")
@@ -34,20 +35,11 @@ HEADER = "preconditioner,krylov,status,iterations,total_ms,true_abs_l2,true_rela
 
 
 def diagnosis(c: dict) -> str:
-    """The reference tool's CSR line: rows, nnz, missing and near-zero diagonals
-    (|a_ii| <= 1e-14 max(1, max|a|), diagnose_matrix's default), checksum."""
-    ro, co, va = c["row_offsets"], c["columns"], c["values"]
-    n = ro.size - 1
-    rows = np.repeat(np.arange(n), np.diff(ro))
-    on_diag = rows == co
-    present = np.zeros(n, bool)
-    present[rows[on_diag]] = True
-    diag = np.zeros(n)
-    np.add.at(diag, rows[on_diag], va[on_diag])
-    scale = max(1.0, float(np.max(np.abs(va))) if va.size else 0.0)
-    near_zero = int(np.count_nonzero(np.abs(diag) <= 1e-14 * scale))
-    return (f"CSR rows={n} nnz={va.size} missing_diagonal={int(n - present.sum())} "
-            f"near_zero_diagonal={near_zero} checksum={c['checksum']:x}")
+    """The reference tool's CSR line from diagnose_matrix (rows, nnz, missing and
+    near-zero diagonals) and the capture's checksum."""
+    d = diagnose_matrix(c["row_offsets"], c["columns"], c["values"])
+    return (f"CSR rows={d['rows']} nnz={d['nnz']} missing_diagonal={d['missing_diagonal']} "
+            f"near_zero_diagonal={d['near_zero_diagonal']} checksum={c['checksum']:x}")
 
 
 def _true_residual(ro, co, va, x, b):

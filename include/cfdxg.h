@@ -472,6 +472,26 @@ const char* cfdxg_plan_last_error(void);
 int cfdxg_scale_matrix(int64_t n, const int64_t* row_offsets, const int64_t* columns, const double* values,
                        int32_t scaling, double zero_tolerance, double* row_scale, double* column_scale,
                        double* scaled_values, int64_t* zero_counts);
+/* diagnose_matrix (core/linalg/matrix_diagnostics.h:126-280) of an n_rows x
+ * n_cols CSR matrix: counts and coefficient ranges as the reference's
+ * MatrixDiagnostics (:23-59).  A matrix that is not consistent (offsets,
+ * columns in range and strictly increasing, finite values) returns with
+ * structurally_consistent = finite = 0 and the other fields at their
+ * defaults, as the reference does. */
+typedef struct {
+    int64_t rows, columns, nnz;
+    int32_t finite, structurally_consistent;
+    int64_t empty_rows, empty_columns, missing_diagonal, near_zero_diagonal, isolated_dofs, duplicate_entries;
+    double max_abs_value, min_nonzero_abs_value;
+    double max_row_sum, min_nonzero_row_sum, max_column_sum, min_nonzero_column_sum;
+    double max_abs_diagonal, min_nonzero_abs_diagonal;
+    double diagonal_dynamic_range, row_sum_dynamic_range, column_sum_dynamic_range;
+    double minimum_gershgorin_margin;   /* NaN for a rectangular matrix */
+    int64_t connected_components;       /* of the bipartite row/column graph; 0 without topology */
+} cfdxg_matrix_diagnostics;
+int cfdxg_diagnose_matrix(int64_t n_rows, int64_t n_cols, const int64_t* row_offsets, const int64_t* columns,
+                          const double* values, double diagonal_relative_tolerance, int32_t include_topology,
+                          cfdxg_matrix_diagnostics* out);
 /* The plan and its reason of the last cfdxg_solve_linear_system on the context. */
 const char* cfdxg_plan_reason(const cfdxg_context* ctx);
 

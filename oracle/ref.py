@@ -434,3 +434,26 @@ def scale_matrix(ro, co, va, scaling, zero_tolerance=0.0):
                               _p(sv), _p(zc), C.byref(nnz)), "scale_matrix")
     assert nnz.value == va.size
     return rs, cs, sv, int(zc[0]), int(zc[1])
+
+
+_DIAG_COUNTS = ("rows", "columns", "nnz", "finite", "structurally_consistent", "empty_rows", "empty_columns",
+                "missing_diagonal", "near_zero_diagonal", "isolated_dofs", "duplicate_entries", "connected_components")
+_DIAG_VALUES = ("max_abs_value", "min_nonzero_abs_value", "max_row_sum", "min_nonzero_row_sum", "max_column_sum",
+                "min_nonzero_column_sum", "max_abs_diagonal", "min_nonzero_abs_diagonal", "diagonal_dynamic_range",
+                "row_sum_dynamic_range", "column_sum_dynamic_range", "minimum_gershgorin_margin")
+
+
+def diagnose_matrix(ro, co, va, n_cols=None, tolerance=1e-14, topology=True) -> dict:
+    """core/linalg/matrix_diagnostics.h:126 diagnose_matrix."""
+    ro, co, va = (np.ascontiguousarray(ro, np.int64), np.ascontiguousarray(co, np.int64),
+                  np.ascontiguousarray(va, np.float64))
+    n = ro.size - 1
+    c, v = np.zeros(12, np.int64), np.zeros(12)
+    L = lib()
+    L.ref_diagnose_matrix.argtypes = [C.c_int64, C.c_int64, C.c_void_p, C.c_void_p, C.c_void_p, C.c_double,
+                                      C.c_int32, C.c_void_p, C.c_void_p]
+    _check(L.ref_diagnose_matrix(n, n if n_cols is None else int(n_cols), _p(ro), _p(co), _p(va), float(tolerance),
+                                 int(bool(topology)), _p(c), _p(v)), "diagnose_matrix")
+    out = {k: int(x) for k, x in zip(_DIAG_COUNTS, c)}
+    out.update({k: float(x) for k, x in zip(_DIAG_VALUES, v)})
+    return out

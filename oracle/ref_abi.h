@@ -159,6 +159,9 @@ int ref_measure_characteristics(int64_t n, const int64_t* row_offsets, const int
 int ref_select_linear_solver(int32_t problem, int64_t equations, double average_nnz,
                              double coefficient_range, const int32_t* flags, const int32_t* req,
                              double braess_sarazin_alpha, int32_t* plan);
+/* core/linalg/matrix_diagnostics.h:126  diagnose_matrix (field order in ref_linalg.cpp) */
+int ref_diagnose_matrix(int64_t n_rows, int64_t n_cols, const int64_t* row_offsets, const int64_t* columns,
+                        const double* values, double tolerance, int32_t topology, int64_t* counts, double* values_out);
 /* core/linalg/matrix_diagnostics.h:410  scale_matrix (MatrixScaling numbering) */
 int ref_scale_matrix(int64_t n, const int64_t* row_offsets, const int64_t* columns, const double* values,
                      int32_t scaling, double zero_tolerance, double* row_scale, double* column_scale,

@@ -393,3 +393,41 @@ extern "C" int ref_scale_matrix(int64_t n, const int64_t* ro, const int64_t* co,
         return -1;
     }
 }
+
+// core/linalg/matrix_diagnostics.h:126  diagnose_matrix
+// counts: rows, columns, nnz, finite, structurally_consistent, empty_rows, empty_columns,
+//         missing_diagonal, near_zero_diagonal, isolated_dofs, duplicate_entries, connected_components
+// values: max_abs_value, min_nonzero_abs_value, max_row_sum, min_nonzero_row_sum, max_column_sum,
+//         min_nonzero_column_sum, max_abs_diagonal, min_nonzero_abs_diagonal, diagonal_dynamic_range,
+//         row_sum_dynamic_range, column_sum_dynamic_range, minimum_gershgorin_margin
+extern "C" int ref_diagnose_matrix(int64_t n_rows, int64_t n_cols, const int64_t* ro, const int64_t* co,
+                                   const double* va, double tolerance, int32_t topology, int64_t* counts,
+                                   double* values) {
+    try {
+        std::vector<SparseMatrix::Index> off(ro, ro + n_rows + 1), col(co, co + ro[n_rows]);
+        std::vector<double> val(va, va + ro[n_rows]);
+        const SparseMatrix A = SparseMatrix::from_sorted_csr(static_cast<std::size_t>(n_rows),
+                                                             static_cast<std::size_t>(n_cols), std::move(off),
+                                                             std::move(col), std::move(val));
+        const MatrixDiagnostics d = diagnose_matrix(A, tolerance, topology != 0);
+        const int64_t c[12] = {static_cast<int64_t>(d.rows), static_cast<int64_t>(d.columns),
+                               static_cast<int64_t>(d.nnz), d.finite ? 1 : 0, d.structurally_consistent ? 1 : 0,
+                               static_cast<int64_t>(d.empty_rows), static_cast<int64_t>(d.empty_columns),
+                               static_cast<int64_t>(d.missing_diagonal), static_cast<int64_t>(d.near_zero_diagonal),
+                               static_cast<int64_t>(d.isolated_dofs), static_cast<int64_t>(d.duplicate_entries),
+                               static_cast<int64_t>(d.connected_components)};
+        const double v[12] = {d.max_abs_value, d.min_nonzero_abs_value, d.max_row_sum, d.min_nonzero_row_sum,
+                              d.max_column_sum, d.min_nonzero_column_sum, d.max_abs_diagonal,
+                              d.min_nonzero_abs_diagonal, d.diagonal_dynamic_range, d.row_sum_dynamic_range,
+                              d.column_sum_dynamic_range, d.minimum_gershgorin_margin};
+        for (int k = 0; k < 12; ++k) {
+            counts[k] = c[k];
+            values[k] = v[k];
+        }
+        cfdx_ref::g_error.clear();
+        return 0;
+    } catch (const std::exception& e) {
+        cfdx_ref::set_error(e);
+        return -1;
+    }
+}

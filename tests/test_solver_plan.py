@@ -237,3 +237,31 @@ def test_reference_case_diagonal_dynamic_range_avoids_cg_amg():
     assert not c["strongly_scaled"]
     plan = cg.select_linear_solver("pressure_poisson", c)
     assert (plan["krylov"], plan["preconditioner"]) == ("gmres", "jacobi")
+
+
+# ------------------------------------------------------------- diagnose_matrix
+@pytest.mark.parametrize("name", sorted(MATRICES))
+@pytest.mark.parametrize("tol,topology", [(1e-14, True), (0.5, False)])
+def test_diagnosis_matches_reference(ref, name, tol, topology):
+    ro, co_, va = MATRICES[name]
+    mine = cg.diagnose_matrix(ro, co_, va, diagonal_relative_tolerance=tol, include_topology=topology)
+    theirs = ref.diagnose_matrix(ro, co_, va, tolerance=tol, topology=topology)
+    for k, v in theirs.items():
+        if isinstance(v, float):
+            assert np.float64(mine[k]).tobytes() == np.float64(v).tobytes(), (k, mine[k], v)
+        else:
+            assert mine[k] == v, (k, mine[k], v)
+
+
+def test_diagnosis_of_a_rectangular_matrix_and_an_inconsistent_one(ref):
+    # 3 x 4 with an empty column, and the chain of a block-diagonal pattern (two components)
+    ro, co_, va = np.array([0, 2, 3, 4]), np.array([0, 1, 1, 3]), np.array([2.0, -1.0, 3.0, 4.0])
+    mine = cg.diagnose_matrix(ro, co_, va, n_cols=4)
+    theirs = ref.diagnose_matrix(ro, co_, va, n_cols=4)
+    assert np.isnan(mine["minimum_gershgorin_margin"]) and np.isnan(theirs["minimum_gershgorin_margin"])
+    for k in theirs:
+        if k != "minimum_gershgorin_margin":
+            assert mine[k] == theirs[k], k
+    assert mine["empty_columns"] == 1 and mine["connected_components"] == 3
+    bad = cg.diagnose_matrix([0, 2, 3], [1, 0, 1], [1.0, 2.0, 3.0])   # unsorted row: not consistent
+    assert bad["structurally_consistent"] == 0 and bad["finite"] == 0 and bad["rows"] == 2
