@@ -16,7 +16,6 @@
 // lane through shuffles measured 1.2-1.4x slower on the 64^3 tet mesh.)
 #include <algorithm>
 #include <cmath>
-#include <mutex>
 #include <numeric>
 #include <string>
 
@@ -788,10 +787,6 @@ constexpr std::size_t kNoAllocBytes = kNoAllocGradBytes + sizeof(double) * kNoAl
                                       sizeof(int) * kNoAllocMaxPatches;
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocBytes];
 
-// Host-side device address of g_noalloc_scratch, looked up once per device.
-std::mutex g_noalloc_mutex;
-void* g_noalloc_address[64] = {};
-
 struct PatchTable {
     int n;
     int fixed[kNoAllocMaxPatches];
@@ -806,19 +801,39 @@ __global__ void k_fill_patch_table(PatchTable t, int* fixed, double* value) {
     }
 }
 
-void* noalloc_scratch_address(int device) {
-    if (device < 0 || device >= 64) throw Error(CFDXG_ERR_INVALID_ARGUMENT, "device index out of range");
-    std::lock_guard<std::mutex> lock(g_noalloc_mutex);
-    if (!g_noalloc_address[device]) {
-        void* ptr = nullptr;
-        const cudaError_t rc = cudaGetSymbolAddress(&ptr, g_noalloc_scratch);
-        if (rc != cudaSuccess || !ptr)
-            throw Error(CFDXG_ERR_CUDA, std::string("cudaGetSymbolAddress(g_noalloc_scratch): ") +
-                                            cudaGetErrorString(rc));
-        g_noalloc_address[device] = ptr;
-    }
-    return g_noalloc_address[device];
+// Device address of g_noalloc_scratch in the calling thread's current context.
+// Looked up on every call rather than cached: the address belongs to the
+// module as loaded in that context, and a context that is destroyed and made
+// again (cudaDeviceReset, or a driver-API context made current by the caller)
+// loads the module at another address.  The lookup allocates nothing.
+void* noalloc_scratch_address() {
+    void* ptr = nullptr;
+    const cudaError_t rc = cudaGetSymbolAddress(&ptr, g_noalloc_scratch);
+    if (rc != cudaSuccess || !ptr)
+        throw Error(CFDXG_ERR_CUDA, std::string("cudaGetSymbolAddress(g_noalloc_scratch): ") +
+                                        cudaGetErrorString(rc));
+    return ptr;
 }
+
+// Makes the context's device current for the call and gives the caller's
+// current device back on every exit path.
+class CurrentDevice {
+public:
+    explicit CurrentDevice(int device) {
+        CFDXG_CUDA(cudaGetDevice(&saved_));
+        if (saved_ != device) CFDXG_CUDA(cudaSetDevice(device));
+        switched_ = saved_ != device;
+    }
+    ~CurrentDevice() {
+        if (switched_) cudaSetDevice(saved_);
+    }
+    CurrentDevice(const CurrentDevice&) = delete;
+    CurrentDevice& operator=(const CurrentDevice&) = delete;
+
+private:
+    int saved_ = 0;
+    bool switched_ = false;
+};
 
 }  // namespace
 }  // namespace cfdxg
@@ -837,8 +852,8 @@ extern "C" int cfdxg_rhie_chow_flux_noalloc(cfdxg_context* ctx, cfdxg_mesh* m, c
     if (m->n_patches > kNoAllocMaxPatches)
         throw Error(CFDXG_ERR_INVALID_ARGUMENT,
                     "cfdxg_rhie_chow_flux_noalloc: at most 32 boundary patches are supported");
-    CFDXG_CUDA(cudaSetDevice(ctx->device));
-    auto* base = static_cast<unsigned char*>(noalloc_scratch_address(ctx->device));
+    const CurrentDevice on_device(ctx->device);
+    auto* base = static_cast<unsigned char*>(noalloc_scratch_address());
     double* grad = reinterpret_cast<double*>(base);
     double* tvalue = reinterpret_cast<double*>(base + kNoAllocGradBytes);
     int* tfixed = reinterpret_cast<int*>(base + kNoAllocGradBytes + sizeof(double) * kNoAllocMaxPatches);

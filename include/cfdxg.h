@@ -205,11 +205,15 @@ int cfdxg_rhie_chow_flux(cfdxg_context* ctx, cfdxg_mesh* mesh, const double* Hby
  * Limits: at most 262,144 cells and 32 patches; larger meshes are rejected
  * with CFDXG_ERR_INVALID_ARGUMENT.  HbyA, rAU, p and flux must be device
  * pointers (mesh already uploaded, geometry built); p_bc_fixed / p_bc_value
- * are host arrays of n_patches entries.  The first call on a device looks up
- * the array's device address (so make that first call before any stream
- * capture).  All calls share the array and it keeps the last call's
- * contents; every call overwrites what it reads, but calls that overlap on
- * the GPU (two streams or threads at once) race on it. */
+ * are host arrays of n_patches entries (either may be NULL: no fixed-pressure
+ * patch).  Each call makes the context's device current, looks up the
+ * array's device address in that context (cudaGetSymbolAddress, which
+ * allocates nothing) and gives the caller's current device back before it
+ * returns.  The first call on a device can load the library's device code,
+ * so make that first call before any stream capture.  All calls share the
+ * array and it keeps the last call's contents; every call overwrites what it
+ * reads, but calls that overlap on the GPU (two streams or threads at once)
+ * race on it. */
 int cfdxg_rhie_chow_flux_noalloc(cfdxg_context* ctx, cfdxg_mesh* mesh, const double* HbyA,
                                  const double* rAU, const double* p, double rho,
                                  const int32_t* p_bc_fixed, const double* p_bc_value,

@@ -18,7 +18,8 @@ ROOT = Path(__file__).resolve().parents[1]
 if str(ROOT) not in sys.path:
     sys.path.insert(0, str(ROOT))
 
-REF_SRC = Path("/root/reference")
+# the reference source tree (read only); override with CFDX_REFERENCE_ROOT
+REF_SRC = Path(os.environ.get("CFDX_REFERENCE_ROOT", "/root/reference"))
 
 
 def pytest_configure(config):
@@ -29,7 +30,7 @@ def pytest_configure(config):
         b.build()
     ref_lib = ROOT / "oracle" / "_ref" / "libcfdx_ref.so"
     if not ref_lib.exists() and REF_SRC.exists():
-        subprocess.run(["make", "-s", "-C", str(ROOT / "oracle"), "ref", "oracle"], check=True)
+        subprocess.run(["make", "-s", "-C", str(ROOT / "oracle"), "ref", "oracle", f"REF_ROOT={REF_SRC}"], check=True)
     c_lib = ROOT / "oracle" / "_build" / "libcfdx_oracle.so"
     if not c_lib.exists() and (ROOT / "oracle" / "cfdx_oracle.c").exists():
         subprocess.run(["make", "-s", "-C", str(ROOT / "oracle"), "oracle"], check=True)
