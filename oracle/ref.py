@@ -295,6 +295,53 @@ class AmgFromLevels(Amg):
         self.setup_seconds = float("nan")
 
 
+class AmgFromTransfers(Amg):
+    """The reference's setup() with each level's C/F interpolation read from a
+    complete earlier run of that setup (``transfers``: p_offsets_l, p_columns_l,
+    p_values_l, aggregate_l per level l, as ``Amg.level`` exports them) and
+    every other step -- Galerkin products, diagonals, damping -- run by the
+    reference's own code (ref_amg_create_from_transfers)."""
+
+    def __init__(self, ro, co, va, transfers, level_rows):
+        self.ro, self.co, self.va = (np.ascontiguousarray(ro, np.int64), np.ascontiguousarray(co, np.int64),
+                                     np.ascontiguousarray(va, np.float64))
+        L = len(level_rows)
+        self._keep = {k: np.ascontiguousarray(v, np.float64 if k.startswith("p_values") else np.int64)
+                      for k, v in transfers.items()}
+        P64 = C.POINTER(C.c_int64)
+        PD = C.POINTER(C.c_double)
+
+        def arr(t, key):
+            return (t * max(1, L - 1))(*[self._keep[f"{key}_{l}"].ctypes.data_as(t) for l in range(L - 1)])
+
+        self._ptrs = [arr(P64, "p_offsets"), arr(P64, "p_columns"), arr(PD, "p_values"), arr(P64, "aggregate")]
+        rows = np.ascontiguousarray(level_rows, np.int64)
+        f = lib().ref_amg_create_from_transfers
+        f.restype = C.c_void_p
+        f.argtypes = [C.c_int64, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int32, C.c_void_p] + [C.c_void_p] * 5
+        sec = C.c_double()
+        self.h = f(self.ro.size - 1, _p(self.ro), _p(self.co), _p(self.va), L, _p(rows),
+                   *[C.cast(p, C.c_void_p) for p in self._ptrs], C.byref(sec))
+        if not self.h:
+            raise RuntimeError(f"reference AMG rebuild failed: {lib().ref_last_error().decode()}")
+        self.setup_seconds = sec.value
+
+
+def hierarchy_sha256(amg) -> list[dict]:
+    """Per level, the SHA-256 of each exported array (int64 indices, FP64 values)
+    -- the fingerprint used to compare hierarchies too large to store."""
+    import hashlib
+    out = []
+    for l in range(amg.num_levels()):
+        lv = amg.level(l)
+        e = {"n_rows": int(lv["inv_diag"].size), "nnz": int(lv["columns"].size)}
+        for k in ("row_offsets", "columns", "values", "inv_diag", "p_offsets", "p_columns", "p_values", "aggregate"):
+            if lv.get(k) is not None and (k not in ("p_columns", "p_values") or lv["p_offsets"] is not None):
+                e[k] = hashlib.sha256(np.ascontiguousarray(lv[k]).tobytes()).hexdigest()
+        out.append(e)
+    return out
+
+
 def solve_linear_system(ro, co, va, rhs, x0=None, krylov=3, preconditioner=6, restart=30, max_iterations=1000,
                         tolerance=1e-8):
     ro, co, va = (np.ascontiguousarray(ro, np.int64), np.ascontiguousarray(co, np.int64),

@@ -123,6 +123,86 @@ extern "C" void* ref_amg_create_from_levels(int32_t n_levels, const int64_t* n_r
     }
 }
 
+// MatrixFreeVcyclePreconditioner::setup (amg_preconditioner.h:76-243) for the
+// DirectCF policy with one step replaced: the C/F interpolation of each level
+// (build_cf_interpolation, :1511-1885, the step whose second pass makes the
+// reference's setup take hours at 10^6 rows) is read from arrays that a
+// complete run of that same setup wrote out, instead of being recomputed.
+// Everything else is the reference's own code in setup()'s order: the fine
+// diagonal, GalerkinCSRProduct symbolic + numeric for every coarse operator
+// (galerkin_csr_product.h:33-176), matrix_is_valid, build_diagonal,
+// build_level_lines, and compute_stable_smoother_omega for the damping.
+// coarse_rows[l] is the row count of level l (level 0 = the input matrix).
+extern "C" void* ref_amg_create_from_transfers(int64_t n, const int64_t* ro, const int64_t* co,
+                                               const double* va, int32_t n_levels,
+                                               const int64_t* coarse_rows,
+                                               const int64_t* const* p_off,
+                                               const int64_t* const* p_col,
+                                               const double* const* p_val,
+                                               const int64_t* const* aggregate, double* seconds) {
+    try {
+        auto h = std::make_unique<AmgHandle>();
+        h->op = std::make_unique<OwnedOperator>(cfdx_ref::make_csr(n, ro, co, va));
+        h->amg = std::make_unique<MatrixFreeVcyclePreconditioner>(
+            *h->op, 0.7, 6, 6, 0.25, 25, AMGInterpolationPolicy::DirectCF, false, false,
+            AMGSmootherPolicy::DampedJacobi, 0.0, 0, 1.0);
+        auto& P = *h->amg;
+        using Level = MatrixFreeVcyclePreconditioner::Level;
+        const double t0 = cfdx_ref::now_seconds();
+        const auto fail = [&](const std::string& why) -> void* {
+            cfdx_ref::g_error = "AMG rebuild failed: " + why;
+            return nullptr;
+        };
+        if (n_levels < 1 || coarse_rows[0] != n) return fail("level sizes");
+        P.levels_.clear();
+        P.first_aggregate_.clear();
+        Level fine;
+        fine.A = h->op->matrix_;
+        if (!MatrixFreeVcyclePreconditioner::build_diagonal(fine)) return fail("fine diagonal");
+        if (!P.build_level_lines(fine)) return fail("fine lines");
+        P.levels_.push_back(std::move(fine));
+        for (int32_t l = 0; l + 1 < n_levels; ++l) {
+            const int64_t rows = coarse_rows[l];
+            if (static_cast<int64_t>(P.levels_.back().A.n_rows()) != rows) return fail("level rows");
+            std::vector<MatrixFreeVcyclePreconditioner::TransferRow> prolongation(static_cast<std::size_t>(rows));
+            std::vector<std::size_t> agg(static_cast<std::size_t>(rows));
+            for (int64_t i = 0; i < rows; ++i) {
+                for (int64_t q = p_off[l][i]; q < p_off[l][i + 1]; ++q)
+                    prolongation[i].push_back({static_cast<std::size_t>(p_col[l][q]), p_val[l][q]});
+                agg[i] = static_cast<std::size_t>(aggregate[l][i]);
+            }
+            const std::size_t coarse_n = static_cast<std::size_t>(coarse_rows[l + 1]);
+            GalerkinCSRProduct product;
+            SparseMatrix coarse;
+            if (!product.symbolic(P.levels_.back().A, prolongation, coarse_n) ||
+                !product.numeric(P.levels_.back().A, prolongation, coarse,
+                                 &P.last_footprint_.galerkin_dropped_entries) ||
+                !MatrixFreeVcyclePreconditioner::matrix_is_valid(coarse))
+                return fail("Galerkin product at level " + std::to_string(l));
+            if (P.levels_.size() == 1) P.first_aggregate_ = agg;
+            Level next;
+            next.A = std::move(coarse);
+            if (!MatrixFreeVcyclePreconditioner::build_diagonal(next)) return fail("coarse diagonal");
+            if (!P.build_level_lines(next)) return fail("coarse lines");
+            P.levels_.back().aggregate = std::move(agg);
+            P.levels_.back().prolongation = std::move(prolongation);
+            P.levels_.back().coarse_product = std::move(product);
+            P.levels_.push_back(std::move(next));
+        }
+        double safe_omega = 0.0;
+        if (P.compute_stable_smoother_omega(P.levels_, safe_omega, &P.last_setup_error_))
+            P.omega_ = safe_omega;
+        else
+            P.omega_ = P.configured_omega_;
+        if (seconds) *seconds = cfdx_ref::now_seconds() - t0;
+        cfdx_ref::g_error.clear();
+        return h.release();
+    } catch (const std::exception& e) {
+        cfdx_ref::set_error(e);
+        return nullptr;
+    }
+}
+
 // MatrixFreeVcyclePreconditioner::update_values (amg_preconditioner.h:245-314)
 // on the owned operator's matrix replaced by the new values (same pattern).
 extern "C" int ref_amg_update_values(void* hv, int64_t n, const int64_t* ro, const int64_t* co,

@@ -61,7 +61,7 @@ def _compare_hierarchy(ref, ro, co, va):
     return amg
 
 
-@pytest.mark.parametrize("n", [8, 16])
+@pytest.mark.parametrize("n", [8, 16, 32])   # 32: the 32^3 hex Poisson benchmark system itself
 def test_amg_setup_bit_exact_poisson_hex(ref, n):
     m, bc, src = cases.poisson_case(n)
     ro, co, va, rhs, _ = ref.assemble_diffusion(m, bc, 1.0, src)
@@ -85,6 +85,30 @@ def test_amg_setup_bit_exact_anisotropic_boundary_layer(ref):
     src = cg.random_field(m.n_cells, "uniform", -1.0, 1.0, 3)
     ro, co, va, rhs, _ = ref.assemble_diffusion(m, bc, 1.0, src)
     _compare_hierarchy(ref, ro, co, va)
+
+
+def test_reference_rebuild_from_stored_transfers_is_its_own_setup(ref):
+    # The reference's setup with each level's C/F interpolation read back from
+    # an earlier complete run (the way the benchmark's CPU legs rebuild the
+    # reference's own 64^3 hierarchy) gives the identical hierarchy.
+    m = cases.simple_mesh(12)
+    g = ref.geometry(m)
+    U, rAU, aP, p, fixed, value = cases.simple_fields(m, g["cell_centres"])
+    r = ref.simple_assemble(m, U, rAU, p, 1.0, fixed, value)
+    R = ref.Amg(r["row_offsets"], r["columns"], r["values"])
+    transfers, rows = {}, []
+    for l in range(R.num_levels()):
+        lv = R.level(l)
+        rows.append(lv["inv_diag"].size)
+        if lv["p_offsets"] is not None:
+            for k in ("p_offsets", "p_columns", "p_values", "aggregate"):
+                transfers[f"{k}_{l}"] = lv[k]
+    T = ref.AmgFromTransfers(r["row_offsets"], r["columns"], r["values"], transfers, rows)
+    assert ref.hierarchy_sha256(T) == ref.hierarchy_sha256(R)
+    assert T.omega == R.omega
+    x0, rep0 = R.solve_gmres(r["b"])
+    x1, rep1 = T.solve_gmres(r["b"])
+    assert rep0["iterations"] == rep1["iterations"] and np.array_equal(x0, x1)
 
 
 def test_amg_setup_rejects_zero_diagonal():
