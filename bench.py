@@ -22,9 +22,16 @@ flushed before every timed step.  Rank-local device timing with CUDA events on
 the library's stream, max over ranks.  N > 1 runs independent replicas (each
 rank its own right-hand sides); there is no data-path collective.
 
-`--impl reference` times the reference's own CPU solve phase (oracle/_ref,
-one host core; the bit-identical C restatement where that build is absent)
-on the same system.
+`parity` (rank 0, one GPU): the reference's own solve of the first right-hand
+side on its own hierarchy (one host core, also the `cpu_baseline`), its
+corrector assembly compared bit for bit with the GPU's, and each GPU form's
+pressure and corrected face fluxes against the reference's (relative L2) with
+the iteration counts.
+
+`--impl reference` times the reference's own CPU implementation (oracle/_ref,
+one host core): its assembly of the same system, its own AMG hierarchy
+rebuilt from the stored output of its complete setup, and one complete
+GMRES(30) solve per step; it loads only oracle libraries.
 """
 from __future__ import annotations
 
@@ -235,6 +242,7 @@ def run_cfdxg(args):
         return rep.as_dict()
 
     ref_solutions = {}
+    first_solution = {}   # per form, its solution of right-hand side 0 (parity against the reference)
     sampler = ClockSampler(local_rank)
     for form, prec, krylov, learned in plan:
         amg = amgs[form]
@@ -266,6 +274,8 @@ def run_cfdxg(args):
             if rep["status_name"] != "converged" or rep["physical_residual_relative"] > TOL:
                 raise RuntimeError(f"{form} did not converge: {rep}")
             x = x_dev.cpu().numpy()
+            if k == 0 and form not in first_solution:
+                first_solution[form] = (x.copy(), rep["iterations"])
             if form == "plain_fp64":
                 ref_solutions[k] = x.copy()
             elif k in ref_solutions:
@@ -352,24 +362,22 @@ def run_cfdxg(args):
 
     result = None
     if rank == 0:
-        cpu = None
+        cpu = parity = None
         if world == 1 and not args.no_cpu_baseline and "plain_fp64" in amgs:
-            cpu = cpu_baseline(amgs["plain_fp64"], rhs_list[0])
+            cpu, parity = cpu_baseline_and_parity(args.n, amgs["plain_fp64"], A, rhs_list[0], m, mesh, base_fields,
+                                                  first_solution)
         result = {
             "metric": METRIC,
             "value": value, "unit": "s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": value * 1e3, "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
             "dtype": "f64 (Krylov) / f32 (V-cycle)", "data": "synthetic (seeded)",
-            "config": {"workload": f"Kuhn-tet {args.n}^3 x6 = {n_cells} cells, SIMPLE pressure correction, "
-                                   f"{N_RHS} seeded RHS, GMRES/FGMRES({RESTART}) + native RS AMG to 1e-8",
-                       "form": headline, "cells": n_cells, "nnz": int(A.nnz), "amg_levels": levels,
-                       "operator_complexity": round(sum(level_nnz) / level_nnz[0], 2),
-                       "l2": "inputs > L2 and L2 flushed before every timed step",
-                       "parallelism": f"replicas x{world}"},
+            "config": dict(_config(args.n, n_cells, int(A.nnz), headline), amg_levels=levels,
+                           operator_complexity=round(sum(level_nnz) / level_nnz[0], 2),
+                           parallelism=f"replicas x{world}"),
             "forms": forms, "case_build_s": case_s,
             "e2e": e2e, "gpu_launches": int(launches), "clocks": clocks, "roofline": roofline,
             "assembly": assembly,
-            "kernels": kernels, "cpu_baseline": cpu,
+            "kernels": kernels, "cpu_baseline": cpu, "parity": parity,
         }
         print(json.dumps(result), flush=True)
     if world > 1:
@@ -443,80 +451,186 @@ def _export_levels(amg):
     return [amg.export_level(l) for l in range(len(amg.hierarchy_level_sizes()))]
 
 
-class _CpuSolver:
-    """The reference's CPU solve phase around a given hierarchy: the reference
-    itself (oracle/_ref, kind "reference") where it was built, else the plain-C
-    restatement (oracle/cfdx_oracle.c, bit-identical to it, kind "port")."""
+def reference_hierarchy(n, ro, co, va):
+    """The reference's own AMG hierarchy of the n^3 system: its setup's stored
+    C/F interpolation (oracle/_ref/tet{n}_transfers.npz, written by
+    oracle/reference_hierarchy.py from a complete run of the reference's setup)
+    with every other setup step -- Galerkin products, diagonals, damping -- run
+    by the reference's own code, then checked level by level against the
+    committed SHA-256 of that complete setup.  -> (ref.Amg, info) or (None, info)."""
+    from oracle import ref
+    from oracle import reference_hierarchy as rh
+    got = rh.load_transfers(n) if ref.available() else None
+    if got is None:
+        return None, {"hierarchy": "stored reference transfers absent"}
+    transfers, rows, gold = got
+    t = time.perf_counter()
+    R = ref.AmgFromTransfers(ro, co, va, transfers, rows)
+    rebuild_s = time.perf_counter() - t
+    hashes = ref.hierarchy_sha256(R)
+    match = len(hashes) == len(gold["levels"]) and R.omega == gold["omega"] and all(
+        all(g.get(k) == v for k, v in h.items()) for h, g in zip(hashes, gold["levels"]))
+    if not match:
+        raise RuntimeError("the rebuilt reference hierarchy differs from the reference setup's fingerprint")
+    return R, {"hierarchy": "the reference's own setup (stored C/F interpolation of a complete run, Galerkin "
+                            "products rebuilt by its code); per-level SHA-256 equal to that run's",
+               "rebuild_s": rebuild_s, "reference_setup_s": gold["setup_seconds"], "levels": len(hashes),
+               "fingerprint": hashes}
 
-    def __init__(self, levels, omega):
+
+class _CpuSolver:
+    """The reference's CPU solve phase: the reference itself (oracle/_ref, kind
+    "reference") on its own hierarchy where that is stored, else on the library's
+    host-built hierarchy (bit-identical to the reference's, as the tests check);
+    the plain-C restatement (oracle/cfdx_oracle.c, kind "port") where the
+    reference build is absent."""
+
+    def __init__(self, n, amg, ro, co, va):
         from oracle import ref
+        self.info = {}
+        self.R = None
         if ref.available():
             self.kind = "reference"
-            self.R = ref.AmgFromLevels(levels, omega)
+            self.R, self.info = reference_hierarchy(n, ro, co, va)
+            if self.R is None:
+                self.R = ref.AmgFromLevels(_export_levels(amg), amg.omega)
+                self.info["hierarchy"] = "library host setup loaded into the reference's V-cycle"
         else:
-            from oracle import cfdx_oracle as co
+            from oracle import cfdx_oracle as co_
             self.kind = "port"
-            self.co = co
-            self.H = co.Hierarchy(levels, omega)
-            self.csr = (levels[0]["row_offsets"], levels[0]["columns"], levels[0]["values"])
+            self.co = co_
+            self.H = co_.Hierarchy(_export_levels(amg), amg.omega)
+            self.csr = (ro, co, va)
+            self.info["hierarchy"] = "library host setup (C restatement of the V-cycle)"
 
-    def solve(self, b, max_iterations):
-        """-> (iterations, solve seconds)"""
+    def solve(self, b, max_iterations=1000):
+        """-> (solution, iterations, solve seconds)"""
         if self.kind == "reference":
             x, rep = self.R.solve_gmres(b, restart=RESTART, max_iterations=max_iterations, tolerance=TOL)
-            return rep["iterations"], rep["solve_seconds"]
+            return x, rep["iterations"], rep["solve_seconds"]
         t = time.perf_counter()
         x, rep = self.co.solve_gmres(*self.csr, b, self.H, restart=RESTART, max_iterations=max_iterations,
                                      tolerance=TOL)
-        return rep["iterations"], time.perf_counter() - t
+        return x, rep["iterations"], time.perf_counter() - t
 
 
-def cpu_baseline(amg, b):
-    """The reference's solve phase on the same system, one host core."""
-    S = _CpuSolver(_export_levels(amg), amg.omega)
+def rel_l2(a, b):
+    return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
+
+
+def cpu_baseline_and_parity(n, amg, A, b, m, mesh, fields, first_solution):
+    """The reference's solve phase on the same system and first right-hand side
+    (one host core), and the GPU forms' parity against its solution: pressure
+    relative L2, iteration count and the corrected face fluxes of each
+    solution (make_rhie_chow_mass_flux: the library's on the GPU, the
+    reference's own on the host)."""
+    import cfdx_dev_b200 as cg
+    ro, co, va = (np.ascontiguousarray(a, t) for a, t in zip(A.to_csr(), (np.int64, np.int64, np.float64)))
+    S = _CpuSolver(n, amg, ro, co, va)
     t = time.time()
-    iters, sec = S.solve(b, 1000)
-    return {"value": sec, "unit": "s", "cores": 1, "kind": S.kind, "iterations": iters, "wall_s": time.time() - t,
-            "sample": "one complete GMRES(30)+NativeAMG solve phase to 1e-8 on the full system, first right-hand "
-                      "side (hierarchy loaded: bit-identical to the reference setup, which takes hours at this "
-                      "size)"}
+    x_ref, iters, sec = S.solve(b)
+    cpu = {"value": sec, "unit": "s", "cores": 1, "kind": S.kind, "iterations": iters, "wall_s": time.time() - t,
+           "sample": "one complete GMRES(30)+NativeAMG solve phase to 1e-8 on the full system, first right-hand "
+                     "side; hierarchy: " + S.info.get("hierarchy", "")}
+    U, rAU, p, fixed, value = fields
+    parity = {"tolerance_rel_l2": 1e-10, "reference": S.kind, "reference_iterations": int(iters),
+              "hierarchy": S.info.get("hierarchy")}
+    if "rebuild_s" in S.info:
+        parity["reference_rebuild_s"] = S.info["rebuild_s"]
+        parity["reference_setup_s"] = S.info["reference_setup_s"]
+        # the library's own host setup against the reference's setup, level by level
+        parity["library_hierarchy_equals_reference"] = _library_fingerprint(amg) == S.info["fingerprint"]
+    if S.kind == "reference":
+        from oracle import ref
+        r = ref.simple_assemble(m, U, rAU, p, 1.0, fixed, value)
+        parity["assembly_bit_exact"] = bool(np.array_equal(r["row_offsets"], ro) and np.array_equal(
+            r["columns"], co) and np.array_equal(r["values"], va) and np.array_equal(r["b"], b))
+        flux_ref = ref.rhie_chow_flux(m, U, rAU, x_ref, 1.0, fixed, value)
+    else:
+        from oracle import cfdx_oracle as co_
+        flux_ref = co_.rhie_chow_flux(m, U, rAU, x_ref, 1.0, fixed, value)
+    forms = {}
+    for form, (x, its) in first_solution.items():
+        flux = cg.make_rhie_chow_mass_flux(mesh, U, rAU, x, 1.0, fixed, value)
+        forms[form] = {"pressure_rel_l2": rel_l2(x, x_ref), "flux_rel_l2": rel_l2(flux, flux_ref),
+                       "iterations": int(its)}
+    parity["forms"] = forms
+    if "plain_fp64" in forms:
+        f = forms["plain_fp64"]
+        parity["plain_fp64_within_tolerance"] = bool(f["pressure_rel_l2"] <= 1e-10 and f["flux_rel_l2"] <= 1e-10)
+        parity["plain_fp64_same_iterations"] = f["iterations"] == int(iters)
+    return cpu, parity
+
+
+def _library_fingerprint(amg):
+    from oracle import ref
+    out = []
+    for l in range(len(amg.hierarchy_level_sizes())):
+        out += ref.fingerprint_levels([amg.export_level(l)])
+    return out
 
 
 def run_reference(args):
-    """Reference arm: the reference's own CPU solve phase on this config."""
+    """Reference arm: the reference's own CPU implementation of the path on this
+    config, loading only oracle libraries -- inputs from the generator compiled
+    alone (oracle/cases.py), geometry and corrector assembly by the reference's
+    code, its own AMG hierarchy (reference_hierarchy), and one complete
+    GMRES(30) solve to 1e-8 per step (about 27 s each on one core, so the arm
+    runs at most one warm-up and three timed solves)."""
     rank, local_rank, world = dist_env()
     if rank != 0:
         return None
-    import cfdx_dev_b200 as cg
-    from oracle import cfdx_oracle as co
-    from tests import cases
-    m = cases.simple_mesh(args.n)
-    g = co.geometry(m)
-    U, rAU, aP, p, fixed, value = cases.simple_fields(m, g["cell_centres"])
-    r = co.simple_assemble(m, U, rAU, p, 1.0, fixed, value)
-    amg = cg.NativeBoomerAMGPreconditioner(None)
-    if not amg.setup_host(r["row_offsets"], r["columns"], r["values"]):
-        raise RuntimeError(amg.last_error())
-    S = _CpuSolver(_export_levels(amg), amg.omega)
-    # first warm-up step: one complete solve, for the iteration count
-    iters, full_s = S.solve(r["b"], 1000)
-    sample_its = 2
-    for _ in range(max(0, args.warmup - 1)):
-        S.solve(r["b"], sample_its)
-    ts = [S.solve(r["b"], sample_its)[1] for _ in range(args.steps)]
-    v = float(np.mean(ts)) / sample_its * iters
-    out = {"impl": "reference", "metric": METRIC, "value": v, "unit": "s", "n_gpus": world, "steps": args.steps,
-           "warmup": args.warmup, "ms_per_step": v * 1e3, "higher_is_better": False, "scaling": "weak",
-           "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)",
-           "config": {"workload": f"Kuhn-tet {args.n}^3 x6 = {m.n_cells} cells, SIMPLE pressure correction, "
-                                  f"GMRES({RESTART}) + native RS AMG to 1e-8"},
-           "cpu_baseline": {"value": v, "unit": "s", "cores": 1, "kind": S.kind,
-                            "sample": f"GMRES(30)+NativeAMG solve phase capped at {sample_its} iterations "
-                                      f"per step, scaled to the full solve's {iters} iterations "
-                                      f"(full solve measured once in warm-up: {full_s:.2f} s)"},
-           "e2e": {"value": v, "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    from oracle import cases as oc
+    from oracle import ref
+    from oracle import reference_hierarchy as rh
+    base = {"impl": "reference", "metric": METRIC}
+    if not ref.available() or rh.load_transfers(args.n) is None:
+        out = dict(base, unavailable="the reference build (oracle/_ref) or its stored 64^3 AMG transfers are "
+                                     "absent; its own setup takes hours at this size")
+        print(json.dumps(out), flush=True)
+        return out
+    t0 = time.time()
+    m = oc.simple_mesh(args.n)
+    g = ref.geometry(m)
+    U, rAU, aP, p, fixed, value = oc.simple_fields(m, g["cell_centres"])
+    r = ref.simple_assemble(m, U, rAU, p, 1.0, fixed, value)
+    case_s = time.time() - t0
+    gold = rh.load_transfers(args.n)[2]
+    if rh.system_sha256(r) != gold["system"]:
+        raise RuntimeError("the reference-assembled system differs from the stored fingerprint")
+    R, info = reference_hierarchy(args.n, r["row_offsets"], r["columns"], r["values"])
+    warmup, steps = min(args.warmup, 1), min(args.steps, 3)
+    for _ in range(warmup):
+        R.solve_gmres(r["b"], restart=RESTART, tolerance=TOL)
+    ts, its = [], []
+    for _ in range(steps):
+        x, rep = R.solve_gmres(r["b"], restart=RESTART, tolerance=TOL)
+        if rep["status"] != 0:
+            raise RuntimeError(f"reference solve did not converge: {rep}")
+        ts.append(rep["solve_seconds"])
+        its.append(rep["iterations"])
+    v = float(np.mean(ts))
+    out = dict(base, value=v, unit="s", n_gpus=world, steps=steps, warmup=warmup, steps_requested=args.steps,
+               warmup_requested=args.warmup, ms_per_step=v * 1e3, higher_is_better=False, scaling="weak",
+               vs_baseline=None, dtype="f64", data="synthetic (seeded)",
+               config=_config(args.n, m.n_cells, int(r["columns"].size), "plain_fp64 (the reference, host)"),
+               iterations=float(np.mean(its)), case_build_s=case_s, hierarchy_rebuild_s=info["rebuild_s"],
+               reference_setup_s=gold["setup_seconds"],
+               cpu_baseline={"value": v, "unit": "s", "cores": 1, "kind": "reference",
+                             "sample": f"{steps} complete GMRES(30)+NativeAMG solves to 1e-8 of the full system "
+                                       f"(one per step, first right-hand side) on the reference's own hierarchy "
+                                       f"({info['hierarchy']}; its setup took {gold['setup_seconds']:.0f} s once, "
+                                       f"not timed here)"},
+               e2e={"value": v, "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0})
     print(json.dumps(out), flush=True)
     return out
+
+
+def _config(n, cells, nnz, form):
+    return {"workload": f"Kuhn-tet {n}^3 x6 = {cells} cells, SIMPLE pressure correction, "
+                        f"{N_RHS} seeded RHS, GMRES/FGMRES({RESTART}) + native RS AMG to 1e-8",
+            "form": form, "cells": cells, "nnz": nnz,
+            "l2": "inputs > L2 and L2 flushed before every timed step", "parallelism": "replicas x1"}
 
 
 def main():

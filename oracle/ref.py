@@ -327,18 +327,28 @@ class AmgFromTransfers(Amg):
         self.setup_seconds = sec.value
 
 
-def hierarchy_sha256(amg) -> list[dict]:
-    """Per level, the SHA-256 of each exported array (int64 indices, FP64 values)
-    -- the fingerprint used to compare hierarchies too large to store."""
+def fingerprint_levels(levels) -> list[dict]:
+    """Per level (dicts as ``Amg.level`` or the library's ``export_level`` give
+    them), the SHA-256 of each array as int64 indices / FP64 values -- the
+    fingerprint used to compare hierarchies too large to store."""
     import hashlib
     out = []
-    for l in range(amg.num_levels()):
-        lv = amg.level(l)
+    for lv in levels:
         e = {"n_rows": int(lv["inv_diag"].size), "nnz": int(lv["columns"].size)}
         for k in ("row_offsets", "columns", "values", "inv_diag", "p_offsets", "p_columns", "p_values", "aggregate"):
-            if lv.get(k) is not None and (k not in ("p_columns", "p_values") or lv["p_offsets"] is not None):
-                e[k] = hashlib.sha256(np.ascontiguousarray(lv[k]).tobytes()).hexdigest()
+            a = lv.get(k)
+            if a is not None and (k not in ("p_columns", "p_values") or lv.get("p_offsets") is not None):
+                a = np.ascontiguousarray(a, np.float64 if k in ("values", "inv_diag", "p_values") else np.int64)
+                e[k] = hashlib.sha256(a.tobytes()).hexdigest()
         out.append(e)
+    return out
+
+
+def hierarchy_sha256(amg) -> list[dict]:
+    """fingerprint_levels of a reference hierarchy, one level in memory at a time."""
+    out = []
+    for l in range(amg.num_levels()):
+        out += fingerprint_levels([amg.level(l)])
     return out
 
 

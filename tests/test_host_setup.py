@@ -212,3 +212,17 @@ def test_reusable_context_lifecycle_on_the_host():
     assert ctx.prepare((ro2, co[keep], va[keep]))
     assert ctx.stats["full_setups"] == 2
     assert not ctx.prepare((ro, co, np.where(np.arange(va.size) == 3, np.nan, va)))   # rejected input
+
+
+def test_oracle_case_library_builds_the_same_inputs(ref):
+    # the CPU reference legs build their inputs with the generator compiled
+    # alone (oracle/cases.py); they must equal the package's, bit for bit
+    from oracle import cases as oc
+    a, b = cases.simple_mesh(9), oc.simple_mesh(9)
+    for k in ("px", "py", "pz", "face_offsets", "face_vertices", "owner", "neighbour", "cell_offsets",
+              "cell_faces", "patch_of_face", "patch_types"):
+        assert np.array_equal(getattr(a, k), getattr(b, k)), k
+    cc = ref.geometry(a)["cell_centres"]
+    for s in (0, 3):
+        for x, y in zip(cases.simple_fields(a, cc, seed_offset=s), oc.simple_fields(b, cc, seed_offset=s)):
+            assert np.array_equal(x, y)

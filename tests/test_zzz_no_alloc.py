@@ -48,7 +48,9 @@ class _Case:
         self.ctx, self.m = ctx, m
         self.mesh = cg.Mesh(ctx, m)
         g = self.mesh.geometry()
-        U, rAU, aP, p0, fixed, value = cases.simple_fields(m, g["cell_centres"])
+        # the benchmark's HbyA and rAU (tests/cases.py seeds); no patch table needed
+        U = cg.fourier_field(g["cell_centres"], 8, 0.01, cases.SEED_HBYA)
+        rAU = np.concatenate([1.0 / cg.random_field(m.n_cells, "loguniform", 1.0, 100.0, cases.SEED_AP)] * 3)
         self.U, self.rAU = U, rAU
         self.cc = g["cell_centres"].reshape(3, -1)
         dev = torch.device("cuda", 0)
