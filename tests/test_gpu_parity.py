@@ -237,6 +237,26 @@ def test_fp32_vcycle_solve_reaches_fp64_tolerance(ctx, tet_setup):
         assert rel_l2(x32, x64) < 1e-6
 
 
+@pytest.mark.parametrize("limit", [2000, 300])
+def test_fp32_vcycle_fp64_dense_coarse_solve(ctx, ref, tet_setup, limit):
+    # The mixed-precision configuration's FP64 coarsest-level direct solve:
+    # the cycle ends at the first level with <= limit rows in a dense inverse
+    # formed and applied in FP64.  Converges to the FP64 true residual, and
+    # the solution agrees with the reference's own solve.
+    m, mesh, g, (U, rAU, aP, p, fixed, value) = tet_setup
+    A, b, phi, grad = cg.assemble_pressure_correction(mesh, U, rAU, p, 1.0, fixed, value)
+    ro, co, va = A.to_csr()
+    x_ref, rep_ref = ref.solve_linear_system(ro, co, va, b, restart=30, tolerance=1e-8)
+    amg = cg.NativeBoomerAMGPreconditioner(ctx, precision="fp32_vcycle", coarse_dense_limit=limit, dense_fp64=1)
+    assert amg.setup(A)
+    sizes = amg.hierarchy_level_sizes()
+    assert any(s <= limit for s in sizes), sizes
+    x32, rep32 = cg.solve_fgmres(A, b, amg=amg, restart=30, tolerance=1e-8, orthogonalization=1)
+    assert rep32["status_name"] == "converged"
+    assert rep32["physical_residual_relative"] <= 1e-8
+    assert rel_l2(x32, x_ref) < 1e-6
+
+
 def test_solve_is_deterministic(ctx, tet_setup):
     m, mesh, g, (U, rAU, aP, p, fixed, value) = tet_setup
     A, b, phi, grad = cg.assemble_pressure_correction(mesh, U, rAU, p, 1.0, fixed, value)
