@@ -20,6 +20,7 @@ from .api import (  # noqa: F401
     assemble_cell_diffusion_matrix,
     assemble_pressure_correction,
     boundary_layer_case,
+    build_hbya,
     fourier_field,
     gauss_gradient_with_boundary,
     hex_case,

@@ -57,7 +57,7 @@ class AmgOptions(C.Structure):
         ("require_smoother_certificate", C.c_int32), ("precision", C.c_int32),
         ("coarse_dense_limit", C.c_int32), ("reference_order", C.c_int32),
         ("coarse_pre_sweeps", C.c_int32), ("coarse_post_sweeps", C.c_int32), ("narrow_columns", C.c_int32),
-        ("half_values", C.c_int32),
+        ("half_values", C.c_int32), ("dense_fp64", C.c_int32),
     ]
 
 
@@ -183,6 +183,7 @@ PROTOTYPES = {
         C.c_int, [_V, _V, _V, _V, _V, C.c_double, _V, _V, C.c_int32, _P(_V), _V, _V, _V]),
     "cfdxg_rhie_chow_flux": (C.c_int, [_V, _V, _V, _V, _V, C.c_double, _V, _V, C.c_int32, _V]),
     "cfdxg_gauss_gradient": (C.c_int, [_V, _V, _V, _V, _V, C.c_int32, _V]),
+    "cfdxg_build_hbya": (C.c_int, [_V, _V, _V, _V, _V, _V, _V, C.c_int32, _V]),
     "cfdxg_rhie_chow_flux_noalloc": (C.c_int, [_V, _V, _V, _V, _V, C.c_double, _V, _V, _V]),
     "cfdxg_amg_options_default": (C.c_int, [_P(AmgOptions)]),
     "cfdxg_amg_create": (C.c_int, [_V, _P(AmgOptions), _P(_V)]),

@@ -380,6 +380,21 @@ def make_rhie_chow_mass_flux(mesh: Mesh, HbyA, rAU, p, rho=1.0, p_bc_fixed=None,
     return flux
 
 
+def build_hbya(mesh: Mesh, momentum, rhs, U, gradp, rAU):
+    """physics/steady_incompressible_solver.h:6430-6465 (build_hbya) -> HbyA (3*n_cells).
+
+    ``momentum``: one SparseMatrix, or three (one per component) sharing a pattern."""
+    ctx, hm = mesh.ctx, mesh.host
+    mats = list(momentum) if isinstance(momentum, (list, tuple)) else [momentum] * 3
+    handles = (C.c_void_p * 3)(*[M.handle.value for M in mats])
+    n3 = 3 * hm.n_cells
+    b, u, g, r = (_f64(a, n3) for a in (rhs, U, gradp, rAU))
+    out = np.empty(n3)
+    ctx.check(ctx.lib.cfdxg_build_hbya(ctx.handle, mesh.handle, handles, N.ptr(b), N.ptr(u), N.ptr(g), N.ptr(r),
+                                       N.CFDXG_MEM_HOST, N.ptr(out)), "build_hbya")
+    return out
+
+
 def gauss_gradient_with_boundary(mesh: Mesh, p, p_bc_fixed=None, p_bc_value=None):
     ctx, hm = mesh.ctx, mesh.host
     pp = _f64(p, hm.n_cells)

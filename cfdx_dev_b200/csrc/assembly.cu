@@ -5,15 +5,21 @@
 // compute_cell_geometry(_oriented) (core/geometry/cell_geometry.h:49-147) and the
 // two-pass orientation of build_fv_geometry (physics/finite_volume_transport.h:92-176);
 // compute_geometry_cache (core/geometry/geometry_cache.h:66-237) yields the same
-// values.  Assembly is cell-centric: one thread per cell recomputes the face
-// quantities of its own faces (identical inputs and operations from either side
-// of a face) and sums them in the order the reference does -- cell-face order
-// for continuity and the Gauss gradient, global face order for the diagonal
-// and the boundary sources -- so no atomics are needed and every FP64 result
-// is bit-identical to the reference's (this file is compiled without FMA
-// contraction).  Each row of the CSR is written by the thread of its cell.
-// (A variant with one lane per face and the sums formed by the cell's first
-// lane through shuffles measured 1.2-1.4x slower on the 64^3 tet mesh.)
+// values.  The Gauss gradient and the corrector assembly are cell-centric: a
+// thread per cell recomputes the quantities of its faces (identical inputs and
+// operations from either side of a face) and sums them in the order the
+// reference does -- cell-face order for continuity and the gradient, global
+// face order for the diagonal and the boundary sources -- so no atomics are
+// needed and every FP64 result is bit-identical to the reference's (this file
+// is compiled without FMA contraction).  The geometry build also forms
+// per-mesh tables so that no call repeats geometric work: per cell-face slot
+// the face, side and other cell in one 8-byte record (no owner/neighbour
+// lookup chain), the gradient weight of the cell's side, and per face the
+// corrector's d, e and Sf . e (no square roots or divisions of geometry per
+// call).  (A warp-per-tile variant with one lane per slot and the per-cell
+// sums formed in order through shuffles was bit-identical but measured 1.8x
+// slower for the assembly on the 64^3 tets: the shuffles cost more
+// instructions than the extra parallelism saved.)
 #include <algorithm>
 #include <cmath>
 #include <numeric>
@@ -28,6 +34,7 @@ constexpr int kT = 128;
 constexpr int kMaxCellFaces = 16;
 constexpr int kPatchSymmetry = 3;
 constexpr int kPatchEmpty = 6;
+constexpr int kOtherSide = int(0x80000000u);   // slot record: the cell is the face's neighbour
 
 struct D3 {
     double x, y, z;
@@ -130,6 +137,7 @@ struct MeshView {
     int nc, nf;
     const int *co, *cf, *cs, *owner, *neigh, *patch, *ptype;
     const double *fc, *sf, *cc, *vol;
+    const double* geo;   // per-face d, e, Sf . e (face-loop table), null until built
 };
 
 struct BcView {
@@ -138,28 +146,45 @@ struct BcView {
     int n_patches;
 };
 
-// steady_incompressible_solver.h:1914-1935
-__device__ __forceinline__ double ortho_coefficient(D3 S, D3 dvec, D3 dau, int* status) {
-    const double d = mag(dvec), area = mag(S);
-    if (!(d > 0.0) || !isfinite(d) || !(area > 0.0) || !isfinite(area)) atomicOr(status, kStatusGeometry);
-    const D3 e{dvec.x / d, dvec.y / d, dvec.z / d};
-    const double oa = dot(S, e);
-    if (!(oa > 0.0) || !isfinite(oa)) atomicOr(status, kStatusGeometry);
-    const double rfn = dau.x * e.x * e.x + dau.y * e.y * e.y + dau.z * e.z * e.z;
-    const double coefficient = rfn * oa / d;
+// Geometry of one face as the corrector uses it (pressure_face_orthogonal_coefficient,
+// steady_incompressible_solver.h:1914-1935, and the same terms of
+// pressure_face_nonorthogonal_flux, :1941-1965): d = |dvec|, e = dvec / d and
+// oa = Sf . e, with dvec = Cn - Co on an interior face and Cf - Co on a
+// boundary face.  They depend on the geometry only, so k_face_terms forms them
+// once per mesh with exactly these operations; the corrector reads them back
+// and forms rfn = sum_d dAU_d e_d^2, which depends on rAU.  (The area check of
+// those functions is the geometry build's: Sf never changes.)
+struct FaceTerms {
+    D3 e;
+    double d, oa, rfn;
+};
+
+// per-face table layout (SoA, nf each): d, e.x, e.y, e.z, oa
+constexpr int kFaceTermArrays = 5;
+
+__device__ __forceinline__ FaceTerms face_terms(const double* __restrict__ geo, int nf, int f, D3 dau,
+                                                int* status) {
+    FaceTerms t;
+    t.d = geo[f];
+    t.e = D3{geo[nf + f], geo[2 * nf + f], geo[3 * nf + f]};
+    t.oa = geo[4 * nf + f];
+    if (!(t.d > 0.0) || !isfinite(t.d)) atomicOr(status, kStatusGeometry);
+    if (!(t.oa > 0.0) || !isfinite(t.oa)) atomicOr(status, kStatusGeometry);
+    t.rfn = dau.x * t.e.x * t.e.x + dau.y * t.e.y * t.e.y + dau.z * t.e.z * t.e.z;
+    return t;
+}
+
+// :1914-1935 -- rfn (Sf . e) / d
+__device__ __forceinline__ double ortho_coefficient(const FaceTerms& t, int* status) {
+    const double coefficient = t.rfn * t.oa / t.d;
     if (!isfinite(coefficient)) atomicOr(status, kStatusGeometry);
     return coefficient;
 }
 
-// steady_incompressible_solver.h:1941-1965
-__device__ __forceinline__ double nonortho_flux(D3 S, D3 dvec, D3 dau, D3 gp, int* status) {
-    const double d = mag(dvec);
-    if (!(d > 0.0) || !isfinite(d)) atomicOr(status, kStatusGeometry);
-    const D3 e{dvec.x / d, dvec.y / d, dvec.z / d};
-    const double oa = dot(S, e);
-    const double rfn = dau.x * e.x * e.x + dau.y * e.y * e.y + dau.z * e.z * e.z;
+// :1941-1965 -- (dAU o grad p) . Sf - rfn (grad p . e)(Sf . e)
+__device__ __forceinline__ double nonortho_flux(const FaceTerms& t, D3 S, D3 dau, D3 gp, int* status) {
     const double full = dau.x * gp.x * S.x + dau.y * gp.y * S.y + dau.z * gp.z * S.z;
-    const double implicit_flux = rfn * dot(gp, e) * oa;
+    const double implicit_flux = t.rfn * dot(gp, t.e) * t.oa;
     const double deferred = full - implicit_flux;
     if (!isfinite(deferred)) atomicOr(status, kStatusGeometry);
     return deferred;
@@ -173,28 +198,27 @@ __device__ __forceinline__ D3 face_dau(int o, int n, int nc, const double* vol, 
             wo * vol[o] * rau[2 * nc + o] + wn * vol[n] * rau[2 * nc + n]};
 }
 
-// rhie_chow_pressure_flux_internal (:1967-2024) for interior face f; also returns the
-// implicit coefficient (the pressure-matrix face coefficient before rho).
-__device__ __forceinline__ double rc_internal(const MeshView& m, int f, const double* p, const double* grad,
-                                              const double* rau, double rho, double* implicit_out, int* status) {
-    const int o = m.owner[f], n = m.neigh[f];
+// rhie_chow_pressure_flux_internal (:1967-2024) for the interior face f with
+// owner o and neighbour n; also returns the implicit coefficient (the
+// pressure-matrix face coefficient before rho).
+__device__ __forceinline__ double rc_internal(const MeshView& m, int f, int o, int n, const double* p,
+                                              const double* grad, const double* rau, double rho,
+                                              double* implicit_out, int* status) {
     const D3 S = ld3(m.sf, m.nf, f);
-    const double area = mag(S);
-    if (!(area > 0.0) || !isfinite(area)) atomicOr(status, kStatusGeometry);
-    const D3 dvec = sub(ld3(m.cc, m.nc, n), ld3(m.cc, m.nc, o));
     const double wn = 0.5, wo = 1.0 - wn;
     const D3 dau = face_dau(o, n, m.nc, m.vol, rau);
     const D3 gp{wo * grad[o] + wn * grad[n], wo * grad[m.nc + o] + wn * grad[m.nc + n],
                 wo * grad[2 * m.nc + o] + wn * grad[2 * m.nc + n]};
-    const double ic = ortho_coefficient(S, dvec, dau, status);
-    const double no = nonortho_flux(S, dvec, dau, gp, status);
+    const FaceTerms t = face_terms(m.geo, m.nf, f, dau, status);
+    const double ic = ortho_coefficient(t, status);
+    const double no = nonortho_flux(t, S, dau, gp, status);
     if (implicit_out) *implicit_out = ic;
     return rho * (ic * (p[n] - p[o]) + no);
 }
 
-// make_mass_flux (:1842-1905), zero-gradient velocity boundaries
-__device__ __forceinline__ double mass_flux(const MeshView& m, int f, const double* U, double rho) {
-    const int o = m.owner[f], n = m.neigh[f];
+// make_mass_flux (:1842-1905) on face f with owner o and neighbour n (< 0 on
+// the boundary), zero-gradient velocity boundaries
+__device__ __forceinline__ double mass_flux(const MeshView& m, int f, int o, int n, const double* U, double rho) {
     D3 Uf = ld3(U, m.nc, o);
     if (n >= 0) {
         const double wn = 0.5;
@@ -207,16 +231,15 @@ __device__ __forceinline__ double mass_flux(const MeshView& m, int f, const doub
 }
 
 // Fixed-pressure boundary coefficient and source (:8130-8175 / :2176-2205)
-__device__ __forceinline__ void fixed_boundary(const MeshView& m, int f, const double* p, const double* grad,
+__device__ __forceinline__ void fixed_boundary(const MeshView& m, int f, int o, const double* p, const double* grad,
                                                const double* rau, double rho, double value,
                                                double* coeff, double* source, int* status) {
-    const int o = m.owner[f];
-    const D3 dvec = sub(ld3(m.fc, m.nf, f), ld3(m.cc, m.nc, o));
     const D3 S = ld3(m.sf, m.nf, f);
     const D3 dau{m.vol[o] * rau[o], m.vol[o] * rau[m.nc + o], m.vol[o] * rau[2 * m.nc + o]};
-    const double bc = ortho_coefficient(S, dvec, dau, status);
+    const FaceTerms t = face_terms(m.geo, m.nf, f, dau, status);
+    const double bc = ortho_coefficient(t, status);
     const D3 gp = ld3(grad, m.nc, o);
-    const double deferred = nonortho_flux(S, dvec, dau, gp, status);
+    const double deferred = nonortho_flux(t, S, dau, gp, status);
     *coeff = bc;
     *source = rho * (bc * (value - p[o]) + deferred);
 }
@@ -229,26 +252,29 @@ __device__ __forceinline__ bool boundary_fixed(const MeshView& m, const BcView& 
     return true;
 }
 
-// gauss_gradient_with_boundary (:1634-1744), single sweep, distance weight
-__global__ void k_gauss_gradient(MeshView m, BcView bc, const double* __restrict__ p, double* grad, int* status) {
+// gauss_gradient_with_boundary (:1634-1744), single sweep, distance weight:
+// a thread per cell over its slots in cell-face order.  The slot records give
+// the face, the side and the other cell in one load, and the interpolation
+// weight of the cell's side comes from the table (no face-centre or
+// cell-centre reads, no square roots or divisions per call).
+__global__ void k_gauss_gradient(MeshView m, BcView bc, const int2* __restrict__ rec,
+                                 const double* __restrict__ wslot, const double* __restrict__ p, double* grad,
+                                 int* status) {
     const int c = blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= m.nc) return;
+    const int b = m.co[c], e = m.co[c + 1];
+    const double pc = p[c];
     D3 sum{0.0, 0.0, 0.0};
-    const D3 cc = ld3(m.cc, m.nc, c);
-    for (int k = m.co[c]; k < m.co[c + 1]; ++k) {
-        const int f = m.cf[k];
-        const bool own = m.owner[f] == c;
+#pragma unroll 4
+    for (int k = b; k < e; ++k) {
+        const int2 r = rec[k];
+        const int f = r.x & 0x7fffffff;
         D3 S = ld3(m.sf, m.nf, f);
-        if (!own) S = mul(S, -1.0);
-        double vf = p[c];
-        if (m.neigh[f] >= 0) {
-            const int other = own ? m.neigh[f] : m.owner[f];
-            const D3 fcv = ld3(m.fc, m.nf, f);
-            const double dc = mag(sub(fcv, cc));
-            const double dn = mag(sub(ld3(m.cc, m.nc, other), fcv));
-            if (!(dc + dn > 0.0)) atomicOr(status, kStatusGeometry);
-            const double w = dn / (dc + dn);
-            vf = w * p[c] + (1.0 - w) * p[other];
+        if (r.x < 0) S = mul(S, -1.0);
+        double vf = pc;
+        if (r.y >= 0) {
+            const double w = wslot[k];
+            vf = w * pc + (1.0 - w) * p[r.y];
         } else {
             const int pt = m.patch[f];
             if (pt >= 0 && m.ptype[pt] == kPatchEmpty) continue;
@@ -263,12 +289,16 @@ __global__ void k_gauss_gradient(MeshView m, BcView bc, const double* __restrict
     grad[c] = gx; grad[m.nc + c] = gy; grad[2 * m.nc + c] = gz;
 }
 
-// Pressure-corrector block (:8048-8181): one thread per cell writes its CSR row and b.
-__global__ void k_pressure_assembly(MeshView m, BcView bc, const double* __restrict__ U,
-                                    const double* __restrict__ rau, const double* __restrict__ p,
-                                    const double* __restrict__ grad, double rho, const int* __restrict__ slot,
-                                    const int* __restrict__ diag_pos, double* __restrict__ values,
-                                    double* __restrict__ b, double* __restrict__ phi_out, int* status) {
+// Pressure-corrector block (:8048-8181): one thread per cell writes its CSR
+// row and b.  Continuity is summed in cell-face order, the diagonal and the
+// fixed-pressure boundary terms in global face order (the per-cell sorted
+// permutation cs), as the reference sums them.
+__global__ void k_pressure_assembly(MeshView m, BcView bc, const int2* __restrict__ rec,
+                                    const double* __restrict__ U, const double* __restrict__ rau,
+                                    const double* __restrict__ p, const double* __restrict__ grad, double rho,
+                                    const int* __restrict__ slot, const int* __restrict__ diag_pos,
+                                    double* __restrict__ values, double* __restrict__ b,
+                                    double* __restrict__ phi_out, int* status) {
     const int c = blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= m.nc) return;
     const int beg = m.co[c], nfc = m.co[c + 1] - beg;
@@ -276,34 +306,37 @@ __global__ void k_pressure_assembly(MeshView m, BcView bc, const double* __restr
     double coeff[kMaxCellFaces];
     double cont = 0.0;
     for (int k = 0; k < nfc; ++k) {
-        const int f = m.cf[beg + k];
-        const bool own = m.owner[f] == c;
-        const double phi = mass_flux(m, f, U, rho);
+        const int2 r = rec[beg + k];
+        const int f = r.x & 0x7fffffff;
+        const bool own = r.x >= 0;
+        const int o = own ? c : r.y, n = own ? r.y : c;
+        const double phi = mass_flux(m, f, o, n, U, rho);
         if (phi_out && own) phi_out[f] = phi;
         cont += own ? phi : -phi;
         coeff[k] = 0.0;
-        if (m.neigh[f] >= 0) {
+        if (r.y >= 0) {
             double ic;
-            const double rc = rc_internal(m, f, p, grad, rau, rho, &ic, status);
+            const double rc = rc_internal(m, f, o, n, p, grad, rau, rho, &ic, status);
             cont += own ? -rc : rc;
             coeff[k] = rho * ic;
         }
     }
     double diag = 0.0;
-    for (int r = 0; r < nfc; ++r) {
-        const int k = m.cs[beg + r];
-        if (m.neigh[m.cf[beg + k]] >= 0) diag += coeff[k];
+    for (int q = 0; q < nfc; ++q) {
+        const int k = m.cs[beg + q];
+        if (rec[beg + k].y >= 0) diag += coeff[k];
     }
     double acc = 0.0 + diag;
     double bb = -cont;
-    for (int r = 0; r < nfc; ++r) {
-        const int k = m.cs[beg + r];
-        const int f = m.cf[beg + k];
-        if (m.neigh[f] >= 0) continue;
+    for (int q = 0; q < nfc; ++q) {
+        const int k = m.cs[beg + q];
+        const int2 r = rec[beg + k];
+        if (r.y >= 0) continue;
+        const int f = r.x & 0x7fffffff;
         double value;
         if (!boundary_fixed(m, bc, f, &value)) continue;
         double bcoef, source;
-        fixed_boundary(m, f, p, grad, rau, rho, value, &bcoef, &source, status);
+        fixed_boundary(m, f, c, p, grad, rau, rho, value, &bcoef, &source, status);
         acc += rho * bcoef;
         bb += source;
     }
@@ -326,7 +359,7 @@ __global__ void k_rhie_chow_flux(MeshView m, BcView bc, const double* __restrict
     if (n >= 0) {
         const double wn = 0.5;
         Hf = add(mul(Hf, 1.0 - wn), mul(ld3(U, m.nc, n), wn));
-        correction = rc_internal(m, f, p, grad, rau, rho, nullptr, status);
+        correction = rc_internal(m, f, o, n, p, grad, rau, rho, nullptr, status);
     } else {
         const int pt = m.patch[f];
         if (pt >= 0 && (m.ptype[pt] == kPatchEmpty || m.ptype[pt] == kPatchSymmetry)) {
@@ -336,11 +369,53 @@ __global__ void k_rhie_chow_flux(MeshView m, BcView bc, const double* __restrict
         double value;
         if (boundary_fixed(m, bc, f, &value)) {
             double bcoef, source;
-            fixed_boundary(m, f, p, grad, rau, rho, value, &bcoef, &source, status);
+            fixed_boundary(m, f, o, p, grad, rau, rho, value, &bcoef, &source, status);
             correction = source;
         }
     }
     flux[f] = rho * dot(Hf, ld3(m.sf, m.nf, f)) - correction;
+}
+
+// The corrector's geometric face terms (see FaceTerms): d, e and Sf . e with
+// dvec = Cn - Co (interior) or Cf - Co (boundary), the operations of
+// pressure_face_orthogonal_coefficient (:1914-1935).
+__global__ void k_face_terms(int nf, int nc, const int* __restrict__ owner, const int* __restrict__ neigh,
+                             const double* __restrict__ fc, const double* __restrict__ sf,
+                             const double* __restrict__ cc, double* geo) {
+    const int f = blockIdx.x * blockDim.x + threadIdx.x;
+    if (f >= nf) return;
+    const int o = owner[f], n = neigh[f];
+    const D3 dvec = n >= 0 ? sub(ld3(cc, nc, n), ld3(cc, nc, o)) : sub(ld3(fc, nf, f), ld3(cc, nc, o));
+    const double d = mag(dvec);
+    const D3 e{dvec.x / d, dvec.y / d, dvec.z / d};
+    geo[f] = d;
+    geo[nf + f] = e.x;
+    geo[2 * nf + f] = e.y;
+    geo[3 * nf + f] = e.z;
+    geo[4 * nf + f] = dot(ld3(sf, nf, f), e);
+}
+
+// Gauss-gradient weight of each interior slot from its cell's side,
+// w = dn / (dc + dn) with dc = |Cf - Cc| and dn = |Cother - Cf| (:1660-1700):
+// geometry only, so formed once with the geometry.
+__global__ void k_slot_weights(int nc, int nf, const int* __restrict__ co, const int2* __restrict__ rec,
+                               const double* __restrict__ fc, const double* __restrict__ cc, double* w,
+                               int* status) {
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= nc) return;
+    const D3 ccv = ld3(cc, nc, c);
+    for (int k = co[c]; k < co[c + 1]; ++k) {
+        const int2 r = rec[k];
+        if (r.y < 0) {
+            w[k] = 0.0;
+            continue;
+        }
+        const D3 fcv = ld3(fc, nf, r.x & 0x7fffffff);
+        const double dc = mag(sub(fcv, ccv));
+        const double dn = mag(sub(ld3(cc, nc, r.y), fcv));
+        if (!(dc + dn > 0.0)) atomicOr(status, kStatusGeometry);
+        w[k] = dn / (dc + dn);
+    }
 }
 
 // assemble_cell_diffusion_matrix (core/solvers/scalar_diffusion.h:39-163), one thread per cell.
@@ -381,17 +456,69 @@ __global__ void k_diffusion_assembly(MeshView m, const double* __restrict__ bcv,
     rhs[c] = r;
 }
 
+// The build_hbya step of solve_steady_incompressible (:6430-6465), one
+// thread per (cell, component): h = rhs + gradp * V (:6437), minus the
+// off-diagonal products of the component's momentum row in CSR order
+// (:6438-6443), HbyA = rAU * h (:6459); non-finite HbyA is flagged (:6460).
+__global__ void k_build_hbya(int n, const int* __restrict__ ro, const int* __restrict__ co,
+                             const double* __restrict__ va0, const double* __restrict__ va1,
+                             const double* __restrict__ va2, const double* __restrict__ rhs,
+                             const double* __restrict__ U, const double* __restrict__ gradp,
+                             const double* __restrict__ vol, const double* __restrict__ rau,
+                             double* __restrict__ hbya, int* status) {
+    const int64_t t = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (t >= 3 * static_cast<int64_t>(n)) return;
+    const int d = static_cast<int>(t / n), c = static_cast<int>(t % n);
+    const double* va = d == 0 ? va0 : (d == 1 ? va1 : va2);
+    const double* Ud = U + static_cast<int64_t>(d) * n;
+    double h = rhs[t] + gradp[t] * vol[c];
+    for (int k = ro[c]; k < ro[c + 1]; ++k) {
+        const int col = co[k];
+        if (col != c) h -= va[k] * Ud[col];
+    }
+    const double v = rau[t] * h;
+    hbya[t] = v;
+    if (!isfinite(v)) atomicOr(status, kStatusNonFinite);
+}
+
 MeshView view(const cfdxg_mesh* m) {
     return {static_cast<int>(m->n_cells), static_cast<int>(m->n_faces), m->cell_off.get(), m->cell_face.get(),
             m->cell_sorted.get(), m->owner.get(), m->neigh.get(), m->patch_of_face.get(), m->patch_type.get(),
-            m->face_centre.get(), m->face_sf.get(), m->cell_centre.get(), m->cell_volume.get()};
+            m->face_centre.get(), m->face_sf.get(), m->cell_centre.get(), m->cell_volume.get(),
+            m->face_geo.get()};
 }
 
-// A thread per cell (the cell-centric loop above).  (Unrolling the face loop
-// into load phases raised it to 118 registers and measured 1.25x slower.)
 void launch_gradient(cfdxg_context* ctx, const cfdxg_mesh* m, const MeshView& mv, const BcView& bc,
                      const double* p, double* grad) {
-    k_gauss_gradient<<<blocks_for(m->n_cells, kT), kT, 0, ctx->stream>>>(mv, bc, p, grad, ctx->scratch.status);
+    k_gauss_gradient<<<blocks_for(m->n_cells, kT), kT, 0, ctx->stream>>>(mv, bc, m->slot_rec.get(), m->slot_w.get(),
+                                                                        p, grad, ctx->scratch.status);
+    check_launch(ctx);
+}
+
+// The face-loop tables of the mesh (slot records, gradient weights, face
+// terms); called by the geometry build, after the geometry.
+void build_face_tables(cfdxg_context* ctx, cfdxg_mesh* m) {
+    const int64_t nc = m->n_cells, nf = m->n_faces, nslot = static_cast<int64_t>(m->h_cell_face.size());
+    std::vector<int2> rec(nslot);
+    for (int64_t c = 0; c < nc; ++c)
+        for (int64_t k = m->h_cell_off[c]; k < m->h_cell_off[c + 1]; ++k) {
+            const int64_t f = m->h_cell_face[k];
+            const bool own = m->h_owner[f] == c;
+            const int64_t n = m->h_neigh[f];
+            rec[k].x = static_cast<int>(f) | (own ? 0 : kOtherSide);
+            rec[k].y = n < 0 ? -1 : static_cast<int>(own ? n : m->h_owner[f]);
+        }
+    m->slot_rec.upload(rec, ctx->stream);
+    m->slot_w.resize(static_cast<std::size_t>(nslot));
+    k_slot_weights<<<blocks_for(nc, kT), kT, 0, ctx->stream>>>(
+        static_cast<int>(nc), static_cast<int>(nf), m->cell_off.get(), m->slot_rec.get(), m->face_centre.get(),
+        m->cell_centre.get(), m->slot_w.get(), ctx->scratch.status);
+    check_launch(ctx);
+    m->face_geo.resize(static_cast<std::size_t>(kFaceTermArrays) * nf);
+    k_face_terms<<<blocks_for(nf, kT), kT, 0, ctx->stream>>>(static_cast<int>(nf), static_cast<int>(nc),
+                                                             m->owner.get(), m->neigh.get(), m->face_centre.get(),
+                                                             m->face_sf.get(), m->cell_centre.get(),
+                                                             m->face_geo.get());
     check_launch(ctx);
 }
 
@@ -596,6 +723,7 @@ extern "C" int cfdxg_geometry_build(cfdxg_context* ctx, cfdxg_mesh* m) {
                                                       m->face_centre.get(), m->face_sf.get(), m->cell_centre.get(),
                                                       m->cell_volume.get(), st);
     check_launch(ctx);
+    build_face_tables(ctx, m);
     check_device_status(ctx, "geometry");
     m->geometry_ready = true;
     ctx->error.clear();
@@ -723,8 +851,8 @@ extern "C" int cfdxg_assemble_pressure_correction(cfdxg_context* ctx, cfdxg_mesh
     }
     {
         ProfScope ps(ctx, "pressure_assembly", assembly_bytes(m, A->nnz));
-        k_pressure_assembly<<<blocks_for(nc, kT), kT, 0, ctx->stream>>>(mv, bc, U.get(), rau.get(), pin.get(), g,
-                                                                        rho, m->pattern.d_slot.get(),
+        k_pressure_assembly<<<blocks_for(nc, kT), kT, 0, ctx->stream>>>(mv, bc, m->slot_rec.get(), U.get(), rau.get(),
+                                                                        pin.get(), g, rho, m->pattern.d_slot.get(),
                                                                         m->pattern.d_diag.get(), A->va.get(),
                                                                         bout.get(), phi.get(), ctx->scratch.status);
         check_launch(ctx);
@@ -874,6 +1002,46 @@ extern "C" int cfdxg_rhie_chow_flux_noalloc(cfdxg_context* ctx, cfdxg_mesh* m, c
                                                                  ctx->scratch.status);
     check_launch(ctx);
     check_device_status(ctx, "make_rhie_chow_mass_flux (no-alloc)");
+    ctx->error.clear();
+    return CFDXG_OK;
+    CFDXG_GUARD_END(ctx)
+}
+
+extern "C" int cfdxg_build_hbya(cfdxg_context* ctx, cfdxg_mesh* m, const cfdxg_matrix* const* momentum,
+                                const double* rhs, const double* U, const double* gradp, const double* rAU,
+                                int32_t mem, double* HbyA) {
+    if (!ctx || !m) return CFDXG_ERR_INVALID_ARGUMENT;
+    CFDXG_GUARD_BEGIN
+    NvtxRange nvtx_range("cfdxg.build_hbya");
+    check_mem_flag(mem);
+    require_geometry(m);
+    if (!momentum || !rhs || !U || !gradp || !rAU || !HbyA)
+        throw Error(CFDXG_ERR_INVALID_ARGUMENT, "missing argument");
+    const int64_t nc = m->n_cells;
+    for (int d = 0; d < 3; ++d) {
+        const cfdxg_matrix* M = momentum[d];
+        if (!M || M->n != nc) throw Error(CFDXG_ERR_INVALID_ARGUMENT, "momentum matrix size differs from the mesh");
+        if (d > 0 && (M->nnz != momentum[0]->nnz || M->host.ro != momentum[0]->host.ro ||
+                      M->host.co != momentum[0]->host.co))
+            throw Error(CFDXG_ERR_INVALID_ARGUMENT, "the three momentum matrices must share one pattern");
+    }
+    In<double> b(ctx, rhs, 3 * nc, mem), u(ctx, U, 3 * nc, mem), gp(ctx, gradp, 3 * nc, mem),
+        rau(ctx, rAU, 3 * nc, mem);
+    Out<double> out(ctx, HbyA, 3 * nc, mem);
+    clear_status(ctx);
+    {
+        // momentum values of three components + pattern, rhs/U/gradp/rAU reads, V, HbyA write
+        ProfScope ps(ctx, "build_hbya", 3.0 * 8.0 * momentum[0]->nnz + 4.0 * (nc + 1) + 4.0 * momentum[0]->nnz +
+                                            (4 * 24.0 + 8.0 + 24.0) * nc);
+        k_build_hbya<<<blocks_for(3 * nc, kT), kT, 0, ctx->stream>>>(
+            static_cast<int>(nc), momentum[0]->ro.get(), momentum[0]->co.get(), momentum[0]->va.get(),
+            momentum[1]->va.get(), momentum[2]->va.get(), b.get(), u.get(), gp.get(), m->cell_volume.get(),
+            rau.get(), out.get(), ctx->scratch.status);
+        check_launch(ctx);
+    }
+    out.finish();
+    const int st = read_status(ctx);
+    if (st & kStatusNonFinite) throw Error(CFDXG_ERR_NONFINITE, "solve_steady_incompressible: non-finite HbyA");
     ctx->error.clear();
     return CFDXG_OK;
     CFDXG_GUARD_END(ctx)

@@ -164,6 +164,7 @@ void amg_setup_impl(cfdxg_context* ctx, cfdxg_amg* amg, cfdxg_matrix* A) {
     if (amg->opts.precision == CFDXG_PRECISION_FP32_VCYCLE) {
         up.coarse_dense_limit = amg->opts.coarse_dense_limit;
         up.half_values = amg->opts.half_values != 0;
+        up.dense_fp64 = amg->opts.dense_fp64 != 0;
         d32 = upload_hierarchy<float>(ctx, staged, up);
     } else {
         d64 = upload_hierarchy<double>(ctx, staged, up);
@@ -381,6 +382,7 @@ extern "C" int cfdxg_amg_options_default(cfdxg_amg_options* o) {
     o->coarse_post_sweeps = -1;
     o->narrow_columns = 1;
     o->half_values = 1;
+    o->dense_fp64 = 0;
     return CFDXG_OK;
 }
 

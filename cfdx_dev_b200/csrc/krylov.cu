@@ -236,6 +236,137 @@ __global__ void k_multi_axpy(int n, const double* __restrict__ V, int i0, int c,
     }
 }
 
+// ---- fused classical Gram-Schmidt passes (the CGS2 option, at most kChunk
+// basis vectors): three passes over the basis per Arnoldi step instead of
+// four, and the two norms of w taken inside them (plain sums of squares: this
+// option is the library's own orthogonalisation, not the reference's MGS2).
+// They run on a fixed grid (a partition that depends only on n and the GPU,
+// so the sums are deterministic) and reduce all outputs at once: per warp by
+// a fixed butterfly, per block in warp order, and over the blocks by one warp
+// per output in a fixed lane/butterfly order.  The first pass keeps eight
+// blocks per SM (its loads need the warps); the fused update-and-dot pass,
+// at 120 registers, takes kGsBlocksPerSm blocks per SM, the most that fit at
+// once, so its reduction tail runs once (3.9 instead of 6.1 ms per eight
+// 64^3 solves).
+constexpr int kGsBlocksPerSm = 2;
+constexpr int kGsWarps = kT / 32;
+
+// out[q] = grid sum of acc[q] for q < c; with EXTRA also out[c] = grid sum of extra.
+template <int NMAX, bool EXTRA>
+__device__ __forceinline__ void grid_multi_sum(const double (&acc)[NMAX], int c, double extra, double* partial,
+                                               unsigned* ticket, double* out) {
+    __shared__ double wsum[kGsWarps][NMAX + 1];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+    for (int q = 0; q < NMAX; ++q) {
+        if (q < c) {
+            double v = acc[q];
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+            if (lane == 0) wsum[warp][q] = v;
+        }
+    }
+    if (EXTRA) {
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) extra += __shfl_xor_sync(0xffffffffu, extra, o);
+        if (lane == 0) wsum[warp][c] = extra;
+        ++c;
+    }
+    __syncthreads();
+    if (threadIdx.x < c) {
+        double t = 0.0;
+#pragma unroll
+        for (int w = 0; w < kGsWarps; ++w) t += wsum[w][threadIdx.x];
+        partial[threadIdx.x * gridDim.x + blockIdx.x] = t;
+    }
+    if (last_block(ticket)) {
+        for (int q = warp; q < c; q += kGsWarps) {
+            double t = 0.0;
+            for (int b = lane; b < static_cast<int>(gridDim.x); b += 32) t += partial[q * gridDim.x + b];
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) t += __shfl_xor_sync(0xffffffffu, t, o);
+            if (lane == 0) out[q] = t;
+        }
+        if (threadIdx.x == 0) *ticket = 0;
+    }
+}
+
+// out[q] = v_q . w for q < c, and out[c] = w . w (the Arnoldi action norm squared)
+__global__ void __launch_bounds__(kT) k_gs_first(int n, const double* __restrict__ V, int c,
+                                                 const double* __restrict__ w, double* partial, unsigned* ticket,
+                                                 double* out) {
+    pdl_entry();
+    double acc[kChunk];
+#pragma unroll
+    for (int q = 0; q < kChunk; ++q) acc[q] = 0.0;
+    double ww = 0.0;
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
+        const double wk = w[k];
+#pragma unroll
+        for (int q = 0; q < kChunk; ++q)
+            if (q < c) acc[q] += V[static_cast<size_t>(q) * n + k] * wk;
+        ww += wk * wk;
+    }
+    grid_multi_sum<kChunk, true>(acc, c, ww, partial, ticket, out);
+}
+
+// w -= sum_{q<c} h[q] v_q (in q order per element), then out[q] = v_q . w over the updated w
+__global__ void __launch_bounds__(kT) k_gs_axpy_dot(int n, const double* __restrict__ V, int c, const double* h,
+                                                    double* __restrict__ w, double* partial, unsigned* ticket,
+                                                    double* out) {
+    pdl_entry();
+    __shared__ double hs[kChunk];
+    if (threadIdx.x < c) hs[threadIdx.x] = h[threadIdx.x];
+    __syncthreads();
+    double acc[kChunk];
+#pragma unroll
+    for (int q = 0; q < kChunk; ++q) acc[q] = 0.0;
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
+        double vk[kChunk];
+        double wk = w[k];
+#pragma unroll
+        for (int q = 0; q < kChunk; ++q) {
+            vk[q] = q < c ? V[static_cast<size_t>(q) * n + k] : 0.0;
+            if (q < c) wk = wk - hs[q] * vk[q];
+        }
+        w[k] = wk;
+#pragma unroll
+        for (int q = 0; q < kChunk; ++q)
+            if (q < c) acc[q] += vk[q] * wk;
+    }
+    grid_multi_sum<kChunk, false>(acc, c, 0.0, partial, ticket, out);
+}
+
+// w -= sum_{q<c} h[q] v_q, then *norm_out = sqrt(w . w) (NaN when not finite)
+__global__ void k_gs_axpy_norm(int n, const double* __restrict__ V, int c, const double* h,
+                               double* __restrict__ w, double* partial, unsigned* ticket, double* norm_out) {
+    pdl_entry();
+    __shared__ double sm[32];
+    __shared__ double hs[kChunk];
+    if (threadIdx.x < c) hs[threadIdx.x] = h[threadIdx.x];
+    __syncthreads();
+    double ss = 0.0;
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
+        double wk = w[k];
+#pragma unroll
+        for (int q = 0; q < kChunk; ++q)
+            if (q < c) wk = wk - hs[q] * V[static_cast<size_t>(q) * n + k];
+        w[k] = wk;
+        ss += wk * wk;
+    }
+    ss = block_sum(ss, sm);
+    if (threadIdx.x == 0) partial[blockIdx.x] = ss;
+    if (last_block(ticket)) {
+        double t = 0.0;
+        for (int b = threadIdx.x; b < gridDim.x; b += blockDim.x) t += partial[b];
+        t = block_sum(t, sm);
+        if (threadIdx.x == 0) {
+            *norm_out = isfinite(t) ? sqrt(t) : nan("");
+            *ticket = 0;
+        }
+    }
+}
+
 // w = w - c * v   (gmres_solver.h:283 / :289)
 __global__ void k_axpy_neg(int n, double* __restrict__ w, const double* __restrict__ v, const double* c) {
     pdl_entry();
@@ -277,6 +408,12 @@ __global__ void k_update(int n, const double* __restrict__ x, const double* __re
     out[i] = v;
 }
 
+// *to = sqrt(*from) (NaN when *from is not finite)
+__global__ void k_sqrt_slot(const double* from, double* to) {
+    const double v = *from;
+    *to = isfinite(v) ? sqrt(v) : nan("");
+}
+
 __global__ void k_neg(int n, const double* __restrict__ a, double* __restrict__ b) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i < n) b[i] = -a[i];
@@ -291,7 +428,7 @@ struct Workspace {
     int64_t n = 0;
     int m = 0;
     DevBuf<double> V, Z, w, r, ax, best, trial, tmp;
-    DevBuf<double> mpartial;   // kChunk x kWideBlocks partial sums of the multi-dot
+    DevBuf<double> mpartial;   // (kChunk + 1) x kWideBlocks partial sums of the multi-dot
 };
 
 Workspace& workspace(cfdxg_context* ctx, int64_t n, int m) {
@@ -306,7 +443,7 @@ Workspace& workspace(cfdxg_context* ctx, int64_t n, int m) {
         ws->Z.resize(static_cast<size_t>(mm) * n);
         ws->w.resize(n); ws->r.resize(n); ws->ax.resize(n); ws->best.resize(n);
         ws->trial.resize(n); ws->tmp.resize(n);
-        ws->mpartial.resize(static_cast<size_t>(kChunk) * kWideBlocks);
+        ws->mpartial.resize(static_cast<size_t>(kChunk + 1) * kWideBlocks);
         ws->n = n;
         ws->m = mm;
     }
@@ -322,7 +459,12 @@ public:
     int gb() const { return blocks_for(n_, kT); }
     int rb() const { return reduce_blocks(n_); }
 
+    // Live profiler classes (algorithmic bytes: FP64 vectors of n, each read
+    // or written once): krylov_norm, krylov_dot, gram_schmidt_dot,
+    // gram_schmidt_axpy, krylov_scale, true_residual, krylov_update.
+    double nb() const { return 8.0 * n_; }
     void norm2(const double* a, int out) {
+        ProfScope ps(ctx_, "krylov_norm", 2.0 * nb());
         launch_pdl(ctx_->stream, k_absmax, rb(), kT, n_, a, ctx_->scratch.partial, ctx_->scratch.ticket,
                                                 slot(kMax), slot(kInvalid));
         check_launch(ctx_);
@@ -331,17 +473,20 @@ public:
         check_launch(ctx_);
     }
     void dot(const double* a, const double* b, int out) {
+        ProfScope ps(ctx_, "krylov_dot", 2.0 * nb());
         launch_pdl(ctx_->stream, k_dot, rb(), kT, n_, a, b, ctx_->scratch.partial, ctx_->scratch.ticket, slot(out));
         check_launch(ctx_);
     }
     // w -= H[coef] v, then H[out] = u . w
     void axpy_dot(double* w, const double* v, int coef, const double* u, int out) {
+        ProfScope ps(ctx_, "gram_schmidt_axpy_dot", 4.0 * nb());
         launch_pdl(ctx_->stream, k_axpy_dot, rb(), kT, n_, w, v, slot(coef), u, ctx_->scratch.partial,
                                                   ctx_->scratch.ticket, slot(out));
         check_launch(ctx_);
     }
     // w -= H[coef] v, then the norm of w into slot out (two passes, as norm2)
     void axpy_norm2(double* w, const double* v, int coef, int out) {
+        ProfScope ps(ctx_, "gram_schmidt_axpy_norm", 4.0 * nb());
         launch_pdl(ctx_->stream, k_axpy_absmax, rb(), kT, n_, w, v, slot(coef), ctx_->scratch.partial,
                                                      ctx_->scratch.ticket, slot(kMax), slot(kInvalid));
         check_launch(ctx_);
@@ -354,6 +499,7 @@ public:
     void multidot(const double* V, int count, const double* w, int out, double* mpartial) {
         for (int i0 = 0; i0 < count; i0 += kChunk) {
             const int c = std::min(kChunk, count - i0);
+            ProfScope ps(ctx_, "gram_schmidt_dot", (c + 1.0) * nb());
             launch_pdl(ctx_->stream, k_multidot, wb(), kT, n_, V, i0, c, w, mpartial, ctx_->scratch.ticket,
                                                       slot(out + i0));
             check_launch(ctx_);
@@ -364,6 +510,7 @@ public:
         for (int i0 = 0; i0 < count; i0 += kChunk) {
             const int c = std::min(kChunk, count - i0);
             const bool last = i0 + c == count && norm_out >= 0;
+            ProfScope ps(ctx_, "gram_schmidt_axpy", (c + 2.0) * nb());
             if (last)
                 launch_pdl(ctx_->stream, k_multi_axpy<true>, wb(), kT, n_, V, i0, c, slot(coef + i0), w,
                                                                  ctx_->scratch.partial, ctx_->scratch.ticket,
@@ -374,20 +521,53 @@ public:
             check_launch(ctx_);
         }
         if (norm_out >= 0) {
+            ProfScope ps(ctx_, "krylov_norm", nb());
             launch_pdl(ctx_->stream, k_sumsq, rb(), kT, n_, w, slot(kMax), slot(kInvalid), ctx_->scratch.partial,
                                                    ctx_->scratch.ticket, slot(norm_out));
             check_launch(ctx_);
         }
     }
+    // Two passes of classical Gram-Schmidt of w against v_0..v_{count-1}
+    // (count <= kChunk) in three passes over the basis: h1 = V^T w (with the
+    // action norm), w -= V h1 fused with h2 = V^T w, w -= V h2 fused with
+    // ||w||.  Fills slots kH1.., kH2.., kAction and kHnext.
+    int gsb() const { return std::min(kGsBlocksPerSm * ctx_->sm_count, blocks_for(n_, kT)); }
+    void gram_schmidt_cgs2_fused(const double* V, int count, double* w, double* mpartial) {
+        {
+            ProfScope ps(ctx_, "gram_schmidt_dot", (count + 1.0) * nb());
+            launch_pdl(ctx_->stream, k_gs_first, wb(), kT, n_, V, count, static_cast<const double*>(w), mpartial,
+                       ctx_->scratch.ticket, slot(kH1));
+            check_launch(ctx_);
+        }
+        {
+            ProfScope ps(ctx_, "gram_schmidt_axpy_dot", (count + 2.0) * nb());
+            launch_pdl(ctx_->stream, k_gs_axpy_dot, gsb(), kT, n_, V, count, static_cast<const double*>(slot(kH1)), w,
+                       mpartial, ctx_->scratch.ticket, slot(kH2));
+            check_launch(ctx_);
+        }
+        {
+            ProfScope ps(ctx_, "gram_schmidt_axpy_norm", (count + 2.0) * nb());
+            launch_pdl(ctx_->stream, k_gs_axpy_norm, wb(), kT, n_, V, count, static_cast<const double*>(slot(kH2)),
+                       w, ctx_->scratch.partial, ctx_->scratch.ticket, slot(kHnext));
+            check_launch(ctx_);
+        }
+    }
+    void sqrt_slot(int from, int to) {
+        k_sqrt_slot<<<1, 1, 0, ctx_->stream>>>(slot(from), slot(to));
+        check_launch(ctx_);
+    }
     void axpy_neg(double* w, const double* v, int coef) {
+        ProfScope ps(ctx_, "gram_schmidt_axpy", 3.0 * nb());
         launch_pdl(ctx_->stream, k_axpy_neg, gb(), kT, n_, w, v, slot(coef));
         check_launch(ctx_);
     }
     void div(const double* w, int d, double* v) {
+        ProfScope ps(ctx_, "krylov_scale", 2.0 * nb());
         launch_pdl(ctx_->stream, k_div, gb(), kT, n_, w, slot(d), v);
         check_launch(ctx_);
     }
     void residual(const double* b, const double* x, double* r) {
+        ProfScope ps(ctx_, "true_residual", 12.0 * A_->nnz + 4.0 * (n_ + 1) + 3.0 * nb());
         launch_pdl(ctx_->stream, k_true_residual, gb(), kT, n_, A_->ro.get(), A_->co.get(), A_->va.get(), b, x, r);
         check_launch(ctx_);
     }
@@ -399,6 +579,7 @@ public:
         if (used > 0)
             CFDXG_CUDA(cudaMemcpyAsync(slot(kY), y.data(), sizeof(double) * used, cudaMemcpyHostToDevice,
                                        ctx_->stream));
+        ProfScope ps(ctx_, "krylov_update", (used + 2.0) * nb());
         launch_pdl(ctx_->stream, k_update, gb(), kT, n_, x, Z, slot(kY), used, out);
         check_launch(ctx_);
     }
@@ -648,11 +829,20 @@ KrylovResult gmres_solve(cfdxg_context* ctx, const cfdxg_matrix* A, const double
                 E.copy(z(j), v(j));
             }
             E.spmv(z(j), ws->w.get());
-            E.norm2(ws->w.get(), kAction);
+            double* w = ws->w.get();
+            if (controls.classical_gram_schmidt && j + 1 <= kChunk) {
+                // classical Gram-Schmidt twice in three fused passes; the
+                // action norm comes from the first (slot kH1 + j + 1)
+                E.gram_schmidt_cgs2_fused(V, j + 1, w, ws->mpartial.get());
+                E.sqrt_slot(kH1 + j + 1, kAction);
+            } else {
+                E.norm2(w, kAction);
+            }
             // two passes of modified Gram-Schmidt (h = v_i . w; w -= h v_i for
             // i = 0..j, twice), each update fused with the next dot
-            double* w = ws->w.get();
-            if (controls.classical_gram_schmidt) {
+            if (controls.classical_gram_schmidt && j + 1 <= kChunk) {
+                // done above
+            } else if (controls.classical_gram_schmidt) {
                 // two passes of classical Gram-Schmidt: h = V^T w; w -= V h, twice
                 E.multidot(V, j + 1, w, kH1, ws->mpartial.get());
                 E.multi_axpy(V, j + 1, kH1, w, -1);

@@ -54,6 +54,8 @@ struct DevHierarchy {
     int coarse_pre = 6, coarse_post = 6;   // sweeps on levels >= 1
     int coarse_mode = 0;       // 0: 24 Jacobi sweeps, 1: reference dense LU (n <= 16), 2: dense inverse
     DevBuf<float> dense;       // mode 2: the n*n inverse (row-major), formed in FP64, stored FP32
+    DevBuf<double> dense64;    // mode 2 with dense_fp64: the same inverse stored FP64
+    bool dense_fp64 = false;
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
     int64_t graph_kernels = 0;
@@ -79,6 +81,13 @@ struct cfdxg_mesh {
     bool geometry_ready = false;
     cfdxg::DevBuf<double> face_centre, face_sf, cell_centre, cell_volume;
     cfdxg::MeshPattern pattern;
+    // face-loop tables, built with the geometry (assembly.cu): per cell-face
+    // slot (cell-face order) the face id, with bit 31 set where the cell is
+    // the face's neighbour, and the other cell (-1 on the boundary); the Gauss
+    // gradient's interpolation weight of the cell's side; per face the
+    // corrector's geometric terms d, e, Sf . e (5 x n_faces, SoA)
+    cfdxg::DevBuf<int2> slot_rec;
+    cfdxg::DevBuf<double> slot_w, face_geo;
     // per-call boundary table and gradient scratch, kept so the face-loop entry
     // points neither allocate nor free device memory after their first call
     cfdxg::DevBuf<int> bc_fixed;
@@ -157,6 +166,7 @@ struct UploadOptions {
     bool reference_order = false; // one thread per row everywhere (the reference's sums)
     bool narrow_columns = true;   // int16 column offsets on one-thread-per-row levels
     bool half_values = false;     // FP32: FP16 row-scaled matrix values
+    bool dense_fp64 = false;      // FP32: the dense coarse inverse stored (and applied) in FP64
 };
 
 template <class T>

@@ -65,8 +65,10 @@ __device__ __forceinline__ T ldv(const VS* __restrict__ p, int k) {
     else return p[k];
 }
 
-template <class T, int TPR>
-__device__ __forceinline__ T row_reduce(T s, int lane) {
+// NWARPS: warps of the launching block (rows wider than a warp are combined
+// through a per-warp shared array of that size).
+template <class T, int TPR, int NWARPS>
+__device__ __forceinline__ T row_reduce_n(T s, int lane) {
     if (TPR > 1) {
         constexpr int W = TPR < 32 ? TPR : 32;
 #pragma unroll
@@ -75,7 +77,7 @@ __device__ __forceinline__ T row_reduce(T s, int lane) {
     if constexpr (TPR > 32) {
         // rows spread over TPR / 32 warps of the block (levels with few, long
         // rows): warp partials summed in warp order by the row's first thread
-        __shared__ T part[kT / 32];
+        __shared__ T part[NWARPS];
         const int warp = threadIdx.x >> 5;
         if ((threadIdx.x & 31) == 0) part[warp] = s;
         __syncthreads();
@@ -88,6 +90,9 @@ __device__ __forceinline__ T row_reduce(T s, int lane) {
     }
     return s;
 }
+
+template <class T, int TPR>
+__device__ __forceinline__ T row_reduce(T s, int lane) { return row_reduce_n<T, TPR, kT / 32>(s, lane); }
 
 template <class T, int TPR, class CI = int, class VS = T>
 __device__ __forceinline__ T row_dot(int b, int e, int lane, const CI* __restrict__ co,
@@ -325,15 +330,15 @@ __global__ void k_dense_lu_reference(int n, const int* __restrict__ ro, const in
 // x = Ainv * r, one warp per row: the inverse (formed in FP64) is read as
 // FP32 -- half the bytes of the largest single read of the FP32 cycle -- and
 // the products are summed in FP64.
-template <class T>
-__global__ void k_dense_inverse_apply(int n, const float* __restrict__ inv, const T* __restrict__ r,
+template <class T, class S>
+__global__ void k_dense_inverse_apply(int n, const S* __restrict__ inv, const T* __restrict__ r,
                                       T* __restrict__ x, int* status) {
     pdl_entry();
     const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int lane = threadIdx.x & 31;
     if (warp >= n) return;
     double s = 0.0;
-    const float* row = inv + static_cast<size_t>(warp) * n;
+    const S* row = inv + static_cast<size_t>(warp) * n;
 #pragma unroll 4
     for (int j = lane; j < n; j += 32) s += static_cast<double>(row[j]) * static_cast<double>(r[j]);
     for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
@@ -397,11 +402,12 @@ __global__ void k_gj_eliminate(int n, double* a, const double* factors, int k) {
     a[idx] -= f * a[static_cast<size_t>(k) * 2 * n + j];
 }
 
-__global__ void k_gj_extract(int n, const double* a, float* inv) {
+template <class S>
+__global__ void k_gj_extract(int n, const double* a, S* inv) {
     const size_t idx = static_cast<size_t>(blockIdx.x) * blockDim.x + threadIdx.x;
     if (idx >= static_cast<size_t>(n) * n) return;
     const int i = static_cast<int>(idx / n), j = static_cast<int>(idx % n);
-    inv[idx] = static_cast<float>(a[static_cast<size_t>(i) * 2 * n + n + j]);
+    inv[idx] = static_cast<S>(a[static_cast<size_t>(i) * 2 * n + n + j]);
 }
 
 __global__ void k_gj_init(int n, const int* ro, const int* co, const double* va, double* a) {
@@ -654,7 +660,8 @@ void build_dense_inverse_dev(cfdxg_context* ctx, DevHierarchy<T>& d, int n, cons
     DevBuf<double> a, f;
     a.resize(static_cast<std::size_t>(n) * 2 * n);
     f.resize(n);
-    d.dense.resize(static_cast<std::size_t>(n) * n);
+    if (d.dense_fp64) d.dense64.resize(static_cast<std::size_t>(n) * n);
+    else d.dense.resize(static_cast<std::size_t>(n) * n);
     k_gj_init<<<blocks_for(n, kT), kT, 0, ctx->stream>>>(n, ro, co, va, a.get());
     check_launch(ctx);
     const size_t total = static_cast<size_t>(n) * 2 * n;
@@ -665,7 +672,12 @@ void build_dense_inverse_dev(cfdxg_context* ctx, DevHierarchy<T>& d, int n, cons
         k_gj_eliminate<<<eb, kT, 0, ctx->stream>>>(n, a.get(), f.get(), k);
         check_launch(ctx);
     }
-    k_gj_extract<<<blocks_for(static_cast<int64_t>(n) * n, kT), kT, 0, ctx->stream>>>(n, a.get(), d.dense.get());
+    if (d.dense_fp64)
+        k_gj_extract<double><<<blocks_for(static_cast<int64_t>(n) * n, kT), kT, 0, ctx->stream>>>(n, a.get(),
+                                                                                                d.dense64.get());
+    else
+        k_gj_extract<float><<<blocks_for(static_cast<int64_t>(n) * n, kT), kT, 0, ctx->stream>>>(n, a.get(),
+                                                                                               d.dense.get());
     check_launch(ctx);
     CFDXG_CUDA(cudaStreamSynchronize(ctx->stream));
 }
@@ -714,9 +726,13 @@ void enqueue_from(cfdxg_context* ctx, DevHierarchy<T>& d, int l) {
             check_launch(ctx);
             L.xout = L.x.get();
         } else if (d.coarse_mode == 2) {
-            account(4.0 * L.n * L.n + 2.0 * sizeof(T) * L.n);
-            launch_pdl(s, k_dense_inverse_apply<T>, blocks_for(static_cast<int64_t>(L.n) * 32, kT), kT, 
-                L.n, d.dense.get(), L.r.get(), L.x.get(), d.status);
+            account((d.dense_fp64 ? 8.0 : 4.0) * L.n * L.n + 2.0 * sizeof(T) * L.n);
+            if (d.dense_fp64)
+                launch_pdl(s, k_dense_inverse_apply<T, double>, blocks_for(static_cast<int64_t>(L.n) * 32, kT), kT,
+                           L.n, d.dense64.get(), L.r.get(), L.x.get(), d.status);
+            else
+                launch_pdl(s, k_dense_inverse_apply<T, float>, blocks_for(static_cast<int64_t>(L.n) * 32, kT), kT,
+                           L.n, d.dense.get(), L.r.get(), L.x.get(), d.status);
             check_launch(ctx);
             L.xout = L.x.get();
         } else {
@@ -786,6 +802,7 @@ std::unique_ptr<DevHierarchy<T>> upload_hierarchy(cfdxg_context* ctx, const AmgH
     d->coarse_pre = h.options.coarse_pre >= 0 ? h.options.coarse_pre : coarse_default_pre;
     d->coarse_post = h.options.coarse_post >= 0 ? h.options.coarse_post : coarse_default_post;
     d->status = ctx->scratch.status;
+    d->dense_fp64 = opt.dense_fp64;
     int used = static_cast<int>(h.levels.size());
     d->coarse_mode = 0;
     if (std::is_same<T, float>::value && coarse_dense_limit > 0) {

@@ -8,7 +8,11 @@ sets up the AMG hierarchy and runs each hot-path kernel a few times:
   * ``vcycle``: three V-cycle applications (``--precision fp32_vcycle|fp64``);
   * ``solve``: one FGMRES(30) solve to 1e-8 with the FP32 V-cycle, two
     applications of the learned stage (when trained weights are present) and
-    the Rhie-Chow face flux of the solution.
+    the Rhie-Chow face flux of the solution;
+  * ``face``: the face loop alone -- ``--cycles`` pressure-corrector
+    assemblies (Gauss gradient + assembly) and Rhie-Chow fluxes with a
+    non-zero pressure, inputs on the device, L2 flushed before each call;
+    prints each kernel's device time from the library's live profiler.
 
 Example (one kernel, one launch, at 663,552 cells):
 
@@ -52,13 +56,16 @@ def build_system(ctx, n):
 def main(argv=None):
     ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
     ap.add_argument("--n", type=int, default=48, help="lattice size (cells = 6 n^3)")
-    ap.add_argument("--mode", choices=["vcycle", "solve"], default="solve")
+    ap.add_argument("--mode", choices=["vcycle", "solve", "face"], default="solve")
     ap.add_argument("--precision", choices=["fp32_vcycle", "fp64"], default="fp32_vcycle")
     ap.add_argument("--wide-columns", action="store_true", help="int32 columns on every level (narrow_columns = 0)")
     ap.add_argument("--cycles", type=int, default=3, help="V-cycle applications in --mode vcycle")
     args = ap.parse_args(argv)
     ctx = cg.Context(0)
     m, mesh, (U, rAU, aP, p, fixed, value), A, b = build_system(ctx, args.n)
+    if args.mode == "face":
+        face_loop(ctx, m, mesh, (U, rAU, p, fixed, value), A, args.cycles)
+        return
     amg = cg.NativeBoomerAMGPreconditioner(ctx, precision=args.precision,
                                            narrow_columns=0 if args.wide_columns else 1)
     if not amg.setup(A):
@@ -80,6 +87,49 @@ def main(argv=None):
     flux = cg.make_rhie_chow_mass_flux(mesh, U, rAU, x, 1.0, fixed, value)
     print(f"solve n={args.n} cells={A.n} iterations={rep['iterations']} |flux|={np.linalg.norm(flux):.6e}")
     ctx.close()
+
+
+def face_loop(ctx, m, mesh, fields, A, calls):
+    import ctypes as C
+
+    import torch
+
+    from cfdx_dev_b200 import _native as N
+    U, rAU, p, fixed, value = fields
+    dev = torch.device("cuda", 0)
+    cc = mesh.geometry()["cell_centres"].reshape(3, -1)
+    p = np.sin(3.0 * cc[0]) * cc[1] + cc[2]     # non-zero pressure: every term of the face loop is live
+    Ud, rd, pd = (torch.from_numpy(np.ascontiguousarray(a)).to(dev) for a in (U, rAU, p))
+    nc, nf = m.n_cells, m.n_faces
+    bd = torch.empty(nc, dtype=torch.float64, device=dev)
+    phid = torch.empty(nf, dtype=torch.float64, device=dev)
+    gd = torch.empty(3 * nc, dtype=torch.float64, device=dev)
+    fl = torch.empty(nf, dtype=torch.float64, device=dev)
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=dev)
+    fx = np.ascontiguousarray(fixed, np.int32)
+    vv = np.ascontiguousarray(value, np.float64)
+    h = C.c_void_p(A.handle.value)
+    ptr = lambda t: C.c_void_p(t.data_ptr())
+    lib = ctx.lib
+    ctx.profile(True)
+    for s in range(calls):
+        flush.fill_(float(s))
+        torch.cuda.synchronize()
+        ctx.check(lib.cfdxg_assemble_pressure_correction(ctx.handle, mesh.handle, ptr(Ud), ptr(rd), ptr(pd), 1.0,
+                                                         N.ptr(fx), N.ptr(vv), N.CFDXG_MEM_DEVICE, C.byref(h),
+                                                         ptr(bd), ptr(phid), ptr(gd)), "assembly")
+        flush.fill_(float(s))
+        torch.cuda.synchronize()
+        ctx.check(lib.cfdxg_rhie_chow_flux(ctx.handle, mesh.handle, ptr(Ud), ptr(rd), ptr(pd), 1.0, N.ptr(fx),
+                                           N.ptr(vv), N.CFDXG_MEM_DEVICE, ptr(fl)), "flux")
+    torch.cuda.synchronize()
+    for e in ctx.profile_read():
+        if e["launches"]:
+            ms = e["total_ms"] / e["launches"]
+            print(f"{e['name']}: {e['launches']} launches, {ms * 1e3:.1f} us, "
+                  f"{e['bytes'] / e['launches'] / (ms / 1e3) / 1e9:.0f} GB/s on the algorithmic bytes")
+    ctx.profile(False)
+    print(f"face n={m.n_cells} cells |b|={float(bd.norm()):.6e} |flux|={float(fl.norm()):.6e}")
 
 
 if __name__ == "__main__":

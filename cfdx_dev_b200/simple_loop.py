@@ -8,20 +8,30 @@ column spans [0, 1]), x and z lattice lines are jittered by +-0.05h (seeded).
 Per-cell eddy-viscosity ratio log-uniform on [1, 1e3], smoothed by 3 Jacobi
 sweeps (average of the cell and its face neighbours).
 
-The momentum solve is outside this library, so each outer iteration k builds
-the momentum diagonal and the predicted velocity from what the pressure side
-produced in iteration k - 1, the way SIMPLE feeds them back:
+The momentum solve is outside this library's path, so the loop drives the
+reference's pressure-side steps with a momentum operator of its own: a
+viscous-plus-upwind-convection matrix on the cell graph built from the previous
+iteration's face fluxes (the same matrix for the three velocity components,
+zero-gradient velocity boundaries),
 
-  a_P = sum_f (1 + nu_t,f) |S_f| / |d_f|  +  sum_f max(phi_f, 0)   (viscous + upwind outflow)
-  rAU = 1 / a_P (all three directions);  HbyA = U  (the corrected cell velocity)
+  a_oo += G_f + max(phi_f, 0),   a_on = -G_f - max(-phi_f, 0),
+  a_nn += G_f + max(-phi_f, 0),  a_no = -G_f - max(phi_f, 0),
+  G_f = (1 + nu_t,f) |S_f| / |d_f|   (boundary faces: owner diagonal only),
 
-then runs the pressure-corrector chain of the reference
-(physics/steady_incompressible_solver.h:8048-8181 assembly, the AMG numeric
-refresh of core/linalg/amg_preconditioner.h:245-314 on the unchanged pattern,
-the solve, make_rhie_chow_mass_flux :2064-2217 with the correction, and the
-under-relaxed update p += alpha_p p', U = HbyA - V rAU grad p').  The initial
-velocity is a unit stream in x plus an 8-mode divergence-free Fourier field;
-p = 0 is fixed on the x = 0 patch.
+with right-hand side -grad(p) V, taking the current cell velocity as the
+momentum solution.  Each outer iteration then runs the reference's chain:
+
+  rAU = 1 / diag(M);  HbyA = build_hbya (steady_incompressible_solver.h:6430-6465);
+  pressure-corrector assembly (:8048-8181);  AMG setup, then numeric refresh on the
+  unchanged pattern (amg_preconditioner.h:245-314);  the pressure solve;
+  p += alpha_p p' (:9339-9343, fixed-pressure boundary: no gauge shift);
+  phi = make_rhie_chow_mass_flux(HbyA, p) (:2064-2217);  grad p;  U = HbyA - V rAU grad p.
+
+The initial velocity is a unit stream in x plus an 8-mode divergence-free
+Fourier field; p = 0 is fixed on the x = 0 patch.  tests/test_gpu_simple.py
+checks five iterations of this chain on the GPU against the same chain built
+from the C oracle (HbyA, assembly, flux and gradient bit-identical; the
+pressure to 1e-10 with equal iteration counts).
 
 Forms: plain FP64 GMRES(30) + FP64 AMG (the reference's method); FP64
 FGMRES(30) + FP32 V-cycle; and the same with the learned stage in front
@@ -97,6 +107,50 @@ def outflow(m, phi):
     return out
 
 
+def cell_pattern(m):
+    """CSR pattern of the cell graph (sorted rows, diagonal included) and, per
+    interior face, the positions of (owner, neighbour) and (neighbour, owner)."""
+    nc = m.n_cells
+    internal = np.flatnonzero(m.neighbour >= 0)
+    o, n = m.owner[internal], m.neighbour[internal]
+    rows = np.concatenate([np.arange(nc), o, n])
+    cols = np.concatenate([np.arange(nc), n, o])
+    order = np.lexsort((cols, rows))
+    ro = np.zeros(nc + 1, np.int64)
+    np.add.at(ro, rows + 1, 1)
+    ro = np.cumsum(ro)
+    co = cols[order].astype(np.int64)
+    pos = np.empty(rows.size, np.int64)
+    pos[order] = np.arange(rows.size)
+    diag_pos = pos[:nc]
+    on_pos, no_pos = pos[nc:nc + internal.size], pos[nc + internal.size:]
+    return ro, co, diag_pos, internal, on_pos, no_pos
+
+
+def momentum_values(m, g, nu_t, phi, pattern):
+    """Values of the synthetic momentum matrix (see the module docstring) on cell_pattern's pattern."""
+    ro, co, diag_pos, internal, on_pos, no_pos = pattern
+    nf, nc = m.n_faces, m.n_cells
+    S = g["face_Sf"].reshape(3, nf)
+    area = np.sqrt((S * S).sum(0))
+    cc = g["cell_centres"].reshape(3, nc)
+    fc = g["face_centres"].reshape(3, nf)
+    o, nb = m.owner, m.neighbour
+    isin = nb >= 0
+    other = np.where(isin, nb, 0)
+    d = np.where(isin[None, :], cc[:, other] - cc[:, o], fc - cc[:, o])
+    dist = np.sqrt((d * d).sum(0))
+    nu_f = np.where(isin, 0.5 * (nu_t[o] + nu_t[other]), nu_t[o])
+    G = (1.0 + nu_f) * area / dist
+    va = np.zeros(co.size)
+    diag = np.bincount(o, weights=G + np.maximum(phi, 0.0), minlength=nc)
+    diag += np.bincount(nb[internal], weights=G[internal] + np.maximum(-phi[internal], 0.0), minlength=nc)
+    va[diag_pos] = diag
+    va[on_pos] = -G[internal] - np.maximum(-phi[internal], 0.0)
+    va[no_pos] = -G[internal] - np.maximum(phi[internal], 0.0)
+    return va, diag
+
+
 def finetune(ctx, net, mesh, A, aP, amg64, amg32, pairs, epochs, seed):
     rng = np.random.default_rng(seed)
     R, E = [], []
@@ -123,28 +177,38 @@ def finetune(ctx, net, mesh, A, aP, amg64, amg32, pairs, epochs, seed):
     return losses
 
 
-def run_form(ctx, form, m, mesh, g, nu_t, iterations, alpha_p, net, sync):
+def initial_state(m, g):
+    """(U, p, phi) at the first outer iteration."""
+    U = cg.fourier_field(g["cell_centres"], 8, 0.01, SEED + 1)
+    U[:m.n_cells] += 1.0   # unit stream in x
+    return U, np.zeros(m.n_cells), np.zeros(m.n_faces)
+
+
+def run_form(ctx, form, m, mesh, g, nu_t, iterations, alpha_p, net, sync, keep=False):
     nc = m.n_cells
     fixed = np.zeros(m.n_patches, np.int32)
     fixed[0] = 1
     value = np.zeros(m.n_patches)
     vol = g["cell_volumes"]
-    U = cg.fourier_field(g["cell_centres"], 8, 0.01, SEED + 1)
-    U[:nc] += 1.0   # unit stream in x
-    p = np.zeros(nc)
-    phi = np.zeros(m.n_faces)
-    a_visc = viscous_diagonal(m, g, nu_t)
+    U, p, phi = initial_state(m, g)
+    gradp = np.zeros(3 * nc)
+    pattern = cell_pattern(m)
     precision = "fp64" if form == "plain_fp64" else "fp32_vcycle"
     krylov = "gmres" if form == "plain_fp64" else "fgmres"
     A = None
     amg = None
-    records = []
+    records, states = [], []
     for k in range(iterations):
         rec = {"iteration": k}
-        aP = a_visc + outflow(m, phi)
-        rAU = np.concatenate([1.0 / aP] * 3)
         t = time.perf_counter()
-        A, b, phiH, grad = cg.assemble_pressure_correction(mesh, U, rAU, p, 1.0, fixed, value, matrix=A)
+        va, aP = momentum_values(m, g, nu_t, phi, pattern)
+        rAU = np.concatenate([1.0 / aP] * 3)
+        rhs = -(gradp.reshape(3, nc) * vol[None, :]).ravel()
+        M = cg.SparseMatrix.from_csr(ctx, pattern[0], pattern[1], va)
+        HbyA = cg.build_hbya(mesh, M, rhs, U, gradp, rAU)
+        rec["momentum_s"] = time.perf_counter() - t
+        t = time.perf_counter()
+        A, b, phiH, _ = cg.assemble_pressure_correction(mesh, HbyA, rAU, p, 1.0, fixed, value, matrix=A)
         sync()
         rec["assembly_s"] = time.perf_counter() - t
         rec["continuity_l2"] = float(np.linalg.norm(b))
@@ -170,30 +234,37 @@ def run_form(ctx, form, m, mesh, g, nu_t, iterations, alpha_p, net, sync):
             rec["learned_bind_s"] = time.perf_counter() - t
             kw = dict(learned=net)
         t = time.perf_counter()
-        dp, rep = cg.solve_gmres(A, b, amg=amg, restart=30, tolerance=1e-8, krylov=krylov, max_iterations=1000, **kw)
+        ortho = {} if form == "plain_fp64" else {"orthogonalization": 1}
+        dp, rep = cg.solve_gmres(A, b, amg=amg, restart=30, tolerance=1e-8, krylov=krylov, max_iterations=1000,
+                                 **ortho, **kw)
         sync()
         rec["solve_s"] = time.perf_counter() - t
         rec["krylov_iterations"] = rep["iterations"]
         rec["status"] = rep["status_name"]
         rec["physical_residual_relative"] = rep["physical_residual_relative"]
         t = time.perf_counter()
-        phi = cg.make_rhie_chow_mass_flux(mesh, U, rAU, dp, 1.0, fixed, value)
-        gdp = cg.gauss_gradient_with_boundary(mesh, dp, fixed, np.zeros(m.n_patches)).reshape(3, nc)
+        p = p + alpha_p * dp
+        phi = cg.make_rhie_chow_mass_flux(mesh, HbyA, rAU, p, 1.0, fixed, value)
+        gradp = cg.gauss_gradient_with_boundary(mesh, p, fixed, value)
         sync()
         rec["flux_s"] = time.perf_counter() - t
         # cell velocity correction with dAU = V rAU (the volume enters at the projection)
-        U = (U.reshape(3, nc) - vol[None, :] * rAU.reshape(3, nc) * gdp).ravel()
-        p = p + alpha_p * dp
+        U = (HbyA.reshape(3, nc) - vol[None, :] * rAU.reshape(3, nc) * gradp.reshape(3, nc)).ravel()
         records.append(rec)
+        if keep:
+            states.append({"HbyA": HbyA, "b": b, "dp": dp, "p": p.copy(), "phi": phi, "iterations": rep["iterations"]})
         print(json.dumps({"form": form, **{q: v for q, v in rec.items() if q != "amg_levels"}}), flush=True)
     total = {q: float(sum(r.get(q, 0.0) for r in records))
-             for q in ("assembly_s", "amg_setup_s", "amg_refresh_s", "amg_resetup_s", "learned_bind_s", "solve_s",
-                       "flux_s")}
+             for q in ("momentum_s", "assembly_s", "amg_setup_s", "amg_refresh_s", "amg_resetup_s", "learned_bind_s",
+                       "solve_s", "flux_s")}
     total["refreshes"] = sum(1 for r in records if "amg_refresh_s" in r)
     total["resetups"] = sum(1 for r in records if "amg_resetup_s" in r)
     total["krylov_iterations"] = int(sum(r["krylov_iterations"] for r in records))
-    return {"records": records, "totals": total,
-            "final_continuity_l2": records[-1]["continuity_l2"], "first_continuity_l2": records[0]["continuity_l2"]}
+    out = {"records": records, "totals": total,
+           "final_continuity_l2": records[-1]["continuity_l2"], "first_continuity_l2": records[0]["continuity_l2"]}
+    if keep:
+        out["states"] = states
+    return out
 
 
 def main(argv=None):

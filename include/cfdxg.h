@@ -219,6 +219,18 @@ int cfdxg_rhie_chow_flux_noalloc(cfdxg_context* ctx, cfdxg_mesh* mesh, const dou
                                  const int32_t* p_bc_fixed, const double* p_bc_value,
                                  double* flux);
 
+/* Replaces the build_hbya step of solve_steady_incompressible
+ * (physics/steady_incompressible_solver.h:6430-6465): per velocity component d,
+ *   HbyA_d[c] = rAU_d[c] * (rhs_d[c] + gradp_d[c] * V_c - sum_{k: col != c} a_d[k] U_d[col])
+ * with the off-diagonal entries of component d's momentum matrix in CSR
+ * order.  momentum: three matrices (one per component, may be the same
+ * handle) sharing one pattern of n_cells rows; rhs (the momentum equations'
+ * right-hand sides), U, gradp, rAU and HbyA: 3*n_cells, component-major.  A
+ * non-finite HbyA returns CFDXG_ERR_NONFINITE (the reference throws). */
+int cfdxg_build_hbya(cfdxg_context* ctx, cfdxg_mesh* mesh, const cfdxg_matrix* const* momentum,
+                     const double* rhs, const double* U, const double* gradp, const double* rAU,
+                     int32_t mem, double* HbyA);
+
 /* Replaces gauss_gradient_with_boundary (physics/steady_incompressible_solver.h:1634-1744),
  * default single sweep, distance-weighted interpolation.  grad: 3*n_cells. */
 int cfdxg_gauss_gradient(cfdxg_context* ctx, cfdxg_mesh* mesh, const double* p,
@@ -292,6 +304,11 @@ typedef struct {
                                         of each row's largest magnitude, times that magnitude
                                         in FP32: 2 bytes per nonzero instead of 4, sums stay
                                         FP32.  0: FP32 values everywhere. */
+    int32_t dense_fp64;              /* FP32 V-cycle only.  0 (default): the dense coarse
+                                        inverse is stored FP32; 1: stored FP64 and applied
+                                        in FP64 -- with coarse_dense_limit 2000, the FP64
+                                        coarsest-level direct solve of the mixed-precision
+                                        configuration (1,933 rows at 64^3). */
 } cfdxg_amg_options;
 
 int cfdxg_amg_options_default(cfdxg_amg_options* opts);

@@ -1198,3 +1198,27 @@ int64_t co_gauge_identity_row(int64_t n, const int64_t* ro, const int64_t* co, c
     }
     return nnz;
 }
+
+/* ---------------------------------------------------- momentum-inverse HbyA */
+
+/* physics/steady_incompressible_solver.h:6430-6465 (build_hbya): h starts at
+ * the component's momentum right-hand side plus gradp * V (:6437), subtracts
+ * the off-diagonal products in the row's CSR order (:6438-6443), and HbyA is
+ * rAU * h (:6459), refused when not finite (:6460-6461). */
+int co_build_hbya(int64_t n, const int64_t* ro, const int64_t* co, const double* va, const double* rhs,
+                  const double* U, const double* gradp, const double* vol, const double* rAU, double* HbyA) {
+    const int64_t nnz = ro[n];
+    for (int d = 0; d < 3; ++d) {
+        const double* a = va + d * nnz;
+        for (int64_t c = 0; c < n; ++c) {
+            double h = rhs[d * n + c] + gradp[d * n + c] * vol[c];
+            for (int64_t k = ro[c]; k < ro[c + 1]; ++k) {
+                const int64_t col = co[k];
+                if (col != c) h -= a[k] * U[d * n + col];
+            }
+            HbyA[d * n + c] = rAU[d * n + c] * h;
+            if (!isfinite(HbyA[d * n + c])) return fail("solve_steady_incompressible: non-finite HbyA");
+        }
+    }
+    return 0;
+}

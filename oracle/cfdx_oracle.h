@@ -84,6 +84,17 @@ int co_rhie_chow_flux(const co_mesh_t* m, const double* HbyA, const double* rAU,
 /* core/solvers/scalar_diffusion.h:39-163 assemble_cell_diffusion_matrix;
  * bc_face_values NaN = unprescribed face, bc_types NULL = all Dirichlet
  * (0 Dirichlet, 1 prescribed flux).  Returns nnz or < 0. */
+/* The build_hbya step of solve_steady_incompressible
+ * (physics/steady_incompressible_solver.h:6430-6465), per velocity component d
+ * (SoA arrays of 3*n, d-th block):
+ *   HbyA_d[c] = rAU_d[c] * (rhs_d[c] + gradp_d[c] * V_c - sum_{k: col != c} a_d[k] * U_d[col])
+ * with the off-diagonal entries of the component's momentum matrix in CSR
+ * order.  values: 3 arrays of nnz (one matrix per component, same pattern).
+ * Returns -1 on a non-finite HbyA (the reference throws). */
+int co_build_hbya(int64_t n, const int64_t* row_offsets, const int64_t* columns, const double* values,
+                  const double* rhs, const double* U, const double* gradp, const double* volumes,
+                  const double* rAU, double* HbyA);
+
 int64_t co_assemble_diffusion(const co_mesh_t* m, const double* bc_face_values,
                               const int32_t* bc_types, double diffusivity,
                               const double* source, int64_t* row_offsets,

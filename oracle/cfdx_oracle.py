@@ -76,6 +76,7 @@ def lib():
             L.co_pressure_assemble.restype = C.c_int64
             L.co_pressure_assemble.argtypes = [C.c_void_p] * 4 + [C.c_double] + [C.c_void_p] * 8
             L.co_rhie_chow_flux.argtypes = [C.c_void_p] * 4 + [C.c_double] + [C.c_void_p] * 3
+            L.co_build_hbya.argtypes = [C.c_int64] + [C.c_void_p] * 9
             L.co_assemble_diffusion.restype = C.c_int64
             L.co_assemble_diffusion.argtypes = [C.c_void_p] * 3 + [C.c_double] + [C.c_void_p] * 5
             L.co_spmv.argtypes = [C.c_int64] + [C.c_void_p] * 5
@@ -284,3 +285,16 @@ def gauge_identity_row(ro, co, va, b, ref, value=0.0):
     nnz = _check(f(n, _p(ro), _p(co), _p(va), _p(b), int(ref), float(value), _p(ro_o), _p(co_o), _p(va_o),
                    _p(b_o)), "gauge")
     return ro_o, co_o[:nnz].copy(), va_o[:nnz].copy(), b_o
+
+
+def build_hbya(row_offsets, columns, values3, rhs, U, gradp, volumes, rAU):
+    """physics/steady_incompressible_solver.h:6430-6465 (build_hbya): values3 is
+    the three components' momentum values (3 x nnz, one pattern)."""
+    ro = np.ascontiguousarray(row_offsets, np.int64)
+    co = np.ascontiguousarray(columns, np.int64)
+    n = ro.size - 1
+    va = np.ascontiguousarray(values3, np.float64).reshape(-1)
+    out = np.empty(3 * n)
+    args = [_f64(a) for a in (rhs, U, gradp, volumes, rAU)]
+    _check(lib().co_build_hbya(n, _p(ro), _p(co), _p(va), *(_p(a) for a in args), _p(out)), "build_hbya")
+    return out
