@@ -29,8 +29,10 @@ def pytest_configure(config):
         from cfdx_dev_b200 import build as b
         b.build()
     ref_lib = ROOT / "oracle" / "_ref" / "libcfdx_ref.so"
-    if not ref_lib.exists() and REF_SRC.exists():
-        subprocess.run(["make", "-s", "-C", str(ROOT / "oracle"), "ref", "oracle", f"REF_ROOT={REF_SRC}"], check=True)
+    demo = ROOT / "oracle" / "_ref" / "cfdx_adapter_demo"
+    if (not ref_lib.exists() or not demo.exists()) and REF_SRC.exists():
+        subprocess.run(["make", "-s", "-C", str(ROOT / "oracle"), "ref", "oracle", "adapter", f"REF_ROOT={REF_SRC}"],
+                       check=True)
     c_lib = ROOT / "oracle" / "_build" / "libcfdx_oracle.so"
     if not c_lib.exists() and (ROOT / "oracle" / "cfdx_oracle.c").exists():
         subprocess.run(["make", "-s", "-C", str(ROOT / "oracle"), "oracle"], check=True)
