@@ -14,8 +14,9 @@ Forms timed: plain FP64 AMG-GMRES (the reference's algorithm, two-pass
 modified Gram-Schmidt), FP32 V-cycle inside FP64 FGMRES, and -- when trained
 weights are present -- the learned message-passing preconditioner in front of
 the FP32 V-cycle; the two FGMRES forms orthogonalise with two-pass classical
-Gram-Schmidt.  `value` is the headline form (learned+FP32 if available, else
-FP32 V-cycle).
+Gram-Schmidt.  `value` is the headline form, the FP32 V-cycle (the learned
+form is timed beside it: with the full training set it saves 0.1 iteration
+per solve and costs more than that).
 
 Inputs are larger than L2 (the hierarchy alone is > 2 GB), and L2 is also
 flushed before every timed step.  Rank-local device timing with CUDA events on
@@ -215,7 +216,11 @@ def run_cfdxg(args):
         net.load(str(WEIGHTS))
         net.bind(mesh, A, base_aP)
         plan.append(("learned_fp32", "fp32_vcycle", "fgmres", True))
-    headline = plan[-1][0]
+    # The headline is the FP32 V-cycle form: trained on the full config-4 set
+    # (4,096 pairs on 256 meshes of 16^3-48^3) the learned stage saves 0.1
+    # FGMRES iteration per solve at 64^3 and costs 0.8 ms, so it is timed and
+    # reported as its own form but does not set `value`.
+    headline = "fp32_vcycle" if any(e[0] == "fp32_vcycle" for e in plan) else plan[-1][0]
     forms = {}
     amgs = {}
     by_precision = {}   # one hierarchy per V-cycle precision, shared by the forms that use it
@@ -329,7 +334,8 @@ def run_cfdxg(args):
         b_host = torch.empty(n_cells, dtype=torch.float64, pin_memory=True)
         x_host = torch.empty(n_cells, dtype=torch.float64, pin_memory=True)
         bh, xh = b_host.numpy(), x_host.numpy()
-        req = request(plan[-1][2], plan[-1][3])
+        hk = next(e for e in plan if e[0] == headline)
+        req = request(hk[2], hk[3])
         e2e_times = []
         for s in range(args.warmup + args.steps):
             k = s % N_RHS

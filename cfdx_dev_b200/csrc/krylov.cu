@@ -424,11 +424,39 @@ __global__ void k_add(int n, double* __restrict__ x, const double* __restrict__ 
     if (i < n) x[i] += y[i];
 }
 
+// Pinned copies of one Arnoldi step's scalar slots [0, kH2 + m + 1) and of
+// the status word, two of them (step j uses buffer j & 1), each with the
+// event that marks its copy done: the host reads step j's results while the
+// GPU runs step j + 1.
+struct StepMirror {
+    double* scalars[2] = {nullptr, nullptr};
+    int* status[2] = {nullptr, nullptr};
+    cudaEvent_t done[2] = {nullptr, nullptr};
+    StepMirror() {
+        for (int k = 0; k < 2; ++k) {
+            CFDXG_CUDA(cudaHostAlloc(reinterpret_cast<void**>(&scalars[k]), sizeof(double) * kSlots,
+                                     cudaHostAllocDefault));
+            CFDXG_CUDA(cudaHostAlloc(reinterpret_cast<void**>(&status[k]), sizeof(int), cudaHostAllocDefault));
+            CFDXG_CUDA(cudaEventCreateWithFlags(&done[k], cudaEventDisableTiming));
+        }
+    }
+    ~StepMirror() {
+        for (int k = 0; k < 2; ++k) {
+            if (scalars[k]) cudaFreeHost(scalars[k]);
+            if (status[k]) cudaFreeHost(status[k]);
+            if (done[k]) cudaEventDestroy(done[k]);
+        }
+    }
+    StepMirror(const StepMirror&) = delete;
+    StepMirror& operator=(const StepMirror&) = delete;
+};
+
 struct Workspace {
     int64_t n = 0;
     int m = 0;
     DevBuf<double> V, Z, w, r, ax, best, trial, tmp;
     DevBuf<double> mpartial;   // (kChunk + 1) x kWideBlocks partial sums of the multi-dot
+    std::unique_ptr<StepMirror> mirror;
 };
 
 Workspace& workspace(cfdxg_context* ctx, int64_t n, int m) {
@@ -447,6 +475,7 @@ Workspace& workspace(cfdxg_context* ctx, int64_t n, int m) {
         ws->n = n;
         ws->m = mm;
     }
+    if (!ws->mirror) ws->mirror = std::make_unique<StepMirror>();
     return *ws;
 }
 
@@ -598,6 +627,15 @@ public:
         return read_status(ctx_);
     }
     double host(int s) const { return ctx_->scratch.host_scalars[s]; }
+    // Queues the copy of slots [0, count) and of the status word into mirror
+    // buffer k, then marks it with the buffer's event (no synchronisation).
+    void fetch_async(StepMirror& M, int k, int count) {
+        CFDXG_CUDA(cudaMemcpyAsync(M.scalars[k], sc_, sizeof(double) * count, cudaMemcpyDeviceToHost,
+                                   ctx_->stream));
+        CFDXG_CUDA(cudaMemcpyAsync(M.status[k], ctx_->scratch.status, sizeof(int), cudaMemcpyDeviceToHost,
+                                   ctx_->stream));
+        CFDXG_CUDA(cudaEventRecord(M.done[k], ctx_->stream));
+    }
     double scalar(int s) {   // read one slot
         fetch(s + 1);
         return host(s);
@@ -821,52 +859,72 @@ KrylovResult gmres_solve(cfdxg_context* ctx, const cfdxg_matrix* A, const double
         bool arnoldi_breakdown = false;
         bool reliable_restart = false;
 
-        for (int j = 0; j < m && iterations < max_iter; ++j) {
+        // One Arnoldi step on the device: z_j = M^-1 v_j, w = A z_j, the
+        // Gram-Schmidt passes into the H slots, v_{j+1} = w / h_{j+1,j}, and
+        // the queued copy of the step's slots into mirror buffer j & 1.
+        StepMirror& mirror = *ws->mirror;
+        auto enqueue_step = [&](int jj) -> bool {
             if (pc) {
-                if (!(*pc)(v(j), z(j), j)) return fail(CFDXG_NOT_APPLICABLE);
-                ++result.preconditioner_applications;
+                if (!(*pc)(v(jj), z(jj), jj)) return false;
             } else {
-                E.copy(z(j), v(j));
+                E.copy(z(jj), v(jj));
             }
-            E.spmv(z(j), ws->w.get());
+            E.spmv(z(jj), ws->w.get());
             double* w = ws->w.get();
-            if (controls.classical_gram_schmidt && j + 1 <= kChunk) {
+            if (controls.classical_gram_schmidt && jj + 1 <= kChunk) {
                 // classical Gram-Schmidt twice in three fused passes; the
-                // action norm comes from the first (slot kH1 + j + 1)
-                E.gram_schmidt_cgs2_fused(V, j + 1, w, ws->mpartial.get());
-                E.sqrt_slot(kH1 + j + 1, kAction);
-            } else {
-                E.norm2(w, kAction);
-            }
-            // two passes of modified Gram-Schmidt (h = v_i . w; w -= h v_i for
-            // i = 0..j, twice), each update fused with the next dot
-            if (controls.classical_gram_schmidt && j + 1 <= kChunk) {
-                // done above
+                // action norm comes from the first (slot kH1 + jj + 1)
+                E.gram_schmidt_cgs2_fused(V, jj + 1, w, ws->mpartial.get());
+                E.sqrt_slot(kH1 + jj + 1, kAction);
             } else if (controls.classical_gram_schmidt) {
                 // two passes of classical Gram-Schmidt: h = V^T w; w -= V h, twice
-                E.multidot(V, j + 1, w, kH1, ws->mpartial.get());
-                E.multi_axpy(V, j + 1, kH1, w, -1);
-                E.multidot(V, j + 1, w, kH2, ws->mpartial.get());
-                E.multi_axpy(V, j + 1, kH2, w, kHnext);
+                E.norm2(w, kAction);
+                E.multidot(V, jj + 1, w, kH1, ws->mpartial.get());
+                E.multi_axpy(V, jj + 1, kH1, w, -1);
+                E.multidot(V, jj + 1, w, kH2, ws->mpartial.get());
+                E.multi_axpy(V, jj + 1, kH2, w, kHnext);
             } else {
+                // two passes of modified Gram-Schmidt (h = v_i . w; w -= h v_i
+                // for i = 0..jj, twice), each update fused with the next dot
+                E.norm2(w, kAction);
                 E.dot(v(0), w, kH1);
-                for (int i = 0; i < j; ++i) E.axpy_dot(w, v(i), kH1 + i, v(i + 1), kH1 + i + 1);
-                E.axpy_dot(w, v(j), kH1 + j, v(0), kH2);
-                for (int i = 0; i < j; ++i) E.axpy_dot(w, v(i), kH2 + i, v(i + 1), kH2 + i + 1);
-                E.axpy_norm2(w, v(j), kH2 + j, kHnext);
+                for (int i = 0; i < jj; ++i) E.axpy_dot(w, v(i), kH1 + i, v(i + 1), kH1 + i + 1);
+                E.axpy_dot(w, v(jj), kH1 + jj, v(0), kH2);
+                for (int i = 0; i < jj; ++i) E.axpy_dot(w, v(i), kH2 + i, v(i + 1), kH2 + i + 1);
+                E.axpy_norm2(w, v(jj), kH2 + jj, kHnext);
             }
-            E.div(w, kHnext, v(j + 1));
-            const int st = E.fetch(kSlots);
-            if (st & kStatusNonFinite) {
+            E.div(w, kHnext, v(jj + 1));
+            E.fetch_async(mirror, jj & 1, kH2 + jj + 1);
+            return true;
+        };
+        // Run-ahead: step j + 1 is queued before step j's results are read
+        // whenever step j is predicted not to stop the cycle (its residual
+        // estimate, extrapolated from the last two, stays above 4 x tol), so
+        // the GPU is not idle while the host runs the Givens update.  A step
+        // queued in vain only writes z, w and v beyond the cycle's used
+        // columns and H slots already copied; its results are ignored.
+        double est_prev = beta, ratio_prev = 1.0;
+        bool queued = enqueue_step(0);
+        if (!queued) return fail(CFDXG_NOT_APPLICABLE);
+        for (int j = 0; j < m && iterations < max_iter; ++j) {
+            bool ahead = false, ahead_failed = false;
+            if (j + 1 < m && iterations + 1 < max_iter && est_prev * ratio_prev > 4.0 * tol) {
+                ahead = true;
+                ahead_failed = !enqueue_step(j + 1);
+            }
+            CFDXG_CUDA(cudaEventSynchronize(mirror.done[j & 1]));
+            const double* hs = mirror.scalars[j & 1];
+            if (pc) ++result.preconditioner_applications;
+            if (*mirror.status[j & 1] & kStatusNonFinite) {
                 if (pc) return fail(CFDXG_NOT_APPLICABLE);   // preconditioner produced a non-finite z
             }
-            const double arnoldi_action_norm = E.host(kAction);
+            const double arnoldi_action_norm = hs[kAction];
             if (!std::isfinite(arnoldi_action_norm)) return fail(CFDXG_DIVERGED);
             for (int i = 0; i <= j; ++i) {
-                H(i, j) = E.host(kH1 + i);
-                H(i, j) += E.host(kH2 + i);
+                H(i, j) = hs[kH1 + i];
+                H(i, j) += hs[kH2 + i];
             }
-            const double hnext = E.host(kHnext);
+            const double hnext = hs[kHnext];
             if (!std::isfinite(hnext)) return fail(CFDXG_DIVERGED);
             H(j + 1, j) = hnext;
             const double floor = 4096.0 * kEps * std::max(arnoldi_action_norm, 1e-300);
@@ -934,6 +992,11 @@ KrylovResult gmres_solve(cfdxg_context* ctx, const cfdxg_matrix* A, const double
                         break;
                     }
                 }
+            }
+            if (estimated_residual > 0.0 && est_prev > 0.0) ratio_prev = std::min(1.0, estimated_residual / est_prev);
+            est_prev = estimated_residual;
+            if (j + 1 < m && iterations < max_iter) {
+                if (ahead ? ahead_failed : !enqueue_step(j + 1)) return fail(CFDXG_NOT_APPLICABLE);
             }
         }
         if (used == 0) break;

@@ -235,7 +235,10 @@ __global__ void k_restrict(int nc, const int* __restrict__ r_off, const int* __r
 // x += P xc.  TPR == 1 adds the entries to x one by one in P's row order (the
 // reference's order); TPR > 1 forms the row sum cooperatively (deterministic
 // butterfly, as row_dot) and adds it once.
-template <class T, int TPR>
+// With ASSIGN the level's x is taken as zero (no pre-sweeps: the cycle would
+// otherwise clear it first) and x = 0 + P xc is written without reading x --
+// the same arithmetic as clearing x and adding, one graph node fewer per level.
+template <class T, int TPR, bool ASSIGN = false>
 __global__ void k_prolong(int n, const int* __restrict__ p_off, const int* __restrict__ p_col,
                           const T* __restrict__ p_val, const T* __restrict__ xc, T* __restrict__ x,
                           int* status) {
@@ -251,7 +254,7 @@ __global__ void k_prolong(int n, const int* __restrict__ p_off, const int* __res
     pdl_wait();
     if constexpr (TPR == 1) {
         if (!valid) return;
-        T v = x[i];
+        T v = ASSIGN ? T(0) : x[i];
 #pragma unroll
         for (int q = 0; q < 4; ++q)
             if (b + q < e) v += head.v[q] * __ldg(xc + head.c[q]);
@@ -261,7 +264,7 @@ __global__ void k_prolong(int n, const int* __restrict__ p_off, const int* __res
     } else {
         const T s = row_dot_head<T, TPR, int, 4>(head, b, e, lane, p_col, p_val, xc, 0);
         if (!valid || lane != 0) return;
-        const T v = x[i] + s;
+        const T v = (ASSIGN ? T(0) : x[i]) + s;
         x[i] = v;
         if (!finite_(v)) atomicOr(status, kStatusNonFinite);
     }
@@ -507,13 +510,20 @@ void launch_restrict(cfdxg_context* ctx, const DevLevel<T>& L, const T* res, T* 
 }
 
 template <class T>
-void launch_prolong(cfdxg_context* ctx, const DevLevel<T>& L, const T* xc, T* x, int* status) {
+void launch_prolong(cfdxg_context* ctx, const DevLevel<T>& L, const T* xc, T* x, int* status,
+                    bool assign = false) {
     const double pnnz = static_cast<double>(L.p_col.size());
-    const double bytes = account((sizeof(T) + 4.0) * pnnz + 4.0 * (L.n + 1) + sizeof(T) * (L.nc + 2.0 * L.n));
+    const double bytes = account((sizeof(T) + 4.0) * pnnz + 4.0 * (L.n + 1) +
+                                 sizeof(T) * (L.nc + (assign ? 1.0 : 2.0) * L.n));
     ProfScope ps(ctx, tname<T>("prolong_fp64_L0", "prolong_fp32_L0"), bytes);
     const int64_t threads = static_cast<int64_t>(L.n) * L.tpr_p;
-    CFDXG_TPR_SWITCH(L.tpr_p, (launch_pdl(ctx->stream, k_prolong<T, TPR>, blocks_for(threads, kT), kT, 
-        L.n, L.p_off.get(), L.p_col.get(), L.p_val.get(), xc, x, status)));
+    if (assign) {
+        CFDXG_TPR_SWITCH(L.tpr_p, (launch_pdl(ctx->stream, k_prolong<T, TPR, true>, blocks_for(threads, kT), kT,
+                                              L.n, L.p_off.get(), L.p_col.get(), L.p_val.get(), xc, x, status)));
+    } else {
+        CFDXG_TPR_SWITCH(L.tpr_p, (launch_pdl(ctx->stream, k_prolong<T, TPR, false>, blocks_for(threads, kT), kT,
+                                              L.n, L.p_off.get(), L.p_col.get(), L.p_val.get(), xc, x, status)));
+    }
     check_launch(ctx);
 }
 
@@ -740,7 +750,8 @@ void enqueue_from(cfdxg_context* ctx, DevHierarchy<T>& d, int l) {
         }
         return;
     }
-    sweeps_from_zero(ctx, d, L, L.r.get(), d.coarse_pre);
+    if (d.coarse_pre > 0) sweeps_from_zero(ctx, d, L, L.r.get(), d.coarse_pre);
+    else L.xout = L.x.get();   // x = 0: the prolongation below assigns it
     T* x = L.xout;
     T* x2 = (x == L.x.get()) ? L.x2.get() : L.x.get();
     DevLevel<T>& C = d.L[l + 1];
@@ -751,7 +762,7 @@ void enqueue_from(cfdxg_context* ctx, DevHierarchy<T>& d, int l) {
         launch_restrict<T>(ctx, L, L.r.get(), C.r.get());   // x = 0: the residual is r
     }
     enqueue_from(ctx, d, l + 1);
-    launch_prolong<T>(ctx, L, C.xout, x, d.status);
+    launch_prolong<T>(ctx, L, C.xout, x, d.status, d.coarse_pre == 0);
     for (int k = 0; k < d.coarse_post; ++k) {
         launch_sweep<T, T>(ctx, L, L.r.get(), x, x2, d.omega, d.status);
         std::swap(x, x2);
