@@ -135,8 +135,30 @@ __device__ __forceinline__ T row_dot_head(const RowHead<T, CI, PF>& h, int b, in
 #pragma unroll
     for (int q = 0; q < PF; ++q)
         if (b + lane + q * TPR < e) s += h.v[q] * __ldg(x + (base + static_cast<int>(h.c[q])));
+    int k = b + lane + PF * TPR;
+    if constexpr (TPR > 1) {
+        // Shared rows are long: take the lane's entries eight at a time --
+        // all eight columns and values, then all eight x gathers, then the
+        // products in entry order (the same additions as the loop below) --
+        // so eight gathers are in flight per lane instead of four (the
+        // coarse sweeps stall on load latency, not on bandwidth).
+        constexpr int B = 8;
+        for (; k + (B - 1) * TPR < e; k += B * TPR) {
+            CI c[B];
+            T v[B], xv[B];
+#pragma unroll
+            for (int q = 0; q < B; ++q) {
+                c[q] = co[k + q * TPR];
+                v[q] = ldv<T>(va, k + q * TPR);
+            }
+#pragma unroll
+            for (int q = 0; q < B; ++q) xv[q] = __ldg(x + (base + static_cast<int>(c[q])));
+#pragma unroll
+            for (int q = 0; q < B; ++q) s += v[q] * xv[q];
+        }
+    }
 #pragma unroll 4
-    for (int k = b + lane + PF * TPR; k < e; k += TPR)
+    for (; k < e; k += TPR)
         s += ldv<T>(va, k) * __ldg(x + (base + static_cast<int>(co[k])));
     return row_reduce<T, TPR>(s, lane);
 }
