@@ -13,6 +13,8 @@
 //
 // Level 0 is launched directly with the caller's vectors; levels >= 1 are
 // captured once into a CUDA graph with fixed buffers and replayed.
+#include <cusolverDn.h>
+
 #include <cmath>
 #include <limits>
 #include <type_traits>
@@ -427,6 +429,25 @@ __global__ void k_gj_eliminate(int n, double* a, const double* factors, int k) {
     a[idx] -= f * a[static_cast<size_t>(k) * 2 * n + j];
 }
 
+// A^T, dense column-major (so element (j, i) of the array is a_ij): the LU
+// path solves A^T X = I, whose column-major X read row-major is A^-1.
+__global__ void k_dense_init_t(int n, const int* ro, const int* co, const double* va, double* at) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    for (int k = ro[i]; k < ro[i + 1]; ++k) at[static_cast<size_t>(i) * n + co[k]] += va[k];
+}
+
+__global__ void k_identity(int64_t n, double* x) {
+    const int64_t idx = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (idx < n * n) x[idx] = (idx / n == idx % n) ? 1.0 : 0.0;
+}
+
+template <class S>
+__global__ void k_dense_copy(int64_t count, const double* __restrict__ a, S* __restrict__ b) {
+    const int64_t idx = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (idx < count) b[idx] = static_cast<S>(a[idx]);
+}
+
 template <class S>
 __global__ void k_gj_extract(int n, const double* a, S* inv) {
     const size_t idx = static_cast<size_t>(blockIdx.x) * blockDim.x + threadIdx.x;
@@ -685,33 +706,60 @@ void upload_level(cfdxg_context* ctx, DevLevel<T>& D, const AmgLevel& H, bool wi
     }
 }
 
-// FP64 Gauss-Jordan inverse of the dense coarse level from its device CSR.
+// The dense coarse level's inverse, formed in FP64 from its device CSR by LU
+// with partial pivoting (cuSOLVER getrf, then getrs on the identity) and
+// stored FP32 (or FP64 with dense_fp64).  A singular level sets the status
+// word's non-finite flag.  This is set-up work (once per setup and per
+// numeric refresh); the cycle applies the stored inverse with its own kernel.
+// (The earlier one-column-per-step Gauss-Jordan took 1.5 s at 5,287 rows:
+// every pivot step read and wrote the whole n x 2n augmented matrix.)
 template <class T>
 void build_dense_inverse_dev(cfdxg_context* ctx, DevHierarchy<T>& d, int n, const int* ro, const int* co,
                              const double* va) {
-    DevBuf<double> a, f;
-    a.resize(static_cast<std::size_t>(n) * 2 * n);
-    f.resize(n);
-    if (d.dense_fp64) d.dense64.resize(static_cast<std::size_t>(n) * n);
-    else d.dense.resize(static_cast<std::size_t>(n) * n);
-    k_gj_init<<<blocks_for(n, kT), kT, 0, ctx->stream>>>(n, ro, co, va, a.get());
+    const std::size_t nn = static_cast<std::size_t>(n) * n;
+    DevBuf<double> at, x;
+    DevBuf<int> ipiv, info;
+    at.resize(nn);
+    x.resize(nn);
+    ipiv.resize(n);
+    info.resize(1);
+    if (d.dense_fp64) d.dense64.resize(nn);
+    else d.dense.resize(nn);
+    cudaStream_t s = ctx->stream;
+    CFDXG_CUDA(cudaMemsetAsync(at.get(), 0, sizeof(double) * nn, s));
+    k_dense_init_t<<<blocks_for(n, kT), kT, 0, s>>>(n, ro, co, va, at.get());
     check_launch(ctx);
-    const size_t total = static_cast<size_t>(n) * 2 * n;
-    const int eb = static_cast<int>((total + kT - 1) / kT);
-    for (int k = 0; k < n; ++k) {
-        k_gj_pivot<<<1, kT, 0, ctx->stream>>>(n, a.get(), f.get(), k, ctx->scratch.status);
-        check_launch(ctx);
-        k_gj_eliminate<<<eb, kT, 0, ctx->stream>>>(n, a.get(), f.get(), k);
-        check_launch(ctx);
-    }
+    k_identity<<<blocks_for(static_cast<int64_t>(nn), kT), kT, 0, s>>>(n, x.get());
+    check_launch(ctx);
+    cusolverDnHandle_t h = nullptr;
+    if (cusolverDnCreate(&h) != CUSOLVER_STATUS_SUCCESS)
+        throw Error(CFDXG_ERR_CUDA, "cusolverDnCreate failed");
+    struct HandleGuard {
+        cusolverDnHandle_t h;
+        ~HandleGuard() { cusolverDnDestroy(h); }
+    } guard{h};
+    if (cusolverDnSetStream(h, s) != CUSOLVER_STATUS_SUCCESS) throw Error(CFDXG_ERR_CUDA, "cusolverDnSetStream failed");
+    int lwork = 0;
+    if (cusolverDnDgetrf_bufferSize(h, n, n, at.get(), n, &lwork) != CUSOLVER_STATUS_SUCCESS)
+        throw Error(CFDXG_ERR_CUDA, "cusolverDnDgetrf_bufferSize failed");
+    DevBuf<double> work(static_cast<std::size_t>(std::max(lwork, 1)));
+    // at holds A^T column-major: factor it, then solve A^T X = I
+    if (cusolverDnDgetrf(h, n, n, at.get(), n, work.get(), ipiv.get(), info.get()) != CUSOLVER_STATUS_SUCCESS ||
+        cusolverDnDgetrs(h, CUBLAS_OP_N, n, n, at.get(), n, ipiv.get(), x.get(), n, info.get()) !=
+            CUSOLVER_STATUS_SUCCESS)
+        throw Error(CFDXG_ERR_CUDA, "dense coarse LU failed");
+    int host_info = 0;
+    CFDXG_CUDA(cudaMemcpyAsync(&host_info, info.get(), sizeof(int), cudaMemcpyDeviceToHost, s));
     if (d.dense_fp64)
-        k_gj_extract<double><<<blocks_for(static_cast<int64_t>(n) * n, kT), kT, 0, ctx->stream>>>(n, a.get(),
-                                                                                                d.dense64.get());
+        k_dense_copy<double><<<blocks_for(static_cast<int64_t>(nn), kT), kT, 0, s>>>(static_cast<int64_t>(nn),
+                                                                                   x.get(), d.dense64.get());
     else
-        k_gj_extract<float><<<blocks_for(static_cast<int64_t>(n) * n, kT), kT, 0, ctx->stream>>>(n, a.get(),
-                                                                                               d.dense.get());
+        k_dense_copy<float><<<blocks_for(static_cast<int64_t>(nn), kT), kT, 0, s>>>(static_cast<int64_t>(nn),
+                                                                                  x.get(), d.dense.get());
     check_launch(ctx);
-    CFDXG_CUDA(cudaStreamSynchronize(ctx->stream));
+    CFDXG_CUDA(cudaStreamSynchronize(s));
+    if (host_info != 0) throw Error(CFDXG_ERR_SETUP, "dense coarse level is singular (LU pivot " +
+                                                         std::to_string(host_info) + ")");
 }
 
 template <class T>
