@@ -548,7 +548,17 @@ void co_spmv(int64_t n, const int64_t* ro, const int64_t* co, const double* va, 
 
 /* ----------------------------------------------------------- V-cycle */
 
-/* amg_preconditioner.h:2369-2409 damped Jacobi, x += omega * inv_diag (r - A x) */
+/* amg_preconditioner.h:1310-1319 remove_constant: subtract the mean, summed in order */
+static void remove_constant(int64_t n, double* v) {
+    if (n == 0) return;
+    double mean = 0.0;
+    for (int64_t i = 0; i < n; ++i) mean += v[i];
+    mean /= (double)n;
+    for (int64_t i = 0; i < n; ++i) v[i] -= mean;
+}
+
+/* amg_preconditioner.h:2369-2409 damped Jacobi, x += omega * inv_diag (r - A x),
+ * the mean removed after every sweep under the constant null space */
 static int smooth(const co_hierarchy_t* h, int l, const double* r, double* x, int sweeps, double* ax) {
     const int64_t n = h->n_rows[l];
     for (int s = 0; s < sweeps; ++s) {
@@ -558,6 +568,7 @@ static int smooth(const co_hierarchy_t* h, int l, const double* r, double* x, in
             x[i] += h->omega * delta;
             if (!isfinite(x[i])) return fail("non-finite smoother update");
         }
+        if (h->constant_null_space) remove_constant(n, x);
     }
     return 0;
 }
@@ -574,44 +585,54 @@ static int coarsest(const co_hierarchy_t* h, int l, const double* r, double* x) 
         return rc;
     }
     free(ax);
-    double m[16 * 16], b[16], sol[16];
-    for (int64_t q = 0; q < n * n; ++q) m[q] = 0.0;
+    /* :2590-2611 under the constant null space, the system bordered by a row
+     * and a column of ones (a zero-mean correction) */
+    const int64_t sn = n + (h->constant_null_space ? 1 : 0);
+    double m[17 * 17], b[17], sol[17];
+    for (int64_t q = 0; q < sn * sn; ++q) m[q] = 0.0;
+    for (int64_t i = 0; i < sn; ++i) b[i] = 0.0;
     for (int64_t i = 0; i < n; ++i) {
         b[i] = r[i];
         for (int64_t k = h->row_offsets[l][i]; k < h->row_offsets[l][i + 1]; ++k)
-            m[i * n + h->columns[l][k]] += h->values[l][k];
+            m[i * sn + h->columns[l][k]] += h->values[l][k];
     }
+    if (h->constant_null_space)
+        for (int64_t i = 0; i < n; ++i) {
+            m[i * sn + n] = 1.0;
+            m[n * sn + i] = 1.0;
+        }
     double scale = 0.0;
-    for (int64_t q = 0; q < n * n; ++q) scale = fmax(scale, fabs(m[q]));
+    for (int64_t q = 0; q < sn * sn; ++q) scale = fmax(scale, fabs(m[q]));
     const double tol = 128.0 * DBL_EPSILON * fmax(1.0, scale);
-    for (int64_t k = 0; k < n; ++k) {
+    for (int64_t k = 0; k < sn; ++k) {
         int64_t piv = k;
-        double pa = fabs(m[k * n + k]);
-        for (int64_t i = k + 1; i < n; ++i)
-            if (fabs(m[i * n + k]) > pa) { pa = fabs(m[i * n + k]); piv = i; }
+        double pa = fabs(m[k * sn + k]);
+        for (int64_t i = k + 1; i < sn; ++i)
+            if (fabs(m[i * sn + k]) > pa) { pa = fabs(m[i * sn + k]); piv = i; }
         if (!isfinite(pa) || pa <= tol) return fail("singular coarsest level");
         if (piv != k) {
-            for (int64_t j = k; j < n; ++j) { const double t = m[k * n + j]; m[k * n + j] = m[piv * n + j]; m[piv * n + j] = t; }
+            for (int64_t j = k; j < sn; ++j) { const double t = m[k * sn + j]; m[k * sn + j] = m[piv * sn + j]; m[piv * sn + j] = t; }
             const double t = b[k]; b[k] = b[piv]; b[piv] = t;
         }
-        const double dg = m[k * n + k];
-        for (int64_t i = k + 1; i < n; ++i) {
-            const double factor = m[i * n + k] / dg;
+        const double dg = m[k * sn + k];
+        for (int64_t i = k + 1; i < sn; ++i) {
+            const double factor = m[i * sn + k] / dg;
             if (!isfinite(factor)) return fail("non-finite elimination factor");
-            m[i * n + k] = 0.0;
-            for (int64_t j = k + 1; j < n; ++j) m[i * n + j] -= factor * m[k * n + j];
+            m[i * sn + k] = 0.0;
+            for (int64_t j = k + 1; j < sn; ++j) m[i * sn + j] -= factor * m[k * sn + j];
             b[i] -= factor * b[k];
         }
     }
-    for (int64_t ii = n; ii-- > 0;) {
+    for (int64_t ii = sn; ii-- > 0;) {
         double sum = b[ii];
-        for (int64_t j = ii + 1; j < n; ++j) sum -= m[ii * n + j] * sol[j];
-        const double dg = m[ii * n + ii];
+        for (int64_t j = ii + 1; j < sn; ++j) sum -= m[ii * sn + j] * sol[j];
+        const double dg = m[ii * sn + ii];
         if (!isfinite(dg) || fabs(dg) <= tol) return fail("singular coarsest level");
         sol[ii] = sum / dg;
         if (!isfinite(sol[ii])) return fail("non-finite coarsest solution");
     }
     for (int64_t i = 0; i < n; ++i) x[i] = sol[i];
+    if (h->constant_null_space) remove_constant(n, x);
     return 0;
 }
 
@@ -632,6 +653,7 @@ static int vcycle(const co_hierarchy_t* h, int l, const double* r, double* x) {
         for (int64_t k = h->p_offsets[l][i]; k < h->p_offsets[l][i + 1]; ++k)
             cr[h->p_columns[l][k]] += h->p_values[l][k] * res;
     }
+    if (h->constant_null_space) remove_constant(nc, cr);
     if (vcycle(h, l + 1, cr, cx)) goto done;
     /* prolongation: x_i += sum_k p_ik e_k in P's row order */
     for (int64_t i = 0; i < n; ++i) {
@@ -639,12 +661,15 @@ static int vcycle(const co_hierarchy_t* h, int l, const double* r, double* x) {
             x[i] += h->p_values[l][k] * cx[h->p_columns[l][k]];
         if (!isfinite(x[i])) { fail("non-finite prolongation"); goto done; }
     }
+    if (h->constant_null_space) remove_constant(n, x);
     rc = smooth(h, l, r, x, h->post_sweeps, ax);
 done:
     free(ax); free(cr); free(cx);
     return rc;
 }
 
+/* amg_preconditioner.h:1191-1203 apply: the cycle from z = 0 on r, with the
+ * mean removed from a copy of r and from z under the constant null space */
 int co_vcycle(const co_hierarchy_t* h, const double* r, double* z) {
     if (!h || h->n_levels <= 0) return fail("empty hierarchy");
     const int64_t n = h->n_rows[0];
@@ -652,7 +677,18 @@ int co_vcycle(const co_hierarchy_t* h, const double* r, double* z) {
         if (!isfinite(r[i])) return fail("non-finite residual");
         z[i] = 0.0;
     }
-    if (vcycle(h, 0, r, z)) return -1;
+    if (h->constant_null_space) {
+        double* rc = malloc(sizeof(double) * (size_t)(n > 0 ? n : 1));
+        if (!rc) return fail("out of memory");
+        memcpy(rc, r, sizeof(double) * (size_t)n);
+        remove_constant(n, rc);
+        const int bad = vcycle(h, 0, rc, z);
+        free(rc);
+        if (bad) return -1;
+        remove_constant(n, z);
+    } else if (vcycle(h, 0, r, z)) {
+        return -1;
+    }
     for (int64_t i = 0; i < n; ++i)
         if (!isfinite(z[i])) return fail("non-finite V-cycle result");
     return 0;
@@ -694,12 +730,86 @@ static int choose_restart(int current, double reduction) {
     return current < rmin ? rmin : (current > rmax ? rmax : current);
 }
 
+/* ------------------------------------------------------- null space */
+
+/* null_space.h:58-62 constant(n): ones scaled by 1 / their hypot-accumulated
+ * norm (:141-146 stable_norm), so every entry is this one value */
+double co_null_space_entry(int64_t n) {
+    double norm = 0.0;
+    for (int64_t i = 0; i < n; ++i) norm = hypot(norm, 1.0);
+    return 1.0 * (1.0 / norm);
+}
+
+/* null_space.h:64-71 remove: v -= (v . e) e with every e_i = e, the dot in order */
+static int ns_remove(int64_t n, double e, double* v) {
+    double c = 0.0;
+    for (int64_t i = 0; i < n; ++i) {
+        if (!isfinite(v[i])) return fail("cannot project a non-finite vector");
+        c += v[i] * e;
+    }
+    for (int64_t i = 0; i < n; ++i) v[i] -= c * e;
+    return 0;
+}
+
+static double hypot_norm(int64_t n, const double* a) {
+    double s = 0.0;
+    for (int64_t i = 0; i < n; ++i) s = hypot(s, a[i]);
+    return s;
+}
+
+int co_null_space_checks(int64_t n, const int64_t* ro, const int64_t* co, const double* va, const double* b,
+                         int32_t* out) {
+    out[0] = out[1] = out[2] = 0;
+    if (n <= 0) return 0;
+    const double e = co_null_space_entry(n);
+    /* :97-105 is_compatible: |b . e| <= 1e-14 + 1e-12 ||b|| */
+    double c = 0.0;
+    for (int64_t i = 0; i < n; ++i) c += b[i] * e;
+    const double component = sqrt(fmax(0.0, c * c));
+    out[0] = component <= 1e-14 + 1e-12 * hypot_norm(n, b);
+    /* :107-134 operator_residual: ||A e|| / ||A||_F (hypot sums), <= 1e-12 */
+    double fro = 0.0;
+    for (int64_t k = 0; k < ro[n]; ++k) {
+        if (!isfinite(va[k])) return fail("null space operator contains non-finite values");
+        fro = hypot(fro, va[k]);
+    }
+    double* y = calloc((size_t)n, sizeof(double));
+    if (!y) return fail("out of memory");
+    double pn = 0.0;
+    for (int64_t i = 0; i < n; ++i) {
+        double sum = 0.0;
+        for (int64_t k = ro[i]; k < ro[i + 1]; ++k) sum += va[k] * e;
+        pn = hypot(pn, sum);
+    }
+    out[1] = pn / fmax(fro, DBL_MIN) <= 1e-12;
+    /* projected_gmres.h:53-82: and ||A^T e|| <= 1e-12 ||A||_F */
+    for (int64_t i = 0; i < n; ++i)
+        for (int64_t k = ro[i]; k < ro[i + 1]; ++k) y[co[k]] += va[k] * e;
+    out[2] = out[1] && !(hypot_norm(n, y) > 1e-12 * fmax(fro, DBL_MIN));
+    free(y);
+    return 0;
+}
+
 typedef struct {
     int64_t n;
     const int64_t *ro, *co;
     const double* va;
     const co_hierarchy_t* h;
+    double ns;          /* entry of the constant null-space vector; 0: no projection */
+    double* scratch;    /* n values for the projected operator */
 } system_t;
+
+/* The Krylov operator: A, or projected_gmres.h:122-131 P A P */
+static int op_apply(const system_t* S, const double* in, double* out) {
+    if (S->ns == 0.0) {
+        co_spmv(S->n, S->ro, S->co, S->va, in, out);
+        return 0;
+    }
+    memcpy(S->scratch, in, sizeof(double) * (size_t)S->n);
+    if (ns_remove(S->n, S->ns, S->scratch)) return -1;
+    co_spmv(S->n, S->ro, S->co, S->va, S->scratch, out);
+    return ns_remove(S->n, S->ns, out);
+}
 
 static int gmres(const system_t* S, const double* b, double* x, int restart, int64_t max_iter, double tolerance,
                  co_report_t* R);
@@ -727,7 +837,7 @@ static int gmres(const system_t* S, const double* b, double* x, int restart, int
         /* :64-134: shifted solve A y = -A x0 */
         double* ax0 = malloc(sizeof(double) * n);
         if (!ax0) return fail("out of memory");
-        co_spmv(n, S->ro, S->co, S->va, x, ax0);
+        if (op_apply(S, x, ax0)) { free(ax0); return -1; }
         const double ax0n = norm2(n, ax0);
         if (!isfinite(ax0n)) { free(ax0); finish(R, 2, 0, ax0n, ax0n); return 0; }
         if (ax0n > 0.0) {
@@ -738,7 +848,7 @@ static int gmres(const system_t* S, const double* b, double* x, int restart, int
             co_report_t inner;
             if (gmres(S, sh, y, restart, max_iter, tolerance, &inner)) { free(ax0); free(sh); free(y); return -1; }
             for (int64_t i = 0; i < n; ++i) x[i] += y[i];
-            co_spmv(n, S->ro, S->co, S->va, x, ax0);
+            if (op_apply(S, x, ax0)) { free(ax0); free(sh); free(y); return -1; }
             for (int64_t i = 0; i < n; ++i) sh[i] = b[i] - ax0[i];
             const double res = norm2(n, sh), rel = res / ax0n;
             const int ok = isfinite(res) && isfinite(rel) && rel <= tolerance;
@@ -759,7 +869,7 @@ static int gmres(const system_t* S, const double* b, double* x, int restart, int
     if (!r || !w || !best || !trial || !tmp) { fail("out of memory"); goto out; }
 #define TRUE_RESIDUAL(dst)                                      \
     do {                                                        \
-        co_spmv(n, S->ro, S->co, S->va, x, tmp);                \
+        if (op_apply(S, x, tmp)) goto out;                      \
         for (int64_t i_ = 0; i_ < n; ++i_) r[i_] = b[i_] - tmp[i_]; \
         dst = norm2(n, r);                                      \
     } while (0)
@@ -805,8 +915,22 @@ static int gmres(const system_t* S, const double* b, double* x, int restart, int
         for (int j = 0; j < m && iterations < max_iter; ++j) {
             double* vj = V + (size_t)j * N;
             double* zj = Z + (size_t)j * N;
-            if (S->h) {
-                if (co_vcycle(S->h, vj, zj)) {
+            if (S->h || S->ns != 0.0) {
+                /* projected_gmres.h:32-44 ProjectedPreconditioner: P M P */
+                const double* in = vj;
+                if (S->ns != 0.0) {
+                    memcpy(trial, vj, sizeof(double) * N);
+                    if (ns_remove(n, S->ns, trial)) goto out;
+                    in = trial;
+                }
+                int bad = 0;
+                if (S->h) bad = co_vcycle(S->h, in, zj) != 0;
+                else memcpy(zj, in, sizeof(double) * N);
+                if (!bad && S->ns != 0.0) {
+                    for (int64_t i = 0; i < n; ++i) bad |= !isfinite(zj[i]);
+                    if (!bad) ns_remove(n, S->ns, zj);
+                }
+                if (bad) {
                     memcpy(x, best, sizeof(double) * N);
                     finish(R, 3, iterations, best_res, best_res / rhs_scale);
                     rc = 0;
@@ -816,7 +940,7 @@ static int gmres(const system_t* S, const double* b, double* x, int restart, int
             } else {
                 memcpy(zj, vj, sizeof(double) * N);
             }
-            co_spmv(n, S->ro, S->co, S->va, zj, w);
+            if (op_apply(S, zj, w)) goto out;
             action = norm2(n, w);
             if (!isfinite(action)) { memcpy(x, best, sizeof(double) * N); finish(R, 2, iterations, best_res, best_res / rhs_scale); rc = 0; goto out; }
             /* :271-290 two passes of modified Gram-Schmidt */
@@ -882,7 +1006,7 @@ static int gmres(const system_t* S, const double* b, double* x, int restart, int
                         const double* zk = Z + (size_t)k * N;
                         for (int64_t i = 0; i < n; ++i) trial[i] += y[k] * zk[i];
                     }
-                    co_spmv(n, S->ro, S->co, S->va, trial, tmp);
+                    if (op_apply(S, trial, tmp)) goto out;
                     for (int64_t i = 0; i < n; ++i) tmp[i] = b[i] - tmp[i];
                     const double verified = norm2(n, tmp);
                     if (!isfinite(verified) || verified / fmax(est, 1e-300) > 10.0) {
@@ -950,10 +1074,61 @@ out:
 int co_solve_gmres(int64_t n, const int64_t* ro, const int64_t* co, const double* va, const co_hierarchy_t* h,
                    const double* b, double* x, int32_t restart, int64_t max_iterations, double tolerance,
                    co_report_t* report) {
-    const system_t S = {n, ro, co, va, h};
+    const system_t S = {n, ro, co, va, h, 0.0, NULL};
     co_report_t local;
     co_report_t* R = report ? report : &local;
     return gmres(&S, b, x, restart, max_iterations, tolerance, R);
+}
+
+int co_solve_projected_gmres(int64_t n, const int64_t* ro, const int64_t* co, const double* va,
+                             const co_hierarchy_t* h, const double* b, double* x, int32_t restart,
+                             int64_t max_iterations, double tolerance, co_report_t* report) {
+    co_report_t local;
+    co_report_t* R = report ? report : &local;
+    memset(R, 0, sizeof *R);
+    R->status = 3;
+    if (n <= 0 || restart <= 0 || max_iterations <= 0 || !(tolerance > 0.0) || !isfinite(tolerance)) return 0;
+    for (int64_t i = 0; i < n; ++i)
+        if (!isfinite(b[i]) || !isfinite(x[i])) return 0;
+    int32_t checks[3];
+    if (co_null_space_checks(n, ro, co, va, b, checks)) return -1;
+    if (!checks[0] || !checks[2]) return 0;
+    const size_t N = (size_t)n;
+    double* gf = malloc(sizeof(double) * N);
+    double* ax = malloc(sizeof(double) * N);
+    double* scratch = malloc(sizeof(double) * N);
+    int rc = -1;
+    if (!gf || !ax || !scratch) { fail("out of memory"); goto done; }
+    /* :101-104 a gauge-free copy of the iterate */
+    const double e = co_null_space_entry(n);
+    memcpy(gf, x, sizeof(double) * N);
+    if (ns_remove(n, e, gf)) goto done;
+    /* :105-119 already satisfied in physical coordinates */
+    co_spmv(n, ro, co, va, gf, ax);
+    double r0 = 0.0;
+    for (int64_t i = 0; i < n; ++i) r0 = hypot(r0, b[i] - ax[i]);
+    const double bn = hypot_norm(n, b);
+    if (r0 == 0.0 || (bn > 0.0 && r0 <= tolerance * bn)) {
+        R->status = 0;
+        R->residual = r0;
+        R->residual_relative = bn > 0.0 ? r0 / bn : 0.0;
+        memcpy(x, gf, sizeof(double) * N);
+        rc = 0;
+        goto done;
+    }
+    /* :120-141 FGMRES on P A P, preconditioned by P M P */
+    const system_t S = {n, ro, co, va, h, e, scratch};
+    if (gmres(&S, b, gf, restart, max_iterations, tolerance, R)) goto done;
+    int valid = 1;
+    for (int64_t i = 0; i < n; ++i) valid &= isfinite(gf[i]) != 0;
+    if (R->status != 3 && valid) {
+        if (ns_remove(n, e, gf)) goto done;
+        memcpy(x, gf, sizeof(double) * N);
+    }
+    rc = 0;
+done:
+    free(gf); free(ax); free(scratch);
+    return rc;
 }
 
 /* ---------------------------------------------------------------- CG */
@@ -965,9 +1140,11 @@ typedef struct {
     int32_t kind;
     const co_hierarchy_t* h;
     const double* diag;      /* kind 0: first diagonal entry; kind 2: its inverse */
+    double ns;               /* entry of the constant null-space vector; 0: none */
 } cg_pc_t;
 
-/* cg_solver.h:203-216 apply_preconditioner: z = M^-1 r, every entry finite */
+/* cg_solver.h:203-216 apply_preconditioner: z = M^-1 r (projected under a
+ * null space), every entry finite */
 static int cg_apply(const cg_pc_t* P, int64_t n, const double* r, double* z) {
     switch (P->kind) {
         case CO_CG_INTERNAL_JACOBI:
@@ -980,8 +1157,12 @@ static int cg_apply(const cg_pc_t* P, int64_t n, const double* r, double* z) {
             for (int64_t i = 0; i < n; ++i) z[i] = P->diag[i] * r[i];
             break;
         default:
-            memset(z, 0, sizeof(double) * (size_t)n);
-            if (vcycle(P->h, 0, r, z)) return 0;
+            if (co_vcycle(P->h, r, z)) return 0;
+    }
+    if (P->ns != 0.0) {
+        for (int64_t i = 0; i < n; ++i)
+            if (!isfinite(z[i])) return 0;
+        ns_remove(n, P->ns, z);
     }
     for (int64_t i = 0; i < n; ++i)
         if (!isfinite(z[i])) return 0;
@@ -991,6 +1172,12 @@ static int cg_apply(const cg_pc_t* P, int64_t n, const double* r, double* z) {
 int co_solve_cg(int64_t n, const int64_t* ro, const int64_t* co, const double* va, int32_t preconditioner,
                 const co_hierarchy_t* h, const double* b, double* x, int64_t max_iter, double tolerance,
                 co_report_t* report) {
+    return co_solve_cg_ns(n, ro, co, va, preconditioner, h, b, x, max_iter, tolerance, 0, report);
+}
+
+int co_solve_cg_ns(int64_t n, const int64_t* ro, const int64_t* co, const double* va, int32_t preconditioner,
+                   const co_hierarchy_t* h, const double* b, double* x, int64_t max_iter, double tolerance,
+                   int32_t null_space, co_report_t* report) {
     co_report_t local;
     co_report_t* R = report ? report : &local;
     memset(R, 0, sizeof *R);
@@ -1000,16 +1187,26 @@ int co_solve_cg(int64_t n, const int64_t* ro, const int64_t* co, const double* v
         preconditioner != CO_CG_JACOBI && preconditioner != CO_CG_AMG)
         return fail("unknown CG preconditioner %d", (int)preconditioner);
     const int has_pc = preconditioner != CO_CG_INTERNAL_JACOBI;
+    double ns = 0.0;
+    if (null_space) {
+        /* :74-79 a compatible right-hand side and A e = 0, else NOT_APPLICABLE */
+        int32_t checks[3];
+        if (co_null_space_checks(n, ro, co, va, b, checks)) return -1;
+        if (!checks[0] || !checks[1]) { R->status = 3; return 0; }
+        ns = co_null_space_entry(n);
+    }
     for (int64_t k = 0; k < ro[n]; ++k)
         if (!isfinite(va[k])) { R->status = 2; return 0; }
     for (int64_t i = 0; i < n; ++i)
         if (!isfinite(b[i]) || !isfinite(x[i])) { R->status = 2; return 0; }
+    if (ns != 0.0) ns_remove(n, ns, x);                            /* :93 */
     const size_t N = (size_t)n;
     double *r = malloc(sizeof(double) * N), *rv = malloc(sizeof(double) * N), *z = malloc(sizeof(double) * N);
     double *p = malloc(sizeof(double) * N), *Ap = malloc(sizeof(double) * N), *M = calloc(N, sizeof(double));
     int rc = -1;
     if (!r || !rv || !z || !p || !Ap || !M) { fail("out of memory"); goto out; }
-    cg_pc_t P = {preconditioner, h, M};
+    cg_pc_t P = {preconditioner, h, M, ns};
+#define NS_REMOVE(v) do { if (ns != 0.0) ns_remove(n, ns, (v)); } while (0)
     double homogeneous = 0.0;
     /* cg_solver.h:108-120 update_true_residual (reports of failed solves) */
 #define TRUE_RES()                                                                   \
@@ -1042,6 +1239,7 @@ int co_solve_cg(int64_t n, const int64_t* ro, const int64_t* co, const double* v
 #define APPLY() (++R->preconditioner_applications, cg_apply(&P, n, r, z))
     /* :149-169 initial true residual, converged before any preconditioner work */
     TRUE_RES();
+    NS_REMOVE(rv);                                                 /* :149 */
     memcpy(r, rv, sizeof(double) * N);
     const double b_norm = norm2(n, b);
     const double initial = norm2(n, rv);
@@ -1072,6 +1270,7 @@ int co_solve_cg(int64_t n, const int64_t* ro, const int64_t* co, const double* v
     double at_last_replacement = INFINITY;
     for (int64_t iter = 1; iter <= max_iter; ++iter) {
         co_spmv(n, ro, co, va, p, Ap);
+        NS_REMOVE(Ap);                                             /* :262 */
         const double pAp = dot(n, p, Ap);
         if (!(pAp > 0.0) || !isfinite(pAp)) FAILED_REPORT(3, iter);
         const double alpha = rsold / pAp;
@@ -1079,6 +1278,12 @@ int co_solve_cg(int64_t n, const int64_t* ro, const int64_t* co, const double* v
         for (int64_t i = 0; i < n; ++i) {
             x[i] += alpha * p[i];
             r[i] -= alpha * Ap[i];
+        }
+        if (ns != 0.0) {                                           /* :295-298 */
+            for (int64_t i = 0; i < n; ++i)
+                if (!isfinite(x[i]) || !isfinite(r[i])) FAILED_REPORT(2, iter);
+            ns_remove(n, ns, x);
+            ns_remove(n, ns, r);
         }
         for (int64_t i = 0; i < n; ++i)
             if (!isfinite(x[i]) || !isfinite(r[i])) FAILED_REPORT(2, iter);
@@ -1095,6 +1300,7 @@ int co_solve_cg(int64_t n, const int64_t* ro, const int64_t* co, const double* v
             if (isfinite(rr) && rr <= tol_abs && res > tol_abs) {
                 ++R->residual_replacements;
                 memcpy(r, rv, sizeof(double) * N);
+                NS_REMOVE(r);                                      /* :376 */
                 if (!APPLY()) { R->status = 3; R->iterations = iter; rc = 0; goto out; }
                 const double replaced = dot(n, r, z);
                 if (!isfinite(replaced) || !(replaced > 0.0)) FINISH(1, iter, res);
@@ -1118,6 +1324,7 @@ int co_solve_cg(int64_t n, const int64_t* ro, const int64_t* co, const double* v
                 ++R->residual_replacements;
                 at_last_replacement = res;
                 memcpy(r, rv, sizeof(double) * N);
+                NS_REMOVE(r);                                      /* :517 */
                 if (!APPLY()) FAILED_REPORT(3, iter);
                 const double replaced = dot(n, r, z);
                 if (!isfinite(replaced) || !(replaced > 0.0)) FAILED_REPORT(3, iter);
@@ -1128,6 +1335,7 @@ int co_solve_cg(int64_t n, const int64_t* ro, const int64_t* co, const double* v
         }
         const double beta = rsnew / rsold;
         for (int64_t i = 0; i < n; ++i) p[i] = z[i] + beta * p[i];
+        NS_REMOVE(p);                                              /* :558 */
         rsold = rsnew;
     }
     TRUE_RES();
@@ -1136,6 +1344,7 @@ int co_solve_cg(int64_t n, const int64_t* ro, const int64_t* co, const double* v
 #undef FAILED_REPORT
 #undef FINISH
 #undef APPLY
+#undef NS_REMOVE
 out:
     free(r); free(rv); free(z); free(p); free(Ap); free(M);
     return rc;

@@ -122,6 +122,12 @@ typedef struct {
     const double* const* p_values;
     double omega;
     int32_t pre_sweeps, post_sweeps;
+    /* the constant_null_space flag of the native AMG (hypre_amg.h:35,
+     * amg_preconditioner.h:1197-1201, 2382, 2406, 2430, 2440, 2590-2664):
+     * mean subtraction on the cycle's input and output, after every smoother
+     * sweep, after the restriction and after the prolongation; the <= 16-row
+     * coarsest level solves the system bordered by a row and column of ones */
+    int32_t constant_null_space;
 } co_hierarchy_t;
 
 int co_vcycle(const co_hierarchy_t* h, const double* r, double* z);
@@ -152,6 +158,29 @@ int co_solve_cg(int64_t n, const int64_t* row_offsets, const int64_t* columns,
                 const double* values, int32_t preconditioner, const co_hierarchy_t* h,
                 const double* b, double* x, int64_t max_iterations, double tolerance,
                 co_report_t* report);
+
+/* The constant null space (core/linalg/null_space.h, projected_gmres.h).
+ * co_null_space_entry: every entry of NullSpaceProjector::constant(n)'s basis
+ * vector (null_space.h:58-62: ones over their hypot-accumulated norm).
+ * co_null_space_checks: out[0] is_compatible(b) (null_space.h:97-105),
+ * out[1] is_null_space(A) (:107-134), out[2] is_bilateral_null_space(A)
+ * (projected_gmres.h:53-82), each 0 or 1.
+ * co_solve_projected_gmres: solve_projected_gmres (projected_gmres.h:84-150),
+ * the right-preconditioned FGMRES of co_solve_gmres on P A P with the
+ * preconditioner P M P (h may be NULL: the identity); x untouched and status 3
+ * when the checks fail.
+ * co_solve_cg_ns: co_solve_cg with the NullSpaceProjector of
+ * cg_solver.h:74-79, 93, 149, 203, 262, 295-298, 376, 419, 517, 558
+ * (null_space 0: exactly co_solve_cg). */
+double co_null_space_entry(int64_t n);
+int co_null_space_checks(int64_t n, const int64_t* row_offsets, const int64_t* columns, const double* values,
+                         const double* b, int32_t* out);
+int co_solve_projected_gmres(int64_t n, const int64_t* row_offsets, const int64_t* columns,
+                             const double* values, const co_hierarchy_t* h, const double* b, double* x,
+                             int32_t restart, int64_t max_iterations, double tolerance, co_report_t* report);
+int co_solve_cg_ns(int64_t n, const int64_t* row_offsets, const int64_t* columns, const double* values,
+                   int32_t preconditioner, const co_hierarchy_t* h, const double* b, double* x,
+                   int64_t max_iterations, double tolerance, int32_t null_space, co_report_t* report);
 
 /* Pressure gauge of a pure-Neumann system.  co_gauge_eliminate: the
  * pure-Neumann branch of the corrector (physics/steady_incompressible_solver.h

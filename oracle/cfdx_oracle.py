@@ -52,7 +52,8 @@ class CoHierarchy(C.Structure):
                 ("values", C.POINTER(_c_f64p)), ("inv_diag", C.POINTER(_c_f64p)),
                 ("p_offsets", C.POINTER(_c_i64p)), ("p_columns", C.POINTER(_c_i64p)),
                 ("p_values", C.POINTER(_c_f64p)), ("omega", C.c_double),
-                ("pre_sweeps", C.c_int32), ("post_sweeps", C.c_int32)]
+                ("pre_sweeps", C.c_int32), ("post_sweeps", C.c_int32),
+                ("constant_null_space", C.c_int32)]
 
 
 _lib = None
@@ -85,6 +86,13 @@ def lib():
                                                                           C.c_void_p]
             L.co_solve_cg.argtypes = [C.c_int64] + [C.c_void_p] * 3 + [C.c_int32] + [C.c_void_p] * 3 + [
                 C.c_int64, C.c_double, C.c_void_p]
+            L.co_solve_cg_ns.argtypes = [C.c_int64] + [C.c_void_p] * 3 + [C.c_int32] + [C.c_void_p] * 3 + [
+                C.c_int64, C.c_double, C.c_int32, C.c_void_p]
+            L.co_solve_projected_gmres.argtypes = [C.c_int64] + [C.c_void_p] * 6 + [C.c_int32, C.c_int64,
+                                                                                    C.c_double, C.c_void_p]
+            L.co_null_space_entry.restype = C.c_double
+            L.co_null_space_entry.argtypes = [C.c_int64]
+            L.co_null_space_checks.argtypes = [C.c_int64] + [C.c_void_p] * 5
             _lib = L
     return _lib
 
@@ -189,7 +197,7 @@ class Hierarchy:
     inv_diag and, on all but the last level, p_offsets, p_columns, p_values)
     with the reference's V(pre, post) damped-Jacobi cycle."""
 
-    def __init__(self, levels, omega, pre_sweeps=6, post_sweeps=6):
+    def __init__(self, levels, omega, pre_sweeps=6, post_sweeps=6, constant_null_space=False):
         L = len(levels)
         self.levels = [{k: (None if v is None else np.ascontiguousarray(v)) for k, v in lv.items()} for lv in levels]
         lv = self.levels
@@ -214,6 +222,7 @@ class Hierarchy:
         (h.row_offsets, h.columns, h.values, h.inv_diag, h.p_offsets, h.p_columns, h.p_values) = self._arrays
         h.omega = float(omega)
         h.pre_sweeps, h.post_sweeps = int(pre_sweeps), int(post_sweeps)
+        h.constant_null_space = int(bool(constant_null_space))
 
     @property
     def ptr(self):
@@ -239,17 +248,45 @@ CG_PRECONDITIONERS = {"internal_jacobi": 0, "none": 1, "jacobi": 2, "native_amg"
 
 
 def solve_cg(ro, co, va, b, preconditioner="native_amg", hierarchy=None, x0=None, max_iterations=1000,
-             tolerance=1e-8):
-    """co_solve_cg: the reference's CG (cg_solver.h:45-560) with the solver's
+             tolerance=1e-8, null_space=False):
+    """co_solve_cg_ns: the reference's CG (cg_solver.h:45-560) with the solver's
     own diagonal ("internal_jacobi") or the dispatch's identity / Jacobi /
-    native-AMG preconditioner object (the AMG one applies ``hierarchy``)."""
+    native-AMG preconditioner object (the AMG one applies ``hierarchy``);
+    null_space: the constant NullSpaceProjector of the solve."""
     ro, co, va, b = (np.ascontiguousarray(ro, np.int64), np.ascontiguousarray(co, np.int64), _f64(va), _f64(b))
     x = np.zeros_like(b) if x0 is None else np.array(x0, dtype=np.float64)
     rep = CoReport()
-    _check(lib().co_solve_cg(b.size, _p(ro), _p(co), _p(va), CG_PRECONDITIONERS[preconditioner],
-                             hierarchy.ptr if hierarchy else None, _p(b), _p(x), int(max_iterations),
-                             float(tolerance), C.byref(rep)), "CG")
+    _check(lib().co_solve_cg_ns(b.size, _p(ro), _p(co), _p(va), CG_PRECONDITIONERS[preconditioner],
+                                hierarchy.ptr if hierarchy else None, _p(b), _p(x), int(max_iterations),
+                                float(tolerance), int(bool(null_space)), C.byref(rep)), "CG")
     return x, rep.as_dict()
+
+
+def solve_projected_gmres(ro, co, va, b, hierarchy=None, x0=None, restart=30, max_iterations=1000,
+                          tolerance=1e-8):
+    """co_solve_projected_gmres: solve_projected_gmres (projected_gmres.h:84-150),
+    FGMRES on P A P preconditioned by P M P; status 3 with x unchanged when the
+    right-hand side or the operator does not fit the constant null space."""
+    ro, co, va, b = (np.ascontiguousarray(ro, np.int64), np.ascontiguousarray(co, np.int64), _f64(va), _f64(b))
+    x = np.zeros_like(b) if x0 is None else np.array(x0, dtype=np.float64)
+    rep = CoReport()
+    _check(lib().co_solve_projected_gmres(b.size, _p(ro), _p(co), _p(va), hierarchy.ptr if hierarchy else None,
+                                          _p(b), _p(x), int(restart), int(max_iterations), float(tolerance),
+                                          C.byref(rep)), "projected GMRES")
+    return x, rep.as_dict()
+
+
+def null_space_entry(n):
+    """Every entry of NullSpaceProjector::constant(n)'s normalised basis vector."""
+    return lib().co_null_space_entry(int(n))
+
+
+def null_space_checks(ro, co, va, b):
+    """(is_compatible(b), is_null_space(A), is_bilateral_null_space(A)) of the constant null space."""
+    ro, co, va, b = (np.ascontiguousarray(ro, np.int64), np.ascontiguousarray(co, np.int64), _f64(va), _f64(b))
+    out = np.zeros(3, np.int32)
+    _check(lib().co_null_space_checks(b.size, _p(ro), _p(co), _p(va), _p(b), _p(out)), "null-space checks")
+    return tuple(bool(v) for v in out)
 
 
 def gauge_eliminate(ro, co, va, b, ref):

@@ -205,12 +205,15 @@ def spmv(ro, co, va, x):
 class Amg:
     """The reference's native Boomer-style AMG, Balanced policy."""
 
-    def __init__(self, ro, co, va, require_smoother_certificate=False):
+    def __init__(self, ro, co, va, require_smoother_certificate=False, constant_null_space=False):
         self.ro, self.co, self.va = (np.ascontiguousarray(ro, np.int64), np.ascontiguousarray(co, np.int64),
                                      np.ascontiguousarray(va, np.float64))
         sec = C.c_double()
-        self.h = lib().ref_amg_create(self.ro.size - 1, _p(self.ro), _p(self.co), _p(self.va),
-                                      int(require_smoother_certificate), C.byref(sec))
+        f = lib().ref_amg_create_ns
+        f.restype = C.c_void_p
+        f.argtypes = [C.c_int64] + [C.c_void_p] * 3 + [C.c_int32, C.c_int32, C.c_void_p]
+        self.h = f(self.ro.size - 1, _p(self.ro), _p(self.co), _p(self.va), int(require_smoother_certificate),
+                   int(bool(constant_null_space)), C.byref(sec))
         if not self.h:
             raise RuntimeError(f"reference AMG setup failed: {lib().ref_last_error().decode()}")
         self.setup_seconds = sec.value
@@ -275,7 +278,7 @@ class AmgFromLevels(Amg):
     """The reference's V-cycle/GMRES around a supplied hierarchy (list of level dicts with
     row_offsets, columns, values, inv_diag, p_offsets, p_columns, p_values) and damping."""
 
-    def __init__(self, levels, omega):
+    def __init__(self, levels, omega, constant_null_space=False):
         L = len(levels)
         self._keep = levels
         self.ro, self.co, self.va = levels[0]["row_offsets"], levels[0]["columns"], levels[0]["values"]
@@ -293,6 +296,9 @@ class AmgFromLevels(Amg):
         if not self.h:
             raise RuntimeError(f"reference AMG from levels failed: {lib().ref_last_error().decode()}")
         self.setup_seconds = float("nan")
+        g = lib().ref_amg_set_constant_null_space
+        g.argtypes = [C.c_void_p, C.c_int32]
+        g(self.h, int(bool(constant_null_space)))
 
 
 class AmgFromTransfers(Amg):
@@ -361,6 +367,21 @@ def solve_linear_system(ro, co, va, rhs, x0=None, krylov=3, preconditioner=6, re
     rep = RefReport()
     _check(lib().ref_solve_linear_system(b.size, _p(ro), _p(co), _p(va), _p(b), _p(x), krylov, preconditioner,
                                          restart, max_iterations, tolerance, C.byref(rep)), "solve_linear_system")
+    return x, rep.as_dict()
+
+
+def solve_linear_system_null_space(ro, co, va, rhs, x0=None, krylov=3, preconditioner=6, restart=30,
+                                   max_iterations=1000, tolerance=1e-8, null_space=1):
+    """solve_linear_system with LinearSolverRequest::null_space (1: NullSpaceModel::Constant)."""
+    f = lib().ref_solve_linear_system_ns
+    f.argtypes = [C.c_int64] + [C.c_void_p] * 5 + [C.c_int32] * 3 + [C.c_int64, C.c_double, C.c_int32, C.c_void_p]
+    ro, co, va = (np.ascontiguousarray(ro, np.int64), np.ascontiguousarray(co, np.int64),
+                  np.ascontiguousarray(va, np.float64))
+    b = np.ascontiguousarray(rhs, np.float64)
+    x = np.zeros_like(b) if x0 is None else np.array(x0, dtype=np.float64)
+    rep = RefReport()
+    _check(f(b.size, _p(ro), _p(co), _p(va), _p(b), _p(x), krylov, preconditioner, restart, max_iterations,
+             tolerance, null_space, C.byref(rep)), "solve_linear_system (null space)")
     return x, rep.as_dict()
 
 

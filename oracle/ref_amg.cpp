@@ -61,13 +61,15 @@ struct AmgHandle {
 
 }  // namespace
 
-extern "C" void* ref_amg_create(int64_t n, const int64_t* ro, const int64_t* co,
-                                const double* va, int32_t require_cert, double* seconds) {
+// constant_null_space: the flag NativeBoomerAMGPreconditioner passes through
+// (hypre_amg.cpp:211-212) when the dispatch solves with NullSpaceModel::Constant.
+extern "C" void* ref_amg_create_ns(int64_t n, const int64_t* ro, const int64_t* co, const double* va,
+                                   int32_t require_cert, int32_t constant_null_space, double* seconds) {
     try {
         auto h = std::make_unique<AmgHandle>();
         h->op = std::make_unique<OwnedOperator>(cfdx_ref::make_csr(n, ro, co, va));
         h->amg = std::make_unique<MatrixFreeVcyclePreconditioner>(
-            *h->op, 0.7, 6, 6, 0.25, 25, AMGInterpolationPolicy::DirectCF, false,
+            *h->op, 0.7, 6, 6, 0.25, 25, AMGInterpolationPolicy::DirectCF, constant_null_space != 0,
             require_cert != 0, AMGSmootherPolicy::DampedJacobi, 0.0, 0, 1.0);
         const double t0 = cfdx_ref::now_seconds();
         const bool ok = h->amg->setup(h->op->matrix_);
@@ -82,6 +84,11 @@ extern "C" void* ref_amg_create(int64_t n, const int64_t* ro, const int64_t* co,
         cfdx_ref::set_error(e);
         return nullptr;
     }
+}
+
+extern "C" void* ref_amg_create(int64_t n, const int64_t* ro, const int64_t* co,
+                                const double* va, int32_t require_cert, double* seconds) {
+    return ref_amg_create_ns(n, ro, co, va, require_cert, 0, seconds);
 }
 
 // Builds the reference preconditioner around an externally supplied hierarchy
@@ -223,6 +230,12 @@ extern "C" int ref_amg_update_values(void* hv, int64_t n, const int64_t* ro, con
 }
 
 extern "C" void ref_amg_destroy(void* h) { delete static_cast<AmgHandle*>(h); }
+
+// The cycle's constant_null_space flag on an existing handle (e.g. one built
+// from supplied levels); the hierarchy itself does not depend on it.
+extern "C" void ref_amg_set_constant_null_space(void* h, int32_t flag) {
+    static_cast<AmgHandle*>(h)->amg->constant_null_space_ = flag != 0;
+}
 
 extern "C" int32_t ref_amg_num_levels(void* h) {
     return static_cast<int32_t>(static_cast<AmgHandle*>(h)->amg->levels_.size());

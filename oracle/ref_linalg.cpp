@@ -142,6 +142,49 @@ extern "C" int ref_solve_linear_system(int64_t n, const int64_t* ro, const int64
     }
 }
 
+// solve_linear_system with the request's null-space model
+// (LinearSolverRequest::null_space, linear_solver_dispatch.h:360-400): with
+// NullSpaceModel::Constant the dispatch builds the native AMG with a constant
+// null space and runs solve_projected_gmres (projected_gmres.h:84-155) or the
+// projected CG (cg_solver.h:45-650).
+extern "C" int ref_solve_linear_system_ns(int64_t n, const int64_t* ro, const int64_t* co,
+                                          const double* va, const double* rhs, double* x,
+                                          int32_t krylov, int32_t preconditioner, int32_t restart,
+                                          int64_t max_iterations, double tolerance, int32_t null_space,
+                                          ref_report_t* report) {
+    try {
+        const SparseMatrix A = cfdx_ref::make_csr(n, ro, co, va);
+        Vector b(static_cast<std::size_t>(n)), xv(static_cast<std::size_t>(n));
+        for (int64_t i = 0; i < n; ++i) {
+            b(i) = rhs[i];
+            xv(i) = x[i];
+        }
+        LinearSolverRequest request;
+        request.krylov = static_cast<KrylovModel>(krylov);
+        request.preconditioner = static_cast<PreconditionerModel>(preconditioner);
+        request.gmres_restart = restart;
+        request.null_space = static_cast<NullSpaceModel>(null_space);
+        const LinearSolveReport r = solve_linear_system(
+            A, b, xv, LinearProblemKind::PressurePoisson, request,
+            static_cast<std::size_t>(max_iterations), tolerance);
+        for (int64_t i = 0; i < n; ++i) x[i] = xv(i);
+        if (report) {
+            report->status = static_cast<int32_t>(r.result.status);
+            report->iterations = static_cast<int64_t>(r.result.iterations);
+            report->residual = r.result.residual;
+            report->residual_relative = r.result.residual_relative;
+            report->physical_residual_relative = r.physical_residual_relative;
+            report->setup_seconds = 0.0;
+            report->solve_seconds = 0.0;
+        }
+        cfdx_ref::g_error = r.preconditioner_error;
+        return 0;
+    } catch (const std::exception& e) {
+        cfdx_ref::set_error(e);
+        return -1;
+    }
+}
+
 extern "C" int ref_spmv(int64_t n, const int64_t* ro, const int64_t* co, const double* va,
                         const double* x, double* y) {
     try {

@@ -11,6 +11,12 @@ inputs of tests/cases.py and stores its outputs:
   with its iteration count, and the CG + native-AMG solution of the
   reference's solve_linear_system to 1e-10 (cg_x, cg_iterations);
 * poisson_hex6.npz -- hex 6^3 Poisson system (CSR and right-hand side);
+* neumann_tet5.npz -- the Kuhn-tet 5^3 x 6 pressure-correction system with
+  no fixed-pressure patch (a constant null space) and its right-hand side
+  less its mean: CSR, the hierarchy of the native AMG built with
+  constant_null_space, one V-cycle of it (r, z), and the solutions of the
+  reference's solve_linear_system with NullSpaceModel::Constant -- FGMRES(30)
+  + native AMG to 1e-8 (projected GMRES) and CG + native AMG to 1e-10;
 * pressure_tet4.cfdxlin -- the pressure system of pressure_tet4.npz with a
   zero initial guess, written by the reference's write_linear_system_capture
   (PressurePoisson, no null space, tolerance 1e-8, 1000 iterations).
@@ -62,6 +68,35 @@ def pressure(n: int):
     np.savez_compressed(HERE / f"pressure_tet{n}.npz", **out)
 
 
+def neumann(n: int):
+    m = cases.simple_mesh(n)
+    g = ref.geometry(m, "fv")
+    U, rAU, aP, p, fixed, value = cases.simple_fields(m, g["cell_centres"])
+    fixed[:] = 0
+    a = ref.simple_assemble(m, U, rAU, p, 1.0, fixed, value)
+    ro, co, va = a["row_offsets"], a["columns"], a["values"]
+    b = a["b"] - a["b"].mean()
+    R = ref.Amg(ro, co, va, constant_null_space=True)
+    out = dict(n=n, row_offsets=ro, columns=co, values=va, b=b, n_levels=R.num_levels(), omega=R.omega)
+    for l in range(R.num_levels()):
+        lv = R.level(l)
+        for k in ("row_offsets", "columns", "values", "inv_diag"):
+            out[f"L{l}_{k}"] = lv[k]
+        if lv["p_offsets"] is not None:
+            for k in ("p_offsets", "p_columns", "p_values"):
+                out[f"L{l}_{k}"] = lv[k]
+    r = np.random.default_rng(13).standard_normal(ro.size - 1)
+    out.update(vcycle_r=r, vcycle_z=R.apply(r))
+    x, rep = ref.solve_linear_system_null_space(ro, co, va, b, krylov=4, preconditioner=6, restart=30,
+                                                tolerance=1e-8)
+    assert rep["status"] == 0
+    out.update(x=x, iterations=rep["iterations"])
+    xc, repc = ref.solve_linear_system_null_space(ro, co, va, b, krylov=1, preconditioner=6, tolerance=1e-10)
+    assert repc["status"] == 0
+    out.update(cg_x=xc, cg_iterations=repc["iterations"])
+    np.savez_compressed(HERE / f"neumann_tet{n}.npz", **out)
+
+
 def capture(n: int):
     z = np.load(HERE / f"pressure_tet{n}.npz")
     b = z["b"]
@@ -79,5 +114,6 @@ if __name__ == "__main__":
     pressure(4)
     capture(4)
     poisson(6)
+    neumann(5)
     for p in sorted(HERE.glob("*.npz")) + sorted(HERE.glob("*.cfdxlin")):
         print(p.name, p.stat().st_size)

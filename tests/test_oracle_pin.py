@@ -192,6 +192,113 @@ def test_invalid_inputs_fail_loudly():
     assert co.geometry(m)["cell_volumes"].min() > 0
 
 
+def _golden_levels(z):
+    levels = []
+    for l in range(int(z["n_levels"])):
+        lv = {k: z[f"L{l}_{k}"] for k in ("row_offsets", "columns", "values", "inv_diag")}
+        if f"L{l}_p_offsets" in z:
+            lv.update({k: z[f"L{l}_{k}"] for k in ("p_offsets", "p_columns", "p_values")})
+        levels.append(lv)
+    return levels
+
+
+def _neumann_pressure(n):
+    """The pressure-correction system without a fixed-pressure patch (a
+    constant null space), its right-hand side less its mean."""
+    m, g, U, rAU, p, fixed, value = _pressure_inputs(n)
+    a = co.simple_assemble(m, U, rAU, p, 1.0, np.zeros_like(fixed), value)
+    return a["row_offsets"], a["columns"], a["values"], a["b"] - a["b"].mean()
+
+
+def _neumann_poisson(n):
+    import cfdx_dev_b200 as cg
+    m = cg.hex_case(n)
+    ro, cols, va, rhs = co.assemble_diffusion(m, np.full(m.n_faces, np.nan), 1.0,
+                                              cg.random_field(m.n_cells, "uniform", -1.0, 1.0, 7))
+    return ro, cols, va, rhs - rhs.mean()
+
+
+@pytest.mark.parametrize("case", ["tet6", "tet8", "hex10"])
+def test_null_space_solves_match_reference(ref, case):
+    """NullSpaceModel::Constant (linear_solver_dispatch.h:354-400): the native
+    AMG's constant-null-space cycle (mean removals, bordered coarsest LU),
+    solve_projected_gmres for FGMRES and GMRES, and the projected CG with each
+    preconditioner object -- iterate and count bit-identical to the reference's
+    solve_linear_system."""
+    ro, cols, va, b = _neumann_poisson(10) if case == "hex10" else _neumann_pressure(int(case[3:]))
+    assert co.null_space_checks(ro, cols, va, b) == (True, True, True)
+    R = ref.Amg(ro, cols, va, constant_null_space=True)
+    H = co.Hierarchy([R.level(l) for l in range(R.num_levels())], R.omega, constant_null_space=True)
+    assert H.n_rows[-1] <= 16
+    for seed in (0, 1):
+        r = np.random.default_rng(seed).standard_normal(b.size)
+        assert np.array_equal(H.apply(r), R.apply(r))
+    for krylov in (4, 3):   # FGMRES, GMRES
+        x_ref, rep_ref = ref.solve_linear_system_null_space(ro, cols, va, b, krylov=krylov, preconditioner=6,
+                                                            restart=30, tolerance=1e-8)
+        x_co, rep_co = co.solve_projected_gmres(ro, cols, va, b, H, restart=30, tolerance=1e-8)
+        assert rep_co["status"] == rep_ref["status"] == 0
+        assert rep_co["iterations"] == rep_ref["iterations"]
+        assert np.array_equal(x_co, x_ref)
+    try:
+        Rc = ref.Amg(ro, cols, va, require_smoother_certificate=True, constant_null_space=True)
+        Hc = co.Hierarchy([Rc.level(l) for l in range(Rc.num_levels())], Rc.omega, constant_null_space=True)
+    except RuntimeError:
+        # the Jacobi certificate of CG's AMG refuses the hierarchy (the hex
+        # case's one-row coarsest level has a zero diagonal): NOT_APPLICABLE
+        Hc = None
+    for pc, model in (("native_amg", 6), ("jacobi", 2), ("none", 1)):
+        x_ref, rep_ref = ref.solve_linear_system_null_space(ro, cols, va, b, krylov=1, preconditioner=model,
+                                                            tolerance=1e-8)
+        if pc == "native_amg" and Hc is None:
+            assert rep_ref["status"] == 3
+            continue
+        x_co, rep_co = co.solve_cg(ro, cols, va, b, pc, Hc if pc == "native_amg" else None, tolerance=1e-8,
+                                   null_space=True)
+        assert rep_co["status"] == rep_ref["status"] == 0
+        assert rep_co["iterations"] == rep_ref["iterations"]
+        assert np.array_equal(x_co, x_ref)
+
+
+def test_null_space_cycle_with_swept_coarsest_level(ref):
+    """A hierarchy cut at a 52-row level: the coarsest treatment is 24 damped-
+    Jacobi sweeps from zero, each followed by the mean removal."""
+    ro, cols, va, b = _neumann_poisson(10)
+    R = ref.Amg(ro, cols, va, constant_null_space=True)
+    levels = [R.level(l) for l in range(4)]
+    assert levels[-1]["inv_diag"].size > 16
+    RT = ref.AmgFromLevels(levels, R.omega, constant_null_space=True)
+    H = co.Hierarchy(levels, R.omega, constant_null_space=True)
+    for seed in (0, 1, 2):
+        r = np.random.default_rng(seed).standard_normal(b.size)
+        assert np.array_equal(H.apply(r), RT.apply(r))
+
+
+def test_null_space_refusals(ref):
+    """An incompatible right-hand side or an operator without the constant
+    null space: NOT_APPLICABLE with the iterate untouched."""
+    ro, cols, va, b = _neumann_pressure(6)
+    bad_b = b + 1.0
+    assert co.null_space_checks(ro, cols, va, bad_b) == (False, True, True)
+    x0 = np.full(b.size, 0.25)
+    for krylov in (4, 1):
+        x_ref, rep_ref = ref.solve_linear_system_null_space(ro, cols, va, bad_b, x0=x0, krylov=krylov,
+                                                            preconditioner=1)
+        assert rep_ref["status"] == 3 and np.array_equal(x_ref, x0)
+    x_co, rep = co.solve_projected_gmres(ro, cols, va, bad_b, None, x0=x0)
+    assert rep["status"] == 3 and np.array_equal(x_co, x0)
+    x_co, rep = co.solve_cg(ro, cols, va, bad_b, "none", x0=x0, null_space=True)
+    assert rep["status"] == 3 and np.array_equal(x_co, x0)
+    # a Dirichlet-fixed system has no constant null space
+    m, g, U, rAU, p, fixed, value = _pressure_inputs(6)
+    a = co.simple_assemble(m, U, rAU, p, 1.0, fixed, value)
+    checks = co.null_space_checks(a["row_offsets"], a["columns"], a["values"], a["b"] - a["b"].mean())
+    assert checks[1:] == (False, False)
+    x_ref, rep_ref = ref.solve_linear_system_null_space(a["row_offsets"], a["columns"], a["values"],
+                                                        a["b"] - a["b"].mean(), krylov=4, preconditioner=1)
+    assert rep_ref["status"] == 3
+
+
 @pytest.mark.parametrize("name", sorted(p.stem for p in GOLDEN.glob("*.npz")))
 def test_oracle_reproduces_golden_fixtures(name):
     z = dict(np.load(GOLDEN / f"{name}.npz"))
@@ -216,6 +323,22 @@ def test_oracle_reproduces_golden_fixtures(name):
         assert np.array_equal(co.rhie_chow_flux(m, U, rAU, x, 1.0, fixed, value), z["flux_solved"])
         xc, repc = co.solve_cg(a["row_offsets"], a["columns"], a["values"], a["b"], "native_amg", H,
                                max_iterations=1000, tolerance=1e-10)
+        assert repc["status"] == 0 and repc["iterations"] == int(z["cg_iterations"])
+        assert np.array_equal(xc, z["cg_x"])
+    elif name.startswith("neumann"):
+        m, g, U, rAU, p, fixed, value = _pressure_inputs(n)
+        a = co.simple_assemble(m, U, rAU, p, 1.0, np.zeros_like(fixed), value)
+        for k in ("row_offsets", "columns", "values"):
+            assert np.array_equal(a[k], z[k]), k
+        assert np.array_equal(a["b"] - a["b"].mean(), z["b"])
+        ro, cols, va, b = z["row_offsets"], z["columns"], z["values"], z["b"]
+        assert co.null_space_checks(ro, cols, va, b) == (True, True, True)
+        H = co.Hierarchy(_golden_levels(z), float(z["omega"]), constant_null_space=True)
+        assert np.array_equal(H.apply(z["vcycle_r"]), z["vcycle_z"])
+        x, rep = co.solve_projected_gmres(ro, cols, va, b, H, restart=30, tolerance=1e-8)
+        assert rep["status"] == 0 and rep["iterations"] == int(z["iterations"])
+        assert np.array_equal(x, z["x"])
+        xc, repc = co.solve_cg(ro, cols, va, b, "native_amg", H, tolerance=1e-10, null_space=True)
         assert repc["status"] == 0 and repc["iterations"] == int(z["cg_iterations"])
         assert np.array_equal(xc, z["cg_x"])
     elif name.startswith("poisson"):
