@@ -57,7 +57,7 @@ class AmgOptions(C.Structure):
         ("require_smoother_certificate", C.c_int32), ("precision", C.c_int32),
         ("coarse_dense_limit", C.c_int32), ("reference_order", C.c_int32),
         ("coarse_pre_sweeps", C.c_int32), ("coarse_post_sweeps", C.c_int32), ("narrow_columns", C.c_int32),
-        ("half_values", C.c_int32), ("dense_fp64", C.c_int32),
+        ("half_values", C.c_int32), ("dense_fp64", C.c_int32), ("constant_null_space", C.c_int32),
     ]
 
 
@@ -73,7 +73,7 @@ class Request(C.Structure):
         ("residual_replacement_period", C.c_int64), ("residual_replacement_gap_ratio", C.c_double),
         ("target_reduction_per_cycle", C.c_double), ("learned", C.c_void_p),
         ("learned_applications", C.c_int32), ("orthogonalization", C.c_int32), ("problem", C.c_int32),
-        ("scaling", C.c_int32),
+        ("scaling", C.c_int32), ("null_space", C.c_int32),
     ]
 
 

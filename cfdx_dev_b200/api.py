@@ -585,8 +585,9 @@ class ReusablePreconditionerContext:
 
 
 def make_request(krylov="gmres", preconditioner="native_amg", restart=40, precision="fp64", learned=None,
-                 problem="pressure_poisson", scaling="none", **kw):
-    """A cfdxg_request; krylov / preconditioner "auto" select the plan from the measured matrix."""
+                 problem="pressure_poisson", scaling="none", null_space="none", **kw):
+    """A cfdxg_request; krylov / preconditioner "auto" select the plan from the measured matrix.
+    null_space="constant": the projected solves of a pure-Neumann operator (NullSpaceModel::Constant)."""
     lib = N.load()
     r = N.Request()
     lib.cfdxg_request_default(C.byref(r))
@@ -597,6 +598,7 @@ def make_request(krylov="gmres", preconditioner="native_amg", restart=40, precis
     r.learned = learned.handle if learned is not None else None
     r.problem = N.PROBLEMS.index(problem)
     r.scaling = N.SCALINGS.index(scaling)
+    r.null_space = N.NULL_SPACES.index(null_space)
     for k, v in kw.items():
         setattr(r, k, v)
     return r
@@ -679,6 +681,7 @@ def solve_linear_system(A: SparseMatrix, rhs, x0=None, krylov="gmres", precondit
     if linear_capture_path:
         ro, co, va = A.to_csr()
         write_linear_system_capture(linear_capture_path, ro, co, va, b, x, problem=CAPTURE_PRESSURE_POISSON,
+                                    null_space=N.NULL_SPACES.index(kw.get("null_space", "none")),
                                     scaling=N.SCALINGS.index(kw.get("scaling", "none")),
                                     max_iterations=max_iterations, tolerance=tolerance)
     req = make_request(krylov, preconditioner, restart, precision, learned, **kw)

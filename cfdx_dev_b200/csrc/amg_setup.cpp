@@ -669,9 +669,26 @@ bool build_inverse_diagonal(const HostCsr& A, std::vector<double>& inv_diag) {
     return ok;
 }
 
+// amg_preconditioner.h:1289-1308 has_constant_null_space: every |row sum|
+// within 256 eps max(1, largest absolute row sum), rows summed in CSR order
+bool has_constant_null_space(const HostCsr& A) {
+    double matrix_scale = 0.0, residual_scale = 0.0;
+    for (int64_t i = 0; i < A.n; ++i) {
+        double row_sum = 0.0, row_norm = 0.0;
+        for (uint32_t k = A.ro[i]; k < A.ro[i + 1]; ++k) {
+            row_sum += A.va[k];
+            row_norm += std::abs(A.va[k]);
+        }
+        matrix_scale = std::max(matrix_scale, row_norm);
+        residual_scale = std::max(residual_scale, std::abs(row_sum));
+    }
+    const double tolerance = 256.0 * std::numeric_limits<double>::epsilon() * std::max(1.0, matrix_scale);
+    return std::isfinite(residual_scale) && residual_scale <= tolerance;
+}
+
 bool amg_setup(const HostCsr& A, const AmgOptions& opt, AmgHierarchy& out, std::string& error) {
     error.clear();
-    if (A.n == 0 || !matrix_is_valid(A)) {
+    if (A.n == 0 || !matrix_is_valid(A) || (opt.constant_null_space && !has_constant_null_space(A))) {
         error = "invalid finest matrix, dimensions, CSR, or null-space contract";
         return false;
     }
@@ -740,7 +757,8 @@ bool amg_setup(const HostCsr& A, const AmgOptions& opt, AmgHierarchy& out, std::
 bool amg_update_values(AmgHierarchy& h, const HostCsr& A, std::string& error) {
     error.clear();
     if (h.levels.empty() || A.n != h.levels.front().A.n || A.ro != h.levels.front().A.ro ||
-        A.co != h.levels.front().A.co || !matrix_is_valid(A)) {
+        A.co != h.levels.front().A.co || !matrix_is_valid(A) ||
+        (h.options.constant_null_space && !has_constant_null_space(A))) {
         error = "native AMG numeric update requires an unchanged CSR pattern";
         return false;
     }

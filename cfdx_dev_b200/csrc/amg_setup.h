@@ -57,6 +57,7 @@ struct AmgOptions {
     double strength_threshold = 0.25;
     int max_levels = 25;
     bool require_smoother_certificate = false;
+    bool constant_null_space = false;   // the finest operator must have the constant null space
 };
 
 struct AmgHierarchy {
@@ -76,6 +77,7 @@ bool amg_update_values(AmgHierarchy& h, const HostCsr& A, std::string& error);
 
 // Helpers shared with the device upload.
 bool build_inverse_diagonal(const HostCsr& A, std::vector<double>& inv_diag);
+bool has_constant_null_space(const HostCsr& A);
 int host_threads();
 
 }  // namespace cfdxg

@@ -150,6 +150,7 @@ void amg_setup_impl(cfdxg_context* ctx, cfdxg_amg* amg, cfdxg_matrix* A) {
     o.strength_threshold = amg->opts.strength_threshold;
     o.max_levels = amg->opts.max_levels;
     o.require_smoother_certificate = amg->opts.require_smoother_certificate != 0;
+    o.constant_null_space = amg->opts.constant_null_space != 0;
     AmgHierarchy staged;
     std::string err;
     if (!amg_setup(A->host, o, staged, err)) {
@@ -161,6 +162,7 @@ void amg_setup_impl(cfdxg_context* ctx, cfdxg_amg* amg, cfdxg_matrix* A) {
     UploadOptions up;
     up.reference_order = amg->opts.reference_order != 0;
     up.narrow_columns = amg->opts.narrow_columns != 0;
+    up.constant_null_space = amg->opts.constant_null_space != 0;
     if (amg->opts.precision == CFDXG_PRECISION_FP32_VCYCLE) {
         up.coarse_dense_limit = amg->opts.coarse_dense_limit;
         up.half_values = amg->opts.half_values != 0;
@@ -383,6 +385,7 @@ extern "C" int cfdxg_amg_options_default(cfdxg_amg_options* o) {
     o->narrow_columns = 1;
     o->half_values = 1;
     o->dense_fp64 = 0;
+    o->constant_null_space = 0;
     return CFDXG_OK;
 }
 
@@ -541,6 +544,7 @@ extern "C" int cfdxg_amg_setup_host(cfdxg_amg* amg, int64_t n, const int64_t* ro
     o.strength_threshold = amg->opts.strength_threshold;
     o.max_levels = amg->opts.max_levels;
     o.require_smoother_certificate = amg->opts.require_smoother_certificate != 0;
+    o.constant_null_space = amg->opts.constant_null_space != 0;
     AmgHierarchy staged;
     std::string err;
     if (!amg_setup(A, o, staged, err)) {
@@ -630,10 +634,14 @@ extern "C" const char* cfdxg_plan_reason(const cfdxg_context* ctx) { return ctx 
 namespace {
 
 // Runs the Krylov solve on device vectors with an optional prepared AMG, Jacobi
-// inverse diagonal, and learned network.
+// inverse diagonal, and learned network.  `setup`, when given, prepares the
+// preconditioner where the solver does (CG and the projected GMRES: after the
+// initial-residual check); with the constant null space the solve is the
+// projected one.
 KrylovResult run_krylov(cfdxg_context* ctx, const cfdxg_matrix* A, cfdxg_amg* amg, const double* inv_diag,
                         const double* b, double* x, const cfdxg_request& req, int64_t max_it, double tol,
-                        int64_t* learned_fallbacks, const std::function<bool()>* cg_setup = nullptr) {
+                        int64_t* learned_fallbacks, const std::function<bool()>* setup = nullptr) {
+    const bool null_space = req.null_space == CFDXG_NULL_SPACE_CONSTANT;
     RightPreconditioner pc;
     const int n = static_cast<int>(A->n);
     if (req.krylov == CFDXG_KRYLOV_CG) {
@@ -663,7 +671,8 @@ KrylovResult run_krylov(cfdxg_context* ctx, const cfdxg_matrix* A, cfdxg_amg* am
                 check_launch(ctx);
                 return true;
             };
-        return cg_solve(ctx, A, b, x, max_it, tol, pc, cg_setup, req.preconditioner == CFDXG_PC_OWN_DIAGONAL);
+        return cg_solve(ctx, A, b, x, max_it, tol, pc, setup, req.preconditioner == CFDXG_PC_OWN_DIAGONAL,
+                        null_space);
     }
     // Learned stage: dropped for the rest of the solve (plain AMG fallback)
     // as soon as an iteration fails to cut the residual estimate by 10%.
@@ -704,6 +713,9 @@ KrylovResult run_krylov(cfdxg_context* ctx, const cfdxg_matrix* A, cfdxg_amg* am
         };
     }
     const RightPreconditioner* p = pc ? &pc : nullptr;
+    if (null_space)
+        return projected_gmres_solve(ctx, A, b, x, req.gmres_restart, max_it, tol, p, controls_from(req), nullptr,
+                                     setup);
     KrylovResult r = gmres_solve(ctx, A, b, x, req.gmres_restart, max_it, tol, p, controls_from(req),
                                  req.learned && amg ? &observer : nullptr);
     if (learned_fallbacks) *learned_fallbacks = state.fallbacks;
@@ -743,6 +755,19 @@ void validate_request(const cfdxg_request& r) {
         throw Error(CFDXG_ERR_INVALID_ARGUMENT, "CG requires symmetry-preserving scaling (symmetric_diagonal)");
     if (r.scaling != CFDXG_SCALING_NONE && r.problem == CFDXG_PROBLEM_COUPLED_PRESSURE_VELOCITY)
         throw Error(CFDXG_ERR_INVALID_ARGUMENT, "scaling is provided for scalar systems only");
+    // linear_solver_dispatch.h:292-295, linear_solver_models.h:415-423
+    if (r.null_space != CFDXG_NULL_SPACE_NONE && r.null_space != CFDXG_NULL_SPACE_CONSTANT)
+        throw Error(CFDXG_ERR_INVALID_ARGUMENT, "unknown null-space model");
+    if (r.null_space == CFDXG_NULL_SPACE_CONSTANT) {
+        if (r.scaling != CFDXG_SCALING_NONE)
+            throw Error(CFDXG_ERR_INVALID_ARGUMENT,
+                        "explicit algebraic scaling is not currently combined with a projected null-space solve");
+        if (!elliptic)
+            throw Error(CFDXG_ERR_INVALID_ARGUMENT,
+                        "constant null space is currently qualified only for pressure/diffusion problems");
+        if (r.learned)
+            throw Error(CFDXG_ERR_INVALID_ARGUMENT, "the learned stage is not combined with a projected null space");
+    }
 }
 
 // Scaled solve (linear_solver_dispatch.h:302-328, 466-490): scale_matrix on
@@ -900,7 +925,8 @@ extern "C" int cfdxg_solve_linear_system(cfdxg_context* ctx, const cfdxg_matrix*
             // a forced CG fails closed before any plan is drawn
             req.preconditioner = CFDXG_PC_NONE;
         } else {
-            const cfdxg_plan_request pr{req.krylov, req.preconditioner, req.gmres_restart, 0, req.scaling, 1.0};
+            const cfdxg_plan_request pr{req.krylov, req.preconditioner, req.gmres_restart, req.null_space,
+                                        req.scaling, 1.0};
             cfdxg_solver_plan plan;
             std::string why;
             if (!select_solver(req.problem, ch, pr, plan, why)) throw Error(CFDXG_ERR_INVALID_ARGUMENT, why);
@@ -950,6 +976,7 @@ extern "C" int cfdxg_solve_linear_system(cfdxg_context* ctx, const cfdxg_matrix*
         cfdxg_amg_options_default(&amg.opts);
         amg.opts.precision = req.precision;
         amg.opts.require_smoother_certificate = 1;
+        amg.opts.constant_null_space = req.null_space == CFDXG_NULL_SPACE_CONSTANT;
         DevBuf<double> inv(req.preconditioner == CFDXG_PC_JACOBI || req.preconditioner == CFDXG_PC_OWN_DIAGONAL ? n : 0);
         std::function<bool()> setup = [&]() {
             if (req.preconditioner == CFDXG_PC_NATIVE_AMG) {
@@ -981,6 +1008,40 @@ extern "C" int cfdxg_solve_linear_system(cfdxg_context* ctx, const cfdxg_matrix*
             return true;
         };
         r = run_krylov(ctx, A, &amg, inv.get(), b.get(), xo.get(), req, max_iterations, tolerance, nullptr, &setup);
+    } else if (req.null_space == CFDXG_NULL_SPACE_CONSTANT) {
+        // solve_projected_gmres (projected_gmres.h:84-150): the preconditioner
+        // is set up after the null-space checks and the early exit; a failed
+        // setup is NOT_APPLICABLE
+        cfdxg_amg amg;
+        cfdxg_amg_options_default(&amg.opts);
+        amg.opts.precision = req.precision;
+        amg.opts.constant_null_space = 1;
+        const bool use_amg = req.preconditioner == CFDXG_PC_NATIVE_AMG;
+        DevBuf<double> inv(req.preconditioner == CFDXG_PC_JACOBI ? n : 0);
+        std::function<bool()> setup = [&]() {
+            if (use_amg) {
+                try {
+                    amg_setup_impl(ctx, &amg, const_cast<cfdxg_matrix*>(A));
+                } catch (const Error& e) {
+                    if (e.code != CFDXG_ERR_SETUP) throw;
+                    ctx->error = amg.error;
+                    setup_s = amg.setup_seconds;
+                    return false;
+                }
+                setup_s = amg.setup_seconds;
+                return true;
+            }
+            if (req.preconditioner == CFDXG_PC_JACOBI) {
+                clear_status(ctx);
+                k_first_diag_inverse<<<blocks_for(n, 256), 256, 0, ctx->stream>>>(
+                    static_cast<int>(n), A->ro.get(), A->co.get(), A->va.get(), inv.get(), ctx->scratch.status);
+                check_launch(ctx);
+                return read_status(ctx) == 0;
+            }
+            return true;
+        };
+        r = run_krylov(ctx, A, use_amg ? &amg : nullptr, req.preconditioner == CFDXG_PC_JACOBI ? inv.get() : nullptr,
+                       b.get(), xo.get(), req, max_iterations, tolerance, nullptr, &setup);
     } else if (req.preconditioner == CFDXG_PC_NATIVE_AMG) {
         cfdxg_amg amg;
         cfdxg_amg_options_default(&amg.opts);

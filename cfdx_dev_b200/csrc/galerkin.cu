@@ -300,6 +300,47 @@ void build_refresh(cfdxg_context* ctx, cfdxg_amg* amg) {
     amg->refresh = std::move(R);
 }
 
+// has_constant_null_space (amg_preconditioner.h:1289-1308) on the device:
+// each row's sum and absolute sum in CSR order (one thread per row), then the
+// largest |row sum| and absolute row sum per block (maxima are order-free).
+__global__ void k_row_sum_bounds(int n, const int* __restrict__ ro, const double* __restrict__ va,
+                                 double* __restrict__ partial) {
+    __shared__ double sm[32];
+    double residual = 0.0, scale = 0.0;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        double sum = 0.0, norm = 0.0;
+        for (int k = ro[i]; k < ro[i + 1]; ++k) {
+            sum += va[k];
+            norm += fabs(va[k]);
+        }
+        scale = fmax(scale, norm);
+        residual = fmax(residual, fabs(sum));
+    }
+    residual = block_max(residual, sm);
+    scale = block_max(scale, sm);
+    if (threadIdx.x == 0) {
+        partial[2 * blockIdx.x] = residual;
+        partial[2 * blockIdx.x + 1] = scale;
+    }
+}
+
+bool device_has_constant_null_space(cfdxg_context* ctx, const cfdxg_matrix* A) {
+    const int nb = std::max(1, std::min(blocks_for(A->n, kT), 148 * 4));
+    DevBuf<double> partial(2 * static_cast<std::size_t>(nb));
+    k_row_sum_bounds<<<nb, kT, 0, ctx->stream>>>(static_cast<int>(A->n), A->ro.get(), A->va.get(), partial.get());
+    check_launch(ctx);
+    std::vector<double> h(2 * static_cast<std::size_t>(nb));
+    partial.download(h.data(), ctx->stream);
+    CFDXG_CUDA(cudaStreamSynchronize(ctx->stream));
+    double residual = 0.0, scale = 0.0;
+    for (int b = 0; b < nb; ++b) {
+        residual = std::max(residual, h[2 * b]);
+        scale = std::max(scale, h[2 * b + 1]);
+    }
+    const double tolerance = 256.0 * std::numeric_limits<double>::epsilon() * std::max(1.0, scale);
+    return std::isfinite(residual) && residual <= tolerance;
+}
+
 }  // namespace
 
 bool amg_refresh_device(cfdxg_context* ctx, cfdxg_amg* amg, const cfdxg_matrix* A, std::string& error) {
@@ -308,6 +349,10 @@ bool amg_refresh_device(cfdxg_context* ctx, cfdxg_amg* amg, const cfdxg_matrix* 
     if (h.levels.empty() || A->n != h.levels.front().A.n || A->host.ro != h.levels.front().A.ro ||
         A->host.co != h.levels.front().A.co) {
         error = "native AMG numeric update requires an unchanged CSR pattern";
+        return false;
+    }
+    if (h.options.constant_null_space && !device_has_constant_null_space(ctx, A)) {
+        error = "native AMG numeric update: the operator no longer has the constant null space";
         return false;
     }
     if (!amg->refresh) build_refresh(ctx, amg);

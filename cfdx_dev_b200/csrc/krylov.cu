@@ -17,8 +17,10 @@
 #include <cmath>
 #include <functional>
 #include <limits>
+#include <mutex>
 
 #include "krylov.h"
+#include "nullspace.cuh"
 
 namespace cfdxg {
 
@@ -424,6 +426,28 @@ __global__ void k_add(int n, double* __restrict__ x, const double* __restrict__ 
     if (i < n) x[i] += y[i];
 }
 
+// r = b - y
+__global__ void k_sub(int n, const double* __restrict__ b, const double* __restrict__ y, double* __restrict__ r) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) r[i] = b[i] - y[i];
+}
+
+__global__ void k_fill(int n, double v, double* __restrict__ x) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) x[i] = v;
+}
+
+// y = A^T x (column sums of a_ij x_i; the order of the additions varies with
+// scheduling -- used only for the threshold of is_bilateral_null_space)
+__global__ void k_transpose_apply(int n, const int* __restrict__ ro, const int* __restrict__ co,
+                                  const double* __restrict__ va, const double* __restrict__ x,
+                                  double* __restrict__ y) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const double xi = x[i];
+    for (int k = ro[i]; k < ro[i + 1]; ++k) atomicAdd(y + co[k], va[k] * xi);
+}
+
 // Pinned copies of one Arnoldi step's scalar slots [0, kH2 + m + 1) and of
 // the status word, two of them (step j uses buffer j & 1), each with the
 // event that marks its copy done: the host reads step j's results while the
@@ -455,6 +479,7 @@ struct Workspace {
     int64_t n = 0;
     int m = 0;
     DevBuf<double> V, Z, w, r, ax, best, trial, tmp;
+    DevBuf<double> ns1, ns2, ns_partials;   // the projected operator's scratch
     DevBuf<double> mpartial;   // (kChunk + 1) x kWideBlocks partial sums of the multi-dot
     std::unique_ptr<StepMirror> mirror;
 };
@@ -471,6 +496,8 @@ Workspace& workspace(cfdxg_context* ctx, int64_t n, int m) {
         ws->Z.resize(static_cast<size_t>(mm) * n);
         ws->w.resize(n); ws->r.resize(n); ws->ax.resize(n); ws->best.resize(n);
         ws->trial.resize(n); ws->tmp.resize(n);
+        ws->ns1.resize(n); ws->ns2.resize(n);
+        ws->ns_partials.resize(kNsMaxBlocks);
         ws->mpartial.resize(static_cast<size_t>(kChunk + 1) * kWideBlocks);
         ws->n = n;
         ws->m = mm;
@@ -601,6 +628,72 @@ public:
         check_launch(ctx_);
     }
     void spmv(const double* x, double* y) { spmv_fp64(ctx_, A_, x, y); }
+    // Projection onto the complement of the constant null space,
+    // v -= (v . e) e (null_space.h:64-71), the sum in a fixed order.
+    void set_projection(double e, Workspace& ws) {
+        ns_e_ = e;
+        ns1_ = ws.ns1.get();
+        ns2_ = ws.ns2.get();
+        nsp_ = ws.ns_partials.get();
+    }
+    bool projected() const { return ns_e_ != 0.0; }
+    double projection_entry() const { return ns_e_; }
+    void project(double* v) {
+        ProfScope ps(ctx_, "null_space_projection", 3.0 * nb());
+        enqueue_remove_constant<double>(ctx_->stream, n_, v, nsp_, false, false, ns_e_);
+        check_launch(ctx_);
+        count_launch(ctx_);
+    }
+    // The Krylov operator: A, or P A P under a projected null space
+    // (projected_gmres.h:122-131).
+    void op(const double* x, double* y) {
+        if (!projected()) {
+            spmv(x, y);
+            return;
+        }
+        copy(ns1_, x);
+        project(ns1_);
+        spmv(ns1_, y);
+        project(y);
+    }
+    // r = b - op(x): the residual the Krylov solve certifies against
+    void op_residual(const double* b, const double* x, double* r) {
+        if (!projected()) {
+            residual(b, x, r);
+            return;
+        }
+        op(x, ns2_);
+        k_sub<<<gb(), kT, 0, ctx_->stream>>>(n_, b, ns2_, r);
+        check_launch(ctx_);
+    }
+    // z = P M P v, the ProjectedPreconditioner (projected_gmres.h:32-44); M is
+    // pc, or the identity without one
+    bool precondition(const RightPreconditioner* pc, const double* v, double* z, int j) {
+        if (!projected()) {
+            if (pc) return (*pc)(v, z, j);
+            copy(z, v);
+            return true;
+        }
+        copy(ns1_, v);
+        project(ns1_);
+        if (pc) {
+            if (!(*pc)(ns1_, z, j)) return false;
+        } else {
+            copy(z, ns1_);
+        }
+        project(z);
+        return true;
+    }
+    // scaled two-pass norm of count entries of a (count may exceed n)
+    void norm2_n(const double* a, int count, int out) {
+        const int b = reduce_blocks(count);
+        launch_pdl(ctx_->stream, k_absmax, b, kT, count, a, ctx_->scratch.partial, ctx_->scratch.ticket,
+                   slot(kMax), slot(kInvalid));
+        check_launch(ctx_);
+        launch_pdl(ctx_->stream, k_sumsq, b, kT, count, a, slot(kMax), slot(kInvalid), ctx_->scratch.partial,
+                   ctx_->scratch.ticket, slot(out));
+        check_launch(ctx_);
+    }
     void copy(double* dst, const double* src) {
         CFDXG_CUDA(cudaMemcpyAsync(dst, src, sizeof(double) * n_, cudaMemcpyDeviceToDevice, ctx_->stream));
     }
@@ -646,6 +739,8 @@ private:
     const cfdxg_matrix* A_;
     int n_;
     double* sc_;
+    double ns_e_ = 0.0;
+    double *ns1_ = nullptr, *ns2_ = nullptr, *nsp_ = nullptr;
 };
 
 // ---------------------------------------------------------------- CG kernels
@@ -724,7 +819,7 @@ int choose_restart(int current, double reduction, const KrylovControls& c) {
 
 KrylovResult gmres_solve(cfdxg_context* ctx, const cfdxg_matrix* A, const double* b, double* x,
                          int restart, int64_t max_iter, double tolerance, const RightPreconditioner* pc,
-                         const KrylovControls& controls, const IterationObserver* observer) {
+                         const KrylovControls& controls, const IterationObserver* observer, double projection) {
     KrylovResult result;
     const int64_t n = A->n;
     if (n == 0 || restart <= 0 || max_iter == 0 || !std::isfinite(tolerance) || tolerance <= 0.0) {
@@ -743,6 +838,7 @@ KrylovResult gmres_solve(cfdxg_context* ctx, const cfdxg_matrix* A, const double
     clear_status(ctx);
     int current_restart = std::clamp(restart, controls.restart_min, controls.restart_max);
     if (n < current_restart) current_restart = static_cast<int>(n);
+    if (projection != 0.0) E.set_projection(projection, workspace(ctx, n, current_restart));
 
     E.norm2(b, kNorm);
     const double b_norm = E.scalar(kNorm);
@@ -753,7 +849,7 @@ KrylovResult gmres_solve(cfdxg_context* ctx, const cfdxg_matrix* A, const double
     if (b_norm == 0.0) {
         // gmres_solver.h:64-134: b == 0 with x0 != 0 -> solve A y = -A x0, certify on ||A x0||.
         Workspace& ws = workspace(ctx, n, current_restart);
-        E.spmv(x, ws.ax.get());
+        E.op(x, ws.ax.get());
         E.norm2(ws.ax.get(), kNorm);
         const double ax0_norm = E.scalar(kNorm);
         if (!std::isfinite(ax0_norm)) {
@@ -767,10 +863,10 @@ KrylovResult gmres_solve(cfdxg_context* ctx, const cfdxg_matrix* A, const double
             E.neg(ws.ax.get(), shifted.get());
             y.zero(ctx->stream);
             const KrylovResult sh = gmres_solve(ctx, A, shifted.get(), y.get(), restart, max_iter, tolerance, pc,
-                                                controls, observer);
+                                                controls, observer, projection);
             Workspace& ws2 = workspace(ctx, n, current_restart);
             E.add(x, y.get());
-            E.residual(b, x, ws2.r.get());
+            E.op_residual(b, x, ws2.r.get());
             E.norm2(ws2.r.get(), kNorm);
             const double residual = E.scalar(kNorm);
             const double relative = residual / ax0_norm;
@@ -788,7 +884,7 @@ KrylovResult gmres_solve(cfdxg_context* ctx, const cfdxg_matrix* A, const double
 
     Workspace* ws = &workspace(ctx, n, current_restart);
     auto true_residual = [&]() {
-        E.residual(b, x, ws->r.get());
+        E.op_residual(b, x, ws->r.get());
         E.norm2(ws->r.get(), kBeta);
         return E.scalar(kBeta);
     };
@@ -864,12 +960,8 @@ KrylovResult gmres_solve(cfdxg_context* ctx, const cfdxg_matrix* A, const double
         // the queued copy of the step's slots into mirror buffer j & 1.
         StepMirror& mirror = *ws->mirror;
         auto enqueue_step = [&](int jj) -> bool {
-            if (pc) {
-                if (!(*pc)(v(jj), z(jj), jj)) return false;
-            } else {
-                E.copy(z(jj), v(jj));
-            }
-            E.spmv(z(jj), ws->w.get());
+            if (!E.precondition(pc, v(jj), z(jj), jj)) return false;
+            E.op(z(jj), ws->w.get());
             double* w = ws->w.get();
             if (controls.classical_gram_schmidt && jj + 1 <= kChunk) {
                 // classical Gram-Schmidt twice in three fused passes; the
@@ -914,9 +1006,10 @@ KrylovResult gmres_solve(cfdxg_context* ctx, const cfdxg_matrix* A, const double
             }
             CFDXG_CUDA(cudaEventSynchronize(mirror.done[j & 1]));
             const double* hs = mirror.scalars[j & 1];
-            if (pc) ++result.preconditioner_applications;
+            const bool preconditioned = pc || E.projected();
+            if (preconditioned) ++result.preconditioner_applications;
             if (*mirror.status[j & 1] & kStatusNonFinite) {
-                if (pc) return fail(CFDXG_NOT_APPLICABLE);   // preconditioner produced a non-finite z
+                if (preconditioned) return fail(CFDXG_NOT_APPLICABLE);   // preconditioner produced a non-finite z
             }
             const double arnoldi_action_norm = hs[kAction];
             if (!std::isfinite(arnoldi_action_norm)) return fail(CFDXG_DIVERGED);
@@ -972,7 +1065,7 @@ KrylovResult gmres_solve(cfdxg_context* ctx, const cfdxg_matrix* A, const double
                 }
                 if (usable) {
                     E.update(x, Z, coef, used, ws->trial.get());
-                    E.residual(b, ws->trial.get(), ws->tmp.get());
+                    E.op_residual(b, ws->trial.get(), ws->tmp.get());
                     E.norm2(ws->tmp.get(), kNorm);
                     const double verified = E.scalar(kNorm);
                     if (std::isfinite(verified)) {
@@ -1087,25 +1180,151 @@ KrylovResult gmres_solve(cfdxg_context* ctx, const cfdxg_matrix* A, const double
     return result;
 }
 
+// ---------------------------------------------------------------- null space
+double constant_null_space_entry(int64_t n) {
+    // null_space.h:58-62: the ones vector over its hypot-accumulated norm
+    // (:141-146), computed once per size
+    static std::mutex mu;
+    static int64_t last_n = -1;
+    static double last_e = 0.0;
+    std::lock_guard<std::mutex> lock(mu);
+    if (n != last_n) {
+        double norm = 0.0;
+        for (int64_t i = 0; i < n; ++i) norm = std::hypot(norm, 1.0);
+        last_e = 1.0 * (1.0 / norm);
+        last_n = n;
+    }
+    return last_e;
+}
+
+NullSpaceChecks null_space_checks(cfdxg_context* ctx, const cfdxg_matrix* A, const double* b) {
+    NullSpaceChecks c;
+    const int64_t n = A->n;
+    if (n <= 0) return c;
+    if (A->nnz > std::numeric_limits<int>::max()) throw Error(CFDXG_ERR_INVALID_ARGUMENT, "system too large");
+    const double e = constant_null_space_entry(n);
+    Engine E(ctx, A);
+    Workspace& ws = workspace(ctx, n, 1);
+    const int ni = static_cast<int>(n);
+    // null_space.h:90-105 is_compatible: |b . e| <= 1e-14 + 1e-12 ||b||
+    const int nb = ns_blocks(n);
+    k_ns_partials<double><<<nb, kNsThreads, 0, ctx->stream>>>(ni, b, e, ws.ns_partials.get());
+    check_launch(ctx);
+    std::vector<double> part(ws.ns_partials.size());
+    ws.ns_partials.download(part.data(), ctx->stream);
+    E.norm2(b, kNorm);
+    const double b_norm = E.scalar(kNorm);
+    double coefficient = 0.0;
+    for (int q = 0; q < nb; ++q) coefficient += part[q];
+    c.component = std::sqrt(std::max(0.0, coefficient * coefficient));
+    c.compatible = c.component <= 1e-14 + 1e-12 * b_norm;
+    // :107-134 operator_residual: ||A e|| / ||A||_F <= 1e-12
+    E.norm2_n(A->va.get(), static_cast<int>(A->nnz), kNorm);
+    const double frobenius = E.scalar(kNorm);
+    k_fill<<<blocks_for(n, kT), kT, 0, ctx->stream>>>(ni, e, ws.ns1.get());
+    check_launch(ctx);
+    E.spmv(ws.ns1.get(), ws.ns2.get());
+    E.norm2(ws.ns2.get(), kNorm);
+    const double product = E.scalar(kNorm);
+    if (!std::isfinite(frobenius)) return c;
+    c.operator_residual = product / std::max(frobenius, std::numeric_limits<double>::min());
+    c.null_space = c.operator_residual <= 1e-12;
+    // projected_gmres.h:53-82 is_bilateral_null_space: and ||A^T e|| <= 1e-12 ||A||_F
+    ws.ns2.zero(ctx->stream);
+    k_transpose_apply<<<blocks_for(n, kT), kT, 0, ctx->stream>>>(ni, A->ro.get(), A->co.get(), A->va.get(),
+                                                                ws.ns1.get(), ws.ns2.get());
+    check_launch(ctx);
+    E.norm2(ws.ns2.get(), kNorm);
+    const double transpose = E.scalar(kNorm);
+    c.bilateral = c.null_space &&
+                  !(transpose > 1e-12 * std::max(frobenius, std::numeric_limits<double>::min()));
+    return c;
+}
+
+// projected_gmres.h:84-150 solve_projected_gmres: parameter and null-space
+// checks (NOT_APPLICABLE, x untouched), a gauge-free copy of the iterate, the
+// early exit when it already satisfies b in physical coordinates, the
+// preconditioner setup, then FGMRES on P A P preconditioned by P M P and the
+// projected result.
+KrylovResult projected_gmres_solve(cfdxg_context* ctx, const cfdxg_matrix* A, const double* b, double* x,
+                                   int restart, int64_t max_iter, double tolerance, const RightPreconditioner* pc,
+                                   const KrylovControls& controls, const IterationObserver* observer,
+                                   const std::function<bool()>* setup) {
+    KrylovResult result;   // NOT_APPLICABLE
+    const int64_t n = A->n;
+    if (n == 0 || restart <= 0 || max_iter == 0 || !(tolerance > 0.0) || !std::isfinite(tolerance)) return result;
+    if (n > std::numeric_limits<int>::max()) throw Error(CFDXG_ERR_INVALID_ARGUMENT, "system too large");
+    Engine E(ctx, A);
+    Workspace& ws = workspace(ctx, n, 1);
+    CFDXG_CUDA(cudaMemsetAsync(E.slot(kDot), 0, sizeof(double), ctx->stream));
+    k_any_nonfinite<<<blocks_for(n, kT), kT, 0, ctx->stream>>>(n, b, E.slot(kDot));
+    k_any_nonfinite<<<blocks_for(n, kT), kT, 0, ctx->stream>>>(n, x, E.slot(kDot));
+    check_launch(ctx);
+    if (E.scalar(kDot) > 0.0) return result;
+    const NullSpaceChecks checks = null_space_checks(ctx, A, b);
+    if (!checks.compatible || !checks.bilateral) return result;
+    const double e = constant_null_space_entry(n);
+    E.set_projection(e, ws);
+    DevBuf<double> gauge_free(n);
+    E.copy(gauge_free.get(), x);
+    E.project(gauge_free.get());
+    E.residual(b, gauge_free.get(), ws.tmp.get());
+    E.norm2(ws.tmp.get(), kNorm);
+    const double r0 = E.scalar(kNorm);
+    E.norm2(b, kNorm);
+    const double b_norm = E.scalar(kNorm);
+    if (r0 == 0.0 || (b_norm > 0.0 && r0 <= tolerance * b_norm)) {
+        result.status = CFDXG_CONVERGED;
+        result.residual = r0;
+        result.residual_relative = b_norm > 0.0 ? r0 / b_norm : 0.0;
+        E.copy(x, gauge_free.get());
+        CFDXG_CUDA(cudaStreamSynchronize(ctx->stream));
+        return result;
+    }
+    if (setup && !(*setup)()) return result;
+    result = gmres_solve(ctx, A, b, gauge_free.get(), restart, max_iter, tolerance, pc, controls, observer, e);
+    if (result.status != CFDXG_NOT_APPLICABLE) {
+        CFDXG_CUDA(cudaMemsetAsync(E.slot(kDot), 0, sizeof(double), ctx->stream));
+        k_any_nonfinite<<<blocks_for(n, kT), kT, 0, ctx->stream>>>(n, gauge_free.get(), E.slot(kDot));
+        check_launch(ctx);
+        if (!(E.scalar(kDot) > 0.0)) {
+            E.project(gauge_free.get());
+            E.copy(x, gauge_free.get());
+        }
+    }
+    CFDXG_CUDA(cudaStreamSynchronize(ctx->stream));
+    return result;
+}
+
 // ---------------------------------------------------------------- CG
-// cg_solver.h:45-560 solve_cg_impl (FP64 operator and reductions, no null
-// space, adaptive residual replacement) with a preconditioner object.  Each
+// cg_solver.h:45-560 solve_cg_impl (FP64 operator and reductions, adaptive
+// residual replacement, optionally the constant null space) with a
+// preconditioner object.  Each
 // iteration is one stream of kernels -- A p, p^T A p, the fused x/r update,
 // z = M^-1 r, r^T z with the z check, the FP64 true residual b - A x and its
 // scaled norm, ||r||^2 -- and one read-back of eight scalars, after which the
 // host takes the reference's decisions in the reference's order.
 KrylovResult cg_solve(cfdxg_context* ctx, const cfdxg_matrix* A, const double* b, double* x, int64_t max_iter,
                       double tolerance, const RightPreconditioner& pc, const std::function<bool()>* setup,
-                      bool own_diagonal) {
+                      bool own_diagonal, bool null_space) {
     KrylovResult result;
     const int64_t n = A->n;
     if (n == 0) return result;   // NOT_APPLICABLE
     if (n > std::numeric_limits<int>::max()) throw Error(CFDXG_ERR_INVALID_ARGUMENT, "system too large");
+    if (null_space) {
+        // :74-79 a compatible right-hand side and A e = 0, else NOT_APPLICABLE (x untouched)
+        const NullSpaceChecks c = null_space_checks(ctx, A, b);
+        if (!c.compatible || !c.null_space) return result;
+    }
     Engine E(ctx, A);
     clear_status(ctx);
     const int ni = static_cast<int>(n);
     const int gb = blocks_for(n, kT);
     Workspace& ws = workspace(ctx, n, 1);
+    if (null_space) E.set_projection(constant_null_space_entry(n), ws);
+    auto project = [&](double* v) {
+        if (null_space) E.project(v);
+    };
     DevBuf<double> p(n), z(n), Ap(n);
     double* r = ws.r.get();
     double* rv = ws.tmp.get();
@@ -1120,7 +1339,9 @@ KrylovResult cg_solve(cfdxg_context* ctx, const cfdxg_matrix* A, const double* b
     };
     auto apply = [&]() {
         ++result.preconditioner_applications;
-        return pc(r, z.get(), 0);
+        if (!pc(r, z.get(), 0)) return false;
+        project(z.get());                                            // :203
+        return true;
     };
 
     // :75-85 non-finite operator, right-hand side or initial guess
@@ -1130,8 +1351,18 @@ KrylovResult cg_solve(cfdxg_context* ctx, const cfdxg_matrix* A, const double* b
     k_any_nonfinite<<<gb, kT, 0, ctx->stream>>>(n, b, E.slot(kCgXBad));
     k_any_nonfinite<<<gb, kT, 0, ctx->stream>>>(n, x, E.slot(kCgXBad));
     check_launch(ctx);
+    if (null_space) {
+        // :93 the gauge removed from the initial guess, once it is known to be finite
+        E.fetch(kCgCount);
+        if (E.host(kCgXBad) > 0.0) {
+            result.status = CFDXG_DIVERGED;
+            return result;
+        }
+        project(x);
+    }
     // :149-169 r = b - A x before any preconditioner work
     E.residual(b, x, rv);
+    project(rv);                                                     // :149
     E.norm2(b, kCgMax);                 // ||b|| (slots kMax/kInvalid are the norm's own scratch)
     E.norm2(rv, kCgRes);
     E.fetch(kCgCount);
@@ -1180,9 +1411,12 @@ KrylovResult cg_solve(cfdxg_context* ctx, const cfdxg_matrix* A, const double* b
     for (int64_t iter = 1; iter <= max_iter; ++iter) {
         zero_flags();
         E.spmv(p.get(), Ap.get());
+        project(Ap.get());                                           // :262
         E.dot(p.get(), Ap.get(), kCgPAp);
         k_cg_update<<<gb, kT, 0, ctx->stream>>>(ni, x, r, p.get(), Ap.get(), E.slot(0));
         check_launch(ctx);
+        project(x);                                                  // :295-298
+        project(r);
         if (!apply()) return failed(CFDXG_NOT_APPLICABLE, iter, std::numeric_limits<double>::quiet_NaN());
         dot_check(r, z.get(), kCgRsNew);
         E.residual(b, x, rv);
@@ -1207,6 +1441,7 @@ KrylovResult cg_solve(cfdxg_context* ctx, const cfdxg_matrix* A, const double* b
                 if (result.first_residual_replacement == 0) result.first_residual_replacement = iter;
                 result.last_residual_replacement = iter;
                 E.copy(r, rv);
+                project(r);                                          // :376
                 zero_flags();
                 if (!apply()) return failed(CFDXG_NOT_APPLICABLE, iter, res);
                 dot_check(r, z.get(), kCgRsOld);
@@ -1220,6 +1455,7 @@ KrylovResult cg_solve(cfdxg_context* ctx, const cfdxg_matrix* A, const double* b
             }
             k_cg_direction<<<gb, kT, 0, ctx->stream>>>(ni, p.get(), z.get(), E.slot(0));
             check_launch(ctx);
+            project(p.get());                                        // :558
             CFDXG_CUDA(cudaMemcpyAsync(E.slot(kCgRsOld), E.slot(kCgRsNew), sizeof(double), cudaMemcpyDeviceToDevice,
                                        ctx->stream));
             rsold = rsnew;
@@ -1247,6 +1483,7 @@ KrylovResult cg_solve(cfdxg_context* ctx, const cfdxg_matrix* A, const double* b
             if (result.first_residual_replacement == 0) result.first_residual_replacement = iter;
             result.last_residual_replacement = iter;
             E.copy(r, rv);
+            project(r);                                              // :517
             zero_flags();
             if (!apply()) return failed(CFDXG_NOT_APPLICABLE, iter, res);
             dot_check(r, z.get(), kCgRsOld);
@@ -1260,6 +1497,7 @@ KrylovResult cg_solve(cfdxg_context* ctx, const cfdxg_matrix* A, const double* b
         }
         k_cg_direction<<<gb, kT, 0, ctx->stream>>>(ni, p.get(), z.get(), E.slot(0));
         check_launch(ctx);
+        project(p.get());                                            // :558
         CFDXG_CUDA(cudaMemcpyAsync(E.slot(kCgRsOld), E.slot(kCgRsNew), sizeof(double), cudaMemcpyDeviceToDevice,
                                    ctx->stream));
         rsold = rsnew;

@@ -48,9 +48,30 @@ using RightPreconditioner = std::function<bool(const double* v, double* z, int j
 // Called after every Arnoldi step with the Givens estimate of the residual norm.
 using IterationObserver = std::function<void(double estimated_residual)>;
 
+// projection: 0, or the entry e of the normalised constant null-space vector,
+// every operator application and preconditioner action then being projected
+// (P A P and P M P, P v = v - (v . e) e).
 KrylovResult gmres_solve(cfdxg_context* ctx, const cfdxg_matrix* A, const double* b, double* x,
                          int restart, int64_t max_iter, double tolerance, const RightPreconditioner* pc,
-                         const KrylovControls& controls, const IterationObserver* observer = nullptr);
+                         const KrylovControls& controls, const IterationObserver* observer = nullptr,
+                         double projection = 0.0);
+
+// The constant null space (core/linalg/null_space.h, projected_gmres.h).
+// Every entry of NullSpaceProjector::constant(n)'s normalised basis vector.
+double constant_null_space_entry(int64_t n);
+// is_compatible(b), is_null_space(A) and is_bilateral_null_space(A), their
+// norms taken on the device (scaled two-pass norms instead of hypot sums).
+struct NullSpaceChecks {
+    bool compatible = false, null_space = false, bilateral = false;
+    double component = 0.0, operator_residual = 0.0;
+};
+NullSpaceChecks null_space_checks(cfdxg_context* ctx, const cfdxg_matrix* A, const double* b);
+// solve_projected_gmres (projected_gmres.h:84-150); `setup`, when given, runs
+// after the early-exit check, and a false return makes the solve NOT_APPLICABLE.
+KrylovResult projected_gmres_solve(cfdxg_context* ctx, const cfdxg_matrix* A, const double* b, double* x,
+                                   int restart, int64_t max_iter, double tolerance, const RightPreconditioner* pc,
+                                   const KrylovControls& controls, const IterationObserver* observer,
+                                   const std::function<bool()>* setup);
 
 // core/linalg/cg_solver.h:45-560 with a preconditioner object (pc, its j
 // argument unused); `setup`, when given, runs after the initial-residual
@@ -59,9 +80,14 @@ KrylovResult gmres_solve(cfdxg_context* ctx, const cfdxg_matrix* A, const double
 // the solve follows the solver's own-diagonal branch (no preconditioner
 // object, the legacy solve_cg overload, cg_solver.h:591-603) -- its residual
 // replacement rule instead of the adaptive one.
+// null_space: the projected CG of solve_cg(..., NullSpaceProjector) -- a
+// compatible b and A e = 0 or NOT_APPLICABLE, then x, the initial residual,
+// every z, A p, x and r after the update, the replaced residuals and every
+// search direction projected (cg_solver.h:74-79, 93, 149, 203, 262, 295-298,
+// 376, 517, 558).
 KrylovResult cg_solve(cfdxg_context* ctx, const cfdxg_matrix* A, const double* b, double* x, int64_t max_iter,
                       double tolerance, const RightPreconditioner& pc, const std::function<bool()>* setup,
-                      bool own_diagonal = false);
+                      bool own_diagonal = false, bool null_space = false);
 
 // Scaled two-pass 2-norm of a device vector (krylov_norm2).
 double device_norm2(cfdxg_context* ctx, const cfdxg_matrix* A, const double* a);

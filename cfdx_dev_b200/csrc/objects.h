@@ -56,6 +56,11 @@ struct DevHierarchy {
     DevBuf<float> dense;       // mode 2: the n*n inverse (row-major), formed in FP64, stored FP32
     DevBuf<double> dense64;    // mode 2 with dense_fp64: the same inverse stored FP64
     bool dense_fp64 = false;
+    // constant null space: the cycle's mean removals (in index order with
+    // reference_order) and the bordered coarsest solve
+    bool null_space = false;
+    bool ns_in_order = false;
+    DevBuf<double> ns_partials;
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
     int64_t graph_kernels = 0;
@@ -167,6 +172,7 @@ struct UploadOptions {
     bool narrow_columns = true;   // int16 column offsets on one-thread-per-row levels
     bool half_values = false;     // FP32: FP16 row-scaled matrix values
     bool dense_fp64 = false;      // FP32: the dense coarse inverse stored (and applied) in FP64
+    bool constant_null_space = false;   // the cycle of a pure-Neumann operator (mean removals)
 };
 
 template <class T>

@@ -13,12 +13,20 @@
 //
 // Level 0 is launched directly with the caller's vectors; levels >= 1 are
 // captured once into a CUDA graph with fixed buffers and replayed.
+//
+// Under the constant null space (constant_null_space) the cycle removes the
+// mean from its input and output, after every sweep, after the restriction
+// and after the prolongation, and the <= 16-row coarsest level solves the
+// system bordered by a row and a column of ones (amg_preconditioner.h:1197-1201,
+// 2382, 2406, 2430, 2440, 2590-2664); the FP32 cycle's dense coarse inverse
+// is then the leading block of the bordered matrix's inverse.
 #include <cusolverDn.h>
 
 #include <cmath>
 #include <limits>
 #include <type_traits>
 
+#include "nullspace.cuh"
 #include "objects.h"
 
 namespace cfdxg {
@@ -302,54 +310,70 @@ __global__ void k_copy_cast(int n, const T* __restrict__ a, XO* __restrict__ b) 
 }
 
 // Reference dense pivoted solve of the coarsest level (amg_preconditioner.h:2592-2663),
-// constant_null_space = false, executed by one thread in the reference's order.
+// executed by one thread in the reference's order; under the constant null
+// space (ns = 1) the system is bordered by a row and a column of ones and the
+// mean of the solution is removed, summed in order.
 template <class T>
 __global__ void k_dense_lu_reference(int n, const int* __restrict__ ro, const int* __restrict__ co,
                                      const T* __restrict__ va, const T* __restrict__ r,
-                                     T* __restrict__ x, int* status) {
+                                     T* __restrict__ x, int ns, int* status) {
     if (threadIdx.x != 0 || blockIdx.x != 0) return;
-    double m[kDenseDirectLimit * kDenseDirectLimit];
-    double b[kDenseDirectLimit];
-    double sol[kDenseDirectLimit];
-    for (int q = 0; q < n * n; ++q) m[q] = 0.0;
+    constexpr int kMax = kDenseDirectLimit + 1;
+    double m[kMax * kMax];
+    double b[kMax];
+    double sol[kMax];
+    const int sn = n + (ns ? 1 : 0);
+    for (int q = 0; q < sn * sn; ++q) m[q] = 0.0;
+    for (int i = 0; i < sn; ++i) b[i] = 0.0;
     for (int i = 0; i < n; ++i) {
         b[i] = static_cast<double>(r[i]);
-        for (int k = ro[i]; k < ro[i + 1]; ++k) m[i * n + co[k]] += static_cast<double>(va[k]);
+        for (int k = ro[i]; k < ro[i + 1]; ++k) m[i * sn + co[k]] += static_cast<double>(va[k]);
     }
+    if (ns)
+        for (int i = 0; i < n; ++i) {
+            m[i * sn + n] = 1.0;
+            m[n * sn + i] = 1.0;
+        }
     double matrix_scale = 0.0;
-    for (int q = 0; q < n * n; ++q) {
+    for (int q = 0; q < sn * sn; ++q) {
         const double a = fabs(m[q]);
         matrix_scale = (matrix_scale < a) ? a : matrix_scale;
     }
     const double pivot_tol = 128.0 * 2.220446049250313080847e-16 * (1.0 < matrix_scale ? matrix_scale : 1.0);
-    for (int k = 0; k < n; ++k) {
+    for (int k = 0; k < sn; ++k) {
         int pivot = k;
-        double pivot_abs = fabs(m[k * n + k]);
-        for (int i = k + 1; i < n; ++i) {
-            const double c = fabs(m[i * n + k]);
+        double pivot_abs = fabs(m[k * sn + k]);
+        for (int i = k + 1; i < sn; ++i) {
+            const double c = fabs(m[i * sn + k]);
             if (c > pivot_abs) { pivot_abs = c; pivot = i; }
         }
         if (!isfinite(pivot_abs) || pivot_abs <= pivot_tol) { atomicOr(status, kStatusNonFinite); return; }
         if (pivot != k) {
-            for (int j = k; j < n; ++j) { const double t = m[k * n + j]; m[k * n + j] = m[pivot * n + j]; m[pivot * n + j] = t; }
+            for (int j = k; j < sn; ++j) { const double t = m[k * sn + j]; m[k * sn + j] = m[pivot * sn + j]; m[pivot * sn + j] = t; }
             const double t = b[k]; b[k] = b[pivot]; b[pivot] = t;
         }
-        const double diagonal = m[k * n + k];
-        for (int i = k + 1; i < n; ++i) {
-            const double factor = m[i * n + k] / diagonal;
+        const double diagonal = m[k * sn + k];
+        for (int i = k + 1; i < sn; ++i) {
+            const double factor = m[i * sn + k] / diagonal;
             if (!isfinite(factor)) { atomicOr(status, kStatusNonFinite); return; }
-            m[i * n + k] = 0.0;
-            for (int j = k + 1; j < n; ++j) m[i * n + j] -= factor * m[k * n + j];
+            m[i * sn + k] = 0.0;
+            for (int j = k + 1; j < sn; ++j) m[i * sn + j] -= factor * m[k * sn + j];
             b[i] -= factor * b[k];
         }
     }
-    for (int ii = n - 1; ii >= 0; --ii) {
+    for (int ii = sn - 1; ii >= 0; --ii) {
         double sum = b[ii];
-        for (int j = ii + 1; j < n; ++j) sum -= m[ii * n + j] * sol[j];
-        const double diagonal = m[ii * n + ii];
+        for (int j = ii + 1; j < sn; ++j) sum -= m[ii * sn + j] * sol[j];
+        const double diagonal = m[ii * sn + ii];
         if (!isfinite(diagonal) || fabs(diagonal) <= pivot_tol) { atomicOr(status, kStatusNonFinite); return; }
         sol[ii] = sum / diagonal;
         if (!isfinite(sol[ii])) { atomicOr(status, kStatusNonFinite); return; }
+    }
+    if (ns) {
+        double mean = 0.0;
+        for (int i = 0; i < n; ++i) mean += sol[i];
+        mean /= static_cast<double>(n);
+        for (int i = 0; i < n; ++i) sol[i] -= mean;
     }
     for (int i = 0; i < n; ++i) x[i] = static_cast<T>(sol[i]);
 }
@@ -375,66 +399,20 @@ __global__ void k_dense_inverse_apply(int n, const S* __restrict__ inv, const T*
     }
 }
 
-// ---- Gauss-Jordan inverse (FP64, partial pivoting) for the dense coarse solve ----
-__global__ void k_gj_pivot(int n, double* a /* n x 2n */, double* factors, int k, int* status) {
-    // one block: find pivot row, swap, normalise row k, save column-k factors
-    __shared__ double best_v[kT];
-    __shared__ int best_i[kT];
-    double bv = -1.0;
-    int bi = k;
-    for (int i = k + threadIdx.x; i < n; i += blockDim.x) {
-        const double v = fabs(a[static_cast<size_t>(i) * 2 * n + k]);
-        if (v > bv) { bv = v; bi = i; }
-    }
-    best_v[threadIdx.x] = bv;
-    best_i[threadIdx.x] = bi;
-    __syncthreads();
-    for (int s = blockDim.x / 2; s > 0; s >>= 1) {
-        if (threadIdx.x < s) {
-            const double ov = best_v[threadIdx.x + s];
-            const int oi = best_i[threadIdx.x + s];
-            if (ov > best_v[threadIdx.x] || (ov == best_v[threadIdx.x] && oi < best_i[threadIdx.x])) {
-                best_v[threadIdx.x] = ov;
-                best_i[threadIdx.x] = oi;
-            }
-        }
-        __syncthreads();
-    }
-    const int p = best_i[0];
-    if (!(best_v[0] > 0.0) || !isfinite(best_v[0])) {
-        if (threadIdx.x == 0) atomicOr(status, kStatusNonFinite);
-        return;
-    }
-    double* rk = a + static_cast<size_t>(k) * 2 * n;
-    double* rp = a + static_cast<size_t>(p) * 2 * n;
-    if (p != k)
-        for (int j = threadIdx.x; j < 2 * n; j += blockDim.x) { const double t = rk[j]; rk[j] = rp[j]; rp[j] = t; }
-    __syncthreads();
-    const double inv_piv = 1.0 / rk[k];
-    __syncthreads();
-    for (int j = threadIdx.x; j < 2 * n; j += blockDim.x) rk[j] *= inv_piv;
-    __syncthreads();
-    for (int i = threadIdx.x; i < n; i += blockDim.x) factors[i] = (i == k) ? 0.0 : a[static_cast<size_t>(i) * 2 * n + k];
-}
-
-__global__ void k_gj_eliminate(int n, double* a, const double* factors, int k) {
-    const size_t idx = static_cast<size_t>(blockIdx.x) * blockDim.x + threadIdx.x;
-    const size_t total = static_cast<size_t>(n) * 2 * n;
-    if (idx >= total) return;
-    const int i = static_cast<int>(idx / (2 * n));
-    const int j = static_cast<int>(idx % (2 * n));
-    if (i == k) return;
-    const double f = factors[i];
-    if (f == 0.0) return;
-    a[idx] -= f * a[static_cast<size_t>(k) * 2 * n + j];
-}
-
-// A^T, dense column-major (so element (j, i) of the array is a_ij): the LU
-// path solves A^T X = I, whose column-major X read row-major is A^-1.
-__global__ void k_dense_init_t(int n, const int* ro, const int* co, const double* va, double* at) {
+// ---- dense coarse inverse (LU with partial pivoting, cuSOLVER) ----
+// A^T, dense column-major with leading dimension ld (so element (j, i) of the
+// array is a_ij): the LU path solves A^T X = I, whose column-major X read
+// row-major is A^-1.  With ld = n + 1 and `border`, the matrix is bordered by
+// a row and a column of ones (a zero in the corner).
+__global__ void k_dense_init_t(int n, int ld, const int* ro, const int* co, const double* va, int border,
+                               double* at) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
-    for (int k = ro[i]; k < ro[i + 1]; ++k) at[static_cast<size_t>(i) * n + co[k]] += va[k];
+    for (int k = ro[i]; k < ro[i + 1]; ++k) at[static_cast<size_t>(i) * ld + co[k]] += va[k];
+    if (border) {
+        at[static_cast<size_t>(i) * ld + n] = 1.0;
+        at[static_cast<size_t>(n) * ld + i] = 1.0;
+    }
 }
 
 __global__ void k_identity(int64_t n, double* x) {
@@ -442,27 +420,13 @@ __global__ void k_identity(int64_t n, double* x) {
     if (idx < n * n) x[idx] = (idx / n == idx % n) ? 1.0 : 0.0;
 }
 
+// b (n x n) = the leading n x n block of a (row-major, leading dimension ld)
 template <class S>
-__global__ void k_dense_copy(int64_t count, const double* __restrict__ a, S* __restrict__ b) {
+__global__ void k_dense_block_copy(int n, int ld, const double* __restrict__ a, S* __restrict__ b) {
     const int64_t idx = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
-    if (idx < count) b[idx] = static_cast<S>(a[idx]);
-}
-
-template <class S>
-__global__ void k_gj_extract(int n, const double* a, S* inv) {
-    const size_t idx = static_cast<size_t>(blockIdx.x) * blockDim.x + threadIdx.x;
-    if (idx >= static_cast<size_t>(n) * n) return;
-    const int i = static_cast<int>(idx / n), j = static_cast<int>(idx % n);
-    inv[idx] = static_cast<S>(a[static_cast<size_t>(i) * 2 * n + n + j]);
-}
-
-__global__ void k_gj_init(int n, const int* ro, const int* co, const double* va, double* a) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    double* row = a + static_cast<size_t>(i) * 2 * n;
-    for (int j = 0; j < 2 * n; ++j) row[j] = 0.0;
-    for (int k = ro[i]; k < ro[i + 1]; ++k) row[co[k]] += va[k];
-    row[n + i] = 1.0;
+    if (idx >= static_cast<int64_t>(n) * n) return;
+    const int64_t i = idx / n, j = idx % n;
+    b[idx] = static_cast<S>(a[i * ld + j]);
 }
 
 #define CFDXG_TPR_SWITCH(tpr, ...)                            \
@@ -716,20 +680,24 @@ void upload_level(cfdxg_context* ctx, DevLevel<T>& D, const AmgLevel& H, bool wi
 template <class T>
 void build_dense_inverse_dev(cfdxg_context* ctx, DevHierarchy<T>& d, int n, const int* ro, const int* co,
                              const double* va) {
+    // under the constant null space: the inverse of the bordered matrix, of
+    // which the cycle applies the leading n x n block
+    const int N = n + (d.null_space ? 1 : 0);
     const std::size_t nn = static_cast<std::size_t>(n) * n;
+    const std::size_t NN = static_cast<std::size_t>(N) * N;
     DevBuf<double> at, x;
     DevBuf<int> ipiv, info;
-    at.resize(nn);
-    x.resize(nn);
-    ipiv.resize(n);
+    at.resize(NN);
+    x.resize(NN);
+    ipiv.resize(N);
     info.resize(1);
     if (d.dense_fp64) d.dense64.resize(nn);
     else d.dense.resize(nn);
     cudaStream_t s = ctx->stream;
-    CFDXG_CUDA(cudaMemsetAsync(at.get(), 0, sizeof(double) * nn, s));
-    k_dense_init_t<<<blocks_for(n, kT), kT, 0, s>>>(n, ro, co, va, at.get());
+    CFDXG_CUDA(cudaMemsetAsync(at.get(), 0, sizeof(double) * NN, s));
+    k_dense_init_t<<<blocks_for(n, kT), kT, 0, s>>>(n, N, ro, co, va, d.null_space ? 1 : 0, at.get());
     check_launch(ctx);
-    k_identity<<<blocks_for(static_cast<int64_t>(nn), kT), kT, 0, s>>>(n, x.get());
+    k_identity<<<blocks_for(static_cast<int64_t>(NN), kT), kT, 0, s>>>(N, x.get());
     check_launch(ctx);
     cusolverDnHandle_t h = nullptr;
     if (cusolverDnCreate(&h) != CUSOLVER_STATUS_SUCCESS)
@@ -740,22 +708,22 @@ void build_dense_inverse_dev(cfdxg_context* ctx, DevHierarchy<T>& d, int n, cons
     } guard{h};
     if (cusolverDnSetStream(h, s) != CUSOLVER_STATUS_SUCCESS) throw Error(CFDXG_ERR_CUDA, "cusolverDnSetStream failed");
     int lwork = 0;
-    if (cusolverDnDgetrf_bufferSize(h, n, n, at.get(), n, &lwork) != CUSOLVER_STATUS_SUCCESS)
+    if (cusolverDnDgetrf_bufferSize(h, N, N, at.get(), N, &lwork) != CUSOLVER_STATUS_SUCCESS)
         throw Error(CFDXG_ERR_CUDA, "cusolverDnDgetrf_bufferSize failed");
     DevBuf<double> work(static_cast<std::size_t>(std::max(lwork, 1)));
     // at holds A^T column-major: factor it, then solve A^T X = I
-    if (cusolverDnDgetrf(h, n, n, at.get(), n, work.get(), ipiv.get(), info.get()) != CUSOLVER_STATUS_SUCCESS ||
-        cusolverDnDgetrs(h, CUBLAS_OP_N, n, n, at.get(), n, ipiv.get(), x.get(), n, info.get()) !=
+    if (cusolverDnDgetrf(h, N, N, at.get(), N, work.get(), ipiv.get(), info.get()) != CUSOLVER_STATUS_SUCCESS ||
+        cusolverDnDgetrs(h, CUBLAS_OP_N, N, N, at.get(), N, ipiv.get(), x.get(), N, info.get()) !=
             CUSOLVER_STATUS_SUCCESS)
         throw Error(CFDXG_ERR_CUDA, "dense coarse LU failed");
     int host_info = 0;
     CFDXG_CUDA(cudaMemcpyAsync(&host_info, info.get(), sizeof(int), cudaMemcpyDeviceToHost, s));
     if (d.dense_fp64)
-        k_dense_copy<double><<<blocks_for(static_cast<int64_t>(nn), kT), kT, 0, s>>>(static_cast<int64_t>(nn),
-                                                                                   x.get(), d.dense64.get());
+        k_dense_block_copy<double><<<blocks_for(static_cast<int64_t>(nn), kT), kT, 0, s>>>(n, N, x.get(),
+                                                                                         d.dense64.get());
     else
-        k_dense_copy<float><<<blocks_for(static_cast<int64_t>(nn), kT), kT, 0, s>>>(static_cast<int64_t>(nn),
-                                                                                  x.get(), d.dense.get());
+        k_dense_block_copy<float><<<blocks_for(static_cast<int64_t>(nn), kT), kT, 0, s>>>(n, N, x.get(),
+                                                                                        d.dense.get());
     check_launch(ctx);
     CFDXG_CUDA(cudaStreamSynchronize(s));
     if (host_info != 0) throw Error(CFDXG_ERR_SETUP, "dense coarse level is singular (LU pivot " +
@@ -772,6 +740,18 @@ void build_dense_inverse(cfdxg_context* ctx, DevHierarchy<T>& d, const AmgLevel&
     build_dense_inverse_dev(ctx, d, n, ro.get(), co.get(), va.get());
 }
 
+// The cycle's mean removal under the constant null space
+// (amg_preconditioner.h:1310-1319); nothing without it.
+template <class T, class V>
+void remove_mean(cfdxg_context* ctx, DevHierarchy<T>& d, int n, V* v) {
+    if (!d.null_space) return;
+    const double bytes = account(3.0 * sizeof(V) * n);
+    ProfScope ps(ctx, tname<T>("mean_removal_fp64", "mean_removal_fp32"), bytes);
+    enqueue_remove_constant<V>(ctx->stream, n, v, d.ns_partials.get(), d.ns_in_order, true, 0.0);
+    check_launch(ctx);
+    count_launch(ctx);
+}
+
 template <class T>
 void sweeps_from_zero(cfdxg_context* ctx, DevHierarchy<T>& d, DevLevel<T>& L, const T* r_in,
                       int sweeps) {
@@ -785,9 +765,11 @@ void sweeps_from_zero(cfdxg_context* ctx, DevHierarchy<T>& d, DevLevel<T>& L, co
         account(3.0 * sizeof(T) * L.n);
         launch_pdl(s, k_sweep_zero<T, T>, gb, kT, L.n, d.omega, L.inv_diag.get(), r_in, nullptr, x, d.status);
         check_launch(ctx);
+        remove_mean(ctx, d, L.n, x);
         for (int k = 1; k < sweeps; ++k) {
             launch_sweep<T, T>(ctx, L, r_in, x, x2, d.omega, d.status);
             std::swap(x, x2);
+            remove_mean(ctx, d, L.n, x);
         }
     }
     L.xout = x;
@@ -802,7 +784,7 @@ void enqueue_from(cfdxg_context* ctx, DevHierarchy<T>& d, int l) {
     if (l == d.used - 1) {
         if (d.coarse_mode == 1) {
             k_dense_lu_reference<T><<<1, 32, 0, s>>>(L.n, L.ro.get(), L.co.get(), L.va.get(), L.r.get(),
-                                                     L.x.get(), d.status);
+                                                     L.x.get(), d.null_space ? 1 : 0, d.status);
             check_launch(ctx);
             L.xout = L.x.get();
         } else if (d.coarse_mode == 2) {
@@ -814,6 +796,7 @@ void enqueue_from(cfdxg_context* ctx, DevHierarchy<T>& d, int l) {
                 launch_pdl(s, k_dense_inverse_apply<T, float>, blocks_for(static_cast<int64_t>(L.n) * 32, kT), kT,
                            L.n, d.dense.get(), L.r.get(), L.x.get(), d.status);
             check_launch(ctx);
+            remove_mean(ctx, d, L.n, L.x.get());
             L.xout = L.x.get();
         } else {
             sweeps_from_zero(ctx, d, L, L.r.get(), kCoarseSweeps);
@@ -831,11 +814,14 @@ void enqueue_from(cfdxg_context* ctx, DevHierarchy<T>& d, int l) {
     } else {
         launch_restrict<T>(ctx, L, L.r.get(), C.r.get());   // x = 0: the residual is r
     }
+    remove_mean(ctx, d, C.n, C.r.get());
     enqueue_from(ctx, d, l + 1);
     launch_prolong<T>(ctx, L, C.xout, x, d.status, d.coarse_pre == 0);
+    remove_mean(ctx, d, L.n, x);
     for (int k = 0; k < d.coarse_post; ++k) {
         launch_sweep<T, T>(ctx, L, L.r.get(), x, x2, d.omega, d.status);
         std::swap(x, x2);
+        remove_mean(ctx, d, L.n, x);
     }
     L.xout = x;
 }
@@ -884,6 +870,9 @@ std::unique_ptr<DevHierarchy<T>> upload_hierarchy(cfdxg_context* ctx, const AmgH
     d->coarse_post = h.options.coarse_post >= 0 ? h.options.coarse_post : coarse_default_post;
     d->status = ctx->scratch.status;
     d->dense_fp64 = opt.dense_fp64;
+    d->null_space = opt.constant_null_space;
+    d->ns_in_order = opt.reference_order;
+    if (d->null_space) d->ns_partials.resize(kNsMaxBlocks);
     int used = static_cast<int>(h.levels.size());
     d->coarse_mode = 0;
     if (std::is_same<T, float>::value && coarse_dense_limit > 0) {
@@ -974,59 +963,75 @@ void vcycle_apply(cfdxg_context* ctx, DevHierarchy<T>& d, const double* r, doubl
         // single-level hierarchy: the coarsest treatment applies to the fine level
         launch_pdl(s, k_copy_cast<double, T>, gb, kT, L.n, r, L.r.get());
         check_launch(ctx);
+        remove_mean(ctx, d, L.n, L.r.get());
         enqueue_from(ctx, d, 0);
         launch_pdl(s, k_copy_cast<T, double>, gb, kT, L.n, L.xout, z);
         check_launch(ctx);
+        remove_mean(ctx, d, L.n, z);
         return;
     }
     ensure_graph(ctx, d);
-    // Level-0 right-hand side: FP64 reads the caller's r directly; FP32 converts it in the first sweep.
+    // Level-0 right-hand side: FP64 reads the caller's r directly; FP32 converts
+    // it in the first sweep.  Under the constant null space both first copy it
+    // and remove its mean (the compatible right-hand side of apply()).
     const T* rl = nullptr;
     T* x = L.x.get();
     T* x2 = L.x2.get();
-    if (std::is_same<T, double>::value) {
-        rl = reinterpret_cast<const T*>(r);
-    } else {
-        rl = L.r.get();
+    const bool own_copy = d.null_space || !std::is_same<T, double>::value;
+    if (d.null_space) {
+        launch_pdl(s, k_copy_cast<double, T>, gb, kT, L.n, r, L.r.get());
+        check_launch(ctx);
+        remove_mean(ctx, d, L.n, L.r.get());
     }
+    rl = own_copy ? L.r.get() : reinterpret_cast<const T*>(r);
     if (d.pre == 0) {
-        if (!std::is_same<T, double>::value) {
+        if (!std::is_same<T, double>::value && !d.null_space) {
             launch_pdl(s, k_copy_cast<double, T>, gb, kT, L.n, r, L.r.get());
             check_launch(ctx);
         }
         CFDXG_CUDA(cudaMemsetAsync(x, 0, sizeof(T) * L.n, s));
     } else {
-        launch_pdl(s, k_sweep_zero<T, double>, gb, kT, L.n, d.omega, L.inv_diag.get(), r,
-                                                  std::is_same<T, double>::value ? nullptr : L.r.get(), x,
-                                                  d.status);
+        if (d.null_space)
+            launch_pdl(s, k_sweep_zero<T, T>, gb, kT, L.n, d.omega, L.inv_diag.get(), rl, nullptr, x, d.status);
+        else
+            launch_pdl(s, k_sweep_zero<T, double>, gb, kT, L.n, d.omega, L.inv_diag.get(), r,
+                       std::is_same<T, double>::value ? nullptr : L.r.get(), x, d.status);
         check_launch(ctx);
+        remove_mean(ctx, d, L.n, x);
         for (int k = 1; k < d.pre; ++k) {
             launch_sweep<T, T>(ctx, L, rl, x, x2, d.omega, d.status);
             std::swap(x, x2);
+            remove_mean(ctx, d, L.n, x);
         }
     }
     launch_residual<T>(ctx, L, rl, x, L.res.get());
     DevLevel<T>& C = d.L[1];
     launch_restrict<T>(ctx, L, L.res.get(), C.r.get());
+    remove_mean(ctx, d, C.n, C.r.get());
     {
         ProfScope ps(ctx, tname<T>("vcycle_levels_1plus_fp64_graph", "vcycle_levels_1plus_fp32_graph"), d.graph_bytes);
         CFDXG_CUDA(cudaGraphLaunch(d.exec, s));
     }
     count_launch(ctx, d.graph_kernels);
     launch_prolong<T>(ctx, L, C.xout, x, d.status);
+    remove_mean(ctx, d, L.n, x);
     if (d.post == 0) {
         launch_pdl(s, k_copy_cast<T, double>, gb, kT, L.n, x, z);
         check_launch(ctx);
+        remove_mean(ctx, d, L.n, z);
         return;
     }
     for (int k = 0; k < d.post; ++k) {
         if (k + 1 == d.post) {
             launch_sweep<T, double>(ctx, L, rl, x, z, d.omega, d.status);
+            remove_mean(ctx, d, L.n, z);
         } else {
             launch_sweep<T, T>(ctx, L, rl, x, x2, d.omega, d.status);
             std::swap(x, x2);
+            remove_mean(ctx, d, L.n, x);
         }
     }
+    remove_mean(ctx, d, L.n, z);   // apply()'s removal from the result
 }
 
 template <class T>

@@ -75,6 +75,9 @@ extern "C" {
 #define CFDXG_SCALING_COLUMN 2
 #define CFDXG_SCALING_ROW_COLUMN 3
 #define CFDXG_SCALING_SYMMETRIC_DIAGONAL 4
+/* NullSpaceModel (core/linalg/linear_solver_models.h:59) */
+#define CFDXG_NULL_SPACE_NONE 0
+#define CFDXG_NULL_SPACE_CONSTANT 1
 
 typedef struct cfdxg_context cfdxg_context;
 typedef struct cfdxg_mesh cfdxg_mesh;
@@ -280,7 +283,7 @@ typedef struct {
     int32_t precision;               /* CFDXG_PRECISION_* of the V-cycle */
     int32_t coarse_dense_limit;      /* FP32 V-cycle: the cycle ends at the first level with
                                         <= this many rows (6000) in a dense inverse, formed
-                                        in FP64 (Gauss-Jordan, partial pivoting) and stored
+                                        in FP64 (LU with partial pivoting) and stored
                                         FP32; at 64^3 this is the 5,287-row level, 12 instead
                                         of 13 FGMRES iterations, 10.4 instead of 11.8 ms */
     int32_t reference_order;         /* 1: every row sum in CSR order, so the FP64
@@ -309,6 +312,17 @@ typedef struct {
                                         in FP64 -- with coarse_dense_limit 2000, the FP64
                                         coarsest-level direct solve of the mixed-precision
                                         configuration (1,933 rows at 64^3). */
+    int32_t constant_null_space;     /* 0 (default) / 1: the native AMG's constant_null_space
+                                        (hypre_amg.h:35): setup and update_values require every
+                                        row sum of the operator to vanish (|row sum| <= 256 eps
+                                        max(1, largest absolute row sum),
+                                        amg_preconditioner.h:1289-1308); the cycle removes the
+                                        mean from its input and output, after every sweep,
+                                        the restriction and the prolongation, and solves the
+                                        <= 16-row coarsest level bordered by a row and a column
+                                        of ones (:1191-1203, 2369-2443, 2564-2666).  With
+                                        reference_order the means are summed in index order,
+                                        so the FP64 cycle is the reference's bit for bit. */
 } cfdxg_amg_options;
 
 int cfdxg_amg_options_default(cfdxg_amg_options* opts);
@@ -384,6 +398,19 @@ typedef struct {
                                         solves the scaled system to 0.1 tolerance and certifies
                                         the unscaled one (linear_solver_dispatch.h:302-328,
                                         466-490); CG takes NONE or SYMMETRIC_DIAGONAL only */
+    int32_t null_space;              /* CFDXG_NULL_SPACE_* (default NONE).  CONSTANT: the
+                                        projected solves of linear_solver_dispatch.h:354-400 for
+                                        a singular pure-Neumann pressure / diffusion operator --
+                                        GMRES / FGMRES run solve_projected_gmres
+                                        (projected_gmres.h:84-150: FGMRES on P A P with the
+                                        preconditioner P M P, P v = v - (v.e)e, e the normalised
+                                        ones vector), CG the projected CG of cg_solver.h; the
+                                        native AMG is built with constant_null_space.  b must
+                                        be compatible (|b.e| <= 1e-14 + 1e-12 ||b||) and A e = 0
+                                        (and A^T e = 0 for GMRES) to 1e-12 ||A||_F, else
+                                        CFDXG_NOT_APPLICABLE with x untouched.  Not combined
+                                        with scaling or the learned stage; the unprojected FP64
+                                        residual still certifies the result. */
 } cfdxg_request;
 
 /* Mirrors SolverResult (core/linalg/solver_status.h:45-72) + LinearSolveReport. */
@@ -406,7 +433,7 @@ typedef struct {
 int cfdxg_request_default(cfdxg_request* req);
 
 /* Replaces solve_linear_system (core/linalg/linear_solver_dispatch.h:227-492) for
- * scalar pressure systems without scaling / null space.  With krylov or
+ * scalar pressure systems.  With krylov or
  * preconditioner CFDXG_*_AUTO it first measures the matrix and selects the
  * plan (cfdxg_measure_matrix_characteristics, cfdxg_select_linear_solver, on the
  * host); a plan whose model this library does not provide (BiCGStab, ILU0, ...)
@@ -428,7 +455,9 @@ int cfdxg_solve_linear_system(cfdxg_context* ctx, const cfdxg_matrix* A, const d
  * (core/linalg/gmres_solver.h:28-600, 690-757, setup_preconditioner = false).
  * amg may be NULL (identity).  With req->krylov == CFDXG_KRYLOV_CG it runs
  * solve_cg(A, b, x, preconditioner) (cg_solver.h:605-618) on that hierarchy,
- * or the identity without one. */
+ * or the identity without one.  With req->null_space == CONSTANT: the
+ * projected GMRES of solve_projected_gmres without its setup step, or
+ * solve_cg_prepared with the projector (cg_solver.h:653-666). */
 int cfdxg_solve_gmres(cfdxg_context* ctx, const cfdxg_matrix* A, cfdxg_amg* amg,
                       const double* rhs, double* x, int32_t mem, const cfdxg_request* req,
                       int64_t max_iterations, double tolerance, cfdxg_report* report);

@@ -226,3 +226,33 @@ def test_oracle_case_library_builds_the_same_inputs(ref):
     for s in (0, 3):
         for x, y in zip(cases.simple_fields(a, cc, seed_offset=s), oc.simple_fields(b, cc, seed_offset=s)):
             assert np.array_equal(x, y)
+
+
+def test_null_space_setup_contract_and_hierarchy(ref):
+    """NativeBoomerAMGPreconditioner(constant_null_space=true): setup and
+    update_values require vanishing row sums (amg_preconditioner.h:84, 250,
+    1289-1308); the hierarchy itself is the ordinary one, bit for bit."""
+    m = cases.simple_mesh(6)
+    g = ref.geometry(m)
+    U, rAU, aP, p, fixed, value = cases.simple_fields(m, g["cell_centres"])
+    neumann = ref.simple_assemble(m, U, rAU, p, 1.0, np.zeros_like(fixed), value)
+    dirichlet = ref.simple_assemble(m, U, rAU, p, 1.0, fixed, value)
+    ro, co_, va = neumann["row_offsets"], neumann["columns"], neumann["values"]
+    R = ref.Amg(ro, co_, va, constant_null_space=True)
+    amg = cg.NativeBoomerAMGPreconditioner(None, constant_null_space=1)
+    assert amg.setup_host(ro, co_, va), amg.last_error()
+    assert R.num_levels() == len(amg.hierarchy_level_sizes())
+    for l in range(R.num_levels()):
+        a, b = R.level(l), amg.export_level(l)
+        for k in ("row_offsets", "columns", "values", "inv_diag", "p_columns", "p_values"):
+            assert np.array_equal(a[k], b[k]), (l, k)
+    assert R.omega == amg.omega
+    # a refresh with values that keep the row sums zero is accepted (a scaled copy) ...
+    assert amg.update_values_host(ro, co_, 2.0 * va)
+    # ... one that breaks them is refused, as is a setup on the Dirichlet-fixed operator
+    assert not amg.update_values_host(ro, co_, va + 1e-3 * np.abs(va))
+    other = cg.NativeBoomerAMGPreconditioner(None, constant_null_space=1)
+    assert not other.setup_host(dirichlet["row_offsets"], dirichlet["columns"], dirichlet["values"])
+    assert "null-space" in other.last_error()
+    with pytest.raises(RuntimeError):
+        ref.Amg(dirichlet["row_offsets"], dirichlet["columns"], dirichlet["values"], constant_null_space=True)
