@@ -168,6 +168,7 @@ bool build_cf_interpolation(const HostCsr& A, const std::vector<double>& inv_dia
     const double t_start = tnow();
     Strength strong;
     build_strength_graph(A, inv_diag, threshold, strong);
+    const double t_strength = tnow();
 
     // transpose of the strength graph, rows in increasing source order
     std::vector<uint32_t> t_off(static_cast<std::size_t>(n) + 1, 0), t_col;
@@ -379,8 +380,9 @@ bool build_cf_interpolation(const HostCsr& A, const std::vector<double>& inv_dia
     }
     if (failed) return false;
     if (profile_setup())
-        std::fprintf(stderr, "[cfdxg setup] n=%lld strength+pass1 %.3fs pass2 %.3fs weights %.3fs\n",
-                     static_cast<long long>(n), t_pass1 - t_start, t_pass2 - t_pass1, tnow() - t_pass2);
+        std::fprintf(stderr, "[cfdxg setup] n=%lld strength %.3fs pass1 %.3fs pass2 %.3fs weights %.3fs\n",
+                     static_cast<long long>(n), t_strength - t_start, t_pass1 - t_strength, t_pass2 - t_pass1,
+                     tnow() - t_pass2);
     level.p_off.assign(static_cast<std::size_t>(n) + 1, 0);
     level.p_col.clear();
     level.p_val.clear();
@@ -686,7 +688,8 @@ bool has_constant_null_space(const HostCsr& A) {
     return std::isfinite(residual_scale) && residual_scale <= tolerance;
 }
 
-bool amg_setup(const HostCsr& A, const AmgOptions& opt, AmgHierarchy& out, std::string& error) {
+bool amg_setup(const HostCsr& A, const AmgOptions& opt, AmgHierarchy& out, std::string& error,
+               const GalerkinHook* galerkin) {
     error.clear();
     if (A.n == 0 || !matrix_is_valid(A) || (opt.constant_null_space && !has_constant_null_space(A))) {
         error = "invalid finest matrix, dimensions, CSR, or null-space contract";
@@ -713,9 +716,17 @@ bool amg_setup(const HostCsr& A, const AmgOptions& opt, AmgHierarchy& out, std::
         GalerkinPlan plan;
         HostCsr coarse;
         const double tg0 = tnow();
-        const bool sym_ok = galerkin_symbolic(cur.A, staged, coarse_n, plan);
-        const double tg1 = tnow();
-        const bool num_ok = sym_ok && galerkin_numeric(cur.A, staged, plan, coarse);
+        bool sym_ok = true, num_ok = true;
+        double tg1 = tg0;
+        if (galerkin) {
+            // the product on the device; the plan stays there for the refresh
+            num_ok = (*galerkin)(static_cast<int>(levels.size() - 1), cur.A, staged, coarse_n, coarse);
+            tg1 = tnow();
+        } else {
+            sym_ok = galerkin_symbolic(cur.A, staged, coarse_n, plan);
+            tg1 = tnow();
+            num_ok = sym_ok && galerkin_numeric(cur.A, staged, plan, coarse);
+        }
         if (profile_setup())
             std::fprintf(stderr, "[cfdxg setup]   galerkin symbolic %.3fs numeric %.3fs -> %lld rows %lld nnz\n",
                          tg1 - tg0, tnow() - tg1, static_cast<long long>(coarse.n),

@@ -12,6 +12,7 @@
 // per-row work (strength rows, interpolation rows, Galerkin rows) runs on
 // host threads, each row still computed in the reference's order.
 #pragma once
+#include <functional>
 #include <cstdint>
 #include <string>
 #include <vector>
@@ -67,9 +68,17 @@ struct AmgHierarchy {
     std::string error;
 };
 
+// The Galerkin product P^T A P of one setup level computed elsewhere (on the
+// device): (level index, A, the level's prolongation in p_off/p_col/p_val,
+// coarse size, out: the pruned coarse operator).  The product must be the one
+// galerkin_symbolic + galerkin_numeric give, bit for bit; the level's host
+// plan then stays empty.
+using GalerkinHook = std::function<bool(int, const HostCsr&, const AmgLevel&, int64_t, HostCsr&)>;
+
 // Full setup.  Returns false (and leaves `out` untouched) on failure, with the
 // reason in `error`.
-bool amg_setup(const HostCsr& A, const AmgOptions& options, AmgHierarchy& out, std::string& error);
+bool amg_setup(const HostCsr& A, const AmgOptions& options, AmgHierarchy& out, std::string& error,
+               const GalerkinHook* galerkin = nullptr);
 
 // Numeric refresh on an unchanged fine pattern (amg_preconditioner.h:245-314).
 // Transactional: on failure the hierarchy is unchanged.

@@ -153,10 +153,16 @@ void amg_setup_impl(cfdxg_context* ctx, cfdxg_amg* amg, cfdxg_matrix* A) {
     o.constant_null_space = amg->opts.constant_null_space != 0;
     AmgHierarchy staged;
     std::string err;
-    if (!amg_setup(A->host, o, staged, err)) {
+    // the C/F splitting and interpolation on the host, the Galerkin products on the device
+    DeviceGalerkin galerkin(ctx, A);
+    const GalerkinHook hook = [&galerkin](int l, const HostCsr& a, const AmgLevel& p, int64_t nc, HostCsr& c) {
+        return galerkin(l, a, p, nc, c);
+    };
+    if (!amg_setup(A->host, o, staged, err, &hook)) {
         amg->error = "native AMG hierarchy construction failed: " + err;
         throw Error(CFDXG_ERR_SETUP, amg->error);
     }
+    std::unique_ptr<DevRefresh> refresh = galerkin.take(static_cast<int>(staged.levels.size()));
     std::unique_ptr<DevHierarchy<double>> d64;
     std::unique_ptr<DevHierarchy<float>> d32;
     UploadOptions up;
@@ -175,7 +181,7 @@ void amg_setup_impl(cfdxg_context* ctx, cfdxg_amg* amg, cfdxg_matrix* A) {
     amg->host = std::move(staged);
     amg->d64 = std::move(d64);
     amg->d32 = std::move(d32);
-    amg->refresh.reset();
+    amg->refresh = std::move(refresh);
     amg->host_values_stale = false;
     amg->ctx = ctx;
     amg->ready = true;

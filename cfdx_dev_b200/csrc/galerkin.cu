@@ -19,8 +19,23 @@
 //   damping:           per row the normalised Gershgorin sum in CSR order, the
 //                      level bound its maximum (order-free), omega from the host
 //
-// The symbolic plans built at setup (AP and P^T A P graphs, P^T adjacency) are
-// uploaded once, at the first refresh.
+// The symbolic plans (AP and P^T A P graphs, P^T adjacency) come from the
+// first setup: built on the device by DeviceGalerkin below, or, for a
+// hierarchy set up on the host, uploaded once at the first refresh.
+//
+// DeviceGalerkin runs the first setup's Galerkin products on the device
+// (galerkin_csr_product.h:33-167 symbolic + numeric): each symbolic graph by
+// expand, sort, unique -- every contribution (row, column) as a 64-bit key,
+// radix-sorted, duplicates dropped, so each row's columns come out sorted and
+// unique, the sets the host's marker loops produce -- the P^T adjacency by a
+// stable sort of (coarse column, fine row) keys, then the numeric products of
+// the refresh kernels and the pruning of |v| <= 1e-30.  The coarse operator
+// is therefore the host restatement's bit for bit, and the plan stays on the
+// device for later refreshes.
+#include <cub/device/device_radix_sort.cuh>
+#include <cub/device/device_scan.cuh>
+#include <cub/device/device_select.cuh>
+
 #include <algorithm>
 #include <cmath>
 #include <cstring>
@@ -341,7 +356,332 @@ bool device_has_constant_null_space(cfdxg_context* ctx, const cfdxg_matrix* A) {
     return std::isfinite(residual) && residual <= tolerance;
 }
 
+// ---- first-setup Galerkin product (expand, sort, unique) ----
+
+// the row r with off[r] <= k < off[r + 1] (off non-decreasing, off[0] = 0)
+template <class Off>
+__device__ __forceinline__ int row_of(const Off* __restrict__ off, int rows, int64_t k) {
+    int b = 0, e = rows;   // invariant: off[b] <= k < off[e]
+    while (e - b > 1) {
+        const int m = (b + e) >> 1;
+        if (static_cast<int64_t>(off[m]) <= k) b = m;
+        else e = m;
+    }
+    return b;
+}
+
+// P^T adjacency keys: (coarse column << 32 | fine row) and the entry's position in its P row
+__global__ void k_pt_keys(int n, const int* __restrict__ p_off, const int* __restrict__ p_col,
+                          unsigned long long* __restrict__ keys, int* __restrict__ pos) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    for (int q = p_off[i]; q < p_off[i + 1]; ++q) {
+        keys[q] = (static_cast<unsigned long long>(p_col[q]) << 32) | static_cast<unsigned>(i);
+        pos[q] = q - p_off[i];
+    }
+}
+
+// contributions of A's entry k to AP: the length of P's row co[k]
+__global__ void k_ap_expand_len(int64_t nnz, const int* __restrict__ co, const int* __restrict__ p_off,
+                                int64_t* __restrict__ len) {
+    const int64_t k = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (k < nnz) len[k] = p_off[co[k] + 1] - p_off[co[k]];
+}
+
+__global__ void k_ap_expand(int64_t nnz, int n, const int* __restrict__ ro, const int* __restrict__ co,
+                            const int* __restrict__ p_off, const int* __restrict__ p_col,
+                            const int64_t* __restrict__ eoff, unsigned long long* __restrict__ keys) {
+    const int64_t k = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (k >= nnz) return;
+    const unsigned long long row = static_cast<unsigned long long>(row_of(ro, n, k)) << 32;
+    const int j = co[k];
+    int64_t o = eoff[k];
+    for (int q = p_off[j]; q < p_off[j + 1]; ++q) keys[o++] = row | static_cast<unsigned>(p_col[q]);
+}
+
+// contributions of P^T's entry t to C: the length of AP's row t_row[t]
+__global__ void k_c_expand_len(int64_t tn, const int* __restrict__ t_row, const int* __restrict__ ap_off,
+                               int64_t* __restrict__ len) {
+    const int64_t t = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (t < tn) len[t] = ap_off[t_row[t] + 1] - ap_off[t_row[t]];
+}
+
+__global__ void k_c_expand(int64_t tn, int nc, const int* __restrict__ t_off, const int* __restrict__ t_row,
+                           const int* __restrict__ ap_off, const int* __restrict__ ap_col,
+                           const int64_t* __restrict__ eoff, unsigned long long* __restrict__ keys) {
+    const int64_t t = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (t >= tn) return;
+    const unsigned long long row = static_cast<unsigned long long>(row_of(t_off, nc, t)) << 32;
+    const int i = t_row[t];
+    int64_t o = eoff[t];
+    for (int p = ap_off[i]; p < ap_off[i + 1]; ++p) keys[o++] = row | static_cast<unsigned>(ap_col[p]);
+}
+
+// per-row counts (counts[row + 1]) and the columns of sorted unique keys
+__global__ void k_key_rows(int64_t m, const unsigned long long* __restrict__ keys, int* __restrict__ counts,
+                           int* __restrict__ cols) {
+    const int64_t u = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (u >= m) return;
+    const unsigned long long key = keys[u];
+    atomicAdd(counts + (key >> 32) + 1, 1);
+    cols[u] = static_cast<int>(key & 0xffffffffull);
+}
+
+// galerkin_csr_product.h:141-167 pruning: keep |v| > 1e-30
+__global__ void k_prune_flags(int64_t m, const double* __restrict__ cv, int* __restrict__ flags) {
+    const int64_t p = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (p < m) flags[p] = fabs(cv[p]) > 1e-30 ? 1 : 0;
+    if (p == m) flags[p] = 0;
+}
+
+__global__ void k_prune_scatter(int64_t m, const int* __restrict__ c_col, const double* __restrict__ cv,
+                                const int* __restrict__ flags, const int* __restrict__ slot,
+                                int* __restrict__ keep_pos, int* __restrict__ co, double* __restrict__ va) {
+    const int64_t p = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (p >= m) return;
+    if (flags[p]) {
+        const int d = slot[p];
+        keep_pos[p] = d;
+        co[d] = c_col[p];
+        va[d] = cv[p];
+    } else {
+        keep_pos[p] = -1;
+    }
+}
+
+__global__ void k_pruned_offsets(int nc, const int* __restrict__ c_off, const int* __restrict__ slot,
+                                 int* __restrict__ ro) {
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c <= nc) ro[c] = slot[c_off[c]];
+}
+
+int key_bits(int64_t rows) {
+    int b = 1;
+    while ((int64_t{1} << b) < rows + 1) ++b;
+    return 32 + b;
+}
+
+template <class T>
+void exclusive_sum(cudaStream_t s, const T* in, T* out, int64_t n) {
+    std::size_t bytes = 0;
+    CFDXG_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, bytes, in, out, n, s));
+    DevBuf<unsigned char> tmp(std::max<std::size_t>(bytes, 1));
+    CFDXG_CUDA(cub::DeviceScan::ExclusiveSum(tmp.get(), bytes, in, out, n, s));
+}
+
+// sorted unique keys of `keys` (m entries, begin/end bits) into out; returns their count
+int64_t sort_unique(cudaStream_t s, DevBuf<unsigned long long>& keys, int64_t m, int end_bit,
+                    DevBuf<unsigned long long>& out) {
+    DevBuf<unsigned long long> sorted(std::max<int64_t>(m, 1));
+    std::size_t bytes = 0;
+    CFDXG_CUDA(cub::DeviceRadixSort::SortKeys(nullptr, bytes, keys.get(), sorted.get(), m, 0, end_bit, s));
+    {
+        DevBuf<unsigned char> tmp(std::max<std::size_t>(bytes, 1));
+        CFDXG_CUDA(cub::DeviceRadixSort::SortKeys(tmp.get(), bytes, keys.get(), sorted.get(), m, 0, end_bit, s));
+    }
+    keys.release();
+    out.resize(static_cast<std::size_t>(std::max<int64_t>(m, 1)));
+    DevBuf<int64_t> count(1);
+    bytes = 0;
+    CFDXG_CUDA(cub::DeviceSelect::Unique(nullptr, bytes, sorted.get(), out.get(), count.get(), m, s));
+    {
+        DevBuf<unsigned char> tmp(std::max<std::size_t>(bytes, 1));
+        CFDXG_CUDA(cub::DeviceSelect::Unique(tmp.get(), bytes, sorted.get(), out.get(), count.get(), m, s));
+    }
+    int64_t h = 0;
+    CFDXG_CUDA(cudaMemcpyAsync(&h, count.get(), sizeof(int64_t), cudaMemcpyDeviceToHost, s));
+    CFDXG_CUDA(cudaStreamSynchronize(s));
+    return h;
+}
+
+// CSR (off: rows + 1, col) of sorted unique (row << 32 | col) keys: counts[r + 1]
+// = row r's length, and their inclusive sum is off
+void keys_to_csr(cfdxg_context* ctx, const unsigned long long* keys, int64_t m, int rows, DevBuf<int>& off,
+                 DevBuf<int>& col) {
+    cudaStream_t s = ctx->stream;
+    DevBuf<int> counts(static_cast<std::size_t>(rows) + 1);
+    counts.zero(s);
+    col.resize(static_cast<std::size_t>(std::max<int64_t>(m, 1)));
+    if (m > 0) {
+        k_key_rows<<<blocks_for(m, kT), kT, 0, s>>>(m, keys, counts.get(), col.get());
+        check_launch(ctx);
+    }
+    off.resize(static_cast<std::size_t>(rows) + 1);
+    std::size_t bytes = 0;
+    CFDXG_CUDA(cub::DeviceScan::InclusiveSum(nullptr, bytes, counts.get(), off.get(), rows + 1, s));
+    DevBuf<unsigned char> tmp(std::max<std::size_t>(bytes, 1));
+    CFDXG_CUDA(cub::DeviceScan::InclusiveSum(tmp.get(), bytes, counts.get(), off.get(), rows + 1, s));
+    CFDXG_CUDA(cudaStreamSynchronize(s));
+}
+
 }  // namespace
+
+DeviceGalerkin::DeviceGalerkin(cfdxg_context* ctx, const cfdxg_matrix* A)
+    : ctx_(ctx), A_(A), R_(std::make_unique<DevRefresh>()) {}
+
+bool DeviceGalerkin::operator()(int level, const HostCsr& A, const AmgLevel& P, int64_t coarse_n,
+                                HostCsr& coarse) {
+    cudaStream_t s = ctx_->stream;
+    const int64_t n = A.n, nnz = A.nnz(), pn = static_cast<int64_t>(P.p_col.size());
+    if (n > std::numeric_limits<int>::max() || nnz > std::numeric_limits<int>::max() ||
+        coarse_n > std::numeric_limits<int>::max() || static_cast<int64_t>(P.p_off.size()) != n + 1 ||
+        static_cast<int64_t>(P.p_off[n]) != pn || static_cast<int64_t>(P.p_val.size()) != pn)
+        return false;
+    // galerkin_csr_product.h:52-60: every prolongation column in range, every weight finite
+    for (int64_t q = 0; q < pn; ++q)
+        if (P.p_col[q] >= coarse_n || !std::isfinite(P.p_val[q])) return false;
+    if (static_cast<int>(R_->L.size()) < level + 2) R_->L.resize(level + 2);
+    DevRefreshLevel& F = R_->L[level];
+    const int nc = static_cast<int>(coarse_n);
+    if (level == 0) {
+        // the fine level: the device matrix itself
+        F.n = static_cast<int>(n);
+        F.nnz = nnz;
+        F.ro.resize(n + 1);
+        F.co.resize(nnz);
+        F.va.resize(nnz);
+        CFDXG_CUDA(cudaMemcpyAsync(F.ro.get(), A_->ro.get(), sizeof(int) * (n + 1), cudaMemcpyDeviceToDevice, s));
+        CFDXG_CUDA(cudaMemcpyAsync(F.co.get(), A_->co.get(), sizeof(int) * nnz, cudaMemcpyDeviceToDevice, s));
+        CFDXG_CUDA(cudaMemcpyAsync(F.va.get(), A_->va.get(), sizeof(double) * nnz, cudaMemcpyDeviceToDevice, s));
+    }
+    if (F.n != static_cast<int>(n) || F.nnz != nnz) return false;
+    F.inv_diag.resize(static_cast<std::size_t>(n));
+    F.n_coarse = nc;
+    F.p_off.upload(std::vector<int>(P.p_off.begin(), P.p_off.end()), s);
+    F.p_col.upload(std::vector<int>(P.p_col.begin(), P.p_col.end()), s);
+    F.p_val.upload(P.p_val, s);
+    clear_status(ctx_);
+    int* st = ctx_->scratch.status;
+
+    // P^T adjacency, stable: (column, fine row) keys sorted, positions alongside
+    {
+        DevBuf<unsigned long long> keys(std::max<int64_t>(pn, 1)), sorted(std::max<int64_t>(pn, 1));
+        DevBuf<int> pos(std::max<int64_t>(pn, 1));
+        F.t_pos.resize(std::max<int64_t>(pn, 1));
+        k_pt_keys<<<blocks_for(n, kT), kT, 0, s>>>(static_cast<int>(n), F.p_off.get(), F.p_col.get(), keys.get(),
+                                                  pos.get());
+        check_launch(ctx_);
+        std::size_t bytes = 0;
+        const int end_bit = key_bits(coarse_n);
+        CFDXG_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, bytes, keys.get(), sorted.get(), pos.get(),
+                                                   F.t_pos.get(), pn, 0, end_bit, s));
+        {
+            DevBuf<unsigned char> tmp(std::max<std::size_t>(bytes, 1));
+            CFDXG_CUDA(cub::DeviceRadixSort::SortPairs(tmp.get(), bytes, keys.get(), sorted.get(), pos.get(),
+                                                       F.t_pos.get(), pn, 0, end_bit, s));
+        }
+        keys_to_csr(ctx_, sorted.get(), pn, nc, F.t_off, F.t_row);   // rows: coarse columns; cols: fine rows
+    }
+    // symbolic AP: every (i, p_col[q]) for k in A's row i and q in P's row co[k]
+    {
+        DevBuf<int64_t> len(nnz + 1), eoff(nnz + 1);
+        CFDXG_CUDA(cudaMemsetAsync(len.get() + nnz, 0, sizeof(int64_t), s));
+        k_ap_expand_len<<<blocks_for(nnz, kT), kT, 0, s>>>(nnz, F.co.get(), F.p_off.get(), len.get());
+        check_launch(ctx_);
+        exclusive_sum<int64_t>(s, len.get(), eoff.get(), nnz + 1);
+        int64_t m = 0;
+        CFDXG_CUDA(cudaMemcpyAsync(&m, eoff.get() + nnz, sizeof(int64_t), cudaMemcpyDeviceToHost, s));
+        CFDXG_CUDA(cudaStreamSynchronize(s));
+        DevBuf<unsigned long long> keys(std::max<int64_t>(m, 1)), uniq;
+        k_ap_expand<<<blocks_for(nnz, kT), kT, 0, s>>>(nnz, static_cast<int>(n), F.ro.get(), F.co.get(),
+                                                      F.p_off.get(), F.p_col.get(), eoff.get(), keys.get());
+        check_launch(ctx_);
+        len.release();
+        eoff.release();
+        const int64_t u = sort_unique(s, keys, m, key_bits(n), uniq);
+        if (u > std::numeric_limits<int>::max()) return false;
+        keys_to_csr(ctx_, uniq.get(), u, static_cast<int>(n), F.ap_off, F.ap_col);
+        F.ap.resize(static_cast<std::size_t>(std::max<int64_t>(u, 1)));
+    }
+    // numeric AP
+    {
+        const int grid = static_cast<int>(std::min<int64_t>((n + kWarpRows - 1) / kWarpRows, 148 * 32));
+        k_ap_rows<<<std::max(grid, 1), 32 * kWarpRows, 0, s>>>(static_cast<int>(n), F.ro.get(), F.co.get(),
+                                                               F.va.get(), F.p_off.get(), F.p_col.get(),
+                                                               F.p_val.get(), F.ap_off.get(), F.ap_col.get(),
+                                                               F.ap.get(), st);
+        check_launch(ctx_);
+    }
+    // symbolic C = P^T (AP): every (c, ap_col[p]) for t in P^T's row c and p in AP's row t_row[t]
+    int64_t cm = 0;
+    {
+        DevBuf<int64_t> len(pn + 1), eoff(pn + 1);
+        CFDXG_CUDA(cudaMemsetAsync(len.get() + pn, 0, sizeof(int64_t), s));
+        k_c_expand_len<<<blocks_for(std::max<int64_t>(pn, 1), kT), kT, 0, s>>>(pn, F.t_row.get(), F.ap_off.get(),
+                                                                             len.get());
+        check_launch(ctx_);
+        exclusive_sum<int64_t>(s, len.get(), eoff.get(), pn + 1);
+        int64_t m = 0;
+        CFDXG_CUDA(cudaMemcpyAsync(&m, eoff.get() + pn, sizeof(int64_t), cudaMemcpyDeviceToHost, s));
+        CFDXG_CUDA(cudaStreamSynchronize(s));
+        DevBuf<unsigned long long> keys(std::max<int64_t>(m, 1)), uniq;
+        k_c_expand<<<blocks_for(std::max<int64_t>(pn, 1), kT), kT, 0, s>>>(pn, nc, F.t_off.get(), F.t_row.get(),
+                                                                         F.ap_off.get(), F.ap_col.get(),
+                                                                         eoff.get(), keys.get());
+        check_launch(ctx_);
+        len.release();
+        eoff.release();
+        cm = sort_unique(s, keys, m, key_bits(coarse_n), uniq);
+        if (cm > std::numeric_limits<int>::max()) return false;
+        keys_to_csr(ctx_, uniq.get(), cm, nc, F.c_off, F.c_col);
+        F.cv.resize(static_cast<std::size_t>(std::max<int64_t>(cm, 1)));
+    }
+    // numeric C
+    {
+        const int grid = static_cast<int>(std::min<int64_t>((coarse_n + kWarpRows - 1) / kWarpRows, 148 * 32));
+        k_c_rows<<<std::max(grid, 1), 32 * kWarpRows, 0, s>>>(nc, F.t_off.get(), F.t_row.get(), F.t_pos.get(),
+                                                              F.p_off.get(), F.p_val.get(), F.ap_off.get(),
+                                                              F.ap_col.get(), F.ap.get(), F.c_off.get(),
+                                                              F.c_col.get(), F.cv.get(), st);
+        check_launch(ctx_);
+    }
+    // pruning into the next level's CSR (device) and the refresh's keep positions
+    DevRefreshLevel& C = R_->L[level + 1];
+    {
+        DevBuf<int> flags(cm + 1), slot(cm + 1);
+        k_prune_flags<<<blocks_for(cm + 1, kT), kT, 0, s>>>(cm, F.cv.get(), flags.get());
+        check_launch(ctx_);
+        exclusive_sum<int>(s, flags.get(), slot.get(), cm + 1);
+        int kept = 0;
+        CFDXG_CUDA(cudaMemcpyAsync(&kept, slot.get() + cm, sizeof(int), cudaMemcpyDeviceToHost, s));
+        CFDXG_CUDA(cudaStreamSynchronize(s));
+        C.n = nc;
+        C.nnz = kept;
+        C.ro.resize(static_cast<std::size_t>(nc) + 1);
+        C.co.resize(static_cast<std::size_t>(std::max(kept, 1)));
+        C.va.resize(static_cast<std::size_t>(std::max(kept, 1)));
+        F.keep_pos.resize(static_cast<std::size_t>(std::max<int64_t>(cm, 1)));
+        if (cm > 0) {
+            k_prune_scatter<<<blocks_for(cm, kT), kT, 0, s>>>(cm, F.c_col.get(), F.cv.get(), flags.get(), slot.get(),
+                                                             F.keep_pos.get(), C.co.get(), C.va.get());
+            check_launch(ctx_);
+        }
+        k_pruned_offsets<<<blocks_for(nc + 1, kT), kT, 0, s>>>(nc, F.c_off.get(), slot.get(), C.ro.get());
+        check_launch(ctx_);
+    }
+    if (read_status(ctx_) & kRefreshInvalid) return false;   // synchronises
+    // the coarse operator back to the host for the next level's C/F splitting
+    coarse.n = coarse_n;
+    std::vector<int> ro(static_cast<std::size_t>(nc) + 1), co(static_cast<std::size_t>(C.nnz));
+    coarse.va.resize(static_cast<std::size_t>(C.nnz));
+    CFDXG_CUDA(cudaMemcpyAsync(ro.data(), C.ro.get(), sizeof(int) * (nc + 1), cudaMemcpyDeviceToHost, s));
+    if (C.nnz > 0) {
+        CFDXG_CUDA(cudaMemcpyAsync(co.data(), C.co.get(), sizeof(int) * C.nnz, cudaMemcpyDeviceToHost, s));
+        CFDXG_CUDA(cudaMemcpyAsync(coarse.va.data(), C.va.get(), sizeof(double) * C.nnz, cudaMemcpyDeviceToHost, s));
+    }
+    CFDXG_CUDA(cudaStreamSynchronize(s));
+    coarse.ro.assign(ro.begin(), ro.end());
+    coarse.co.assign(co.begin(), co.end());
+    C.inv_diag.resize(static_cast<std::size_t>(nc));
+    return true;
+}
+
+std::unique_ptr<DevRefresh> DeviceGalerkin::take(int levels) {
+    if (static_cast<int>(R_->L.size()) < levels) return nullptr;
+    R_->L.resize(static_cast<std::size_t>(levels));
+    R_->bounds.resize(static_cast<std::size_t>(levels));
+    return std::move(R_);
+}
 
 bool amg_refresh_device(cfdxg_context* ctx, cfdxg_amg* amg, const cfdxg_matrix* A, std::string& error) {
     AmgHierarchy& h = amg->host;

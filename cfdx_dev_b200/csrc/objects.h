@@ -149,6 +149,23 @@ struct cfdxg_amg {
 
 namespace cfdxg {
 
+// The Galerkin products of a first setup on the device (galerkin.cu), as the
+// setup's GalerkinHook: symbolic graphs by expand, sort, unique, numeric
+// products and pruning by the refresh kernels -- the host restatement's
+// coarse operators bit for bit.  It keeps every level's plan; take() hands
+// them over as the hierarchy's refresh plan.
+class DeviceGalerkin {
+public:
+    DeviceGalerkin(cfdxg_context* ctx, const cfdxg_matrix* A);
+    bool operator()(int level, const HostCsr& A, const AmgLevel& P, int64_t coarse_n, HostCsr& coarse);
+    std::unique_ptr<DevRefresh> take(int levels);
+
+private:
+    cfdxg_context* ctx_;
+    const cfdxg_matrix* A_;
+    std::unique_ptr<DevRefresh> R_;
+};
+
 // numeric refresh of the hierarchy on the device (galerkin.cu): the
 // reference's update_values (amg_preconditioner.h:245-314) with the Galerkin
 // products, pruning check, inverse diagonals and damping computed in its

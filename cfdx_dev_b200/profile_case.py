@@ -12,7 +12,11 @@ sets up the AMG hierarchy and runs each hot-path kernel a few times:
   * ``face``: the face loop alone -- ``--cycles`` pressure-corrector
     assemblies (Gauss gradient + assembly) and Rhie-Chow fluxes with a
     non-zero pressure, inputs on the device, L2 flushed before each call;
-    prints each kernel's device time from the library's live profiler.
+    prints each kernel's device time from the library's live profiler;
+  * ``setup``: the AMG setup with its Galerkin products on the device
+    (cfdxg_amg_setup) and the all-host setup of the same matrix, timed;
+  * ``refresh``: ``--cycles`` numeric refreshes (update_values) with the
+    other seed's a_P (same pattern), each refresh stage's device time.
 
 Example (one kernel, one launch, at 663,552 cells):
 
@@ -56,7 +60,7 @@ def build_system(ctx, n):
 def main(argv=None):
     ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
     ap.add_argument("--n", type=int, default=48, help="lattice size (cells = 6 n^3)")
-    ap.add_argument("--mode", choices=["vcycle", "solve", "face"], default="solve")
+    ap.add_argument("--mode", choices=["vcycle", "solve", "face", "setup", "refresh"], default="solve")
     ap.add_argument("--precision", choices=["fp32_vcycle", "fp64"], default="fp32_vcycle")
     ap.add_argument("--wide-columns", action="store_true", help="int32 columns on every level (narrow_columns = 0)")
     ap.add_argument("--cycles", type=int, default=3, help="V-cycle applications in --mode vcycle")
@@ -65,6 +69,41 @@ def main(argv=None):
     m, mesh, (U, rAU, aP, p, fixed, value), A, b = build_system(ctx, args.n)
     if args.mode == "face":
         face_loop(ctx, m, mesh, (U, rAU, p, fixed, value), A, args.cycles)
+        return
+    if args.mode == "setup":
+        import time
+        amg = cg.NativeBoomerAMGPreconditioner(ctx, precision=args.precision)
+        t0 = time.perf_counter()
+        if not amg.setup(A):
+            raise SystemExit(amg.last_error())
+        t1 = time.perf_counter()
+        host = cg.NativeBoomerAMGPreconditioner(None)
+        ro, co, va = A.to_csr()
+        t2 = time.perf_counter()
+        if not host.setup_host(ro, co, va):
+            raise SystemExit(host.last_error())
+        t3 = time.perf_counter()
+        same = all(np.array_equal(amg.export_level(l)["values"], host.export_level(l)["values"])
+                   for l in range(len(host.hierarchy_level_sizes())))
+        print(f"setup n={args.n} cells={A.n} levels={len(amg.hierarchy_level_sizes())} "
+              f"device-Galerkin setup {t1 - t0:.3f} s (with the device upload), host setup {t3 - t2:.3f} s, "
+              f"identical level values: {same}")
+        return
+    if args.mode == "refresh":
+        amg = cg.NativeBoomerAMGPreconditioner(ctx, precision=args.precision)
+        if not amg.setup(A):
+            raise SystemExit(amg.last_error())
+        aP2 = cg.random_field(m.n_cells, "loguniform", 1.0, 100.0, SEED_AP + 1)
+        A2, _, _, _ = cg.assemble_pressure_correction(mesh, U, np.concatenate([1.0 / aP2] * 3), p, 1.0, fixed,
+                                                      value)
+        ctx.profile(True)
+        for k in range(args.cycles):
+            if not amg.update_values(A2 if k % 2 == 0 else A):
+                raise SystemExit(amg.last_error())
+        ctx.synchronize()
+        for e in ctx.profile_read():
+            if e["launches"] and e["name"].startswith("refresh"):
+                print(f"{e['name']}: {e['launches']} launches, {e['total_ms'] / e['launches']:.2f} ms each")
         return
     amg = cg.NativeBoomerAMGPreconditioner(ctx, precision=args.precision,
                                            narrow_columns=0 if args.wide_columns else 1)
