@@ -161,6 +161,69 @@ void build_strength_graph(const HostCsr& A, const std::vector<double>& inv_diag,
 
 enum : uint8_t { kUndecided = 0, kFine = 1, kCoarse = 2 };
 
+// The undecided points of the first pass by influence: per influence value a
+// three-level 64-ary bitmap over the point indices, so that the selection --
+// the largest influence, then the smallest index -- and every insertion and
+// removal take a few word operations.  It selects exactly the point the
+// reference's heap over (measure, n - i) with lazily skipped stale entries
+// selects.
+class InfluenceBuckets {
+public:
+    explicit InfluenceBuckets(int64_t n)
+        : w0_((n + 63) / 64), w1_((w0_ + 63) / 64), w2_((w1_ + 63) / 64) {}
+    void insert(uint32_t m, uint32_t i) {
+        if (m >= words_.size()) {
+            words_.resize(static_cast<std::size_t>(m) + 1);
+            count_.resize(static_cast<std::size_t>(m) + 1, 0);
+        }
+        auto& b = words_[m];
+        if (b.empty()) b.assign(static_cast<std::size_t>(w0_ + w1_ + w2_), 0);
+        uint64_t* l0 = b.data();
+        uint64_t* l1 = l0 + w0_;
+        uint64_t* l2 = l1 + w1_;
+        l0[i >> 6] |= uint64_t{1} << (i & 63);
+        l1[i >> 12] |= uint64_t{1} << ((i >> 6) & 63);
+        l2[i >> 18] |= uint64_t{1} << ((i >> 12) & 63);
+        ++count_[m];
+        if (static_cast<int64_t>(m) > top_) top_ = m;
+    }
+    void erase(uint32_t m, uint32_t i) {
+        auto& b = words_[m];
+        uint64_t* l0 = b.data();
+        uint64_t* l1 = l0 + w0_;
+        uint64_t* l2 = l1 + w1_;
+        l0[i >> 6] &= ~(uint64_t{1} << (i & 63));
+        if (l0[i >> 6] == 0) {
+            l1[i >> 12] &= ~(uint64_t{1} << ((i >> 6) & 63));
+            if (l1[i >> 12] == 0) l2[i >> 18] &= ~(uint64_t{1} << ((i >> 12) & 63));
+        }
+        --count_[m];
+    }
+    // the largest non-empty influence and its smallest index; false when empty
+    bool best(uint32_t& m, uint32_t& i) {
+        while (top_ >= 0 && count_[top_] == 0) --top_;
+        if (top_ < 0) return false;
+        const auto& b = words_[top_];
+        const uint64_t* l0 = b.data();
+        const uint64_t* l1 = l0 + w0_;
+        const uint64_t* l2 = l1 + w1_;
+        int64_t w2 = 0;
+        while (w2 < w2_ && l2[w2] == 0) ++w2;
+        if (w2 == w2_) return false;
+        const int64_t w1 = w2 * 64 + __builtin_ctzll(l2[w2]);
+        const int64_t w0 = w1 * 64 + __builtin_ctzll(l1[w1]);
+        i = static_cast<uint32_t>(w0 * 64 + __builtin_ctzll(l0[w0]));
+        m = static_cast<uint32_t>(top_);
+        return true;
+    }
+
+private:
+    int64_t w0_, w1_, w2_;
+    std::vector<std::vector<uint64_t>> words_;
+    std::vector<int64_t> count_;
+    int64_t top_ = -1;
+};
+
 // amg_preconditioner.h:1511-1885 (DirectCF, no row cap)
 bool build_cf_interpolation(const HostCsr& A, const std::vector<double>& inv_diag,
                             double threshold, AmgLevel& level, int64_t& coarse_n) {
@@ -183,46 +246,34 @@ bool build_cf_interpolation(const HostCsr& A, const std::vector<double>& inv_dia
                 t_col[cursor[*p]++] = static_cast<uint32_t>(i);
     }
 
-    // First pass: dynamic-influence selection with lowest-index tie break.
-    // Max-heap over (measure, n - i), packed into one key (measure < 2^31).
+    // First pass: dynamic-influence selection (the largest influence, the
+    // lowest index among equals), the undecided points kept by influence.
     std::vector<uint8_t> point(static_cast<std::size_t>(n), kUndecided);
     std::vector<uint32_t> influence(static_cast<std::size_t>(n));
-    std::vector<uint64_t> heap;
-    heap.reserve(static_cast<std::size_t>(n) * 2);
-    const auto key = [n](uint64_t measure, int64_t i) {
-        return (measure << 32) | static_cast<uint64_t>(n - i);
-    };
+    InfluenceBuckets candidates(n);
     for (int64_t i = 0; i < n; ++i) {
         influence[i] = t_off[i + 1] - t_off[i];
-        heap.push_back(key(influence[i], i));
+        candidates.insert(influence[i], static_cast<uint32_t>(i));
     }
-    std::priority_queue<uint64_t> candidates(std::less<uint64_t>(), std::move(heap));
     int64_t undecided = n;
     while (undecided > 0) {
-        int64_t best = n;
-        while (!candidates.empty()) {
-            const uint64_t top = candidates.top();
-            candidates.pop();
-            const uint64_t measure = top >> 32;
-            const int64_t i = n - static_cast<int64_t>(top & 0xffffffffull);
-            if (point[i] == kUndecided && measure == influence[i]) {
-                best = i;
-                break;
-            }
-        }
-        if (best == n) return false;
+        uint32_t measure = 0, best = 0;
+        if (!candidates.best(measure, best)) return false;
+        candidates.erase(measure, best);
         point[best] = kCoarse;
         --undecided;
         for (uint32_t t = t_off[best]; t < t_off[best + 1]; ++t) {
             const uint32_t j = t_col[t];
             if (point[j] != kUndecided) continue;
+            candidates.erase(influence[j], j);
             point[j] = kFine;
             --undecided;
             for (const uint32_t* p = strong.begin(j); p != strong.end(j); ++p) {
                 const uint32_t k = *p;
                 if (point[k] == kUndecided) {
+                    candidates.erase(influence[k], k);
                     ++influence[k];
-                    candidates.push(key(influence[k], k));
+                    candidates.insert(influence[k], k);
                 }
             }
         }

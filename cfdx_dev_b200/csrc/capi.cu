@@ -2,6 +2,8 @@
 // solve_linear_system / solve_gmres entry points.
 #include <chrono>
 #include <cmath>
+#include <cstdio>
+#include <cstdlib>
 #include <cstring>
 
 #include "io.h"
@@ -163,6 +165,7 @@ void amg_setup_impl(cfdxg_context* ctx, cfdxg_amg* amg, cfdxg_matrix* A) {
         throw Error(CFDXG_ERR_SETUP, amg->error);
     }
     std::unique_ptr<DevRefresh> refresh = galerkin.take(static_cast<int>(staged.levels.size()));
+    const double t_hierarchy = now_seconds();
     std::unique_ptr<DevHierarchy<double>> d64;
     std::unique_ptr<DevHierarchy<float>> d32;
     UploadOptions up;
@@ -173,10 +176,13 @@ void amg_setup_impl(cfdxg_context* ctx, cfdxg_amg* amg, cfdxg_matrix* A) {
         up.coarse_dense_limit = amg->opts.coarse_dense_limit;
         up.half_values = amg->opts.half_values != 0;
         up.dense_fp64 = amg->opts.dense_fp64 != 0;
-        d32 = upload_hierarchy<float>(ctx, staged, up);
+        d32 = upload_hierarchy<float>(ctx, staged, up, refresh.get());
     } else {
-        d64 = upload_hierarchy<double>(ctx, staged, up);
+        d64 = upload_hierarchy<double>(ctx, staged, up, refresh.get());
     }
+    if (std::getenv("CFDXG_SETUP_PROFILE"))
+        std::fprintf(stderr, "[cfdxg setup] hierarchy %.3fs, device upload %.3fs\n", t_hierarchy - t0,
+                     now_seconds() - t_hierarchy);
     // commit only after every stage succeeded (hypre_amg.cpp:163-236 is transactional)
     amg->host = std::move(staged);
     amg->d64 = std::move(d64);

@@ -192,11 +192,11 @@ struct UploadOptions {
     bool constant_null_space = false;   // the cycle of a pure-Neumann operator (mean removals)
 };
 
+// From the host hierarchy, or, with R (the device levels a device-Galerkin
+// setup left), from the device copy -- the same layout and values.
 template <class T>
 std::unique_ptr<DevHierarchy<T>> upload_hierarchy(cfdxg_context* ctx, const AmgHierarchy& h,
-                                                  const UploadOptions& opt);
-template <class T>
-void refresh_hierarchy_values(cfdxg_context* ctx, DevHierarchy<T>& d, const AmgHierarchy& h);
+                                                  const UploadOptions& opt, const DevRefresh* R = nullptr);
 // z = V-cycle(r); r, z are FP64 device vectors.
 template <class T>
 void vcycle_apply(cfdxg_context* ctx, DevHierarchy<T>& d, const double* r, double* z);

@@ -851,52 +851,6 @@ void ensure_graph(cfdxg_context* ctx, DevHierarchy<T>& d) {
 
 }  // namespace
 
-template <class T>
-std::unique_ptr<DevHierarchy<T>> upload_hierarchy(cfdxg_context* ctx, const AmgHierarchy& h,
-                                                  const UploadOptions& opt) {
-    const int coarse_dense_limit = opt.coarse_dense_limit;
-    auto d = std::make_unique<DevHierarchy<T>>();
-    d->omega = static_cast<T>(h.omega);
-    d->pre = h.options.pre;
-    d->post = h.options.post;
-    // Levels >= 1: the reference's pre/post counts for the FP64 cycle.  The FP32
-    // cycle defaults to one post-sweep and no pre-sweep there (its fine level
-    // keeps pre/post): the coarse operators hold ~25x the fine level's nonzeros,
-    // and V(0,1) reads each of them once per cycle instead of twice for V(1,1).
-    const bool fp32 = std::is_same<T, float>::value;
-    const int coarse_default_pre = fp32 ? kFp32CoarsePre : h.options.pre;
-    const int coarse_default_post = fp32 ? kFp32CoarsePost : h.options.post;
-    d->coarse_pre = h.options.coarse_pre >= 0 ? h.options.coarse_pre : coarse_default_pre;
-    d->coarse_post = h.options.coarse_post >= 0 ? h.options.coarse_post : coarse_default_post;
-    d->status = ctx->scratch.status;
-    d->dense_fp64 = opt.dense_fp64;
-    d->null_space = opt.constant_null_space;
-    d->ns_in_order = opt.reference_order;
-    if (d->null_space) d->ns_partials.resize(kNsMaxBlocks);
-    int used = static_cast<int>(h.levels.size());
-    d->coarse_mode = 0;
-    if (std::is_same<T, float>::value && coarse_dense_limit > 0) {
-        for (int l = 0; l < used; ++l)
-            if (h.levels[l].A.n <= coarse_dense_limit) { used = l + 1; d->coarse_mode = 2; break; }
-    }
-    if (d->coarse_mode == 0 && h.levels[used - 1].A.n <= kDenseDirectLimit) d->coarse_mode = 1;
-    d->used = used;
-    d->L.resize(used);
-    for (int l = 0; l < used; ++l) upload_level(ctx, d->L[l], h.levels[l], l + 1 < used, opt);
-    if (d->coarse_mode == 2) build_dense_inverse(ctx, *d, h.levels[used - 1]);
-    return d;
-}
-
-template <class T>
-void refresh_hierarchy_values(cfdxg_context* ctx, DevHierarchy<T>& d, const AmgHierarchy& h) {
-    d.omega = static_cast<T>(h.omega);
-    for (int l = 0; l < d.used; ++l) upload_level_values(ctx, d.L[l], h.levels[l]);
-    if (d.coarse_mode == 2) build_dense_inverse(ctx, d, h.levels[d.used - 1]);
-    // omega is a kernel argument baked into the graph: recapture
-    if (d.exec) { cudaGraphExecDestroy(d.exec); d.exec = nullptr; }
-    if (d.graph) { cudaGraphDestroy(d.graph); d.graph = nullptr; }
-}
-
 // FP16 fractions of each row's largest magnitude and that magnitude (the
 // host upload's rounding, operation for operation).
 __global__ void k_quantize_rows(int n, const int* __restrict__ ro, const double* __restrict__ va,
@@ -925,6 +879,160 @@ void copy_or_cast(cfdxg_context* ctx, const double* src, T* dst, int64_t n) {
         k_cast_values<T><<<blocks_for(n, kT), kT, 0, ctx->stream>>>(n, src, dst);
         check_launch(ctx);
     }
+}
+
+// ---- the same upload from the device copy the setup's Galerkin products left
+
+// flag = 1 when some |column - row| does not fit in 16 bits
+__global__ void k_narrow_check(int n, const int* __restrict__ ro, const int* __restrict__ co, int* flag) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    for (int k = ro[i]; k < ro[i + 1]; ++k) {
+        const int d = co[k] - i;
+        if (d < INT16_MIN || d > INT16_MAX) { atomicOr(flag, 1); return; }
+    }
+}
+
+__global__ void k_narrow_columns(int n, const int* __restrict__ ro, const int* __restrict__ co,
+                                 int16_t* __restrict__ c16) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    for (int k = ro[i]; k < ro[i + 1]; ++k) c16[k] = static_cast<int16_t>(co[k] - i);
+}
+
+// P^T values in the stable fine-row order of the setup's P^T adjacency
+template <class T>
+__global__ void k_transpose_values(int64_t m, const int* __restrict__ t_row, const int* __restrict__ t_pos,
+                                   const int* __restrict__ p_off, const double* __restrict__ p_val,
+                                   T* __restrict__ r_val) {
+    const int64_t t = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (t < m) r_val[t] = static_cast<T>(p_val[p_off[t_row[t]] + t_pos[t]]);
+}
+
+template <class T>
+void device_copy(cfdxg_context* ctx, DevBuf<T>& dst, const T* src, int64_t count) {
+    dst.resize(static_cast<std::size_t>(std::max<int64_t>(count, 1)));
+    if (count > 0)
+        CFDXG_CUDA(cudaMemcpyAsync(dst.get(), src, sizeof(T) * count, cudaMemcpyDeviceToDevice, ctx->stream));
+}
+
+// upload_level from the setup's device level (int CSR, FP64 values, P and the
+// stable P^T adjacency): the same layout choices and the same values, formed
+// by kernels instead of host loops.
+template <class T>
+void upload_level_device(cfdxg_context* ctx, DevLevel<T>& D, const AmgLevel& H, const DevRefreshLevel& R,
+                         bool with_transfer, const UploadOptions& opt) {
+    cudaStream_t s = ctx->stream;
+    D.n = R.n;
+    D.nnz = static_cast<int>(R.nnz);
+    D.tpr = choose_tpr(D.nnz, D.n, opt.reference_order);
+    device_copy(ctx, D.ro, R.ro.get(), D.n + 1);
+    bool narrow = with_transfer && opt.narrow_columns && D.tpr == 1;
+    if (narrow) {
+        DevBuf<int> flag(1);
+        flag.zero(s);
+        k_narrow_check<<<blocks_for(D.n, kT), kT, 0, s>>>(D.n, R.ro.get(), R.co.get(), flag.get());
+        check_launch(ctx);
+        int h = 0;
+        CFDXG_CUDA(cudaMemcpyAsync(&h, flag.get(), sizeof(int), cudaMemcpyDeviceToHost, s));
+        CFDXG_CUDA(cudaStreamSynchronize(s));
+        narrow = h == 0;
+    }
+    D.narrow = narrow;
+    if (narrow) {
+        D.co16.resize(static_cast<std::size_t>(std::max(D.nnz, 1)));
+        k_narrow_columns<<<blocks_for(D.n, kT), kT, 0, s>>>(D.n, R.ro.get(), R.co.get(), D.co16.get());
+        check_launch(ctx);
+        D.co.release();
+    } else {
+        device_copy(ctx, D.co, R.co.get(), D.nnz);
+        D.co16.release();
+    }
+    D.half = std::is_same<T, float>::value && opt.half_values && with_transfer && D.tpr > 1;
+    if (D.half) {
+        if constexpr (std::is_same<T, float>::value) {
+            D.vh.resize(static_cast<std::size_t>(std::max(D.nnz, 1)));
+            D.rscale.resize(static_cast<std::size_t>(D.n));
+            k_quantize_rows<<<blocks_for(D.n, kT), kT, 0, s>>>(D.n, R.ro.get(), R.va.get(), D.vh.get(),
+                                                               D.rscale.get());
+            check_launch(ctx);
+        }
+        D.va.release();
+    } else {
+        D.va.resize(static_cast<std::size_t>(std::max(D.nnz, 1)));
+        copy_or_cast<T>(ctx, R.va.get(), D.va.get(), D.nnz);
+    }
+    std::vector<T> d(H.inv_diag.size());
+    for (std::size_t k = 0; k < d.size(); ++k) d[k] = static_cast<T>(H.inv_diag[k]);
+    D.inv_diag.upload(d, s);
+    D.r.resize(D.n); D.x.resize(D.n); D.x2.resize(D.n); D.res.resize(D.n);
+    if (with_transfer) {
+        const int64_t pn = static_cast<int64_t>(H.p_col.size());
+        D.nc = R.n_coarse;
+        D.tpr_r = choose_transfer_tpr(pn, D.nc, opt.reference_order);
+        D.tpr_p = choose_transfer_tpr(pn, D.n, opt.reference_order);
+        device_copy(ctx, D.p_off, R.p_off.get(), D.n + 1);
+        device_copy(ctx, D.p_col, R.p_col.get(), pn);
+        D.p_val.resize(static_cast<std::size_t>(std::max<int64_t>(pn, 1)));
+        copy_or_cast<T>(ctx, R.p_val.get(), D.p_val.get(), pn);
+        device_copy(ctx, D.r_off, R.t_off.get(), D.nc + 1);
+        device_copy(ctx, D.r_row, R.t_row.get(), pn);
+        D.r_val.resize(static_cast<std::size_t>(std::max<int64_t>(pn, 1)));
+        if (pn > 0) {
+            k_transpose_values<T><<<blocks_for(pn, kT), kT, 0, s>>>(pn, R.t_row.get(), R.t_pos.get(), R.p_off.get(),
+                                                                    R.p_val.get(), D.r_val.get());
+            check_launch(ctx);
+        }
+    }
+    CFDXG_CUDA(cudaStreamSynchronize(s));
+}
+
+template <class T>
+std::unique_ptr<DevHierarchy<T>> upload_hierarchy(cfdxg_context* ctx, const AmgHierarchy& h,
+                                                  const UploadOptions& opt, const DevRefresh* R) {
+    const int coarse_dense_limit = opt.coarse_dense_limit;
+    auto d = std::make_unique<DevHierarchy<T>>();
+    d->omega = static_cast<T>(h.omega);
+    d->pre = h.options.pre;
+    d->post = h.options.post;
+    // Levels >= 1: the reference's pre/post counts for the FP64 cycle.  The FP32
+    // cycle defaults to one post-sweep and no pre-sweep there (its fine level
+    // keeps pre/post): the coarse operators hold ~25x the fine level's nonzeros,
+    // and V(0,1) reads each of them once per cycle instead of twice for V(1,1).
+    const bool fp32 = std::is_same<T, float>::value;
+    const int coarse_default_pre = fp32 ? kFp32CoarsePre : h.options.pre;
+    const int coarse_default_post = fp32 ? kFp32CoarsePost : h.options.post;
+    d->coarse_pre = h.options.coarse_pre >= 0 ? h.options.coarse_pre : coarse_default_pre;
+    d->coarse_post = h.options.coarse_post >= 0 ? h.options.coarse_post : coarse_default_post;
+    d->status = ctx->scratch.status;
+    d->dense_fp64 = opt.dense_fp64;
+    d->null_space = opt.constant_null_space;
+    d->ns_in_order = opt.reference_order;
+    if (d->null_space) d->ns_partials.resize(kNsMaxBlocks);
+    int used = static_cast<int>(h.levels.size());
+    d->coarse_mode = 0;
+    if (std::is_same<T, float>::value && coarse_dense_limit > 0) {
+        for (int l = 0; l < used; ++l)
+            if (h.levels[l].A.n <= coarse_dense_limit) { used = l + 1; d->coarse_mode = 2; break; }
+    }
+    if (d->coarse_mode == 0 && h.levels[used - 1].A.n <= kDenseDirectLimit) d->coarse_mode = 1;
+    d->used = used;
+    d->L.resize(used);
+    // from the setup's device copy of the levels when there is one
+    const bool from_device = R && static_cast<int>(R->L.size()) >= used;
+    for (int l = 0; l < used; ++l) {
+        if (from_device) upload_level_device(ctx, d->L[l], h.levels[l], R->L[l], l + 1 < used, opt);
+        else upload_level(ctx, d->L[l], h.levels[l], l + 1 < used, opt);
+    }
+    if (d->coarse_mode == 2) {
+        if (from_device) {
+            const DevRefreshLevel& C = R->L[used - 1];
+            build_dense_inverse_dev(ctx, *d, C.n, C.ro.get(), C.co.get(), C.va.get());
+        } else {
+            build_dense_inverse(ctx, *d, h.levels[used - 1]);
+        }
+    }
+    return d;
 }
 
 // New level values, inverse diagonals and damping from the device refresh
@@ -1037,10 +1145,10 @@ void vcycle_apply(cfdxg_context* ctx, DevHierarchy<T>& d, const double* r, doubl
 template <class T>
 void destroy_hierarchy(DevHierarchy<T>* d) { delete d; }
 
-template std::unique_ptr<DevHierarchy<double>> upload_hierarchy<double>(cfdxg_context*, const AmgHierarchy&, const UploadOptions&);
-template std::unique_ptr<DevHierarchy<float>> upload_hierarchy<float>(cfdxg_context*, const AmgHierarchy&, const UploadOptions&);
-template void refresh_hierarchy_values<double>(cfdxg_context*, DevHierarchy<double>&, const AmgHierarchy&);
-template void refresh_hierarchy_values<float>(cfdxg_context*, DevHierarchy<float>&, const AmgHierarchy&);
+template std::unique_ptr<DevHierarchy<double>> upload_hierarchy<double>(cfdxg_context*, const AmgHierarchy&, const UploadOptions&,
+                                                                         const DevRefresh*);
+template std::unique_ptr<DevHierarchy<float>> upload_hierarchy<float>(cfdxg_context*, const AmgHierarchy&, const UploadOptions&,
+                                                                       const DevRefresh*);
 template void set_hierarchy_values_device<double>(cfdxg_context*, DevHierarchy<double>&, const DevRefresh&, double);
 template void set_hierarchy_values_device<float>(cfdxg_context*, DevHierarchy<float>&, const DevRefresh&, double);
 template void vcycle_apply<double>(cfdxg_context*, DevHierarchy<double>&, const double*, double*);
