@@ -92,14 +92,19 @@ bool matrix_is_valid(const HostCsr& A) {
     if (A.n <= 0 || static_cast<int64_t>(A.ro.size()) != A.n + 1 || A.ro[0] != 0 ||
         A.ro[A.n] != static_cast<uint32_t>(A.co.size()) || A.co.size() != A.va.size())
         return false;
-    for (int64_t i = 0; i < A.n; ++i) {
+    for (int64_t i = 0; i < A.n; ++i)
         if (A.ro[i + 1] < A.ro[i]) return false;
-        for (uint32_t k = A.ro[i]; k < A.ro[i + 1]; ++k) {
-            if (A.co[k] >= A.n || !std::isfinite(A.va[k])) return false;
-            if (k > A.ro[i] && A.co[k] <= A.co[k - 1]) return false;
-        }
-    }
-    return true;
+    std::atomic<bool> ok{true};
+    parallel_chunks(A.n, 4096, [&](int64_t b, int64_t e, int) {
+        for (int64_t i = b; i < e && ok.load(std::memory_order_relaxed); ++i)
+            for (uint32_t k = A.ro[i]; k < A.ro[i + 1]; ++k) {
+                if (A.co[k] >= A.n || !std::isfinite(A.va[k]) || (k > A.ro[i] && A.co[k] <= A.co[k - 1])) {
+                    ok = false;
+                    return;
+                }
+            }
+    });
+    return ok;
 }
 
 // Value lookup on a row with sorted unique columns: identical to the

@@ -37,7 +37,11 @@
 #include <cub/device/device_select.cuh>
 
 #include <algorithm>
+#include <climits>
+#include <chrono>
 #include <cmath>
+#include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <limits>
 
@@ -61,15 +65,34 @@ __device__ __forceinline__ int find_col(const int* __restrict__ col, int b, int 
     return -1;
 }
 
+// The output row's columns staged in shared memory when they fit (the
+// binary searches of every contribution then read shared memory); the
+// position returned is global (base + index), -1 when absent.
+constexpr int kStageCols = 1024;
+
+__device__ __forceinline__ int find_staged(const int* __restrict__ col, int len, int key, int base) {
+    int b = 0, e = len;
+    while (b < e) {
+        const int m = (b + e) >> 1;
+        const int v = col[m];
+        if (v == key) return base + m;
+        if (v < key) b = m + 1;
+        else e = m;
+    }
+    return -1;
+}
+
 // Both Galerkin products run one warp per output row.  The row's
 // contributions form an ordered stream -- for AP row i the pairs (k, q) of A's
 // row i in CSR order and, inside each, P's row co[k] in order; for C row c the
 // pairs (t, p) of P^T's row c (fine rows increasing) and, inside each, AP's
 // row t_row[t] in order.  Lanes evaluate 32 consecutive contributions at a
-// time (product and target entry), then, slot by slot in stream order, the
-// lane that owns the target entry (position mod 32) adds it.  Every entry
-// therefore receives its contributions in exactly the order of the reference's
-// row-wise accumulation, and the sum is bit-identical to it.
+// time (product and target entry); lanes whose targets coincide (always from
+// different source entries, since every row of P and of AP has distinct
+// columns) are combined by the lowest of them, which adds their values to the
+// entry in lane order -- the stream order.  Every entry therefore receives its
+// contributions in exactly the order of the reference's row-wise
+// accumulation, and the sum is bit-identical to it.
 constexpr int kWarpRows = 8;   // warps per block
 
 // Exclusive scan over the warp of v (lane order); returns the total in *total.
@@ -84,15 +107,67 @@ __device__ __forceinline__ int warp_exclusive_scan(int v, int lane, int* total) 
     return x - v;
 }
 
-// Adds the 32 evaluated contributions (value, target position; pos < 0: none)
-// in slot order, each by the lane owning its target.
-__device__ __forceinline__ void ordered_add(double value, int pos, int lane, double* __restrict__ out) {
-#pragma unroll 4
-    for (int slot = 0; slot < 32; ++slot) {
-        const double v = __shfl_sync(0xffffffffu, value, slot);
-        const int p = __shfl_sync(0xffffffffu, pos, slot);
-        if (p >= 0 && (p & 31) == lane) out[p] = out[p] + v;
+// The lane whose segment [end - len, end) holds stream index s: the number of
+// lanes whose (non-decreasing) segment end is <= s, by a five-step search.
+__device__ __forceinline__ int segment_owner(int end, int s) {
+    int pos = 0;
+#pragma unroll
+    for (int step = 16; step >= 1; step >>= 1) {
+        const int e = __shfl_sync(0xffffffffu, end, pos + step - 1);
+        if (e <= s) pos += step;
     }
+    return pos;
+}
+
+// Adds the 32 evaluated contributions (value, target position; pos < 0: none)
+// to out; lanes with equal targets are added by the lowest of them in lane
+// order.  stage: this warp's 32 doubles of shared memory.
+__device__ __forceinline__ void ordered_add(double value, int pos, int lane, double* __restrict__ out,
+                                            double* __restrict__ stage) {
+    const unsigned active = __ballot_sync(0xffffffffu, pos >= 0);
+    stage[lane] = value;
+    __syncwarp();
+    if (pos >= 0) {
+        const unsigned peers = __match_any_sync(active, pos);
+        if ((peers & ((1u << lane) - 1u)) == 0u) {
+            double acc = out[pos];
+            for (unsigned m = peers; m != 0u; m &= m - 1u) acc = acc + stage[__ffs(m) - 1];
+            out[pos] = acc;
+        }
+    }
+    __syncwarp();
+}
+
+// first index in col[b, e) (sorted) whose value is >= key
+__device__ __forceinline__ int lower_bound_col(const int* __restrict__ col, int b, int e, int key) {
+    while (b < e) {
+        const int m = (b + e) >> 1;
+        if (col[m] < key) b = m + 1;
+        else e = m;
+    }
+    return b;
+}
+
+// Long output rows on levels with few rows are split among `splits` warps by
+// their (sorted) columns: warp s of a row owns the output positions
+// [b + L s / splits, b + L (s + 1) / splits) and takes from each source row
+// only the entries whose column falls in its slice (a binary search in the
+// sorted source row), so the entries it owns still receive every one of their
+// contributions in stream order.  splits = 1 is the plain one-warp-per-row
+// form.
+struct RowSlice {
+    int lo, hi;            // owned output positions
+    int col_lo, col_hi;    // their column range [col_lo, col_hi)
+};
+
+__device__ __forceinline__ RowSlice row_slice(const int* __restrict__ col, int b, int e, int split, int splits) {
+    const int len = e - b;
+    RowSlice r;
+    r.lo = b + static_cast<int>(static_cast<int64_t>(len) * split / splits);
+    r.hi = b + static_cast<int>(static_cast<int64_t>(len) * (split + 1) / splits);
+    r.col_lo = r.lo < e ? col[r.lo] : INT_MAX;
+    r.col_hi = r.hi < e ? col[r.hi] : INT_MAX;
+    return r;
 }
 
 // AP = A P (galerkin_csr_product.h accumulate, first product)
@@ -104,13 +179,25 @@ __global__ void __launch_bounds__(32 * kWarpRows) k_ap_rows(int n, const int* __
                                                             const double* __restrict__ p_val,
                                                             const int* __restrict__ ap_off,
                                                             const int* __restrict__ ap_col,
-                                                            double* __restrict__ ap, int* status) {
+                                                            double* __restrict__ ap, int splits, int* status) {
+    __shared__ double stage_all[kWarpRows][32];
+    __shared__ int cols_all[kWarpRows][kStageCols];
     const int lane = threadIdx.x & 31;
-    const int warps = gridDim.x * kWarpRows;
-    for (int i = blockIdx.x * kWarpRows + (threadIdx.x >> 5); i < n; i += warps) {
-        const int b = ap_off[i], e = ap_off[i + 1];
-        for (int p = b + lane; p < e; p += 32) ap[p] = 0.0;
+    double* stage = stage_all[threadIdx.x >> 5];
+    int* scols = cols_all[threadIdx.x >> 5];
+    const int64_t units = static_cast<int64_t>(n) * splits;
+    const int64_t warps = static_cast<int64_t>(gridDim.x) * kWarpRows;
+    for (int64_t u = static_cast<int64_t>(blockIdx.x) * kWarpRows + (threadIdx.x >> 5); u < units; u += warps) {
+        const int i = static_cast<int>(u / splits);
+        const RowSlice sl = row_slice(ap_col, ap_off[i], ap_off[i + 1], static_cast<int>(u % splits), splits);
+        const int b = sl.lo, e = sl.hi;
+        const bool staged = e - b <= kStageCols;
+        for (int p = b + lane; p < e; p += 32) {
+            ap[p] = 0.0;
+            if (staged) scols[p - b] = ap_col[p];
+        }
         __syncwarp();
+        if (b == e) continue;
         for (int kb = ro[i]; kb < ro[i + 1]; kb += 32) {
             const int k = kb + lane;
             int len = 0, qb = 0;
@@ -119,34 +206,33 @@ __global__ void __launch_bounds__(32 * kWarpRows) k_ap_rows(int n, const int* __
                 const int j = co[k];
                 a = va[k];
                 qb = p_off[j];
-                len = p_off[j + 1] - qb;
+                int qe = p_off[j + 1];
+                if (splits > 1) {
+                    qb = lower_bound_col(p_col, qb, qe, sl.col_lo);
+                    qe = lower_bound_col(p_col, qb, qe, sl.col_hi);
+                }
+                len = qe - qb;
             }
             int total;
             const int start = warp_exclusive_scan(len, lane, &total);
+            const int end = start + len;
             for (int s0 = 0; s0 < total; s0 += 32) {
                 const int s = s0 + lane;
-                double value = 0.0;
-                int pos = -1;
-                // the entry k whose segment holds s: the last lane with a
-                // non-empty segment starting at or before s (warp-wide loop)
-                int own = 0;
-                for (int l = 0; l < 32; ++l) {
-                    const int st = __shfl_sync(0xffffffffu, start, l);
-                    const int ln = __shfl_sync(0xffffffffu, len, l);
-                    if (ln > 0 && st <= s) own = l;
-                }
+                const int own = segment_owner(end, s < total ? s : total - 1);
                 const double a_own = __shfl_sync(0xffffffffu, a, own);
                 const int qb_own = __shfl_sync(0xffffffffu, qb, own);
                 const int st_own = __shfl_sync(0xffffffffu, start, own);
+                double value = 0.0;
+                int pos = -1;
                 if (s < total) {
                     const int q = qb_own + (s - st_own);
                     const double w = p_val[q];
                     if (!isfinite(w)) atomicOr(status, kRefreshInvalid);
-                    pos = find_col(ap_col, b, e, p_col[q]);
+                    pos = staged ? find_staged(scols, e - b, p_col[q], b) : find_col(ap_col, b, e, p_col[q]);
                     if (pos < 0) atomicOr(status, kRefreshInvalid);
                     value = a_own * w;
                 }
-                ordered_add(value, pos, lane, ap);
+                ordered_add(value, pos, lane, ap, stage);
             }
         }
     }
@@ -163,13 +249,25 @@ __global__ void __launch_bounds__(32 * kWarpRows) k_c_rows(int nc, const int* __
                                                            const double* __restrict__ ap,
                                                            const int* __restrict__ c_off,
                                                            const int* __restrict__ c_col,
-                                                           double* __restrict__ cv, int* status) {
+                                                           double* __restrict__ cv, int splits, int* status) {
+    __shared__ double stage_all[kWarpRows][32];
+    __shared__ int cols_all[kWarpRows][kStageCols];
     const int lane = threadIdx.x & 31;
-    const int warps = gridDim.x * kWarpRows;
-    for (int c = blockIdx.x * kWarpRows + (threadIdx.x >> 5); c < nc; c += warps) {
-        const int b = c_off[c], e = c_off[c + 1];
-        for (int p = b + lane; p < e; p += 32) cv[p] = 0.0;
+    double* stage = stage_all[threadIdx.x >> 5];
+    int* scols = cols_all[threadIdx.x >> 5];
+    const int64_t units = static_cast<int64_t>(nc) * splits;
+    const int64_t warps = static_cast<int64_t>(gridDim.x) * kWarpRows;
+    for (int64_t u = static_cast<int64_t>(blockIdx.x) * kWarpRows + (threadIdx.x >> 5); u < units; u += warps) {
+        const int c = static_cast<int>(u / splits);
+        const RowSlice sl = row_slice(c_col, c_off[c], c_off[c + 1], static_cast<int>(u % splits), splits);
+        const int b = sl.lo, e = sl.hi;
+        const bool staged = e - b <= kStageCols;
+        for (int p = b + lane; p < e; p += 32) {
+            cv[p] = 0.0;
+            if (staged) scols[p - b] = c_col[p];
+        }
         __syncwarp();
+        if (b == e) continue;
         for (int tb = t_off[c]; tb < t_off[c + 1]; tb += 32) {
             const int t = tb + lane;
             int len = 0, pb = 0;
@@ -178,18 +276,19 @@ __global__ void __launch_bounds__(32 * kWarpRows) k_c_rows(int nc, const int* __
                 const int i = t_row[t];
                 weight = p_val[p_off[i] + t_pos[t]];
                 pb = ap_off[i];
-                len = ap_off[i + 1] - pb;
+                int pe = ap_off[i + 1];
+                if (splits > 1) {
+                    pb = lower_bound_col(ap_col, pb, pe, sl.col_lo);
+                    pe = lower_bound_col(ap_col, pb, pe, sl.col_hi);
+                }
+                len = pe - pb;
             }
             int total;
             const int start = warp_exclusive_scan(len, lane, &total);
+            const int end = start + len;
             for (int s0 = 0; s0 < total; s0 += 32) {
                 const int s = s0 + lane;
-                int own = 0;
-                for (int l = 0; l < 32; ++l) {
-                    const int st = __shfl_sync(0xffffffffu, start, l);
-                    const int ln = __shfl_sync(0xffffffffu, len, l);
-                    if (ln > 0 && st <= s) own = l;
-                }
+                const int own = segment_owner(end, s < total ? s : total - 1);
                 const double w_own = __shfl_sync(0xffffffffu, weight, own);
                 const int pb_own = __shfl_sync(0xffffffffu, pb, own);
                 const int st_own = __shfl_sync(0xffffffffu, start, own);
@@ -197,14 +296,28 @@ __global__ void __launch_bounds__(32 * kWarpRows) k_c_rows(int nc, const int* __
                 int pos = -1;
                 if (s < total) {
                     const int p = pb_own + (s - st_own);
-                    pos = find_col(c_col, b, e, ap_col[p]);
+                    pos = staged ? find_staged(scols, e - b, ap_col[p], b) : find_col(c_col, b, e, ap_col[p]);
                     if (pos < 0) atomicOr(status, kRefreshInvalid);
                     value = w_own * ap[p];
                 }
-                ordered_add(value, pos, lane, cv);
+                ordered_add(value, pos, lane, cv, stage);
             }
         }
     }
+}
+
+// Splits per output row: enough warps to fill the GPU twice over on levels
+// with few rows, each owning at least 64 output entries.
+int choose_splits(int64_t rows, int64_t entries) {
+    if (rows <= 0) return 1;
+    const int64_t want = (2 * 148 * 48 + rows - 1) / rows;
+    const int64_t cap = std::max<int64_t>(1, entries / (rows * 64));
+    return static_cast<int>(std::max<int64_t>(1, std::min<int64_t>({want, cap, 64})));
+}
+
+int galerkin_grid(int64_t rows, int splits) {
+    const int64_t units = rows * splits;
+    return static_cast<int>(std::max<int64_t>(1, std::min<int64_t>((units + kWarpRows - 1) / kWarpRows, 148 * 32)));
 }
 
 // numeric_into_existing: keep |v| > 1e-30 at the existing positions; the kept
@@ -244,21 +357,32 @@ __device__ __forceinline__ void atomic_max_nonneg(double* addr, double v) {
     atomicMax(reinterpret_cast<unsigned long long*>(addr), static_cast<unsigned long long>(__double_as_longlong(v)));
 }
 
-__global__ void k_gershgorin(int n, const int* __restrict__ ro, const int* __restrict__ co,
-                             const double* __restrict__ va, const double* __restrict__ inv, double* bound) {
+// sqrt(1 / inv_i) per row, formed once (the host forms the same value per
+// entry); a non-positive or non-finite inverse diagonal or diagonal makes the
+// bound +inf (every row's diagonal entry references its own inverse)
+__global__ void k_sqrt_diagonal(int n, const double* __restrict__ inv, double* __restrict__ sd, double* bound) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     const double inf = __longlong_as_double(0x7ff0000000000000LL);
     const double ii = inv[i];
-    if (!(ii > 0.0) || !isfinite(ii)) { atomic_max_nonneg(bound, inf); return; }
     const double di = 1.0 / ii;
-    if (!(di > 0.0) || !isfinite(di)) { atomic_max_nonneg(bound, inf); return; }
+    if (!(ii > 0.0) || !isfinite(ii) || !(di > 0.0) || !isfinite(di)) {
+        atomic_max_nonneg(bound, inf);
+        sd[i] = 0.0;
+        return;
+    }
+    sd[i] = sqrt(di);
+}
+
+__global__ void k_gershgorin(int n, const int* __restrict__ ro, const int* __restrict__ co,
+                             const double* __restrict__ va, const double* __restrict__ sd, double* bound) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const double inf = __longlong_as_double(0x7ff0000000000000LL);
+    const double si = sd[i];
     double row_sum = 0.0;
     for (int k = ro[i]; k < ro[i + 1]; ++k) {
-        const double ij = inv[co[k]];
-        const double dj = 1.0 / ij;
-        if (!(ij > 0.0) || !isfinite(ij) || !(dj > 0.0) || !isfinite(dj)) { atomic_max_nonneg(bound, inf); return; }
-        const double scale = sqrt(di) * sqrt(dj);
+        const double scale = si * sd[co[k]];
         if (!(scale > 0.0) || !isfinite(scale)) { atomic_max_nonneg(bound, inf); return; }
         row_sum += fabs(va[k]) / scale;
     }
@@ -461,35 +585,49 @@ int key_bits(int64_t rows) {
     return 32 + b;
 }
 
-template <class T>
-void exclusive_sum(cudaStream_t s, const T* in, T* out, int64_t n) {
-    std::size_t bytes = 0;
-    CFDXG_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, bytes, in, out, n, s));
-    DevBuf<unsigned char> tmp(std::max<std::size_t>(bytes, 1));
-    CFDXG_CUDA(cub::DeviceScan::ExclusiveSum(tmp.get(), bytes, in, out, n, s));
+double wall_seconds() {
+    return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
 }
 
-// sorted unique keys of `keys` (m entries, begin/end bits) into out; returns their count
-int64_t sort_unique(cudaStream_t s, DevBuf<unsigned long long>& keys, int64_t m, int end_bit,
-                    DevBuf<unsigned long long>& out) {
-    DevBuf<unsigned long long> sorted(std::max<int64_t>(m, 1));
+// grow-only scratch: reallocated only when a level needs more, then with a
+// quarter of headroom (the expansions grow for several levels)
+template <class T>
+T* grow(DevBuf<T>& b, int64_t n) {
+    if (static_cast<int64_t>(b.size()) < std::max<int64_t>(n, 1)) {
+        static const bool profile = std::getenv("CFDXG_SETUP_PROFILE") != nullptr;
+        const double t0 = profile ? wall_seconds() : 0.0;
+        b.release();
+        b.resize(static_cast<std::size_t>(std::max<int64_t>(n + n / 4, 1)));
+        if (profile)
+            std::fprintf(stderr, "[cfdxg setup]       scratch grown to %.1f MB in %.3fs\n",
+                         static_cast<double>(b.size() * sizeof(T)) / 1e6, wall_seconds() - t0);
+    }
+    return b.get();
+}
+
+template <class T>
+void exclusive_sum(cudaStream_t s, const T* in, T* out, int64_t n, DevBuf<unsigned char>& temp) {
     std::size_t bytes = 0;
-    CFDXG_CUDA(cub::DeviceRadixSort::SortKeys(nullptr, bytes, keys.get(), sorted.get(), m, 0, end_bit, s));
-    {
-        DevBuf<unsigned char> tmp(std::max<std::size_t>(bytes, 1));
-        CFDXG_CUDA(cub::DeviceRadixSort::SortKeys(tmp.get(), bytes, keys.get(), sorted.get(), m, 0, end_bit, s));
-    }
-    keys.release();
-    out.resize(static_cast<std::size_t>(std::max<int64_t>(m, 1)));
-    DevBuf<int64_t> count(1);
+    CFDXG_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, bytes, in, out, n, s));
+    CFDXG_CUDA(cub::DeviceScan::ExclusiveSum(grow(temp, static_cast<int64_t>(bytes)), bytes, in, out, n, s));
+}
+
+// sorted unique keys of keys[0, m) (bits [0, end_bit)) into out; returns their count
+int64_t sort_unique(cudaStream_t s, const unsigned long long* keys, int64_t m, int end_bit,
+                    DevBuf<unsigned long long>& sorted, DevBuf<unsigned long long>& out, DevBuf<int64_t>& count,
+                    DevBuf<unsigned char>& temp) {
+    std::size_t bytes = 0;
+    unsigned long long* so = grow(sorted, m);
+    CFDXG_CUDA(cub::DeviceRadixSort::SortKeys(nullptr, bytes, keys, so, m, 0, end_bit, s));
+    CFDXG_CUDA(cub::DeviceRadixSort::SortKeys(grow(temp, static_cast<int64_t>(bytes)), bytes, keys, so, m, 0,
+                                              end_bit, s));
+    unsigned long long* uo = grow(out, m);
+    int64_t* c = grow(count, 1);
     bytes = 0;
-    CFDXG_CUDA(cub::DeviceSelect::Unique(nullptr, bytes, sorted.get(), out.get(), count.get(), m, s));
-    {
-        DevBuf<unsigned char> tmp(std::max<std::size_t>(bytes, 1));
-        CFDXG_CUDA(cub::DeviceSelect::Unique(tmp.get(), bytes, sorted.get(), out.get(), count.get(), m, s));
-    }
+    CFDXG_CUDA(cub::DeviceSelect::Unique(nullptr, bytes, so, uo, c, m, s));
+    CFDXG_CUDA(cub::DeviceSelect::Unique(grow(temp, static_cast<int64_t>(bytes)), bytes, so, uo, c, m, s));
     int64_t h = 0;
-    CFDXG_CUDA(cudaMemcpyAsync(&h, count.get(), sizeof(int64_t), cudaMemcpyDeviceToHost, s));
+    CFDXG_CUDA(cudaMemcpyAsync(&h, c, sizeof(int64_t), cudaMemcpyDeviceToHost, s));
     CFDXG_CUDA(cudaStreamSynchronize(s));
     return h;
 }
@@ -497,27 +635,61 @@ int64_t sort_unique(cudaStream_t s, DevBuf<unsigned long long>& keys, int64_t m,
 // CSR (off: rows + 1, col) of sorted unique (row << 32 | col) keys: counts[r + 1]
 // = row r's length, and their inclusive sum is off
 void keys_to_csr(cfdxg_context* ctx, const unsigned long long* keys, int64_t m, int rows, DevBuf<int>& off,
-                 DevBuf<int>& col) {
+                 DevBuf<int>& col, DevBuf<int>& counts, DevBuf<unsigned char>& temp) {
     cudaStream_t s = ctx->stream;
-    DevBuf<int> counts(static_cast<std::size_t>(rows) + 1);
-    counts.zero(s);
+    int* cnt = grow(counts, static_cast<int64_t>(rows) + 1);
+    CFDXG_CUDA(cudaMemsetAsync(cnt, 0, sizeof(int) * (static_cast<std::size_t>(rows) + 1), s));
     col.resize(static_cast<std::size_t>(std::max<int64_t>(m, 1)));
     if (m > 0) {
-        k_key_rows<<<blocks_for(m, kT), kT, 0, s>>>(m, keys, counts.get(), col.get());
+        k_key_rows<<<blocks_for(m, kT), kT, 0, s>>>(m, keys, cnt, col.get());
         check_launch(ctx);
     }
     off.resize(static_cast<std::size_t>(rows) + 1);
     std::size_t bytes = 0;
-    CFDXG_CUDA(cub::DeviceScan::InclusiveSum(nullptr, bytes, counts.get(), off.get(), rows + 1, s));
-    DevBuf<unsigned char> tmp(std::max<std::size_t>(bytes, 1));
-    CFDXG_CUDA(cub::DeviceScan::InclusiveSum(tmp.get(), bytes, counts.get(), off.get(), rows + 1, s));
-    CFDXG_CUDA(cudaStreamSynchronize(s));
+    CFDXG_CUDA(cub::DeviceScan::InclusiveSum(nullptr, bytes, cnt, off.get(), rows + 1, s));
+    CFDXG_CUDA(cub::DeviceScan::InclusiveSum(grow(temp, static_cast<int64_t>(bytes)), bytes, cnt, off.get(),
+                                             rows + 1, s));
 }
 
 }  // namespace
 
 DeviceGalerkin::DeviceGalerkin(cfdxg_context* ctx, const cfdxg_matrix* A)
     : ctx_(ctx), A_(A), R_(std::make_unique<DevRefresh>()) {}
+
+DeviceGalerkin::~DeviceGalerkin() {
+    for (int k = 0; k < 2; ++k) {
+        if (stage_[k]) cudaFreeHost(stage_[k]);
+        if (staged_[k]) cudaEventDestroy(staged_[k]);
+    }
+}
+
+// Device-to-host copy through two fixed pinned chunks: the next chunk's
+// transfer runs while the host copies the previous one out.
+void DeviceGalerkin::download(const void* src, void* dst, std::size_t bytes) {
+    cudaStream_t s = ctx_->stream;
+    if (!stage_[0]) {
+        for (int k = 0; k < 2; ++k) {
+            CFDXG_CUDA(cudaHostAlloc(&stage_[k], kStageBytes, cudaHostAllocDefault));
+            CFDXG_CUDA(cudaEventCreateWithFlags(&staged_[k], cudaEventDisableTiming));
+        }
+    }
+    const char* from = static_cast<const char*>(src);
+    char* to = static_cast<char*>(dst);
+    const std::size_t chunks = (bytes + kStageBytes - 1) / kStageBytes;
+    for (std::size_t c = 0; c <= chunks; ++c) {
+        if (c < chunks) {
+            const std::size_t len = std::min(kStageBytes, bytes - c * kStageBytes);
+            CFDXG_CUDA(cudaMemcpyAsync(stage_[c & 1], from + c * kStageBytes, len, cudaMemcpyDeviceToHost, s));
+            CFDXG_CUDA(cudaEventRecord(staged_[c & 1], s));
+        }
+        if (c > 0) {
+            const std::size_t p = c - 1;
+            const std::size_t len = std::min(kStageBytes, bytes - p * kStageBytes);
+            CFDXG_CUDA(cudaEventSynchronize(staged_[p & 1]));
+            std::memcpy(to + p * kStageBytes, stage_[p & 1], len);
+        }
+    }
+}
 
 bool DeviceGalerkin::operator()(int level, const HostCsr& A, const AmgLevel& P, int64_t coarse_n,
                                 HostCsr& coarse) {
@@ -553,97 +725,106 @@ bool DeviceGalerkin::operator()(int level, const HostCsr& A, const AmgLevel& P, 
     clear_status(ctx_);
     int* st = ctx_->scratch.status;
 
+    // per-phase device times with CFDXG_SETUP_PROFILE (synchronising)
+    static const bool profile = std::getenv("CFDXG_SETUP_PROFILE") != nullptr;
+    double tp = wall_seconds();
+    auto phase = [&](const char* what) {
+        if (!profile) return;
+        CFDXG_CUDA(cudaStreamSynchronize(s));
+        const double t = wall_seconds();
+        std::fprintf(stderr, "[cfdxg setup]     device %s %.3fs\n", what, t - tp);
+        tp = t;
+    };
     // P^T adjacency, stable: (column, fine row) keys sorted, positions alongside
     {
-        DevBuf<unsigned long long> keys(std::max<int64_t>(pn, 1)), sorted(std::max<int64_t>(pn, 1));
-        DevBuf<int> pos(std::max<int64_t>(pn, 1));
+        unsigned long long* keys = grow(keys_, pn);
+        unsigned long long* sorted = grow(sorted_, pn);
+        int* pos = grow(ints_, pn);
         F.t_pos.resize(std::max<int64_t>(pn, 1));
-        k_pt_keys<<<blocks_for(n, kT), kT, 0, s>>>(static_cast<int>(n), F.p_off.get(), F.p_col.get(), keys.get(),
-                                                  pos.get());
+        k_pt_keys<<<blocks_for(n, kT), kT, 0, s>>>(static_cast<int>(n), F.p_off.get(), F.p_col.get(), keys, pos);
         check_launch(ctx_);
         std::size_t bytes = 0;
         const int end_bit = key_bits(coarse_n);
-        CFDXG_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, bytes, keys.get(), sorted.get(), pos.get(),
-                                                   F.t_pos.get(), pn, 0, end_bit, s));
-        {
-            DevBuf<unsigned char> tmp(std::max<std::size_t>(bytes, 1));
-            CFDXG_CUDA(cub::DeviceRadixSort::SortPairs(tmp.get(), bytes, keys.get(), sorted.get(), pos.get(),
-                                                       F.t_pos.get(), pn, 0, end_bit, s));
-        }
-        keys_to_csr(ctx_, sorted.get(), pn, nc, F.t_off, F.t_row);   // rows: coarse columns; cols: fine rows
+        CFDXG_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, bytes, keys, sorted, pos, F.t_pos.get(), pn, 0, end_bit,
+                                                   s));
+        CFDXG_CUDA(cub::DeviceRadixSort::SortPairs(grow(temp_, static_cast<int64_t>(bytes)), bytes, keys, sorted,
+                                                   pos, F.t_pos.get(), pn, 0, end_bit, s));
+        keys_to_csr(ctx_, sorted, pn, nc, F.t_off, F.t_row, counts_, temp_);   // rows: coarse columns
     }
+    phase("P^T adjacency");
     // symbolic AP: every (i, p_col[q]) for k in A's row i and q in P's row co[k]
     {
-        DevBuf<int64_t> len(nnz + 1), eoff(nnz + 1);
-        CFDXG_CUDA(cudaMemsetAsync(len.get() + nnz, 0, sizeof(int64_t), s));
-        k_ap_expand_len<<<blocks_for(nnz, kT), kT, 0, s>>>(nnz, F.co.get(), F.p_off.get(), len.get());
+        int64_t* len = grow(len_, nnz + 1);
+        int64_t* eoff = grow(eoff_, nnz + 1);
+        CFDXG_CUDA(cudaMemsetAsync(len + nnz, 0, sizeof(int64_t), s));
+        k_ap_expand_len<<<blocks_for(nnz, kT), kT, 0, s>>>(nnz, F.co.get(), F.p_off.get(), len);
         check_launch(ctx_);
-        exclusive_sum<int64_t>(s, len.get(), eoff.get(), nnz + 1);
+        exclusive_sum<int64_t>(s, len, eoff, nnz + 1, temp_);
         int64_t m = 0;
-        CFDXG_CUDA(cudaMemcpyAsync(&m, eoff.get() + nnz, sizeof(int64_t), cudaMemcpyDeviceToHost, s));
+        CFDXG_CUDA(cudaMemcpyAsync(&m, eoff + nnz, sizeof(int64_t), cudaMemcpyDeviceToHost, s));
         CFDXG_CUDA(cudaStreamSynchronize(s));
-        DevBuf<unsigned long long> keys(std::max<int64_t>(m, 1)), uniq;
+        unsigned long long* keys = grow(keys_, m);
         k_ap_expand<<<blocks_for(nnz, kT), kT, 0, s>>>(nnz, static_cast<int>(n), F.ro.get(), F.co.get(),
-                                                      F.p_off.get(), F.p_col.get(), eoff.get(), keys.get());
+                                                      F.p_off.get(), F.p_col.get(), eoff, keys);
         check_launch(ctx_);
-        len.release();
-        eoff.release();
-        const int64_t u = sort_unique(s, keys, m, key_bits(n), uniq);
+        const int64_t u = sort_unique(s, keys, m, key_bits(n), sorted_, uniq_, count_, temp_);
         if (u > std::numeric_limits<int>::max()) return false;
-        keys_to_csr(ctx_, uniq.get(), u, static_cast<int>(n), F.ap_off, F.ap_col);
+        keys_to_csr(ctx_, uniq_.get(), u, static_cast<int>(n), F.ap_off, F.ap_col, counts_, temp_);
         F.ap.resize(static_cast<std::size_t>(std::max<int64_t>(u, 1)));
     }
+    phase("AP graph");
     // numeric AP
     {
-        const int grid = static_cast<int>(std::min<int64_t>((n + kWarpRows - 1) / kWarpRows, 148 * 32));
-        k_ap_rows<<<std::max(grid, 1), 32 * kWarpRows, 0, s>>>(static_cast<int>(n), F.ro.get(), F.co.get(),
-                                                               F.va.get(), F.p_off.get(), F.p_col.get(),
-                                                               F.p_val.get(), F.ap_off.get(), F.ap_col.get(),
-                                                               F.ap.get(), st);
+        const int splits = choose_splits(n, static_cast<int64_t>(F.ap.size()));
+        k_ap_rows<<<galerkin_grid(n, splits), 32 * kWarpRows, 0, s>>>(
+            static_cast<int>(n), F.ro.get(), F.co.get(), F.va.get(), F.p_off.get(), F.p_col.get(), F.p_val.get(),
+            F.ap_off.get(), F.ap_col.get(), F.ap.get(), splits, st);
         check_launch(ctx_);
     }
+    phase("AP values");
     // symbolic C = P^T (AP): every (c, ap_col[p]) for t in P^T's row c and p in AP's row t_row[t]
     int64_t cm = 0;
     {
-        DevBuf<int64_t> len(pn + 1), eoff(pn + 1);
-        CFDXG_CUDA(cudaMemsetAsync(len.get() + pn, 0, sizeof(int64_t), s));
+        int64_t* len = grow(len_, pn + 1);
+        int64_t* eoff = grow(eoff_, pn + 1);
+        CFDXG_CUDA(cudaMemsetAsync(len + pn, 0, sizeof(int64_t), s));
         k_c_expand_len<<<blocks_for(std::max<int64_t>(pn, 1), kT), kT, 0, s>>>(pn, F.t_row.get(), F.ap_off.get(),
-                                                                             len.get());
+                                                                             len);
         check_launch(ctx_);
-        exclusive_sum<int64_t>(s, len.get(), eoff.get(), pn + 1);
+        exclusive_sum<int64_t>(s, len, eoff, pn + 1, temp_);
         int64_t m = 0;
-        CFDXG_CUDA(cudaMemcpyAsync(&m, eoff.get() + pn, sizeof(int64_t), cudaMemcpyDeviceToHost, s));
+        CFDXG_CUDA(cudaMemcpyAsync(&m, eoff + pn, sizeof(int64_t), cudaMemcpyDeviceToHost, s));
         CFDXG_CUDA(cudaStreamSynchronize(s));
-        DevBuf<unsigned long long> keys(std::max<int64_t>(m, 1)), uniq;
+        unsigned long long* keys = grow(keys_, m);
         k_c_expand<<<blocks_for(std::max<int64_t>(pn, 1), kT), kT, 0, s>>>(pn, nc, F.t_off.get(), F.t_row.get(),
-                                                                         F.ap_off.get(), F.ap_col.get(),
-                                                                         eoff.get(), keys.get());
+                                                                         F.ap_off.get(), F.ap_col.get(), eoff,
+                                                                         keys);
         check_launch(ctx_);
-        len.release();
-        eoff.release();
-        cm = sort_unique(s, keys, m, key_bits(coarse_n), uniq);
+        cm = sort_unique(s, keys, m, key_bits(coarse_n), sorted_, uniq_, count_, temp_);
         if (cm > std::numeric_limits<int>::max()) return false;
-        keys_to_csr(ctx_, uniq.get(), cm, nc, F.c_off, F.c_col);
+        keys_to_csr(ctx_, uniq_.get(), cm, nc, F.c_off, F.c_col, counts_, temp_);
         F.cv.resize(static_cast<std::size_t>(std::max<int64_t>(cm, 1)));
     }
+    phase("C graph");
     // numeric C
     {
-        const int grid = static_cast<int>(std::min<int64_t>((coarse_n + kWarpRows - 1) / kWarpRows, 148 * 32));
-        k_c_rows<<<std::max(grid, 1), 32 * kWarpRows, 0, s>>>(nc, F.t_off.get(), F.t_row.get(), F.t_pos.get(),
-                                                              F.p_off.get(), F.p_val.get(), F.ap_off.get(),
-                                                              F.ap_col.get(), F.ap.get(), F.c_off.get(),
-                                                              F.c_col.get(), F.cv.get(), st);
+        const int splits = choose_splits(coarse_n, cm);
+        k_c_rows<<<galerkin_grid(coarse_n, splits), 32 * kWarpRows, 0, s>>>(
+            nc, F.t_off.get(), F.t_row.get(), F.t_pos.get(), F.p_off.get(), F.p_val.get(), F.ap_off.get(),
+            F.ap_col.get(), F.ap.get(), F.c_off.get(), F.c_col.get(), F.cv.get(), splits, st);
         check_launch(ctx_);
     }
+    phase("C values");
     // pruning into the next level's CSR (device) and the refresh's keep positions
     DevRefreshLevel& C = R_->L[level + 1];
     {
-        DevBuf<int> flags(cm + 1), slot(cm + 1);
-        k_prune_flags<<<blocks_for(cm + 1, kT), kT, 0, s>>>(cm, F.cv.get(), flags.get());
+        int* flags = grow(ints_, cm + 1);
+        int* slot = grow(ints2_, cm + 1);
+        k_prune_flags<<<blocks_for(cm + 1, kT), kT, 0, s>>>(cm, F.cv.get(), flags);
         check_launch(ctx_);
-        exclusive_sum<int>(s, flags.get(), slot.get(), cm + 1);
+        exclusive_sum<int>(s, flags, slot, cm + 1, temp_);
         int kept = 0;
-        CFDXG_CUDA(cudaMemcpyAsync(&kept, slot.get() + cm, sizeof(int), cudaMemcpyDeviceToHost, s));
+        CFDXG_CUDA(cudaMemcpyAsync(&kept, slot + cm, sizeof(int), cudaMemcpyDeviceToHost, s));
         CFDXG_CUDA(cudaStreamSynchronize(s));
         C.n = nc;
         C.nnz = kept;
@@ -652,27 +833,27 @@ bool DeviceGalerkin::operator()(int level, const HostCsr& A, const AmgLevel& P, 
         C.va.resize(static_cast<std::size_t>(std::max(kept, 1)));
         F.keep_pos.resize(static_cast<std::size_t>(std::max<int64_t>(cm, 1)));
         if (cm > 0) {
-            k_prune_scatter<<<blocks_for(cm, kT), kT, 0, s>>>(cm, F.c_col.get(), F.cv.get(), flags.get(), slot.get(),
+            k_prune_scatter<<<blocks_for(cm, kT), kT, 0, s>>>(cm, F.c_col.get(), F.cv.get(), flags, slot,
                                                              F.keep_pos.get(), C.co.get(), C.va.get());
             check_launch(ctx_);
         }
-        k_pruned_offsets<<<blocks_for(nc + 1, kT), kT, 0, s>>>(nc, F.c_off.get(), slot.get(), C.ro.get());
+        k_pruned_offsets<<<blocks_for(nc + 1, kT), kT, 0, s>>>(nc, F.c_off.get(), slot, C.ro.get());
         check_launch(ctx_);
     }
     if (read_status(ctx_) & kRefreshInvalid) return false;   // synchronises
+    phase("pruning");
     // the coarse operator back to the host for the next level's C/F splitting
+    // (the offsets and columns are non-negative, so their int bits are the
+    // uint32 values)
     coarse.n = coarse_n;
-    std::vector<int> ro(static_cast<std::size_t>(nc) + 1), co(static_cast<std::size_t>(C.nnz));
+    coarse.ro.resize(static_cast<std::size_t>(nc) + 1);
+    coarse.co.resize(static_cast<std::size_t>(C.nnz));
     coarse.va.resize(static_cast<std::size_t>(C.nnz));
-    CFDXG_CUDA(cudaMemcpyAsync(ro.data(), C.ro.get(), sizeof(int) * (nc + 1), cudaMemcpyDeviceToHost, s));
-    if (C.nnz > 0) {
-        CFDXG_CUDA(cudaMemcpyAsync(co.data(), C.co.get(), sizeof(int) * C.nnz, cudaMemcpyDeviceToHost, s));
-        CFDXG_CUDA(cudaMemcpyAsync(coarse.va.data(), C.va.get(), sizeof(double) * C.nnz, cudaMemcpyDeviceToHost, s));
-    }
-    CFDXG_CUDA(cudaStreamSynchronize(s));
-    coarse.ro.assign(ro.begin(), ro.end());
-    coarse.co.assign(co.begin(), co.end());
+    download(C.ro.get(), coarse.ro.data(), sizeof(int) * (static_cast<std::size_t>(nc) + 1));
+    download(C.co.get(), coarse.co.data(), sizeof(int) * static_cast<std::size_t>(C.nnz));
+    download(C.va.get(), coarse.va.data(), sizeof(double) * static_cast<std::size_t>(C.nnz));
     C.inv_diag.resize(static_cast<std::size_t>(nc));
+    phase("download");
     return true;
 }
 
@@ -699,6 +880,16 @@ bool amg_refresh_device(cfdxg_context* ctx, cfdxg_amg* amg, const cfdxg_matrix* 
     DevRefresh& R = *amg->refresh;
     cudaStream_t s = ctx->stream;
     const std::size_t nl = R.L.size();
+    // per-phase times with CFDXG_SETUP_PROFILE (synchronising)
+    static const bool profile = std::getenv("CFDXG_SETUP_PROFILE") != nullptr;
+    double tp = wall_seconds();
+    auto phase = [&](const char* what) {
+        if (!profile) return;
+        CFDXG_CUDA(cudaStreamSynchronize(s));
+        const double t = wall_seconds();
+        std::fprintf(stderr, "[cfdxg refresh] %s %.4fs\n", what, t - tp);
+        tp = t;
+    };
     clear_status(ctx);
     int* st = ctx->scratch.status;
     // staged: level values land in R (the device hierarchies are untouched until commit)
@@ -709,19 +900,18 @@ bool amg_refresh_device(cfdxg_context* ctx, cfdxg_amg* amg, const cfdxg_matrix* 
             DevRefreshLevel& F = R.L[l - 1];
             {
                 ProfScope ps(ctx, "refresh_galerkin_ap", 0.0);
-                const int grid = std::min<int64_t>((F.n + kWarpRows - 1) / kWarpRows, 148 * 32);
-                k_ap_rows<<<grid, 32 * kWarpRows, 0, s>>>(F.n, F.ro.get(), F.co.get(), F.va.get(), F.p_off.get(),
-                                                          F.p_col.get(), F.p_val.get(), F.ap_off.get(),
-                                                          F.ap_col.get(), F.ap.get(), st);
+                const int splits = choose_splits(F.n, static_cast<int64_t>(F.ap.size()));
+                k_ap_rows<<<galerkin_grid(F.n, splits), 32 * kWarpRows, 0, s>>>(
+                    F.n, F.ro.get(), F.co.get(), F.va.get(), F.p_off.get(), F.p_col.get(), F.p_val.get(),
+                    F.ap_off.get(), F.ap_col.get(), F.ap.get(), splits, st);
                 check_launch(ctx);
             }
             {
                 ProfScope ps(ctx, "refresh_galerkin_c", 0.0);
-                const int grid = std::min<int64_t>((F.n_coarse + kWarpRows - 1) / kWarpRows, 148 * 32);
-                k_c_rows<<<grid, 32 * kWarpRows, 0, s>>>(F.n_coarse, F.t_off.get(), F.t_row.get(), F.t_pos.get(),
-                                                         F.p_off.get(), F.p_val.get(), F.ap_off.get(),
-                                                         F.ap_col.get(), F.ap.get(), F.c_off.get(), F.c_col.get(),
-                                                         F.cv.get(), st);
+                const int splits = choose_splits(F.n_coarse, static_cast<int64_t>(F.cv.size()));
+                k_c_rows<<<galerkin_grid(F.n_coarse, splits), 32 * kWarpRows, 0, s>>>(
+                    F.n_coarse, F.t_off.get(), F.t_row.get(), F.t_pos.get(), F.p_off.get(), F.p_val.get(),
+                    F.ap_off.get(), F.ap_col.get(), F.ap.get(), F.c_off.get(), F.c_col.get(), F.cv.get(), splits, st);
                 check_launch(ctx);
             }
             const int64_t entries = static_cast<int64_t>(F.cv.size());
@@ -732,17 +922,26 @@ bool amg_refresh_device(cfdxg_context* ctx, cfdxg_amg* amg, const cfdxg_matrix* 
                                                               L.inv_diag.get(), st);
         check_launch(ctx);
     }
+    phase("Galerkin products and diagonals");
     R.bounds.zero(s);
-    ProfScope ps_bounds(ctx, "refresh_gershgorin", 0.0);
-    for (std::size_t l = 0; l < nl; ++l) {
-        DevRefreshLevel& L = R.L[l];
-        k_gershgorin<<<blocks_for(L.n, kT), kT, 0, s>>>(L.n, L.ro.get(), L.co.get(), L.va.get(), L.inv_diag.get(),
-                                                        R.bounds.get() + l);
-        check_launch(ctx);
+    {
+        ProfScope ps_bounds(ctx, "refresh_gershgorin", 0.0);
+        int64_t most = 0;
+        for (std::size_t l = 0; l < nl; ++l) most = std::max<int64_t>(most, R.L[l].n);
+        if (static_cast<int64_t>(R.sqrt_diag.size()) < most) R.sqrt_diag.resize(static_cast<std::size_t>(most));
+        for (std::size_t l = 0; l < nl; ++l) {
+            DevRefreshLevel& L = R.L[l];
+            k_sqrt_diagonal<<<blocks_for(L.n, kT), kT, 0, s>>>(L.n, L.inv_diag.get(), R.sqrt_diag.get(),
+                                                               R.bounds.get() + l);
+            k_gershgorin<<<blocks_for(L.n, kT), kT, 0, s>>>(L.n, L.ro.get(), L.co.get(), L.va.get(),
+                                                            R.sqrt_diag.get(), R.bounds.get() + l);
+            check_launch(ctx);
+        }
     }
     std::vector<double> bounds(nl);
     R.bounds.download(bounds.data(), s);
     const int status = read_status(ctx);   // synchronises the stream
+    phase("damping bounds");
     if (status & kRefreshPattern) {
         error = "native AMG numeric update failed: the pruned coarse pattern changed";
         return false;
@@ -776,6 +975,7 @@ bool amg_refresh_device(cfdxg_context* ctx, cfdxg_amg* amg, const cfdxg_matrix* 
         if (amg->d64) set_hierarchy_values_device<double>(ctx, *amg->d64, R, omega);
         if (amg->d32) set_hierarchy_values_device<float>(ctx, *amg->d32, R, omega);
     }
+    phase("commit");
     h.omega = omega;
     amg->host_values_stale = true;
     return true;

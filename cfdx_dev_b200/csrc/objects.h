@@ -56,6 +56,10 @@ struct DevHierarchy {
     DevBuf<float> dense;       // mode 2: the n*n inverse (row-major), formed in FP64, stored FP32
     DevBuf<double> dense64;    // mode 2 with dense_fp64: the same inverse stored FP64
     bool dense_fp64 = false;
+    // the dense inverse's LU solver handle and work arrays, kept for refreshes
+    std::shared_ptr<void> solver;
+    DevBuf<double> lu_a, lu_x, lu_work;
+    DevBuf<int> lu_ipiv, lu_info;
     // constant null space: the cycle's mean removals (in index order with
     // reference_order) and the bordered coarsest solve
     bool null_space = false;
@@ -128,6 +132,7 @@ struct DevRefreshLevel {
 struct DevRefresh {
     std::vector<DevRefreshLevel> L;
     DevBuf<double> bounds;                    // per-level normalised Gershgorin bound
+    DevBuf<double> sqrt_diag;                 // scratch: sqrt(1 / inv_diag) of one level
 };
 }  // namespace cfdxg
 
@@ -157,6 +162,9 @@ namespace cfdxg {
 class DeviceGalerkin {
 public:
     DeviceGalerkin(cfdxg_context* ctx, const cfdxg_matrix* A);
+    ~DeviceGalerkin();
+    DeviceGalerkin(const DeviceGalerkin&) = delete;
+    DeviceGalerkin& operator=(const DeviceGalerkin&) = delete;
     bool operator()(int level, const HostCsr& A, const AmgLevel& P, int64_t coarse_n, HostCsr& coarse);
     std::unique_ptr<DevRefresh> take(int levels);
 
@@ -164,6 +172,18 @@ private:
     cfdxg_context* ctx_;
     const cfdxg_matrix* A_;
     std::unique_ptr<DevRefresh> R_;
+    // grow-only scratch shared by the levels: expansion keys and their sorted
+    // and unique copies, per-entry lengths and offsets, integer flags, CUB
+    // temporaries
+    DevBuf<unsigned long long> keys_, sorted_, uniq_;
+    DevBuf<int64_t> len_, eoff_, count_;
+    DevBuf<int> ints_, ints2_, counts_;
+    DevBuf<unsigned char> temp_;
+    // two pinned chunks staging the coarse operators' downloads
+    static constexpr std::size_t kStageBytes = std::size_t{32} << 20;
+    void* stage_[2] = {nullptr, nullptr};
+    cudaEvent_t staged_[2] = {nullptr, nullptr};
+    void download(const void* src, void* dst, std::size_t bytes);
 };
 
 // numeric refresh of the hierarchy on the device (galerkin.cu): the

@@ -685,12 +685,13 @@ void build_dense_inverse_dev(cfdxg_context* ctx, DevHierarchy<T>& d, int n, cons
     const int N = n + (d.null_space ? 1 : 0);
     const std::size_t nn = static_cast<std::size_t>(n) * n;
     const std::size_t NN = static_cast<std::size_t>(N) * N;
-    DevBuf<double> at, x;
-    DevBuf<int> ipiv, info;
+    // the work arrays and the solver handle stay with the hierarchy for its refreshes
+    DevBuf<double>& at = d.lu_a;
+    DevBuf<double>& x = d.lu_x;
     at.resize(NN);
     x.resize(NN);
-    ipiv.resize(N);
-    info.resize(1);
+    d.lu_ipiv.resize(N);
+    d.lu_info.resize(1);
     if (d.dense_fp64) d.dense64.resize(nn);
     else d.dense.resize(nn);
     cudaStream_t s = ctx->stream;
@@ -699,18 +700,21 @@ void build_dense_inverse_dev(cfdxg_context* ctx, DevHierarchy<T>& d, int n, cons
     check_launch(ctx);
     k_identity<<<blocks_for(static_cast<int64_t>(NN), kT), kT, 0, s>>>(N, x.get());
     check_launch(ctx);
-    cusolverDnHandle_t h = nullptr;
-    if (cusolverDnCreate(&h) != CUSOLVER_STATUS_SUCCESS)
-        throw Error(CFDXG_ERR_CUDA, "cusolverDnCreate failed");
-    struct HandleGuard {
-        cusolverDnHandle_t h;
-        ~HandleGuard() { cusolverDnDestroy(h); }
-    } guard{h};
+    if (!d.solver) {
+        cusolverDnHandle_t created = nullptr;
+        if (cusolverDnCreate(&created) != CUSOLVER_STATUS_SUCCESS)
+            throw Error(CFDXG_ERR_CUDA, "cusolverDnCreate failed");
+        d.solver = std::shared_ptr<void>(created, [](void* p) { cusolverDnDestroy(static_cast<cusolverDnHandle_t>(p)); });
+    }
+    cusolverDnHandle_t h = static_cast<cusolverDnHandle_t>(d.solver.get());
     if (cusolverDnSetStream(h, s) != CUSOLVER_STATUS_SUCCESS) throw Error(CFDXG_ERR_CUDA, "cusolverDnSetStream failed");
     int lwork = 0;
     if (cusolverDnDgetrf_bufferSize(h, N, N, at.get(), N, &lwork) != CUSOLVER_STATUS_SUCCESS)
         throw Error(CFDXG_ERR_CUDA, "cusolverDnDgetrf_bufferSize failed");
-    DevBuf<double> work(static_cast<std::size_t>(std::max(lwork, 1)));
+    if (static_cast<int64_t>(d.lu_work.size()) < std::max(lwork, 1)) d.lu_work.resize(static_cast<std::size_t>(std::max(lwork, 1)));
+    DevBuf<double>& work = d.lu_work;
+    DevBuf<int>& ipiv = d.lu_ipiv;
+    DevBuf<int>& info = d.lu_info;
     // at holds A^T column-major: factor it, then solve A^T X = I
     if (cusolverDnDgetrf(h, N, N, at.get(), N, work.get(), ipiv.get(), info.get()) != CUSOLVER_STATUS_SUCCESS ||
         cusolverDnDgetrs(h, CUBLAS_OP_N, N, N, at.get(), N, ipiv.get(), x.get(), N, info.get()) !=
