@@ -306,12 +306,16 @@ __global__ void __launch_bounds__(32 * kWarpRows) k_c_rows(int nc, const int* __
     }
 }
 
-// Splits per output row: enough warps to fill the GPU twice over on levels
-// with few rows, each owning at least 64 output entries.
+// Splits per output row: slices of at most about 256 output entries (their
+// columns then always fit the shared-memory staging, and a row's stream is
+// shared among warps), and enough warps to fill the GPU twice over on levels
+// with few rows, each slice owning at least 32 entries.
 int choose_splits(int64_t rows, int64_t entries) {
     if (rows <= 0) return 1;
-    const int64_t want = (2 * 148 * 48 + rows - 1) / rows;
-    const int64_t cap = std::max<int64_t>(1, entries / (rows * 64));
+    const int64_t fill = (2 * 148 * 48 + rows - 1) / rows;
+    const int64_t length = entries / rows;
+    const int64_t want = std::max<int64_t>(fill, length / 256);
+    const int64_t cap = std::max<int64_t>(1, length / 32);
     return static_cast<int>(std::max<int64_t>(1, std::min<int64_t>({want, cap, 64})));
 }
 
@@ -388,6 +392,45 @@ __global__ void k_gershgorin(int n, const int* __restrict__ ro, const int* __res
     }
     if (!isfinite(row_sum)) { atomic_max_nonneg(bound, inf); return; }
     atomic_max_nonneg(bound, row_sum);
+}
+
+// The same bound with one warp per row, for levels with long rows: the lanes
+// form 32 terms at a time, and one lane adds them to the row sum in CSR
+// order, so the sum is the sequential one bit for bit.
+__global__ void k_gershgorin_warp(int n, const int* __restrict__ ro, const int* __restrict__ co,
+                                  const double* __restrict__ va, const double* __restrict__ sd, double* bound) {
+    __shared__ double terms_all[8][32];
+    const int lane = threadIdx.x & 31;
+    double* terms = terms_all[threadIdx.x >> 5];
+    const double inf = __longlong_as_double(0x7ff0000000000000LL);
+    const int warps = gridDim.x * 8;
+    for (int i = blockIdx.x * 8 + (threadIdx.x >> 5); i < n; i += warps) {
+        const double si = sd[i];
+        double row_sum = 0.0;
+        bool bad = false;
+        for (int kb = ro[i]; kb < ro[i + 1]; kb += 32) {
+            const int k = kb + lane;
+            double term = 0.0;
+            bool invalid = false;
+            if (k < ro[i + 1]) {
+                const double scale = si * sd[co[k]];
+                invalid = !(scale > 0.0) || !isfinite(scale);
+                term = fabs(va[k]) / scale;
+            }
+            if (__any_sync(0xffffffffu, invalid)) { bad = true; break; }
+            terms[lane] = term;
+            __syncwarp();
+            if (lane == 0) {
+                const int count = min(32, ro[i + 1] - kb);
+                for (int q = 0; q < count; ++q) row_sum += terms[q];
+            }
+            __syncwarp();
+        }
+        if (lane == 0) {
+            if (bad || !isfinite(row_sum)) atomic_max_nonneg(bound, inf);
+            else atomic_max_nonneg(bound, row_sum);
+        }
+    }
 }
 
 std::vector<int> as_int(const std::vector<uint32_t>& v) { return std::vector<int>(v.begin(), v.end()); }
@@ -933,8 +976,12 @@ bool amg_refresh_device(cfdxg_context* ctx, cfdxg_amg* amg, const cfdxg_matrix* 
             DevRefreshLevel& L = R.L[l];
             k_sqrt_diagonal<<<blocks_for(L.n, kT), kT, 0, s>>>(L.n, L.inv_diag.get(), R.sqrt_diag.get(),
                                                                R.bounds.get() + l);
-            k_gershgorin<<<blocks_for(L.n, kT), kT, 0, s>>>(L.n, L.ro.get(), L.co.get(), L.va.get(),
-                                                            R.sqrt_diag.get(), R.bounds.get() + l);
+            if (L.nnz >= 32 * static_cast<int64_t>(L.n))
+                k_gershgorin_warp<<<std::max(1, std::min(blocks_for(L.n, 8), 148 * 32)), 256, 0, s>>>(
+                    L.n, L.ro.get(), L.co.get(), L.va.get(), R.sqrt_diag.get(), R.bounds.get() + l);
+            else
+                k_gershgorin<<<blocks_for(L.n, kT), kT, 0, s>>>(L.n, L.ro.get(), L.co.get(), L.va.get(),
+                                                                R.sqrt_diag.get(), R.bounds.get() + l);
             check_launch(ctx);
         }
     }

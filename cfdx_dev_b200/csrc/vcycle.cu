@@ -868,6 +868,34 @@ __global__ void k_quantize_rows(int n, const int* __restrict__ ro, const double*
     for (int k = ro[i]; k < ro[i + 1]; ++k) vh[k] = __float2half_rn(static_cast<float>(va[k] / static_cast<double>(s)));
 }
 
+// The same quantisation with one warp per row, for levels with long rows (the
+// row maximum is order-free, each entry's rounding is independent).
+__global__ void k_quantize_rows_warp(int n, const int* __restrict__ ro, const double* __restrict__ va,
+                                     __half* __restrict__ vh, float* __restrict__ rscale) {
+    const int lane = threadIdx.x & 31;
+    const int warps = gridDim.x * (blockDim.x >> 5);
+    for (int i = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); i < n; i += warps) {
+        double m = 0.0;
+        for (int k = ro[i] + lane; k < ro[i + 1]; k += 32) m = fmax(m, fabs(va[k]));
+        for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+        const float sc = m > 0.0 ? static_cast<float>(m) : 1.0f;
+        if (lane == 0) rscale[i] = sc;
+        for (int k = ro[i] + lane; k < ro[i + 1]; k += 32)
+            vh[k] = __float2half_rn(static_cast<float>(va[k] / static_cast<double>(sc)));
+    }
+}
+
+// FP16 re-quantisation of a shared-row level from FP64 values (thread or warp per row)
+void quantize_level(cfdxg_context* ctx, int n, int64_t nnz, const int* ro, const double* va, __half* vh,
+                    float* rscale) {
+    if (nnz >= 32 * static_cast<int64_t>(n))
+        k_quantize_rows_warp<<<std::max(1, std::min(blocks_for(n, 8), 148 * 32)), 256, 0, ctx->stream>>>(
+            n, ro, va, vh, rscale);
+    else
+        k_quantize_rows<<<blocks_for(n, kT), kT, 0, ctx->stream>>>(n, ro, va, vh, rscale);
+    check_launch(ctx);
+}
+
 template <class T>
 __global__ void k_cast_values(int64_t n, const double* __restrict__ a, T* __restrict__ b) {
     const int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
@@ -957,9 +985,7 @@ void upload_level_device(cfdxg_context* ctx, DevLevel<T>& D, const AmgLevel& H, 
         if constexpr (std::is_same<T, float>::value) {
             D.vh.resize(static_cast<std::size_t>(std::max(D.nnz, 1)));
             D.rscale.resize(static_cast<std::size_t>(D.n));
-            k_quantize_rows<<<blocks_for(D.n, kT), kT, 0, s>>>(D.n, R.ro.get(), R.va.get(), D.vh.get(),
-                                                               D.rscale.get());
-            check_launch(ctx);
+            quantize_level(ctx, D.n, R.nnz, R.ro.get(), R.va.get(), D.vh.get(), D.rscale.get());
         }
         D.va.release();
     } else {
@@ -1046,17 +1072,16 @@ void set_hierarchy_values_device(cfdxg_context* ctx, DevHierarchy<T>& d, const D
     d.omega = static_cast<T>(omega);
     for (int l = 0; l < d.used; ++l) {
         if (d.L[l].half) {
-            if constexpr (std::is_same<T, float>::value) {
-                k_quantize_rows<<<blocks_for(d.L[l].n, kT), kT, 0, ctx->stream>>>(
-                    d.L[l].n, d.L[l].ro.get(), R.L[l].va.get(), d.L[l].vh.get(), d.L[l].rscale.get());
-                check_launch(ctx);
-            }
+            if constexpr (std::is_same<T, float>::value)
+                quantize_level(ctx, d.L[l].n, R.L[l].nnz, d.L[l].ro.get(), R.L[l].va.get(), d.L[l].vh.get(),
+                               d.L[l].rscale.get());
         } else {
             copy_or_cast<T>(ctx, R.L[l].va.get(), d.L[l].va.get(), R.L[l].nnz);
         }
         copy_or_cast<T>(ctx, R.L[l].inv_diag.get(), d.L[l].inv_diag.get(), R.L[l].n);
     }
     if (d.coarse_mode == 2) {
+        ProfScope ps(ctx, "refresh_dense_inverse", 0.0);
         const DevRefreshLevel& C = R.L[d.used - 1];
         build_dense_inverse_dev(ctx, d, C.n, C.ro.get(), C.co.get(), C.va.get());
     }
