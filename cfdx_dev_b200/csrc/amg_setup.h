@@ -14,17 +14,42 @@
 #pragma once
 #include <functional>
 #include <cstdint>
+#include <memory>
+#include <type_traits>
+#include <utility>
 #include <string>
 #include <vector>
 
 namespace cfdxg {
 
 // CSR with the reference's 32-bit index type (core/linalg/sparse_matrix.h:30).
+// Allocator whose resize() leaves new elements default-initialised (for
+// arithmetic types: unwritten), so that a large level filled by a copy right
+// after is touched once, not zero-filled first.
+template <class T>
+struct DefaultInitAllocator : std::allocator<T> {
+    template <class U>
+    struct rebind { using other = DefaultInitAllocator<U>; };
+    DefaultInitAllocator() = default;
+    template <class U>
+    DefaultInitAllocator(const DefaultInitAllocator<U>&) noexcept {}
+    template <class U>
+    void construct(U* p) noexcept(std::is_nothrow_default_constructible<U>::value) {
+        ::new (static_cast<void*>(p)) U;
+    }
+    template <class U, class... Args>
+    void construct(U* p, Args&&... args) {
+        ::new (static_cast<void*>(p)) U(std::forward<Args>(args)...);
+    }
+};
+template <class T>
+using HostVec = std::vector<T, DefaultInitAllocator<T>>;
+
 struct HostCsr {
     int64_t n = 0;
-    std::vector<uint32_t> ro;   // n + 1
-    std::vector<uint32_t> co;   // nnz, strictly increasing per row
-    std::vector<double> va;     // nnz
+    HostVec<uint32_t> ro;   // n + 1
+    HostVec<uint32_t> co;   // nnz, strictly increasing per row
+    HostVec<double> va;     // nnz
     int64_t nnz() const { return static_cast<int64_t>(co.size()); }
 };
 

@@ -329,12 +329,12 @@ extern "C" int cfdxg_matrix_create(cfdxg_context* ctx, int64_t n, const int64_t*
     std::vector<int> iro(n + 1), ico(nnz);
     for (int64_t i = 0; i <= n; ++i) { iro[i] = static_cast<int>(hro[i]); A->host.ro[i] = static_cast<uint32_t>(hro[i]); }
     for (int64_t k = 0; k < nnz; ++k) { ico[k] = static_cast<int>(hco[k]); A->host.co[k] = static_cast<uint32_t>(hco[k]); }
-    A->host.va = std::move(hva);
+    A->host.va.assign(hva.begin(), hva.end());
     A->host_values_valid = true;
     A->nnz = nnz;
     A->ro.upload(iro, ctx->stream);
     A->co.upload(ico, ctx->stream);
-    A->va.upload(A->host.va, ctx->stream);
+    A->va.upload(A->host.va.data(), A->host.va.size(), ctx->stream);
     CFDXG_CUDA(cudaStreamSynchronize(ctx->stream));
     *out = A.release();
     ctx->error.clear();

@@ -44,6 +44,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <limits>
+#include <thread>
 
 #include "objects.h"
 
@@ -433,7 +434,8 @@ __global__ void k_gershgorin_warp(int n, const int* __restrict__ ro, const int* 
     }
 }
 
-std::vector<int> as_int(const std::vector<uint32_t>& v) { return std::vector<int>(v.begin(), v.end()); }
+template <class V>
+std::vector<int> as_int(const V& v) { return std::vector<int>(v.begin(), v.end()); }
 
 void build_refresh(cfdxg_context* ctx, cfdxg_amg* amg) {
     const AmgHierarchy& h = amg->host;
@@ -706,6 +708,25 @@ DeviceGalerkin::~DeviceGalerkin() {
     }
 }
 
+// memcpy split over a few host threads (the destination is first touched
+// here, so its page faults are spread over the threads too)
+void parallel_memcpy(char* dst, const char* src, std::size_t len) {
+    constexpr std::size_t kPiece = std::size_t{4} << 20;
+    const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
+    const std::size_t pieces = std::min<std::size_t>(std::min<unsigned>(hw, 8u), (len + kPiece - 1) / kPiece);
+    if (pieces <= 1) {
+        std::memcpy(dst, src, len);
+        return;
+    }
+    std::vector<std::thread> pool;
+    pool.reserve(pieces);
+    for (std::size_t w = 0; w < pieces; ++w) {
+        const std::size_t b = len * w / pieces, e = len * (w + 1) / pieces;
+        pool.emplace_back([=] { std::memcpy(dst + b, src + b, e - b); });
+    }
+    for (auto& t : pool) t.join();
+}
+
 // Device-to-host copy through two fixed pinned chunks: the next chunk's
 // transfer runs while the host copies the previous one out.
 void DeviceGalerkin::download(const void* src, void* dst, std::size_t bytes) {
@@ -729,7 +750,7 @@ void DeviceGalerkin::download(const void* src, void* dst, std::size_t bytes) {
             const std::size_t p = c - 1;
             const std::size_t len = std::min(kStageBytes, bytes - p * kStageBytes);
             CFDXG_CUDA(cudaEventSynchronize(staged_[p & 1]));
-            std::memcpy(to + p * kStageBytes, stage_[p & 1], len);
+            parallel_memcpy(to + p * kStageBytes, static_cast<const char*>(stage_[p & 1]), len);
         }
     }
 }

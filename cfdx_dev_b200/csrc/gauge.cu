@@ -161,8 +161,8 @@ extern "C" int cfdxg_gauge_apply(cfdxg_context* ctx, const cfdxg_gauge* g, const
         B->n = g->n_out;
         B->nnz = g->nnz_out;
         B->host.n = g->n_out;
-        B->host.ro = g->hro;
-        B->host.co = g->hco;
+        B->host.ro.assign(g->hro.begin(), g->hro.end());
+        B->host.co.assign(g->hco.begin(), g->hco.end());
         B->ro.resize(static_cast<size_t>(g->n_out) + 1);
         B->co.resize(static_cast<size_t>(g->nnz_out));
         CFDXG_CUDA(cudaMemcpyAsync(B->ro.get(), g->ro.get(), sizeof(int) * (g->n_out + 1), cudaMemcpyDeviceToDevice,

@@ -740,7 +740,7 @@ void build_dense_inverse(cfdxg_context* ctx, DevHierarchy<T>& d, const AmgLevel&
     DevBuf<int> ro, co;
     DevBuf<double> va;
     std::vector<int> hro(H.A.ro.begin(), H.A.ro.end()), hco(H.A.co.begin(), H.A.co.end());
-    ro.upload(hro, ctx->stream); co.upload(hco, ctx->stream); va.upload(H.A.va, ctx->stream);
+    ro.upload(hro, ctx->stream); co.upload(hco, ctx->stream); va.upload(H.A.va.data(), H.A.va.size(), ctx->stream);
     build_dense_inverse_dev(ctx, d, n, ro.get(), co.get(), va.get());
 }
 
