@@ -293,9 +293,7 @@ __global__ void k_gauss_gradient(MeshView m, BcView bc, const int2* __restrict__
 // row and b.  Continuity is summed in cell-face order, the diagonal and the
 // fixed-pressure boundary terms in global face order (the per-cell sorted
 // permutation cs), as the reference sums them.
-// 64 registers: 8 resident blocks of kT = 128 threads per SM instead of 7 at
-// the compiler's 68 (no spills)
-__global__ void __launch_bounds__(128, 8) k_pressure_assembly(MeshView m, BcView bc, const int2* __restrict__ rec,
+__global__ void k_pressure_assembly(MeshView m, BcView bc, const int2* __restrict__ rec,
                                     const double* __restrict__ U, const double* __restrict__ rau,
                                     const double* __restrict__ p, const double* __restrict__ grad, double rho,
                                     const int* __restrict__ slot, const int* __restrict__ diag_pos,
