@@ -215,10 +215,8 @@ def run_form(ctx, form, m, mesh, g, nu_t, iterations, alpha_p, net, sync, keep=F
         t = time.perf_counter()
         if amg is None:
             # The FP32 forms end the cycle at <= 2,000 rows in an FP64 dense
-            # inverse (the mixed-precision configuration as specified): its
-            # Gauss-Jordan re-formation on every numeric refresh then costs
-            # ~0.1 s at this mesh's 1.9 k-row level instead of ~1.5 s at the
-            # 5 k-row level the pressure-solve benchmark cuts at.
+            # inverse (the mixed-precision configuration as specified), which
+            # every numeric refresh re-forms by LU.
             extra = {} if precision == "fp64" else {"coarse_dense_limit": 2000, "dense_fp64": 1}
             amg = cg.NativeBoomerAMGPreconditioner(ctx, precision=precision, **extra)
             if not amg.setup(A):
