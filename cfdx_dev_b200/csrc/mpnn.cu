@@ -19,11 +19,14 @@
 // read) and the readout into the last, so inference is four kernels.
 #include <cuda_bf16.h>
 
+#include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
 #include <limits>
 #include <random>
+#include <thread>
 
 #include "io.h"
 #include "krylov.h"
@@ -928,57 +931,90 @@ extern "C" int cfdxg_mpnn_bind(cfdxg_context* ctx, cfdxg_mpnn* net, cfdxg_mesh* 
     matrix_sync_host_values(ctx, M);
     const int64_t n = A->n;
     const HostCsr& H = M->host;
+    // per-row work on the host threads (every value is formed as before; only
+    // the sums of the feature standardisation stay sequential, in row order)
+    const auto rows = [n](auto&& fn) {
+        const int workers = static_cast<int>(std::max<int64_t>(1, std::min<int64_t>(host_threads(), n / 65536)));
+        if (workers <= 1) { fn(int64_t(0), n); return; }
+        std::vector<std::thread> pool;
+        for (int w = 0; w < workers; ++w) pool.emplace_back([&fn, n, w, workers] { fn(n * w / workers, n * (w + 1) / workers); });
+        for (auto& t : pool) t.join();
+    };
     std::vector<double> diag(n, 0.0), vol(n), ap(n);
-    for (int64_t i = 0; i < n; ++i)
-        for (uint32_t k = H.ro[i]; k < H.ro[i + 1]; ++k)
-            if (H.co[k] == i) diag[i] = H.va[k];
-    for (int64_t i = 0; i < n; ++i)
-        if (!(diag[i] > 0.0)) throw Error(CFDXG_ERR_INVALID_ARGUMENT, "the learned preconditioner needs a positive diagonal");
+    std::atomic<bool> bad_diag{false}, asymmetric{false}, bad_cell{false};
+    rows([&](int64_t b, int64_t e) {
+        for (int64_t i = b; i < e; ++i) {
+            for (uint32_t k = H.ro[i]; k < H.ro[i + 1]; ++k)
+                if (H.co[k] == i) diag[i] = H.va[k];
+            if (!(diag[i] > 0.0)) bad_diag = true;
+        }
+    });
+    if (bad_diag) throw Error(CFDXG_ERR_INVALID_ARGUMENT, "the learned preconditioner needs a positive diagonal");
     // symmetric couplings are required (the backward pass gathers over the same graph)
     std::vector<float> ew(H.co.size(), 0.0f);
-    for (int64_t i = 0; i < n; ++i)
-        for (uint32_t k = H.ro[i]; k < H.ro[i + 1]; ++k) {
-            const uint32_t j = H.co[k];
-            if (j == i) continue;
-            const uint32_t* b = H.co.data() + H.ro[j];
-            const uint32_t* e = H.co.data() + H.ro[j + 1];
-            const uint32_t* it = std::lower_bound(b, e, static_cast<uint32_t>(i));
-            if (it == e || *it != i || H.va[it - H.co.data()] != H.va[k])
-                throw Error(CFDXG_ERR_INVALID_ARGUMENT, "the learned preconditioner needs a symmetric matrix");
-            ew[k] = static_cast<float>(-H.va[k] / std::sqrt(diag[i] * diag[j]));
+    std::vector<int> gro(n + 1, 0);
+    rows([&](int64_t b, int64_t e) {
+        for (int64_t i = b; i < e; ++i) {
+            int off = 0;
+            for (uint32_t k = H.ro[i]; k < H.ro[i + 1]; ++k) {
+                const uint32_t j = H.co[k];
+                if (j == i) continue;
+                ++off;
+                const uint32_t* lo = H.co.data() + H.ro[j];
+                const uint32_t* hi = H.co.data() + H.ro[j + 1];
+                const uint32_t* it = std::lower_bound(lo, hi, static_cast<uint32_t>(i));
+                if (it == hi || *it != i || H.va[it - H.co.data()] != H.va[k]) {
+                    asymmetric = true;
+                    return;
+                }
+                ew[k] = static_cast<float>(-H.va[k] / std::sqrt(diag[i] * diag[j]));
+            }
+            gro[i + 1] = off;
         }
+    });
+    if (asymmetric) throw Error(CFDXG_ERR_INVALID_ARGUMENT, "the learned preconditioner needs a symmetric matrix");
     mesh->cell_volume.download(vol.data(), ctx->stream);
     if (mem == CFDXG_MEM_DEVICE) CFDXG_CUDA(cudaMemcpyAsync(ap.data(), a_P, n * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
     else std::memcpy(ap.data(), a_P, n * sizeof(double));
     CFDXG_CUDA(cudaStreamSynchronize(ctx->stream));
     std::vector<float> feats(3 * n);
+    std::vector<double> logs(n);
     const auto standardise = [&](const std::vector<double>& v, int slot) {
+        rows([&](int64_t b, int64_t e) { for (int64_t i = b; i < e; ++i) logs[i] = std::log(v[i]); });
         double mean = 0.0, sq = 0.0;
-        for (int64_t i = 0; i < n; ++i) mean += std::log(v[i]);
+        for (int64_t i = 0; i < n; ++i) mean += logs[i];
         mean /= n;
-        for (int64_t i = 0; i < n; ++i) sq += (std::log(v[i]) - mean) * (std::log(v[i]) - mean);
+        for (int64_t i = 0; i < n; ++i) sq += (logs[i] - mean) * (logs[i] - mean);
         const double sd = std::sqrt(sq / n);
-        for (int64_t i = 0; i < n; ++i)
-            feats[slot * n + i] = static_cast<float>((std::log(v[i]) - mean) / (sd > 0.0 ? sd : 1.0));
+        rows([&](int64_t b, int64_t e) {
+            for (int64_t i = b; i < e; ++i)
+                feats[slot * n + i] = static_cast<float>((logs[i] - mean) / (sd > 0.0 ? sd : 1.0));
+        });
     };
-    for (int64_t i = 0; i < n; ++i)
-        if (!(vol[i] > 0.0) || !(ap[i] > 0.0)) throw Error(CFDXG_ERR_INVALID_ARGUMENT, "volumes and a_P must be positive");
+    rows([&](int64_t b, int64_t e) {
+        for (int64_t i = b; i < e; ++i)
+            if (!(vol[i] > 0.0) || !(ap[i] > 0.0)) bad_cell = true;
+    });
+    if (bad_cell) throw Error(CFDXG_ERR_INVALID_ARGUMENT, "volumes and a_P must be positive");
     standardise(vol, 0);
     standardise(ap, 1);
     standardise(diag, 2);
     net->ew.upload(ew, ctx->stream);
-    std::vector<int> gro(n + 1, 0), gco;
-    std::vector<float> gew;
-    gco.reserve(H.co.size());
-    gew.reserve(H.co.size());
-    for (int64_t i = 0; i < n; ++i) {
-        for (uint32_t k = H.ro[i]; k < H.ro[i + 1]; ++k)
-            if (H.co[k] != i) {
-                gco.push_back(static_cast<int>(H.co[k]));
-                gew.push_back(ew[k]);
-            }
-        gro[i + 1] = static_cast<int>(gco.size());
-    }
+    // the coupling list without the diagonal: row offsets by a prefix sum, then rows in parallel
+    for (int64_t i = 0; i < n; ++i) gro[i + 1] += gro[i];
+    std::vector<int> gco(static_cast<std::size_t>(gro[n]));
+    std::vector<float> gew(static_cast<std::size_t>(gro[n]));
+    rows([&](int64_t b, int64_t e) {
+        for (int64_t i = b; i < e; ++i) {
+            int o = gro[i];
+            for (uint32_t k = H.ro[i]; k < H.ro[i + 1]; ++k)
+                if (H.co[k] != i) {
+                    gco[o] = static_cast<int>(H.co[k]);
+                    gew[o] = ew[k];
+                    ++o;
+                }
+        }
+    });
     net->gro.upload(gro, ctx->stream);
     net->gco.upload(gco, ctx->stream);
     net->gew.upload(gew, ctx->stream);
