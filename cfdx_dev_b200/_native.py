@@ -58,6 +58,7 @@ class AmgOptions(C.Structure):
         ("coarse_dense_limit", C.c_int32), ("reference_order", C.c_int32),
         ("coarse_pre_sweeps", C.c_int32), ("coarse_post_sweeps", C.c_int32), ("narrow_columns", C.c_int32),
         ("half_values", C.c_int32), ("dense_fp64", C.c_int32), ("constant_null_space", C.c_int32),
+        ("coarse_drop_tolerance", C.c_double),
     ]
 
 

@@ -289,10 +289,84 @@ __global__ void k_gauss_gradient(MeshView m, BcView bc, const int2* __restrict__
     grad[c] = gx; grad[m.nc + c] = gy; grad[2 * m.nc + c] = gz;
 }
 
-// Pressure-corrector block (:8048-8181): one thread per cell writes its CSR
-// row and b.  Continuity is summed in cell-face order, the diagonal and the
-// fixed-pressure boundary terms in global face order (the per-cell sorted
-// permutation cs), as the reference sums them.
+// coeff[k] of a cell's NF slots, k known only at run time: a select over the
+// unrolled slots keeps the array in registers
+template <int NF>
+__device__ __forceinline__ double pick_slot(const double (&a)[NF], int k) {
+    double v = a[0];
+#pragma unroll
+    for (int j = 1; j < NF; ++j)
+        if (j == k) v = a[j];
+    return v;
+}
+
+// Pressure-corrector block (:8048-8181) of cell c: its CSR row and b.
+// Continuity is summed in cell-face order, the diagonal and the fixed-pressure
+// boundary terms in global face order (the per-cell sorted permutation cs), as
+// the reference sums them.  NF > 0: a cell of exactly NF faces, every loop
+// unrolled and the face coefficients in registers; NF = 0: up to
+// kMaxCellFaces faces, the coefficients in local memory.
+template <int NF>
+__device__ __forceinline__ void assemble_cell(const MeshView& m, const BcView& bc, const int2* __restrict__ rec,
+                                              const double* __restrict__ U, const double* __restrict__ rau,
+                                              const double* __restrict__ p, const double* __restrict__ grad,
+                                              double rho, const int* __restrict__ slot,
+                                              const int* __restrict__ diag_pos, double* __restrict__ values,
+                                              double* __restrict__ b, double* __restrict__ phi_out, int* status,
+                                              int c, int beg, int nfc) {
+    constexpr int kCap = NF > 0 ? NF : kMaxCellFaces;
+    const int n_slots = NF > 0 ? NF : nfc;
+    double coeff[kCap];
+    unsigned interior = 0;
+    double cont = 0.0;
+#pragma unroll
+    for (int k = 0; k < n_slots; ++k) {
+        const int2 r = rec[beg + k];
+        const int f = r.x & 0x7fffffff;
+        const bool own = r.x >= 0;
+        const int o = own ? c : r.y, n = own ? r.y : c;
+        const double phi = mass_flux(m, f, o, n, U, rho);
+        if (phi_out && own) phi_out[f] = phi;
+        cont += own ? phi : -phi;
+        coeff[k] = 0.0;
+        if (r.y >= 0) {
+            interior |= 1u << k;
+            double ic;
+            const double rc = rc_internal(m, f, o, n, p, grad, rau, rho, &ic, status);
+            cont += own ? -rc : rc;
+            coeff[k] = rho * ic;
+        }
+    }
+    double diag = 0.0;
+#pragma unroll
+    for (int q = 0; q < n_slots; ++q) {
+        const int k = m.cs[beg + q];
+        if (interior >> k & 1u) diag += NF > 0 ? pick_slot(coeff, k) : coeff[k];
+    }
+    double acc = 0.0 + diag;
+    double bb = -cont;
+    const unsigned all = n_slots >= 32 ? ~0u : (1u << n_slots) - 1u;
+    if (interior != all) {
+        for (int q = 0; q < n_slots; ++q) {
+            const int k = m.cs[beg + q];
+            if (interior >> k & 1u) continue;
+            const int f = rec[beg + k].x & 0x7fffffff;
+            double value;
+            if (!boundary_fixed(m, bc, f, &value)) continue;
+            double bcoef, source;
+            fixed_boundary(m, f, c, p, grad, rau, rho, value, &bcoef, &source, status);
+            acc += rho * bcoef;
+            bb += source;
+        }
+    }
+    values[diag_pos[c]] = acc;
+#pragma unroll
+    for (int k = 0; k < n_slots; ++k)
+        if (slot[beg + k] >= 0) values[slot[beg + k]] = 0.0 - coeff[k];
+    b[c] = bb;
+}
+
+// One thread per cell; tetrahedra and hexahedra take the unrolled forms.
 __global__ void k_pressure_assembly(MeshView m, BcView bc, const int2* __restrict__ rec,
                                     const double* __restrict__ U, const double* __restrict__ rau,
                                     const double* __restrict__ p, const double* __restrict__ grad, double rho,
@@ -303,47 +377,12 @@ __global__ void k_pressure_assembly(MeshView m, BcView bc, const int2* __restric
     if (c >= m.nc) return;
     const int beg = m.co[c], nfc = m.co[c + 1] - beg;
     if (nfc > kMaxCellFaces) { atomicOr(status, kStatusGeometry); return; }
-    double coeff[kMaxCellFaces];
-    double cont = 0.0;
-    for (int k = 0; k < nfc; ++k) {
-        const int2 r = rec[beg + k];
-        const int f = r.x & 0x7fffffff;
-        const bool own = r.x >= 0;
-        const int o = own ? c : r.y, n = own ? r.y : c;
-        const double phi = mass_flux(m, f, o, n, U, rho);
-        if (phi_out && own) phi_out[f] = phi;
-        cont += own ? phi : -phi;
-        coeff[k] = 0.0;
-        if (r.y >= 0) {
-            double ic;
-            const double rc = rc_internal(m, f, o, n, p, grad, rau, rho, &ic, status);
-            cont += own ? -rc : rc;
-            coeff[k] = rho * ic;
-        }
-    }
-    double diag = 0.0;
-    for (int q = 0; q < nfc; ++q) {
-        const int k = m.cs[beg + q];
-        if (rec[beg + k].y >= 0) diag += coeff[k];
-    }
-    double acc = 0.0 + diag;
-    double bb = -cont;
-    for (int q = 0; q < nfc; ++q) {
-        const int k = m.cs[beg + q];
-        const int2 r = rec[beg + k];
-        if (r.y >= 0) continue;
-        const int f = r.x & 0x7fffffff;
-        double value;
-        if (!boundary_fixed(m, bc, f, &value)) continue;
-        double bcoef, source;
-        fixed_boundary(m, f, c, p, grad, rau, rho, value, &bcoef, &source, status);
-        acc += rho * bcoef;
-        bb += source;
-    }
-    values[diag_pos[c]] = acc;
-    for (int k = 0; k < nfc; ++k)
-        if (slot[beg + k] >= 0) values[slot[beg + k]] = 0.0 - coeff[k];
-    b[c] = bb;
+    if (nfc == 4)
+        assemble_cell<4>(m, bc, rec, U, rau, p, grad, rho, slot, diag_pos, values, b, phi_out, status, c, beg, nfc);
+    else if (nfc == 6)
+        assemble_cell<6>(m, bc, rec, U, rau, p, grad, rho, slot, diag_pos, values, b, phi_out, status, c, beg, nfc);
+    else
+        assemble_cell<0>(m, bc, rec, U, rau, p, grad, rho, slot, diag_pos, values, b, phi_out, status, c, beg, nfc);
 }
 
 // make_rhie_chow_mass_flux (:2064-2217), HBYA_PREDICTOR, zero-gradient velocity boundaries

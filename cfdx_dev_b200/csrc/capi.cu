@@ -176,6 +176,7 @@ void amg_setup_impl(cfdxg_context* ctx, cfdxg_amg* amg, cfdxg_matrix* A) {
         up.coarse_dense_limit = amg->opts.coarse_dense_limit;
         up.half_values = amg->opts.half_values != 0;
         up.dense_fp64 = amg->opts.dense_fp64 != 0;
+        up.coarse_drop_tolerance = amg->opts.coarse_drop_tolerance;
         d32 = upload_hierarchy<float>(ctx, staged, up, refresh.get());
     } else {
         d64 = upload_hierarchy<double>(ctx, staged, up, refresh.get());
@@ -398,6 +399,7 @@ extern "C" int cfdxg_amg_options_default(cfdxg_amg_options* o) {
     o->half_values = 1;
     o->dense_fp64 = 0;
     o->constant_null_space = 0;
+    o->coarse_drop_tolerance = 0.02;
     return CFDXG_OK;
 }
 
@@ -411,7 +413,8 @@ extern "C" int cfdxg_amg_create(cfdxg_context* ctx, const cfdxg_amg_options* opt
     // MatrixFreeVcyclePreconditioner constructor checks (amg_preconditioner.h:64-75)
     if (!(o.omega > 0.0 && o.omega < 2.0) || !std::isfinite(o.strength_threshold) || o.strength_threshold < 0.0 ||
         o.strength_threshold > 1.0 || o.max_levels <= 0 || o.pre_sweeps < -1 || o.post_sweeps < -1 ||
-        (o.precision != CFDXG_PRECISION_FP64 && o.precision != CFDXG_PRECISION_FP32_VCYCLE))
+        (o.precision != CFDXG_PRECISION_FP64 && o.precision != CFDXG_PRECISION_FP32_VCYCLE) ||
+        !(o.coarse_drop_tolerance >= 0.0 && o.coarse_drop_tolerance < 1.0))
         throw Error(CFDXG_ERR_INVALID_ARGUMENT, "invalid AMG operator");
     *out = amg.release();
     return CFDXG_OK;

@@ -35,6 +35,12 @@ struct DevLevel {
     DevBuf<__half> vh;
     DevBuf<T> rscale;
     bool half = false;
+    // Sparsified smoothing operator (FP32 cycle, coarse_drop_tolerance): ro,
+    // co and the values hold the Galerkin operator's diagonal and its kept
+    // off-diagonal entries (one bit per Galerkin entry in keep), the dropped
+    // entries added to the diagonal; inv_diag is that diagonal's inverse.
+    DevBuf<uint32_t> keep;
+    bool sparsified = false;
     DevBuf<T> va, inv_diag;
     DevBuf<int> p_off, p_col, r_off, r_row;
     DevBuf<T> p_val, r_val;
@@ -210,6 +216,7 @@ struct UploadOptions {
     bool half_values = false;     // FP32: FP16 row-scaled matrix values
     bool dense_fp64 = false;      // FP32: the dense coarse inverse stored (and applied) in FP64
     bool constant_null_space = false;   // the cycle of a pure-Neumann operator (mean removals)
+    double coarse_drop_tolerance = 0.0; // FP32: sparsified smoothing operators between fine and coarsest
 };
 
 // From the host hierarchy, or, with R (the device levels a device-Galerkin

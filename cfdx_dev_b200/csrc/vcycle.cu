@@ -20,6 +20,7 @@
 // system bordered by a row and a column of ones (amg_preconditioner.h:1197-1201,
 // 2382, 2406, 2430, 2440, 2590-2664); the FP32 cycle's dense coarse inverse
 // is then the leading block of the bordered matrix's inverse.
+#include <cub/device/device_scan.cuh>
 #include <cusolverDn.h>
 
 #include <cmath>
@@ -913,6 +914,161 @@ void copy_or_cast(cfdxg_context* ctx, const double* src, T* dst, int64_t n) {
     }
 }
 
+// ---- sparsified smoothing operators (FP32 cycle, coarse_drop_tolerance)
+//
+// Between the fine and the coarsest level the Galerkin operators of the
+// classical RS hierarchy carry many small entries (operator complexity ~27 at
+// 64^3, the levels >= 1 holding 95% of the nonzeros).  The FP32 cycle's
+// smoother on those levels may use a sparser operator: each row keeps its
+// diagonal and the off-diagonal entries of at least theta times the row's
+// largest off-diagonal magnitude, and every dropped entry is added to the
+// row's diagonal (row sums, and so the constant vector's image, unchanged).
+// The transfers and the coarser Galerkin operators are formed from the full
+// operators as before.  A warp per row; all sums and maxima are fixed-order
+// butterflies, so the result is deterministic.
+
+// Marks the kept entries of each row (keep bits, zeroed before) and counts them.
+__global__ void k_drop_mark(int n, const int* __restrict__ ro, const int* __restrict__ co,
+                            const double* __restrict__ va, double theta, uint32_t* __restrict__ keep,
+                            int* __restrict__ cnt) {
+    const int lane = threadIdx.x & 31;
+    const int warps = gridDim.x * (blockDim.x >> 5);
+    for (int i = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); i < n; i += warps) {
+        const int b = ro[i], e = ro[i + 1];
+        double m = 0.0;
+        for (int k = b + lane; k < e; k += 32)
+            if (co[k] != i) m = fmax(m, fabs(va[k]));
+        for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+        const double cut = theta * m;
+        int kept = 0;
+        for (int k0 = b; k0 < e; k0 += 32) {
+            const int k = k0 + lane;
+            const bool kp = k < e && (co[k] == i || fabs(va[k]) >= cut);
+            const uint32_t bits = __ballot_sync(0xffffffffu, kp);
+            kept += __popc(bits);
+            if (lane == 0 && bits) {
+                // the 32 entries from k0 span at most two words; rows share only their end words
+                const int w = k0 >> 5, sh = k0 & 31;
+                atomicOr(&keep[w], bits << sh);
+                if (sh && (bits >> (32 - sh))) atomicOr(&keep[w + 1], bits >> (32 - sh));
+            }
+        }
+        if (lane == 0) cnt[i] = kept;
+    }
+}
+
+// Fills the sparsified row i from the Galerkin row and its keep bits: the
+// lumped diagonal d = a_ii + sum of the dropped entries, inv_diag = 1 / d,
+// the kept columns (write_columns) and values -- FP16 fractions of the kept
+// row's largest magnitude (vh, rscale; the rounding of k_quantize_rows_warp)
+// or T.  A zero or non-finite lumped diagonal sets the status word's
+// non-finite flag.
+template <class T>
+__global__ void k_drop_fill(int n, const int* __restrict__ ro, const int* __restrict__ co,
+                            const double* __restrict__ va, const uint32_t* __restrict__ keep,
+                            const int* __restrict__ ro_s, int* __restrict__ co_s, __half* __restrict__ vh,
+                            float* __restrict__ rscale, T* __restrict__ va_s, T* __restrict__ inv_diag,
+                            int* status) {
+    const int lane = threadIdx.x & 31;
+    const int warps = gridDim.x * (blockDim.x >> 5);
+    for (int i = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); i < n; i += warps) {
+        const int b = ro[i], e = ro[i + 1];
+        double lump = 0.0, mk = 0.0, dia = 0.0;
+        for (int k = b + lane; k < e; k += 32) {
+            const double v = va[k];
+            if (co[k] == i) dia += v;
+            else if (keep[k >> 5] >> (k & 31) & 1u) mk = fmax(mk, fabs(v));
+            else lump += v;
+        }
+        for (int o = 16; o > 0; o >>= 1) {
+            lump += __shfl_xor_sync(0xffffffffu, lump, o);
+            dia += __shfl_xor_sync(0xffffffffu, dia, o);
+            mk = fmax(mk, __shfl_xor_sync(0xffffffffu, mk, o));
+        }
+        const double d = dia + lump;
+        const double m = fmax(mk, fabs(d));
+        const float sc = m > 0.0 ? static_cast<float>(m) : 1.0f;
+        if (lane == 0) {
+            const double id = 1.0 / d;
+            if (!(d != 0.0) || !isfinite(id)) atomicOr(status, kStatusNonFinite);
+            inv_diag[i] = static_cast<T>(id);
+            if (vh) rscale[i] = sc;
+        }
+        int base = ro_s[i];
+        for (int k0 = b; k0 < e; k0 += 32) {
+            const int k = k0 + lane;
+            const bool diag = k < e && co[k] == i;
+            const bool kp = k < e && (diag || (keep[k >> 5] >> (k & 31) & 1u));
+            const uint32_t bits = __ballot_sync(0xffffffffu, kp);
+            if (kp) {
+                const int pos = base + __popc(bits & ((1u << lane) - 1u));
+                const double v = diag ? d : va[k];
+                if (co_s) co_s[pos] = co[k];
+                if (vh) vh[pos] = __float2half_rn(static_cast<float>(v / static_cast<double>(sc)));
+                else va_s[pos] = static_cast<T>(v);
+            }
+            base += __popc(bits);
+        }
+    }
+}
+
+int warp_rows_grid(int n) { return std::max(1, std::min(blocks_for(n, kT / 32), 148 * 16)); }
+
+// Sparsifies level D from its device Galerkin operator R (setup): marks the
+// kept entries, forms the row offsets and fills columns, values and inverse
+// diagonal.  D keeps the keep bits for refreshes.
+template <class T>
+void sparsify_level(cfdxg_context* ctx, DevLevel<T>& D, const DevRefreshLevel& R, double theta, bool half) {
+    cudaStream_t s = ctx->stream;
+    const int n = R.n;
+    D.keep.resize(static_cast<std::size_t>(std::max<int64_t>((R.nnz + 31) / 32 + 1, 1)));
+    D.keep.zero(s);
+    DevBuf<int> cnt(static_cast<std::size_t>(n) + 1);
+    CFDXG_CUDA(cudaMemsetAsync(cnt.get() + n, 0, sizeof(int), s));
+    k_drop_mark<<<warp_rows_grid(n), kT, 0, s>>>(n, R.ro.get(), R.co.get(), R.va.get(), theta, D.keep.get(),
+                                                 cnt.get());
+    check_launch(ctx);
+    D.ro.resize(static_cast<std::size_t>(n) + 1);
+    std::size_t bytes = 0;
+    CFDXG_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, bytes, cnt.get(), D.ro.get(), n + 1, s));
+    DevBuf<unsigned char> temp(std::max<std::size_t>(bytes, 1));
+    CFDXG_CUDA(cub::DeviceScan::ExclusiveSum(temp.get(), bytes, cnt.get(), D.ro.get(), n + 1, s));
+    int nnz = 0;
+    CFDXG_CUDA(cudaMemcpyAsync(&nnz, D.ro.get() + n, sizeof(int), cudaMemcpyDeviceToHost, s));
+    CFDXG_CUDA(cudaStreamSynchronize(s));
+    D.nnz = nnz;
+    D.narrow = false;
+    D.co16.release();
+    D.co.resize(static_cast<std::size_t>(std::max(nnz, 1)));
+    D.half = half;
+    if (half) {
+        D.vh.resize(static_cast<std::size_t>(std::max(nnz, 1)));
+        D.rscale.resize(static_cast<std::size_t>(n));
+        D.va.release();
+    } else {
+        D.va.resize(static_cast<std::size_t>(std::max(nnz, 1)));
+        D.vh.release();
+        D.rscale.release();
+    }
+    D.inv_diag.resize(static_cast<std::size_t>(n));
+    D.sparsified = true;
+}
+
+// (Re-)forms the sparsified level's values and inverse diagonal from the
+// Galerkin values R.va (setup and numeric refresh; the kept pattern is fixed).
+template <class T>
+void fill_sparsified(cfdxg_context* ctx, DevLevel<T>& D, const DevRefreshLevel& R, bool columns) {
+    __half* vh = nullptr;
+    float* rs = nullptr;
+    if constexpr (std::is_same<T, float>::value) {
+        if (D.half) { vh = D.vh.get(); rs = D.rscale.get(); }
+    }
+    k_drop_fill<T><<<warp_rows_grid(R.n), kT, 0, ctx->stream>>>(
+        R.n, R.ro.get(), R.co.get(), R.va.get(), D.keep.get(), D.ro.get(), columns ? D.co.get() : nullptr, vh, rs,
+        D.half ? nullptr : D.va.get(), D.inv_diag.get(), ctx->scratch.status);
+    check_launch(ctx);
+}
+
 // ---- the same upload from the device copy the setup's Galerkin products left
 
 // flag = 1 when some |column - row| does not fit in 16 bits
@@ -948,15 +1104,28 @@ void device_copy(cfdxg_context* ctx, DevBuf<T>& dst, const T* src, int64_t count
         CFDXG_CUDA(cudaMemcpyAsync(dst.get(), src, sizeof(T) * count, cudaMemcpyDeviceToDevice, ctx->stream));
 }
 
+template <class T>
+void upload_transfers_device(cfdxg_context* ctx, DevLevel<T>& D, const AmgLevel& H, const DevRefreshLevel& R,
+                             const UploadOptions& opt);
+
 // upload_level from the setup's device level (int CSR, FP64 values, P and the
 // stable P^T adjacency): the same layout choices and the same values, formed
 // by kernels instead of host loops.
 template <class T>
 void upload_level_device(cfdxg_context* ctx, DevLevel<T>& D, const AmgLevel& H, const DevRefreshLevel& R,
-                         bool with_transfer, const UploadOptions& opt) {
+                         bool with_transfer, const UploadOptions& opt, bool sparsify) {
     cudaStream_t s = ctx->stream;
     D.n = R.n;
     D.nnz = static_cast<int>(R.nnz);
+    if (sparsify) {
+        sparsify_level(ctx, D, R, opt.coarse_drop_tolerance, std::is_same<T, float>::value && opt.half_values);
+        D.tpr = choose_tpr(D.nnz, D.n, false);
+        fill_sparsified(ctx, D, R, true);
+        upload_transfers_device(ctx, D, H, R, opt);
+        D.r.resize(D.n); D.x.resize(D.n); D.x2.resize(D.n); D.res.resize(D.n);
+        CFDXG_CUDA(cudaStreamSynchronize(s));
+        return;
+    }
     D.tpr = choose_tpr(D.nnz, D.n, opt.reference_order);
     device_copy(ctx, D.ro, R.ro.get(), D.n + 1);
     bool narrow = with_transfer && opt.narrow_columns && D.tpr == 1;
@@ -996,7 +1165,16 @@ void upload_level_device(cfdxg_context* ctx, DevLevel<T>& D, const AmgLevel& H, 
     for (std::size_t k = 0; k < d.size(); ++k) d[k] = static_cast<T>(H.inv_diag[k]);
     D.inv_diag.upload(d, s);
     D.r.resize(D.n); D.x.resize(D.n); D.x2.resize(D.n); D.res.resize(D.n);
-    if (with_transfer) {
+    if (with_transfer) upload_transfers_device(ctx, D, H, R, opt);
+    CFDXG_CUDA(cudaStreamSynchronize(s));
+}
+
+// P and P^T of a level from the setup's device copy
+template <class T>
+void upload_transfers_device(cfdxg_context* ctx, DevLevel<T>& D, const AmgLevel& H, const DevRefreshLevel& R,
+                             const UploadOptions& opt) {
+    cudaStream_t s = ctx->stream;
+    {
         const int64_t pn = static_cast<int64_t>(H.p_col.size());
         D.nc = R.n_coarse;
         D.tpr_r = choose_transfer_tpr(pn, D.nc, opt.reference_order);
@@ -1051,7 +1229,10 @@ std::unique_ptr<DevHierarchy<T>> upload_hierarchy(cfdxg_context* ctx, const AmgH
     // from the setup's device copy of the levels when there is one
     const bool from_device = R && static_cast<int>(R->L.size()) >= used;
     for (int l = 0; l < used; ++l) {
-        if (from_device) upload_level_device(ctx, d->L[l], h.levels[l], R->L[l], l + 1 < used, opt);
+        // the FP32 cycle's smoothing operators between the fine and the coarsest level
+        const bool sparsify = fp32 && opt.coarse_drop_tolerance > 0.0 && !opt.reference_order && l >= 1 &&
+                              l + 1 < used;
+        if (from_device) upload_level_device(ctx, d->L[l], h.levels[l], R->L[l], l + 1 < used, opt, sparsify);
         else upload_level(ctx, d->L[l], h.levels[l], l + 1 < used, opt);
     }
     if (d->coarse_mode == 2) {
@@ -1071,6 +1252,10 @@ template <class T>
 void set_hierarchy_values_device(cfdxg_context* ctx, DevHierarchy<T>& d, const DevRefresh& R, double omega) {
     d.omega = static_cast<T>(omega);
     for (int l = 0; l < d.used; ++l) {
+        if (d.L[l].sparsified) {
+            fill_sparsified(ctx, d.L[l], R.L[l], false);
+            continue;
+        }
         if (d.L[l].half) {
             if constexpr (std::is_same<T, float>::value)
                 quantize_level(ctx, d.L[l].n, R.L[l].nnz, d.L[l].ro.get(), R.L[l].va.get(), d.L[l].vh.get(),

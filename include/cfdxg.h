@@ -323,6 +323,19 @@ typedef struct {
                                         of ones (:1191-1203, 2369-2443, 2564-2666).  With
                                         reference_order the means are summed in index order,
                                         so the FP64 cycle is the reference's bit for bit. */
+    double coarse_drop_tolerance;    /* FP32 V-cycle only (0 with reference_order).  theta > 0
+                                        (default 0.02): the smoothing operator of every level
+                                        between the fine and the coarsest keeps its diagonal and
+                                        the off-diagonal entries with |a_ij| >= theta * max over
+                                        k != i of |a_ik|; each dropped entry is added to its
+                                        row's diagonal, so row sums are unchanged.  The Galerkin
+                                        hierarchy, its transfers and the FP64 Krylov operator are
+                                        untouched: only the FP32 preconditioner changes, and
+                                        the solve stops on the same FP64 true residual.  At
+                                        64^3 theta = 0.02 keeps 17% of those levels' nonzeros
+                                        at the same FGMRES iteration count.  The kept pattern
+                                        is fixed at setup; a numeric refresh re-forms its
+                                        values and diagonals.  0: the Galerkin operators. */
 } cfdxg_amg_options;
 
 int cfdxg_amg_options_default(cfdxg_amg_options* opts);

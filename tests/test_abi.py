@@ -1,4 +1,5 @@
 """The C ABI library loads and exports every entry point include/cfdxg.h declares."""
+import pytest
 import re
 from pathlib import Path
 
@@ -33,6 +34,18 @@ def test_host_only_calls_need_no_device():
     assert m.n_cells == 27 and m.n_faces == 108
     amg = cg.NativeBoomerAMGPreconditioner(None)
     assert amg.name() == "NativeBoomerStyleAMG"
+
+
+def test_amg_options_are_validated():
+    """cfdxg_amg_create refuses out-of-range options (host-only, no device)."""
+    import cfdx_dev_b200 as cg
+    for bad in (dict(omega=0.0), dict(omega=2.0), dict(strength_threshold=1.5), dict(max_levels=0),
+                dict(coarse_drop_tolerance=-0.1), dict(coarse_drop_tolerance=1.0),
+                dict(coarse_drop_tolerance=float("nan"))):
+        with pytest.raises(cg.CfdxgError):
+            cg.NativeBoomerAMGPreconditioner(None, **bad)
+    cg.NativeBoomerAMGPreconditioner(None, precision="fp32_vcycle", coarse_drop_tolerance=0.0)
+    cg.NativeBoomerAMGPreconditioner(None, precision="fp32_vcycle", coarse_drop_tolerance=0.5)
 
 
 def test_header_is_plain_c_and_links_from_c(tmp_path):
