@@ -217,9 +217,10 @@ def run_cfdxg(args):
         net.bind(mesh, A, base_aP)
         plan.append(("learned_fp32", "fp32_vcycle", "fgmres", True))
     # The headline is the FP32 V-cycle form: trained on the full config-4 set
-    # (4,096 pairs on 256 meshes of 16^3-48^3) the learned stage saves 0.1
-    # FGMRES iteration per solve at 64^3 and costs 0.8 ms, so it is timed and
-    # reported as its own form but does not set `value`.
+    # (4,096 pairs on 256 meshes of 16^3-48^3) the learned stage saves no
+    # FGMRES iteration per solve at 64^3 in front of the default cycle and
+    # costs about 0.5 ms, so it is timed and reported as its own form but
+    # does not set `value`.
     headline = "fp32_vcycle" if any(e[0] == "fp32_vcycle" for e in plan) else plan[-1][0]
     forms = {}
     amgs = {}

@@ -133,11 +133,13 @@ void fill_report(cfdxg_report* rep, const KrylovResult& r) {
 }
 
 // Fine-level sweeps; -1 selects the precision's default: V(6,6), the
-// reference's Balanced policy, for the FP64 cycle; V(4,4) for the FP32 cycle,
-// which measured the same FGMRES iteration count as V(6,6) at 64^3 (13) in
-// 11.2 instead of 11.8 ms, where V(3,3) and V(2,2) took one iteration more.
+// reference's Balanced policy, for the FP64 cycle; V(3,3) for the FP32 cycle
+// with its sparsified coarse smoothers, which measured the same FGMRES
+// iteration count as V(4,4) (13 at 64^3, 6.9 instead of 7.2 ms per solve; 16
+// on the 4.2 M-cell boundary layer, 19.3 instead of 21.0 ms), where V(2,2)
+// took one to two iterations more.
 int resolve_sweeps(int32_t v, int32_t precision) {
-    return v >= 0 ? v : (precision == CFDXG_PRECISION_FP32_VCYCLE ? 4 : 6);
+    return v >= 0 ? v : (precision == CFDXG_PRECISION_FP32_VCYCLE ? 3 : 6);
 }
 
 void amg_setup_impl(cfdxg_context* ctx, cfdxg_amg* amg, cfdxg_matrix* A) {

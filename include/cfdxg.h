@@ -276,7 +276,7 @@ int cfdxg_gauge_destroy(cfdxg_gauge* g);
 typedef struct {
     double omega;                    /* 0.7 (Balanced policy, hypre_amg.cpp:172) */
     int32_t pre_sweeps;              /* fine-level sweeps; -1 (default): 6 for the FP64 cycle */
-    int32_t post_sweeps;             /* (the reference's Balanced policy), 4 for the FP32 cycle */
+    int32_t post_sweeps;             /* (the reference's Balanced policy), 3 for the FP32 cycle */
     double strength_threshold;       /* 0.25 */
     int32_t max_levels;              /* 25 */
     int32_t require_smoother_certificate; /* 1 for CG plans, 0 for GMRES/FGMRES */
@@ -284,8 +284,7 @@ typedef struct {
     int32_t coarse_dense_limit;      /* FP32 V-cycle: the cycle ends at the first level with
                                         <= this many rows (6000) in a dense inverse, formed
                                         in FP64 (LU with partial pivoting) and stored
-                                        FP32; at 64^3 this is the 5,287-row level, 12 instead
-                                        of 13 FGMRES iterations, 10.4 instead of 11.8 ms */
+                                        FP32; at 64^3 this is the 5,287-row level */
     int32_t reference_order;         /* 1: every row sum in CSR order, so the FP64
                                         V-cycle is bit-identical to the reference's;
                                         0 (default): levels with long rows use a
