@@ -18,6 +18,7 @@
 #include <functional>
 #include <limits>
 #include <mutex>
+#include <type_traits>
 
 #include "krylov.h"
 #include "nullspace.cuh"
@@ -242,47 +243,41 @@ __global__ void k_multi_axpy(int n, const double* __restrict__ V, int i0, int c,
 // basis vectors): three passes over the basis per Arnoldi step instead of
 // four, and the two norms of w taken inside them (plain sums of squares: this
 // option is the library's own orthogonalisation, not the reference's MGS2).
-// They run on a fixed grid (a partition that depends only on n and the GPU,
-// so the sums are deterministic) and reduce all outputs at once: per warp by
-// a fixed butterfly, per block in warp order, and over the blocks by one warp
-// per output in a fixed lane/butterfly order.  The first pass keeps eight
-// blocks per SM (its loads need the warps); the fused update-and-dot pass,
-// at 120 registers, takes kGsBlocksPerSm blocks per SM, the most that fit at
-// once, so its reduction tail runs once (3.9 instead of 6.1 ms per eight
-// 64^3 solves).
-constexpr int kGsBlocksPerSm = 2;
+// Each pass runs one resident wave (the blocks of its instance that fit on
+// the GPU at once: a partition that depends only on n, the basis count and
+// the GPU, so the sums are deterministic) and reduces all outputs at once:
+// per warp by a fixed butterfly, per block in warp order, and over the
+// blocks by one warp per output in a fixed lane/butterfly order.
 constexpr int kGsWarps = kT / 32;
 
-// out[q] = grid sum of acc[q] for q < c; with EXTRA also out[c] = grid sum of extra.
-template <int NMAX, bool EXTRA>
-__device__ __forceinline__ void grid_multi_sum(const double (&acc)[NMAX], int c, double extra, double* partial,
+// out[q] = grid sum of acc[q] for q < C; with EXTRA also out[C] = grid sum of extra.
+template <int C, bool EXTRA>
+__device__ __forceinline__ void grid_multi_sum(const double (&acc)[C], double extra, double* partial,
                                                unsigned* ticket, double* out) {
-    __shared__ double wsum[kGsWarps][NMAX + 1];
+    constexpr int kOut = C + (EXTRA ? 1 : 0);
+    __shared__ double wsum[kGsWarps][kOut];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
 #pragma unroll
-    for (int q = 0; q < NMAX; ++q) {
-        if (q < c) {
-            double v = acc[q];
+    for (int q = 0; q < C; ++q) {
+        double v = acc[q];
 #pragma unroll
-            for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-            if (lane == 0) wsum[warp][q] = v;
-        }
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+        if (lane == 0) wsum[warp][q] = v;
     }
     if (EXTRA) {
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) extra += __shfl_xor_sync(0xffffffffu, extra, o);
-        if (lane == 0) wsum[warp][c] = extra;
-        ++c;
+        if (lane == 0) wsum[warp][kOut - 1] = extra;
     }
     __syncthreads();
-    if (threadIdx.x < c) {
+    if (threadIdx.x < kOut) {
         double t = 0.0;
 #pragma unroll
         for (int w = 0; w < kGsWarps; ++w) t += wsum[w][threadIdx.x];
         partial[threadIdx.x * gridDim.x + blockIdx.x] = t;
     }
     if (last_block(ticket)) {
-        for (int q = warp; q < c; q += kGsWarps) {
+        for (int q = warp; q < kOut; q += kGsWarps) {
             double t = 0.0;
             for (int b = lane; b < static_cast<int>(gridDim.x); b += 32) t += partial[q * gridDim.x + b];
 #pragma unroll
@@ -293,66 +288,70 @@ __device__ __forceinline__ void grid_multi_sum(const double (&acc)[NMAX], int c,
     }
 }
 
-// out[q] = v_q . w for q < c, and out[c] = w . w (the Arnoldi action norm squared)
-__global__ void __launch_bounds__(kT) k_gs_first(int n, const double* __restrict__ V, int c,
+// The fused passes are instantiated for each basis count C (1..kChunk): the
+// per-vector accumulators and loads take exactly C registers' worth, so the
+// small counts of the first Arnoldi steps run at higher occupancy.
+
+// out[q] = v_q . w for q < C, and out[C] = w . w (the Arnoldi action norm squared)
+template <int C>
+__global__ void __launch_bounds__(kT) k_gs_first(int n, const double* __restrict__ V,
                                                  const double* __restrict__ w, double* partial, unsigned* ticket,
                                                  double* out) {
     pdl_entry();
-    double acc[kChunk];
+    double acc[C];
 #pragma unroll
-    for (int q = 0; q < kChunk; ++q) acc[q] = 0.0;
+    for (int q = 0; q < C; ++q) acc[q] = 0.0;
     double ww = 0.0;
     for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
         const double wk = w[k];
 #pragma unroll
-        for (int q = 0; q < kChunk; ++q)
-            if (q < c) acc[q] += V[static_cast<size_t>(q) * n + k] * wk;
+        for (int q = 0; q < C; ++q) acc[q] += V[static_cast<size_t>(q) * n + k] * wk;
         ww += wk * wk;
     }
-    grid_multi_sum<kChunk, true>(acc, c, ww, partial, ticket, out);
+    grid_multi_sum<C, true>(acc, ww, partial, ticket, out);
 }
 
-// w -= sum_{q<c} h[q] v_q (in q order per element), then out[q] = v_q . w over the updated w
-__global__ void __launch_bounds__(kT) k_gs_axpy_dot(int n, const double* __restrict__ V, int c, const double* h,
+// w -= sum_{q<C} h[q] v_q (in q order per element), then out[q] = v_q . w over the updated w
+template <int C>
+__global__ void __launch_bounds__(kT) k_gs_axpy_dot(int n, const double* __restrict__ V, const double* h,
                                                     double* __restrict__ w, double* partial, unsigned* ticket,
                                                     double* out) {
     pdl_entry();
-    __shared__ double hs[kChunk];
-    if (threadIdx.x < c) hs[threadIdx.x] = h[threadIdx.x];
+    __shared__ double hs[C];
+    if (threadIdx.x < C) hs[threadIdx.x] = h[threadIdx.x];
     __syncthreads();
-    double acc[kChunk];
+    double acc[C];
 #pragma unroll
-    for (int q = 0; q < kChunk; ++q) acc[q] = 0.0;
+    for (int q = 0; q < C; ++q) acc[q] = 0.0;
     for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
-        double vk[kChunk];
+        double vk[C];
         double wk = w[k];
 #pragma unroll
-        for (int q = 0; q < kChunk; ++q) {
-            vk[q] = q < c ? V[static_cast<size_t>(q) * n + k] : 0.0;
-            if (q < c) wk = wk - hs[q] * vk[q];
+        for (int q = 0; q < C; ++q) {
+            vk[q] = V[static_cast<size_t>(q) * n + k];
+            wk = wk - hs[q] * vk[q];
         }
         w[k] = wk;
 #pragma unroll
-        for (int q = 0; q < kChunk; ++q)
-            if (q < c) acc[q] += vk[q] * wk;
+        for (int q = 0; q < C; ++q) acc[q] += vk[q] * wk;
     }
-    grid_multi_sum<kChunk, false>(acc, c, 0.0, partial, ticket, out);
+    grid_multi_sum<C, false>(acc, 0.0, partial, ticket, out);
 }
 
-// w -= sum_{q<c} h[q] v_q, then *norm_out = sqrt(w . w) (NaN when not finite)
-__global__ void k_gs_axpy_norm(int n, const double* __restrict__ V, int c, const double* h,
-                               double* __restrict__ w, double* partial, unsigned* ticket, double* norm_out) {
+// w -= sum_{q<C} h[q] v_q, then *norm_out = sqrt(w . w) (NaN when not finite)
+template <int C>
+__global__ void k_gs_axpy_norm(int n, const double* __restrict__ V, const double* h, double* __restrict__ w,
+                               double* partial, unsigned* ticket, double* norm_out) {
     pdl_entry();
     __shared__ double sm[32];
-    __shared__ double hs[kChunk];
-    if (threadIdx.x < c) hs[threadIdx.x] = h[threadIdx.x];
+    __shared__ double hs[C];
+    if (threadIdx.x < C) hs[threadIdx.x] = h[threadIdx.x];
     __syncthreads();
     double ss = 0.0;
     for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
         double wk = w[k];
 #pragma unroll
-        for (int q = 0; q < kChunk; ++q)
-            if (q < c) wk = wk - hs[q] * V[static_cast<size_t>(q) * n + k];
+        for (int q = 0; q < C; ++q) wk = wk - hs[q] * V[static_cast<size_t>(q) * n + k];
         w[k] = wk;
         ss += wk * wk;
     }
@@ -366,6 +365,31 @@ __global__ void k_gs_axpy_norm(int n, const double* __restrict__ V, int c, const
             *norm_out = isfinite(t) ? sqrt(t) : nan("");
             *ticket = 0;
         }
+    }
+}
+
+// Blocks of kT threads of `kernel` resident on one SM (cached per kernel
+// instance: the answer depends only on the binary and the architecture).
+template <class K>
+int resident_per_sm(K kernel) {
+    static const int per_sm = [kernel] {
+        int b = 0;
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, kernel, kT, 0) != cudaSuccess) b = 1;
+        return std::max(1, b);
+    }();
+    return per_sm;
+}
+
+// Calls go(std::integral_constant<int, C>) for the basis count c in 1..kChunk.
+template <class Go>
+void with_basis_count(int c, Go&& go) {
+    switch (c) {
+#define CFDXG_GS_CASE(C) case C: go(std::integral_constant<int, C>{}); break;
+        CFDXG_GS_CASE(1) CFDXG_GS_CASE(2) CFDXG_GS_CASE(3) CFDXG_GS_CASE(4) CFDXG_GS_CASE(5) CFDXG_GS_CASE(6)
+        CFDXG_GS_CASE(7) CFDXG_GS_CASE(8) CFDXG_GS_CASE(9) CFDXG_GS_CASE(10) CFDXG_GS_CASE(11)
+        CFDXG_GS_CASE(12) CFDXG_GS_CASE(13) CFDXG_GS_CASE(14) CFDXG_GS_CASE(15) CFDXG_GS_CASE(16)
+#undef CFDXG_GS_CASE
+        default: throw Error(CFDXG_ERR_INVALID_ARGUMENT, "Gram-Schmidt basis count out of range");
     }
 }
 
@@ -587,26 +611,34 @@ public:
     // (count <= kChunk) in three passes over the basis: h1 = V^T w (with the
     // action norm), w -= V h1 fused with h2 = V^T w, w -= V h2 fused with
     // ||w||.  Fills slots kH1.., kH2.., kAction and kHnext.
-    int gsb() const { return std::min(kGsBlocksPerSm * ctx_->sm_count, blocks_for(n_, kT)); }
+    // One resident wave of each pass (a fixed partition for a given count and
+    // GPU, so the sums stay deterministic).
+    template <class K>
+    int gs_grid(K kernel) const {
+        return std::min({resident_per_sm(kernel) * ctx_->sm_count, kMaxReduceBlocks, blocks_for(n_, kT)});
+    }
     void gram_schmidt_cgs2_fused(const double* V, int count, double* w, double* mpartial) {
-        {
-            ProfScope ps(ctx_, "gram_schmidt_dot", (count + 1.0) * nb());
-            launch_pdl(ctx_->stream, k_gs_first, wb(), kT, n_, V, count, static_cast<const double*>(w), mpartial,
-                       ctx_->scratch.ticket, slot(kH1));
-            check_launch(ctx_);
-        }
-        {
-            ProfScope ps(ctx_, "gram_schmidt_axpy_dot", (count + 2.0) * nb());
-            launch_pdl(ctx_->stream, k_gs_axpy_dot, gsb(), kT, n_, V, count, static_cast<const double*>(slot(kH1)), w,
-                       mpartial, ctx_->scratch.ticket, slot(kH2));
-            check_launch(ctx_);
-        }
-        {
-            ProfScope ps(ctx_, "gram_schmidt_axpy_norm", (count + 2.0) * nb());
-            launch_pdl(ctx_->stream, k_gs_axpy_norm, wb(), kT, n_, V, count, static_cast<const double*>(slot(kH2)),
-                       w, ctx_->scratch.partial, ctx_->scratch.ticket, slot(kHnext));
-            check_launch(ctx_);
-        }
+        with_basis_count(count, [&](auto cc) {
+            constexpr int C = decltype(cc)::value;
+            {
+                ProfScope ps(ctx_, "gram_schmidt_dot", (count + 1.0) * nb());
+                launch_pdl(ctx_->stream, k_gs_first<C>, gs_grid(k_gs_first<C>), kT, n_, V, static_cast<const double*>(w), mpartial,
+                           ctx_->scratch.ticket, slot(kH1));
+                check_launch(ctx_);
+            }
+            {
+                ProfScope ps(ctx_, "gram_schmidt_axpy_dot", (count + 2.0) * nb());
+                launch_pdl(ctx_->stream, k_gs_axpy_dot<C>, gs_grid(k_gs_axpy_dot<C>), kT, n_, V, static_cast<const double*>(slot(kH1)),
+                           w, mpartial, ctx_->scratch.ticket, slot(kH2));
+                check_launch(ctx_);
+            }
+            {
+                ProfScope ps(ctx_, "gram_schmidt_axpy_norm", (count + 2.0) * nb());
+                launch_pdl(ctx_->stream, k_gs_axpy_norm<C>, gs_grid(k_gs_axpy_norm<C>), kT, n_, V, static_cast<const double*>(slot(kH2)),
+                           w, ctx_->scratch.partial, ctx_->scratch.ticket, slot(kHnext));
+                check_launch(ctx_);
+            }
+        });
     }
     void sqrt_slot(int from, int to) {
         k_sqrt_slot<<<1, 1, 0, ctx_->stream>>>(slot(from), slot(to));
