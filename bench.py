@@ -126,13 +126,25 @@ class ClockSampler:
         self.path = Path(os.environ.get("TMPDIR", "/tmp")) / f"cfdxg_clocks_{os.getpid()}.csv"
 
     def start(self):
+        """Starts sampling every 50 ms and returns once the first sample is in
+        (nvidia-smi takes ~0.1-0.3 s to start; the timed region of one form is
+        ~0.2 s), so that the samples after this call fall in the timed region."""
+        self.skip = 0
         try:
             self.fh = open(self.path, "w")
             self.proc = subprocess.Popen(
-                ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits", "-lms", "200",
+                ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits", "-lms", "50",
                  "-i", str(self.device)], stdout=self.fh, stderr=subprocess.DEVNULL)
         except Exception:
             self.proc = None
+            return
+        t0 = time.time()
+        while time.time() - t0 < 5.0 and self.proc.poll() is None:
+            n = len(self.path.read_text().splitlines())
+            if n:
+                self.skip = n
+                break
+            time.sleep(0.01)
 
     def stop(self):
         if not self.proc:
@@ -145,7 +157,10 @@ class ClockSampler:
         self.fh.close()
         sm, smax, reasons = [], None, set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for line in self.path.read_text().splitlines():
+        lines = self.path.read_text().splitlines()
+        # the samples taken after start() returned; the one before, if none came later
+        window = lines[self.skip:] or lines[-1:]
+        for line in window:
             parts = [p.strip() for p in line.split(",")]
             if len(parts) < 9:
                 continue

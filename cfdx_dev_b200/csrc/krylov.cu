@@ -368,13 +368,13 @@ __global__ void k_gs_axpy_norm(int n, const double* __restrict__ V, const double
     }
 }
 
-// Blocks of kT threads of `kernel` resident on one SM (cached per kernel
+// Blocks of kT threads of the kernel K resident on one SM (cached per kernel
 // instance: the answer depends only on the binary and the architecture).
-template <class K>
-int resident_per_sm(K kernel) {
-    static const int per_sm = [kernel] {
+template <auto K>
+int resident_per_sm() {
+    static const int per_sm = [] {
         int b = 0;
-        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, kernel, kT, 0) != cudaSuccess) b = 1;
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, K, kT, 0) != cudaSuccess) b = 1;
         return std::max(1, b);
     }();
     return per_sm;
@@ -613,28 +613,28 @@ public:
     // ||w||.  Fills slots kH1.., kH2.., kAction and kHnext.
     // One resident wave of each pass (a fixed partition for a given count and
     // GPU, so the sums stay deterministic).
-    template <class K>
-    int gs_grid(K kernel) const {
-        return std::min({resident_per_sm(kernel) * ctx_->sm_count, kMaxReduceBlocks, blocks_for(n_, kT)});
+    template <auto K>
+    int gs_grid() const {
+        return std::min({resident_per_sm<K>() * ctx_->sm_count, kMaxReduceBlocks, blocks_for(n_, kT)});
     }
     void gram_schmidt_cgs2_fused(const double* V, int count, double* w, double* mpartial) {
         with_basis_count(count, [&](auto cc) {
             constexpr int C = decltype(cc)::value;
             {
                 ProfScope ps(ctx_, "gram_schmidt_dot", (count + 1.0) * nb());
-                launch_pdl(ctx_->stream, k_gs_first<C>, gs_grid(k_gs_first<C>), kT, n_, V, static_cast<const double*>(w), mpartial,
+                launch_pdl(ctx_->stream, k_gs_first<C>, gs_grid<k_gs_first<C>>(), kT, n_, V, static_cast<const double*>(w), mpartial,
                            ctx_->scratch.ticket, slot(kH1));
                 check_launch(ctx_);
             }
             {
                 ProfScope ps(ctx_, "gram_schmidt_axpy_dot", (count + 2.0) * nb());
-                launch_pdl(ctx_->stream, k_gs_axpy_dot<C>, gs_grid(k_gs_axpy_dot<C>), kT, n_, V, static_cast<const double*>(slot(kH1)),
+                launch_pdl(ctx_->stream, k_gs_axpy_dot<C>, gs_grid<k_gs_axpy_dot<C>>(), kT, n_, V, static_cast<const double*>(slot(kH1)),
                            w, mpartial, ctx_->scratch.ticket, slot(kH2));
                 check_launch(ctx_);
             }
             {
                 ProfScope ps(ctx_, "gram_schmidt_axpy_norm", (count + 2.0) * nb());
-                launch_pdl(ctx_->stream, k_gs_axpy_norm<C>, gs_grid(k_gs_axpy_norm<C>), kT, n_, V, static_cast<const double*>(slot(kH2)),
+                launch_pdl(ctx_->stream, k_gs_axpy_norm<C>, gs_grid<k_gs_axpy_norm<C>>(), kT, n_, V, static_cast<const double*>(slot(kH2)),
                            w, ctx_->scratch.partial, ctx_->scratch.ticket, slot(kHnext));
                 check_launch(ctx_);
             }
