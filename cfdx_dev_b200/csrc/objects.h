@@ -66,6 +66,7 @@ struct DevHierarchy {
     std::shared_ptr<void> solver;
     DevBuf<double> lu_a, lu_x, lu_work;
     DevBuf<int> lu_ipiv, lu_info;
+    bool dense_cholesky = false;   // the last inverse came from a Cholesky factor (symmetric level)
     // constant null space: the cycle's mean removals (in index order with
     // reference_order) and the bordered coarsest solve
     bool null_space = false;

@@ -24,6 +24,8 @@
 #include <cusolverDn.h>
 
 #include <cmath>
+#include <cstdio>
+#include <cstdlib>
 #include <limits>
 #include <type_traits>
 
@@ -430,6 +432,32 @@ __global__ void k_dense_block_copy(int n, int ld, const double* __restrict__ a, 
     b[idx] = static_cast<S>(a[i * ld + j]);
 }
 
+// flag = 1 when the N x N matrix a is not symmetric: |a_ij - a_ji| above
+// 1e-12 of the pair's magnitude plus 1e-14 of sqrt(|a_ii a_jj|) (the coarse
+// Galerkin operators of a symmetric system differ from symmetry only by the
+// rounding of their sums, which leaves entries cancelled to near zero with
+// differences far above their own size but far below the diagonal's)
+__global__ void k_symmetry_check(int N, const double* __restrict__ a, int* flag) {
+    const int64_t idx = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (idx >= static_cast<int64_t>(N) * N) return;
+    const int64_t i = idx / N, j = idx % N;
+    if (j <= i) return;
+    const double x = a[i * N + j], y = a[j * N + i];
+    const double scale = sqrt(fabs(a[i * N + i]) * fabs(a[j * N + j]));
+    if (!(fabs(x - y) <= 1e-12 * (fabs(x) + fabs(y)) + 1e-14 * scale)) atomicOr(flag, 1);
+}
+
+// b (n x n, row-major) = the symmetric matrix whose lower triangle is held
+// column-major in a (leading dimension ld)
+template <class S>
+__global__ void k_dense_sym_copy(int n, int ld, const double* __restrict__ a, S* __restrict__ b) {
+    const int64_t idx = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (idx >= static_cast<int64_t>(n) * n) return;
+    const int64_t i = idx / n, j = idx % n;
+    const int64_t lo = i < j ? i : j, hi = i < j ? j : i;
+    b[idx] = static_cast<S>(a[lo * ld + hi]);
+}
+
 #define CFDXG_TPR_SWITCH(tpr, ...)                            \
     switch (tpr) {                                               \
         case 1: { constexpr int TPR = 1; __VA_ARGS__; } break;   \
@@ -704,17 +732,18 @@ void build_dense_inverse_dev(cfdxg_context* ctx, DevHierarchy<T>& d, int n, cons
     DevBuf<double>& at = d.lu_a;
     DevBuf<double>& x = d.lu_x;
     at.resize(NN);
-    x.resize(NN);
     d.lu_ipiv.resize(N);
-    d.lu_info.resize(1);
+    d.lu_info.resize(2);
     if (d.dense_fp64) d.dense64.resize(nn);
     else d.dense.resize(nn);
     cudaStream_t s = ctx->stream;
-    CFDXG_CUDA(cudaMemsetAsync(at.get(), 0, sizeof(double) * NN, s));
-    k_dense_init_t<<<blocks_for(n, kT), kT, 0, s>>>(n, N, ro, co, va, d.null_space ? 1 : 0, at.get());
-    check_launch(ctx);
-    k_identity<<<blocks_for(static_cast<int64_t>(NN), kT), kT, 0, s>>>(N, x.get());
-    check_launch(ctx);
+    const int64_t grid_nn = blocks_for(static_cast<int64_t>(NN), kT);
+    auto init = [&] {
+        CFDXG_CUDA(cudaMemsetAsync(at.get(), 0, sizeof(double) * NN, s));
+        k_dense_init_t<<<blocks_for(n, kT), kT, 0, s>>>(n, N, ro, co, va, d.null_space ? 1 : 0, at.get());
+        check_launch(ctx);
+    };
+    init();
     if (!d.solver) {
         cusolverDnHandle_t created = nullptr;
         if (cusolverDnCreate(&created) != CUSOLVER_STATUS_SUCCESS)
@@ -723,20 +752,73 @@ void build_dense_inverse_dev(cfdxg_context* ctx, DevHierarchy<T>& d, int n, cons
     }
     cusolverDnHandle_t h = static_cast<cusolverDnHandle_t>(d.solver.get());
     if (cusolverDnSetStream(h, s) != CUSOLVER_STATUS_SUCCESS) throw Error(CFDXG_ERR_CUDA, "cusolverDnSetStream failed");
+    int* info = d.lu_info.get();
+    int host_info[2] = {0, 0};
+    // A symmetric level (no border) is inverted by Cholesky: potrf, then potri
+    // on the factor -- a third of the LU route's flops (getrf, then getrs on the
+    // identity).  A level that is not symmetric, or not positive definite,
+    // takes the LU route.
+    if (!d.null_space) {
+        CFDXG_CUDA(cudaMemsetAsync(info + 1, 0, sizeof(int), s));
+        k_symmetry_check<<<grid_nn, kT, 0, s>>>(N, at.get(), info + 1);
+        check_launch(ctx);
+        CFDXG_CUDA(cudaMemcpyAsync(&host_info[1], info + 1, sizeof(int), cudaMemcpyDeviceToHost, s));
+        CFDXG_CUDA(cudaStreamSynchronize(s));
+        if (host_info[1] == 0) {
+            int lw1 = 0, lw2 = 0;
+            if (cusolverDnDpotrf_bufferSize(h, CUBLAS_FILL_MODE_LOWER, N, at.get(), N, &lw1) !=
+                    CUSOLVER_STATUS_SUCCESS ||
+                cusolverDnDpotri_bufferSize(h, CUBLAS_FILL_MODE_LOWER, N, at.get(), N, &lw2) !=
+                    CUSOLVER_STATUS_SUCCESS)
+                throw Error(CFDXG_ERR_CUDA, "cusolverDnDpotrf/potri_bufferSize failed");
+            const int lwork = std::max({lw1, lw2, 1});
+            if (static_cast<int64_t>(d.lu_work.size()) < lwork) d.lu_work.resize(static_cast<std::size_t>(lwork));
+            if (cusolverDnDpotrf(h, CUBLAS_FILL_MODE_LOWER, N, at.get(), N, d.lu_work.get(), lwork, info) !=
+                CUSOLVER_STATUS_SUCCESS)
+                throw Error(CFDXG_ERR_CUDA, "dense coarse Cholesky failed");
+            CFDXG_CUDA(cudaMemcpyAsync(&host_info[0], info, sizeof(int), cudaMemcpyDeviceToHost, s));
+            CFDXG_CUDA(cudaStreamSynchronize(s));
+            if (host_info[0] == 0) {
+                if (cusolverDnDpotri(h, CUBLAS_FILL_MODE_LOWER, N, at.get(), N, d.lu_work.get(), lwork, info) !=
+                    CUSOLVER_STATUS_SUCCESS)
+                    throw Error(CFDXG_ERR_CUDA, "dense coarse Cholesky inverse failed");
+                CFDXG_CUDA(cudaMemcpyAsync(&host_info[0], info, sizeof(int), cudaMemcpyDeviceToHost, s));
+                if (d.dense_fp64)
+                    k_dense_sym_copy<double><<<blocks_for(static_cast<int64_t>(nn), kT), kT, 0, s>>>(
+                        n, N, at.get(), d.dense64.get());
+                else
+                    k_dense_sym_copy<float><<<blocks_for(static_cast<int64_t>(nn), kT), kT, 0, s>>>(
+                        n, N, at.get(), d.dense.get());
+                check_launch(ctx);
+                CFDXG_CUDA(cudaStreamSynchronize(s));
+                if (host_info[0] != 0)
+                    throw Error(CFDXG_ERR_SETUP, "dense coarse level is singular (Cholesky inverse " +
+                                                     std::to_string(host_info[0]) + ")");
+                d.dense_cholesky = true;
+                if (std::getenv("CFDXG_SETUP_PROFILE"))
+                    std::fprintf(stderr, "[cfdxg setup] dense coarse inverse of %d rows by Cholesky\n", N);
+                return;
+            }
+            init();   // not positive definite: the factor overwrote the matrix
+        }
+    }
+    d.dense_cholesky = false;
+    if (std::getenv("CFDXG_SETUP_PROFILE"))
+        std::fprintf(stderr, "[cfdxg setup] dense coarse inverse of %d rows by LU (%s)\n", N,
+                     d.null_space ? "bordered" : (host_info[1] ? "not symmetric" : "not positive definite"));
+    x.resize(NN);
+    k_identity<<<grid_nn, kT, 0, s>>>(N, x.get());
+    check_launch(ctx);
     int lwork = 0;
     if (cusolverDnDgetrf_bufferSize(h, N, N, at.get(), N, &lwork) != CUSOLVER_STATUS_SUCCESS)
         throw Error(CFDXG_ERR_CUDA, "cusolverDnDgetrf_bufferSize failed");
     if (static_cast<int64_t>(d.lu_work.size()) < std::max(lwork, 1)) d.lu_work.resize(static_cast<std::size_t>(std::max(lwork, 1)));
-    DevBuf<double>& work = d.lu_work;
-    DevBuf<int>& ipiv = d.lu_ipiv;
-    DevBuf<int>& info = d.lu_info;
     // at holds A^T column-major: factor it, then solve A^T X = I
-    if (cusolverDnDgetrf(h, N, N, at.get(), N, work.get(), ipiv.get(), info.get()) != CUSOLVER_STATUS_SUCCESS ||
-        cusolverDnDgetrs(h, CUBLAS_OP_N, N, N, at.get(), N, ipiv.get(), x.get(), N, info.get()) !=
+    if (cusolverDnDgetrf(h, N, N, at.get(), N, d.lu_work.get(), d.lu_ipiv.get(), info) != CUSOLVER_STATUS_SUCCESS ||
+        cusolverDnDgetrs(h, CUBLAS_OP_N, N, N, at.get(), N, d.lu_ipiv.get(), x.get(), N, info) !=
             CUSOLVER_STATUS_SUCCESS)
         throw Error(CFDXG_ERR_CUDA, "dense coarse LU failed");
-    int host_info = 0;
-    CFDXG_CUDA(cudaMemcpyAsync(&host_info, info.get(), sizeof(int), cudaMemcpyDeviceToHost, s));
+    CFDXG_CUDA(cudaMemcpyAsync(&host_info[0], info, sizeof(int), cudaMemcpyDeviceToHost, s));
     if (d.dense_fp64)
         k_dense_block_copy<double><<<blocks_for(static_cast<int64_t>(nn), kT), kT, 0, s>>>(n, N, x.get(),
                                                                                          d.dense64.get());
@@ -745,8 +827,8 @@ void build_dense_inverse_dev(cfdxg_context* ctx, DevHierarchy<T>& d, int n, cons
                                                                                         d.dense.get());
     check_launch(ctx);
     CFDXG_CUDA(cudaStreamSynchronize(s));
-    if (host_info != 0) throw Error(CFDXG_ERR_SETUP, "dense coarse level is singular (LU pivot " +
-                                                         std::to_string(host_info) + ")");
+    if (host_info[0] != 0) throw Error(CFDXG_ERR_SETUP, "dense coarse level is singular (LU pivot " +
+                                                            std::to_string(host_info[0]) + ")");
 }
 
 template <class T>

@@ -212,8 +212,8 @@ int cfdxg_rhie_chow_flux(cfdxg_context* ctx, cfdxg_mesh* mesh, const double* Hby
  * patch).  Each call makes the context's device current, looks up the
  * array's device address in that context (cudaGetSymbolAddress, which
  * allocates nothing) and gives the caller's current device back before it
- * returns.  The first call on a device can load the library's device code,
- * so make that first call before any stream capture.  All calls share the
+ * returns.  The first call on a device can load the library's device code.
+ * All calls share the
  * array and it keeps the last call's contents; every call overwrites what it
  * reads, but calls that overlap on the GPU (two streams or threads at once)
  * race on it. */
