@@ -74,6 +74,30 @@ def test_pressure_assembly_bit_exact(ctx, oracle, tet_setup):
     assert np.array_equal(grad, r["grad_p"])
 
 
+@pytest.mark.parametrize("kind", ["hex", "bl", "prism"])
+def test_pressure_assembly_other_cells_bit_exact(ctx, oracle, kind):
+    # hexahedra take the assembly's form unrolled for six faces, the five-face
+    # prisms its general form; p != 0 and a non-zero fixed value, so every
+    # term is live
+    m = {"hex": lambda: cases.poisson_case(7)[0], "bl": lambda: cg.boundary_layer_case(9, 7, 5),
+         "prism": lambda: cases.prism_case(6, 5, 4)}[kind]()
+    mesh = cg.Mesh(ctx, m)
+    g = mesh.geometry()
+    U, rAU, aP, p, fixed, value = cases.simple_fields(m, g["cell_centres"])
+    cc = g["cell_centres"].reshape(3, -1)
+    p1 = np.cos(2 * cc[0]) + cc[1] * cc[2]
+    value1 = value.copy()
+    value1[0] = -0.5
+    A, b, phi, grad = cg.assemble_pressure_correction(mesh, U, rAU, p1, 1.1, fixed, value1)
+    r = oracle.simple_assemble(m, U, rAU, p1, 1.1, fixed, value1)
+    ro, co, va = A.to_csr()
+    assert np.array_equal(ro, r["row_offsets"]) and np.array_equal(co, r["columns"])
+    assert np.array_equal(va, r["values"])
+    assert np.array_equal(b, r["b"])
+    assert np.array_equal(phi, r["phiHbyA"])
+    assert np.array_equal(grad, r["grad_p"])
+
+
 def test_pressure_assembly_nonzero_pressure_bit_exact(ctx, oracle, tet_setup):
     # a later corrector: p != 0, so the gradient and deferred fluxes are active
     m, mesh, g, (U, rAU, aP, p, fixed, value) = tet_setup

@@ -26,11 +26,11 @@ def _pressure_inputs(n, seed_offset=0):
     return m, g, U, rAU, p, fixed, value
 
 
-@pytest.mark.parametrize("kind", ["hex", "tet", "bl"])
+@pytest.mark.parametrize("kind", ["hex", "tet", "bl", "prism"])
 def test_geometry_matches_reference(ref, kind):
     import cfdx_dev_b200 as cg
     m = {"hex": lambda: cases.poisson_case(5)[0], "tet": lambda: cases.simple_mesh(5),
-         "bl": lambda: cg.boundary_layer_case(6, 5, 4)}[kind]()
+         "bl": lambda: cg.boundary_layer_case(6, 5, 4), "prism": lambda: cases.prism_case(4, 3, 3)}[kind]()
     mine = co.geometry(m)
     for which in ("fv", "cache"):   # build_fv_geometry and compute_geometry_cache agree
         theirs = ref.geometry(m, which)
@@ -55,6 +55,24 @@ def test_pressure_assembly_and_flux_match_reference(ref, nonzero_p):
     assert np.array_equal(co.gauss_gradient(m, p, fixed, value), ref.gauss_gradient(m, p, fixed, value))
     assert np.array_equal(co.rhie_chow_flux(m, U, rAU, p, rho, fixed, value),
                           ref.rhie_chow_flux(m, U, rAU, p, rho, fixed, value))
+
+
+@pytest.mark.parametrize("kind", ["hex", "prism"])
+def test_pressure_assembly_on_other_cells_matches_reference(ref, kind):
+    # six- and five-face cells (the GPU assembly's unrolled and general forms)
+    m = cases.poisson_case(5)[0] if kind == "hex" else cases.prism_case(4, 3, 3)
+    g = co.geometry(m)
+    U, rAU, aP, p, fixed, value = cases.simple_fields(m, g["cell_centres"])
+    cc = g["cell_centres"].reshape(3, -1)
+    p = np.cos(2 * cc[0]) + cc[1] * cc[2]
+    value = value.copy()
+    value[0] = -0.5
+    a = co.simple_assemble(m, U, rAU, p, 1.1, fixed, value)
+    b = ref.simple_assemble(m, U, rAU, p, 1.1, fixed, value)
+    for k in ("row_offsets", "columns", "values", "b", "phiHbyA", "grad_p"):
+        assert np.array_equal(a[k], b[k]), k
+    assert np.array_equal(co.rhie_chow_flux(m, U, rAU, p, 1.1, fixed, value),
+                          ref.rhie_chow_flux(m, U, rAU, p, 1.1, fixed, value))
 
 
 def test_poisson_assembly_matches_reference(ref):
