@@ -713,13 +713,15 @@ void upload_level(cfdxg_context* ctx, DevLevel<T>& D, const AmgLevel& H, bool wi
     }
 }
 
-// The dense coarse level's inverse, formed in FP64 from its device CSR by LU
-// with partial pivoting (cuSOLVER getrf, then getrs on the identity) and
-// stored FP32 (or FP64 with dense_fp64).  A singular level sets the status
-// word's non-finite flag.  This is set-up work (once per setup and per
-// numeric refresh); the cycle applies the stored inverse with its own kernel.
-// (The earlier one-column-per-step Gauss-Jordan took 1.5 s at 5,287 rows:
-// every pivot step read and wrote the whole n x 2n augmented matrix.)
+// The dense coarse level's inverse, formed in FP64 from its device CSR --
+// by Cholesky (cuSOLVER potrf, then potri) when the level is symmetric and
+// positive definite, else by LU with partial pivoting (getrf, then getrs on
+// the identity) -- and stored FP32 (or FP64 with dense_fp64).  A singular
+// level fails the setup (CFDXG_ERR_SETUP).  This is set-up work (once per
+// setup and per numeric refresh); the cycle applies the stored inverse with
+// its own kernel.  (The earlier one-column-per-step Gauss-Jordan took 1.5 s
+// at 5,287 rows: every pivot step read and wrote the whole n x 2n augmented
+// matrix.)
 template <class T>
 void build_dense_inverse_dev(cfdxg_context* ctx, DevHierarchy<T>& d, int n, const int* ro, const int* co,
                              const double* va) {
