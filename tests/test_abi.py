@@ -36,6 +36,20 @@ def test_host_only_calls_need_no_device():
     assert amg.name() == "NativeBoomerStyleAMG"
 
 
+def test_amg_option_defaults():
+    """cfdxg_amg_options_default: the reference's smoother and coarsening
+    parameters, and the FP32 cycle's own defaults (host-only, no device)."""
+    import ctypes as C
+    from cfdx_dev_b200 import _native as N
+    o = N.AmgOptions()
+    assert N.load().cfdxg_amg_options_default(C.byref(o)) == 0
+    assert (o.omega, o.strength_threshold, o.max_levels) == (0.7, 0.25, 25)
+    assert (o.pre_sweeps, o.post_sweeps, o.coarse_pre_sweeps, o.coarse_post_sweeps) == (-1, -1, -1, -1)
+    assert (o.coarse_dense_limit, o.narrow_columns, o.half_values, o.dense_fp64) == (6000, 1, 1, 0)
+    assert (o.reference_order, o.constant_null_space) == (0, 0)
+    assert o.coarse_drop_tolerance == 0.02
+
+
 def test_amg_options_are_validated():
     """cfdxg_amg_create refuses out-of-range options (host-only, no device)."""
     import cfdx_dev_b200 as cg
