@@ -83,8 +83,14 @@ def test_poisson_assembly_matches_reference(ref):
     assert np.array_equal(va, r_va) and np.array_equal(rhs, r_rhs)
 
 
-def test_spmv_vcycle_and_solve_match_reference(ref):
-    m, g, U, rAU, p, fixed, value = _pressure_inputs(7)
+@pytest.mark.parametrize("mesh", ["tet", "prism"])
+def test_spmv_vcycle_and_solve_match_reference(ref, mesh):
+    if mesh == "tet":
+        m, g, U, rAU, p, fixed, value = _pressure_inputs(7)
+    else:   # five-face cells
+        m = cases.prism_case(9, 8, 7)
+        g = co.geometry(m)
+        U, rAU, aP, p, fixed, value = cases.simple_fields(m, g["cell_centres"])
     A = co.simple_assemble(m, U, rAU, p, 1.0, fixed, value)
     ro, cols, va, b = A["row_offsets"], A["columns"], A["values"], A["b"]
     x = np.random.default_rng(5).standard_normal(ro.size - 1)
