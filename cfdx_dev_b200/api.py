@@ -409,8 +409,14 @@ def gauss_gradient_with_boundary(mesh: Mesh, p, p_bc_fixed=None, p_bc_value=None
 class NativeBoomerAMGPreconditioner:
     """Native classical RS AMG (core/linalg/hypre_amg.h:106), GPU V-cycle.
 
-    ``precision="fp32_vcycle"`` runs the V-cycle in FP32 with an FP64 dense
-    coarse solve (the hierarchy itself is identical)."""
+    ``precision="fp32_vcycle"`` runs the V-cycle in FP32 with a dense coarse
+    inverse formed in FP64 (the hierarchy itself is identical); between the
+    fine and the coarsest level it smooths with sparsified copies of the
+    Galerkin operators (``coarse_drop_tolerance``, default 0.02: each row's
+    diagonal and its entries of at least that fraction of the row's largest
+    off-diagonal magnitude, the rest added to the diagonal; 0 smooths with
+    the Galerkin operators).  Other keyword options are the fields of
+    ``cfdxg_amg_options`` (include/cfdxg.h)."""
 
     def __init__(self, ctx: Context | None = None, precision: str = "fp64", require_smoother_certificate=False,
                  **options):
